@@ -1,0 +1,193 @@
+"""ctypes binding of the C ABI (include/cumpm_b200.h) with PyTorch at the edge.
+
+``Field`` wraps the batched field operator on device buffers: moments and
+fields are complex128 CUDA tensors of shape (rows, M), rows = 3N (+5Nq), the
+same [row][M] layout the kernels use; self coefficients are (N, M).
+``batch_solve`` runs the batched device Krylov solve on such tensors.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _load
+
+_dp = C.POINTER(C.c_double)
+_ip = C.POINTER(C.c_int)
+
+MPM_OK, MPM_ERR_INVALID, MPM_ERR_RUNTIME, MPM_ERR_CUDA = 0, 1, 2, 3
+FIELD_DIRECT, FIELD_MONO = 0, 1
+MODE_SOLVER_AX, MODE_INTERACTION = 0, 1
+METHOD_GMRES, METHOD_BICGSTAB = 0, 1
+
+# every symbol the header declares (checked by the CPU test suite)
+EXPORTS = [
+    "mpm_last_error", "mpm_version",
+    "mpm_solver_create", "mpm_solver_destroy", "mpm_solver_compute", "mpm_solver_dims",
+    "mpm_solver_get_dipoles", "mpm_solver_get_quadrupoles", "mpm_solver_get_eff_polarizability",
+    "mpm_solver_set_jacobi", "mpm_solver_get_jacobi", "mpm_solver_set_options", "mpm_solver_iterations",
+    "mpm_near_create", "mpm_near_destroy", "mpm_near_set_dipoles", "mpm_near_set_dipole_positions",
+    "mpm_near_set_field_points", "mpm_near_calculate",
+    "mpm_field_create", "mpm_field_destroy", "mpm_field_set_positions", "mpm_field_set_field_points",
+    "mpm_field_apply", "mpm_field_apply_part", "mpm_field_info_get", "mpm_batch_solve",
+    "mpm_mono_tables", "mpm_ewald_geometry",
+]
+
+
+class SolveOptions(C.Structure):
+    _fields_ = [("method", C.c_int), ("restart", C.c_int), ("maxiter", C.c_int), ("tol", C.c_double),
+                ("jacobi", C.c_int), ("recip_fp32", C.c_int), ("real_fp32", C.c_int), ("refine", C.c_int),
+                ("inner_tol", C.c_double)]
+
+
+class SolveReport(C.Structure):
+    _fields_ = [("matvecs", C.c_int), ("refine_steps", C.c_int), ("total_iterations", C.c_int),
+                ("max_iterations", C.c_int), ("num_converged", C.c_int), ("max_rel_resid", C.c_double)]
+
+
+class FieldInfo(C.Structure):
+    _fields_ = [("kind", C.c_int), ("mode", C.c_int), ("num_particles", C.c_int), ("num_targets", C.c_int),
+                ("num_quads", C.c_int), ("grid", C.c_int * 3), ("stencil", C.c_int), ("pruned", C.c_int),
+                ("z_slots", C.c_int), ("num_pairs", C.c_longlong), ("rc", C.c_double), ("h", C.c_double * 3),
+                ("eta", C.c_double * 3), ("selfo", C.c_double)]
+
+
+def lib():
+    L = _load.library()
+    if not getattr(L, "_mpm_typed", False):
+        L.mpm_last_error.restype = C.c_char_p
+        L.mpm_version.restype = C.c_char_p
+        L.mpm_field_create.argtypes = [C.POINTER(C.c_void_p), C.c_int, C.c_int, _dp, C.c_double, C.c_double, _dp,
+                                       C.c_int, C.c_int, _ip, C.c_int]
+        L.mpm_field_destroy.argtypes = [C.c_void_p]
+        L.mpm_field_set_positions.argtypes = [C.c_void_p, _dp, _dp, _dp, C.c_int, C.c_void_p]
+        L.mpm_field_set_field_points.argtypes = [C.c_void_p, _dp, _dp, _dp, C.c_int, C.c_void_p]
+        L.mpm_field_apply.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_int, C.c_int,
+                                      C.c_int, C.c_void_p]
+        L.mpm_field_apply_part.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_int,
+                                           C.c_int, C.c_int, C.c_void_p]
+        L.mpm_field_info_get.argtypes = [C.c_void_p, C.POINTER(FieldInfo)]
+        L.mpm_batch_solve.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p,
+                                      C.POINTER(SolveOptions), C.POINTER(SolveReport), C.c_void_p]
+        L.mpm_mono_tables.argtypes = [C.c_double, _dp, _dp, _dp]
+        L.mpm_ewald_geometry.argtypes = [_dp, C.c_double, C.c_double, _ip, _ip, _dp, _dp, _dp]
+        L._mpm_typed = True
+    return L
+
+
+def check(status):
+    if status != MPM_OK:
+        msg = lib().mpm_last_error().decode()
+        if status == MPM_ERR_INVALID:
+            raise ValueError(msg)
+        raise RuntimeError(msg)
+
+
+def _arr(a, dtype=np.float64):
+    a = np.ascontiguousarray(a, dtype=dtype)
+    return a, a.ctypes.data_as(_dp if dtype == np.float64 else _ip)
+
+
+def mono_tables(xi):
+    """Host-side real-space tables: (r, {name: values}, selfo, self_grad)."""
+    out = np.zeros(10 * 9001)
+    so, sg = C.c_double(), C.c_double()
+    check(lib().mpm_mono_tables(float(xi), out.ctypes.data_as(_dp), C.byref(so), C.byref(sg)))
+    out = out.reshape(10, 9001)
+    names = ["fd1", "fd2", "fq1", "fq2", "fq3", "gq1", "gq2", "gq3", "gq4"]
+    return out[0], {n: out[i + 1] for i, n in enumerate(names)}, so.value, sg.value
+
+
+def ewald_geometry(box, errortol, xi):
+    b, bp = _arr(box)
+    grid = (C.c_int * 3)()
+    st = C.c_int()
+    rc = C.c_double()
+    h = (C.c_double * 3)()
+    eta = (C.c_double * 3)()
+    check(lib().mpm_ewald_geometry(bp, float(errortol), float(xi), grid, C.byref(st), C.byref(rc), h, eta))
+    return dict(grid=list(grid), stencil=st.value, rc=rc.value, h=list(h), eta=list(eta))
+
+
+def _stream_ptr(stream):
+    if stream is None:
+        import torch
+        stream = torch.cuda.current_stream()
+    return C.c_void_p(stream.cuda_stream)
+
+
+class Field:
+    """Batched field operator A(omega) on CUDA tensors (see module docstring)."""
+
+    def __init__(self, kind, box=None, errortol=1e-3, xi=0.5, mode=MODE_SOLVER_AX, radius=None, quad_idxs=None,
+                 solve_quads=False):
+        L = lib()
+        self._h = C.c_void_p()
+        bx, bp = _arr(box if box is not None else [0.0, 0.0, 0.0])
+        rad = None if radius is None else np.ascontiguousarray(radius, dtype=np.float64)
+        qi = None if quad_idxs is None else np.ascontiguousarray(quad_idxs, dtype=np.int32)
+        check(L.mpm_field_create(C.byref(self._h), int(kind), int(mode), bp, float(errortol), float(xi),
+                                 None if rad is None else rad.ctypes.data_as(_dp), 0 if rad is None else len(rad),
+                                 int(bool(solve_quads) or qi is not None),
+                                 None if qi is None else qi.ctypes.data_as(_ip), 0 if qi is None else len(qi)))
+        self.kind = kind
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            try:
+                lib().mpm_field_destroy(h)
+            except Exception:  # interpreter shutdown: module globals already cleared
+                pass
+            self._h = None
+
+    def set_positions(self, pos, stream=None):
+        p = np.ascontiguousarray(np.asarray(pos, dtype=np.float64))
+        x, y, z = (np.ascontiguousarray(p[:, d]) for d in range(3))
+        check(lib().mpm_field_set_positions(self._h, x.ctypes.data_as(_dp), y.ctypes.data_as(_dp),
+                                            z.ctypes.data_as(_dp), len(p), _stream_ptr(stream)))
+
+    def set_field_points(self, pts, stream=None):
+        p = np.ascontiguousarray(np.asarray(pts, dtype=np.float64))
+        x, y, z = (np.ascontiguousarray(p[:, d]) for d in range(3))
+        check(lib().mpm_field_set_field_points(self._h, x.ctypes.data_as(_dp), y.ctypes.data_as(_dp),
+                                               z.ctypes.data_as(_dp), len(p), _stream_ptr(stream)))
+
+    def info(self):
+        fi = FieldInfo()
+        check(lib().mpm_field_info_get(self._h, C.byref(fi)))
+        return {k: (list(getattr(fi, k)) if k in ("grid", "h", "eta") else getattr(fi, k)) for k, _ in fi._fields_}
+
+    def apply(self, X, Y=None, self_coef=None, jacobi=False, recip_fp32=False, real_fp32=False, stream=None):
+        import torch
+        assert X.is_cuda and X.dtype == torch.complex128 and X.is_contiguous() and X.dim() == 2
+        info = self.info()
+        rows_out = 3 * info["num_targets"] + 5 * info["num_quads"]
+        if Y is None:
+            Y = torch.empty((rows_out, X.shape[1]), dtype=torch.complex128, device=X.device)
+        sc = None if self_coef is None else self_coef.contiguous()
+        check(lib().mpm_field_apply(self._h, C.c_void_p(X.data_ptr()), C.c_void_p(Y.data_ptr()), X.shape[1],
+                                    None if sc is None else C.c_void_p(sc.data_ptr()), int(jacobi),
+                                    int(recip_fp32), int(real_fp32), _stream_ptr(stream)))
+        return Y
+
+    def apply_part(self, X, part, self_coef=None, recip_fp32=False, real_fp32=False, stream=None):
+        import torch
+        info = self.info()
+        rows_out = 3 * info["num_targets"] + 5 * info["num_quads"]
+        Y = torch.zeros((rows_out, X.shape[1]), dtype=torch.complex128, device=X.device)
+        sc = None if self_coef is None else self_coef.contiguous()
+        check(lib().mpm_field_apply_part(self._h, C.c_void_p(X.data_ptr()), C.c_void_p(Y.data_ptr()), X.shape[1],
+                                         None if sc is None else C.c_void_p(sc.data_ptr()), int(recip_fp32),
+                                         int(real_fp32), int(part), _stream_ptr(stream)))
+        return Y
+
+    def batch_solve(self, B, X, self_coef, tol, method=METHOD_GMRES, restart=50, maxiter=1000, jacobi=True,
+                    recip_fp32=True, real_fp32=False, refine=False, inner_tol=1e-4, stream=None):
+        o = SolveOptions(int(method), int(restart), int(maxiter), float(tol), int(jacobi), int(recip_fp32),
+                         int(real_fp32), int(refine), float(inner_tol))
+        r = SolveReport()
+        check(lib().mpm_batch_solve(self._h, C.c_void_p(B.data_ptr()), C.c_void_p(X.data_ptr()), B.shape[1],
+                                    C.c_void_p(self_coef.data_ptr()), C.byref(o), C.byref(r), _stream_ptr(stream)))
+        return {k: getattr(r, k) for k, _ in r._fields_}

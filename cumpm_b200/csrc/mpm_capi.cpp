@@ -1,0 +1,355 @@
+// extern "C" entry points (include/cumpm_b200.h).  Exceptions never cross
+// the boundary: each call maps them to a status code and a thread-local
+// message.
+#include "../../include/cumpm_b200.h"
+
+#include <complex>
+#include <cstring>
+#include <string>
+
+#include "mpm_field.h"
+#include "mpm_krylov.h"
+#include "mpm_solver.h"
+
+struct mpm_solver { mpm::DipoleSolver* impl; };
+struct mpm_near { mpm::NearField* impl; };
+struct mpm_field {
+    mpm::Field* impl;
+    mpm::BatchSolver* solver;
+};
+
+namespace {
+
+thread_local std::string g_last_error;
+
+template <typename F>
+int guard(F&& f) {
+    try {
+        f();
+        return MPM_OK;
+    } catch (const std::invalid_argument& e) {
+        g_last_error = e.what();
+        return MPM_ERR_INVALID;
+    } catch (const mpm::CudaError& e) {
+        g_last_error = e.what();
+        return MPM_ERR_CUDA;
+    } catch (const std::exception& e) {
+        g_last_error = e.what();
+        return MPM_ERR_RUNTIME;
+    } catch (...) {
+        g_last_error = "unknown error";
+        return MPM_ERR_RUNTIME;
+    }
+}
+
+using cd = std::complex<double>;
+
+std::vector<cd> as_complex(const double* p, size_t n) {
+    std::vector<cd> v(n);
+    for (size_t i = 0; i < n; ++i) v[i] = cd(p[2 * i], p[2 * i + 1]);
+    return v;
+}
+
+void need(const void* p, const char* what) {
+    if (!p) throw std::invalid_argument(std::string(what) + " must not be NULL");
+}
+
+void copy_out(const std::vector<cd>& v, double* out, size_t cap) {
+    if (cap < v.size()) throw std::invalid_argument("output buffer too small");
+    std::memcpy(out, v.data(), v.size() * sizeof(cd));
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* mpm_last_error(void) { return g_last_error.c_str(); }
+const char* mpm_version(void) { return "cumpm_b200 0.1"; }
+
+int mpm_solver_create(mpm_solver** out, const double box[3], const double* eps, int n_freq, int eps_cols,
+                      const double* radius, int n_radius, double eps_m, double xi, double tol, int quiet,
+                      const char* guess_type, const char* solver_type, const char* field_type, const double* E0,
+                      const int* E0_sizes, int n_E0, int solve_quads, const int* quad_idxs, int n_quad_idxs,
+                      int precision) {
+    return guard([&] {
+        need(out, "out");
+        need(box, "box");
+        need(eps, "eps");
+        if (n_freq <= 0 || eps_cols <= 0) throw std::invalid_argument("eps_p must have at least one value");
+        std::vector<std::vector<cd>> e(n_freq);
+        for (int w = 0; w < n_freq; ++w) e[w] = as_complex(eps + 2 * size_t(w) * eps_cols, eps_cols);
+        std::vector<double> rad(radius, radius + (radius ? n_radius : 0));
+        std::vector<std::vector<cd>> e0(n_E0);
+        size_t off = 0;
+        for (int k = 0; k < n_E0; ++k) {
+            e0[k] = as_complex(E0 + 2 * off, E0_sizes[k]);
+            off += E0_sizes[k];
+        }
+        std::vector<int> qi(quad_idxs, quad_idxs + (quad_idxs ? n_quad_idxs : 0));
+        *out = new mpm_solver{new mpm::DipoleSolver(
+            std::vector<double>(box, box + 3), std::move(e), std::move(rad), eps_m, xi, tol, quiet != 0,
+            guess_type ? guess_type : "derivative", solver_type ? solver_type : "gmres",
+            field_type ? field_type : "auto", std::move(e0), solve_quads != 0, std::move(qi), precision)};
+    });
+}
+
+void mpm_solver_destroy(mpm_solver* s) {
+    if (!s) return;
+    delete s->impl;
+    delete s;
+}
+
+int mpm_solver_compute(mpm_solver* s, const double* x, const double* y, const double* z, int n) {
+    return guard([&] {
+        need(s, "solver");
+        if (n < 0) throw std::invalid_argument("negative particle count");
+        std::vector<double> a(x, x + n), b(y, y + n), c(z, z + n);
+        s->impl->compute(a, b, c);
+    });
+}
+
+int mpm_solver_dims(const mpm_solver* s, int64_t dims[5]) {
+    return guard([&] {
+        need(s, "solver");
+        dims[0] = int64_t(s->impl->num_frames());
+        dims[1] = int64_t(s->impl->num_wavevectors());
+        dims[2] = int64_t(s->impl->num_particles());
+        dims[3] = int64_t(s->impl->num_polarizations());
+        dims[4] = int64_t(s->impl->num_quads());
+    });
+}
+
+int mpm_solver_get_dipoles(const mpm_solver* s, int physical, double* out, size_t n) {
+    return guard([&] { need(s, "solver"); copy_out(s->impl->get_dipoles(physical != 0), out, n); });
+}
+int mpm_solver_get_quadrupoles(const mpm_solver* s, int physical, double* out, size_t n) {
+    return guard([&] { need(s, "solver"); copy_out(s->impl->get_quadrupoles(physical != 0), out, n); });
+}
+int mpm_solver_get_eff_polarizability(const mpm_solver* s, int physical, double* out, size_t n) {
+    return guard([&] { need(s, "solver"); copy_out(s->impl->get_eff_polarizability(physical != 0), out, n); });
+}
+int mpm_solver_set_jacobi(mpm_solver* s, int enable) {
+    return guard([&] { need(s, "solver"); s->impl->set_jacobi(enable != 0); });
+}
+int mpm_solver_get_jacobi(const mpm_solver* s, int* enable) {
+    return guard([&] { need(s, "solver"); *enable = s->impl->jacobi() ? 1 : 0; });
+}
+int mpm_solver_set_options(mpm_solver* s, int restart, int maxiter, int batch_all, int refine, double inner_tol,
+                           int real_fp32) {
+    return guard([&] {
+        need(s, "solver");
+        if (restart < 1 || maxiter < 1 || !(inner_tol > 0)) throw std::invalid_argument("invalid solver options");
+        auto& o = s->impl->options();
+        o.restart = restart;
+        o.maxiter = maxiter;
+        o.batch_all = batch_all != 0;
+        o.refine = refine != 0;
+        o.inner_tol = inner_tol;
+        o.real_fp32 = real_fp32 != 0;
+    });
+}
+int mpm_solver_iterations(const mpm_solver* s, int* out, size_t cap, size_t* n_out) {
+    return guard([&] {
+        need(s, "solver");
+        const auto& v = s->impl->all_iterations();
+        if (n_out) *n_out = v.size();
+        if (out) std::memcpy(out, v.data(), sizeof(int) * std::min(cap, v.size()));
+    });
+}
+
+int mpm_near_create(mpm_near** out, const double box[3], const double E0[6], const double* radius, int n_radius,
+                    double xi, double errortol, const char* field_type) {
+    return guard([&] {
+        need(out, "out");
+        need(box, "box");
+        need(E0, "E0");
+        *out = new mpm_near{new mpm::NearField(std::vector<double>(box, box + 3), as_complex(E0, 3),
+                                               std::vector<double>(radius, radius + (radius ? n_radius : 0)), xi,
+                                               errortol, field_type ? field_type : "auto")};
+    });
+}
+void mpm_near_destroy(mpm_near* nf) {
+    if (!nf) return;
+    delete nf->impl;
+    delete nf;
+}
+int mpm_near_set_dipoles(mpm_near* nf, const double* dip, int n) {
+    return guard([&] { need(nf, "near field"); nf->impl->set_dipoles(as_complex(dip, n)); });
+}
+int mpm_near_set_dipole_positions(mpm_near* nf, const double* x, const double* y, const double* z, int n) {
+    return guard([&] {
+        need(nf, "near field");
+        nf->impl->set_dipole_positions({x, x + n}, {y, y + n}, {z, z + n});
+    });
+}
+int mpm_near_set_field_points(mpm_near* nf, const double* x, const double* y, const double* z, int n) {
+    return guard([&] {
+        need(nf, "near field");
+        nf->impl->set_field_points({x, x + n}, {y, y + n}, {z, z + n});
+    });
+}
+int mpm_near_calculate(mpm_near* nf, double* intensity, int n) {
+    return guard([&] {
+        need(nf, "near field");
+        auto v = nf->impl->calculate();
+        if (size_t(n) < v.size()) throw std::invalid_argument("output buffer too small");
+        std::memcpy(intensity, v.data(), sizeof(double) * v.size());
+    });
+}
+
+int mpm_field_create(mpm_field** out, int kind, int mode, const double box[3], double errortol, double xi,
+                     const double* radius, int n_radius, int solve_quads, const int* quad_idxs, int n_quad_idxs) {
+    return guard([&] {
+        need(out, "out");
+        mpm::FieldSpec fs;
+        if (kind != MPM_FIELD_DIRECT && kind != MPM_FIELD_MONO) throw std::invalid_argument("unknown field kind");
+        fs.kind = kind == MPM_FIELD_DIRECT ? mpm::FIELD_DIRECT : mpm::FIELD_MONO;
+        fs.solver_ax = mode == MPM_MODE_SOLVER_AX;
+        if (box) for (int d = 0; d < 3; ++d) fs.box[d] = box[d];
+        if (fs.kind == mpm::FIELD_MONO) need(box, "box");
+        fs.errortol = errortol;
+        fs.xi = xi;
+        if (radius) fs.radius.assign(radius, radius + n_radius);
+        fs.quads = solve_quads != 0;
+        if (quad_idxs) fs.quad_idxs.assign(quad_idxs, quad_idxs + n_quad_idxs);
+        auto* f = new mpm::Field(fs);
+        *out = new mpm_field{f, nullptr};
+    });
+}
+void mpm_field_destroy(mpm_field* f) {
+    if (!f) return;
+    delete f->solver;
+    delete f->impl;
+    delete f;
+}
+int mpm_field_set_positions(mpm_field* f, const double* x, const double* y, const double* z, int n, void* stream) {
+    return guard([&] {
+        need(f, "field");
+        if (f->impl->spec().kind == mpm::FIELD_DIRECT && !f->impl->spec().radius.empty() &&
+            int(f->impl->spec().radius.size()) != n && f->impl->spec().radius.size() != 1)
+            throw std::invalid_argument("Direct field: radius size must match num_particles.");
+        f->impl->set_positions(x, y, z, n, static_cast<cudaStream_t>(stream));
+    });
+}
+int mpm_field_set_field_points(mpm_field* f, const double* x, const double* y, const double* z, int n,
+                               void* stream) {
+    return guard([&] {
+        need(f, "field");
+        f->impl->set_field_points(x, y, z, n, static_cast<cudaStream_t>(stream));
+    });
+}
+int mpm_field_apply(mpm_field* f, const void* X, void* Y, int M, const void* sc, int jacobi, int recip_fp32,
+                    int real_fp32, void* stream) {
+    return guard([&] {
+        need(f, "field");
+        need(X, "X");
+        need(Y, "Y");
+        if (M < 1) throw std::invalid_argument("M must be >= 1");
+        if (jacobi && !sc) throw std::invalid_argument("jacobi scaling needs self coefficients");
+        f->impl->apply(static_cast<const double2*>(X), static_cast<double2*>(Y), M, static_cast<const double2*>(sc),
+                       jacobi != 0, recip_fp32 != 0, real_fp32 != 0, static_cast<cudaStream_t>(stream));
+    });
+}
+int mpm_field_apply_part(mpm_field* f, const void* X, void* Y, int M, const void* sc, int recip_fp32, int real_fp32,
+                         int part, void* stream) {
+    return guard([&] {
+        need(f, "field");
+        need(X, "X");
+        need(Y, "Y");
+        f->impl->apply_part(static_cast<const double2*>(X), static_cast<double2*>(Y), M,
+                            static_cast<const double2*>(sc), recip_fp32 != 0, real_fp32 != 0, part,
+                            static_cast<cudaStream_t>(stream));
+    });
+}
+int mpm_field_info_get(const mpm_field* f, mpm_field_info* info) {
+    return guard([&] {
+        need(f, "field");
+        need(info, "info");
+        const auto& F = *f->impl;
+        const auto st = F.stats();
+        const auto& g = F.geom();
+        std::memset(info, 0, sizeof(*info));
+        info->kind = F.spec().kind == mpm::FIELD_DIRECT ? MPM_FIELD_DIRECT : MPM_FIELD_MONO;
+        info->mode = F.spec().solver_ax ? MPM_MODE_SOLVER_AX : MPM_MODE_INTERACTION;
+        info->num_particles = F.num_particles();
+        info->num_targets = F.num_targets();
+        info->num_quads = F.num_quads();
+        for (int d = 0; d < 3; ++d) {
+            info->grid[d] = g.ng[d];
+            info->h[d] = g.h[d];
+            info->eta[d] = g.eta[d];
+        }
+        info->stencil = 2 * g.off + 1;
+        info->pruned = st.pruned;
+        info->z_slots = st.z_slots;
+        info->num_pairs = st.num_pairs;
+        info->rc = g.rc;
+        info->selfo = F.selfo();
+    });
+}
+
+int mpm_batch_solve(mpm_field* f, const void* B, void* X, int M, const void* sc, const mpm_solve_options* opt,
+                    mpm_solve_report* rep, void* stream) {
+    return guard([&] {
+        need(f, "field");
+        need(opt, "options");
+        need(sc, "self coefficients");
+        if (!f->solver) f->solver = new mpm::BatchSolver();
+        mpm::SolveOptions o;
+        o.method = opt->method == MPM_METHOD_BICGSTAB ? mpm::SOLVER_BICGSTAB : mpm::SOLVER_GMRES;
+        o.restart = opt->restart;
+        o.maxiter = opt->maxiter;
+        o.tol = opt->tol;
+        o.jacobi = opt->jacobi != 0;
+        o.recip_fp32 = opt->recip_fp32 != 0;
+        o.real_fp32 = opt->real_fp32 != 0;
+        o.refine = opt->refine != 0;
+        o.inner_tol = opt->inner_tol;
+        mpm::SolveStats st;
+        f->solver->solve(*f->impl, static_cast<const double2*>(B), static_cast<double2*>(X), M,
+                         static_cast<const double2*>(sc), o, st, static_cast<cudaStream_t>(stream));
+        if (rep) {
+            std::memset(rep, 0, sizeof(*rep));
+            rep->matvecs = st.matvecs;
+            rep->refine_steps = st.refine_steps;
+            for (int m = 0; m < M; ++m) {
+                rep->total_iterations += st.iters[m];
+                rep->max_iterations = std::max(rep->max_iterations, st.iters[m]);
+                rep->num_converged += st.converged[m];
+            }
+            rep->max_rel_resid = -1.0;
+            for (double r : st.rel_resid) rep->max_rel_resid = std::max(rep->max_rel_resid, r);
+        }
+    });
+}
+
+int mpm_mono_tables(double xi, double* out, double* selfo, double* self_grad) {
+    return guard([&] {
+        need(out, "out");
+        if (!(xi > 0)) throw std::invalid_argument("xi must be positive");
+        const auto T = mpm::build_mono_tables(xi);
+        std::memcpy(out, T.r.data(), sizeof(double) * mpm::kTableSize);
+        for (int f = 0; f < mpm::T_COUNT; ++f)
+            std::memcpy(out + size_t(f + 1) * mpm::kTableSize, T.f[f].data(), sizeof(double) * mpm::kTableSize);
+        if (selfo) *selfo = T.selfo;
+        if (self_grad) *self_grad = T.self_grad;
+    });
+}
+
+int mpm_ewald_geometry(const double box[3], double errortol, double xi, int grid[3], int* stencil, double* rc,
+                       double h[3], double eta[3]) {
+    return guard([&] {
+        need(box, "box");
+        if (!(errortol > 0 && errortol < 1) || !(xi > 0)) throw std::invalid_argument("invalid Ewald parameters");
+        const auto g = mpm::make_ewald_geom(box, errortol, xi);
+        for (int d = 0; d < 3; ++d) {
+            if (grid) grid[d] = g.ng[d];
+            if (h) h[d] = g.h[d];
+            if (eta) eta[d] = g.eta[d];
+        }
+        if (stencil) *stencil = 2 * g.off + 1;
+        if (rc) *rc = g.rc;
+    });
+}
+
+}  // extern "C"

@@ -1,0 +1,1290 @@
+// Field operator kernels and host orchestration (see mpm_field.h).
+//
+// Reciprocal space (periodic boxes) follows the reference algorithm
+// (monodisperse_ewald_electric_field.cu:2211-2411: spread -> forward FFT ->
+// k-space Green tensor -> inverse FFT -> contract) with a B200-first layout:
+//
+//  * The grid is stored [ix][iy][slot][b] with b = component*M + rhs, so all
+//    M right-hand sides of a voxel are contiguous and every access is a
+//    coalesced vector.
+//  * Spreading is a gather over voxel tiles: each CTA owns a tile, pulls the
+//    particles whose Gaussian stencil reaches it from a spatial bin index and
+//    writes every voxel exactly once (no atomics, deterministic, no memset).
+//  * Slab geometries (all particles within a few z planes, as in a monolayer
+//    with a vacuum gap) use a pruned transform: 2-D FFTs on the occupied
+//    planes only, and the z part of DFT -> Green tensor -> inverse DFT applied
+//    per (kx, ky) column as a Toeplitz matrix over the occupied planes.  This
+//    is the same discrete operator as the full 3-D FFT path, evaluated
+//    without the zero planes.
+//  * Contraction gathers each particle's stencil for all M columns at once.
+//  * The real-space pair sum is a gather by target over a CSR neighbour list
+//    built on the device from a cell list (no atomics); the self term, the
+//    Jacobi scaling and the INTERACTION_FIELD sign are fused into it.
+#include "mpm_field.h"
+
+#include <cub/cub.cuh>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <numeric>
+
+namespace mpm {
+
+// ---------------------------------------------------------------- geometry
+
+EwaldGeom make_ewald_geom(const double box[3], double errortol, double xi) {
+    EwaldGeom g;
+    double rc = std::sqrt(-std::log(errortol)) / xi;
+    if (rc < 2.0) rc = 2.0;
+    if (rc > box[0] / 2.0 || rc > box[1] / 2.0 || rc > box[2] / 2.0) {
+        throw std::runtime_error("Real space cutoff (" + std::to_string(rc) + ") larger than half the box length.");
+    }
+    g.rc = rc;
+    g.kcut = 2.0 * xi * xi * rc;
+    for (int d = 0; d < 3; ++d) {
+        g.ng[d] = static_cast<int>(std::ceil(1.0 + box[d] * g.kcut / kPi));
+        g.h[d] = box[d] / g.ng[d];
+    }
+    g.P = static_cast<int>(std::ceil(-2.0 * std::log(errortol) / kPi));
+    g.off = g.P / 2;
+    for (int d = 0; d < 3; ++d) g.eta[d] = g.P * std::pow(g.h[d] * xi, 2) / kPi;
+    g.spread_const = std::pow(2.0 * xi * xi / kPi, 1.5) * std::sqrt(1.0 / (g.eta[0] * g.eta[1] * g.eta[2]));
+    return g;
+}
+
+// ------------------------------------------------------------- kernels ---
+
+namespace {
+
+constexpr int kMaxStencil = 32;  // S = 2*off+1 <= 32  (errortol >= ~1e-21)
+
+struct StencilArgs {
+    double h[3];
+    double eta[3];
+    double xi;
+    double cfac;   // folded into the x weights
+    int N[3];
+    int off, S;
+    int z0, pruned, Zs;
+};
+
+// Per point: nearest grid node (C round, halves away from zero), 1-D
+// Gaussian weights along each axis, wrapped indices and z slot
+// (monodisperse_ewald_electric_field.cu:716-746).
+__global__ void k_stencil(const double* __restrict__ xyz, int n, StencilArgs a, int4* __restrict__ base,
+                          double* __restrict__ w64, float* __restrict__ w32) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int gw[3];
+    for (int d = 0; d < 3; ++d) {
+        const double p = xyz[d * n + i];
+        const int g = static_cast<int>(round(p / a.h[d]));
+        const double dd = g * a.h[d] - p;
+        gw[d] = pmod(g, a.N[d]);
+        const double c = (d == 0) ? a.cfac : 1.0;
+        for (int o = 0; o < a.S; ++o) {
+            const double gd = dd + (o - a.off) * a.h[d];
+            const double w = c * exp(-2.0 * a.xi * a.xi * gd * gd / a.eta[d]);
+            w64[(size_t(i) * 3 + d) * a.S + o] = w;
+            w32[(size_t(i) * 3 + d) * a.S + o] = static_cast<float>(w);
+        }
+    }
+    const int slot = a.pruned ? pmod(gw[2] - a.z0, a.N[2]) : gw[2];
+    base[i] = make_int4(gw[0], gw[1], slot, gw[2]);
+}
+
+__global__ void k_bin_keys(const int4* __restrict__ base, int n, int tx, int ty, int tz, int nbx, int nby,
+                           int* __restrict__ key, int* __restrict__ idx) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int4 b = base[i];
+    key[i] = (b.z / tz * nby + b.y / ty) * nbx + b.x / tx;
+    idx[i] = i;
+}
+
+__global__ void k_fill_int(int* p, int n, int v) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) p[i] = v;
+}
+
+__global__ void k_bin_bounds(const int* __restrict__ skey, int n, int* __restrict__ start, int* __restrict__ end) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int k = skey[i];
+    if (i == 0 || skey[i - 1] != k) start[k] = i;
+    if (i == n - 1 || skey[i + 1] != k) end[k] = i + 1;
+}
+
+// Distinct bins whose index range can reach [lo, hi] (inclusive, possibly
+// outside [0, n) and then wrapped when periodic).
+__device__ int reach_bins(int lo, int hi, int n, int t, bool periodic, int* out) {
+    int cnt = 0;
+    for (int v = lo; v <= hi; ++v) {
+        int w = v;
+        if (periodic) w = pmod(v, n);
+        else if (v < 0 || v >= n) continue;
+        const int b = w / t;
+        bool seen = false;
+        for (int k = 0; k < cnt; ++k) seen |= (out[k] == b);
+        if (!seen && cnt < 8) out[cnt++] = b;
+    }
+    return cnt;
+}
+
+// Gather spread: every voxel of this CTA's tile is written once with the sum
+// of all particle contributions (no atomics).  grid[((x*Ny+y)*Zs+s)*B + b].
+template <typename R>
+__global__ void __launch_bounds__(256) k_spread(const double2* __restrict__ X, int M, int N, int C,
+                                                const int* __restrict__ quad_map,
+                                                const int4* __restrict__ base, const R* __restrict__ w1,
+                                                const int* __restrict__ bin_start, const int* __restrict__ bin_end,
+                                                const int* __restrict__ sorted_idx, GridView g, int TX, int TY,
+                                                int TZ, int nbx, int nby, int cap, int bc,
+                                                cplx<R>* __restrict__ grid) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ int bx[8], by[8], bz[8], nbxs, nbys, nbzs;
+    __shared__ int rstart[512], rlen[512], rpre[513], nranges;
+    const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY, z0 = blockIdx.z * TZ;
+    const int x1 = min(x0 + TX, g.Nx), y1 = min(y0 + TY, g.Ny), z1 = min(z0 + TZ, g.Zs);
+    const int B = C * M;
+    if (threadIdx.x == 0) {
+        nbxs = reach_bins(x0 - g.off, x1 - 1 + g.off, g.Nx, TX, true, bx);
+        nbys = reach_bins(y0 - g.off, y1 - 1 + g.off, g.Ny, TY, true, by);
+        nbzs = reach_bins(z0 - g.off, z1 - 1 + g.off, g.Zs, TZ, !g.pruned, bz);
+        int k = 0;
+        rpre[0] = 0;
+        for (int a = 0; a < nbzs; ++a)
+            for (int b2 = 0; b2 < nbys; ++b2)
+                for (int c = 0; c < nbxs; ++c) {
+                    const int key = (bz[a] * nby + by[b2]) * nbx + bx[c];
+                    const int s0 = bin_start[key];
+                    if (s0 < 0 || k >= 512) continue;
+                    rstart[k] = s0;
+                    rlen[k] = bin_end[key] - s0;
+                    rpre[k + 1] = rpre[k] + rlen[k];
+                    ++k;
+                }
+        nranges = k;
+    }
+    __syncthreads();
+    const int total = rpre[nranges];
+    const int wlen = TX + TY + TZ;
+    R* wT = reinterpret_cast<R*>(smem_raw);                                   // [cap][wlen]
+    cplx<R>* pv = reinterpret_cast<cplx<R>*>(smem_raw + sizeof(R) * cap * wlen);  // [cap][bc]
+    int* cid = reinterpret_cast<int*>(pv + size_t(cap) * bc);                  // [cap]
+    const int nvox = TX * TY * TZ;
+    for (int r0 = 0; r0 < max(total, 1); r0 += cap) {
+        const int nc = min(cap, total - r0);
+        // candidate ids
+        for (int t = threadIdx.x; t < nc; t += blockDim.x) {
+            const int gidx = r0 + t;
+            int k = 0;
+            while (rpre[k + 1] <= gidx) ++k;
+            cid[t] = sorted_idx[rstart[k] + gidx - rpre[k]];
+        }
+        __syncthreads();
+        // per-candidate 1-D weights restricted to the tile (0 outside reach)
+        for (int t = threadIdx.x; t < nc * wlen; t += blockDim.x) {
+            const int c = t / wlen, l = t % wlen;
+            const int i = cid[c];
+            const int4 bs = base[i];
+            R w = R(0);
+            if (l < TX) {
+                const int x = x0 + l;
+                if (x < g.Nx) {
+                    const int d = cyc_diff(x, bs.x, g.Nx);
+                    if (d >= -g.off && d <= g.off) w = w1[(size_t(i) * 3 + 0) * g.S + d + g.off];
+                }
+            } else if (l < TX + TY) {
+                const int y = y0 + l - TX;
+                if (y < g.Ny) {
+                    const int d = cyc_diff(y, bs.y, g.Ny);
+                    if (d >= -g.off && d <= g.off) w = w1[(size_t(i) * 3 + 1) * g.S + d + g.off];
+                }
+            } else {
+                const int s = z0 + l - TX - TY;
+                if (s < g.Zs) {
+                    const int d = g.pruned ? (s - bs.z) : cyc_diff(s, bs.z, g.Nz);
+                    if (d >= -g.off && d <= g.off) w = w1[(size_t(i) * 3 + 2) * g.S + d + g.off];
+                }
+            }
+            wT[c * wlen + l] = w;
+        }
+        for (int b0 = 0; b0 < B; b0 += bc) {
+            const int nb = min(bc, B - b0);
+            __syncthreads();
+            for (int t = threadIdx.x; t < nc * nb; t += blockDim.x) {
+                const int c = t / nb, bb = t % nb;
+                const int i = cid[c];
+                const int b = b0 + bb;
+                const int comp = b / M;
+                double2 v;
+                if (comp < 3) {
+                    v = X[size_t(3 * i) * M + b];
+                } else {
+                    const int q = quad_map ? quad_map[i] : -1;
+                    v = (q >= 0) ? X[size_t(3 * N + 5 * q + comp - 3) * M + (b - comp * M)] : make_double2(0, 0);
+                }
+                pv[c * bc + bb] = to_r<R>(v);
+            }
+            __syncthreads();
+            for (int t = threadIdx.x; t < nvox * nb; t += blockDim.x) {
+                const int bb = t % nb, vox = t / nb;
+                const int lz = vox % TZ, ly = (vox / TZ) % TY, lx = vox / (TZ * TY);
+                const int x = x0 + lx, y = y0 + ly, s = z0 + lz;
+                if (x >= g.Nx || y >= g.Ny || s >= g.Zs) continue;
+                cplx<R> acc = mk<R>(0, 0);
+                for (int c = 0; c < nc; ++c) {
+                    const R* wc = wT + c * wlen;
+                    const R w = wc[lx] * wc[TX + ly] * wc[TX + TY + lz];
+                    fma_rc(acc, w, pv[c * bc + bb]);
+                }
+                const size_t o = ((size_t(x) * g.Ny + y) * g.Zs + s) * B + b0 + bb;
+                if (r0 == 0) grid[o] = acc;
+                else grid[o] += acc;
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// Full layout: k-space Green tensor, dipoles only (scale_kernel,
+// monodisperse_ewald_electric_field.cu:1406-1432) or joint dipole/quadrupole
+// (scale_kernel_joint, :1434-1486).  One thread per (voxel, rhs).
+template <typename R>
+__device__ __forceinline__ void khat_at(int ix, int iy, int iz, int Nx, int Ny, int Nz, double Lx, double Ly,
+                                        double Lz, R& kx, R& ky, R& kz) {
+    const double fx = (ix <= (Nx - 1) / 2) ? ix : ix - Nx;
+    const double fy = (iy <= (Ny - 1) / 2) ? iy : iy - Ny;
+    const double fz = (iz <= (Nz - 1) / 2) ? iz : iz - Nz;
+    const double ax = fx * 2.0 * kPi / Lx, ay = fy * 2.0 * kPi / Ly, az = fz * 2.0 * kPi / Lz;
+    const double km = sqrt(ax * ax + ay * ay + az * az);
+    if (km < 1e-12) { kx = ky = kz = R(0); return; }
+    kx = R(ax / km); ky = R(ay / km); kz = R(az / km);
+}
+
+template <typename R, bool QUADS>
+__global__ void k_scale(cplx<R>* __restrict__ grid, const R* __restrict__ sc, int Nx, int Ny, int Nz, double Lx,
+                        double Ly, double Lz, int M) {
+    const size_t V = size_t(Nx) * Ny * Nz;
+    const size_t t = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (t >= V * M) return;
+    const size_t v = t / M;
+    const int m = int(t % M);
+    const int iz = int(v % Nz), iy = int((v / Nz) % Ny), ix = int(v / (size_t(Nz) * Ny));
+    R kx, ky, kz;
+    khat_at<R>(ix, iy, iz, Nx, Ny, Nz, Lx, Ly, Lz, kx, ky, kz);
+    constexpr int C = QUADS ? 8 : 3;
+    cplx<R>* f = grid + v * (size_t(C) * M) + m;
+    const cplx<R> f0 = f[0], f1 = f[size_t(M)], f2 = f[size_t(2) * M];
+    cplx<R> dot = f0 * kx + f1 * ky + f2 * kz;
+    if (!QUADS) {
+        const R s = sc[v];
+        const cplx<R> e = dot * s;
+        f[0] = e * kx; f[size_t(M)] = e * ky; f[size_t(2) * M] = e * kz;
+    } else {
+        const R s = sc[4 * v + 0], sQ = sc[4 * v + 1], sGP = sc[4 * v + 2], sGQ = sc[4 * v + 3];
+        const R qd[5] = {kx * kx - kz * kz, R(2) * kx * ky, R(2) * kx * kz, ky * ky - kz * kz, R(2) * ky * kz};
+        const R third = R(1) / R(3);
+        const R qf[5] = {kx * kx - third, kx * ky, kx * kz, ky * ky - third, ky * kz};
+        cplx<R> gdot = mk<R>(0, 0);
+        for (int c = 0; c < 5; ++c) gdot += f[size_t(3 + c) * M] * qd[c];
+        // i*a*z = (-a z.y, a z.x)
+        const cplx<R> eE = dot * s + mk<R>(-sQ * gdot.y, sQ * gdot.x);
+        const cplx<R> gG = mk<R>(-sGP * dot.y, sGP * dot.x) + gdot * sGQ;
+        f[0] = eE * kx; f[size_t(M)] = eE * ky; f[size_t(2) * M] = eE * kz;
+        for (int c = 0; c < 5; ++c) f[size_t(3 + c) * M] = gG * qf[c];
+    }
+}
+
+// Per-voxel scale coefficients (compute_scale_coefficients_kernel,
+// monodisperse_ewald_electric_field.cu:1300-1404), float64.
+__device__ void scale_coefs(int ix, int iy, int iz, int Nx, int Ny, int Nz, double Lx, double Ly, double Lz,
+                            double xi, const double* eta, double V, double out[4]) {
+    const double fx = (ix <= (Nx - 1) / 2) ? ix : ix - Nx;
+    const double fy = (iy <= (Ny - 1) / 2) ? iy : iy - Ny;
+    const double fz = (iz <= (Nz - 1) / 2) ? iz : iz - Nz;
+    const double gx = fx * 2.0 * kPi / Lx, gy = fy * 2.0 * kPi / Ly, gz = fz * 2.0 * kPi / Lz;
+    const double ks = gx * gx + gy * gy + gz * gz;
+    const double km = sqrt(ks);
+    if (km < 1e-12) { out[0] = out[1] = out[2] = out[3] = 0.0; return; }
+    const double etaksq = ks - (gx * gx * eta[0] + gy * gy * eta[1] + gz * gz * eta[2]);
+    const double term = sin(km) / km - cos(km);
+    const double ex = exp(-etaksq / (4.0 * xi * xi));
+    out[0] = (9.0 * term * term * ex / (ks * ks)) / V;
+    const double j1 = term / km;
+    const double j2 = (3.0 / ks - 1.0) * sin(km) / km - 3.0 * cos(km) / ks;
+    const double e2 = ex / ks;
+    out[1] = (-22.5 * j1 * j2 * e2) / V;
+    out[2] = (45.0 * j1 * j2 * e2) / V;
+    out[3] = (112.5 * j2 * j2 * e2) / V;
+}
+
+struct ScaleArgs {
+    int Nx, Ny, Nz;
+    double Lx, Ly, Lz, xi, eta[3];
+};
+
+__global__ void k_build_scale(ScaleArgs a, int quads, double* __restrict__ s64, float* __restrict__ s32) {
+    const size_t V = size_t(a.Nx) * a.Ny * a.Nz;
+    const size_t v = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (v >= V) return;
+    const int iz = int(v % a.Nz), iy = int((v / a.Nz) % a.Ny), ix = int(v / (size_t(a.Nz) * a.Ny));
+    double o[4];
+    scale_coefs(ix, iy, iz, a.Nx, a.Ny, a.Nz, a.Lx, a.Ly, a.Lz, a.xi, a.eta, double(V), o);
+    if (quads) {
+        for (int c = 0; c < 4; ++c) { s64[4 * v + c] = o[c]; s32[4 * v + c] = float(o[c]); }
+    } else {
+        s64[v] = o[0];
+        s32[v] = float(o[0]);
+    }
+}
+
+// Pruned layout: Toeplitz kernel over the occupied planes for each (kx, ky)
+// column, K_ab(d) = sum_kz exp(+2 pi i kz d / Nz) S(k) khat_a khat_b for the
+// six symmetric ab pairs and d in [-(Z-1), Z-1].  Computed in float64.
+__global__ void k_build_column(ScaleArgs a, int Z, double2* __restrict__ K64, float2* __restrict__ K32) {
+    extern __shared__ double sh[];
+    const int col = blockIdx.x;
+    const int ix = col / a.Ny, iy = col % a.Ny;
+    const int Nz = a.Nz;
+    double* C6 = sh;                 // [Nz][6]
+    double* tw = sh + 6 * Nz;        // [Nz][2] twiddles
+    const double V = double(a.Nx) * a.Ny * a.Nz;
+    for (int iz = threadIdx.x; iz < Nz; iz += blockDim.x) {
+        double o[4];
+        scale_coefs(ix, iy, iz, a.Nx, a.Ny, Nz, a.Lx, a.Ly, a.Lz, a.xi, a.eta, V, o);
+        double kx, ky, kz;
+        khat_at<double>(ix, iy, iz, a.Nx, a.Ny, Nz, a.Lx, a.Ly, a.Lz, kx, ky, kz);
+        const double s = o[0];
+        C6[iz * 6 + 0] = s * kx * kx; C6[iz * 6 + 1] = s * kx * ky; C6[iz * 6 + 2] = s * kx * kz;
+        C6[iz * 6 + 3] = s * ky * ky; C6[iz * 6 + 4] = s * ky * kz; C6[iz * 6 + 5] = s * kz * kz;
+        double sn, cs;
+        sincospi(2.0 * iz / Nz, &sn, &cs);
+        tw[2 * iz] = cs; tw[2 * iz + 1] = sn;
+    }
+    __syncthreads();
+    const int nd = 2 * Z - 1;
+    for (int t = threadIdx.x; t < 6 * nd; t += blockDim.x) {
+        const int ab = t / nd, di = t % nd;
+        const int d = di - (Z - 1);
+        double re = 0.0, im = 0.0;
+        for (int iz = 0; iz < Nz; ++iz) {
+            const int k = pmod(iz * d, Nz);
+            const double c = C6[iz * 6 + ab];
+            re += c * tw[2 * k];
+            im += c * tw[2 * k + 1];
+        }
+        const size_t o = (size_t(col) * 6 + ab) * nd + di;
+        K64[o] = make_double2(re, im);
+        K32[o] = make_float2(float(re), float(im));
+    }
+}
+
+// Pruned layout: out[zo][c'][m] = sum_{zi,c} K_{c'c}(zo - zi) in[zi][c][m]
+// on one (kx, ky) column per CTA, in place.
+template <typename R>
+__global__ void k_column(cplx<R>* __restrict__ grid, const cplx<R>* __restrict__ K, int Z, int M) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int col = blockIdx.x;
+    const int B = 3 * M;
+    const int nd = 2 * Z - 1;
+    cplx<R>* in = reinterpret_cast<cplx<R>*>(smem_raw);   // [Z][B]
+    cplx<R>* kk = in + size_t(Z) * B;                       // [6][nd]
+    cplx<R>* g = grid + size_t(col) * Z * B;
+    for (int t = threadIdx.x; t < Z * B; t += blockDim.x) in[t] = g[t];
+    for (int t = threadIdx.x; t < 6 * nd; t += blockDim.x) kk[t] = K[size_t(col) * 6 * nd + t];
+    __syncthreads();
+    const int pairidx[3][3] = {{0, 1, 2}, {1, 3, 4}, {2, 4, 5}};
+    for (int t = threadIdx.x; t < B; t += blockDim.x) {
+        const int cp = t / M, m = t % M;
+        for (int zo = 0; zo < Z; ++zo) {
+            cplx<R> acc = mk<R>(0, 0);
+            for (int c = 0; c < 3; ++c) {
+                const cplx<R>* kab = kk + pairidx[cp][c] * nd + (Z - 1) + zo;
+                for (int zi = 0; zi < Z; ++zi) acc += kab[-zi] * in[zi * B + c * M + m];
+            }
+            g[zo * B + t] = acc;
+        }
+    }
+}
+
+// Contraction: field at each target from its Gaussian stencil for all B
+// columns (contract_kernel, monodisperse_ewald_electric_field.cu:1488-1587).
+// Writes Y rows (overwrites).  C = 3 (dipoles) or 8 (plus field gradient).
+template <typename R>
+__global__ void k_contract(const cplx<R>* __restrict__ grid, GridView g, int M, int C, int Nt,
+                           const int4* __restrict__ base, const R* __restrict__ w1, double factor,
+                           const int* __restrict__ quad_map, double2* __restrict__ Y, int negate) {
+    __shared__ R w[3 * kMaxStencil];
+    __shared__ int idx[3 * kMaxStencil];
+    const int j = blockIdx.x;
+    const int B = C * M;
+    const int4 bs = base[j];
+    for (int t = threadIdx.x; t < 3 * g.S; t += blockDim.x) {
+        const int d = t / g.S, o = t % g.S;
+        w[t] = w1[(size_t(j) * 3 + d) * g.S + o];
+        const int dd = o - g.off;
+        idx[t] = (d == 0) ? pmod(bs.x + dd, g.Nx) : (d == 1) ? pmod(bs.y + dd, g.Ny)
+                 : (g.pruned ? bs.z + dd : pmod(bs.z + dd, g.Nz));
+    }
+    __syncthreads();
+    const int q = (C > 3 && quad_map) ? quad_map[j] : -1;
+    for (int b = threadIdx.x; b < B; b += blockDim.x) {
+        const int comp = b / M;
+        if (comp >= 3 && q < 0) continue;
+        cplx<R> acc = mk<R>(0, 0);
+        for (int ox = 0; ox < g.S; ++ox) {
+            const R wx = w[ox];
+            const size_t rx = size_t(idx[ox]) * g.Ny;
+            for (int oy = 0; oy < g.S; ++oy) {
+                const R wxy = wx * w[g.S + oy];
+                const size_t rxy = (rx + idx[g.S + oy]) * g.Zs;
+                cplx<R> a2 = mk<R>(0, 0);
+                for (int oz = 0; oz < g.S; ++oz) {
+                    fma_rc(a2, w[2 * g.S + oz], grid[(rxy + idx[2 * g.S + oz]) * B + b]);
+                }
+                fma_rc(acc, wxy, a2);
+            }
+        }
+        double2 v = to_d(acc);
+        v.x *= factor; v.y *= factor;
+        if (negate) { v.x = -v.x; v.y = -v.y; }
+        const int m = b - comp * M;
+        const size_t row = (comp < 3) ? size_t(3 * j + comp) : size_t(3 * Nt + 5 * q + comp - 3);
+        Y[row * M + m] = v;
+    }
+}
+
+// ------------------------------------------------------------ neighbours
+
+struct CellArgs {
+    double L[3];
+    double cs[3];
+    int nc[3];
+};
+
+__device__ __forceinline__ int cell_of(double p, double L, double cs, int nc) {
+    const double w = p - L * floor(p / L);
+    int c = int(floor(w / cs));
+    return min(max(c, 0), nc - 1);
+}
+
+__global__ void k_cell_keys(const double* __restrict__ xyz, int n, CellArgs a, int* __restrict__ key,
+                            int* __restrict__ idx) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int cx = cell_of(xyz[i], a.L[0], a.cs[0], a.nc[0]);
+    const int cy = cell_of(xyz[n + i], a.L[1], a.cs[1], a.nc[1]);
+    const int cz = cell_of(xyz[2 * n + i], a.L[2], a.cs[2], a.nc[2]);
+    key[i] = (cz * a.nc[1] + cy) * a.nc[0] + cx;
+    idx[i] = i;
+}
+
+// For each target: sources within rc (minimum image, d^2 <= rc^2 and then
+// d < rc as in neighbor_list.cu:186-223 + the pair kernels' cut), visiting
+// the distinct neighbouring cells.  pass 0 counts, pass 1 writes pair data.
+__global__ void k_pairs(const double* __restrict__ src, int ns, const double* __restrict__ tgt, int nt, CellArgs a,
+                        const int* __restrict__ cstart, const int* __restrict__ cend,
+                        const int* __restrict__ sidx, double rc, int solver_ax, int pass,
+                        int* __restrict__ cnt, const int* __restrict__ off, int* __restrict__ psrc,
+                        double* __restrict__ pgeo /*[P][4]: dx,dy,dz,d*/) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= nt) return;
+    const double xj = tgt[j], yj = tgt[nt + j], zj = tgt[2 * nt + j];
+    const int c[3] = {cell_of(xj, a.L[0], a.cs[0], a.nc[0]), cell_of(yj, a.L[1], a.cs[1], a.nc[1]),
+                      cell_of(zj, a.L[2], a.cs[2], a.nc[2])};
+    int lst[3][3], nl[3];
+    for (int d = 0; d < 3; ++d) {
+        nl[d] = 0;
+        for (int o = -1; o <= 1; ++o) {
+            const int v = pmod(c[d] + o, a.nc[d]);
+            bool seen = false;
+            for (int k = 0; k < nl[d]; ++k) seen |= lst[d][k] == v;
+            if (!seen) lst[d][nl[d]++] = v;
+        }
+    }
+    int count = 0;
+    const int base = pass ? off[j] : 0;
+    const double rc2 = rc * rc;
+    for (int a2 = 0; a2 < nl[2]; ++a2)
+        for (int a1 = 0; a1 < nl[1]; ++a1)
+            for (int a0 = 0; a0 < nl[0]; ++a0) {
+                const int key = (lst[2][a2] * a.nc[1] + lst[1][a1]) * a.nc[0] + lst[0][a0];
+                const int s0 = cstart[key];
+                if (s0 < 0) continue;
+                const int s1 = cend[key];
+                for (int k = s0; k < s1; ++k) {
+                    const int i = sidx[k];
+                    if (solver_ax && i == j) continue;
+                    double dx = src[i] - xj, dy = src[ns + i] - yj, dz = src[2 * ns + i] - zj;
+                    dx -= a.L[0] * round(dx / a.L[0]);
+                    dy -= a.L[1] * round(dy / a.L[1]);
+                    dz -= a.L[2] * round(dz / a.L[2]);
+                    const double d2 = dx * dx + dy * dy + dz * dz;
+                    if (d2 > rc2) continue;
+                    const double d = sqrt(d2);
+                    if (!(d < rc)) continue;
+                    if (pass) {
+                        const int o = base + count;
+                        psrc[o] = i;
+                        pgeo[4 * size_t(o) + 0] = dx;
+                        pgeo[4 * size_t(o) + 1] = dy;
+                        pgeo[4 * size_t(o) + 2] = dz;
+                        pgeo[4 * size_t(o) + 3] = d;
+                    }
+                    ++count;
+                }
+            }
+    if (!pass) cnt[j] = count;
+}
+
+__device__ double table_at(double r, const double* __restrict__ rt, const double* __restrict__ y) {
+    constexpr int n = kTableSize;
+    if (r <= 0.0) return y[0];
+    if (r >= rt[n - 1]) return y[n - 1];
+    if (r < 1.0) return y[0] * (1.0 - r) + y[1] * r;
+    const size_t k = 1 + static_cast<size_t>((r - 1.0) / kTableDr);
+    if (k >= size_t(n - 1)) return y[n - 1];
+    const double t = (r - rt[k]) / (rt[k + 1] - rt[k]);
+    return y[k] * (1.0 - t) + y[k + 1] * t;
+}
+
+// Pair coefficients (real_space_precalcs_kernel_joint,
+// monodisperse_ewald_electric_field.cu:877-958): delta = r / max(d, 1) and
+// the table values at max(d, 1).  Layout per pair: T64[8] = {dx,dy,dz,perp,
+// para,0,0,0}; Q[8] = {Q1,Q2,Q3,G1,G2,G3,G4,0}.
+__global__ void k_pair_coefs(const double* __restrict__ pgeo, long long np, const double* __restrict__ rt,
+                             const double* __restrict__ tf, int quads, double* __restrict__ T64,
+                             float* __restrict__ T32, double* __restrict__ Q) {
+    const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= np) return;
+    const double d = pgeo[4 * p + 3];
+    const double de = d < 1.0 ? 1.0 : d;
+    const double dx = pgeo[4 * p + 0] / de, dy = pgeo[4 * p + 1] / de, dz = pgeo[4 * p + 2] / de;
+    const double perp = table_at(de, rt, tf + T_FD1 * kTableSize);
+    const double para = table_at(de, rt, tf + T_FD2 * kTableSize);
+    double* t = T64 + 8 * p;
+    t[0] = dx; t[1] = dy; t[2] = dz; t[3] = perp; t[4] = para; t[5] = t[6] = t[7] = 0.0;
+    float* f = T32 + 8 * p;
+    f[0] = float(dx); f[1] = float(dy); f[2] = float(dz); f[3] = float(perp); f[4] = float(para);
+    f[5] = f[6] = f[7] = 0.f;
+    if (quads) {
+        double* qq = Q + 8 * p;
+        for (int k = 0; k < 7; ++k) qq[k] = table_at(de, rt, tf + (T_FQ1 + k) * kTableSize);
+        qq[7] = 0.0;
+    }
+}
+
+// ------------------------------------------------------------ real space
+
+// Gather by target (warp per target, lanes over right-hand sides) of the
+// real-space pair sum, plus self term, optional Jacobi scaling and the
+// INTERACTION_FIELD sign (monodisperse_ewald_electric_field.cu:1589-1869,
+// 2395-2404).  If add_recip, Y already holds the reciprocal part.
+struct RealArgs {
+    int M, N, Nt, Nq;
+    double selfo, self_grad;
+    int solver_ax, jacobi, add_recip, quads;
+};
+
+template <typename R>
+__global__ void __launch_bounds__(128) k_real(const double2* __restrict__ X, double2* __restrict__ Y, RealArgs a,
+                                              const int* __restrict__ off, const int* __restrict__ src,
+                                              const R* __restrict__ T, const double* __restrict__ Qt,
+                                              const int* __restrict__ quad_map,
+                                              const double2* __restrict__ sc) {
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (warp >= a.Nt) return;
+    const int j = warp;
+    const int p0 = off[j], p1 = off[j + 1];
+    const int M = a.M;
+    const double sign = a.solver_ax ? 1.0 : -1.0;
+    const int qt = (a.quads && quad_map && j < a.N) ? quad_map[j] : -1;
+    for (int m = lane; m < M; m += 32) {
+        cplx<R> e0 = mk<R>(0, 0), e1 = e0, e2 = e0;
+        double2 G[5] = {make_double2(0, 0), make_double2(0, 0), make_double2(0, 0), make_double2(0, 0),
+                        make_double2(0, 0)};
+        for (int p = p0; p < p1; ++p) {
+            const int i = src[p];
+            const R* t = T + 8 * size_t(p);
+            const R dx = t[0], dy = t[1], dz = t[2], perp = t[3], para = t[4];
+            const cplx<R> px = to_r<R>(X[size_t(3 * i) * M + m]);
+            const cplx<R> py = to_r<R>(X[size_t(3 * i + 1) * M + m]);
+            const cplx<R> pz = to_r<R>(X[size_t(3 * i + 2) * M + m]);
+            const cplx<R> rp = px * dx + py * dy + pz * dz;
+            const cplx<R> k = rp * (para - perp);
+            e0 += px * perp + k * dx;
+            e1 += py * perp + k * dy;
+            e2 += pz * perp + k * dz;
+            if (a.quads) {
+                // quadrupole couplings in float64 (reference :1758-1866)
+                const double* qc = Qt + 8 * size_t(p);
+                const double Q1 = qc[0], Q2 = qc[1], Q3 = qc[2];
+                const double ddx = dx, ddy = dy, ddz = dz;
+                const int qs = quad_map[i];
+                double2 q[5] = {make_double2(0, 0), make_double2(0, 0), make_double2(0, 0), make_double2(0, 0),
+                                make_double2(0, 0)};
+                if (qs >= 0)
+                    for (int c = 0; c < 5; ++c) q[c] = X[size_t(3 * a.N + 5 * qs + c) * M + m];
+                const double2 Qr0 = q[0] * ddx + q[1] * ddy + q[2] * ddz;
+                const double2 Qr1 = q[1] * ddx + q[3] * ddy + q[4] * ddz;
+                const double2 Qr2 = q[2] * ddx + q[4] * ddy - (q[0] + q[3]) * ddz;
+                if (qs >= 0) {
+                    const double rr0 = ddx * ddx - ddz * ddz, rr1 = 2 * ddx * ddy, rr2 = 2 * ddx * ddz,
+                                 rr3 = ddy * ddy - ddz * ddz, rr4 = 2 * ddy * ddz;
+                    const double2 Qrr = q[0] * rr0 + q[1] * rr1 + q[2] * rr2 + q[3] * rr3 + q[4] * rr4;
+                    const double2 eq0 = (Qrr * (Q1 * ddx) + Qr0 * (2.0 * Q2)) * 0.5;
+                    const double2 eq1 = (Qrr * (Q1 * ddy) + Qr1 * (2.0 * Q2)) * 0.5;
+                    const double2 eq2 = (Qrr * (Q1 * ddz) + Qr2 * (2.0 * Q2)) * 0.5;
+                    e0 -= to_r<R>(eq0); e1 -= to_r<R>(eq1); e2 -= to_r<R>(eq2);
+                }
+                if (qt >= 0) {
+                    const double rs[5] = {ddx * ddx, ddx * ddy, ddx * ddz, ddy * ddy, ddy * ddz};
+                    const double I5[5] = {1, 0, 0, 1, 0};
+                    const double2 dpx = to_d(px), dpy = to_d(py), dpz = to_d(pz);
+                    const double2 drp = dpx * ddx + dpy * ddy + dpz * ddz;
+                    const double2 Pr[5] = {dpx * (2.0 * ddx), dpx * ddy + dpy * ddx, dpx * ddz + dpz * ddx,
+                                           dpy * (2.0 * ddy), dpy * ddz + dpz * ddy};
+                    for (int c = 0; c < 5; ++c) G[c] += (drp * (Q1 * rs[c] + (Q2 + Q3) * I5[c]) + Pr[c] * Q2) * sign;
+                    if (qs >= 0) {
+                        const double G1 = qc[3], G2 = qc[4], G3 = qc[5], G4 = qc[6];
+                        const double2 Qrr2 = Qr0 * ddx + Qr1 * ddy + Qr2 * ddz;
+                        const double2 QQ[5] = {Qr0 * (2.0 * ddx), Qr0 * ddy + Qr1 * ddx, Qr0 * ddz + Qr2 * ddx,
+                                               Qr1 * (2.0 * ddy), Qr1 * ddz + Qr2 * ddy};
+                        for (int c = 0; c < 5; ++c)
+                            G[c] += ((Qrr2 * (G1 * I5[c] + G3 * I5[c] + G4 * rs[c]) + q[c] * G2 + QQ[c] * (2.0 * G3)) *
+                                     0.5) * sign;
+                    }
+                }
+            }
+        }
+        double2 out[3] = {to_d(e0) * sign, to_d(e1) * sign, to_d(e2) * sign};
+        double2 inv = make_double2(1.0, 0.0);
+        double2 s = make_double2(0.0, 0.0);
+        if (a.solver_ax && sc) s = sc[size_t(j) * M + m];
+        if (a.jacobi && sc) {
+            const double den = s.x * s.x + s.y * s.y;
+            inv = den > 1e-30 ? make_double2(s.x / den, -s.y / den) : make_double2(1.0, 0.0);
+        }
+        for (int c = 0; c < 3; ++c) {
+            const size_t o = size_t(3 * j + c) * M + m;
+            double2 v = out[c];
+            if (a.add_recip) {
+                const double2 r = Y[o];
+                v = a.solver_ax ? v + r : (r + v) * -1.0;  // INTERACTION_FIELD: -(recip + sign*pairs)
+            }
+            if (a.solver_ax) {
+                const double2 pj = X[o];
+                v += make_double2(s.x + a.selfo, s.y) * pj;
+            }
+            if (a.jacobi) v = v * inv;
+            Y[o] = v;
+        }
+        if (qt >= 0) {
+            for (int c = 0; c < 5; ++c) {
+                const size_t o = size_t(3 * a.Nt + 5 * qt + c) * M + m;
+                double2 v = G[c];
+                if (a.add_recip) {
+                    const double2 r = Y[o];
+                    v = a.solver_ax ? v + r : (r + v) * -1.0;
+                }
+                if (a.solver_ax) {
+                    const double2 qv = X[size_t(3 * a.N + 5 * qt + c) * M + m];
+                    v += make_double2(2.5 * s.x + 0.5 * a.self_grad, 2.5 * s.y) * qv;
+                }
+                if (a.jacobi) v = v * inv;
+                Y[o] = v;
+            }
+        }
+    }
+}
+
+// -------------------------------------------------------------- direct ---
+
+// Open-boundary all-pairs field (direct_field_kernel,
+// direct_electric_field.cu:42-324).  Thread per target, blockIdx.y = rhs,
+// source tiles staged in shared memory.
+template <typename R>
+__global__ void __launch_bounds__(128) k_direct(const double2* __restrict__ X, double2* __restrict__ Y, int M, int N,
+                                                int Nt, const double* __restrict__ src,
+                                                const double* __restrict__ tgt, const double* __restrict__ rad,
+                                                const int* __restrict__ quad_map, int quads,
+                                                const double2* __restrict__ sc, int solver_ax, int jacobi) {
+    constexpr int TILE = 128;
+    __shared__ R sx[TILE], sy[TILE], sz[TILE], sr[TILE];
+    __shared__ cplx<R> sp[TILE][3];
+    __shared__ cplx<R> sq[TILE][5];
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    const int m = blockIdx.y;
+    const R inv4pi = R(1.0 / (4.0 * kPi));
+    const R k4 = inv4pi * (solver_ax ? R(-1) : R(1));
+    const R jx = j < Nt ? R(tgt[j]) : R(0), jy = j < Nt ? R(tgt[Nt + j]) : R(0),
+            jz = j < Nt ? R(tgt[2 * Nt + j]) : R(0);
+    const int qt = (quads && j < N && j < Nt) ? quad_map[j] : -1;
+    cplx<R> E[3] = {mk<R>(0, 0), mk<R>(0, 0), mk<R>(0, 0)};
+    cplx<R> G[5] = {mk<R>(0, 0), mk<R>(0, 0), mk<R>(0, 0), mk<R>(0, 0), mk<R>(0, 0)};
+    const R eps_orig = sizeof(R) == 4 ? R(1e-6) : R(1e-9);
+    const R eps_sing = sizeof(R) == 4 ? R(1e-12) : R(1e-18);
+    for (int t0 = 0; t0 < N; t0 += TILE) {
+        const int s = t0 + threadIdx.x;
+        if (s < N) {
+            sx[threadIdx.x] = R(src[s]); sy[threadIdx.x] = R(src[N + s]); sz[threadIdx.x] = R(src[2 * N + s]);
+            sr[threadIdx.x] = rad ? R(rad[s]) : R(0);
+            for (int c = 0; c < 3; ++c) sp[threadIdx.x][c] = to_r<R>(X[size_t(3 * s + c) * M + m]);
+            const int qs = quads ? quad_map[s] : -1;
+            for (int c = 0; c < 5; ++c)
+                sq[threadIdx.x][c] = qs >= 0 ? to_r<R>(X[size_t(3 * N + 5 * qs + c) * M + m]) : mk<R>(0, 0);
+        }
+        __syncthreads();
+        if (j < Nt) {
+            const int te = min(TILE, N - t0);
+            for (int k = 0; k < te; ++k) {
+                const int i = t0 + k;
+                if (solver_ax && i == j) continue;
+                R rx = sx[k] - jx, ry = sy[k] - jy, rz = sz[k] - jz;
+                R r2 = rx * rx + ry * ry + rz * rz;
+                const R md2 = sr[k] * sr[k];
+                const R ro = sqrt(r2);
+                if (r2 < md2) {
+                    if (ro > eps_orig) {
+                        const R scl = sqrt(md2 / r2);
+                        rx *= scl; ry *= scl; rz *= scl;
+                    }
+                    r2 = md2;
+                }
+                if (r2 < eps_sing) continue;
+                const R r = sqrt(r2);
+                const R ir = R(1) / r, ir2 = R(1) / r2;
+                const R ir3 = ir2 * ir, ir4 = ir3 * ir, ir5 = ir4 * ir;
+                const R ux = rx * ir, uy = ry * ir, uz = rz * ir;
+                const cplx<R> px = sp[k][0], py = sp[k][1], pz = sp[k][2];
+                const cplx<R> pr = px * ux + py * uy + pz * uz;
+                const R df = k4 * ir3;
+                E[0] += (pr * (R(3) * ux) - px) * df;
+                E[1] += (pr * (R(3) * uy) - py) * df;
+                E[2] += (pr * (R(3) * uz) - pz) * df;
+                if (quads) {
+                    const cplx<R> q0 = sq[k][0] * R(-1), q1 = sq[k][1] * R(-2), q2 = sq[k][2] * R(-2),
+                                  q3 = sq[k][3] * R(-1), q4 = sq[k][4] * R(-2);
+                    const cplx<R> qzz = (q0 + q3) * R(-1);
+                    const cplx<R> Qx = q0 * ux + q1 * uy + q2 * uz;
+                    const cplx<R> Qy = q1 * ux + q3 * uy + q4 * uz;
+                    const cplx<R> Qz = q2 * ux + q4 * uy + qzz * uz;
+                    const cplx<R> Qrr = Qx * ux + Qy * uy + Qz * uz;
+                    const R qf = R(3) * k4 * ir4;
+                    E[0] += (Qrr * (R(2.5) * ux) - Qx) * qf;
+                    E[1] += (Qrr * (R(2.5) * uy) - Qy) * qf;
+                    E[2] += (Qrr * (R(2.5) * uz) - Qz) * qf;
+                    if (qt >= 0) {
+                        const R rs[5] = {ux * ux, ux * uy, ux * uz, uy * uy, uy * uz};
+                        const cplx<R> Gd[5] = {pr * (R(-5) * rs[0] + R(1)) + px * (R(2) * ux),
+                                               pr * (R(-5) * rs[1]) + (px * uy + py * ux),
+                                               pr * (R(-5) * rs[2]) + (px * uz + pz * ux),
+                                               pr * (R(-5) * rs[3] + R(1)) + py * (R(2) * uy),
+                                               pr * (R(-5) * rs[4]) + (py * uz + pz * uy)};
+                        const R gdf = R(-3) * k4 * ir4;
+                        const cplx<R> QQ[5] = {Qx * (R(2) * ux), Qx * uy + Qy * ux, Qx * uz + Qz * ux,
+                                               Qy * (R(2) * uy), Qy * uz + Qz * uy};
+                        const cplx<R> qp[5] = {q0, q1, q2, q3, q4};
+                        const R dg[5] = {R(1), R(0), R(0), R(1), R(0)};
+                        const R f = -k4 * ir5;
+                        for (int c = 0; c < 5; ++c) {
+                            const cplx<R> gq = qp[c] * R(-1.5) + Qrr * (R(52.5) * rs[c] - R(7.5) * dg[c]) -
+                                               QQ[c] * R(15);
+                            G[c] += Gd[c] * gdf + gq * f;
+                        }
+                    }
+                }
+            }
+        }
+        __syncthreads();
+    }
+    if (j >= Nt) return;
+    double2 inv = make_double2(1.0, 0.0);
+    double2 s = make_double2(0.0, 0.0);
+    if (solver_ax && sc) s = sc[size_t(j) * M + m];
+    if (jacobi && sc) {
+        const double den = s.x * s.x + s.y * s.y;
+        inv = den > 1e-30 ? make_double2(s.x / den, -s.y / den) : make_double2(1.0, 0.0);
+    }
+    const double rj = (solver_ax && rad) ? rad[j] : 1.0;
+    const double corr = (1.0 / (4.0 * kPi)) / (rj * rj * rj);
+    for (int c = 0; c < 3; ++c) {
+        const size_t o = size_t(3 * j + c) * M + m;
+        double2 v = to_d(E[c]);
+        if (solver_ax) v += make_double2(s.x + corr, s.y) * X[o];
+        if (jacobi) v = v * inv;
+        Y[o] = v;
+    }
+    if (qt >= 0) {
+        const double cq = 3.0 * corr / (rj * rj);
+        const double fs = 2.5 / (rj * rj);
+        for (int c = 0; c < 5; ++c) {
+            const size_t o = size_t(3 * Nt + 5 * qt + c) * M + m;
+            double2 v = to_d(G[c]);
+            if (solver_ax) v += make_double2(fs * s.x + cq, fs * s.y) * X[size_t(3 * N + 5 * qt + c) * M + m];
+            if (jacobi) v = v * inv;
+            Y[o] = v;
+        }
+    }
+}
+
+inline int nblk(long long n, int b) { return int((n + b - 1) / b); }
+
+}  // namespace
+
+// ------------------------------------------------------------ host side --
+
+Field::Field(const FieldSpec& spec) : spec_(spec) {
+    if (spec_.kind == FIELD_MONO) {
+        geom_ = make_ewald_geom(spec_.box, spec_.errortol, spec_.xi);
+        if (2 * geom_.off + 1 > kMaxStencil) throw std::runtime_error("Ewald stencil wider than supported (errortol too small)");
+        tables_ = build_mono_tables(spec_.xi);
+        tab_r_.ensure(sizeof(double) * kTableSize);
+        tab_f_.ensure(sizeof(double) * kTableSize * T_COUNT);
+        MPM_CUDA(cudaMemcpy(tab_r_.p, tables_.r.data(), sizeof(double) * kTableSize, cudaMemcpyHostToDevice));
+        for (int f = 0; f < T_COUNT; ++f)
+            MPM_CUDA(cudaMemcpy(tab_f_.as<double>() + size_t(f) * kTableSize, tables_.f[f].data(),
+                                sizeof(double) * kTableSize, cudaMemcpyHostToDevice));
+    } else if (spec_.kind != FIELD_DIRECT) {
+        throw std::runtime_error("unsupported field kind");
+    }
+}
+
+Field::~Field() {
+    for (auto& p : plans_) cufftDestroy(p.h);
+}
+
+FieldStats Field::stats() const {
+    FieldStats s;
+    s.pruned = gv_.pruned;
+    s.z_slots = gv_.Zs;
+    s.num_pairs = num_pairs_;
+    for (int d = 0; d < 3; ++d) s.grid[d] = geom_.ng[d];
+    s.stencil = gv_.S;
+    return s;
+}
+
+void Field::set_positions(const double* x, const double* y, const double* z, int n, cudaStream_t s) {
+    if (n <= 0) throw std::invalid_argument("set_positions: empty coordinate set");
+    const bool resized = (n != N_);
+    N_ = n;
+    if (resized || quad_map_.p == nullptr) {
+        // quadrupole bookkeeping (base_electric_field.cu:193-220)
+        std::vector<int> qidx;
+        if (spec_.quads) {
+            if (spec_.quad_idxs.empty()) {
+                qidx.resize(N_);
+                std::iota(qidx.begin(), qidx.end(), 0);
+            } else {
+                qidx = spec_.quad_idxs;
+            }
+        }
+        Nq_ = int(qidx.size());
+        std::vector<int> qmap(N_, -1);
+        for (int q = 0; q < Nq_; ++q)
+            if (qidx[q] >= 0 && qidx[q] < N_) qmap[qidx[q]] = q;
+        quad_map_.ensure(sizeof(int) * N_);
+        MPM_CUDA(cudaMemcpy(quad_map_.p, qmap.data(), sizeof(int) * N_, cudaMemcpyHostToDevice));
+        if (Nq_) {
+            quad_idx_.ensure(sizeof(int) * Nq_);
+            MPM_CUDA(cudaMemcpy(quad_idx_.p, qidx.data(), sizeof(int) * Nq_, cudaMemcpyHostToDevice));
+        }
+        if (spec_.kind == FIELD_DIRECT) {
+            std::vector<double> rad = spec_.radius;
+            if (rad.empty()) rad.assign(N_, 0.0);
+            if (int(rad.size()) != N_) throw std::invalid_argument("Direct field: radius size must match num_particles.");
+            radius_.ensure(sizeof(double) * N_);
+            MPM_CUDA(cudaMemcpy(radius_.p, rad.data(), sizeof(double) * N_, cudaMemcpyHostToDevice));
+        }
+    }
+    sources_.n = n;
+    sources_.xyz.ensure(sizeof(double) * 3 * n);
+    MPM_CUDA(cudaMemcpyAsync(sources_.xyz.as<double>(), x, sizeof(double) * n, cudaMemcpyHostToDevice, s));
+    MPM_CUDA(cudaMemcpyAsync(sources_.xyz.as<double>() + n, y, sizeof(double) * n, cudaMemcpyHostToDevice, s));
+    MPM_CUDA(cudaMemcpyAsync(sources_.xyz.as<double>() + 2 * n, z, sizeof(double) * n, cudaMemcpyHostToDevice, s));
+    if (spec_.kind == FIELD_MONO) {
+        // occupied z planes are decided on the host from the same rounding rule
+        std::vector<double> zz(z, z + n);
+        host_z_.assign(zz.begin(), zz.end());
+    }
+    precalc_dirty_ = true;
+    precalc(s);
+}
+
+void Field::set_field_points(const double* x, const double* y, const double* z, int n, cudaStream_t s) {
+    if (spec_.solver_ax) throw std::runtime_error("Cannot update field coordinates when SOLVER_AX mode is active.");
+    targets_.n = n;
+    targets_.xyz.ensure(sizeof(double) * 3 * std::max(n, 1));
+    MPM_CUDA(cudaMemcpyAsync(targets_.xyz.as<double>(), x, sizeof(double) * n, cudaMemcpyHostToDevice, s));
+    MPM_CUDA(cudaMemcpyAsync(targets_.xyz.as<double>() + n, y, sizeof(double) * n, cudaMemcpyHostToDevice, s));
+    MPM_CUDA(cudaMemcpyAsync(targets_.xyz.as<double>() + 2 * n, z, sizeof(double) * n, cudaMemcpyHostToDevice, s));
+    precalc_dirty_ = true;
+    if (N_ > 0) precalc(s);
+}
+
+void Field::choose_layout(cudaStream_t) {
+    const int Nz = geom_.ng[2];
+    gv_.Nx = geom_.ng[0];
+    gv_.Ny = geom_.ng[1];
+    gv_.Nz = Nz;
+    gv_.off = geom_.off;
+    gv_.S = 2 * geom_.off + 1;
+    gv_.pruned = 0;
+    gv_.z0 = 0;
+    gv_.Zs = Nz;
+    // Pruned slab layout only for the dipole matvec with targets == sources.
+    if (!spec_.solver_ax || Nq_ > 0) return;
+    std::vector<char> occ(Nz, 0);
+    for (double zv : host_z_) {
+        const long g = std::lround(zv / geom_.h[2]);  // C round, halves away from zero
+        for (int o = -geom_.off; o <= geom_.off; ++o) occ[pmod(int(g + o), Nz)] = 1;
+    }
+    // smallest cyclic interval covering all occupied planes = complement of
+    // the largest run of empty planes
+    int best_len = 0, best_start = 0;
+    int run = 0, run_start = 0;
+    for (int k = 0; k < 2 * Nz; ++k) {
+        if (!occ[k % Nz]) {
+            if (run == 0) run_start = k;
+            ++run;
+            if (run > best_len && run <= Nz) { best_len = run; best_start = run_start; }
+        } else {
+            run = 0;
+        }
+    }
+    const int Z = Nz - best_len;
+    if (best_len == 0 || Z > 24 || 4 * Z > Nz) return;
+    gv_.pruned = 1;
+    gv_.Zs = Z;
+    gv_.z0 = (best_start + best_len) % Nz;
+}
+
+void Field::build_stencil(PointSet& ps, cudaStream_t s, bool bins) {
+    const int n = ps.n;
+    const int S = gv_.S;
+    ps.base.ensure(sizeof(int4) * n);
+    ps.w64.ensure(sizeof(double) * size_t(n) * 3 * S);
+    ps.w32.ensure(sizeof(float) * size_t(n) * 3 * S);
+    StencilArgs a;
+    for (int d = 0; d < 3; ++d) { a.h[d] = geom_.h[d]; a.eta[d] = geom_.eta[d]; a.N[d] = geom_.ng[d]; }
+    a.xi = spec_.xi;
+    a.cfac = geom_.spread_const;
+    a.off = geom_.off;
+    a.S = S;
+    a.z0 = gv_.z0;
+    a.pruned = gv_.pruned;
+    a.Zs = gv_.Zs;
+    k_stencil<<<nblk(n, 128), 128, 0, s>>>(ps.xyz.as<double>(), n, a, ps.base.as<int4>(), ps.w64.as<double>(),
+                                            ps.w32.as<float>());
+    MPM_LAUNCH();
+    if (!bins) return;
+    ps.tile[0] = 8;
+    ps.tile[1] = 8;
+    ps.tile[2] = (gv_.pruned && gv_.Zs <= 16) ? gv_.Zs : 8;
+    ps.nb[0] = (gv_.Nx + ps.tile[0] - 1) / ps.tile[0];
+    ps.nb[1] = (gv_.Ny + ps.tile[1] - 1) / ps.tile[1];
+    ps.nb[2] = (gv_.Zs + ps.tile[2] - 1) / ps.tile[2];
+    const int nbins = ps.nb[0] * ps.nb[1] * ps.nb[2];
+    ps.bin_key.ensure(sizeof(int) * n);
+    ps.bin_key_sorted.ensure(sizeof(int) * n);
+    ps.idx.ensure(sizeof(int) * n);
+    ps.idx_sorted.ensure(sizeof(int) * n);
+    ps.bin_start.ensure(sizeof(int) * nbins);
+    ps.bin_end.ensure(sizeof(int) * nbins);
+    k_bin_keys<<<nblk(n, 128), 128, 0, s>>>(ps.base.as<int4>(), n, ps.tile[0], ps.tile[1], ps.tile[2], ps.nb[0],
+                                            ps.nb[1], ps.bin_key.as<int>(), ps.idx.as<int>());
+    MPM_LAUNCH();
+    size_t tmp = 0;
+    int bits = 1;
+    while ((1 << bits) < nbins) ++bits;
+    cub::DeviceRadixSort::SortPairs(nullptr, tmp, ps.bin_key.as<int>(), ps.bin_key_sorted.as<int>(),
+                                    ps.idx.as<int>(), ps.idx_sorted.as<int>(), n, 0, bits, s);
+    ps.cub_tmp.ensure(tmp);
+    MPM_CUDA(cub::DeviceRadixSort::SortPairs(ps.cub_tmp.p, tmp, ps.bin_key.as<int>(), ps.bin_key_sorted.as<int>(),
+                                             ps.idx.as<int>(), ps.idx_sorted.as<int>(), n, 0, bits, s));
+    k_fill_int<<<nblk(nbins, 256), 256, 0, s>>>(ps.bin_start.as<int>(), nbins, -1);
+    k_fill_int<<<nblk(nbins, 256), 256, 0, s>>>(ps.bin_end.as<int>(), nbins, -1);
+    k_bin_bounds<<<nblk(n, 256), 256, 0, s>>>(ps.bin_key_sorted.as<int>(), n, ps.bin_start.as<int>(),
+                                              ps.bin_end.as<int>());
+    MPM_LAUNCH();
+}
+
+void Field::build_pairs(cudaStream_t s) {
+    const PointSet& tg = spec_.solver_ax ? sources_ : targets_;
+    const int ns = sources_.n, nt = tg.n;
+    const double rc = geom_.rc;
+    CellArgs a;
+    for (int d = 0; d < 3; ++d) {
+        a.L[d] = spec_.box[d];
+        a.nc[d] = std::max(1, int(std::floor(spec_.box[d] / rc)));
+        a.cs[d] = spec_.box[d] / a.nc[d];
+    }
+    const int ncell = a.nc[0] * a.nc[1] * a.nc[2];
+    cell_key_.ensure(sizeof(int) * ns);
+    cell_idx_.ensure(sizeof(int) * ns);
+    cell_key_s_.ensure(sizeof(int) * ns);
+    cell_idx_s_.ensure(sizeof(int) * ns);
+    cell_start_.ensure(sizeof(int) * ncell);
+    cell_end_.ensure(sizeof(int) * ncell);
+    k_cell_keys<<<nblk(ns, 128), 128, 0, s>>>(sources_.xyz.as<double>(), ns, a, cell_key_.as<int>(),
+                                               cell_idx_.as<int>());
+    MPM_LAUNCH();
+    int bits = 1;
+    while ((1 << bits) < ncell) ++bits;
+    size_t tmp = 0;
+    cub::DeviceRadixSort::SortPairs(nullptr, tmp, cell_key_.as<int>(), cell_key_s_.as<int>(), cell_idx_.as<int>(),
+                                    cell_idx_s_.as<int>(), ns, 0, bits, s);
+    cub_tmp_.ensure(tmp);
+    MPM_CUDA(cub::DeviceRadixSort::SortPairs(cub_tmp_.p, tmp, cell_key_.as<int>(), cell_key_s_.as<int>(),
+                                             cell_idx_.as<int>(), cell_idx_s_.as<int>(), ns, 0, bits, s));
+    k_fill_int<<<nblk(ncell, 256), 256, 0, s>>>(cell_start_.as<int>(), ncell, -1);
+    k_fill_int<<<nblk(ncell, 256), 256, 0, s>>>(cell_end_.as<int>(), ncell, -1);
+    k_bin_bounds<<<nblk(ns, 256), 256, 0, s>>>(cell_key_s_.as<int>(), ns, cell_start_.as<int>(),
+                                               cell_end_.as<int>());
+    MPM_LAUNCH();
+    pair_cnt_.ensure(sizeof(int) * (nt + 1));
+    pair_off_.ensure(sizeof(int) * (nt + 1));
+    MPM_CUDA(cudaMemsetAsync(pair_cnt_.p, 0, sizeof(int) * (nt + 1), s));
+    k_pairs<<<nblk(nt, 128), 128, 0, s>>>(sources_.xyz.as<double>(), ns, tg.xyz.as<double>(), nt, a,
+                                           cell_start_.as<int>(), cell_end_.as<int>(), cell_idx_s_.as<int>(), rc,
+                                           spec_.solver_ax ? 1 : 0, 0, pair_cnt_.as<int>(), nullptr, nullptr,
+                                           nullptr);
+    MPM_LAUNCH();
+    size_t need = 0;
+    cub::DeviceScan::ExclusiveSum(nullptr, need, pair_cnt_.as<int>(), pair_off_.as<int>(), nt + 1, s);
+    cub_tmp_.ensure(need);
+    MPM_CUDA(cub::DeviceScan::ExclusiveSum(cub_tmp_.p, need, pair_cnt_.as<int>(), pair_off_.as<int>(), nt + 1, s));
+    int total = 0;
+    MPM_CUDA(cudaMemcpyAsync(&total, pair_off_.as<int>() + nt, sizeof(int), cudaMemcpyDeviceToHost, s));
+    MPM_CUDA(cudaStreamSynchronize(s));
+    num_pairs_ = total;
+    const size_t np = std::max<long long>(1, num_pairs_);
+    pair_src_.ensure(sizeof(int) * np);
+    DevBuf geo;
+    geo.ensure(sizeof(double) * 4 * np);
+    k_pairs<<<nblk(nt, 128), 128, 0, s>>>(sources_.xyz.as<double>(), ns, tg.xyz.as<double>(), nt, a,
+                                           cell_start_.as<int>(), cell_end_.as<int>(), cell_idx_s_.as<int>(), rc,
+                                           spec_.solver_ax ? 1 : 0, 1, nullptr, pair_off_.as<int>(),
+                                           pair_src_.as<int>(), geo.as<double>());
+    MPM_LAUNCH();
+    pair_T64_.ensure(sizeof(double) * 8 * np);
+    pair_T32_.ensure(sizeof(float) * 8 * np);
+    if (Nq_) pair_Q_.ensure(sizeof(double) * 8 * np);
+    if (num_pairs_ > 0)
+        k_pair_coefs<<<nblk(num_pairs_, 256), 256, 0, s>>>(geo.as<double>(), num_pairs_, tab_r_.as<double>(),
+                                                            tab_f_.as<double>(), Nq_ > 0, pair_T64_.as<double>(),
+                                                            pair_T32_.as<float>(), pair_Q_.as<double>());
+    MPM_LAUNCH();
+    MPM_CUDA(cudaStreamSynchronize(s));  // geo is released at scope end
+}
+
+void Field::build_scale(cudaStream_t s) {
+    const size_t V = size_t(geom_.ng[0]) * geom_.ng[1] * geom_.ng[2];
+    const int per = Nq_ ? 4 : 1;
+    scale64_.ensure(sizeof(double) * V * per);
+    scale32_.ensure(sizeof(float) * V * per);
+    ScaleArgs a;
+    a.Nx = geom_.ng[0]; a.Ny = geom_.ng[1]; a.Nz = geom_.ng[2];
+    a.Lx = spec_.box[0]; a.Ly = spec_.box[1]; a.Lz = spec_.box[2];
+    a.xi = spec_.xi;
+    for (int d = 0; d < 3; ++d) a.eta[d] = geom_.eta[d];
+    k_build_scale<<<nblk((long long)V, 256), 256, 0, s>>>(a, Nq_ ? 1 : 0, scale64_.as<double>(), scale32_.as<float>());
+    MPM_LAUNCH();
+    scale_built_ = per;
+}
+
+void Field::build_column_kernel(cudaStream_t s) {
+    const int Z = gv_.Zs;
+    const int ncol = gv_.Nx * gv_.Ny;
+    const int nd = 2 * Z - 1;
+    colK64_.ensure(sizeof(double2) * size_t(ncol) * 6 * nd);
+    colK32_.ensure(sizeof(float2) * size_t(ncol) * 6 * nd);
+    ScaleArgs a;
+    a.Nx = gv_.Nx; a.Ny = gv_.Ny; a.Nz = gv_.Nz;
+    a.Lx = spec_.box[0]; a.Ly = spec_.box[1]; a.Lz = spec_.box[2];
+    a.xi = spec_.xi;
+    for (int d = 0; d < 3; ++d) a.eta[d] = geom_.eta[d];
+    const size_t shm = sizeof(double) * 8 * gv_.Nz;
+    if (shm > 48 * 1024)
+        MPM_CUDA(cudaFuncSetAttribute(k_build_column, cudaFuncAttributeMaxDynamicSharedMemorySize, int(shm)));
+    k_build_column<<<ncol, 128, shm, s>>>(a, Z, colK64_.as<double2>(), colK32_.as<float2>());
+    MPM_LAUNCH();
+    colK_Z_ = Z;
+}
+
+void Field::precalc(cudaStream_t s) {
+    if (!precalc_dirty_) return;
+    if (spec_.kind == FIELD_MONO) {
+        choose_layout(s);
+        build_stencil(sources_, s, true);
+        if (!spec_.solver_ax) build_stencil(targets_, s, false);  // SOLVER_AX: targets share the source stencil
+        build_pairs(s);
+        if (gv_.pruned) {
+            if (colK_Z_ != gv_.Zs) build_column_kernel(s);
+        } else if (scale_built_ != (Nq_ ? 4 : 1)) {
+            build_scale(s);
+        }
+    }
+    precalc_dirty_ = false;
+}
+
+cufftHandle Field::plan_for(int M, bool fp32) {
+    const int C = Nq_ ? 8 : 3;
+    for (auto& p : plans_)
+        if (p.M == M && p.fp32 == fp32 && p.pruned == gv_.pruned && p.Zs == gv_.Zs) return p.h;
+    cufftHandle h;
+    const int B = C * M;
+    if (cufftCreate(&h) != CUFFT_SUCCESS) throw std::runtime_error("cuFFT plan creation failed");
+    cufftResult r;
+    size_t ws = 0;
+    if (gv_.pruned) {
+        int n[2] = {gv_.Nx, gv_.Ny};
+        const int stride = gv_.Zs * B;
+        r = cufftMakePlanMany(h, 2, n, n, stride, 1, n, stride, 1, fp32 ? CUFFT_C2C : CUFFT_Z2Z, stride, &ws);
+    } else {
+        int n[3] = {gv_.Nx, gv_.Ny, gv_.Nz};
+        r = cufftMakePlanMany(h, 3, n, n, B, 1, n, B, 1, fp32 ? CUFFT_C2C : CUFFT_Z2Z, B, &ws);
+    }
+    if (r != CUFFT_SUCCESS) {
+        cufftDestroy(h);
+        throw std::runtime_error("cuFFT plan creation failed with code: " + std::to_string(int(r)));
+    }
+    plans_.push_back({M, fp32, gv_.pruned, gv_.Zs, h});
+    return h;
+}
+
+template <typename R>
+void Field::recip(const double2* X, double2* Y, int M, cudaStream_t s) {
+    const int C = Nq_ ? 8 : 3;
+    const int B = C * M;
+    const size_t cells = size_t(gv_.Nx) * gv_.Ny * gv_.Zs;
+    grid_.ensure(sizeof(cplx<R>) * cells * B);
+    cplx<R>* grid = grid_.as<cplx<R>>();
+    // spread
+    const PointSet& ps = sources_;
+    const int TX = ps.tile[0], TY = ps.tile[1], TZ = ps.tile[2];
+    const int bc = sizeof(R) == 4 ? 32 : 16;
+    const int cap = 192;
+    const size_t shm = sizeof(R) * cap * (TX + TY + TZ) + sizeof(cplx<R>) * cap * bc + sizeof(int) * cap;
+    MPM_CUDA(cudaFuncSetAttribute(k_spread<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(shm)));
+    dim3 grd(ps.nb[0], ps.nb[1], ps.nb[2]);
+    const R* w1 = sizeof(R) == 4 ? reinterpret_cast<const R*>(ps.w32.p) : reinterpret_cast<const R*>(ps.w64.p);
+    k_spread<R><<<grd, 256, shm, s>>>(X, M, N_, C, quad_map_.as<int>(), ps.base.as<int4>(), w1,
+                                      ps.bin_start.as<int>(), ps.bin_end.as<int>(), ps.idx_sorted.as<int>(), gv_,
+                                      TX, TY, TZ, ps.nb[0], ps.nb[1], cap, bc, grid);
+    MPM_LAUNCH();
+    // forward transform
+    cufftHandle plan = plan_for(M, sizeof(R) == 4);
+    cufftSetStream(plan, s);
+    cufftResult fr;
+    if (sizeof(R) == 4)
+        fr = cufftExecC2C(plan, reinterpret_cast<cufftComplex*>(grid), reinterpret_cast<cufftComplex*>(grid), CUFFT_FORWARD);
+    else
+        fr = cufftExecZ2Z(plan, reinterpret_cast<cufftDoubleComplex*>(grid), reinterpret_cast<cufftDoubleComplex*>(grid),
+                          CUFFT_FORWARD);
+    if (fr != CUFFT_SUCCESS) throw std::runtime_error("cuFFT forward execution failed with code: " + std::to_string(int(fr)));
+    // k-space Green tensor
+    if (gv_.pruned) {
+        const int Z = gv_.Zs;
+        const int nd = 2 * Z - 1;
+        const size_t shm2 = sizeof(cplx<R>) * (size_t(Z) * B + 6 * nd);
+        MPM_CUDA(cudaFuncSetAttribute(k_column<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(shm2)));
+        const int thr = std::min(1024, ((B + 31) / 32) * 32);
+        const cplx<R>* K = sizeof(R) == 4 ? reinterpret_cast<const cplx<R>*>(colK32_.p)
+                                          : reinterpret_cast<const cplx<R>*>(colK64_.p);
+        k_column<R><<<gv_.Nx * gv_.Ny, thr, shm2, s>>>(grid, K, Z, M);
+    } else {
+        const size_t V = cells;
+        const R* sc = sizeof(R) == 4 ? reinterpret_cast<const R*>(scale32_.p) : reinterpret_cast<const R*>(scale64_.p);
+        if (Nq_)
+            k_scale<R, true><<<nblk((long long)(V * M), 256), 256, 0, s>>>(grid, sc, gv_.Nx, gv_.Ny, gv_.Nz, spec_.box[0],
+                                                                           spec_.box[1], spec_.box[2], M);
+        else
+            k_scale<R, false><<<nblk((long long)(V * M), 256), 256, 0, s>>>(grid, sc, gv_.Nx, gv_.Ny, gv_.Nz, spec_.box[0],
+                                                                            spec_.box[1], spec_.box[2], M);
+    }
+    MPM_LAUNCH();
+    if (sizeof(R) == 4)
+        fr = cufftExecC2C(plan, reinterpret_cast<cufftComplex*>(grid), reinterpret_cast<cufftComplex*>(grid), CUFFT_INVERSE);
+    else
+        fr = cufftExecZ2Z(plan, reinterpret_cast<cufftDoubleComplex*>(grid), reinterpret_cast<cufftDoubleComplex*>(grid),
+                          CUFFT_INVERSE);
+    if (fr != CUFFT_SUCCESS) throw std::runtime_error("cuFFT inverse execution failed with code: " + std::to_string(int(fr)));
+    // contract
+    const PointSet& tg = spec_.solver_ax ? sources_ : targets_;
+    const int nt = tg.n;
+    const double factor = geom_.h[0] * geom_.h[1] * geom_.h[2];
+    const R* tw = sizeof(R) == 4 ? reinterpret_cast<const R*>(tg.w32.p) : reinterpret_cast<const R*>(tg.w64.p);
+    const int thr = std::min(256, ((B + 31) / 32) * 32);
+    k_contract<R><<<nt, thr, 0, s>>>(grid, gv_, M, C, nt, tg.base.as<int4>(), tw, factor,
+                                     spec_.solver_ax ? quad_map_.as<int>() : nullptr, Y, 0);
+    MPM_LAUNCH();
+}
+
+void Field::real_part(const double2* X, double2* Y, int M, const double2* sc, bool jacobi, bool fp32, bool add_recip,
+                      cudaStream_t s) {
+    RealArgs a;
+    a.M = M;
+    a.N = N_;
+    a.Nt = num_targets();
+    a.Nq = Nq_;
+    a.selfo = tables_.selfo;
+    a.self_grad = tables_.self_grad;
+    a.solver_ax = spec_.solver_ax ? 1 : 0;
+    a.jacobi = jacobi ? 1 : 0;
+    a.add_recip = add_recip ? 1 : 0;
+    a.quads = Nq_ > 0 ? 1 : 0;
+    const int warps = a.Nt;
+    const int thr = 128;
+    const int blocks = nblk((long long)warps * 32, thr);
+    if (fp32)
+        k_real<float><<<blocks, thr, 0, s>>>(X, Y, a, pair_off_.as<int>(), pair_src_.as<int>(), pair_T32_.as<float>(),
+                                             pair_Q_.as<double>(), quad_map_.as<int>(), sc);
+    else
+        k_real<double><<<blocks, thr, 0, s>>>(X, Y, a, pair_off_.as<int>(), pair_src_.as<int>(),
+                                              pair_T64_.as<double>(), pair_Q_.as<double>(), quad_map_.as<int>(), sc);
+    MPM_LAUNCH();
+}
+
+void Field::direct(const double2* X, double2* Y, int M, const double2* sc, bool jacobi, bool fp32, cudaStream_t s) {
+    const int nt = num_targets();
+    const double* tg = spec_.solver_ax ? sources_.xyz.as<double>() : targets_.xyz.as<double>();
+    dim3 grd(nblk(nt, 128), M);
+    if (fp32)
+        k_direct<float><<<grd, 128, 0, s>>>(X, Y, M, N_, nt, sources_.xyz.as<double>(), tg, radius_.as<double>(),
+                                            quad_map_.as<int>(), Nq_ > 0, sc, spec_.solver_ax, jacobi);
+    else
+        k_direct<double><<<grd, 128, 0, s>>>(X, Y, M, N_, nt, sources_.xyz.as<double>(), tg, radius_.as<double>(),
+                                             quad_map_.as<int>(), Nq_ > 0, sc, spec_.solver_ax, jacobi);
+    MPM_LAUNCH();
+}
+
+void Field::apply(const double2* X, double2* Y, int M, const double2* sc, bool jacobi, bool recip_fp32,
+                  bool real_fp32, cudaStream_t s) {
+    if (N_ == 0) throw std::runtime_error("Field::apply before set_positions");
+    if (!spec_.solver_ax && targets_.n == 0) throw std::runtime_error("Field::apply without field points");
+    if (spec_.kind == FIELD_DIRECT) {
+        direct(X, Y, M, sc, jacobi, recip_fp32, s);
+        return;
+    }
+    if (recip_fp32) recip<float>(X, Y, M, s);
+    else recip<double>(X, Y, M, s);
+    real_part(X, Y, M, sc, jacobi, real_fp32, true, s);
+}
+
+void Field::apply_part(const double2* X, double2* Y, int M, const double2* sc, bool recip_fp32, bool real_fp32,
+                       int part, cudaStream_t s) {
+    if (spec_.kind != FIELD_MONO) throw std::runtime_error("apply_part needs an Ewald field");
+    if (part == 0) {  // reciprocal only (no self, no sign change)
+        if (recip_fp32) recip<float>(X, Y, M, s);
+        else recip<double>(X, Y, M, s);
+    } else {          // real space + self only
+        real_part(X, Y, M, sc, false, real_fp32, false, s);
+    }
+}
+
+}  // namespace mpm

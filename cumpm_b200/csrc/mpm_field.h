@@ -1,0 +1,155 @@
+// Electric-field operator E = A(p) of the Mutual Polarization Method.
+//
+// One Field object replaces the reference's Electric_Field hierarchy
+// (electric_field/electric_field.h:13-141) for the two boundary conditions
+// the solve uses:
+//   * FIELD_MONO   periodic box, monodisperse spectral Ewald
+//                  (monodisperse_ewald_electric_field.cu)
+//   * FIELD_DIRECT open boundaries, all-pairs sum (direct_electric_field.cu)
+// in either SOLVER_AX mode (the Krylov matvec: self terms, i != j) or
+// INTERACTION_FIELD mode (field at arbitrary points, used by Near_Field).
+//
+// Unlike the reference, apply() takes M right-hand sides at once.  Moment
+// and field vectors are device arrays in [row][M] layout (row = 3*i + c for
+// dipoles, 3*N + 5*q + c for quadrupoles), complex128.
+#pragma once
+
+#include <cufft.h>
+#include <memory>
+#include <vector>
+
+#include "mpm_common.cuh"
+#include "mpm_tables.h"
+
+namespace mpm {
+
+enum FieldKind { FIELD_DIRECT = 0, FIELD_MONO = 1 };
+
+struct FieldSpec {
+    int kind = FIELD_MONO;
+    bool solver_ax = true;
+    double box[3] = {0, 0, 0};
+    double errortol = 1e-3;
+    double xi = 0.5;
+    std::vector<double> radius;       // per particle (direct) or empty
+    bool quads = false;
+    std::vector<int> quad_idxs;       // empty + quads => all particles
+};
+
+// Spectral-Ewald parameters (monodisperse_ewald_electric_field.cu:546-616).
+struct EwaldGeom {
+    double rc = 0, kcut = 0;
+    int ng[3] = {0, 0, 0};
+    double h[3] = {0, 0, 0};
+    int P = 0;          // num_grid_gaussian (sets eta)
+    int off = 0;        // stencil half width, stencil = 2*off+1 points
+    double eta[3] = {0, 0, 0};
+    double spread_const = 0;  // (2 xi^2/pi)^1.5 / sqrt(eta_x eta_y eta_z)
+};
+
+EwaldGeom make_ewald_geom(const double box[3], double errortol, double xi);
+
+// Device-side description of the stored part of the grid.
+struct GridView {
+    int Nx, Ny, Nz;
+    int Zs;        // stored z slots
+    int z0;        // first stored plane (pruned layout)
+    int pruned;    // 1: slots are the occupied planes z0..z0+Zs-1 (mod Nz)
+    int off;       // stencil half width
+    int S;         // stencil width
+};
+
+struct PointSet {
+    int n = 0;
+    DevBuf xyz;     // double[3][n] SoA
+    DevBuf base;    // int4[n] (wrapped gx, wrapped gy, z slot, wrapped gz)
+    DevBuf w64;     // double[n][3][S]
+    DevBuf w32;     // float[n][3][S]
+    // spatial bins (spread sources only)
+    DevBuf bin_key, bin_key_sorted, idx, idx_sorted, bin_start, bin_end, cub_tmp;
+    int nb[3] = {1, 1, 1};
+    int tile[3] = {8, 8, 8};
+};
+
+struct FieldStats {
+    int pruned = 0;
+    int z_slots = 0;
+    long long num_pairs = 0;
+    int grid[3] = {0, 0, 0};
+    int stencil = 0;
+};
+
+class Field {
+public:
+    explicit Field(const FieldSpec& spec);
+    ~Field();
+    Field(const Field&) = delete;
+    Field& operator=(const Field&) = delete;
+
+    // Host coordinate arrays (already non-dimensionalised).  In SOLVER_AX
+    // mode the field points are the particles.
+    void set_positions(const double* x, const double* y, const double* z, int n, cudaStream_t s);
+    void set_field_points(const double* x, const double* y, const double* z, int n, cudaStream_t s);
+
+    // Y = A X for M right-hand sides.  self_coef: device [N][M] complex (may
+    // be null => zero), jacobi: apply diag(self_coef)^-1 to the result rows.
+    // recip_fp32 / real_fp32 pick the arithmetic of the two halves.
+    void apply(const double2* X, double2* Y, int M, const double2* self_coef, bool jacobi, bool recip_fp32,
+               bool real_fp32, cudaStream_t s);
+
+    // Reciprocal-only / real-only parts (for split checks); same layout.
+    void apply_part(const double2* X, double2* Y, int M, const double2* self_coef, bool recip_fp32,
+                    bool real_fp32, int part, cudaStream_t s);
+
+    int num_particles() const { return N_; }
+    int num_targets() const { return spec_.solver_ax ? N_ : targets_.n; }
+    int num_quads() const { return Nq_; }
+    int rows_in() const { return 3 * N_ + 5 * Nq_; }
+    int rows_out() const { return 3 * num_targets() + 5 * Nq_; }
+    const FieldSpec& spec() const { return spec_; }
+    const EwaldGeom& geom() const { return geom_; }
+    FieldStats stats() const;
+    double selfo() const { return tables_.selfo; }
+    const int* quad_map_dev() const { return quad_map_.as<int>(); }
+    const int* quad_idx_dev() const { return quad_idx_.as<int>(); }
+
+private:
+    void precalc(cudaStream_t s);
+    void build_stencil(PointSet& ps, cudaStream_t s, bool bins);
+    void build_pairs(cudaStream_t s);
+    void choose_layout(cudaStream_t s);
+    void build_column_kernel(cudaStream_t s);
+    void build_scale(cudaStream_t s);
+    cufftHandle plan_for(int M, bool fp32);
+    template <typename R> void recip(const double2* X, double2* Y, int M, cudaStream_t s);
+    void real_part(const double2* X, double2* Y, int M, const double2* self_coef, bool jacobi, bool real_fp32,
+                   bool add_recip, cudaStream_t s);
+    void direct(const double2* X, double2* Y, int M, const double2* self_coef, bool jacobi, bool fp32,
+                cudaStream_t s);
+
+    FieldSpec spec_;
+    EwaldGeom geom_;
+    MonoTables tables_;
+    int N_ = 0, Nq_ = 0;
+    PointSet sources_, targets_;
+    GridView gv_{};
+    bool precalc_dirty_ = true;
+    std::vector<double> host_z_;    // source z coordinates (layout choice)
+
+    DevBuf quad_idx_, quad_map_, radius_;
+    DevBuf tab_r_, tab_f_;          // double[kTableSize], double[T_COUNT][kTableSize]
+    // CSR pairs by target
+    DevBuf pair_off_, pair_cnt_, pair_src_, pair_T64_, pair_T32_, pair_Q_, cell_key_, cell_idx_, cell_key_s_,
+        cell_idx_s_, cell_start_, cell_end_, cub_tmp_;
+    long long num_pairs_ = 0;
+    // reciprocal space
+    DevBuf grid_;                   // complex grid, sized for the largest use
+    DevBuf scale64_, scale32_;      // full layout: per-voxel scale
+    DevBuf colK64_, colK32_;        // pruned layout: per-column Toeplitz kernels
+    int colK_Z_ = -1;
+    int scale_built_ = 0;
+    struct PlanKey { int M; bool fp32; int pruned; int Zs; cufftHandle h; };
+    std::vector<PlanKey> plans_;
+};
+
+}  // namespace mpm

@@ -1,0 +1,679 @@
+// Batched device Krylov solvers (see mpm_krylov.h).
+#include "mpm_krylov.h"
+
+#include <algorithm>
+#include <cmath>
+
+namespace mpm {
+
+namespace {
+
+inline int nblk(long long n, int b) { return int((n + b - 1) / b); }
+
+// ----------------------------------------------------------- reductions --
+
+// out[i][m] = sum_row op(V_i[row][m]) * w[row][m], op = conj or identity.
+// Stage 1 writes per-CTA partials; stage 2 sums them.
+__global__ void __launch_bounds__(256) k_dots1(const double2* __restrict__ V, size_t vstride, int nvec,
+                                               const double2* __restrict__ w, int rows, int M, int conj,
+                                               double2* __restrict__ partial) {
+    __shared__ double2 red[8][8][32];
+    const int m = blockIdx.y * 32 + threadIdx.x;
+    const int i0 = blockIdx.z * 8;
+    double2 acc[8];
+    for (int k = 0; k < 8; ++k) acc[k] = make_double2(0, 0);
+    const int nv = min(8, nvec - i0);
+    if (m < M) {
+        for (int row = blockIdx.x * 8 + threadIdx.y; row < rows; row += gridDim.x * 8) {
+            const double2 wv = w[size_t(row) * M + m];
+            for (int k = 0; k < nv; ++k) {
+                const double2 v = V[size_t(i0 + k) * vstride + size_t(row) * M + m];
+                if (conj) acc[k] += conjmul(v, wv);
+                else acc[k] += v * wv;
+            }
+        }
+    }
+    for (int k = 0; k < 8; ++k) red[k][threadIdx.y][threadIdx.x] = acc[k];
+    __syncthreads();
+    if (threadIdx.y < nv && m < M) {
+        double2 s = make_double2(0, 0);
+        for (int r = 0; r < 8; ++r) s += red[threadIdx.y][r][threadIdx.x];
+        partial[(size_t(blockIdx.x) * nvec + i0 + threadIdx.y) * M + m] = s;
+    }
+}
+
+__global__ void k_dots2(const double2* __restrict__ partial, int gx, int nvec, int M, double2* __restrict__ out) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nvec * M) return;
+    double2 s = make_double2(0, 0);
+    for (int b = 0; b < gx; ++b) s += partial[size_t(b) * nvec * M + t];
+    out[t] = s;
+}
+
+__global__ void k_sqrt_re(const double2* __restrict__ in, int M, double* __restrict__ out) {
+    const int m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m < M) out[m] = sqrt(fmax(in[m].x, 0.0));
+}
+
+// w[row][m] += sgn * sum_{i < n_m} V_i[row][m] h[i][m]
+__global__ void k_vupdate(double2* __restrict__ w, const double2* __restrict__ V, size_t vstride, int nvec,
+                          const double2* __restrict__ h, int rows, int M, double sgn, const int* __restrict__ nper) {
+    const size_t t = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (t >= size_t(rows) * M) return;
+    const int m = int(t % M);
+    const int n = nper ? nper[m] : nvec;
+    double2 acc = make_double2(0, 0);
+    for (int i = 0; i < n; ++i) acc += V[size_t(i) * vstride + t] * h[size_t(i) * M + m];
+    w[t] += acc * sgn;
+}
+
+// out = a - b
+__global__ void k_sub(const double2* __restrict__ a, const double2* __restrict__ b, double2* __restrict__ out,
+                      size_t n) {
+    const size_t t = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (t < n) out[t] = a[t] - b[t];
+}
+
+// out = diag(self)^-1 in  over the unknown layout (jacobi_precond_kernel,
+// numerical_solver.cu:250-285: per particle 1/s, quads use their particle).
+__global__ void k_jacobi(const double2* __restrict__ in, double2* __restrict__ out, int N, int Nq, int M,
+                         const int* __restrict__ quad_idx, const double2* __restrict__ sc) {
+    const size_t t = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    const size_t rows = size_t(3 * N + 5 * Nq);
+    if (t >= rows * M) return;
+    const int row = int(t / M), m = int(t % M);
+    int p;
+    if (row < 3 * N) p = row / 3;
+    else {
+        p = quad_idx[(row - 3 * N) / 5];
+        if (p < 0 || p >= N) p = 0;
+    }
+    const double2 s = sc[size_t(p) * M + m];
+    const double den = s.x * s.x + s.y * s.y;
+    const double2 inv = den > 1e-30 ? make_double2(s.x / den, -s.y / den) : make_double2(1.0, 0.0);
+    out[t] = in[t] * inv;
+}
+
+// ------------------------------------------------------------ GMRES state --
+
+struct GState {
+    int active;      // still solving (outer)
+    int cyc;         // in the current Arnoldi cycle
+    int kcount;      // Arnoldi columns of the current cycle
+    int iters;       // total Arnoldi steps
+    int converged;
+    int pad[3];
+};
+
+// start of a restart cycle: residual norm test and V_0 = r / |r|
+__global__ void k_gm_begin(GState* __restrict__ st, const double* __restrict__ rn, const double* __restrict__ bn,
+                           double tol, int maxiter, int restart, double2* __restrict__ g, int M,
+                           int* __restrict__ flag) {
+    const int m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= M) return;
+    GState s = st[m];
+    s.cyc = 0;
+    s.kcount = 0;
+    if (s.active) {
+        if (rn[m] < tol * bn[m]) {
+            s.active = 0;
+            s.converged = 1;
+        } else if (s.iters >= maxiter) {
+            s.active = 0;
+        } else {
+            s.cyc = 1;
+            g[size_t(m) * (restart + 1)] = make_double2(rn[m], 0.0);
+            for (int i = 1; i <= restart; ++i) g[size_t(m) * (restart + 1) + i] = make_double2(0, 0);
+            atomicAdd(flag, 1);
+        }
+    }
+    st[m] = s;
+}
+
+// V_dst[row][m] = src[row][m] / nrm[m] for cycling RHS (0 otherwise)
+__global__ void k_normalize(const double2* __restrict__ src, double2* __restrict__ dst,
+                            const double* __restrict__ nrm, const GState* __restrict__ st, size_t n, int M) {
+    const size_t t = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    const int m = int(t % M);
+    const double d = nrm[m];
+    dst[t] = (st[m].cyc && d > 0.0) ? src[t] * (1.0 / d) : make_double2(0, 0);
+}
+
+// h += h2
+__global__ void k_addto(double2* __restrict__ a, const double2* __restrict__ b, int n) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < n) a[t] += b[t];
+}
+
+// Hessenberg column k, previous rotations, new rotation, residual estimate
+// (gmres_solver.cu:120-184), one thread per RHS.
+__global__ void k_gm_givens(GState* __restrict__ st, const double2* __restrict__ h, const double* __restrict__ wn,
+                            double2* __restrict__ H, double2* __restrict__ g, double* __restrict__ cs,
+                            double2* __restrict__ sn, int k, int restart, int M, const double* __restrict__ bn,
+                            double tol, int maxiter, int* __restrict__ flag) {
+    const int m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= M) return;
+    GState s = st[m];
+    if (!s.cyc) return;
+    const int ld = restart + 1;
+    double2* Hm = H + size_t(m) * ld * restart;   // column-major: Hm[col*ld + row]
+    double2* gm = g + size_t(m) * ld;
+    double* csm = cs + size_t(m) * restart;
+    double2* snm = sn + size_t(m) * restart;
+    double2* col = Hm + size_t(k) * ld;
+    for (int i = 0; i <= k; ++i) col[i] = h[size_t(i) * M + m];
+    col[k + 1] = make_double2(wn[m], 0.0);
+    for (int i = 0; i < k; ++i) {
+        const double2 h1 = col[i], h2 = col[i + 1];
+        const double c = csm[i];
+        const double2 sv = snm[i];
+        const double2 cs_ = make_double2(sv.x, -sv.y);
+        col[i] = h1 * c + cs_ * h2;
+        col[i + 1] = (sv * h1) * -1.0 + h2 * c;
+    }
+    const double2 h1 = col[k], h2 = col[k + 1];
+    double c = 1.0;
+    double2 sv = make_double2(0, 0);
+    if (h2.x != 0.0 || h2.y != 0.0) {
+        const double a1 = hypot(h1.x, h1.y);
+        if (a1 == 0.0) {
+            c = 0.0;
+            sv = make_double2(1.0, 0.0);
+        } else {
+            const double a2 = hypot(h2.x, h2.y);
+            const double sc = a1 + a2;
+            const double n1 = a1 / sc, n2 = a2 / sc;
+            const double hh = sc * sqrt(n1 * n1 + n2 * n2);
+            c = a1 / hh;
+            // (conj(h1)/|h1|) * (h2/hh)
+            const double2 u = make_double2(h1.x / a1, -h1.y / a1);
+            sv = u * make_double2(h2.x / hh, h2.y / hh);
+        }
+    }
+    csm[k] = c;
+    snm[k] = sv;
+    const double2 scj = make_double2(sv.x, -sv.y);
+    col[k] = h1 * c + scj * h2;
+    col[k + 1] = make_double2(0, 0);
+    const double2 g1 = gm[k], g2 = gm[k + 1];
+    gm[k] = g1 * c + scj * g2;
+    gm[k + 1] = (sv * g1) * -1.0 + g2 * c;
+    s.iters += 1;
+    const double resid = hypot(gm[k + 1].x, gm[k + 1].y);
+    if (resid < tol * bn[m] || k + 1 >= restart || s.iters >= maxiter) {
+        s.cyc = 0;
+        s.kcount = k + 1;
+    } else {
+        atomicAdd(flag, 1);
+    }
+    st[m] = s;
+}
+
+// back substitution H y = g, y stored [i][m]
+__global__ void k_gm_backsub(const GState* __restrict__ st, const double2* __restrict__ H,
+                             const double2* __restrict__ g, double2* __restrict__ y, int restart, int M,
+                             int* __restrict__ kper) {
+    const int m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= M) return;
+    const int k = st[m].kcount;
+    kper[m] = k;
+    const int ld = restart + 1;
+    const double2* Hm = H + size_t(m) * ld * restart;
+    const double2* gm = g + size_t(m) * ld;
+    for (int i = k - 1; i >= 0; --i) {
+        double2 v = gm[i];
+        for (int j = i + 1; j < k; ++j) v -= Hm[size_t(j) * ld + i] * y[size_t(j) * M + m];
+        const double2 d = Hm[size_t(i) * ld + i];
+        const double den = d.x * d.x + d.y * d.y;
+        y[size_t(i) * M + m] = make_double2((v.x * d.x + v.y * d.y) / den, (v.y * d.x - v.x * d.y) / den);
+    }
+}
+
+__global__ void k_zero_rhs_cols(double2* __restrict__ x, const double* __restrict__ bn, size_t n, int M) {
+    const size_t t = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    if (bn[t % M] == 0.0) x[t] = make_double2(0, 0);
+}
+
+__global__ void k_gm_init(GState* __restrict__ st, const double* __restrict__ bn, int M) {
+    const int m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= M) return;
+    GState s{};
+    s.active = bn[m] > 0.0 ? 1 : 0;
+    s.converged = bn[m] > 0.0 ? 0 : 1;
+    st[m] = s;
+}
+
+// --------------------------------------------------------- BiCGSTAB state --
+
+struct BState {
+    double2 rho, alpha, omega, beta;
+    int active, converged, iters, pad;
+};
+
+__global__ void k_bi_init(BState* __restrict__ st, const double* __restrict__ bn, const double* __restrict__ rn,
+                          double tol, int M) {
+    const int m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= M) return;
+    BState s{};
+    s.rho = s.alpha = s.omega = make_double2(1.0, 0.0);
+    s.beta = make_double2(0, 0);
+    s.active = 1;
+    if (bn[m] == 0.0) { s.active = 0; s.converged = 1; }
+    else if (rn[m] < tol * bn[m]) { s.active = 0; s.converged = 1; }
+    st[m] = s;
+}
+
+__device__ __forceinline__ double2 cdiv(double2 a, double2 b) {
+    const double den = b.x * b.x + b.y * b.y;
+    return make_double2((a.x * b.x + a.y * b.y) / den, (a.y * b.x - a.x * b.y) / den);
+}
+__device__ __forceinline__ double cabs_(double2 a) { return hypot(a.x, a.y); }
+
+// step A: rho_new test and beta (bicgstab_solver.cu:153-169)
+__global__ void k_bi_a(BState* __restrict__ st, const double2* __restrict__ rho_new, int it, int M) {
+    const int m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= M) return;
+    BState s = st[m];
+    if (!s.active) return;
+    const double2 rn = rho_new[m];
+    if (cabs_(rn) < 1e-16) { s.active = 0; st[m] = s; return; }
+    s.beta = it > 0 ? cdiv(rn, s.rho) * cdiv(s.alpha, s.omega) : make_double2(0, 0);
+    s.rho = rn;
+    s.iters += 1;
+    st[m] = s;
+}
+
+// p = r + beta (p - omega v)  (it > 0), p unchanged at it == 0
+__global__ void k_bi_p(double2* __restrict__ p, const double2* __restrict__ v, const double2* __restrict__ r,
+                       const BState* __restrict__ st, int it, size_t n, int M) {
+    const size_t t = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (t >= n || it == 0) return;
+    const BState& s = st[t % M];
+    if (!s.active) return;
+    p[t] = (p[t] - s.omega * v[t]) * s.beta + r[t];
+}
+
+// step B: alpha = rho / (r0 . v)
+__global__ void k_bi_b(BState* __restrict__ st, const double2* __restrict__ rv, int M) {
+    const int m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= M) return;
+    BState s = st[m];
+    if (!s.active) return;
+    if (cabs_(rv[m]) < 1e-16) { s.active = 0; st[m] = s; return; }
+    s.alpha = cdiv(s.rho, rv[m]);
+    st[m] = s;
+}
+
+// s = r - alpha v
+__global__ void k_bi_s(double2* __restrict__ sv, const double2* __restrict__ r, const double2* __restrict__ v,
+                       const BState* __restrict__ st, size_t n, int M) {
+    const size_t t = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    const BState& s = st[t % M];
+    if (!s.active) return;
+    sv[t] = r[t] - s.alpha * v[t];
+}
+
+// step C: |s| < tol |b| => x += alpha p and stop (mode 1)
+__global__ void k_bi_c(BState* __restrict__ st, const double* __restrict__ sn, const double* __restrict__ bn,
+                       double tol, int* __restrict__ mode, int M) {
+    const int m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= M) return;
+    BState s = st[m];
+    mode[m] = 0;
+    if (!s.active) return;
+    if (sn[m] < tol * bn[m]) {
+        mode[m] = 1;
+        s.active = 0;
+        s.converged = 1;
+        st[m] = s;
+    }
+}
+
+__global__ void k_bi_xfinal(double2* __restrict__ x, const double2* __restrict__ p, const BState* __restrict__ st,
+                            const int* __restrict__ mode, size_t n, int M) {
+    const size_t t = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    const int m = int(t % M);
+    if (mode[m] == 1) x[t] += st[m].alpha * p[t];
+}
+
+// step D: omega = (t, s) / (t, t)
+__global__ void k_bi_d(BState* __restrict__ st, const double2* __restrict__ ts, const double2* __restrict__ tt, int M) {
+    const int m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= M) return;
+    BState s = st[m];
+    if (!s.active) return;
+    if (cabs_(tt[m]) < 1e-16) { s.active = 0; st[m] = s; return; }
+    s.omega = ts[m] * (1.0 / tt[m].x);
+    st[m] = s;
+}
+
+// x += alpha p + omega s ; r = s - omega t
+__global__ void k_bi_xr(double2* __restrict__ x, double2* __restrict__ r, const double2* __restrict__ p,
+                        const double2* __restrict__ sv, const double2* __restrict__ tv,
+                        const BState* __restrict__ st, size_t n, int M) {
+    const size_t t = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    const BState& s = st[t % M];
+    if (!s.active) return;
+    x[t] += s.alpha * p[t] + s.omega * sv[t];
+    r[t] = sv[t] - s.omega * tv[t];
+}
+
+// step E: |r| < tol |b| or omega ~ 0 => stop; count still active
+__global__ void k_bi_e(BState* __restrict__ st, const double* __restrict__ rn, const double* __restrict__ bn,
+                       double tol, int maxiter, int* __restrict__ flag, int M) {
+    const int m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= M) return;
+    BState s = st[m];
+    if (!s.active) return;
+    if (rn[m] < tol * bn[m]) { s.active = 0; s.converged = 1; }
+    else if (cabs_(s.omega) < 1e-16) s.active = 0;
+    else if (s.iters >= maxiter) s.active = 0;
+    if (s.active) atomicAdd(flag, 1);
+    st[m] = s;
+}
+
+__global__ void k_bi_count(const BState* __restrict__ st, int* __restrict__ flag, int M) {
+    const int m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m < M && st[m].active) atomicAdd(flag, 1);
+}
+
+// refinement bookkeeping: zero the correction RHS of converged columns
+__global__ void k_mask_cols(double2* __restrict__ r, const double* __restrict__ rn, const double* __restrict__ bn,
+                            double tol, size_t n, int M) {
+    const size_t t = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    const int m = int(t % M);
+    if (rn[m] <= tol * bn[m]) r[t] = make_double2(0, 0);
+}
+
+__global__ void k_axpy1(double2* __restrict__ x, const double2* __restrict__ d, size_t n) {
+    const size_t t = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (t < n) x[t] += d[t];
+}
+
+}  // namespace
+
+// ------------------------------------------------------------ host side --
+
+BatchSolver::BatchSolver() { MPM_CUDA(cudaMallocHost(&flag_, sizeof(int))); }
+BatchSolver::~BatchSolver() {
+    if (flag_) cudaFreeHost(flag_);
+}
+
+int BatchSolver::read_flag(const int* dflag, cudaStream_t s) {
+    MPM_CUDA(cudaMemcpyAsync(flag_, dflag, sizeof(int), cudaMemcpyDeviceToHost, s));
+    MPM_CUDA(cudaStreamSynchronize(s));
+    return *flag_;
+}
+
+void BatchSolver::dots(const double2* V, size_t vstride, int nvec, const double2* w, int rows, int M, int conj,
+                       double2* out, cudaStream_t s) {
+    const int gx = std::max(1, std::min(296, (rows + 7) / 8));
+    partial_.ensure(sizeof(double2) * size_t(gx) * nvec * M);
+    dim3 grd(gx, (M + 31) / 32, (nvec + 7) / 8);
+    k_dots1<<<grd, dim3(32, 8), 0, s>>>(V, vstride, nvec, w, rows, M, conj, partial_.as<double2>());
+    MPM_LAUNCH();
+    k_dots2<<<nblk(nvec * M, 128), 128, 0, s>>>(partial_.as<double2>(), gx, nvec, M, out);
+    MPM_LAUNCH();
+}
+
+void BatchSolver::norms(const double2* w, int rows, int M, double* out, cudaStream_t s) {
+    h2_.ensure(sizeof(double2) * M);
+    dots(w, 0, 1, w, rows, M, 1, h2_.as<double2>(), s);
+    k_sqrt_re<<<nblk(M, 128), 128, 0, s>>>(h2_.as<double2>(), M, out);
+    MPM_LAUNCH();
+}
+
+void BatchSolver::true_residual(Field& F, const double2* b, const double2* x, int M, const double2* sc,
+                                std::vector<double>& out, cudaStream_t s) {
+    const int rows = F.rows_in();
+    const size_t n = size_t(rows) * M;
+    w_.ensure(sizeof(double2) * n);
+    rr_.ensure(sizeof(double2) * n);
+    rnorm_.ensure(sizeof(double) * M * 2);
+    F.apply(x, w_.as<double2>(), M, sc, false, false, false, s);
+    k_sub<<<nblk((long long)n, 256), 256, 0, s>>>(b, w_.as<double2>(), rr_.as<double2>(), n);
+    MPM_LAUNCH();
+    norms(rr_.as<double2>(), rows, M, rnorm_.as<double>(), s);
+    norms(b, rows, M, rnorm_.as<double>() + M, s);
+    std::vector<double> h(2 * M);
+    MPM_CUDA(cudaMemcpyAsync(h.data(), rnorm_.p, sizeof(double) * 2 * M, cudaMemcpyDeviceToHost, s));
+    MPM_CUDA(cudaStreamSynchronize(s));
+    out.resize(M);
+    for (int m = 0; m < M; ++m) out[m] = h[M + m] > 0 ? h[m] / h[M + m] : 0.0;
+}
+
+void BatchSolver::gmres(Field& F, const double2* b, double2* x, int M, const double2* sc, const SolveOptions& opt,
+                        SolveStats& st, bool r32, bool re32, cudaStream_t s) {
+    const int rows = F.rows_in();
+    const size_t n = size_t(rows) * M;
+    const int restart = std::max(1, std::min(rows, opt.restart));
+    V_.ensure(sizeof(double2) * n * (restart + 1));
+    H_.ensure(sizeof(double2) * size_t(M) * (restart + 1) * restart);
+    g_.ensure(sizeof(double2) * size_t(M) * (restart + 1));
+    cs_.ensure(sizeof(double) * size_t(M) * restart);
+    sn_.ensure(sizeof(double2) * size_t(M) * restart);
+    y_.ensure(sizeof(double2) * size_t(M) * restart);
+    h_.ensure(sizeof(double2) * size_t(M) * (restart + 1));
+    h2_.ensure(sizeof(double2) * size_t(M) * (restart + 1));
+    bnorm_.ensure(sizeof(double) * M);
+    rnorm_.ensure(sizeof(double) * M * 2);
+    state_.ensure(sizeof(GState) * M + sizeof(int) * M);
+    w_.ensure(sizeof(double2) * n);
+    r_.ensure(sizeof(double2) * n);
+    bj_.ensure(sizeof(double2) * n);
+    flagdev_.ensure(sizeof(int));
+    double2* V = V_.as<double2>();
+    GState* gs = state_.as<GState>();
+    int* kper = reinterpret_cast<int*>(gs + M);
+    int* dflag = flagdev_.as<int>();
+    const int mb = nblk(M, 128);
+    const int vb = nblk((long long)n, 256);
+
+    norms(b, rows, M, bnorm_.as<double>(), s);
+    k_gm_init<<<mb, 128, 0, s>>>(gs, bnorm_.as<double>(), M);
+    k_zero_rhs_cols<<<vb, 256, 0, s>>>(x, bnorm_.as<double>(), n, M);
+    MPM_LAUNCH();
+    const double2* bj = b;
+    if (opt.jacobi) {
+        k_jacobi<<<vb, 256, 0, s>>>(b, bj_.as<double2>(), F.num_particles(), F.num_quads(), M, F.quad_idx_dev(), sc);
+        MPM_LAUNCH();
+        bj = bj_.as<double2>();
+    }
+    while (true) {
+        // r = D^-1 (b - A x)
+        F.apply(x, w_.as<double2>(), M, sc, opt.jacobi, r32, re32, s);
+        st.matvecs++;
+        k_sub<<<vb, 256, 0, s>>>(bj, w_.as<double2>(), r_.as<double2>(), n);
+        MPM_LAUNCH();
+        norms(r_.as<double2>(), rows, M, rnorm_.as<double>(), s);
+        MPM_CUDA(cudaMemsetAsync(dflag, 0, sizeof(int), s));
+        k_gm_begin<<<mb, 128, 0, s>>>(gs, rnorm_.as<double>(), bnorm_.as<double>(), opt.tol, opt.maxiter, restart,
+                                      g_.as<double2>(), M, dflag);
+        MPM_LAUNCH();
+        k_normalize<<<vb, 256, 0, s>>>(r_.as<double2>(), V, rnorm_.as<double>(), gs, n, M);
+        MPM_LAUNCH();
+        if (read_flag(dflag, s) == 0) break;
+        for (int k = 0; k < restart; ++k) {
+            double2* Vk = V + size_t(k) * n;
+            double2* w = w_.as<double2>();
+            F.apply(Vk, w, M, sc, opt.jacobi, r32, re32, s);
+            st.matvecs++;
+            // CGS2
+            dots(V, n, k + 1, w, rows, M, 1, h_.as<double2>(), s);
+            k_vupdate<<<vb, 256, 0, s>>>(w, V, n, k + 1, h_.as<double2>(), rows, M, -1.0, nullptr);
+            MPM_LAUNCH();
+            dots(V, n, k + 1, w, rows, M, 1, h2_.as<double2>(), s);
+            k_vupdate<<<vb, 256, 0, s>>>(w, V, n, k + 1, h2_.as<double2>(), rows, M, -1.0, nullptr);
+            k_addto<<<nblk((k + 1) * M, 128), 128, 0, s>>>(h_.as<double2>(), h2_.as<double2>(), (k + 1) * M);
+            MPM_LAUNCH();
+            norms(w, rows, M, rnorm_.as<double>(), s);
+            k_normalize<<<vb, 256, 0, s>>>(w, V + size_t(k + 1) * n, rnorm_.as<double>(), gs, n, M);
+            MPM_CUDA(cudaMemsetAsync(dflag, 0, sizeof(int), s));
+            k_gm_givens<<<mb, 128, 0, s>>>(gs, h_.as<double2>(), rnorm_.as<double>(), H_.as<double2>(),
+                                           g_.as<double2>(), cs_.as<double>(), sn_.as<double2>(), k, restart, M,
+                                           bnorm_.as<double>(), opt.tol, opt.maxiter, dflag);
+            MPM_LAUNCH();
+            if (read_flag(dflag, s) == 0) break;
+        }
+        k_gm_backsub<<<mb, 128, 0, s>>>(gs, H_.as<double2>(), g_.as<double2>(), y_.as<double2>(), restart, M, kper);
+        k_vupdate<<<vb, 256, 0, s>>>(x, V, n, restart, y_.as<double2>(), rows, M, 1.0, kper);
+        MPM_LAUNCH();
+    }
+    std::vector<GState> h(M);
+    MPM_CUDA(cudaMemcpyAsync(h.data(), gs, sizeof(GState) * M, cudaMemcpyDeviceToHost, s));
+    MPM_CUDA(cudaStreamSynchronize(s));
+    st.iters.resize(M);
+    st.converged.resize(M);
+    for (int m = 0; m < M; ++m) {
+        st.iters[m] += h[m].iters;
+        st.converged[m] = h[m].converged;
+    }
+}
+
+void BatchSolver::bicgstab(Field& F, const double2* b, double2* x, int M, const double2* sc, const SolveOptions& opt,
+                           SolveStats& st, bool r32, bool re32, cudaStream_t s) {
+    const int rows = F.rows_in();
+    const size_t n = size_t(rows) * M;
+    for (DevBuf* d : {&r0_, &p_, &v_, &s_, &t_, &r_, &w_, &bj_}) d->ensure(sizeof(double2) * n);
+    bnorm_.ensure(sizeof(double) * M);
+    rnorm_.ensure(sizeof(double) * M * 2);
+    scal_.ensure(sizeof(BState) * M + sizeof(int) * M);
+    h_.ensure(sizeof(double2) * M * 2);
+    flagdev_.ensure(sizeof(int));
+    BState* bs = scal_.as<BState>();
+    int* mode = reinterpret_cast<int*>(bs + M);
+    int* dflag = flagdev_.as<int>();
+    double2* hv = h_.as<double2>();
+    const int mb = nblk(M, 128);
+    const int vb = nblk((long long)n, 256);
+
+    norms(b, rows, M, bnorm_.as<double>(), s);
+    k_zero_rhs_cols<<<vb, 256, 0, s>>>(x, bnorm_.as<double>(), n, M);
+    const double2* bj = b;
+    if (opt.jacobi) {
+        k_jacobi<<<vb, 256, 0, s>>>(b, bj_.as<double2>(), F.num_particles(), F.num_quads(), M, F.quad_idx_dev(), sc);
+        bj = bj_.as<double2>();
+    }
+    MPM_LAUNCH();
+    double2* r = r_.as<double2>();
+    F.apply(x, w_.as<double2>(), M, sc, opt.jacobi, r32, re32, s);
+    st.matvecs++;
+    k_sub<<<vb, 256, 0, s>>>(bj, w_.as<double2>(), r, n);
+    MPM_LAUNCH();
+    norms(r, rows, M, rnorm_.as<double>(), s);
+    k_bi_init<<<mb, 128, 0, s>>>(bs, bnorm_.as<double>(), rnorm_.as<double>(), opt.tol, M);
+    MPM_CUDA(cudaMemcpyAsync(r0_.p, r, sizeof(double2) * n, cudaMemcpyDeviceToDevice, s));
+    MPM_CUDA(cudaMemcpyAsync(p_.p, r, sizeof(double2) * n, cudaMemcpyDeviceToDevice, s));
+    MPM_CUDA(cudaMemsetAsync(v_.p, 0, sizeof(double2) * n, s));
+    MPM_CUDA(cudaMemsetAsync(dflag, 0, sizeof(int), s));
+    k_bi_count<<<mb, 128, 0, s>>>(bs, dflag, M);
+    MPM_LAUNCH();
+    if (read_flag(dflag, s) > 0) {
+        for (int it = 0; it < opt.maxiter; ++it) {
+            dots(r0_.as<double2>(), 0, 1, r, rows, M, 0, hv, s);
+            k_bi_a<<<mb, 128, 0, s>>>(bs, hv, it, M);
+            k_bi_p<<<vb, 256, 0, s>>>(p_.as<double2>(), v_.as<double2>(), r, bs, it, n, M);
+            MPM_LAUNCH();
+            F.apply(p_.as<double2>(), v_.as<double2>(), M, sc, opt.jacobi, r32, re32, s);
+            st.matvecs++;
+            dots(r0_.as<double2>(), 0, 1, v_.as<double2>(), rows, M, 0, hv, s);
+            k_bi_b<<<mb, 128, 0, s>>>(bs, hv, M);
+            k_bi_s<<<vb, 256, 0, s>>>(s_.as<double2>(), r, v_.as<double2>(), bs, n, M);
+            MPM_LAUNCH();
+            norms(s_.as<double2>(), rows, M, rnorm_.as<double>(), s);
+            k_bi_c<<<mb, 128, 0, s>>>(bs, rnorm_.as<double>(), bnorm_.as<double>(), opt.tol, mode, M);
+            k_bi_xfinal<<<vb, 256, 0, s>>>(x, p_.as<double2>(), bs, mode, n, M);
+            MPM_LAUNCH();
+            F.apply(s_.as<double2>(), t_.as<double2>(), M, sc, opt.jacobi, r32, re32, s);
+            st.matvecs++;
+            dots(t_.as<double2>(), 0, 1, s_.as<double2>(), rows, M, 1, hv, s);
+            dots(t_.as<double2>(), 0, 1, t_.as<double2>(), rows, M, 1, hv + M, s);
+            k_bi_d<<<mb, 128, 0, s>>>(bs, hv, hv + M, M);
+            k_bi_xr<<<vb, 256, 0, s>>>(x, r, p_.as<double2>(), s_.as<double2>(), t_.as<double2>(), bs, n, M);
+            MPM_LAUNCH();
+            norms(r, rows, M, rnorm_.as<double>(), s);
+            MPM_CUDA(cudaMemsetAsync(dflag, 0, sizeof(int), s));
+            k_bi_e<<<mb, 128, 0, s>>>(bs, rnorm_.as<double>(), bnorm_.as<double>(), opt.tol, opt.maxiter, dflag, M);
+            MPM_LAUNCH();
+            if (read_flag(dflag, s) == 0) break;
+        }
+    }
+    std::vector<BState> h(M);
+    MPM_CUDA(cudaMemcpyAsync(h.data(), bs, sizeof(BState) * M, cudaMemcpyDeviceToHost, s));
+    MPM_CUDA(cudaStreamSynchronize(s));
+    st.iters.resize(M);
+    st.converged.resize(M);
+    for (int m = 0; m < M; ++m) {
+        st.iters[m] += h[m].iters;
+        st.converged[m] = h[m].converged;
+    }
+}
+
+void BatchSolver::solve(Field& F, const double2* b, double2* x, int M, const double2* sc, const SolveOptions& opt,
+                        SolveStats& st, cudaStream_t s) {
+    st.iters.assign(M, 0);
+    st.converged.assign(M, 0);
+    st.matvecs = 0;
+    st.refine_steps = 0;
+    if (!opt.refine) {
+        if (opt.method == SOLVER_BICGSTAB) bicgstab(F, b, x, M, sc, opt, st, opt.recip_fp32, opt.real_fp32, s);
+        else gmres(F, b, x, M, sc, opt, st, opt.recip_fp32, opt.real_fp32, s);
+        return;
+    }
+    // Mixed-precision iterative refinement: fp64 true residual outside,
+    // fp32 operator inside.
+    const int rows = F.rows_in();
+    const size_t n = size_t(rows) * M;
+    xr_.ensure(sizeof(double2) * n);
+    d_.ensure(sizeof(double2) * n);
+    DevBuf bn2, rn2;
+    bn2.ensure(sizeof(double) * M);
+    rn2.ensure(sizeof(double) * M);
+    const int vb = nblk((long long)n, 256);
+    norms(b, rows, M, bn2.as<double>(), s);
+    SolveOptions in = opt;
+    in.refine = false;
+    in.tol = opt.inner_tol;
+    std::vector<int> conv(M, 0);
+    for (int step = 0; step < opt.max_refine; ++step) {
+        F.apply(x, xr_.as<double2>(), M, sc, false, false, false, s);
+        st.matvecs++;
+        k_sub<<<vb, 256, 0, s>>>(b, xr_.as<double2>(), xr_.as<double2>(), n);
+        MPM_LAUNCH();
+        norms(xr_.as<double2>(), rows, M, rn2.as<double>(), s);
+        std::vector<double> hb(M), hr(M);
+        MPM_CUDA(cudaMemcpyAsync(hb.data(), bn2.p, sizeof(double) * M, cudaMemcpyDeviceToHost, s));
+        MPM_CUDA(cudaMemcpyAsync(hr.data(), rn2.p, sizeof(double) * M, cudaMemcpyDeviceToHost, s));
+        MPM_CUDA(cudaStreamSynchronize(s));
+        int left = 0;
+        st.rel_resid.assign(M, 0.0);
+        for (int m = 0; m < M; ++m) {
+            st.rel_resid[m] = hb[m] > 0 ? hr[m] / hb[m] : 0.0;
+            conv[m] = hr[m] <= opt.tol * hb[m];
+            left += !conv[m];
+        }
+        if (!left) break;
+        k_mask_cols<<<vb, 256, 0, s>>>(xr_.as<double2>(), rn2.as<double>(), bn2.as<double>(), opt.tol, n, M);
+        MPM_CUDA(cudaMemsetAsync(d_.p, 0, sizeof(double2) * n, s));
+        SolveStats inner;
+        inner.iters.assign(M, 0);
+        if (opt.method == SOLVER_BICGSTAB)
+            bicgstab(F, xr_.as<double2>(), d_.as<double2>(), M, sc, in, inner, true, true, s);
+        else
+            gmres(F, xr_.as<double2>(), d_.as<double2>(), M, sc, in, inner, true, true, s);
+        k_axpy1<<<vb, 256, 0, s>>>(x, d_.as<double2>(), n);
+        MPM_LAUNCH();
+        for (int m = 0; m < M; ++m) st.iters[m] += inner.iters[m];
+        st.matvecs += inner.matvecs;
+        st.refine_steps++;
+    }
+    for (int m = 0; m < M; ++m) st.converged[m] = conv[m];
+}
+
+}  // namespace mpm

@@ -1,0 +1,30 @@
+// Real-space pair functions of the monodisperse spectral-Ewald split.
+//
+// Each function is tabulated on r = 0 (self value) and r = 1 + k*0.001,
+// k = 0..8999, and looked up by linear interpolation, exactly as the
+// reference does (monodisperse_ewald_electric_field.cu:92-542 builds the
+// tables, :668-685 interpolates) so that pair couplings agree to rounding.
+#pragma once
+#include <vector>
+
+namespace mpm {
+
+enum TableId { T_FD1 = 0, T_FD2, T_FQ1, T_FQ2, T_FQ3, T_GQ1, T_GQ2, T_GQ3, T_GQ4, T_COUNT };
+
+constexpr int kTableSteps = 9000;         // r = 1 .. 9.999
+constexpr int kTableSize = kTableSteps + 1;  // plus the r = 0 entry
+constexpr double kTableDr = 0.001;
+
+struct MonoTables {
+    std::vector<double> r;                 // kTableSize
+    std::vector<double> f[T_COUNT];        // kTableSize each
+    double selfo = 0.0;                    // r = 0 entry of the dipole tables
+    double self_grad = 0.0;                // r = 0 entry of the gradient tables
+};
+
+MonoTables build_mono_tables(double xi);
+
+// Host copy of the device lookup (used by tests and host precalcs).
+double table_lookup(double r, const double* r_table, const double* y, int n);
+
+}  // namespace mpm

@@ -1,0 +1,172 @@
+/*
+ * cumpm_b200.h -- C ABI of the B200-native Mutual Polarization Method solve.
+ *
+ * Drop-in boundary for the reference cuMPM (TannerWilcoxson/cuMPM) hot path:
+ * the self-consistent dipole/quadrupole solve behind cuMPM.dipole_solver and
+ * cuMPM.Near_Field.  Every entry point returns an int status (MPM_OK on
+ * success); mpm_last_error() gives the message of the last failure on the
+ * calling thread.  Complex arrays are interleaved (re, im) doubles, i.e. the
+ * memory layout of C99 double _Complex / std::complex<double> /
+ * numpy.complex128.  No entry point terminates the process.
+ *
+ * Reference interfaces replaced (file:line in the reference project):
+ *   mpm_solver_*  -> Dipole_Solver (src/cpp/dipole_solver.h:14-166,
+ *                    bound in src/cpp/dipole_solver_bindings.cpp:80-178)
+ *   mpm_near_*    -> Near_Field (src/cpp/near_field.h:12-58,
+ *                    bound in src/cpp/near_field_bindings.cpp:8-25)
+ *   mpm_field_*   -> Electric_Field / Monodisperse_Ewald_Electric_Field /
+ *                    Direct_Electric_Field (src/cpp/electric_field/
+ *                    electric_field.h:13-141, calculate() at
+ *                    monodisperse_ewald_electric_field.cu:2485-2503 and
+ *                    direct_electric_field.cu:555-559), here batched over M
+ *                    right-hand sides on caller-owned device buffers
+ *   mpm_batch_solve -> Numerical_Solver::solve (src/cpp/numerical_solver/
+ *                    numerical_solver.h:34-40; GMRES gmres_solver.cu:56-208,
+ *                    BiCGSTAB bicgstab_solver.cu:58-192), batched
+ */
+#ifndef CUMPM_B200_H
+#define CUMPM_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define MPM_API __attribute__((visibility("default")))
+#else
+#define MPM_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+#define MPM_OK 0
+#define MPM_ERR_INVALID 1   /* bad argument (maps to Python ValueError) */
+#define MPM_ERR_RUNTIME 2   /* runtime/configuration error (RuntimeError) */
+#define MPM_ERR_CUDA 3      /* CUDA / cuFFT failure */
+
+/* precision (reference PrecisionMode, electric_field/direct_electric_field.h:10-16) */
+#define MPM_PREC_AUTO 0     /* fp32 reciprocal space / fp32 direct sum */
+#define MPM_PREC_MIXED 1
+#define MPM_PREC_DOUBLE 2
+
+/* field kinds and modes (reference FieldCalcMode, electric_field.h:8-11) */
+#define MPM_FIELD_DIRECT 0
+#define MPM_FIELD_MONO 1
+#define MPM_MODE_SOLVER_AX 0
+#define MPM_MODE_INTERACTION 1
+
+#define MPM_METHOD_GMRES 0
+#define MPM_METHOD_BICGSTAB 1
+
+typedef struct mpm_solver mpm_solver;
+typedef struct mpm_near mpm_near;
+typedef struct mpm_field mpm_field;
+
+typedef struct mpm_solve_options {
+    int method;        /* MPM_METHOD_* */
+    int restart;       /* GMRES restart length (reference: 50) */
+    int maxiter;       /* per right-hand side (reference: 1000) */
+    double tol;        /* stop when |D^-1(b - A x)| < tol |b| (inner rule) */
+    int jacobi;        /* diagonal (self-coefficient) preconditioning */
+    int recip_fp32;    /* fp32 reciprocal space */
+    int real_fp32;     /* fp32 real-space pair sum */
+    int refine;        /* fp64 true-residual iterative refinement around fp32 solves */
+    double inner_tol;  /* relative tolerance of each refinement's inner solve */
+} mpm_solve_options;
+
+typedef struct mpm_solve_report {
+    int matvecs;           /* batched operator applications */
+    int refine_steps;
+    int total_iterations;  /* sum over right-hand sides */
+    int max_iterations;
+    int num_converged;
+    double max_rel_resid;  /* true fp64 |b-Ax|/|b| (refinement mode), else -1 */
+} mpm_solve_report;
+
+typedef struct mpm_field_info {
+    int kind, mode;
+    int num_particles, num_targets, num_quads;
+    int grid[3];
+    int stencil;           /* Gaussian support per axis */
+    int pruned;            /* 1: occupied-plane (slab) reciprocal transform */
+    int z_slots;           /* stored z planes */
+    long long num_pairs;   /* real-space (target, source) pairs */
+    double rc, h[3], eta[3], selfo;
+} mpm_field_info;
+
+MPM_API const char* mpm_last_error(void);
+MPM_API const char* mpm_version(void);
+
+/* ---- Dipole_Solver ------------------------------------------------------
+ * eps: n_freq x eps_cols complex (eps_cols == 1 or number of particles).
+ * radius: n_radius values (0 => 1.0 for every particle, 1 => shared).
+ * E0: n_E0 vectors, vector k has E0_sizes[k] complex entries (3, 3N or
+ *     3N+5Nq); n_E0 == 0 => three unit polarisations.
+ * quad_idxs: n_quad_idxs particle indices (0 with solve_quads => all). */
+MPM_API int mpm_solver_create(mpm_solver** out, const double box[3], const double* eps, int n_freq, int eps_cols,
+                      const double* radius, int n_radius, double eps_m, double xi, double tol, int quiet,
+                      const char* guess_type, const char* solver_type, const char* field_type, const double* E0,
+                      const int* E0_sizes, int n_E0, int solve_quads, const int* quad_idxs, int n_quad_idxs,
+                      int precision);
+MPM_API void mpm_solver_destroy(mpm_solver* s);
+/* one frame (reference Dipole_Solver::compute, dipole_solver.cu:495) */
+MPM_API int mpm_solver_compute(mpm_solver* s, const double* x, const double* y, const double* z, int n);
+/* dims: frames, wavevectors, particles, polarizations, quads */
+MPM_API int mpm_solver_dims(const mpm_solver* s, int64_t dims[5]);
+/* outputs sized frames*W*N*K*3, frames*W*Nq*K*5 and W*K*3 complex */
+MPM_API int mpm_solver_get_dipoles(const mpm_solver* s, int physical, double* out, size_t n_complex);
+MPM_API int mpm_solver_get_quadrupoles(const mpm_solver* s, int physical, double* out, size_t n_complex);
+MPM_API int mpm_solver_get_eff_polarizability(const mpm_solver* s, int physical, double* out, size_t n_complex);
+MPM_API int mpm_solver_set_jacobi(mpm_solver* s, int enable);
+MPM_API int mpm_solver_get_jacobi(const mpm_solver* s, int* enable);
+/* extras beyond the reference: restart, maxiter, all-frequency batching,
+ * mixed-precision refinement */
+MPM_API int mpm_solver_set_options(mpm_solver* s, int restart, int maxiter, int batch_all, int refine, double inner_tol,
+                           int real_fp32);
+/* iterations of every right-hand side solved so far, in solve order */
+MPM_API int mpm_solver_iterations(const mpm_solver* s, int* out, size_t cap, size_t* n_out);
+
+/* ---- Near_Field --------------------------------------------------------- */
+MPM_API int mpm_near_create(mpm_near** out, const double box[3], const double E0[6], const double* radius, int n_radius,
+                    double xi, double errortol, const char* field_type);
+MPM_API void mpm_near_destroy(mpm_near* nf);
+MPM_API int mpm_near_set_dipoles(mpm_near* nf, const double* dip, int n_complex);
+MPM_API int mpm_near_set_dipole_positions(mpm_near* nf, const double* x, const double* y, const double* z, int n);
+MPM_API int mpm_near_set_field_points(mpm_near* nf, const double* x, const double* y, const double* z, int n);
+MPM_API int mpm_near_calculate(mpm_near* nf, double* intensity, int n);
+
+/* ---- field operator on device buffers ----------------------------------
+ * X, Y: device complex128 [rows][M], rows = 3*N (+ 5*Nq).  self_coef:
+ * device complex128 [N][M] or NULL.  stream: cudaStream_t or NULL. */
+MPM_API int mpm_field_create(mpm_field** out, int kind, int mode, const double box[3], double errortol, double xi,
+                     const double* radius, int n_radius, int solve_quads, const int* quad_idxs, int n_quad_idxs);
+MPM_API void mpm_field_destroy(mpm_field* f);
+MPM_API int mpm_field_set_positions(mpm_field* f, const double* x, const double* y, const double* z, int n, void* stream);
+MPM_API int mpm_field_set_field_points(mpm_field* f, const double* x, const double* y, const double* z, int n,
+                               void* stream);
+MPM_API int mpm_field_apply(mpm_field* f, const void* X, void* Y, int M, const void* self_coef, int jacobi, int recip_fp32,
+                    int real_fp32, void* stream);
+/* part 0: reciprocal space only; part 1: real space + self only */
+MPM_API int mpm_field_apply_part(mpm_field* f, const void* X, void* Y, int M, const void* self_coef, int recip_fp32,
+                         int real_fp32, int part, void* stream);
+MPM_API int mpm_field_info_get(const mpm_field* f, mpm_field_info* info);
+
+/* batched Krylov solve A X = B on device buffers (X holds the guess) */
+MPM_API int mpm_batch_solve(mpm_field* f, const void* B, void* X, int M, const void* self_coef,
+                    const mpm_solve_options* opt, mpm_solve_report* report, void* stream);
+
+/* ---- host-only helpers (no GPU needed) ---------------------------------- */
+/* real-space tables: out has 10 x 9001 doubles (r, fd1, fd2, fq1, fq2, fq3,
+ * gq1, gq2, gq3, gq4); selfo/self_grad may be NULL */
+MPM_API int mpm_mono_tables(double xi, double* out, double* selfo, double* self_grad);
+/* Ewald parameters for a box: grid[3], stencil, rc, h[3], eta[3] */
+MPM_API int mpm_ewald_geometry(const double box[3], double errortol, double xi, int grid[3], int* stencil, double* rc,
+                       double h[3], double eta[3]);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CUMPM_B200_H */
