@@ -130,7 +130,7 @@ class dipole_solver:
         pos = _to_numpy(positions)
         if pos.ndim == 2:
             pos = pos[np.newaxis, ...]
-        elif pos.ndim != 3 or pos.shape[-1] != 3:
+        if pos.ndim != 3 or pos.shape[-1] != 3:
             raise ValueError("positions must be of shape (num_particles, 3) or (num_frames, num_particles, 3)")
         pos = np.ascontiguousarray(pos, dtype=np.float64)
         for frame in pos:
