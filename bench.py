@@ -1,0 +1,425 @@
+#!/usr/bin/env python
+"""solves/s of the self-consistent dipole solve on a B200.
+
+Workload (one "step"): the N=4000 hexagonal monolayer of radius-5 nm spheres
+(nearest-neighbour spacing 12 nm, rows of 128, periodic in-plane box with a
+vacuum gap along z: 1542.0 x 332.6 x 1000 nm), Drude spheres
+(eps_inf 4.0, omega_p 1.8 eV, gamma 0.1 eV) in eps_m = 1.77, 10 frequencies
+evenly spaced over 0.2-1.0 eV x 3 incident polarisations = 30 right-hand
+sides, Ewald accuracy = tol = 1e-6, GMRES(50) with Jacobi preconditioning.
+A step is the per-frame precalculation plus the solve of all 30 right-hand
+sides to a true fp64 relative residual |b - A x| / |b| <= 1e-6; a solve is
+one converged right-hand side.
+
+This arm: all 30 right-hand sides in one batch, fp32 operator inside fp64
+iterative refinement.  `value` is device-timed with device-resident inputs;
+`e2e` runs the same workload through the public drop-in API
+(cumpm_b200.dipole_solver) with host inputs and outputs.
+
+`--impl reference` times the CPU port of the reference algorithm (oracle/)
+on the host cores, per the measurement rules of this project.
+
+Multi-GPU (torchrun): every rank solves an independent replica (the same
+geometry at its own frequency set); no collective on the data path.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N_PART = 4000
+SPACING = 12.0
+RADIUS = 5.0
+EPS_M = 1.77
+TOL = 1e-6
+XI = 0.5
+N_FREQ = 10
+K_POL = 3
+# GMRES(50)+Jacobi matvecs per right-hand side of the reference algorithm on
+# this workload (fp64 operator, reference stop rule), measured on a B200 by
+# this arm's plain-fp64 leg; used to turn one timed CPU matvec into solves/s.
+PLAIN_MATVECS_PER_SOLVE = 40.0
+
+
+def hex_lattice(n, spacing):
+    """Rows of 2*ceil(sqrt(n)) sites, odd rows shifted by half a spacing."""
+    lim = int(np.ceil(np.sqrt(n))) * 2
+    j, i = np.divmod(np.arange(n), lim)
+    return np.stack([(i + 0.5 * (j % 2)) * spacing, j * (np.sqrt(3) / 2) * spacing, np.zeros(n)], axis=1)
+
+
+def workload(rank=0):
+    pos = hex_lattice(N_PART, SPACING)
+    rc = 5.256522
+    mn = 2.1 * rc * RADIUS
+    box = np.array([max(pos[:, 0].max() + SPACING, mn), max(pos[:, 1].max() + SPACING * np.sqrt(3) / 2, mn), 1000.0])
+    lo, hi = 0.2, 1.0
+    if rank:  # independent replica per rank: shifted frequency set
+        lo, hi = 0.2 + 0.01 * rank, 1.0 + 0.01 * rank
+    omega = np.linspace(lo, hi, N_FREQ)
+    eps = 4.0 - 1.8 ** 2 / (omega ** 2 + 1j * omega * 0.1)
+    return pos, box, eps
+
+
+def device_problem(pos, box, eps, torch, dev):
+    """Non-dimensionalised device buffers in the [row][M] layout."""
+    N = len(pos)
+    M = N_FREQ * K_POL
+    e = eps / EPS_M
+    s = 3.0 / (4 * np.pi * (e - 1.0))  # self coefficient, radius 1
+    sc = np.repeat(np.repeat(s, K_POL)[None, :], N, axis=0)
+    B = np.zeros((3 * N, M), complex)
+    for m in range(M):
+        B[m % K_POL::3, m] = 1.0
+    # mean-field initial guess 4 pi a^3 beta / (1 - beta phi) E0
+    phi = N * 4.0 / 3.0 * np.pi / np.prod(box / RADIUS)
+    beta = (e - 1) / (e + 2)
+    g = 4 * np.pi * beta / (1 - beta * phi)
+    X0 = B * np.repeat(g, K_POL)[None, :]
+    t = lambda a: torch.tensor(a, dtype=torch.complex128, device=dev)
+    return t(B), t(X0), t(sc)
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.idx = gpu_index
+        self.rows = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.idx), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.th = threading.Thread(target=self._read, daemon=True)
+            self.th.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([c.strip() for c in line.split(",")])
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.th.join(timeout=2)
+        sm = [float(r[1]) for r in self.rows if len(r) >= 9 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if len(r) >= 9 and r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in self.rows if len(r) >= 9 for k in range(4) if r[5 + k] == "Active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def ncu_traffic():
+    """Per-launch DRAM bytes of the profiled kernels (profiles/traffic.json)."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
+            return json.load(f)
+    except Exception:
+        return {}
+
+
+def algorithmic_bytes(info, M, n_pairs, fp64):
+    """Minimum DRAM bytes of one launch of each stage of the batched matvec.
+
+    Grid G = stored voxels x 3M complex (spread writes it once, each FFT
+    reads and writes it once, the k-space step reads and writes it once,
+    contraction reads it once); moments/fields are [3N][M] complex128.
+    """
+    s = 16 if fp64 else 8
+    nx, ny, nz = info["grid"]
+    zs = info["z_slots"] if info["pruned"] else nz
+    N = info["num_particles"]
+    G = nx * ny * zs * 3 * M * s
+    mom = 3 * N * M * 16
+    S = info["stencil"]
+    b = {
+        "spread": G + mom + N * 3 * S * (8 if fp64 else 4),
+        "fft_fwd": 2 * G,
+        "kspace": 2 * G + (nx * ny * 6 * (2 * zs - 1) * s if info["pruned"] else nx * ny * nz * (8 if fp64 else 4)),
+        "fft_inv": 2 * G,
+        "contract": G + mom + N * 3 * S * (8 if fp64 else 4),
+        "real": n_pairs * (4 + (64 if fp64 else 32)) + 3 * mom,
+    }
+    return b
+
+
+def run_ours(args, rank, world, local_rank):
+    import torch
+
+    from cumpm_b200 import capi
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    pos_nm, box_nm, eps = workload(rank)
+    pos = pos_nm / RADIUS
+    box = box_nm / RADIUS
+    F = capi.Field(capi.FIELD_MONO, box, TOL, XI)
+    B, X0, S = device_problem(pos, box, eps, torch, dev)
+    X = torch.empty_like(X0)
+    M = B.shape[1]
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    opts = dict(tol=TOL, method=capi.METHOD_GMRES, restart=50, maxiter=1000, refine=True, inner_tol=args.inner_tol)
+    reports = []
+
+    def step():
+        F.set_positions(pos)
+        X.copy_(X0)
+        reports.append(F.batch_solve(B, X, S, **opts))
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    info = F.info()
+    reports.clear()
+    capi.profile_reset()
+    capi.profile_enable(not args.no_profile)
+    launches0 = capi.kernel_launches()
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    for k in range(args.steps):
+        flush.fill_(float(k))  # L2 flush (256 MB write) outside the timed interval
+        ev[k][0].record()
+        step()
+        ev[k][1].record()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    clk = clocks.stop()
+    launches = capi.kernel_launches() - launches0
+    capi.profile_enable(False)
+    stages = capi.profile_read()
+    t_ms = sum(a.elapsed_time(b) for a, b in ev)
+    # correctness of the timed result: fp64 true residual of every column
+    R = B - F.apply(X, self_coef=S)
+    rel = (torch.linalg.vector_norm(R, dim=0) / torch.linalg.vector_norm(B, dim=0)).cpu().numpy()
+    converged = int(np.sum(rel <= TOL))
+    t_max = t_ms
+    conv_total = converged * args.steps
+    if dist:
+        tt = torch.tensor([t_ms], device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        t_max = float(tt.item())
+        cc = torch.tensor([conv_total], device=dev, dtype=torch.float64)
+        dist.all_reduce(cc)
+        conv_total = int(cc.item())
+    ms_per_step = t_max / args.steps
+    value = conv_total / (t_max / 1e3)
+
+    # roofline of the dominant operator stage
+    matvecs = sum(r["matvecs"] for r in reports)
+    mv64 = sum(r["refine_steps"] + 1 for r in reports)
+    mv32 = matvecs - mv64
+    b32 = algorithmic_bytes(info, M, info["num_pairs"], False)
+    b64 = algorithmic_bytes(info, M, info["num_pairs"], True)
+    op_stages = ["spread", "fft_fwd", "kspace", "fft_inv", "contract", "real"]
+    dom = max(op_stages, key=lambda k: stages[k][0])
+    dom_ms, dom_n = stages[dom]
+    bytes_total = b32[dom] * mv32 + b64[dom] * mv64
+    peak, peak_kind = measured_peaks()
+    achieved = bytes_total / (dom_ms / 1e3) / 1e9 if dom_ms > 0 else 0.0
+    traffic = ncu_traffic().get(dom)
+    mv_bytes = sum(b32[k] for k in op_stages) * mv32 + sum(b64[k] for k in op_stages) * mv64
+    mv_ms = sum(stages[k][0] for k in op_stages)
+    iters = [r["total_iterations"] / M for r in reports]
+
+    out = None
+    if rank == 0:
+        e2e = run_e2e(args, torch) if world == 1 and not args.no_e2e else None
+        cpu = cpu_baseline(args) if world == 1 and not args.no_cpu else None
+        out = {
+            "metric": "solves/s at N=4000, res 1e-6: batched mixed-prec vs plain; matvec % HBM peak",
+            "value": round(value, 3),
+            "unit": "solves/s",
+            "n_gpus": world,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": round(ms_per_step, 3),
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "c64 operator / c128 refinement",
+            "data": "synthetic (hexagonal monolayer generated as in the reference benchmark)",
+            "config": {
+                "workload": "N=4000 hex monolayer a=5nm spacing 12nm, box 1542.0x332.6x1000nm, Drude "
+                            "(eps_inf 4, wp 1.8 eV, gamma 0.1 eV), eps_m 1.77, 10 freqs 0.2-1.0 eV x 3 pols = 30 RHS, "
+                            "tol 1e-6 (Ewald and true fp64 residual), GMRES(50)+Jacobi, fp32 inner + fp64 refinement",
+                "rhs_per_step": M,
+                "converged_per_step": converged,
+                "max_true_rel_resid": float(rel.max()),
+                "krylov_steps_per_rhs": round(float(np.mean(iters)), 2),
+                "matvecs_per_step": matvecs / max(1, len(reports)),
+                "grid": info["grid"], "pruned_z_slots": info["z_slots"] if info["pruned"] else None,
+                "real_space_pairs": info["num_pairs"],
+                "l2": "inputs larger than L2 (grid + Krylov basis > 126 MB) and a 256 MB L2 flush before each step",
+                "parallelism": f"replicas x{world}",
+                "stage_ms_per_step": {k: round(v[0] / args.steps, 3) for k, v in stages.items()},
+                "matvec_hbm_frac": round(mv_bytes / (mv_ms / 1e3) / 1e9 / peak, 4) if mv_ms > 0 else None,
+            },
+            "roofline": {
+                "kernel": dom,
+                "bound": "hbm",
+                "achieved": round(achieved, 1),
+                "peak": peak,
+                "peak_source": peak_kind,
+                "unit": "GB/s",
+                "frac": round(achieved / peak, 4),
+                "traffic": None if traffic is None else traffic,
+                "algorithmic_bytes_per_launch": b32[dom],
+                "launches": dom_n,
+            },
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "gpu_launches": launches,
+            "clocks": clk,
+        }
+        print(json.dumps(out), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return out
+
+
+def run_e2e(args, torch):
+    """Same workload through the public drop-in API with host buffers."""
+    import cumpm_b200 as cuMPM
+
+    pos, box, eps = workload(0)
+    mk = lambda: cuMPM.dipole_solver(box, eps, radius=RADIUS, eps_m=EPS_M, tol=TOL, quiet=True)
+    s = mk()
+    s.set_solver_options(batch_all=True, refine=True, inner_tol=args.inner_tol)
+    s.compute(pos)  # warm-up (plans, precalc buffers)
+    times = []
+    for k in range(max(2, args.steps)):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        s.compute(pos)
+        d = s._solver.get_dipoles(True)  # host copy of every frame so far (last frame is this step's result)
+        t1 = time.perf_counter()
+        times.append(t1 - t0)
+    N = N_PART
+    M = N_FREQ * K_POL
+    h2d = 3 * N * 8 + 2 * (3 * N * M * 16) + N * M * 16
+    d2h = 3 * N * M * 16
+    t = float(np.median(times))
+    return {"value": round(M / t, 3), "unit": "solves/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+            "timing": "wall clock around compute()+get_dipoles(), median of steps"}
+
+
+def cpu_matvec_sample(threads):
+    """One fp64 matvec (1 RHS) of the CPU port of the reference operator."""
+    from oracle import mpm_oracle as O
+
+    pos, box, eps = workload(0)
+    op = O.MonoEwaldOperator(box / RADIUS, TOL, XI, True, fft_workers=threads)
+    op.set_positions(pos / RADIUS)
+    N = len(pos)
+    rng = np.random.default_rng(0)
+    x = rng.standard_normal(3 * N) + 1j * rng.standard_normal(3 * N)
+    sc = np.full(N, 3.0 / (4 * np.pi * (eps[0] / EPS_M - 1.0)))
+    t0 = time.perf_counter()
+    op.apply(x, sc)
+    return time.perf_counter() - t0
+
+
+def cpu_baseline(args):
+    threads = os.cpu_count() or 1
+    t = cpu_matvec_sample(threads)
+    v = 1.0 / (t * PLAIN_MATVECS_PER_SOLVE)
+    return {"value": round(v, 5), "unit": "solves/s", "cores": threads, "kind": "port",
+            "sample": f"1 fp64 matvec of the CPU port on the full workload ({t:.2f} s, FFT on {threads} threads); "
+                      f"solves/s = 1/(t x {PLAIN_MATVECS_PER_SOLVE:g} matvecs per solve)"}
+
+
+def run_reference(args, rank):
+    if rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    ts = []
+    for _ in range(args.warmup if args.warmup < 1 else 0):
+        pass
+    for _ in range(max(1, args.steps)):
+        ts.append(cpu_matvec_sample(threads))
+    t = float(np.median(ts))
+    v = 1.0 / (t * PLAIN_MATVECS_PER_SOLVE)
+    line = {
+        "impl": "reference",
+        "metric": "solves/s at N=4000, res 1e-6: batched mixed-prec vs plain; matvec % HBM peak",
+        "value": round(v, 5), "unit": "solves/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": round(t * 1e3, 1), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "c128", "data": "synthetic (hexagonal monolayer generated as in the reference benchmark)",
+        "config": {"workload": "N=4000 hex monolayer, 30 RHS, tol 1e-6 (see bench.py docstring)",
+                   "step": "one fp64 matvec of the CPU port of the reference operator (bounded sample)"},
+        "cpu_baseline": {"value": round(v, 5), "unit": "solves/s", "cores": threads, "kind": "port",
+                         "sample": f"1 fp64 matvec per step, median {t:.2f} s; solves/s = 1/(t x "
+                                   f"{PLAIN_MATVECS_PER_SOLVE:g} matvecs per solve)"},
+        "e2e": {"value": round(v, 5), "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--inner-tol", type=float, default=1e-4)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-profile", action="store_true", help="no stage timers in the timed region")
+    args = ap.parse_args()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank)
+        return
+    run_ours(args, rank, world, local_rank)
+
+
+if __name__ == "__main__":
+    main()

@@ -32,7 +32,10 @@ EXPORTS = [
     "mpm_field_create", "mpm_field_destroy", "mpm_field_set_positions", "mpm_field_set_field_points",
     "mpm_field_apply", "mpm_field_apply_part", "mpm_field_info_get", "mpm_batch_solve",
     "mpm_mono_tables", "mpm_ewald_geometry",
+    "mpm_profile_enable", "mpm_profile_reset", "mpm_profile_read", "mpm_kernel_launches",
 ]
+
+STAGES = ["spread", "fft_fwd", "kspace", "fft_inv", "contract", "real", "direct", "krylov", "precalc"]
 
 
 class SolveOptions(C.Structure):
@@ -72,6 +75,8 @@ def lib():
                                       C.POINTER(SolveOptions), C.POINTER(SolveReport), C.c_void_p]
         L.mpm_mono_tables.argtypes = [C.c_double, _dp, _dp, _dp]
         L.mpm_ewald_geometry.argtypes = [_dp, C.c_double, C.c_double, _ip, _ip, _dp, _dp, _dp]
+        L.mpm_profile_read.argtypes = [_dp, C.POINTER(C.c_longlong), C.c_int]
+        L.mpm_kernel_launches.restype = C.c_longlong
         L._mpm_typed = True
     return L
 
@@ -108,6 +113,26 @@ def ewald_geometry(box, errortol, xi):
     eta = (C.c_double * 3)()
     check(lib().mpm_ewald_geometry(bp, float(errortol), float(xi), grid, C.byref(st), C.byref(rc), h, eta))
     return dict(grid=list(grid), stencil=st.value, rc=rc.value, h=list(h), eta=list(eta))
+
+
+def profile_enable(on=True):
+    check(lib().mpm_profile_enable(int(on)))
+
+
+def profile_reset():
+    check(lib().mpm_profile_reset())
+
+
+def profile_read():
+    """{stage: (milliseconds, intervals)} accumulated since the last reset."""
+    ms = (C.c_double * 9)()
+    cnt = (C.c_longlong * 9)()
+    check(lib().mpm_profile_read(ms, cnt, 9))
+    return {n: (ms[i], cnt[i]) for i, n in enumerate(STAGES)}
+
+
+def kernel_launches():
+    return int(lib().mpm_kernel_launches())
 
 
 def _stream_ptr(stream):

@@ -353,3 +353,21 @@ int mpm_ewald_geometry(const double box[3], double errortol, double xi, int grid
 }
 
 }  // extern "C"
+
+// ---- measurement hooks ----------------------------------------------------
+#include "mpm_profile.h"
+
+extern "C" {
+
+int mpm_profile_enable(int on) {
+    return guard([&] { mpm::Profiler::get().enable(on != 0); });
+}
+int mpm_profile_reset(void) {
+    return guard([&] { mpm::Profiler::get().reset(); });
+}
+int mpm_profile_read(double* ms, long long* count, int n) {
+    return guard([&] { mpm::Profiler::get().read(ms, count, n); });
+}
+long long mpm_kernel_launches(void) { return mpm::Profiler::get().launches(); }
+
+}  // extern "C"

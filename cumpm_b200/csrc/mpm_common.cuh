@@ -28,7 +28,9 @@ inline void cuda_check(cudaError_t e, const char* what, const char* file, int li
     }
 }
 #define MPM_CUDA(x) ::mpm::cuda_check((x), #x, __FILE__, __LINE__)
-#define MPM_LAUNCH() ::mpm::cuda_check(cudaGetLastError(), "kernel launch", __FILE__, __LINE__)
+// count one of this library's kernel launches and check it
+void note_launch();
+#define MPM_LAUNCH() (::mpm::note_launch(), ::mpm::cuda_check(cudaGetLastError(), "kernel launch", __FILE__, __LINE__))
 
 // --------------------------------------------------------------- complex --
 

@@ -1,0 +1,286 @@
+// Batched in-place 1-D DFT along a strided axis (see mpm_fft.h).
+#include "mpm_fft.h"
+
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+namespace mpm {
+
+namespace {
+
+constexpr int kFftThreads = 256;
+constexpr size_t kFftSmemBudget = 100 * 1024;   // two CTAs per SM
+constexpr size_t kFftSmemMax = 220 * 1024;
+
+// Stockham autosort, mixed radix.  With Ns = product of the radices already
+// applied and L = Ns * r, butterfly j (j < n/r, k1 = j mod Ns) reads
+// x_q = in[j + q n/r] * W_L^(q k1) (q < r; q k1 < L, no reduction needed)
+// and writes out[(j/Ns) L + p Ns + k1] = sum_q x_q W_r^(p q), W = exp(-+2 pi i/.).
+// Outputs come in conjugate pairs (p, r - p) since W_r^((r-p) q) is the
+// conjugate of W_r^(p q).  Each CTA owns CW adjacent columns of one line;
+// thread = (row lane, column), CW a power of two.
+
+// small radices: the r twiddled inputs live in registers
+template <typename R, int CW, int MAXR>
+__device__ __forceinline__ void pass_reg(const cplx<R>* __restrict__ in, cplx<R>* __restrict__ out,
+                                         const cplx<R>* __restrict__ T, const int2* __restrict__ jt, int n, int r,
+                                         int L) {
+    constexpr int ROWS = kFftThreads / CW;
+    const int c = threadIdx.x & (CW - 1);
+    const int lane = threadIdx.x / CW;
+    const int nr = n / r;
+    const int stepL = n / L;
+    const int stepR = nr;
+    const int H = r / 2 + 1;
+    const int Ns = L / r;
+    for (int j = lane; j < nr; j += ROWS) {
+        const int2 kb = jt[j];  // (k1, output base)
+        cplx<R> x[MAXR];
+#pragma unroll
+        for (int q = 0; q < MAXR; ++q) {
+            if (q < r) {
+                const cplx<R> v = in[(j + q * nr) * CW + c];
+                const cplx<R> w = T[q * kb.x * stepL];
+                x[q] = mk<R>(v.x * w.x - v.y * w.y, v.x * w.y + v.y * w.x);
+            }
+        }
+        for (int h = 0; h < H; ++h) {
+            R s1 = R(0), s2 = R(0), s3 = R(0), s4 = R(0);
+            int ep = 0;
+#pragma unroll
+            for (int q = 0; q < MAXR; ++q) {
+                if (q < r) {
+                    const cplx<R> w = T[ep * stepR];
+                    s1 = fma(x[q].x, w.x, s1);
+                    s2 = fma(x[q].y, w.y, s2);
+                    s3 = fma(x[q].x, w.y, s3);
+                    s4 = fma(x[q].y, w.x, s4);
+                    ep += h;
+                    if (ep >= r) ep -= r;
+                }
+            }
+            out[(kb.y + h * Ns) * CW + c] = mk<R>(s1 - s2, s3 + s4);
+            if (h > 0 && 2 * h != r) out[(kb.y + (r - h) * Ns) * CW + c] = mk<R>(s1 + s2, s4 - s3);
+        }
+    }
+}
+
+// large radices (always odd primes here): twiddle the inputs in place, then
+// stream them from shared memory.  With a_q = x_q + x_{r-q}, b_q = x_q - x_{r-q}
+// (q = 1..(r-1)/2) and W_r^(p q) = (wr, wi):
+//   y_p     = x_0 + sum_q (a.x wr - wi b.y, a.y wr + wi b.x)
+//   y_{r-p} = x_0 + sum_q (a.x wr + wi b.y, a.y wr - wi b.x)
+// i.e. r-1 FMAs per output; each thread accumulates PC output pairs.
+template <typename R, int CW>
+__device__ __forceinline__ void pass_stream(cplx<R>* __restrict__ in, cplx<R>* __restrict__ out,
+                                            const cplx<R>* __restrict__ T, const int2* __restrict__ jt, int n, int r,
+                                            int L) {
+    constexpr int ROWS = kFftThreads / CW;
+    constexpr int PC = 8;
+    const int c = threadIdx.x & (CW - 1);
+    const int lane = threadIdx.x / CW;
+    const int nr = n / r;
+    const int Ns = L / r;
+    const int stepL = n / L;
+    const int stepR = nr;
+    const int half = (r - 1) / 2;
+    const int nchunk = (half + PC - 1) / PC;
+    if (Ns > 1) {
+        for (int q = 1; q < r; ++q)
+            for (int j = lane; j < nr; j += ROWS) {
+                const cplx<R> w = T[q * jt[j].x * stepL];
+                const cplx<R> v = in[(j + q * nr) * CW + c];
+                in[(j + q * nr) * CW + c] = mk<R>(v.x * w.x - v.y * w.y, v.x * w.y + v.y * w.x);
+            }
+        __syncthreads();
+    }
+    for (int u = lane; u < nr * nchunk; u += ROWS) {
+        const int oc = u / nr;
+        const int j = u - oc * nr;
+        const int base = jt[j].y;
+        const int p0 = 1 + oc * PC;
+        const cplx<R> x0 = in[j * CW + c];
+        R px[PC], py[PC], qx[PC], qy[PC];
+        int ep[PC];
+#pragma unroll
+        for (int k = 0; k < PC; ++k) { px[k] = py[k] = qx[k] = qy[k] = R(0); ep[k] = 0; }
+        R sx = R(0), sy = R(0);
+        for (int q = 1; q <= half; ++q) {
+            const cplx<R> xa = in[(j + q * nr) * CW + c];
+            const cplx<R> xb = in[(j + (r - q) * nr) * CW + c];
+            const R ax = xa.x + xb.x, ay = xa.y + xb.y, bx = xa.x - xb.x, by = xa.y - xb.y;
+            sx += ax;
+            sy += ay;
+#pragma unroll
+            for (int k = 0; k < PC; ++k) {
+                ep[k] += p0 + k;
+                if (ep[k] >= r) ep[k] -= r;
+                const cplx<R> w = T[ep[k] * stepR];
+                px[k] = fma(ax, w.x, px[k]);
+                py[k] = fma(ay, w.x, py[k]);
+                qx[k] = fma(bx, w.y, qx[k]);
+                qy[k] = fma(by, w.y, qy[k]);
+            }
+        }
+        if (oc == 0) out[base * CW + c] = mk<R>(x0.x + sx, x0.y + sy);
+#pragma unroll
+        for (int k = 0; k < PC; ++k) {
+            const int p = p0 + k;
+            if (p <= half) {
+                out[(base + p * Ns) * CW + c] = mk<R>(x0.x + px[k] - qy[k], x0.y + py[k] + qx[k]);
+                out[(base + (r - p) * Ns) * CW + c] = mk<R>(x0.x + px[k] + qy[k], x0.y + py[k] - qx[k]);
+            }
+        }
+    }
+}
+
+template <typename R, bool INV, int CW, int MAXR, bool STREAM>
+__global__ void __launch_bounds__(kFftThreads) k_fft_axis(cplx<R>* __restrict__ data, FftFactors f,
+                                                          const cplx<R>* __restrict__ tw, size_t es, int ncols,
+                                                          size_t os) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    constexpr int ROWS = kFftThreads / CW;
+    const int n = f.n;
+    cplx<R>* A = reinterpret_cast<cplx<R>*>(smem_raw);
+    cplx<R>* Bv = A + size_t(n) * CW;
+    cplx<R>* T = Bv + size_t(n) * CW;
+    int2* jt = reinterpret_cast<int2*>(T + n);
+    const int c = threadIdx.x & (CW - 1);
+    const int lane = threadIdx.x / CW;
+    const int c0 = blockIdx.y * CW;
+    const bool live = c0 + c < ncols;
+    cplx<R>* line = data + size_t(blockIdx.x) * os + c0 + c;
+    for (int t = threadIdx.x; t < n; t += kFftThreads) {
+        cplx<R> w = tw[t];
+        if (INV) w.y = -w.y;
+        T[t] = w;
+    }
+    for (int e = lane; e < n; e += ROWS) A[e * CW + c] = live ? line[size_t(e) * es] : mk<R>(0, 0);
+    cplx<R>* in = A;
+    cplx<R>* out = Bv;
+    int Ns = 1;
+    for (int ps = 0; ps < f.nf; ++ps) {
+        const int r = f.r[ps];
+        const int nr = n / r;
+        const int L = Ns * r;
+        __syncthreads();  // previous pass complete; jt free
+        for (int j = threadIdx.x; j < nr; j += kFftThreads) {
+            const int k1 = j % Ns;
+            jt[j] = make_int2(k1, (j / Ns) * L + k1);
+        }
+        __syncthreads();
+        if (r <= 8) pass_reg<R, CW, 8>(in, out, T, jt, n, r, L);
+        else if (MAXR > 8 && r <= MAXR) pass_reg<R, CW, (MAXR > 8 ? MAXR : 8)>(in, out, T, jt, n, r, L);
+        else if (STREAM) pass_stream<R, CW>(in, out, T, jt, n, r, L);
+        cplx<R>* tmp = in;
+        in = out;
+        out = tmp;
+        Ns = L;
+    }
+    __syncthreads();
+    if (live)
+        for (int e = lane; e < n; e += ROWS) line[size_t(e) * es] = in[e * CW + c];
+}
+
+int pick_cw(int n, size_t elem, int ncols) {
+    int cw = 32;
+    while (cw > 1 && ((2 * size_t(n) * cw + n) * elem + 8 * size_t(n)) > kFftSmemBudget) cw /= 2;
+    while (cw > 1 && cw / 2 >= ncols) cw /= 2;
+    return cw;
+}
+
+template <typename R, bool INV, int CW>
+void launch_cw(int cls, bool stream, dim3 grd, size_t shm, cudaStream_t s, cplx<R>* data, const FftFactors& f,
+               const cplx<R>* tw, size_t es, int ncols, size_t os) {
+    auto go = [&](auto kern) {
+        MPM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(shm)));
+        kern<<<grd, kFftThreads, shm, s>>>(data, f, tw, es, ncols, os);
+    };
+    if (stream) {
+        if (cls == 8) go(k_fft_axis<R, INV, CW, 8, true>);
+        else go(k_fft_axis<R, INV, CW, 16, true>);
+    } else {
+        if (cls == 8) go(k_fft_axis<R, INV, CW, 8, false>);
+        else go(k_fft_axis<R, INV, CW, 16, false>);
+    }
+}
+
+template <typename R, bool INV>
+void launch(int cw, int cls, bool stream, dim3 grd, size_t shm, cudaStream_t s, cplx<R>* data, const FftFactors& f,
+            const cplx<R>* tw, size_t es, int ncols, size_t os) {
+    switch (cw) {
+        case 32: launch_cw<R, INV, 32>(cls, stream, grd, shm, s, data, f, tw, es, ncols, os); break;
+        case 16: launch_cw<R, INV, 16>(cls, stream, grd, shm, s, data, f, tw, es, ncols, os); break;
+        case 8: launch_cw<R, INV, 8>(cls, stream, grd, shm, s, data, f, tw, es, ncols, os); break;
+        case 4: launch_cw<R, INV, 4>(cls, stream, grd, shm, s, data, f, tw, es, ncols, os); break;
+        case 2: launch_cw<R, INV, 2>(cls, stream, grd, shm, s, data, f, tw, es, ncols, os); break;
+        default: launch_cw<R, INV, 1>(cls, stream, grd, shm, s, data, f, tw, es, ncols, os); break;
+    }
+}
+
+}  // namespace
+
+bool AxisFFT::fits(int n, bool fp64) {
+    const size_t elem = fp64 ? sizeof(double2) : sizeof(float2);
+    return (3 * size_t(n)) * elem + 8 * size_t(n) <= kFftSmemMax;
+}
+
+void AxisFFT::init(int n) {
+    if (n == f_.n && tw64_.p) return;
+    f_ = FftFactors{};
+    f_.n = n;
+    // prime factors, small ones merged while the product stays <= 8
+    std::vector<int> pf;
+    int m = n;
+    for (int p = 2; p * p <= m; ++p)
+        while (m % p == 0) { pf.push_back(p); m /= p; }
+    if (m > 1) pf.push_back(m);
+    std::sort(pf.begin(), pf.end());
+    std::vector<int> rs;
+    for (int x : pf) {
+        if (!rs.empty() && rs.back() * x <= 8) rs.back() *= x;
+        else rs.push_back(x);
+    }
+    if (int(rs.size()) > kFftMaxFactors) throw std::runtime_error("FFT length has too many factors");
+    f_.nf = int(rs.size());
+    for (int i = 0; i < f_.nf; ++i) f_.r[i] = rs[i];
+    std::vector<double2> t64(n);
+    std::vector<float2> t32(n);
+    for (int t = 0; t < n; ++t) {
+        const double a = -2.0 * kPi * double(t) / double(n);
+        t64[t] = make_double2(std::cos(a), std::sin(a));
+        t32[t] = make_float2(float(t64[t].x), float(t64[t].y));
+    }
+    tw64_.ensure(sizeof(double2) * n);
+    tw32_.ensure(sizeof(float2) * n);
+    MPM_CUDA(cudaMemcpy(tw64_.p, t64.data(), sizeof(double2) * n, cudaMemcpyHostToDevice));
+    MPM_CUDA(cudaMemcpy(tw32_.p, t32.data(), sizeof(float2) * n, cudaMemcpyHostToDevice));
+}
+
+template <typename R>
+void AxisFFT::run(cplx<R>* data, size_t es, int ncols, size_t os, int nouter, bool inverse, cudaStream_t s) const {
+    if (f_.n <= 1 || nouter <= 0 || ncols <= 0) return;
+    const int n = f_.n;
+    const int cw = pick_cw(n, sizeof(cplx<R>), ncols);
+    const size_t shm = (2 * size_t(n) * cw + n) * sizeof(cplx<R>) + 8 * size_t(n);
+    if (shm > kFftSmemMax) throw std::runtime_error("FFT line does not fit in shared memory");
+    const cplx<R>* tw = sizeof(R) == 4 ? reinterpret_cast<const cplx<R>*>(tw32_.p)
+                                       : reinterpret_cast<const cplx<R>*>(tw64_.p);
+    dim3 grd(nouter, (ncols + cw - 1) / cw);
+    int rsmall = 1;
+    bool stream = false;
+    for (int i = 0; i < f_.nf; ++i) {
+        if (f_.r[i] > 16) stream = true;
+        else rsmall = std::max(rsmall, f_.r[i]);
+    }
+    const int cls = rsmall <= 8 ? 8 : 16;
+    if (inverse) launch<R, true>(cw, cls, stream, grd, shm, s, data, f_, tw, es, ncols, os);
+    else launch<R, false>(cw, cls, stream, grd, shm, s, data, f_, tw, es, ncols, os);
+    MPM_LAUNCH();
+}
+
+template void AxisFFT::run<float>(float2*, size_t, int, size_t, int, bool, cudaStream_t) const;
+template void AxisFFT::run<double>(double2*, size_t, int, size_t, int, bool, cudaStream_t) const;
+
+}  // namespace mpm

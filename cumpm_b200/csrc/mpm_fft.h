@@ -1,0 +1,42 @@
+// Batched 1-D DFT along one axis of a grid whose batch index is innermost.
+//
+// The spectral-Ewald grids are stored [x][y][slot][b] with the right-hand
+// sides innermost, so a transform along x or y sees, for every grid point,
+// a contiguous row of independent columns.  Each CTA stages one line of a
+// chunk of columns in shared memory and runs a mixed-radix Stockham
+// autosort there (every radix pass computes each output as an r-term sum
+// with table twiddles, so any prime factor works without Bluestein), then
+// writes the line back in place.  Global loads and stores are row-coalesced.
+// Unnormalised in both directions (the 1/V factor lives in the k-space
+// scale, as in the reference's cuFFT use).
+#pragma once
+
+#include "mpm_common.cuh"
+
+namespace mpm {
+
+constexpr int kFftMaxFactors = 16;
+
+struct FftFactors {
+    int n = 1;
+    int nf = 0;
+    int r[kFftMaxFactors] = {};
+};
+
+class AxisFFT {
+public:
+    void init(int n);
+    int n() const { return f_.n; }
+    // transform `nouter` lines: line o, column c, element e lives at
+    // data[o*os + e*es + c], c in [0, ncols)
+    template <typename R>
+    void run(cplx<R>* data, size_t es, int ncols, size_t os, int nouter, bool inverse, cudaStream_t s) const;
+    // whether one line of this length fits in shared memory
+    static bool fits(int n, bool fp64);
+
+private:
+    FftFactors f_;
+    DevBuf tw64_, tw32_;
+};
+
+}  // namespace mpm

@@ -21,6 +21,7 @@
 //    built on the device from a cell list (no atomics); the self term, the
 //    Jacobi scaling and the INTERACTION_FIELD sign are fused into it.
 #include "mpm_field.h"
+#include "mpm_profile.h"
 
 #include <cub/cub.cuh>
 
@@ -134,6 +135,12 @@ __device__ int reach_bins(int lo, int hi, int n, int t, bool periodic, int* out)
 
 // Gather spread: every voxel of this CTA's tile is written once with the sum
 // of all particle contributions (no atomics).  grid[((x*Ny+y)*Zs+s)*B + b].
+// Candidates come from the spatial bins that can reach the tile; for each
+// (x, y) column of the tile the candidates whose x and y weights are both
+// non-zero are listed once (in candidate order, so sums are deterministic),
+// and each voxel then loops only over its column's list.
+constexpr int kSpreadListCap = 64;
+
 template <typename R>
 __global__ void __launch_bounds__(256) k_spread(const double2* __restrict__ X, int M, int N, int C,
                                                 const int* __restrict__ quad_map,
@@ -170,9 +177,13 @@ __global__ void __launch_bounds__(256) k_spread(const double2* __restrict__ X, i
     __syncthreads();
     const int total = rpre[nranges];
     const int wlen = TX + TY + TZ;
-    R* wT = reinterpret_cast<R*>(smem_raw);                                   // [cap][wlen]
-    cplx<R>* pv = reinterpret_cast<cplx<R>*>(smem_raw + sizeof(R) * cap * wlen);  // [cap][bc]
-    int* cid = reinterpret_cast<int*>(pv + size_t(cap) * bc);                  // [cap]
+    const int ncol = TX * TY;
+    R* wT = reinterpret_cast<R*>(smem_raw);                                       // [cap][wlen]
+    cplx<R>* pv = reinterpret_cast<cplx<R>*>(smem_raw + sizeof(R) * cap * wlen);   // [cap][bc]
+    R* lw = reinterpret_cast<R*>(pv + size_t(cap) * bc);                           // [ncol][cap_l]
+    int* lc = reinterpret_cast<int*>(lw + size_t(ncol) * kSpreadListCap);          // [ncol][cap_l]
+    int* ln = lc + size_t(ncol) * kSpreadListCap;                                  // [ncol]
+    int* cid = ln + ncol;                                                          // [cap]
     const int nvox = TX * TY * TZ;
     for (int r0 = 0; r0 < max(total, 1); r0 += cap) {
         const int nc = min(cap, total - r0);
@@ -211,6 +222,23 @@ __global__ void __launch_bounds__(256) k_spread(const double2* __restrict__ X, i
             }
             wT[c * wlen + l] = w;
         }
+        __syncthreads();
+        // contributor list per (x, y) column, -1 = too many (full loop)
+        for (int col = threadIdx.x; col < ncol; col += blockDim.x) {
+            const int lx = col / TY, ly = col % TY;
+            int n = 0;
+            for (int c = 0; c < nc; ++c) {
+                const R wxy = wT[c * wlen + lx] * wT[c * wlen + TX + ly];
+                if (wxy != R(0)) {
+                    if (n < kSpreadListCap) {
+                        lw[col * kSpreadListCap + n] = wxy;
+                        lc[col * kSpreadListCap + n] = c;
+                    }
+                    ++n;
+                }
+            }
+            ln[col] = n <= kSpreadListCap ? n : -1;
+        }
         for (int b0 = 0; b0 < B; b0 += bc) {
             const int nb = min(bc, B - b0);
             __syncthreads();
@@ -234,11 +262,21 @@ __global__ void __launch_bounds__(256) k_spread(const double2* __restrict__ X, i
                 const int lz = vox % TZ, ly = (vox / TZ) % TY, lx = vox / (TZ * TY);
                 const int x = x0 + lx, y = y0 + ly, s = z0 + lz;
                 if (x >= g.Nx || y >= g.Ny || s >= g.Zs) continue;
+                const int col = lx * TY + ly;
+                const int nl = ln[col];
                 cplx<R> acc = mk<R>(0, 0);
-                for (int c = 0; c < nc; ++c) {
-                    const R* wc = wT + c * wlen;
-                    const R w = wc[lx] * wc[TX + ly] * wc[TX + TY + lz];
-                    fma_rc(acc, w, pv[c * bc + bb]);
+                if (nl >= 0) {
+                    const R* lwc = lw + col * kSpreadListCap;
+                    const int* lcc = lc + col * kSpreadListCap;
+                    for (int k = 0; k < nl; ++k) {
+                        const int c = lcc[k];
+                        fma_rc(acc, lwc[k] * wT[c * wlen + TX + TY + lz], pv[c * bc + bb]);
+                    }
+                } else {
+                    for (int c = 0; c < nc; ++c) {
+                        const R* wc = wT + c * wlen;
+                        fma_rc(acc, wc[lx] * wc[TX + ly] * wc[TX + TY + lz], pv[c * bc + bb]);
+                    }
                 }
                 const size_t o = ((size_t(x) * g.Ny + y) * g.Zs + s) * B + b0 + bb;
                 if (r0 == 0) grid[o] = acc;
@@ -1007,7 +1045,9 @@ void Field::build_stencil(PointSet& ps, cudaStream_t s, bool bins) {
     MPM_CUDA(cub::DeviceRadixSort::SortPairs(ps.cub_tmp.p, tmp, ps.bin_key.as<int>(), ps.bin_key_sorted.as<int>(),
                                              ps.idx.as<int>(), ps.idx_sorted.as<int>(), n, 0, bits, s));
     k_fill_int<<<nblk(nbins, 256), 256, 0, s>>>(ps.bin_start.as<int>(), nbins, -1);
+    MPM_LAUNCH();
     k_fill_int<<<nblk(nbins, 256), 256, 0, s>>>(ps.bin_end.as<int>(), nbins, -1);
+    MPM_LAUNCH();
     k_bin_bounds<<<nblk(n, 256), 256, 0, s>>>(ps.bin_key_sorted.as<int>(), n, ps.bin_start.as<int>(),
                                               ps.bin_end.as<int>());
     MPM_LAUNCH();
@@ -1042,7 +1082,9 @@ void Field::build_pairs(cudaStream_t s) {
     MPM_CUDA(cub::DeviceRadixSort::SortPairs(cub_tmp_.p, tmp, cell_key_.as<int>(), cell_key_s_.as<int>(),
                                              cell_idx_.as<int>(), cell_idx_s_.as<int>(), ns, 0, bits, s));
     k_fill_int<<<nblk(ncell, 256), 256, 0, s>>>(cell_start_.as<int>(), ncell, -1);
+    MPM_LAUNCH();
     k_fill_int<<<nblk(ncell, 256), 256, 0, s>>>(cell_end_.as<int>(), ncell, -1);
+    MPM_LAUNCH();
     k_bin_bounds<<<nblk(ns, 256), 256, 0, s>>>(cell_key_s_.as<int>(), ns, cell_start_.as<int>(),
                                                cell_end_.as<int>());
     MPM_LAUNCH();
@@ -1064,7 +1106,7 @@ void Field::build_pairs(cudaStream_t s) {
     num_pairs_ = total;
     const size_t np = std::max<long long>(1, num_pairs_);
     pair_src_.ensure(sizeof(int) * np);
-    DevBuf geo;
+    DevBuf& geo = pair_geo_;
     geo.ensure(sizeof(double) * 4 * np);
     k_pairs<<<nblk(nt, 128), 128, 0, s>>>(sources_.xyz.as<double>(), ns, tg.xyz.as<double>(), nt, a,
                                            cell_start_.as<int>(), cell_end_.as<int>(), cell_idx_s_.as<int>(), rc,
@@ -1078,8 +1120,7 @@ void Field::build_pairs(cudaStream_t s) {
         k_pair_coefs<<<nblk(num_pairs_, 256), 256, 0, s>>>(geo.as<double>(), num_pairs_, tab_r_.as<double>(),
                                                             tab_f_.as<double>(), Nq_ > 0, pair_T64_.as<double>(),
                                                             pair_T32_.as<float>(), pair_Q_.as<double>());
-    MPM_LAUNCH();
-    MPM_CUDA(cudaStreamSynchronize(s));  // geo is released at scope end
+        MPM_LAUNCH();
 }
 
 void Field::build_scale(cudaStream_t s) {
@@ -1118,8 +1159,15 @@ void Field::build_column_kernel(cudaStream_t s) {
 
 void Field::precalc(cudaStream_t s) {
     if (!precalc_dirty_) return;
+    StageScope scope(ST_PRECALC, s);
     if (spec_.kind == FIELD_MONO) {
         choose_layout(s);
+        own_fft_ = AxisFFT::fits(gv_.Nx, true) && AxisFFT::fits(gv_.Ny, true) && AxisFFT::fits(gv_.Nz, true);
+        if (own_fft_) {
+            fftx_.init(gv_.Nx);
+            ffty_.init(gv_.Ny);
+            if (!gv_.pruned) fftz_.init(gv_.Nz);
+        }
         build_stencil(sources_, s, true);
         if (!spec_.solver_ax) build_stencil(targets_, s, false);  // SOLVER_AX: targets share the source stencil
         build_pairs(s);
@@ -1157,6 +1205,29 @@ cufftHandle Field::plan_for(int M, bool fp32) {
     return h;
 }
 
+// 3-D (full layout) or x-y (pruned layout) transform of the [x][y][slot][b]
+// grid: in-house batched line transforms, cuFFT when a line is too long.
+template <typename R>
+void Field::transform(cplx<R>* grid, int B, bool inverse, cudaStream_t s) {
+    if (own_fft_) {
+        const size_t Bi = size_t(gv_.Zs) * B;
+        if (!gv_.pruned) fftz_.run<R>(grid, size_t(B), B, size_t(gv_.Nz) * B, gv_.Nx * gv_.Ny, inverse, s);
+        ffty_.run<R>(grid, Bi, int(Bi), size_t(gv_.Ny) * Bi, gv_.Nx, inverse, s);
+        fftx_.run<R>(grid, size_t(gv_.Ny) * Bi, int(Bi), Bi, gv_.Ny, inverse, s);
+        return;
+    }
+    const int M = B / (Nq_ ? 8 : 3);
+    cufftHandle plan = plan_for(M, sizeof(R) == 4);
+    cufftSetStream(plan, s);
+    cufftResult fr;
+    const int dir = inverse ? CUFFT_INVERSE : CUFFT_FORWARD;
+    if (sizeof(R) == 4)
+        fr = cufftExecC2C(plan, reinterpret_cast<cufftComplex*>(grid), reinterpret_cast<cufftComplex*>(grid), dir);
+    else
+        fr = cufftExecZ2Z(plan, reinterpret_cast<cufftDoubleComplex*>(grid), reinterpret_cast<cufftDoubleComplex*>(grid), dir);
+    if (fr != CUFFT_SUCCESS) throw std::runtime_error("cuFFT execution failed with code: " + std::to_string(int(fr)));
+}
+
 template <typename R>
 void Field::recip(const double2* X, double2* Y, int M, cudaStream_t s) {
     const int C = Nq_ ? 8 : 3;
@@ -1169,24 +1240,23 @@ void Field::recip(const double2* X, double2* Y, int M, cudaStream_t s) {
     const int TX = ps.tile[0], TY = ps.tile[1], TZ = ps.tile[2];
     const int bc = sizeof(R) == 4 ? 32 : 16;
     const int cap = 192;
-    const size_t shm = sizeof(R) * cap * (TX + TY + TZ) + sizeof(cplx<R>) * cap * bc + sizeof(int) * cap;
+    const size_t ncol = size_t(TX) * TY;
+    const size_t shm = sizeof(R) * cap * (TX + TY + TZ) + sizeof(cplx<R>) * cap * bc +
+                       (sizeof(R) + sizeof(int)) * ncol * kSpreadListCap + sizeof(int) * (ncol + cap);
     MPM_CUDA(cudaFuncSetAttribute(k_spread<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(shm)));
     dim3 grd(ps.nb[0], ps.nb[1], ps.nb[2]);
     const R* w1 = sizeof(R) == 4 ? reinterpret_cast<const R*>(ps.w32.p) : reinterpret_cast<const R*>(ps.w64.p);
+    Profiler::get().begin(ST_SPREAD, s);
     k_spread<R><<<grd, 256, shm, s>>>(X, M, N_, C, quad_map_.as<int>(), ps.base.as<int4>(), w1,
                                       ps.bin_start.as<int>(), ps.bin_end.as<int>(), ps.idx_sorted.as<int>(), gv_,
                                       TX, TY, TZ, ps.nb[0], ps.nb[1], cap, bc, grid);
     MPM_LAUNCH();
+    Profiler::get().end(ST_SPREAD, s);
     // forward transform
-    cufftHandle plan = plan_for(M, sizeof(R) == 4);
-    cufftSetStream(plan, s);
-    cufftResult fr;
-    if (sizeof(R) == 4)
-        fr = cufftExecC2C(plan, reinterpret_cast<cufftComplex*>(grid), reinterpret_cast<cufftComplex*>(grid), CUFFT_FORWARD);
-    else
-        fr = cufftExecZ2Z(plan, reinterpret_cast<cufftDoubleComplex*>(grid), reinterpret_cast<cufftDoubleComplex*>(grid),
-                          CUFFT_FORWARD);
-    if (fr != CUFFT_SUCCESS) throw std::runtime_error("cuFFT forward execution failed with code: " + std::to_string(int(fr)));
+    Profiler::get().begin(ST_FFT_FWD, s);
+    transform<R>(grid, B, false, s);
+    Profiler::get().end(ST_FFT_FWD, s);
+    Profiler::get().begin(ST_KSPACE, s);
     // k-space Green tensor
     if (gv_.pruned) {
         const int Z = gv_.Zs;
@@ -1197,6 +1267,7 @@ void Field::recip(const double2* X, double2* Y, int M, cudaStream_t s) {
         const cplx<R>* K = sizeof(R) == 4 ? reinterpret_cast<const cplx<R>*>(colK32_.p)
                                           : reinterpret_cast<const cplx<R>*>(colK64_.p);
         k_column<R><<<gv_.Nx * gv_.Ny, thr, shm2, s>>>(grid, K, Z, M);
+        MPM_LAUNCH();
     } else {
         const size_t V = cells;
         const R* sc = sizeof(R) == 4 ? reinterpret_cast<const R*>(scale32_.p) : reinterpret_cast<const R*>(scale64_.p);
@@ -1206,14 +1277,13 @@ void Field::recip(const double2* X, double2* Y, int M, cudaStream_t s) {
         else
             k_scale<R, false><<<nblk((long long)(V * M), 256), 256, 0, s>>>(grid, sc, gv_.Nx, gv_.Ny, gv_.Nz, spec_.box[0],
                                                                             spec_.box[1], spec_.box[2], M);
+        MPM_LAUNCH();
     }
-    MPM_LAUNCH();
-    if (sizeof(R) == 4)
-        fr = cufftExecC2C(plan, reinterpret_cast<cufftComplex*>(grid), reinterpret_cast<cufftComplex*>(grid), CUFFT_INVERSE);
-    else
-        fr = cufftExecZ2Z(plan, reinterpret_cast<cufftDoubleComplex*>(grid), reinterpret_cast<cufftDoubleComplex*>(grid),
-                          CUFFT_INVERSE);
-    if (fr != CUFFT_SUCCESS) throw std::runtime_error("cuFFT inverse execution failed with code: " + std::to_string(int(fr)));
+    Profiler::get().end(ST_KSPACE, s);
+    Profiler::get().begin(ST_FFT_INV, s);
+    transform<R>(grid, B, true, s);
+    Profiler::get().end(ST_FFT_INV, s);
+    StageScope scope(ST_CONTRACT, s);
     // contract
     const PointSet& tg = spec_.solver_ax ? sources_ : targets_;
     const int nt = tg.n;
@@ -1241,6 +1311,7 @@ void Field::real_part(const double2* X, double2* Y, int M, const double2* sc, bo
     const int warps = a.Nt;
     const int thr = 128;
     const int blocks = nblk((long long)warps * 32, thr);
+    StageScope scope(ST_REAL, s);
     if (fp32)
         k_real<float><<<blocks, thr, 0, s>>>(X, Y, a, pair_off_.as<int>(), pair_src_.as<int>(), pair_T32_.as<float>(),
                                              pair_Q_.as<double>(), quad_map_.as<int>(), sc);
@@ -1254,6 +1325,7 @@ void Field::direct(const double2* X, double2* Y, int M, const double2* sc, bool 
     const int nt = num_targets();
     const double* tg = spec_.solver_ax ? sources_.xyz.as<double>() : targets_.xyz.as<double>();
     dim3 grd(nblk(nt, 128), M);
+    StageScope scope(ST_DIRECT, s);
     if (fp32)
         k_direct<float><<<grd, 128, 0, s>>>(X, Y, M, N_, nt, sources_.xyz.as<double>(), tg, radius_.as<double>(),
                                             quad_map_.as<int>(), Nq_ > 0, sc, spec_.solver_ax, jacobi);

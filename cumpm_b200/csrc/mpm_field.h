@@ -19,6 +19,7 @@
 #include <vector>
 
 #include "mpm_common.cuh"
+#include "mpm_fft.h"
 #include "mpm_tables.h"
 
 namespace mpm {
@@ -122,6 +123,7 @@ private:
     void build_scale(cudaStream_t s);
     cufftHandle plan_for(int M, bool fp32);
     template <typename R> void recip(const double2* X, double2* Y, int M, cudaStream_t s);
+    template <typename R> void transform(cplx<R>* grid, int B, bool inverse, cudaStream_t s);
     void real_part(const double2* X, double2* Y, int M, const double2* self_coef, bool jacobi, bool real_fp32,
                    bool add_recip, cudaStream_t s);
     void direct(const double2* X, double2* Y, int M, const double2* self_coef, bool jacobi, bool fp32,
@@ -140,7 +142,7 @@ private:
     DevBuf tab_r_, tab_f_;          // double[kTableSize], double[T_COUNT][kTableSize]
     // CSR pairs by target
     DevBuf pair_off_, pair_cnt_, pair_src_, pair_T64_, pair_T32_, pair_Q_, cell_key_, cell_idx_, cell_key_s_,
-        cell_idx_s_, cell_start_, cell_end_, cub_tmp_;
+        cell_idx_s_, cell_start_, cell_end_, cub_tmp_, pair_geo_;
     long long num_pairs_ = 0;
     // reciprocal space
     DevBuf grid_;                   // complex grid, sized for the largest use
@@ -150,6 +152,8 @@ private:
     int scale_built_ = 0;
     struct PlanKey { int M; bool fp32; int pruned; int Zs; cufftHandle h; };
     std::vector<PlanKey> plans_;
+    AxisFFT fftx_, ffty_, fftz_;    // in-house batched transforms (cuFFT only when a line is too long)
+    bool own_fft_ = true;
 };
 
 }  // namespace mpm

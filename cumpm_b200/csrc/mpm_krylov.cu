@@ -1,5 +1,6 @@
 // Batched device Krylov solvers (see mpm_krylov.h).
 #include "mpm_krylov.h"
+#include "mpm_profile.h"
 
 #include <algorithm>
 #include <cmath>
@@ -413,6 +414,7 @@ int BatchSolver::read_flag(const int* dflag, cudaStream_t s) {
 
 void BatchSolver::dots(const double2* V, size_t vstride, int nvec, const double2* w, int rows, int M, int conj,
                        double2* out, cudaStream_t s) {
+    StageScope scope(ST_KRYLOV, s);
     const int gx = std::max(1, std::min(296, (rows + 7) / 8));
     partial_.ensure(sizeof(double2) * size_t(gx) * nvec * M);
     dim3 grd(gx, (M + 31) / 32, (nvec + 7) / 8);
@@ -477,6 +479,7 @@ void BatchSolver::gmres(Field& F, const double2* b, double2* x, int M, const dou
 
     norms(b, rows, M, bnorm_.as<double>(), s);
     k_gm_init<<<mb, 128, 0, s>>>(gs, bnorm_.as<double>(), M);
+    MPM_LAUNCH();
     k_zero_rhs_cols<<<vb, 256, 0, s>>>(x, bnorm_.as<double>(), n, M);
     MPM_LAUNCH();
     const double2* bj = b;
@@ -506,14 +509,22 @@ void BatchSolver::gmres(Field& F, const double2* b, double2* x, int M, const dou
             st.matvecs++;
             // CGS2
             dots(V, n, k + 1, w, rows, M, 1, h_.as<double2>(), s);
-            k_vupdate<<<vb, 256, 0, s>>>(w, V, n, k + 1, h_.as<double2>(), rows, M, -1.0, nullptr);
-            MPM_LAUNCH();
+            {
+                StageScope sc1(ST_KRYLOV, s);
+                k_vupdate<<<vb, 256, 0, s>>>(w, V, n, k + 1, h_.as<double2>(), rows, M, -1.0, nullptr);
+                MPM_LAUNCH();
+            }
             dots(V, n, k + 1, w, rows, M, 1, h2_.as<double2>(), s);
-            k_vupdate<<<vb, 256, 0, s>>>(w, V, n, k + 1, h2_.as<double2>(), rows, M, -1.0, nullptr);
-            k_addto<<<nblk((k + 1) * M, 128), 128, 0, s>>>(h_.as<double2>(), h2_.as<double2>(), (k + 1) * M);
-            MPM_LAUNCH();
+            {
+                StageScope sc2(ST_KRYLOV, s);
+                k_vupdate<<<vb, 256, 0, s>>>(w, V, n, k + 1, h2_.as<double2>(), rows, M, -1.0, nullptr);
+                MPM_LAUNCH();
+                k_addto<<<nblk((k + 1) * M, 128), 128, 0, s>>>(h_.as<double2>(), h2_.as<double2>(), (k + 1) * M);
+                MPM_LAUNCH();
+            }
             norms(w, rows, M, rnorm_.as<double>(), s);
             k_normalize<<<vb, 256, 0, s>>>(w, V + size_t(k + 1) * n, rnorm_.as<double>(), gs, n, M);
+            MPM_LAUNCH();
             MPM_CUDA(cudaMemsetAsync(dflag, 0, sizeof(int), s));
             k_gm_givens<<<mb, 128, 0, s>>>(gs, h_.as<double2>(), rnorm_.as<double>(), H_.as<double2>(),
                                            g_.as<double2>(), cs_.as<double>(), sn_.as<double2>(), k, restart, M,
@@ -522,6 +533,7 @@ void BatchSolver::gmres(Field& F, const double2* b, double2* x, int M, const dou
             if (read_flag(dflag, s) == 0) break;
         }
         k_gm_backsub<<<mb, 128, 0, s>>>(gs, H_.as<double2>(), g_.as<double2>(), y_.as<double2>(), restart, M, kper);
+        MPM_LAUNCH();
         k_vupdate<<<vb, 256, 0, s>>>(x, V, n, restart, y_.as<double2>(), rows, M, 1.0, kper);
         MPM_LAUNCH();
     }
@@ -555,12 +567,13 @@ void BatchSolver::bicgstab(Field& F, const double2* b, double2* x, int M, const 
 
     norms(b, rows, M, bnorm_.as<double>(), s);
     k_zero_rhs_cols<<<vb, 256, 0, s>>>(x, bnorm_.as<double>(), n, M);
+    MPM_LAUNCH();
     const double2* bj = b;
     if (opt.jacobi) {
         k_jacobi<<<vb, 256, 0, s>>>(b, bj_.as<double2>(), F.num_particles(), F.num_quads(), M, F.quad_idx_dev(), sc);
+        MPM_LAUNCH();
         bj = bj_.as<double2>();
     }
-    MPM_LAUNCH();
     double2* r = r_.as<double2>();
     F.apply(x, w_.as<double2>(), M, sc, opt.jacobi, r32, re32, s);
     st.matvecs++;
@@ -568,6 +581,7 @@ void BatchSolver::bicgstab(Field& F, const double2* b, double2* x, int M, const 
     MPM_LAUNCH();
     norms(r, rows, M, rnorm_.as<double>(), s);
     k_bi_init<<<mb, 128, 0, s>>>(bs, bnorm_.as<double>(), rnorm_.as<double>(), opt.tol, M);
+    MPM_LAUNCH();
     MPM_CUDA(cudaMemcpyAsync(r0_.p, r, sizeof(double2) * n, cudaMemcpyDeviceToDevice, s));
     MPM_CUDA(cudaMemcpyAsync(p_.p, r, sizeof(double2) * n, cudaMemcpyDeviceToDevice, s));
     MPM_CUDA(cudaMemsetAsync(v_.p, 0, sizeof(double2) * n, s));
@@ -578,16 +592,19 @@ void BatchSolver::bicgstab(Field& F, const double2* b, double2* x, int M, const 
         for (int it = 0; it < opt.maxiter; ++it) {
             dots(r0_.as<double2>(), 0, 1, r, rows, M, 0, hv, s);
             k_bi_a<<<mb, 128, 0, s>>>(bs, hv, it, M);
+            MPM_LAUNCH();
             k_bi_p<<<vb, 256, 0, s>>>(p_.as<double2>(), v_.as<double2>(), r, bs, it, n, M);
             MPM_LAUNCH();
             F.apply(p_.as<double2>(), v_.as<double2>(), M, sc, opt.jacobi, r32, re32, s);
             st.matvecs++;
             dots(r0_.as<double2>(), 0, 1, v_.as<double2>(), rows, M, 0, hv, s);
             k_bi_b<<<mb, 128, 0, s>>>(bs, hv, M);
+            MPM_LAUNCH();
             k_bi_s<<<vb, 256, 0, s>>>(s_.as<double2>(), r, v_.as<double2>(), bs, n, M);
             MPM_LAUNCH();
             norms(s_.as<double2>(), rows, M, rnorm_.as<double>(), s);
             k_bi_c<<<mb, 128, 0, s>>>(bs, rnorm_.as<double>(), bnorm_.as<double>(), opt.tol, mode, M);
+            MPM_LAUNCH();
             k_bi_xfinal<<<vb, 256, 0, s>>>(x, p_.as<double2>(), bs, mode, n, M);
             MPM_LAUNCH();
             F.apply(s_.as<double2>(), t_.as<double2>(), M, sc, opt.jacobi, r32, re32, s);
@@ -595,6 +612,7 @@ void BatchSolver::bicgstab(Field& F, const double2* b, double2* x, int M, const 
             dots(t_.as<double2>(), 0, 1, s_.as<double2>(), rows, M, 1, hv, s);
             dots(t_.as<double2>(), 0, 1, t_.as<double2>(), rows, M, 1, hv + M, s);
             k_bi_d<<<mb, 128, 0, s>>>(bs, hv, hv + M, M);
+            MPM_LAUNCH();
             k_bi_xr<<<vb, 256, 0, s>>>(x, r, p_.as<double2>(), s_.as<double2>(), t_.as<double2>(), bs, n, M);
             MPM_LAUNCH();
             norms(r, rows, M, rnorm_.as<double>(), s);
@@ -660,6 +678,7 @@ void BatchSolver::solve(Field& F, const double2* b, double2* x, int M, const dou
         }
         if (!left) break;
         k_mask_cols<<<vb, 256, 0, s>>>(xr_.as<double2>(), rn2.as<double>(), bn2.as<double>(), opt.tol, n, M);
+        MPM_LAUNCH();
         MPM_CUDA(cudaMemsetAsync(d_.p, 0, sizeof(double2) * n, s));
         SolveStats inner;
         inner.iters.assign(M, 0);

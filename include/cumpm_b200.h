@@ -157,6 +157,17 @@ MPM_API int mpm_field_info_get(const mpm_field* f, mpm_field_info* info);
 MPM_API int mpm_batch_solve(mpm_field* f, const void* B, void* X, int M, const void* self_coef,
                     const mpm_solve_options* opt, mpm_solve_report* report, void* stream);
 
+/* ---- measurement (no counterpart in the reference) -----------------------
+ * Stage timers from CUDA events recorded on the launching stream, read
+ * without adding synchronisation to the solve.  Stages: 0 spread, 1 forward
+ * FFT, 2 k-space Green tensor, 3 inverse FFT, 4 contraction, 5 real space,
+ * 6 direct sum, 7 Krylov vector work, 8 per-frame precalculation. */
+MPM_API int mpm_profile_enable(int on);
+MPM_API int mpm_profile_reset(void);
+MPM_API int mpm_profile_read(double* ms, long long* count, int n);
+/* kernel launches issued by this library since the last reset */
+MPM_API long long mpm_kernel_launches(void);
+
 /* ---- host-only helpers (no GPU needed) ---------------------------------- */
 /* real-space tables: out has 10 x 9001 doubles (r, fd1, fd2, fq1, fq2, fq3,
  * gq1, gq2, gq3, gq4); selfo/self_grad may be NULL */

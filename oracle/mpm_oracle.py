@@ -451,7 +451,8 @@ class MonoEwaldOperator:
     (``base_electric_field.cu:235``).
     """
 
-    def __init__(self, box, errortol, xi, solver_ax=True, quad_idxs=None):
+    def __init__(self, box, errortol, xi, solver_ax=True, quad_idxs=None, fft_workers=None):
+        self.fft_workers = fft_workers
         self.p = MonoParams(box, errortol, xi)
         self.solver_ax = solver_ax
         self.quad_idxs = None if quad_idxs is None else np.asarray(quad_idxs, dtype=int)
@@ -474,13 +475,25 @@ class MonoEwaldOperator:
         self.pi_, self.pj, self.pr, self.pd = i[keep], j[keep], r[keep], d[keep]
 
     # -- stages --------------------------------------------------------------
+    def _fftn(self, a):
+        if self.fft_workers:
+            import scipy.fft
+            return scipy.fft.fftn(a, axes=(1, 2, 3), workers=self.fft_workers)
+        return np.fft.fftn(a, axes=(1, 2, 3))
+
+    def _ifftn(self, a):
+        if self.fft_workers:
+            import scipy.fft
+            return scipy.fft.ifftn(a, axes=(1, 2, 3), workers=self.fft_workers)
+        return np.fft.ifftn(a, axes=(1, 2, 3))
+
     def reciprocal(self, p, Q=None):
         Nx, Ny, Nz = self.p.num_grid
         ix, iy, iz, w = self.sp
         grid = np.zeros((3, Nx, Ny, Nz), dtype=np.complex128)
         for c in range(3):
             np.add.at(grid[c], (ix, iy, iz), w * p[:, c][:, None, None, None])
-        F = np.fft.fftn(grid, axes=(1, 2, 3))
+        F = self._fftn(grid)
         kh = self.sc["khat"]
         dot = F[0] * kh[..., 0] + F[1] * kh[..., 1] + F[2] * kh[..., 2]
         if Q is None:
@@ -496,7 +509,7 @@ class MonoEwaldOperator:
             Gdot = dot * (1j * self.sc["sGP"]) + gdot * self.sc["sGQ"]
             FG = np.stack([Gdot * self.sc["qf"][..., c] for c in range(5)])
         F = np.stack([Edot * kh[..., c] for c in range(3)])
-        Es = np.fft.ifftn(F, axes=(1, 2, 3)) * float(Nx * Ny * Nz)
+        Es = self._ifftn(F) * float(Nx * Ny * Nz)
         cx, cy, cz, cw = self.ct
         E = np.stack([np.sum(cw * Es[c][cx, cy, cz], axis=(1, 2, 3)) for c in range(3)], axis=1)
         G = None
