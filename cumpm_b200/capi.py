@@ -33,6 +33,7 @@ EXPORTS = [
     "mpm_field_apply", "mpm_field_apply_part", "mpm_field_info_get", "mpm_batch_solve",
     "mpm_mono_tables", "mpm_ewald_geometry",
     "mpm_profile_enable", "mpm_profile_reset", "mpm_profile_read", "mpm_kernel_launches",
+    "mpm_field_apply_noalloc", "mpm_noalloc_scratch_bytes",
 ]
 
 STAGES = ["spread", "fft_fwd", "kspace", "fft_inv", "contract", "real", "direct", "krylov", "precalc"]
@@ -76,6 +77,9 @@ def lib():
         L.mpm_mono_tables.argtypes = [C.c_double, _dp, _dp, _dp]
         L.mpm_ewald_geometry.argtypes = [_dp, C.c_double, C.c_double, _ip, _ip, _dp, _dp, _dp]
         L.mpm_profile_read.argtypes = [_dp, C.POINTER(C.c_longlong), C.c_int]
+        L.mpm_field_apply_noalloc.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_int,
+                                              C.c_int, C.c_int, C.c_void_p]
+        L.mpm_noalloc_scratch_bytes.restype = C.c_size_t
         L.mpm_kernel_launches.restype = C.c_longlong
         L._mpm_typed = True
     return L

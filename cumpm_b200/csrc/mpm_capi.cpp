@@ -11,12 +11,10 @@
 #include "mpm_krylov.h"
 #include "mpm_solver.h"
 
+#include "mpm_capi_internal.h"
+
 struct mpm_solver { mpm::DipoleSolver* impl; };
 struct mpm_near { mpm::NearField* impl; };
-struct mpm_field {
-    mpm::Field* impl;
-    mpm::BatchSolver* solver;
-};
 
 namespace {
 
@@ -60,6 +58,8 @@ void copy_out(const std::vector<cd>& v, double* out, size_t cap) {
 }
 
 }  // namespace
+
+int mpm::capi_guard(const std::function<void()>& f) { return guard(f); }
 
 extern "C" {
 

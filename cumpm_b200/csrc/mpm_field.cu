@@ -1230,11 +1230,20 @@ void Field::transform(cplx<R>* grid, int B, bool inverse, cudaStream_t s) {
 
 template <typename R>
 void Field::recip(const double2* X, double2* Y, int M, cudaStream_t s) {
+    grid_.ensure(grid_bytes(M, sizeof(R) == 8));
+    recip_on<R>(X, Y, M, grid_.as<cplx<R>>(), s);
+}
+
+size_t Field::grid_bytes(int M, bool fp64) const {
+    const int C = Nq_ ? 8 : 3;
+    return (fp64 ? sizeof(double2) : sizeof(float2)) * size_t(gv_.Nx) * gv_.Ny * gv_.Zs * size_t(C) * M;
+}
+
+// Reciprocal-space part on a caller-provided grid of grid_bytes(M) bytes.
+template <typename R>
+void Field::recip_on(const double2* X, double2* Y, int M, cplx<R>* grid, cudaStream_t s) {
     const int C = Nq_ ? 8 : 3;
     const int B = C * M;
-    const size_t cells = size_t(gv_.Nx) * gv_.Ny * gv_.Zs;
-    grid_.ensure(sizeof(cplx<R>) * cells * B);
-    cplx<R>* grid = grid_.as<cplx<R>>();
     // spread
     const PointSet& ps = sources_;
     const int TX = ps.tile[0], TY = ps.tile[1], TZ = ps.tile[2];
@@ -1269,7 +1278,7 @@ void Field::recip(const double2* X, double2* Y, int M, cudaStream_t s) {
         k_column<R><<<gv_.Nx * gv_.Ny, thr, shm2, s>>>(grid, K, Z, M);
         MPM_LAUNCH();
     } else {
-        const size_t V = cells;
+        const size_t V = size_t(gv_.Nx) * gv_.Ny * gv_.Zs;
         const R* sc = sizeof(R) == 4 ? reinterpret_cast<const R*>(scale32_.p) : reinterpret_cast<const R*>(scale64_.p);
         if (Nq_)
             k_scale<R, true><<<nblk((long long)(V * M), 256), 256, 0, s>>>(grid, sc, gv_.Nx, gv_.Ny, gv_.Nz, spec_.box[0],
@@ -1345,6 +1354,24 @@ void Field::apply(const double2* X, double2* Y, int M, const double2* sc, bool j
     }
     if (recip_fp32) recip<float>(X, Y, M, s);
     else recip<double>(X, Y, M, s);
+    real_part(X, Y, M, sc, jacobi, real_fp32, true, s);
+}
+
+void Field::apply_scratch(const double2* X, double2* Y, int M, const double2* sc, bool jacobi, bool recip_fp32,
+                          bool real_fp32, void* scratch, size_t scratch_bytes, cudaStream_t s) {
+    if (N_ == 0) throw std::runtime_error("Field::apply before set_positions");
+    if (!spec_.solver_ax && targets_.n == 0) throw std::runtime_error("Field::apply without field points");
+    if (spec_.kind == FIELD_DIRECT) {
+        direct(X, Y, M, sc, jacobi, recip_fp32, s);
+        return;
+    }
+    if (!own_fft_) throw std::runtime_error("grid lines too long for the in-house transform; scratch apply unavailable");
+    const size_t need = grid_bytes(M, !recip_fp32);
+    if (need > scratch_bytes)
+        throw std::invalid_argument("reciprocal grid needs " + std::to_string(need) + " bytes of scratch, " +
+                                    std::to_string(scratch_bytes) + " available");
+    if (recip_fp32) recip_on<float>(X, Y, M, static_cast<float2*>(scratch), s);
+    else recip_on<double>(X, Y, M, static_cast<double2*>(scratch), s);
     real_part(X, Y, M, sc, jacobi, real_fp32, true, s);
 }
 

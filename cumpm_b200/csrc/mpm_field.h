@@ -98,6 +98,12 @@ public:
     void apply(const double2* X, double2* Y, int M, const double2* self_coef, bool jacobi, bool recip_fp32,
                bool real_fp32, cudaStream_t s);
 
+    // Same as apply(), but the reciprocal-space grid is the caller's scratch
+    // (no allocation here); throws if it is smaller than grid_bytes(M).
+    void apply_scratch(const double2* X, double2* Y, int M, const double2* self_coef, bool jacobi, bool recip_fp32,
+                       bool real_fp32, void* scratch, size_t scratch_bytes, cudaStream_t s);
+    size_t grid_bytes(int M, bool fp64) const;
+
     // Reciprocal-only / real-only parts (for split checks); same layout.
     void apply_part(const double2* X, double2* Y, int M, const double2* self_coef, bool recip_fp32,
                     bool real_fp32, int part, cudaStream_t s);
@@ -123,6 +129,7 @@ private:
     void build_scale(cudaStream_t s);
     cufftHandle plan_for(int M, bool fp32);
     template <typename R> void recip(const double2* X, double2* Y, int M, cudaStream_t s);
+    template <typename R> void recip_on(const double2* X, double2* Y, int M, cplx<R>* grid, cudaStream_t s);
     template <typename R> void transform(cplx<R>* grid, int B, bool inverse, cudaStream_t s);
     void real_part(const double2* X, double2* Y, int M, const double2* self_coef, bool jacobi, bool real_fp32,
                    bool add_recip, cudaStream_t s);

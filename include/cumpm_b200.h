@@ -153,6 +153,22 @@ MPM_API int mpm_field_apply_part(mpm_field* f, const void* X, void* Y, int M, co
                          int real_fp32, int part, void* stream);
 MPM_API int mpm_field_info_get(const mpm_field* f, mpm_field_info* info);
 
+/* Same result as mpm_field_apply, but this call allocates nothing.  No
+ * counterpart in the reference.  For callers that cannot allocate device
+ * memory while they solve (device memory handed to another allocator, or a
+ * loop that must not enter the driver's allocator): the reciprocal-space
+ * grid lives in a static 16 MiB device array of this library (held by every
+ * GPU that loads it, until exit) instead of a cudaMalloc'd buffer.  The
+ * field's per-frame data must already exist (mpm_field_set_positions is the
+ * allocating set-up step).  The first call on a device looks up the array's
+ * device address with that device current; make it before any stream
+ * capture.  All calls share the array: calls that overlap on the GPU race.
+ * Returns MPM_ERR_INVALID if the grid for M right-hand sides exceeds
+ * mpm_noalloc_scratch_bytes(). */
+MPM_API int mpm_field_apply_noalloc(mpm_field* f, const void* X, void* Y, int M, const void* self_coef, int jacobi,
+                                    int recip_fp32, int real_fp32, void* stream);
+MPM_API size_t mpm_noalloc_scratch_bytes(void);
+
 /* batched Krylov solve A X = B on device buffers (X holds the guess) */
 MPM_API int mpm_batch_solve(mpm_field* f, const void* B, void* X, int M, const void* self_coef,
                     const mpm_solve_options* opt, mpm_solve_report* report, void* stream);
