@@ -155,9 +155,11 @@ def ncu_traffic():
 def algorithmic_bytes(info, M, n_pairs, fp64):
     """Minimum DRAM bytes of one launch of each stage of the batched matvec.
 
-    Grid G = stored voxels x 3M complex (spread writes it once, each FFT
-    reads and writes it once, the k-space step reads and writes it once,
-    contraction reads it once); moments/fields are [3N][M] complex128.
+    Grid G = stored voxels x 3M complex.  Spread writes it once; each 3-D
+    transform counts as two read+write sweeps (4G), whatever number of axis
+    passes it uses; the k-space step reads and writes it once plus its
+    coefficients; contraction reads it once.  Moments and fields are
+    [3N][M] complex128; the stencil weights are 3 x S values per particle.
     """
     s = 16 if fp64 else 8
     nx, ny, nz = info["grid"]
@@ -166,12 +168,13 @@ def algorithmic_bytes(info, M, n_pairs, fp64):
     G = nx * ny * zs * 3 * M * s
     mom = 3 * N * M * 16
     S = info["stencil"]
+    w = N * 3 * S * (8 if fp64 else 4)
     b = {
-        "spread": G + mom + N * 3 * S * (8 if fp64 else 4),
-        "fft_fwd": 2 * G,
+        "spread": G + mom + w,
+        "fft_fwd": 4 * G,
         "kspace": 2 * G + (nx * ny * 6 * (2 * zs - 1) * s if info["pruned"] else nx * ny * nz * (8 if fp64 else 4)),
-        "fft_inv": 2 * G,
-        "contract": G + mom + N * 3 * S * (8 if fp64 else 4),
+        "fft_inv": 4 * G,
+        "contract": G + mom + w,
         "real": n_pairs * (4 + (64 if fp64 else 32)) + 3 * mom,
     }
     return b
@@ -198,7 +201,8 @@ def run_ours(args, rank, world, local_rank):
     X = torch.empty_like(X0)
     M = B.shape[1]
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
-    opts = dict(tol=TOL, method=capi.METHOD_GMRES, restart=50, maxiter=1000, refine=True, inner_tol=args.inner_tol)
+    opts = dict(tol=TOL, method=capi.METHOD_GMRES, restart=50, maxiter=1000, refine=True, inner_tol=args.inner_tol,
+                compact=not args.no_compact)
     reports = []
 
     def step():
@@ -206,33 +210,36 @@ def run_ours(args, rank, world, local_rank):
         X.copy_(X0)
         reports.append(F.batch_solve(B, X, S, **opts))
 
+    def timed(nsteps):
+        """nsteps steps, each bracketed by CUDA events after a 256 MB L2 flush."""
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(nsteps)]
+        for k in range(nsteps):
+            flush.fill_(float(k))  # L2 flush outside the timed interval
+            ev[k][0].record()
+            step()
+            ev[k][1].record()
+        torch.cuda.synchronize()
+        if dist:
+            dist.barrier()
+        return sum(a.elapsed_time(b) for a, b in ev)
+
     for _ in range(args.warmup):
         step()
     torch.cuda.synchronize()
     info = F.info()
+
+    # 1) the timed region: no stage timers
     reports.clear()
-    capi.profile_reset()
-    capi.profile_enable(not args.no_profile)
     launches0 = capi.kernel_launches()
     clocks = ClockSampler(local_rank)
     clocks.start()
-    if dist:
-        dist.barrier()
-    torch.cuda.synchronize()
-    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
-    for k in range(args.steps):
-        flush.fill_(float(k))  # L2 flush (256 MB write) outside the timed interval
-        ev[k][0].record()
-        step()
-        ev[k][1].record()
-    torch.cuda.synchronize()
-    if dist:
-        dist.barrier()
+    t_ms = timed(args.steps)
     clk = clocks.stop()
     launches = capi.kernel_launches() - launches0
-    capi.profile_enable(False)
-    stages = capi.profile_read()
-    t_ms = sum(a.elapsed_time(b) for a, b in ev)
+    timed_reports = list(reports)
     # correctness of the timed result: fp64 true residual of every column
     R = B - F.apply(X, self_coef=S)
     rel = (torch.linalg.vector_norm(R, dim=0) / torch.linalg.vector_norm(B, dim=0)).cpu().numpy()
@@ -249,27 +256,53 @@ def run_ours(args, rank, world, local_rank):
     ms_per_step = t_max / args.steps
     value = conv_total / (t_max / 1e3)
 
-    # roofline of the dominant operator stage
+    # 2) the same steps again with per-stage CUDA events on the launching
+    #    stream: stage breakdown and the roofline of the dominant stage
+    reports.clear()
+    capi.profile_reset()
+    capi.profile_enable(not args.no_profile)
+    t_prof = timed(args.steps)
+    capi.profile_enable(False)
+    stages = capi.profile_read()
     matvecs = sum(r["matvecs"] for r in reports)
-    mv64 = sum(r["refine_steps"] + 1 for r in reports)
+    mv64 = sum(r["refine_steps"] + 1 for r in reports)  # fp64 true-residual matvecs, all M columns
     mv32 = matvecs - mv64
-    b32 = algorithmic_bytes(info, M, info["num_pairs"], False)
-    b64 = algorithmic_bytes(info, M, info["num_pairs"], True)
+    col64 = mv64 * M
+    col32 = sum(r["column_matvecs"] for r in reports) - col64
     op_stages = ["spread", "fft_fwd", "kspace", "fft_inv", "contract", "real"]
+
+    def stage_bytes(k):
+        """Algorithmic bytes of stage k over the pass: per-column part x columns + fixed part x launches."""
+        tot = 0.0
+        for fp64, mv, cols in ((False, mv32, col32), (True, mv64, col64)):
+            b0 = algorithmic_bytes(info, 0, info["num_pairs"], fp64)[k]
+            b1 = algorithmic_bytes(info, 1, info["num_pairs"], fp64)[k]
+            tot += b0 * mv + (b1 - b0) * cols
+        return tot
+
+    b32 = algorithmic_bytes(info, M, info["num_pairs"], False)
     dom = max(op_stages, key=lambda k: stages[k][0])
     dom_ms, dom_n = stages[dom]
-    bytes_total = b32[dom] * mv32 + b64[dom] * mv64
+    bytes_total = stage_bytes(dom)
     peak, peak_kind = measured_peaks()
     achieved = bytes_total / (dom_ms / 1e3) / 1e9 if dom_ms > 0 else 0.0
     traffic = ncu_traffic().get(dom)
-    mv_bytes = sum(b32[k] for k in op_stages) * mv32 + sum(b64[k] for k in op_stages) * mv64
+    mv_bytes = sum(stage_bytes(k) for k in op_stages)
     mv_ms = sum(stages[k][0] for k in op_stages)
-    iters = [r["total_iterations"] / M for r in reports]
+    mv_frac = round(mv_bytes / (mv_ms / 1e3) / 1e9 / peak, 4) if mv_ms > 0 else None
+
+    # 3) the plain per-system fp64 solve on the same operator: one right-hand
+    #    side per solve, fp64 reciprocal and real space, no refinement
+    plain = run_plain(args, F, B, X0, S, M, torch, capi) if not args.no_plain else None
+    iters = [r["total_iterations"] / M for r in timed_reports]
+    mv_per_step = sum(r["matvecs"] for r in timed_reports) / max(1, len(timed_reports))
+    colmv_per_step = sum(r["column_matvecs"] for r in timed_reports) / max(1, len(timed_reports))
 
     out = None
     if rank == 0:
         e2e = run_e2e(args, torch) if world == 1 and not args.no_e2e else None
-        cpu = cpu_baseline(args) if world == 1 and not args.no_cpu else None
+        per_solve = plain["matvecs_per_solve"] if plain else PLAIN_MATVECS_PER_SOLVE
+        cpu = cpu_baseline(args, per_solve) if world == 1 and not args.no_cpu else None
         out = {
             "metric": "solves/s at N=4000, res 1e-6: batched mixed-prec vs plain; matvec % HBM peak",
             "value": round(value, 3),
@@ -291,14 +324,21 @@ def run_ours(args, rank, world, local_rank):
                 "converged_per_step": converged,
                 "max_true_rel_resid": float(rel.max()),
                 "krylov_steps_per_rhs": round(float(np.mean(iters)), 2),
-                "matvecs_per_step": matvecs / max(1, len(reports)),
+                "matvecs_per_step": mv_per_step,
+                "column_matvecs_per_step": colmv_per_step,
+                "inner_tol": f"max({args.inner_tol:g}, 0.5 tol |b_m| / |r_m|) per column",
+                "compact_batch": not args.no_compact,
                 "grid": info["grid"], "pruned_z_slots": info["z_slots"] if info["pruned"] else None,
                 "real_space_pairs": info["num_pairs"],
                 "l2": "inputs larger than L2 (grid + Krylov basis > 126 MB) and a 256 MB L2 flush before each step",
                 "parallelism": f"replicas x{world}",
+                "profiled_ms_per_step": round(t_prof / args.steps, 3),
                 "stage_ms_per_step": {k: round(v[0] / args.steps, 3) for k, v in stages.items()},
-                "matvec_hbm_frac": round(mv_bytes / (mv_ms / 1e3) / 1e9 / peak, 4) if mv_ms > 0 else None,
+                "stage_launches_per_step": {k: v[1] / args.steps for k, v in stages.items()},
             },
+            "matvec_hbm_frac": mv_frac,
+            "plain_fp64": plain,
+            "batched_vs_plain": round(value / plain["value"], 2) if plain else None,
             "roofline": {
                 "kernel": dom,
                 "bound": "hbm",
@@ -308,8 +348,10 @@ def run_ours(args, rank, world, local_rank):
                 "unit": "GB/s",
                 "frac": round(achieved / peak, 4),
                 "traffic": None if traffic is None else traffic,
-                "algorithmic_bytes_per_launch": b32[dom],
+                "algorithmic_bytes_per_launch": round(bytes_total / max(1, dom_n)),
+                "algorithmic_bytes_full_batch_fp32": b32[dom],
                 "launches": dom_n,
+                "timing": "per-stage CUDA events on the launching stream over a second pass of the timed steps",
             },
             "cpu_baseline": cpu,
             "e2e": e2e,
@@ -321,6 +363,41 @@ def run_ours(args, rank, world, local_rank):
         dist.barrier()
         dist.destroy_process_group()
     return out
+
+
+def run_plain(args, F, B, X0, S, M, torch, capi):
+    """Plain per-system fp64 solves: one right-hand side at a time.
+
+    All 30 right-hand sides are solved one by one with GMRES(50)+Jacobi on
+    the fp64 operator (the reference's plain method), each timed with CUDA
+    events; their count over the summed time gives plain solves/s.
+    """
+    cols = list(range(M))
+    Xp = torch.empty((B.shape[0], 1), dtype=B.dtype, device=B.device)
+    o = dict(tol=TOL, method=capi.METHOD_GMRES, restart=50, maxiter=1000, recip_fp32=False, refine=False)
+    # warm-up: plans and buffers for M=1
+    Xp.copy_(X0[:, :1])
+    F.batch_solve(B[:, :1].contiguous(), Xp, S[:, :1].contiguous(), **o)
+    torch.cuda.synchronize()
+    tot_ms, mvs, ok = 0.0, 0, 0
+    for c in cols:
+        b = B[:, c:c + 1].contiguous()
+        sc = S[:, c:c + 1].contiguous()
+        Xp.copy_(X0[:, c:c + 1])
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record()
+        r = F.batch_solve(b, Xp, sc, **o)
+        e1.record()
+        torch.cuda.synchronize()
+        tot_ms += e0.elapsed_time(e1)
+        mvs += r["matvecs"]
+        rr = b - F.apply(Xp, self_coef=sc)
+        ok += int(float(torch.linalg.vector_norm(rr) / torch.linalg.vector_norm(b)) <= TOL * 1.0001)
+    n = len(cols)
+    return {"value": round(n / (tot_ms / 1e3), 3), "unit": "solves/s", "rhs_sampled": n, "converged": ok,
+            "ms_per_solve": round(tot_ms / n, 3), "matvecs_per_solve": mvs / n,
+            "method": "GMRES(50)+Jacobi, fp64 operator, 1 RHS per solve, no refinement, all 30 RHS"}
 
 
 def run_e2e(args, torch):
@@ -349,8 +426,12 @@ def run_e2e(args, torch):
             "timing": "wall clock around compute()+get_dipoles(), median of steps"}
 
 
-def cpu_matvec_sample(threads):
-    """One fp64 matvec (1 RHS) of the CPU port of the reference operator."""
+def cpu_matvec_sample(threads, min_s=10.0, max_n=8):
+    """Mean time of fp64 matvecs (1 RHS) of the CPU port of the reference operator.
+
+    Repeats the matvec on the full workload until about min_s seconds of CPU
+    work (at most max_n matvecs); the per-frame precalculation is excluded.
+    """
     from oracle import mpm_oracle as O
 
     pos, box, eps = workload(0)
@@ -360,29 +441,32 @@ def cpu_matvec_sample(threads):
     rng = np.random.default_rng(0)
     x = rng.standard_normal(3 * N) + 1j * rng.standard_normal(3 * N)
     sc = np.full(N, 3.0 / (4 * np.pi * (eps[0] / EPS_M - 1.0)))
-    t0 = time.perf_counter()
-    op.apply(x, sc)
-    return time.perf_counter() - t0
+    ts = []
+    while len(ts) < max_n and sum(ts) < min_s:
+        t0 = time.perf_counter()
+        op.apply(x, sc)
+        ts.append(time.perf_counter() - t0)
+    return float(np.mean(ts)), len(ts)
 
 
-def cpu_baseline(args):
+def cpu_baseline(args, matvecs_per_solve=PLAIN_MATVECS_PER_SOLVE):
     threads = os.cpu_count() or 1
-    t = cpu_matvec_sample(threads)
-    v = 1.0 / (t * PLAIN_MATVECS_PER_SOLVE)
+    t, n = cpu_matvec_sample(threads)
+    v = 1.0 / (t * matvecs_per_solve)
     return {"value": round(v, 5), "unit": "solves/s", "cores": threads, "kind": "port",
-            "sample": f"1 fp64 matvec of the CPU port on the full workload ({t:.2f} s, FFT on {threads} threads); "
-                      f"solves/s = 1/(t x {PLAIN_MATVECS_PER_SOLVE:g} matvecs per solve)"}
+            "sample": f"{n} fp64 matvecs of the CPU port (oracle/) on the full workload, mean {t:.2f} s each, "
+                      f"FFT on {threads} threads; solves/s = 1/(t x {matvecs_per_solve:g} matvecs per plain fp64 solve)"}
 
 
 def run_reference(args, rank):
+    """CPU port of the reference operator on the host cores (rank 0 only)."""
     if rank != 0:
         return
     threads = os.cpu_count() or 1
     ts = []
-    for _ in range(args.warmup if args.warmup < 1 else 0):
-        pass
     for _ in range(max(1, args.steps)):
-        ts.append(cpu_matvec_sample(threads))
+        t, _n = cpu_matvec_sample(threads, min_s=0.0, max_n=1)
+        ts.append(t)
     t = float(np.median(ts))
     v = 1.0 / (t * PLAIN_MATVECS_PER_SOLVE)
     line = {
@@ -391,11 +475,11 @@ def run_reference(args, rank):
         "value": round(v, 5), "unit": "solves/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": round(t * 1e3, 1), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "c128", "data": "synthetic (hexagonal monolayer generated as in the reference benchmark)",
-        "config": {"workload": "N=4000 hex monolayer, 30 RHS, tol 1e-6 (see bench.py docstring)",
+        "config": {"workload": "N=4000 hex monolayer, 30 RHS, tol 1e-6, GMRES(50)+Jacobi, fp64",
                    "step": "one fp64 matvec of the CPU port of the reference operator (bounded sample)"},
         "cpu_baseline": {"value": round(v, 5), "unit": "solves/s", "cores": threads, "kind": "port",
                          "sample": f"1 fp64 matvec per step, median {t:.2f} s; solves/s = 1/(t x "
-                                   f"{PLAIN_MATVECS_PER_SOLVE:g} matvecs per solve)"},
+                                   f"{PLAIN_MATVECS_PER_SOLVE:g} matvecs per plain fp64 solve)"},
         "e2e": {"value": round(v, 5), "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -407,10 +491,12 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--inner-tol", type=float, default=1e-4)
+    ap.add_argument("--inner-tol", type=float, default=1e-4, help="floor of one inner solve's reduction")
+    ap.add_argument("--no-compact", action="store_true", help="idle columns still go through the operator")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--no-profile", action="store_true", help="no stage timers in the timed region")
+    ap.add_argument("--no-profile", action="store_true", help="skip the stage-timer pass")
+    ap.add_argument("--no-plain", action="store_true", help="skip the plain per-system fp64 leg")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))

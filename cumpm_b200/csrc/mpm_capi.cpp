@@ -138,7 +138,7 @@ int mpm_solver_set_options(mpm_solver* s, int restart, int maxiter, int batch_al
                            int real_fp32) {
     return guard([&] {
         need(s, "solver");
-        if (restart < 1 || maxiter < 1 || !(inner_tol > 0)) throw std::invalid_argument("invalid solver options");
+        if (restart < 1 || maxiter < 1 || !(inner_tol >= 0)) throw std::invalid_argument("invalid solver options");
         auto& o = s->impl->options();
         o.restart = restart;
         o.maxiter = maxiter;
@@ -305,6 +305,8 @@ int mpm_batch_solve(mpm_field* f, const void* B, void* X, int M, const void* sc,
         o.real_fp32 = opt->real_fp32 != 0;
         o.refine = opt->refine != 0;
         o.inner_tol = opt->inner_tol;
+        o.compact = opt->compact != 0;
+        if (!(o.inner_tol >= 0.0)) throw std::invalid_argument("inner_tol must be >= 0");
         mpm::SolveStats st;
         f->solver->solve(*f->impl, static_cast<const double2*>(B), static_cast<double2*>(X), M,
                          static_cast<const double2*>(sc), o, st, static_cast<cudaStream_t>(stream));
@@ -312,6 +314,7 @@ int mpm_batch_solve(mpm_field* f, const void* B, void* X, int M, const void* sc,
             std::memset(rep, 0, sizeof(*rep));
             rep->matvecs = st.matvecs;
             rep->refine_steps = st.refine_steps;
+            rep->column_matvecs = st.column_matvecs;
             for (int m = 0; m < M; ++m) {
                 rep->total_iterations += st.iters[m];
                 rep->max_iterations = std::max(rep->max_iterations, st.iters[m]);

@@ -106,17 +106,20 @@ struct GState {
     int pad[3];
 };
 
-// start of a restart cycle: residual norm test and V_0 = r / |r|
+__device__ __forceinline__ double col_tol(double tol, const double* tolv, int m) { return tolv ? tolv[m] : tol; }
+
+// start of a restart cycle: residual norm test and V_0 = r / |r|.
+// flag[0] counts the cycling columns, flag[1 + m] is column m's cycle flag.
 __global__ void k_gm_begin(GState* __restrict__ st, const double* __restrict__ rn, const double* __restrict__ bn,
-                           double tol, int maxiter, int restart, double2* __restrict__ g, int M,
-                           int* __restrict__ flag) {
+                           double tol, const double* __restrict__ tolv, int maxiter, int restart,
+                           double2* __restrict__ g, int M, int* __restrict__ flag) {
     const int m = blockIdx.x * blockDim.x + threadIdx.x;
     if (m >= M) return;
     GState s = st[m];
     s.cyc = 0;
     s.kcount = 0;
     if (s.active) {
-        if (rn[m] < tol * bn[m]) {
+        if (rn[m] < col_tol(tol, tolv, m) * bn[m]) {
             s.active = 0;
             s.converged = 1;
         } else if (s.iters >= maxiter) {
@@ -128,6 +131,7 @@ __global__ void k_gm_begin(GState* __restrict__ st, const double* __restrict__ r
             atomicAdd(flag, 1);
         }
     }
+    flag[1 + m] = s.cyc;
     st[m] = s;
 }
 
@@ -152,11 +156,14 @@ __global__ void k_addto(double2* __restrict__ a, const double2* __restrict__ b, 
 __global__ void k_gm_givens(GState* __restrict__ st, const double2* __restrict__ h, const double* __restrict__ wn,
                             double2* __restrict__ H, double2* __restrict__ g, double* __restrict__ cs,
                             double2* __restrict__ sn, int k, int restart, int M, const double* __restrict__ bn,
-                            double tol, int maxiter, int* __restrict__ flag) {
+                            double tol, const double* __restrict__ tolv, int maxiter, int* __restrict__ flag) {
     const int m = blockIdx.x * blockDim.x + threadIdx.x;
     if (m >= M) return;
     GState s = st[m];
-    if (!s.cyc) return;
+    if (!s.cyc) {
+        flag[1 + m] = 0;
+        return;
+    }
     const int ld = restart + 1;
     double2* Hm = H + size_t(m) * ld * restart;   // column-major: Hm[col*ld + row]
     double2* gm = g + size_t(m) * ld;
@@ -202,12 +209,13 @@ __global__ void k_gm_givens(GState* __restrict__ st, const double2* __restrict__
     gm[k + 1] = (sv * g1) * -1.0 + g2 * c;
     s.iters += 1;
     const double resid = hypot(gm[k + 1].x, gm[k + 1].y);
-    if (resid < tol * bn[m] || k + 1 >= restart || s.iters >= maxiter) {
+    if (resid < col_tol(tol, tolv, m) * bn[m] || k + 1 >= restart || s.iters >= maxiter) {
         s.cyc = 0;
         s.kcount = k + 1;
     } else {
         atomicAdd(flag, 1);
     }
+    flag[1 + m] = s.cyc;
     st[m] = s;
 }
 
@@ -254,7 +262,7 @@ struct BState {
 };
 
 __global__ void k_bi_init(BState* __restrict__ st, const double* __restrict__ bn, const double* __restrict__ rn,
-                          double tol, int M) {
+                          double tol, const double* __restrict__ tolv, int M) {
     const int m = blockIdx.x * blockDim.x + threadIdx.x;
     if (m >= M) return;
     BState s{};
@@ -262,7 +270,7 @@ __global__ void k_bi_init(BState* __restrict__ st, const double* __restrict__ bn
     s.beta = make_double2(0, 0);
     s.active = 1;
     if (bn[m] == 0.0) { s.active = 0; s.converged = 1; }
-    else if (rn[m] < tol * bn[m]) { s.active = 0; s.converged = 1; }
+    else if (rn[m] < col_tol(tol, tolv, m) * bn[m]) { s.active = 0; s.converged = 1; }
     st[m] = s;
 }
 
@@ -319,13 +327,13 @@ __global__ void k_bi_s(double2* __restrict__ sv, const double2* __restrict__ r, 
 
 // step C: |s| < tol |b| => x += alpha p and stop (mode 1)
 __global__ void k_bi_c(BState* __restrict__ st, const double* __restrict__ sn, const double* __restrict__ bn,
-                       double tol, int* __restrict__ mode, int M) {
+                       double tol, const double* __restrict__ tolv, int* __restrict__ mode, int M) {
     const int m = blockIdx.x * blockDim.x + threadIdx.x;
     if (m >= M) return;
     BState s = st[m];
     mode[m] = 0;
     if (!s.active) return;
-    if (sn[m] < tol * bn[m]) {
+    if (sn[m] < col_tol(tol, tolv, m) * bn[m]) {
         mode[m] = 1;
         s.active = 0;
         s.converged = 1;
@@ -366,30 +374,40 @@ __global__ void k_bi_xr(double2* __restrict__ x, double2* __restrict__ r, const 
 
 // step E: |r| < tol |b| or omega ~ 0 => stop; count still active
 __global__ void k_bi_e(BState* __restrict__ st, const double* __restrict__ rn, const double* __restrict__ bn,
-                       double tol, int maxiter, int* __restrict__ flag, int M) {
+                       double tol, const double* __restrict__ tolv, int maxiter, int* __restrict__ flag, int M) {
     const int m = blockIdx.x * blockDim.x + threadIdx.x;
     if (m >= M) return;
     BState s = st[m];
-    if (!s.active) return;
-    if (rn[m] < tol * bn[m]) { s.active = 0; s.converged = 1; }
-    else if (cabs_(s.omega) < 1e-16) s.active = 0;
-    else if (s.iters >= maxiter) s.active = 0;
-    if (s.active) atomicAdd(flag, 1);
-    st[m] = s;
+    if (s.active) {
+        if (rn[m] < col_tol(tol, tolv, m) * bn[m]) { s.active = 0; s.converged = 1; }
+        else if (cabs_(s.omega) < 1e-16) s.active = 0;
+        else if (s.iters >= maxiter) s.active = 0;
+        if (s.active) atomicAdd(flag, 1);
+        st[m] = s;
+    }
+    flag[1 + m] = s.active;
 }
 
 __global__ void k_bi_count(const BState* __restrict__ st, int* __restrict__ flag, int M) {
     const int m = blockIdx.x * blockDim.x + threadIdx.x;
-    if (m < M && st[m].active) atomicAdd(flag, 1);
+    if (m >= M) return;
+    flag[1 + m] = st[m].active;
+    if (st[m].active) atomicAdd(flag, 1);
 }
 
-// refinement bookkeeping: zero the correction RHS of converged columns
-__global__ void k_mask_cols(double2* __restrict__ r, const double* __restrict__ rn, const double* __restrict__ bn,
-                            double tol, size_t n, int M) {
+// refinement bookkeeping: a column stays converged once its true residual
+// met the target (later rounds leave its x and its stale residual alone)
+__global__ void k_conv_update(const double* __restrict__ rn, const double* __restrict__ bn, double tol,
+                              int* __restrict__ conv, int M) {
+    const int m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m < M && !conv[m] && rn[m] <= tol * bn[m]) conv[m] = 1;
+}
+
+// zero the correction right-hand side of converged columns
+__global__ void k_mask_conv(double2* __restrict__ r, const int* __restrict__ conv, size_t n, int M) {
     const size_t t = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
     if (t >= n) return;
-    const int m = int(t % M);
-    if (rn[m] <= tol * bn[m]) r[t] = make_double2(0, 0);
+    if (conv[t % M]) r[t] = make_double2(0, 0);
 }
 
 __global__ void k_axpy1(double2* __restrict__ x, const double2* __restrict__ d, size_t n) {
@@ -397,19 +415,119 @@ __global__ void k_axpy1(double2* __restrict__ x, const double2* __restrict__ d, 
     if (t < n) x[t] += d[t];
 }
 
+// dst[row][j] = src[row][idx[j]]  (compact batch of the listed columns)
+__global__ void k_gather_cols(const double2* __restrict__ src, int M, double2* __restrict__ dst, int Ma,
+                              const int* __restrict__ idx, int rows) {
+    const size_t t = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (t >= size_t(rows) * Ma) return;
+    const size_t row = t / Ma;
+    const int j = int(t - row * Ma);
+    dst[t] = src[row * M + idx[j]];
+}
+
+// dst[row][idx[j]] = src[row][j]
+__global__ void k_scatter_cols(const double2* __restrict__ src, int Ma, double2* __restrict__ dst, int M,
+                               const int* __restrict__ idx, int rows) {
+    const size_t t = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (t >= size_t(rows) * Ma) return;
+    const size_t row = t / Ma;
+    const int j = int(t - row * Ma);
+    dst[row * M + idx[j]] = src[t];
+}
+
+// inner tolerance of column m: stop once its residual is below 0.5 tol |b_m|,
+// i.e. relative to its own right-hand side |r_m|: 0.5 tol |b_m| / |r_m|,
+// but ask no inner solve for a reduction below `floor` (fp32 rounding of
+// the operator limits what one inner solve can reach) nor above 0.5.
+__global__ void k_inner_tol(const double* __restrict__ rn, const double* __restrict__ bn, double tol, double floor,
+                            double* __restrict__ tolv, int M) {
+    const int m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= M) return;
+    double t = rn[m] > 0.0 ? 0.5 * tol * bn[m] / rn[m] : 0.5;
+    tolv[m] = fmin(0.5, fmax(floor, t));
+}
+
 }  // namespace
 
 // ------------------------------------------------------------ host side --
 
-BatchSolver::BatchSolver() { MPM_CUDA(cudaMallocHost(&flag_, sizeof(int))); }
+BatchSolver::BatchSolver() {
+    MPM_CUDA(cudaMallocHost(&flag_, sizeof(int)));
+    flag_cap_ = 1;
+}
 BatchSolver::~BatchSolver() {
     if (flag_) cudaFreeHost(flag_);
+    if (hidx_) cudaFreeHost(hidx_);
 }
 
-int BatchSolver::read_flag(const int* dflag, cudaStream_t s) {
-    MPM_CUDA(cudaMemcpyAsync(flag_, dflag, sizeof(int), cudaMemcpyDeviceToHost, s));
+int BatchSolver::read_flags(const int* dflag, int M, cudaStream_t s) {
+    if (M + 1 > flag_cap_) {
+        MPM_CUDA(cudaStreamSynchronize(s));
+        if (flag_) MPM_CUDA(cudaFreeHost(flag_));
+        flag_ = nullptr;
+        MPM_CUDA(cudaMallocHost(&flag_, sizeof(int) * (M + 1)));
+        flag_cap_ = M + 1;
+    }
+    MPM_CUDA(cudaMemcpyAsync(flag_, dflag, sizeof(int) * (M + 1), cudaMemcpyDeviceToHost, s));
     MPM_CUDA(cudaStreamSynchronize(s));
     return *flag_;
+}
+
+int BatchSolver::apply_cols(Field& F, const double2* X, double2* Y, int M, const double2* sc, bool jacobi,
+                            bool r32, bool re32, const int* active, bool compact, cudaStream_t s) {
+    if (!compact || !active) {
+        F.apply(X, Y, M, sc, jacobi, r32, re32, s);
+        return M;
+    }
+    std::vector<int> cols;
+    cols.reserve(M);
+    for (int m = 0; m < M; ++m)
+        if (active[m]) cols.push_back(m);
+    const int Ma = int(cols.size());
+    if (Ma == 0) return 0;
+    if (Ma == M) {
+        F.apply(X, Y, M, sc, jacobi, r32, re32, s);
+        return M;
+    }
+    const int rin = F.rows_in(), rout = F.rows_out(), N = F.num_particles();
+    if (cols != cur_cols_) {
+        StageScope scope(ST_KRYLOV, s);
+        if (Ma > hidx_cap_) {
+            MPM_CUDA(cudaStreamSynchronize(s));
+            if (hidx_) MPM_CUDA(cudaFreeHost(hidx_));
+            hidx_ = nullptr;
+            MPM_CUDA(cudaMallocHost(&hidx_, sizeof(int) * M));
+            hidx_cap_ = M;
+        }
+        // the previous upload from hidx_ has completed: every change of the
+        // column set follows a flag read, which synchronises the stream
+        std::copy(cols.begin(), cols.end(), hidx_);
+        cidx_.ensure(sizeof(int) * M);
+        MPM_CUDA(cudaMemcpyAsync(cidx_.p, hidx_, sizeof(int) * Ma, cudaMemcpyHostToDevice, s));
+        if (sc) {
+            scc_.ensure(sizeof(double2) * size_t(N) * M);
+            k_gather_cols<<<nblk((long long)N * Ma, 256), 256, 0, s>>>(sc, M, scc_.as<double2>(), Ma,
+                                                                        cidx_.as<int>(), N);
+            MPM_LAUNCH();
+        }
+        cur_cols_ = cols;
+    }
+    xc_.ensure(sizeof(double2) * size_t(rin) * M);
+    yc_.ensure(sizeof(double2) * size_t(rout) * M);
+    {
+        StageScope scope(ST_KRYLOV, s);
+        k_gather_cols<<<nblk((long long)rin * Ma, 256), 256, 0, s>>>(X, M, xc_.as<double2>(), Ma, cidx_.as<int>(),
+                                                                     rin);
+        MPM_LAUNCH();
+    }
+    F.apply(xc_.as<double2>(), yc_.as<double2>(), Ma, sc ? scc_.as<double2>() : nullptr, jacobi, r32, re32, s);
+    {
+        StageScope scope(ST_KRYLOV, s);
+        k_scatter_cols<<<nblk((long long)rout * Ma, 256), 256, 0, s>>>(yc_.as<double2>(), Ma, Y, M,
+                                                                       cidx_.as<int>(), rout);
+        MPM_LAUNCH();
+    }
+    return Ma;
 }
 
 void BatchSolver::dots(const double2* V, size_t vstride, int nvec, const double2* w, int rows, int M, int conj,
@@ -451,7 +569,7 @@ void BatchSolver::true_residual(Field& F, const double2* b, const double2* x, in
 }
 
 void BatchSolver::gmres(Field& F, const double2* b, double2* x, int M, const double2* sc, const SolveOptions& opt,
-                        SolveStats& st, bool r32, bool re32, cudaStream_t s) {
+                        SolveStats& st, bool r32, bool re32, cudaStream_t s, bool x_zero, const double* tolv) {
     const int rows = F.rows_in();
     const size_t n = size_t(rows) * M;
     const int restart = std::max(1, std::min(rows, opt.restart));
@@ -469,7 +587,8 @@ void BatchSolver::gmres(Field& F, const double2* b, double2* x, int M, const dou
     w_.ensure(sizeof(double2) * n);
     r_.ensure(sizeof(double2) * n);
     bj_.ensure(sizeof(double2) * n);
-    flagdev_.ensure(sizeof(int));
+    flagdev_.ensure(sizeof(int) * (M + 1));
+    cur_cols_.clear();  // self coefficients may differ from the previous call
     double2* V = V_.as<double2>();
     GState* gs = state_.as<GState>();
     int* kper = reinterpret_cast<int*>(gs + M);
@@ -488,24 +607,35 @@ void BatchSolver::gmres(Field& F, const double2* b, double2* x, int M, const dou
         MPM_LAUNCH();
         bj = bj_.as<double2>();
     }
+    // columns cycling at the start of the current cycle (empty: all)
+    std::vector<int> begin_cols;
+    bool first = true;
     while (true) {
-        // r = D^-1 (b - A x)
-        F.apply(x, w_.as<double2>(), M, sc, opt.jacobi, r32, re32, s);
-        st.matvecs++;
-        k_sub<<<vb, 256, 0, s>>>(bj, w_.as<double2>(), r_.as<double2>(), n);
-        MPM_LAUNCH();
+        // r = D^-1 (b - A x), for the columns that cycled last time
+        if (first && x_zero) {
+            MPM_CUDA(cudaMemcpyAsync(r_.p, bj, sizeof(double2) * n, cudaMemcpyDeviceToDevice, s));
+        } else {
+            st.column_matvecs += apply_cols(F, x, w_.as<double2>(), M, sc, opt.jacobi, r32, re32,
+                                            begin_cols.empty() ? nullptr : begin_cols.data(), opt.compact, s);
+            st.matvecs++;
+            k_sub<<<vb, 256, 0, s>>>(bj, w_.as<double2>(), r_.as<double2>(), n);
+            MPM_LAUNCH();
+        }
+        first = false;
         norms(r_.as<double2>(), rows, M, rnorm_.as<double>(), s);
         MPM_CUDA(cudaMemsetAsync(dflag, 0, sizeof(int), s));
-        k_gm_begin<<<mb, 128, 0, s>>>(gs, rnorm_.as<double>(), bnorm_.as<double>(), opt.tol, opt.maxiter, restart,
-                                      g_.as<double2>(), M, dflag);
+        k_gm_begin<<<mb, 128, 0, s>>>(gs, rnorm_.as<double>(), bnorm_.as<double>(), opt.tol, tolv, opt.maxiter,
+                                      restart, g_.as<double2>(), M, dflag);
         MPM_LAUNCH();
         k_normalize<<<vb, 256, 0, s>>>(r_.as<double2>(), V, rnorm_.as<double>(), gs, n, M);
         MPM_LAUNCH();
-        if (read_flag(dflag, s) == 0) break;
+        if (read_flags(dflag, M, s) == 0) break;
+        begin_cols.assign(flag_ + 1, flag_ + 1 + M);
+        std::vector<int> cyc = begin_cols;
         for (int k = 0; k < restart; ++k) {
             double2* Vk = V + size_t(k) * n;
             double2* w = w_.as<double2>();
-            F.apply(Vk, w, M, sc, opt.jacobi, r32, re32, s);
+            st.column_matvecs += apply_cols(F, Vk, w, M, sc, opt.jacobi, r32, re32, cyc.data(), opt.compact, s);
             st.matvecs++;
             // CGS2
             dots(V, n, k + 1, w, rows, M, 1, h_.as<double2>(), s);
@@ -528,9 +658,10 @@ void BatchSolver::gmres(Field& F, const double2* b, double2* x, int M, const dou
             MPM_CUDA(cudaMemsetAsync(dflag, 0, sizeof(int), s));
             k_gm_givens<<<mb, 128, 0, s>>>(gs, h_.as<double2>(), rnorm_.as<double>(), H_.as<double2>(),
                                            g_.as<double2>(), cs_.as<double>(), sn_.as<double2>(), k, restart, M,
-                                           bnorm_.as<double>(), opt.tol, opt.maxiter, dflag);
+                                           bnorm_.as<double>(), opt.tol, tolv, opt.maxiter, dflag);
             MPM_LAUNCH();
-            if (read_flag(dflag, s) == 0) break;
+            if (read_flags(dflag, M, s) == 0) break;
+            cyc.assign(flag_ + 1, flag_ + 1 + M);
         }
         k_gm_backsub<<<mb, 128, 0, s>>>(gs, H_.as<double2>(), g_.as<double2>(), y_.as<double2>(), restart, M, kper);
         MPM_LAUNCH();
@@ -549,7 +680,7 @@ void BatchSolver::gmres(Field& F, const double2* b, double2* x, int M, const dou
 }
 
 void BatchSolver::bicgstab(Field& F, const double2* b, double2* x, int M, const double2* sc, const SolveOptions& opt,
-                           SolveStats& st, bool r32, bool re32, cudaStream_t s) {
+                           SolveStats& st, bool r32, bool re32, cudaStream_t s, bool x_zero, const double* tolv) {
     const int rows = F.rows_in();
     const size_t n = size_t(rows) * M;
     for (DevBuf* d : {&r0_, &p_, &v_, &s_, &t_, &r_, &w_, &bj_}) d->ensure(sizeof(double2) * n);
@@ -557,7 +688,8 @@ void BatchSolver::bicgstab(Field& F, const double2* b, double2* x, int M, const 
     rnorm_.ensure(sizeof(double) * M * 2);
     scal_.ensure(sizeof(BState) * M + sizeof(int) * M);
     h_.ensure(sizeof(double2) * M * 2);
-    flagdev_.ensure(sizeof(int));
+    flagdev_.ensure(sizeof(int) * (M + 1));
+    cur_cols_.clear();
     BState* bs = scal_.as<BState>();
     int* mode = reinterpret_cast<int*>(bs + M);
     int* dflag = flagdev_.as<int>();
@@ -575,12 +707,17 @@ void BatchSolver::bicgstab(Field& F, const double2* b, double2* x, int M, const 
         bj = bj_.as<double2>();
     }
     double2* r = r_.as<double2>();
-    F.apply(x, w_.as<double2>(), M, sc, opt.jacobi, r32, re32, s);
-    st.matvecs++;
-    k_sub<<<vb, 256, 0, s>>>(bj, w_.as<double2>(), r, n);
-    MPM_LAUNCH();
+    if (x_zero) {
+        MPM_CUDA(cudaMemcpyAsync(r, bj, sizeof(double2) * n, cudaMemcpyDeviceToDevice, s));
+    } else {
+        F.apply(x, w_.as<double2>(), M, sc, opt.jacobi, r32, re32, s);
+        st.matvecs++;
+        st.column_matvecs += M;
+        k_sub<<<vb, 256, 0, s>>>(bj, w_.as<double2>(), r, n);
+        MPM_LAUNCH();
+    }
     norms(r, rows, M, rnorm_.as<double>(), s);
-    k_bi_init<<<mb, 128, 0, s>>>(bs, bnorm_.as<double>(), rnorm_.as<double>(), opt.tol, M);
+    k_bi_init<<<mb, 128, 0, s>>>(bs, bnorm_.as<double>(), rnorm_.as<double>(), opt.tol, tolv, M);
     MPM_LAUNCH();
     MPM_CUDA(cudaMemcpyAsync(r0_.p, r, sizeof(double2) * n, cudaMemcpyDeviceToDevice, s));
     MPM_CUDA(cudaMemcpyAsync(p_.p, r, sizeof(double2) * n, cudaMemcpyDeviceToDevice, s));
@@ -588,14 +725,16 @@ void BatchSolver::bicgstab(Field& F, const double2* b, double2* x, int M, const 
     MPM_CUDA(cudaMemsetAsync(dflag, 0, sizeof(int), s));
     k_bi_count<<<mb, 128, 0, s>>>(bs, dflag, M);
     MPM_LAUNCH();
-    if (read_flag(dflag, s) > 0) {
+    if (read_flags(dflag, M, s) > 0) {
+        std::vector<int> act(flag_ + 1, flag_ + 1 + M);
         for (int it = 0; it < opt.maxiter; ++it) {
             dots(r0_.as<double2>(), 0, 1, r, rows, M, 0, hv, s);
             k_bi_a<<<mb, 128, 0, s>>>(bs, hv, it, M);
             MPM_LAUNCH();
             k_bi_p<<<vb, 256, 0, s>>>(p_.as<double2>(), v_.as<double2>(), r, bs, it, n, M);
             MPM_LAUNCH();
-            F.apply(p_.as<double2>(), v_.as<double2>(), M, sc, opt.jacobi, r32, re32, s);
+            st.column_matvecs += apply_cols(F, p_.as<double2>(), v_.as<double2>(), M, sc, opt.jacobi, r32, re32,
+                                            act.data(), opt.compact, s);
             st.matvecs++;
             dots(r0_.as<double2>(), 0, 1, v_.as<double2>(), rows, M, 0, hv, s);
             k_bi_b<<<mb, 128, 0, s>>>(bs, hv, M);
@@ -603,11 +742,12 @@ void BatchSolver::bicgstab(Field& F, const double2* b, double2* x, int M, const 
             k_bi_s<<<vb, 256, 0, s>>>(s_.as<double2>(), r, v_.as<double2>(), bs, n, M);
             MPM_LAUNCH();
             norms(s_.as<double2>(), rows, M, rnorm_.as<double>(), s);
-            k_bi_c<<<mb, 128, 0, s>>>(bs, rnorm_.as<double>(), bnorm_.as<double>(), opt.tol, mode, M);
+            k_bi_c<<<mb, 128, 0, s>>>(bs, rnorm_.as<double>(), bnorm_.as<double>(), opt.tol, tolv, mode, M);
             MPM_LAUNCH();
             k_bi_xfinal<<<vb, 256, 0, s>>>(x, p_.as<double2>(), bs, mode, n, M);
             MPM_LAUNCH();
-            F.apply(s_.as<double2>(), t_.as<double2>(), M, sc, opt.jacobi, r32, re32, s);
+            st.column_matvecs += apply_cols(F, s_.as<double2>(), t_.as<double2>(), M, sc, opt.jacobi, r32, re32,
+                                            act.data(), opt.compact, s);
             st.matvecs++;
             dots(t_.as<double2>(), 0, 1, s_.as<double2>(), rows, M, 1, hv, s);
             dots(t_.as<double2>(), 0, 1, t_.as<double2>(), rows, M, 1, hv + M, s);
@@ -617,9 +757,11 @@ void BatchSolver::bicgstab(Field& F, const double2* b, double2* x, int M, const 
             MPM_LAUNCH();
             norms(r, rows, M, rnorm_.as<double>(), s);
             MPM_CUDA(cudaMemsetAsync(dflag, 0, sizeof(int), s));
-            k_bi_e<<<mb, 128, 0, s>>>(bs, rnorm_.as<double>(), bnorm_.as<double>(), opt.tol, opt.maxiter, dflag, M);
+            k_bi_e<<<mb, 128, 0, s>>>(bs, rnorm_.as<double>(), bnorm_.as<double>(), opt.tol, tolv, opt.maxiter, dflag,
+                                      M);
             MPM_LAUNCH();
-            if (read_flag(dflag, s) == 0) break;
+            if (read_flags(dflag, M, s) == 0) break;
+            act.assign(flag_ + 1, flag_ + 1 + M);
         }
     }
     std::vector<BState> h(M);
@@ -638,6 +780,7 @@ void BatchSolver::solve(Field& F, const double2* b, double2* x, int M, const dou
     st.iters.assign(M, 0);
     st.converged.assign(M, 0);
     st.matvecs = 0;
+    st.column_matvecs = 0;
     st.refine_steps = 0;
     if (!opt.refine) {
         if (opt.method == SOLVER_BICGSTAB) bicgstab(F, b, x, M, sc, opt, st, opt.recip_fp32, opt.real_fp32, s);
@@ -650,46 +793,64 @@ void BatchSolver::solve(Field& F, const double2* b, double2* x, int M, const dou
     const size_t n = size_t(rows) * M;
     xr_.ensure(sizeof(double2) * n);
     d_.ensure(sizeof(double2) * n);
-    DevBuf bn2, rn2;
-    bn2.ensure(sizeof(double) * M);
-    rn2.ensure(sizeof(double) * M);
+    bn2_.ensure(sizeof(double) * M);
+    rn2_.ensure(sizeof(double) * M);
+    convd_.ensure(sizeof(int) * M);
+    double* bn2 = bn2_.as<double>();
+    double* rn2 = rn2_.as<double>();
+    int* convd = convd_.as<int>();
     const int vb = nblk((long long)n, 256);
-    norms(b, rows, M, bn2.as<double>(), s);
+    norms(b, rows, M, bn2, s);
+    MPM_CUDA(cudaMemsetAsync(convd, 0, sizeof(int) * M, s));
     SolveOptions in = opt;
     in.refine = false;
-    in.tol = opt.inner_tol;
-    std::vector<int> conv(M, 0);
+    const double floor = opt.inner_tol > 0.0 ? opt.inner_tol : 1e-4;
+    in.tol = 0.5;
+    tolv_.ensure(sizeof(double) * M);
+    std::vector<int> conv(M, 0), act(M, 1);
+    st.rel_resid.assign(M, 0.0);
+    cur_cols_.clear();
     for (int step = 0; step < opt.max_refine; ++step) {
-        F.apply(x, xr_.as<double2>(), M, sc, false, false, false, s);
+        // fp64 true residual of the columns not yet converged (a converged
+        // column's x no longer changes)
+        st.column_matvecs += apply_cols(F, x, xr_.as<double2>(), M, sc, false, false, false,
+                                        step == 0 ? nullptr : act.data(), opt.compact, s);
         st.matvecs++;
         k_sub<<<vb, 256, 0, s>>>(b, xr_.as<double2>(), xr_.as<double2>(), n);
         MPM_LAUNCH();
-        norms(xr_.as<double2>(), rows, M, rn2.as<double>(), s);
+        norms(xr_.as<double2>(), rows, M, rn2, s);
+        k_conv_update<<<nblk(M, 128), 128, 0, s>>>(rn2, bn2, opt.tol, convd, M);
+        MPM_LAUNCH();
         std::vector<double> hb(M), hr(M);
-        MPM_CUDA(cudaMemcpyAsync(hb.data(), bn2.p, sizeof(double) * M, cudaMemcpyDeviceToHost, s));
-        MPM_CUDA(cudaMemcpyAsync(hr.data(), rn2.p, sizeof(double) * M, cudaMemcpyDeviceToHost, s));
+        MPM_CUDA(cudaMemcpyAsync(hb.data(), bn2, sizeof(double) * M, cudaMemcpyDeviceToHost, s));
+        MPM_CUDA(cudaMemcpyAsync(hr.data(), rn2, sizeof(double) * M, cudaMemcpyDeviceToHost, s));
         MPM_CUDA(cudaStreamSynchronize(s));
         int left = 0;
-        st.rel_resid.assign(M, 0.0);
         for (int m = 0; m < M; ++m) {
+            if (!act[m]) continue;  // converged in an earlier round
             st.rel_resid[m] = hb[m] > 0 ? hr[m] / hb[m] : 0.0;
             conv[m] = hr[m] <= opt.tol * hb[m];
-            left += !conv[m];
+            act[m] = !conv[m];
+            left += act[m];
         }
         if (!left) break;
-        k_mask_cols<<<vb, 256, 0, s>>>(xr_.as<double2>(), rn2.as<double>(), bn2.as<double>(), opt.tol, n, M);
+        k_mask_conv<<<vb, 256, 0, s>>>(xr_.as<double2>(), convd, n, M);
         MPM_LAUNCH();
         MPM_CUDA(cudaMemsetAsync(d_.p, 0, sizeof(double2) * n, s));
+        k_inner_tol<<<nblk(M, 128), 128, 0, s>>>(rn2, bn2, opt.tol, floor, tolv_.as<double>(), M);
+        MPM_LAUNCH();
+        const double* tolv = tolv_.as<double>();
         SolveStats inner;
         inner.iters.assign(M, 0);
         if (opt.method == SOLVER_BICGSTAB)
-            bicgstab(F, xr_.as<double2>(), d_.as<double2>(), M, sc, in, inner, true, true, s);
+            bicgstab(F, xr_.as<double2>(), d_.as<double2>(), M, sc, in, inner, true, true, s, true, tolv);
         else
-            gmres(F, xr_.as<double2>(), d_.as<double2>(), M, sc, in, inner, true, true, s);
+            gmres(F, xr_.as<double2>(), d_.as<double2>(), M, sc, in, inner, true, true, s, true, tolv);
         k_axpy1<<<vb, 256, 0, s>>>(x, d_.as<double2>(), n);
         MPM_LAUNCH();
         for (int m = 0; m < M; ++m) st.iters[m] += inner.iters[m];
         st.matvecs += inner.matvecs;
+        st.column_matvecs += inner.column_matvecs;
         st.refine_steps++;
     }
     for (int m = 0; m < M; ++m) st.converged[m] = conv[m];

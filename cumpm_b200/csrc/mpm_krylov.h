@@ -31,9 +31,17 @@ struct SolveOptions {
     bool real_fp32 = false;
     // Mixed-precision refinement: inner solves with the fp32 operator, outer
     // true-residual check |b - A x| <= tol |b| with the fp64 operator.
+    // The inner solve of column m stops once its residual is below half the
+    // outer target, 0.5 tol |b_m|, or once it has reduced its own residual
+    // by inner_tol, whichever comes first (inner_tol <= 0 means 1e-4): the
+    // fp32 operator's rounding keeps one inner solve from reaching much
+    // below that, and later rounds then stop as soon as the target is met.
     bool refine = false;
     double inner_tol = 1e-4;
     int max_refine = 20;
+    // Only the columns still iterating go through the field operator
+    // (gathered into a compact batch); converged columns cost nothing.
+    bool compact = true;
 };
 
 struct SolveStats {
@@ -41,6 +49,7 @@ struct SolveStats {
     std::vector<int> converged;      // 1 if the stop rule was met
     std::vector<double> rel_resid;   // true |b - A x| / |b| (fp64 operator) when computed
     int matvecs = 0;                 // batched operator applications
+    long long column_matvecs = 0;    // columns that went through the operator
     int refine_steps = 0;
 };
 
@@ -59,19 +68,36 @@ public:
                        std::vector<double>& out, cudaStream_t s);
 
 private:
+    // x_zero: x is known to be zero on entry (skips the first matvec).
+    // tolv: optional device per-column tolerance replacing opt.tol.
     void gmres(Field& F, const double2* b, double2* x, int M, const double2* sc, const SolveOptions& opt,
-               SolveStats& st, bool recip32, bool real32, cudaStream_t s);
+               SolveStats& st, bool recip32, bool real32, cudaStream_t s, bool x_zero = false,
+               const double* tolv = nullptr);
+    // Y = op(X) for the columns whose host flag is set (all when cols_ is
+    // empty): gathers them into a compact batch when some are idle.
+    // Returns the number of columns applied.
+    int apply_cols(Field& F, const double2* X, double2* Y, int M, const double2* sc, bool jacobi, bool r32,
+                   bool re32, const int* active, bool compact, cudaStream_t s);
     void bicgstab(Field& F, const double2* b, double2* x, int M, const double2* sc, const SolveOptions& opt,
-                  SolveStats& st, bool recip32, bool real32, cudaStream_t s);
+                  SolveStats& st, bool recip32, bool real32, cudaStream_t s, bool x_zero = false,
+                  const double* tolv = nullptr);
     void dots(const double2* V, size_t vstride, int nvec, const double2* w, int rows, int M, int conj,
               double2* out, cudaStream_t s);
     void norms(const double2* w, int rows, int M, double* out, cudaStream_t s);
 
-    int read_flag(const int* dflag, cudaStream_t s);
+    // reads the count and the M per-column flags that follow it
+    int read_flags(const int* dflag, int M, cudaStream_t s);
 
     DevBuf V_, H_, g_, cs_, sn_, y_, h_, h2_, partial_, bnorm_, rnorm_, state_, w_, r_, bj_;
-    DevBuf r0_, p_, v_, s_, t_, scal_, d_, rr_, xr_, flagdev_;
-    int* flag_ = nullptr;  // pinned host word
+    DevBuf r0_, p_, v_, s_, t_, scal_, d_, rr_, xr_, flagdev_, tolv_;
+    DevBuf cidx_, xc_, yc_, scc_;        // compact-batch gather buffers
+    DevBuf bn2_, rn2_, convd_;           // refinement: |b|, true |r|, converged flags
+    int* flag_ = nullptr;                // pinned host words: count + per-column flags
+    int flag_cap_ = 0;
+    int* hidx_ = nullptr;                // pinned host column list for the gather
+    int hidx_cap_ = 0;
+    std::vector<int> cur_cols_;          // column list the device buffers hold
+    const double2* cur_sc_ = nullptr;    // self coefficients gathered into scc_
 };
 
 }  // namespace mpm

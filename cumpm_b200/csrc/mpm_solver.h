@@ -27,7 +27,7 @@ struct DriverOptions {
     int maxiter = 1000;
     bool batch_all = false;     // all frequencies x polarisations in one batch (mean-field guesses)
     bool refine = false;        // mixed precision + fp64 true-residual refinement
-    double inner_tol = 1e-4;
+    double inner_tol = 1e-4;    // floor of one inner solve's reduction (see SolveOptions)
     bool real_fp32 = false;
 };
 

@@ -163,7 +163,12 @@ class dipole_solver:
     # ---- extensions beyond the reference API --------------------------------
     def set_solver_options(self, restart=50, maxiter=1000, batch_all=False, refine=False, inner_tol=1e-4,
                            real_fp32=False):
-        """GMRES restart/maxiter, all-frequency batching, mixed-precision refinement."""
+        """GMRES restart/maxiter, all-frequency batching, mixed-precision refinement.
+
+        Each fp32 inner solve of the refinement reduces a column's residual by
+        at most inner_tol and stops earlier once that column's residual is
+        below half the outer tolerance.
+        """
         self._solver.set_solver_options(restart, maxiter, batch_all, refine, inner_tol, real_fp32)
 
     def get_iterations(self):

@@ -73,7 +73,9 @@ typedef struct mpm_solve_options {
     int recip_fp32;    /* fp32 reciprocal space */
     int real_fp32;     /* fp32 real-space pair sum */
     int refine;        /* fp64 true-residual iterative refinement around fp32 solves */
-    double inner_tol;  /* relative tolerance of each refinement's inner solve */
+    double inner_tol;  /* smallest relative reduction asked of one inner solve (0: 1e-4); a column's
+                          inner solve also stops once its residual is below 0.5 tol |b| */
+    int compact;       /* only still-iterating columns go through the operator (gathered batch) */
 } mpm_solve_options;
 
 typedef struct mpm_solve_report {
@@ -83,6 +85,7 @@ typedef struct mpm_solve_report {
     int max_iterations;
     int num_converged;
     double max_rel_resid;  /* true fp64 |b-Ax|/|b| (refinement mode), else -1 */
+    long long column_matvecs; /* right-hand-side columns that went through the operator */
 } mpm_solve_report;
 
 typedef struct mpm_field_info {
