@@ -17,7 +17,7 @@ _dp = C.POINTER(C.c_double)
 _ip = C.POINTER(C.c_int)
 
 MPM_OK, MPM_ERR_INVALID, MPM_ERR_RUNTIME, MPM_ERR_CUDA = 0, 1, 2, 3
-FIELD_DIRECT, FIELD_MONO = 0, 1
+FIELD_DIRECT, FIELD_MONO, FIELD_POLY = 0, 1, 2
 MODE_SOLVER_AX, MODE_INTERACTION = 0, 1
 METHOD_GMRES, METHOD_BICGSTAB = 0, 1
 
@@ -31,7 +31,7 @@ EXPORTS = [
     "mpm_near_set_field_points", "mpm_near_calculate",
     "mpm_field_create", "mpm_field_destroy", "mpm_field_set_positions", "mpm_field_set_field_points",
     "mpm_field_apply", "mpm_field_apply_part", "mpm_field_info_get", "mpm_batch_solve",
-    "mpm_mono_tables", "mpm_ewald_geometry",
+    "mpm_mono_tables", "mpm_ewald_geometry", "mpm_poly_geometry", "mpm_poly_pair_functions",
     "mpm_profile_enable", "mpm_profile_reset", "mpm_profile_read", "mpm_kernel_launches",
     "mpm_field_apply_noalloc", "mpm_noalloc_scratch_bytes",
 ]
@@ -77,6 +77,9 @@ def lib():
                                       C.POINTER(SolveOptions), C.POINTER(SolveReport), C.c_void_p]
         L.mpm_mono_tables.argtypes = [C.c_double, _dp, _dp, _dp]
         L.mpm_ewald_geometry.argtypes = [_dp, C.c_double, C.c_double, _ip, _ip, _dp, _dp, _dp]
+        L.mpm_poly_geometry.argtypes = [_dp, C.c_double, C.c_double, _dp, C.c_int, _ip, _ip, _dp, _dp, _ip, _ip]
+        L.mpm_poly_pair_functions.argtypes = [C.c_double, C.c_double, C.c_double, C.c_double, C.c_int, _dp, C.c_int,
+                                              _dp, _dp, _dp]
         L.mpm_profile_read.argtypes = [_dp, C.POINTER(C.c_longlong), C.c_int]
         L.mpm_field_apply_noalloc.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_int,
                                               C.c_int, C.c_int, C.c_void_p]
@@ -107,6 +110,31 @@ def mono_tables(xi):
     out = out.reshape(10, 9001)
     names = ["fd1", "fd2", "fq1", "fq2", "fq3", "gq1", "gq2", "gq3", "gq4"]
     return out[0], {n: out[i + 1] for i, n in enumerate(names)}, so.value, sg.value
+
+
+def poly_geometry(box, errortol, xi, radii):
+    """Polydisperse grid, support, eta, cutoff and radius classes."""
+    b, bp = _arr(box)
+    rr, rp = _arr(radii)
+    grid = (C.c_int * 3)()
+    P, nc = C.c_int(), C.c_int()
+    eta, rc = C.c_double(), C.c_double()
+    cls = np.zeros(len(rr), dtype=np.int32)
+    check(lib().mpm_poly_geometry(bp, float(errortol), float(xi), rp, len(rr), grid, C.byref(P), C.byref(eta),
+                                  C.byref(rc), C.byref(nc), cls.ctypes.data_as(C.POINTER(C.c_int))))
+    return dict(grid=list(grid), P=P.value, eta=eta.value, rc=rc.value, n_classes=nc.value, cls=cls)
+
+
+def poly_pair_functions(a, b, xi, r, rc=None, lookup=False):
+    """(fd1, fd2, self) of the polydisperse pair functions at distances r
+    (the table lookup at r when lookup=True, for a cutoff rc)."""
+    rr, rp = _arr(np.atleast_1d(r))
+    f1 = np.zeros(len(rr))
+    f2 = np.zeros(len(rr))
+    sv = C.c_double()
+    check(lib().mpm_poly_pair_functions(float(a), float(b), float(xi), float(rc or 0.0), int(lookup), rp, len(rr),
+                                        f1.ctypes.data_as(_dp), f2.ctypes.data_as(_dp), C.byref(sv)))
+    return f1, f2, sv.value
 
 
 def ewald_geometry(box, errortol, xi):

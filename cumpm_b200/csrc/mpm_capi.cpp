@@ -12,6 +12,7 @@
 #include "mpm_solver.h"
 
 #include "mpm_capi_internal.h"
+#include "mpm_poly.cuh"
 
 struct mpm_solver { mpm::DipoleSolver* impl; };
 struct mpm_near { mpm::NearField* impl; };
@@ -202,11 +203,14 @@ int mpm_field_create(mpm_field** out, int kind, int mode, const double box[3], d
     return guard([&] {
         need(out, "out");
         mpm::FieldSpec fs;
-        if (kind != MPM_FIELD_DIRECT && kind != MPM_FIELD_MONO) throw std::invalid_argument("unknown field kind");
-        fs.kind = kind == MPM_FIELD_DIRECT ? mpm::FIELD_DIRECT : mpm::FIELD_MONO;
+        if (kind != MPM_FIELD_DIRECT && kind != MPM_FIELD_MONO && kind != MPM_FIELD_POLY)
+            throw std::invalid_argument("unknown field kind");
+        fs.kind = kind == MPM_FIELD_DIRECT ? mpm::FIELD_DIRECT : kind == MPM_FIELD_POLY ? mpm::FIELD_POLY : mpm::FIELD_MONO;
+        if (fs.kind == mpm::FIELD_POLY && (!radius || n_radius < 1))
+            throw std::invalid_argument("polydisperse field needs one radius per particle");
         fs.solver_ax = mode == MPM_MODE_SOLVER_AX;
         if (box) for (int d = 0; d < 3; ++d) fs.box[d] = box[d];
-        if (fs.kind == mpm::FIELD_MONO) need(box, "box");
+        if (fs.kind != mpm::FIELD_DIRECT) need(box, "box");
         fs.errortol = errortol;
         fs.xi = xi;
         if (radius) fs.radius.assign(radius, radius + n_radius);
@@ -269,7 +273,8 @@ int mpm_field_info_get(const mpm_field* f, mpm_field_info* info) {
         const auto st = F.stats();
         const auto& g = F.geom();
         std::memset(info, 0, sizeof(*info));
-        info->kind = F.spec().kind == mpm::FIELD_DIRECT ? MPM_FIELD_DIRECT : MPM_FIELD_MONO;
+        info->kind = F.spec().kind == mpm::FIELD_DIRECT ? MPM_FIELD_DIRECT
+                     : F.spec().kind == mpm::FIELD_POLY ? MPM_FIELD_POLY : MPM_FIELD_MONO;
         info->mode = F.spec().solver_ax ? MPM_MODE_SOLVER_AX : MPM_MODE_INTERACTION;
         info->num_particles = F.num_particles();
         info->num_targets = F.num_targets();
@@ -279,7 +284,9 @@ int mpm_field_info_get(const mpm_field* f, mpm_field_info* info) {
             info->h[d] = g.h[d];
             info->eta[d] = g.eta[d];
         }
-        info->stencil = 2 * g.off + 1;
+        info->stencil = F.spec().kind == mpm::FIELD_POLY ? F.poly_geom().P : 2 * g.off + 1;
+        if (F.spec().kind == mpm::FIELD_POLY)
+            for (int d = 0; d < 3; ++d) info->eta[d] = F.poly_geom().eta;
         info->pruned = st.pruned;
         info->z_slots = st.z_slots;
         info->num_pairs = st.num_pairs;
@@ -352,6 +359,43 @@ int mpm_ewald_geometry(const double box[3], double errortol, double xi, int grid
         }
         if (stencil) *stencil = 2 * g.off + 1;
         if (rc) *rc = g.rc;
+    });
+}
+
+int mpm_poly_geometry(const double box[3], double errortol, double xi, const double* radii, int n, int grid[3],
+                      int* P, double* eta, double* rc, int* n_classes, int* cls) {
+    return guard([&] {
+        need(box, "box");
+        need(radii, "radii");
+        if (n < 1) throw std::invalid_argument("need at least one radius");
+        if (!(errortol > 0 && errortol < 1) || !(xi > 0)) throw std::invalid_argument("invalid Ewald parameters");
+        const auto g = mpm::make_poly_geom(box, errortol, xi, std::vector<double>(radii, radii + n));
+        for (int d = 0; d < 3; ++d)
+            if (grid) grid[d] = g.ng[d];
+        if (P) *P = g.P;
+        if (eta) *eta = g.eta;
+        if (rc) *rc = g.rc;
+        if (n_classes) *n_classes = int(g.unique.size());
+        if (cls) std::copy(g.cls.begin(), g.cls.end(), cls);
+    });
+}
+
+int mpm_poly_pair_functions(double a, double b, double xi, double rc, int lookup, const double* r, int n, double* fd1,
+                            double* fd2, double* self_value) {
+    return guard([&] {
+        if (!(a > 0 && b >= a) || !(xi > 0)) throw std::invalid_argument("need 0 < a <= b and xi > 0");
+        if (n > 0) {
+            need(r, "r");
+            need(fd1, "fd1");
+            need(fd2, "fd2");
+        }
+        const double rc_val = rc < 1.001 ? 1.001 : rc;
+        const int table_n = static_cast<int>(std::ceil((rc_val - 1.0) / 0.001)) + 1;
+        for (int k = 0; k < n; ++k) {
+            if (lookup) mpm::poly::table_lookup(r[k], a, b, xi, table_n, fd1[k], fd2[k]);
+            else mpm::poly::pair_functions(r[k], a, b, xi, fd1[k], fd2[k]);
+        }
+        if (self_value) *self_value = mpm::poly::self_value(a, b, xi);
     });
 }
 

@@ -21,6 +21,7 @@
 //    built on the device from a cell list (no atomics); the self term, the
 //    Jacobi scaling and the INTERACTION_FIELD sign are fused into it.
 #include "mpm_field.h"
+#include "mpm_bins.cuh"
 #include "mpm_profile.h"
 
 #include <cub/cub.cuh>
@@ -93,44 +94,6 @@ __global__ void k_stencil(const double* __restrict__ xyz, int n, StencilArgs a, 
     }
     const int slot = a.pruned ? pmod(gw[2] - a.z0, a.N[2]) : gw[2];
     base[i] = make_int4(gw[0], gw[1], slot, gw[2]);
-}
-
-__global__ void k_bin_keys(const int4* __restrict__ base, int n, int tx, int ty, int tz, int nbx, int nby,
-                           int* __restrict__ key, int* __restrict__ idx) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const int4 b = base[i];
-    key[i] = (b.z / tz * nby + b.y / ty) * nbx + b.x / tx;
-    idx[i] = i;
-}
-
-__global__ void k_fill_int(int* p, int n, int v) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) p[i] = v;
-}
-
-__global__ void k_bin_bounds(const int* __restrict__ skey, int n, int* __restrict__ start, int* __restrict__ end) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    const int k = skey[i];
-    if (i == 0 || skey[i - 1] != k) start[k] = i;
-    if (i == n - 1 || skey[i + 1] != k) end[k] = i + 1;
-}
-
-// Distinct bins whose index range can reach [lo, hi] (inclusive, possibly
-// outside [0, n) and then wrapped when periodic).
-__device__ int reach_bins(int lo, int hi, int n, int t, bool periodic, int* out) {
-    int cnt = 0;
-    for (int v = lo; v <= hi; ++v) {
-        int w = v;
-        if (periodic) w = pmod(v, n);
-        else if (v < 0 || v >= n) continue;
-        const int b = w / t;
-        bool seen = false;
-        for (int k = 0; k < cnt; ++k) seen |= (out[k] == b);
-        if (!seen && cnt < 8) out[cnt++] = b;
-    }
-    return cnt;
 }
 
 // Gather spread: every voxel of this CTA's tile is written once with the sum
@@ -625,6 +588,7 @@ struct RealArgs {
     int M, N, Nt, Nq;
     double selfo, self_grad;
     int solver_ax, jacobi, add_recip, quads;
+    int pairs_plus;   // pairs enter with +1 in INTERACTION_FIELD too (polydisperse, :780-826)
 };
 
 template <typename R>
@@ -632,14 +596,15 @@ __global__ void __launch_bounds__(128) k_real(const double2* __restrict__ X, dou
                                               const int* __restrict__ off, const int* __restrict__ src,
                                               const R* __restrict__ T, const double* __restrict__ Qt,
                                               const int* __restrict__ quad_map,
-                                              const double2* __restrict__ sc) {
+                                              const double2* __restrict__ sc, const double* __restrict__ selfv) {
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     if (warp >= a.Nt) return;
     const int j = warp;
     const int p0 = off[j], p1 = off[j + 1];
     const int M = a.M;
-    const double sign = a.solver_ax ? 1.0 : -1.0;
+    const double sign = (a.solver_ax || a.pairs_plus) ? 1.0 : -1.0;
+    const double selfc = selfv ? selfv[j] : a.selfo;  // polydisperse: self value of the particle's radius class
     const int qt = (a.quads && quad_map && j < a.N) ? quad_map[j] : -1;
     for (int m = lane; m < M; m += 32) {
         cplx<R> e0 = mk<R>(0, 0), e1 = e0, e2 = e0;
@@ -716,7 +681,7 @@ __global__ void __launch_bounds__(128) k_real(const double2* __restrict__ X, dou
             }
             if (a.solver_ax) {
                 const double2 pj = X[o];
-                v += make_double2(s.x + a.selfo, s.y) * pj;
+                v += make_double2(s.x + selfc, s.y) * pj;
             }
             if (a.jacobi) v = v * inv;
             Y[o] = v;
@@ -887,6 +852,8 @@ Field::Field(const FieldSpec& spec) : spec_(spec) {
         for (int f = 0; f < T_COUNT; ++f)
             MPM_CUDA(cudaMemcpy(tab_f_.as<double>() + size_t(f) * kTableSize, tables_.f[f].data(),
                                 sizeof(double) * kTableSize, cudaMemcpyHostToDevice));
+    } else if (spec_.kind == FIELD_POLY) {
+        poly_init();
     } else if (spec_.kind != FIELD_DIRECT) {
         throw std::runtime_error("unsupported field kind");
     }
@@ -931,6 +898,8 @@ void Field::set_positions(const double* x, const double* y, const double* z, int
             quad_idx_.ensure(sizeof(int) * Nq_);
             MPM_CUDA(cudaMemcpy(quad_idx_.p, qidx.data(), sizeof(int) * Nq_, cudaMemcpyHostToDevice));
         }
+        if (spec_.kind == FIELD_POLY && int(spec_.radius.size()) != N_)
+            throw std::invalid_argument("Polydisperse field: radius size must match num_particles.");
         if (spec_.kind == FIELD_DIRECT) {
             std::vector<double> rad = spec_.radius;
             if (rad.empty()) rad.assign(N_, 0.0);
@@ -1116,11 +1085,12 @@ void Field::build_pairs(cudaStream_t s) {
     pair_T64_.ensure(sizeof(double) * 8 * np);
     pair_T32_.ensure(sizeof(float) * 8 * np);
     if (Nq_) pair_Q_.ensure(sizeof(double) * 8 * np);
-    if (num_pairs_ > 0)
+    if (num_pairs_ > 0 && spec_.kind == FIELD_MONO) {  // polydisperse: poly_pair_coefs
         k_pair_coefs<<<nblk(num_pairs_, 256), 256, 0, s>>>(geo.as<double>(), num_pairs_, tab_r_.as<double>(),
                                                             tab_f_.as<double>(), Nq_ > 0, pair_T64_.as<double>(),
                                                             pair_T32_.as<float>(), pair_Q_.as<double>());
         MPM_LAUNCH();
+    }
 }
 
 void Field::build_scale(cudaStream_t s) {
@@ -1176,16 +1146,16 @@ void Field::precalc(cudaStream_t s) {
         } else if (scale_built_ != (Nq_ ? 4 : 1)) {
             build_scale(s);
         }
+    } else if (spec_.kind == FIELD_POLY) {
+        poly_precalc(s);
     }
     precalc_dirty_ = false;
 }
 
-cufftHandle Field::plan_for(int M, bool fp32) {
-    const int C = Nq_ ? 8 : 3;
+cufftHandle Field::plan_for(int B, bool fp32) {
     for (auto& p : plans_)
-        if (p.M == M && p.fp32 == fp32 && p.pruned == gv_.pruned && p.Zs == gv_.Zs) return p.h;
+        if (p.M == B && p.fp32 == fp32 && p.pruned == gv_.pruned && p.Zs == gv_.Zs) return p.h;
     cufftHandle h;
-    const int B = C * M;
     if (cufftCreate(&h) != CUFFT_SUCCESS) throw std::runtime_error("cuFFT plan creation failed");
     cufftResult r;
     size_t ws = 0;
@@ -1201,7 +1171,7 @@ cufftHandle Field::plan_for(int M, bool fp32) {
         cufftDestroy(h);
         throw std::runtime_error("cuFFT plan creation failed with code: " + std::to_string(int(r)));
     }
-    plans_.push_back({M, fp32, gv_.pruned, gv_.Zs, h});
+    plans_.push_back({B, fp32, gv_.pruned, gv_.Zs, h});
     return h;
 }
 
@@ -1216,8 +1186,7 @@ void Field::transform(cplx<R>* grid, int B, bool inverse, cudaStream_t s) {
         fftx_.run<R>(grid, size_t(gv_.Ny) * Bi, int(Bi), Bi, gv_.Ny, inverse, s);
         return;
     }
-    const int M = B / (Nq_ ? 8 : 3);
-    cufftHandle plan = plan_for(M, sizeof(R) == 4);
+    cufftHandle plan = plan_for(B, sizeof(R) == 4);
     cufftSetStream(plan, s);
     cufftResult fr;
     const int dir = inverse ? CUFFT_INVERSE : CUFFT_FORWARD;
@@ -1228,14 +1197,18 @@ void Field::transform(cplx<R>* grid, int B, bool inverse, cudaStream_t s) {
     if (fr != CUFFT_SUCCESS) throw std::runtime_error("cuFFT execution failed with code: " + std::to_string(int(fr)));
 }
 
+template void Field::transform<float>(cplx<float>*, int, bool, cudaStream_t);
+template void Field::transform<double>(cplx<double>*, int, bool, cudaStream_t);
+
 template <typename R>
 void Field::recip(const double2* X, double2* Y, int M, cudaStream_t s) {
     grid_.ensure(grid_bytes(M, sizeof(R) == 8));
-    recip_on<R>(X, Y, M, grid_.as<cplx<R>>(), s);
+    if (spec_.kind == FIELD_POLY) poly_recip_on<R>(X, Y, M, grid_.as<cplx<R>>(), s);
+    else recip_on<R>(X, Y, M, grid_.as<cplx<R>>(), s);
 }
 
 size_t Field::grid_bytes(int M, bool fp64) const {
-    const int C = Nq_ ? 8 : 3;
+    const int C = spec_.kind == FIELD_POLY ? 1 : (Nq_ ? 8 : 3);
     return (fp64 ? sizeof(double2) : sizeof(float2)) * size_t(gv_.Nx) * gv_.Ny * gv_.Zs * size_t(C) * M;
 }
 
@@ -1317,16 +1290,19 @@ void Field::real_part(const double2* X, double2* Y, int M, const double2* sc, bo
     a.jacobi = jacobi ? 1 : 0;
     a.add_recip = add_recip ? 1 : 0;
     a.quads = Nq_ > 0 ? 1 : 0;
+    a.pairs_plus = spec_.kind == FIELD_POLY ? 1 : 0;
+    const double* selfv = spec_.kind == FIELD_POLY ? pself_.as<double>() : nullptr;
     const int warps = a.Nt;
     const int thr = 128;
     const int blocks = nblk((long long)warps * 32, thr);
     StageScope scope(ST_REAL, s);
     if (fp32)
         k_real<float><<<blocks, thr, 0, s>>>(X, Y, a, pair_off_.as<int>(), pair_src_.as<int>(), pair_T32_.as<float>(),
-                                             pair_Q_.as<double>(), quad_map_.as<int>(), sc);
+                                             pair_Q_.as<double>(), quad_map_.as<int>(), sc, selfv);
     else
         k_real<double><<<blocks, thr, 0, s>>>(X, Y, a, pair_off_.as<int>(), pair_src_.as<int>(),
-                                              pair_T64_.as<double>(), pair_Q_.as<double>(), quad_map_.as<int>(), sc);
+                                              pair_T64_.as<double>(), pair_Q_.as<double>(), quad_map_.as<int>(), sc,
+                                              selfv);
     MPM_LAUNCH();
 }
 
@@ -1370,14 +1346,19 @@ void Field::apply_scratch(const double2* X, double2* Y, int M, const double2* sc
     if (need > scratch_bytes)
         throw std::invalid_argument("reciprocal grid needs " + std::to_string(need) + " bytes of scratch, " +
                                     std::to_string(scratch_bytes) + " available");
-    if (recip_fp32) recip_on<float>(X, Y, M, static_cast<float2*>(scratch), s);
-    else recip_on<double>(X, Y, M, static_cast<double2*>(scratch), s);
+    if (spec_.kind == FIELD_POLY) {
+        if (recip_fp32) poly_recip_on<float>(X, Y, M, static_cast<float2*>(scratch), s);
+        else poly_recip_on<double>(X, Y, M, static_cast<double2*>(scratch), s);
+    } else {
+        if (recip_fp32) recip_on<float>(X, Y, M, static_cast<float2*>(scratch), s);
+        else recip_on<double>(X, Y, M, static_cast<double2*>(scratch), s);
+    }
     real_part(X, Y, M, sc, jacobi, real_fp32, true, s);
 }
 
 void Field::apply_part(const double2* X, double2* Y, int M, const double2* sc, bool recip_fp32, bool real_fp32,
                        int part, cudaStream_t s) {
-    if (spec_.kind != FIELD_MONO) throw std::runtime_error("apply_part needs an Ewald field");
+    if (spec_.kind == FIELD_DIRECT) throw std::runtime_error("apply_part needs an Ewald field");
     if (part == 0) {  // reciprocal only (no self, no sign change)
         if (recip_fp32) recip<float>(X, Y, M, s);
         else recip<double>(X, Y, M, s);

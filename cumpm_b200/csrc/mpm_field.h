@@ -1,10 +1,12 @@
 // Electric-field operator E = A(p) of the Mutual Polarization Method.
 //
 // One Field object replaces the reference's Electric_Field hierarchy
-// (electric_field/electric_field.h:13-141) for the two boundary conditions
-// the solve uses:
+// (electric_field/electric_field.h:13-141) for the field kinds the solve
+// uses:
 //   * FIELD_MONO   periodic box, monodisperse spectral Ewald
 //                  (monodisperse_ewald_electric_field.cu)
+//   * FIELD_POLY   periodic box, polydisperse spectral Ewald, dipoles
+//                  (polydisperse_ewald_electric_field.cu)
 //   * FIELD_DIRECT open boundaries, all-pairs sum (direct_electric_field.cu)
 // in either SOLVER_AX mode (the Krylov matvec: self terms, i != j) or
 // INTERACTION_FIELD mode (field at arbitrary points, used by Near_Field).
@@ -24,7 +26,7 @@
 
 namespace mpm {
 
-enum FieldKind { FIELD_DIRECT = 0, FIELD_MONO = 1 };
+enum FieldKind { FIELD_DIRECT = 0, FIELD_MONO = 1, FIELD_POLY = 2 };
 
 struct FieldSpec {
     int kind = FIELD_MONO;
@@ -32,7 +34,7 @@ struct FieldSpec {
     double box[3] = {0, 0, 0};
     double errortol = 1e-3;
     double xi = 0.5;
-    std::vector<double> radius;       // per particle (direct) or empty
+    std::vector<double> radius;       // per particle (direct, polydisperse) or empty
     bool quads = false;
     std::vector<int> quad_idxs;       // empty + quads => all particles
 };
@@ -49,6 +51,22 @@ struct EwaldGeom {
 };
 
 EwaldGeom make_ewald_geom(const double box[3], double errortol, double xi);
+
+// Polydisperse parameters (polydisperse_ewald_electric_field.cu:2039-2112)
+// and radius classes (:39-84).
+struct PolyGeom {
+    double rc = 0;
+    int ng[3] = {0, 0, 0};
+    double h[3] = {0, 0, 0};
+    int P = 0;            // support points per dimension
+    int off_min = 0;      // first offset, -floor((P-1)/2)
+    double eta = 0;
+    int table_n = 0;      // nodes of the reference's pair tables (r = 0, 1, 1.001, ...)
+    std::vector<double> unique;  // sorted radius classes
+    std::vector<int> cls;        // class of each particle
+};
+
+PolyGeom make_poly_geom(const double box[3], double errortol, double xi, const std::vector<double>& radii);
 
 // Device-side description of the stored part of the grid.
 struct GridView {
@@ -116,6 +134,7 @@ public:
     const FieldSpec& spec() const { return spec_; }
     const EwaldGeom& geom() const { return geom_; }
     FieldStats stats() const;
+    const PolyGeom& poly_geom() const { return pgeom_; }
     double selfo() const { return tables_.selfo; }
     const int* quad_map_dev() const { return quad_map_.as<int>(); }
     const int* quad_idx_dev() const { return quad_idx_.as<int>(); }
@@ -127,7 +146,7 @@ private:
     void choose_layout(cudaStream_t s);
     void build_column_kernel(cudaStream_t s);
     void build_scale(cudaStream_t s);
-    cufftHandle plan_for(int M, bool fp32);
+    cufftHandle plan_for(int B, bool fp32);  // B columns per voxel
     template <typename R> void recip(const double2* X, double2* Y, int M, cudaStream_t s);
     template <typename R> void recip_on(const double2* X, double2* Y, int M, cplx<R>* grid, cudaStream_t s);
     template <typename R> void transform(cplx<R>* grid, int B, bool inverse, cudaStream_t s);
@@ -135,6 +154,12 @@ private:
                    bool add_recip, cudaStream_t s);
     void direct(const double2* X, double2* Y, int M, const double2* self_coef, bool jacobi, bool fp32,
                 cudaStream_t s);
+    // polydisperse pieces (mpm_poly.cu)
+    void poly_init();
+    void poly_precalc(cudaStream_t s);
+    void poly_weights(PointSet& ps, const double* radius_dev, cudaStream_t s, bool bins);
+    void poly_pair_coefs(cudaStream_t s);
+    template <typename R> void poly_recip_on(const double2* X, double2* Y, int M, cplx<R>* grid, cudaStream_t s);
 
     FieldSpec spec_;
     EwaldGeom geom_;
@@ -157,10 +182,14 @@ private:
     DevBuf colK64_, colK32_;        // pruned layout: per-column Toeplitz kernels
     int colK_Z_ = -1;
     int scale_built_ = 0;
-    struct PlanKey { int M; bool fp32; int pruned; int Zs; cufftHandle h; };
+    struct PlanKey { int M; bool fp32; int pruned; int Zs; cufftHandle h; };  // M: columns per voxel
     std::vector<PlanKey> plans_;
     AxisFFT fftx_, ffty_, fftz_;    // in-house batched transforms (cuFFT only when a line is too long)
     bool own_fft_ = true;
+    // polydisperse
+    PolyGeom pgeom_;
+    DevBuf pcls_, prad_, pself_, ptrad_;  // class per particle, class radii, self value per particle, target radii
+    int pcand_cap_ = 0;                   // largest spread candidate count of a tile
 };
 
 }  // namespace mpm

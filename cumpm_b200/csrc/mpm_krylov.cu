@@ -43,12 +43,19 @@ __global__ void __launch_bounds__(256) k_dots1(const double2* __restrict__ V, si
     }
 }
 
+// one warp per output: lanes stride over the per-CTA partials, then a fixed
+// shuffle tree (deterministic order)
 __global__ void k_dots2(const double2* __restrict__ partial, int gx, int nvec, int M, double2* __restrict__ out) {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int t = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
     if (t >= nvec * M) return;
     double2 s = make_double2(0, 0);
-    for (int b = 0; b < gx; ++b) s += partial[size_t(b) * nvec * M + t];
-    out[t] = s;
+    for (int b = lane; b < gx; b += 32) s += partial[size_t(b) * nvec * M + t];
+    for (int o = 16; o > 0; o >>= 1) {
+        s.x += __shfl_xor_sync(0xffffffffu, s.x, o);
+        s.y += __shfl_xor_sync(0xffffffffu, s.y, o);
+    }
+    if (lane == 0) out[t] = s;
 }
 
 __global__ void k_sqrt_re(const double2* __restrict__ in, int M, double* __restrict__ out) {
@@ -538,7 +545,7 @@ void BatchSolver::dots(const double2* V, size_t vstride, int nvec, const double2
     dim3 grd(gx, (M + 31) / 32, (nvec + 7) / 8);
     k_dots1<<<grd, dim3(32, 8), 0, s>>>(V, vstride, nvec, w, rows, M, conj, partial_.as<double2>());
     MPM_LAUNCH();
-    k_dots2<<<nblk(nvec * M, 128), 128, 0, s>>>(partial_.as<double2>(), gx, nvec, M, out);
+    k_dots2<<<nblk((long long)nvec * M * 32, 256), 256, 0, s>>>(partial_.as<double2>(), gx, nvec, M, out);
     MPM_LAUNCH();
 }
 

@@ -1,0 +1,545 @@
+// Polydisperse spectral-Ewald dipole field (FIELD_POLY).
+//
+// Same operator as the reference's Polydisperse_Ewald_Electric_Field
+// (electric_field/polydisperse_ewald_electric_field.cu) for dipoles:
+//   spread   rho(v) = sum_i w_i(v) . p_i          (:189-263, :443-562)
+//   FFT      forward, unnormalised                 (:2553-2690)
+//   scale    rho^(k) *= exp(-(1-eta) k^2/4xi^2) / (k^2 V), 0 at k = 0 (:565-651)
+//   FFT      inverse, unnormalised
+//   contract E_j = h^3 sum_v w_j(v) phi(v)          (:265-350, :653-693)
+//   real     self (s_i + self(a_i, a_i)) p_i and pairs T(r; a_i, a_j) p_i
+//            within rc from per-radius-pair tables   (:352-441, :695-826)
+// where w_i(v) is the 3-vector smoothed-sphere weight of particle i at the
+// grid node v (radial profile times direction), P^3 nodes per particle.
+//
+// B200 layout and choices:
+//  * The grid is scalar per right-hand side: [x][y][z][M] complex, so every
+//    voxel's M columns are one coalesced vector.
+//  * Spreading is a gather over 8^3 voxel tiles from spatial bins of the
+//    stencil origins (no atomics, deterministic, every voxel written once).
+//  * Contraction is one CTA per target, its warps splitting the P^3 nodes,
+//    lanes over right-hand sides, a fixed-order reduction at the end.
+//  * The reference tabulates the pair functions on r = 0, 1, 1.001, ... for
+//    every pair of radius classes and interpolates linearly.  Here each
+//    pair's value is that same interpolation, but the two table nodes it
+//    reads are evaluated on the fly, so no table is stored: a continuous
+//    radius distribution (one class per particle) costs nothing extra.
+#include "mpm_bins.cuh"
+#include "mpm_field.h"
+#include "mpm_poly.cuh"
+#include "mpm_profile.h"
+
+#include <cub/cub.cuh>
+
+#include <algorithm>
+#include <cmath>
+#include <set>
+
+namespace mpm {
+
+// ------------------------------------------------------------ parameters
+
+PolyGeom make_poly_geom(const double box[3], double errortol, double xi, const std::vector<double>& radii) {
+    if (radii.empty()) throw std::invalid_argument("polydisperse field needs one radius per particle");
+    PolyGeom g;
+    // radius classes: a radius joins an existing class within 1e-5, classes
+    // are sorted, each particle takes the first sorted class within 1e-5
+    std::set<double> seen;
+    std::vector<double> order;
+    for (double r : radii) {
+        bool found = false;
+        for (auto it = seen.lower_bound(r - 1e-5); it != seen.end() && *it <= r + 1e-5; ++it)
+            if (std::abs(*it - r) < 1e-5) { found = true; break; }
+        if (!found) { seen.insert(r); order.push_back(r); }
+    }
+    g.unique.assign(seen.begin(), seen.end());
+    g.cls.resize(radii.size());
+    for (size_t i = 0; i < radii.size(); ++i) {
+        const double r = radii[i];
+        auto it = std::lower_bound(g.unique.begin(), g.unique.end(), r - 1e-5);
+        while (it != g.unique.end() && !(std::abs(*it - r) < 1e-5)) ++it;
+        if (it == g.unique.end()) throw std::runtime_error("radius class lookup failed");
+        g.cls[i] = int(it - g.unique.begin());
+    }
+    double rc = std::sqrt(-std::log(errortol)) / xi;
+    const double rc_min = 2.0 * g.unique.back();
+    if (rc < rc_min) rc = rc_min;
+    if (rc > box[0] / 2.0 || rc > box[1] / 2.0 || rc > box[2] / 2.0)
+        throw std::runtime_error("Real space cutoff (" + std::to_string(rc) + ") larger than half the box length.");
+    g.rc = rc;
+    const double kcut = 2.0 * xi * xi * rc;
+    for (int d = 0; d < 3; ++d) {
+        g.ng[d] = static_cast<int>(std::ceil(1.0 + box[d] * kcut / kPi));
+        g.h[d] = box[d] / g.ng[d];
+    }
+    const double mean_h = (g.h[0] + g.h[1] + g.h[2]) / 3.0;
+    g.P = static_cast<int>(std::ceil(2.0 / mean_h - 2.0 * std::log(errortol) / kPi));
+    g.eta = g.P * std::pow(mean_h * xi, 2.0) / kPi;
+    g.off_min = -static_cast<int>(std::floor((g.P - 1) / 2.0));
+    const double rc_val = rc < 1.001 ? 1.001 : rc;
+    g.table_n = static_cast<int>(std::ceil((rc_val - 1.0) / 0.001)) + 1;
+    return g;
+}
+
+// --------------------------------------------------------------- kernels
+
+namespace {
+
+inline int nblk(long long n, int b) { return int((n + b - 1) / b); }
+
+struct PolyArgs {
+    double h[3];
+    int N[3];
+    int P, off_min;
+    double eta, xi;
+};
+
+// One thread per (point, support node): the smoothed-sphere weight vector
+// (spread_precalcs_kernel_polydisperse, :189-263; the contraction weights of
+// :265-350 are the same function).  Node order o = (ox*P + oy)*P + oz.
+// base[i] = wrapped first node of the point's P^3 box (x, y, z, z).
+__global__ void k_poly_weights(const double* __restrict__ xyz, int n, const double* __restrict__ rad, PolyArgs a,
+                               int4* __restrict__ base, double* __restrict__ w64, float* __restrict__ w32) {
+    const int P3 = a.P * a.P * a.P;
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long long)n * P3) return;
+    const int i = int(t / P3), o = int(t - (long long)i * P3);
+    const int oo[3] = {o / (a.P * a.P), (o / a.P) % a.P, o % a.P};
+    double gd[3];
+    int g[3];
+    for (int d = 0; d < 3; ++d) {
+        const double p = xyz[size_t(d) * n + i];
+        g[d] = static_cast<int>(round(p / a.h[d]));
+        const double d0 = g[d] * a.h[d] - p;
+        gd[d] = d0 + double(a.off_min + oo[d]) * a.h[d];
+    }
+    if (o == 0)
+        base[i] = make_int4(pmod(g[0] + a.off_min, a.N[0]), pmod(g[1] + a.off_min, a.N[1]),
+                            pmod(g[2] + a.off_min, a.N[2]), pmod(g[2] + a.off_min, a.N[2]));
+    const double dist = sqrt(gd[0] * gd[0] + gd[1] * gd[1] + gd[2] * gd[2]);
+    const double ai = rad[i];
+    const double x2 = a.xi * a.xi;
+    double w[3];
+    if (dist >= 1e-6) {
+        const double k = 3.0 / (8.0 * sqrt(2.0) * pow(kPi, 1.5) * pow(ai, 3.0) * sqrt(a.eta) * a.xi * dist * dist);
+        const double tp = (a.eta + 4.0 * ai * x2 * dist) * exp(-2.0 * pow(dist + ai, 2) * x2 / a.eta);
+        const double tm = (a.eta - 4.0 * ai * x2 * dist) * exp(-2.0 * pow(dist - ai, 2) * x2 / a.eta);
+        const double cs = k * (tp - tm);
+        for (int d = 0; d < 3; ++d) w[d] = cs * (gd[d] / dist);
+    } else {
+        const double kn = 8.0 * sqrt(2.0) * pow(a.xi, 5.0) * exp(-2.0 * ai * x2 / a.eta) /
+                          (pow(kPi, 1.5) * pow(a.eta, 2.5));
+        for (int d = 0; d < 3; ++d) w[d] = kn * gd[d];
+    }
+    for (int d = 0; d < 3; ++d) {
+        w64[size_t(t) * 3 + d] = w[d];
+        w32[size_t(t) * 3 + d] = static_cast<float>(w[d]);
+    }
+}
+
+struct PolyTile {
+    int N[3];
+    int P;
+    int T;        // tile edge (voxels)
+    int nb[3];    // bins per dimension
+    int cap;      // candidate capacity of the shared list
+};
+
+// Candidate particles of tile (bx, by, bz): those binned (by stencil origin)
+// in the bins that can hold an origin within P-1 voxels below the tile.
+__device__ int poly_tile_bins(const PolyTile& t, int bx, int by, int bz, int (&bxs)[8], int (&bys)[8], int (&bzs)[8],
+                              int nbv[3]) {
+    nbv[0] = reach_bins(bx * t.T - t.P + 1, bx * t.T + t.T - 1, t.N[0], t.T, true, bxs);
+    nbv[1] = reach_bins(by * t.T - t.P + 1, by * t.T + t.T - 1, t.N[1], t.T, true, bys);
+    nbv[2] = reach_bins(bz * t.T - t.P + 1, bz * t.T + t.T - 1, t.N[2], t.T, true, bzs);
+    return nbv[0] * nbv[1] * nbv[2];
+}
+
+// Candidate count of every tile (sets the shared-list size).
+__global__ void k_poly_count(PolyTile t, const int* __restrict__ bin_start, const int* __restrict__ bin_end,
+                             int* __restrict__ maxc) {
+    const int tile = blockIdx.x * blockDim.x + threadIdx.x;
+    const int ntile = t.nb[0] * t.nb[1] * t.nb[2];
+    if (tile >= ntile) return;
+    const int bx = tile % t.nb[0], by = (tile / t.nb[0]) % t.nb[1], bz = tile / (t.nb[0] * t.nb[1]);
+    int xs[8], ys[8], zs[8], nbv[3];
+    poly_tile_bins(t, bx, by, bz, xs, ys, zs, nbv);
+    int c = 0;
+    for (int k = 0; k < nbv[2]; ++k)
+        for (int j = 0; j < nbv[1]; ++j)
+            for (int i = 0; i < nbv[0]; ++i) {
+                const int b = (zs[k] * t.nb[1] + ys[j]) * t.nb[0] + xs[i];
+                if (bin_start[b] >= 0) c += bin_end[b] - bin_start[b];
+            }
+    atomicMax(maxc, c);
+}
+
+// Gather spread.  CTA = one 8^3 tile x one block of up to 32*MC columns;
+// warp per voxel, lanes over columns.  grid[((x*Ny+y)*Nz+z)*M + m].
+template <typename R, int MC>
+__global__ void __launch_bounds__(256) k_poly_spread(const double2* __restrict__ X, int M, const int4* __restrict__ base,
+                                                     const R* __restrict__ w, const int* __restrict__ bin_start,
+                                                     const int* __restrict__ bin_end,
+                                                     const int* __restrict__ idx_sorted, PolyTile t,
+                                                     cplx<R>* __restrict__ grid) {
+    extern __shared__ int sh[];
+    int* cand = sh;                               // particle index
+    int4* corg = reinterpret_cast<int4*>(sh + ((t.cap + 3) & ~3));  // stencil origin
+    __shared__ int ncand;
+    const int tile = blockIdx.x;
+    const int bx = tile % t.nb[0], by = (tile / t.nb[0]) % t.nb[1], bz = tile / (t.nb[0] * t.nb[1]);
+    const int m0 = blockIdx.y * 32 * MC;
+    if (threadIdx.x == 0) {
+        int xs[8], ys[8], zs[8], nbv[3];
+        poly_tile_bins(t, bx, by, bz, xs, ys, zs, nbv);
+        int c = 0;
+        for (int k = 0; k < nbv[2]; ++k)
+            for (int j = 0; j < nbv[1]; ++j)
+                for (int i = 0; i < nbv[0]; ++i) {
+                    const int b = (zs[k] * t.nb[1] + ys[j]) * t.nb[0] + xs[i];
+                    if (bin_start[b] < 0) continue;
+                    for (int q = bin_start[b]; q < bin_end[b] && c < t.cap; ++q) cand[c++] = idx_sorted[q];
+                }
+        ncand = c;
+    }
+    __syncthreads();
+    const int nc = ncand;
+    for (int c = threadIdx.x; c < nc; c += blockDim.x) corg[c] = base[cand[c]];
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int P = t.P, P3 = P * P * P;
+    const int T = t.T;
+    for (int v = warp; v < T * T * T; v += 8) {
+        const int vx = bx * T + v / (T * T), vy = by * T + (v / T) % T, vz = bz * T + v % T;
+        if (vx >= t.N[0] || vy >= t.N[1] || vz >= t.N[2]) continue;
+        cplx<R> acc[MC];
+#pragma unroll
+        for (int q = 0; q < MC; ++q) acc[q] = mk<R>(0, 0);
+        for (int c = 0; c < nc; ++c) {
+            const int4 o = corg[c];
+            const int i = cand[c];
+            // every support node of particle i that lands on this voxel
+            // (more than one only when the grid is shorter than P)
+            for (int kx = pmod(vx - o.x, t.N[0]); kx < P; kx += t.N[0])
+                for (int ky = pmod(vy - o.y, t.N[1]); ky < P; ky += t.N[1])
+                    for (int kz = pmod(vz - o.z, t.N[2]); kz < P; kz += t.N[2]) {
+                        const R* wp = w + (size_t(i) * P3 + (kx * P + ky) * P + kz) * 3;
+                        const R w0 = wp[0], w1 = wp[1], w2 = wp[2];
+#pragma unroll
+                        for (int q = 0; q < MC; ++q) {
+                            const int m = m0 + q * 32 + lane;
+                            if (m < M) {
+                                const cplx<R> p0 = to_r<R>(X[size_t(3 * i) * M + m]);
+                                const cplx<R> p1 = to_r<R>(X[size_t(3 * i + 1) * M + m]);
+                                const cplx<R> p2 = to_r<R>(X[size_t(3 * i + 2) * M + m]);
+                                acc[q] += p0 * w0 + p1 * w1 + p2 * w2;
+                            }
+                        }
+                    }
+        }
+        const size_t vo = ((size_t(vx) * t.N[1] + vy) * t.N[2] + vz) * M;
+#pragma unroll
+        for (int q = 0; q < MC; ++q) {
+            const int m = m0 + q * 32 + lane;
+            if (m < M) grid[vo + m] = acc[q];
+        }
+    }
+}
+
+__global__ void k_poly_build_scale(int Nx, int Ny, int Nz, double Lx, double Ly, double Lz, double xi, double eta,
+                                   double* __restrict__ s64, float* __restrict__ s32) {
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long V = (long long)Nx * Ny * Nz;
+    if (t >= V) return;
+    const int ix = int(t / ((long long)Ny * Nz)), iy = int((t / Nz) % Ny), iz = int(t % Nz);
+    const double fx = ix <= (Nx - 1) / 2 ? ix : ix - Nx;
+    const double fy = iy <= (Ny - 1) / 2 ? iy : iy - Ny;
+    const double fz = iz <= (Nz - 1) / 2 ? iz : iz - Nz;
+    const double kx = fx * 2.0 * kPi / Lx, ky = fy * 2.0 * kPi / Ly, kz = fz * 2.0 * kPi / Lz;
+    const double k2 = kx * kx + ky * ky + kz * kz;
+    double v = 0.0;
+    if (!(k2 < 1e-12)) v = (exp(-(1.0 - eta) * k2 / (4.0 * xi * xi)) / k2) * (1.0 / double(V));
+    s64[t] = v;
+    s32[t] = static_cast<float>(v);
+}
+
+template <typename R>
+__global__ void k_poly_scale(cplx<R>* __restrict__ grid, const R* __restrict__ sc, long long n, int M) {
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    grid[t] = grid[t] * sc[t / M];
+}
+
+// Contraction.  CTA = one target x one block of up to 32*MC columns; its 4
+// warps take every 4th support node, lanes over columns, then a fixed-order
+// sum over the warps.  Y rows 3j+c, already scaled by h^3.
+template <typename R, int MC>
+__global__ void __launch_bounds__(128) k_poly_contract(const cplx<R>* __restrict__ grid, int M,
+                                                       const int4* __restrict__ base, const R* __restrict__ w, int P,
+                                                       int Nx, int Ny, int Nz, double factor,
+                                                       double2* __restrict__ Y) {
+    __shared__ cplx<R> red[4][3][32];
+    const int j = blockIdx.x;
+    const int m0 = blockIdx.y * 32 * MC;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int P3 = P * P * P;
+    const int4 o = base[j];
+    cplx<R> acc[3][MC];
+#pragma unroll
+    for (int q = 0; q < MC; ++q) acc[0][q] = acc[1][q] = acc[2][q] = mk<R>(0, 0);
+    for (int k = warp; k < P3; k += 4) {
+        const int kx = k / (P * P), ky = (k / P) % P, kz = k % P;
+        int x = o.x + kx, y = o.y + ky, z = o.z + kz;
+        x = x >= Nx ? x % Nx : x;
+        y = y >= Ny ? y % Ny : y;
+        z = z >= Nz ? z % Nz : z;
+        const size_t vo = ((size_t(x) * Ny + y) * Nz + z) * M;
+        const R* wp = w + (size_t(j) * P3 + k) * 3;
+        const R w0 = wp[0], w1 = wp[1], w2 = wp[2];
+#pragma unroll
+        for (int q = 0; q < MC; ++q) {
+            const int m = m0 + q * 32 + lane;
+            if (m < M) {
+                const cplx<R> g = grid[vo + m];
+                acc[0][q] += g * w0;
+                acc[1][q] += g * w1;
+                acc[2][q] += g * w2;
+            }
+        }
+    }
+#pragma unroll
+    for (int q = 0; q < MC; ++q) {
+        for (int c = 0; c < 3; ++c) red[warp][c][lane] = acc[c][q];
+        __syncthreads();
+        if (warp == 0) {
+            const int m = m0 + q * 32 + lane;
+            if (m < M) {
+                for (int c = 0; c < 3; ++c) {
+                    const cplx<R> s = red[0][c][lane] + red[1][c][lane] + red[2][c][lane] + red[3][c][lane];
+                    const double2 d = to_d(s);
+                    Y[size_t(3 * j + c) * M + m] = make_double2(d.x * factor, d.y * factor);
+                }
+            }
+        }
+        __syncthreads();
+    }
+}
+
+// Per pair: delta = r / max(d, 1e-6) and the pair-table values of the two
+// radius classes at max(d, 1e-6) (real_space_precalcs_kernel_polydisperse,
+// :352-441).  Thread per target; a target index past the particles takes
+// class 0 (:407).  Same layout as the monodisperse pair coefficients.
+__global__ void k_poly_pair_coefs(const double* __restrict__ pgeo, const int* __restrict__ off,
+                                  const int* __restrict__ src, int nt, int N, const int* __restrict__ cls,
+                                  const double* __restrict__ rad, double xi, int table_n, double* __restrict__ T64,
+                                  float* __restrict__ T32) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= nt) return;
+    const int cj = j < N ? cls[j] : 0;
+    for (int p = off[j]; p < off[j + 1]; ++p) {
+        const int ci = cls[src[p]];
+        const double a = rad[min(ci, cj)], b = rad[max(ci, cj)];
+        const double d = pgeo[4 * size_t(p) + 3];
+        const double de = d < 1e-6 ? 1e-6 : d;
+        const double dx = pgeo[4 * size_t(p)] / de, dy = pgeo[4 * size_t(p) + 1] / de, dz = pgeo[4 * size_t(p) + 2] / de;
+        double perp, para;
+        poly::table_lookup(de, a, b, xi, table_n, perp, para);
+        double* t = T64 + 8 * size_t(p);
+        t[0] = dx; t[1] = dy; t[2] = dz; t[3] = perp; t[4] = para; t[5] = t[6] = t[7] = 0.0;
+        float* f = T32 + 8 * size_t(p);
+        f[0] = float(dx); f[1] = float(dy); f[2] = float(dz); f[3] = float(perp); f[4] = float(para);
+        f[5] = f[6] = f[7] = 0.f;
+    }
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------ host
+
+void Field::poly_init() {
+    if (spec_.quads) throw std::runtime_error("polydisperse quadrupoles are not available in this build");
+    pgeom_ = make_poly_geom(spec_.box, spec_.errortol, spec_.xi, spec_.radius);
+    geom_ = EwaldGeom{};
+    geom_.rc = pgeom_.rc;
+    for (int d = 0; d < 3; ++d) {
+        geom_.ng[d] = pgeom_.ng[d];
+        geom_.h[d] = pgeom_.h[d];
+    }
+    const int n = int(spec_.radius.size());
+    const int nu = int(pgeom_.unique.size());
+    std::vector<double> selfv(n);
+    std::vector<double> cself(nu);
+    for (int k = 0; k < nu; ++k) cself[k] = poly::self_value(pgeom_.unique[k], pgeom_.unique[k], spec_.xi);
+    for (int i = 0; i < n; ++i) selfv[i] = cself[pgeom_.cls[i]];
+    pcls_.ensure(sizeof(int) * n);
+    prad_.ensure(sizeof(double) * nu);
+    pself_.ensure(sizeof(double) * n);
+    radius_.ensure(sizeof(double) * n);
+    MPM_CUDA(cudaMemcpy(pcls_.p, pgeom_.cls.data(), sizeof(int) * n, cudaMemcpyHostToDevice));
+    MPM_CUDA(cudaMemcpy(prad_.p, pgeom_.unique.data(), sizeof(double) * nu, cudaMemcpyHostToDevice));
+    MPM_CUDA(cudaMemcpy(pself_.p, selfv.data(), sizeof(double) * n, cudaMemcpyHostToDevice));
+    MPM_CUDA(cudaMemcpy(radius_.p, spec_.radius.data(), sizeof(double) * n, cudaMemcpyHostToDevice));
+    gv_.Nx = pgeom_.ng[0];
+    gv_.Ny = pgeom_.ng[1];
+    gv_.Nz = pgeom_.ng[2];
+    gv_.Zs = gv_.Nz;
+    gv_.z0 = 0;
+    gv_.pruned = 0;
+    gv_.off = 0;
+    gv_.S = pgeom_.P;
+    const size_t V = size_t(gv_.Nx) * gv_.Ny * gv_.Nz;
+    scale64_.ensure(sizeof(double) * V);
+    scale32_.ensure(sizeof(float) * V);
+    k_poly_build_scale<<<nblk((long long)V, 256), 256>>>(gv_.Nx, gv_.Ny, gv_.Nz, spec_.box[0], spec_.box[1],
+                                                         spec_.box[2], spec_.xi, pgeom_.eta, scale64_.as<double>(),
+                                                         scale32_.as<float>());
+    MPM_LAUNCH();
+    MPM_CUDA(cudaDeviceSynchronize());
+    own_fft_ = AxisFFT::fits(gv_.Nx, true) && AxisFFT::fits(gv_.Ny, true) && AxisFFT::fits(gv_.Nz, true);
+    if (own_fft_) {
+        fftx_.init(gv_.Nx);
+        ffty_.init(gv_.Ny);
+        fftz_.init(gv_.Nz);
+    }
+}
+
+void Field::poly_weights(PointSet& ps, const double* radius_dev, cudaStream_t s, bool bins) {
+    const int n = ps.n;
+    const int P3 = pgeom_.P * pgeom_.P * pgeom_.P;
+    ps.base.ensure(sizeof(int4) * n);
+    ps.w64.ensure(sizeof(double) * size_t(n) * P3 * 3);
+    ps.w32.ensure(sizeof(float) * size_t(n) * P3 * 3);
+    PolyArgs a;
+    for (int d = 0; d < 3; ++d) { a.h[d] = pgeom_.h[d]; a.N[d] = pgeom_.ng[d]; }
+    a.P = pgeom_.P;
+    a.off_min = pgeom_.off_min;
+    a.eta = pgeom_.eta;
+    a.xi = spec_.xi;
+    k_poly_weights<<<nblk((long long)n * P3, 256), 256, 0, s>>>(ps.xyz.as<double>(), n, radius_dev, a,
+                                                                 ps.base.as<int4>(), ps.w64.as<double>(),
+                                                                 ps.w32.as<float>());
+    MPM_LAUNCH();
+    if (!bins) return;
+    for (int d = 0; d < 3; ++d) {
+        ps.tile[d] = 8;
+        ps.nb[d] = (pgeom_.ng[d] + 7) / 8;
+    }
+    const int nbins = ps.nb[0] * ps.nb[1] * ps.nb[2];
+    ps.bin_key.ensure(sizeof(int) * n);
+    ps.bin_key_sorted.ensure(sizeof(int) * n);
+    ps.idx.ensure(sizeof(int) * n);
+    ps.idx_sorted.ensure(sizeof(int) * n);
+    ps.bin_start.ensure(sizeof(int) * nbins);
+    ps.bin_end.ensure(sizeof(int) * nbins);
+    k_bin_keys<<<nblk(n, 128), 128, 0, s>>>(ps.base.as<int4>(), n, 8, 8, 8, ps.nb[0], ps.nb[1],
+                                            ps.bin_key.as<int>(), ps.idx.as<int>());
+    MPM_LAUNCH();
+    size_t tmp = 0;
+    int bits = 1;
+    while ((1 << bits) < nbins) ++bits;
+    cub::DeviceRadixSort::SortPairs(nullptr, tmp, ps.bin_key.as<int>(), ps.bin_key_sorted.as<int>(),
+                                    ps.idx.as<int>(), ps.idx_sorted.as<int>(), n, 0, bits, s);
+    ps.cub_tmp.ensure(tmp + sizeof(int));
+    MPM_CUDA(cub::DeviceRadixSort::SortPairs(ps.cub_tmp.p, tmp, ps.bin_key.as<int>(), ps.bin_key_sorted.as<int>(),
+                                             ps.idx.as<int>(), ps.idx_sorted.as<int>(), n, 0, bits, s));
+    k_fill_int<<<nblk(nbins, 256), 256, 0, s>>>(ps.bin_start.as<int>(), nbins, -1);
+    MPM_LAUNCH();
+    k_fill_int<<<nblk(nbins, 256), 256, 0, s>>>(ps.bin_end.as<int>(), nbins, -1);
+    MPM_LAUNCH();
+    k_bin_bounds<<<nblk(n, 256), 256, 0, s>>>(ps.bin_key_sorted.as<int>(), n, ps.bin_start.as<int>(),
+                                              ps.bin_end.as<int>());
+    MPM_LAUNCH();
+    // size of the largest candidate list (one small read per frame)
+    PolyTile t;
+    for (int d = 0; d < 3; ++d) { t.N[d] = pgeom_.ng[d]; t.nb[d] = ps.nb[d]; }
+    t.P = pgeom_.P;
+    t.T = 8;
+    t.cap = 0;
+    DevBuf mx;
+    mx.ensure(sizeof(int));
+    MPM_CUDA(cudaMemsetAsync(mx.p, 0, sizeof(int), s));
+    k_poly_count<<<nblk(nbins, 128), 128, 0, s>>>(t, ps.bin_start.as<int>(), ps.bin_end.as<int>(), mx.as<int>());
+    MPM_LAUNCH();
+    int h = 0;
+    MPM_CUDA(cudaMemcpyAsync(&h, mx.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+    MPM_CUDA(cudaStreamSynchronize(s));
+    pcand_cap_ = std::max(1, h);
+    const size_t shm = sizeof(int) * ((pcand_cap_ + 3) & ~3) + sizeof(int4) * pcand_cap_;
+    if (shm > 200 * 1024)
+        throw std::runtime_error("polydisperse spread: " + std::to_string(h) +
+                                 " particles reach one 8^3 voxel tile, more than the shared candidate list holds");
+}
+
+void Field::poly_pair_coefs(cudaStream_t s) {
+    const int nt = spec_.solver_ax ? N_ : targets_.n;
+    if (num_pairs_ <= 0) return;
+    k_poly_pair_coefs<<<nblk(nt, 128), 128, 0, s>>>(pair_geo_.as<double>(), pair_off_.as<int>(), pair_src_.as<int>(),
+                                                    nt, N_, pcls_.as<int>(), prad_.as<double>(), spec_.xi,
+                                                    pgeom_.table_n, pair_T64_.as<double>(), pair_T32_.as<float>());
+    MPM_LAUNCH();
+}
+
+void Field::poly_precalc(cudaStream_t s) {
+    poly_weights(sources_, radius_.as<double>(), s, true);
+    if (!spec_.solver_ax) {
+        // field points past the particles take the first particle's radius (:297)
+        const int nt = targets_.n;
+        std::vector<double> tr(nt);
+        for (int j = 0; j < nt; ++j) tr[j] = spec_.radius[j < N_ ? j : 0];
+        ptrad_.ensure(sizeof(double) * std::max(1, nt));
+        MPM_CUDA(cudaMemcpyAsync(ptrad_.p, tr.data(), sizeof(double) * nt, cudaMemcpyHostToDevice, s));
+        poly_weights(targets_, ptrad_.as<double>(), s, false);
+        MPM_CUDA(cudaStreamSynchronize(s));  // tr is a host temporary
+    }
+    build_pairs(s);
+    poly_pair_coefs(s);
+}
+
+template <typename R>
+void Field::poly_recip_on(const double2* X, double2* Y, int M, cplx<R>* grid, cudaStream_t s) {
+    constexpr int MC = 8;
+    const int nmb = (M + 32 * MC - 1) / (32 * MC);
+    const PointSet& ps = sources_;
+    PolyTile t;
+    for (int d = 0; d < 3; ++d) { t.N[d] = pgeom_.ng[d]; t.nb[d] = ps.nb[d]; }
+    t.P = pgeom_.P;
+    t.T = 8;
+    t.cap = pcand_cap_;
+    const size_t shm = sizeof(int) * ((t.cap + 3) & ~3) + sizeof(int4) * t.cap;
+    MPM_CUDA(cudaFuncSetAttribute(k_poly_spread<R, MC>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(shm)));
+    const R* w1 = sizeof(R) == 4 ? reinterpret_cast<const R*>(ps.w32.p) : reinterpret_cast<const R*>(ps.w64.p);
+    const int ntile = ps.nb[0] * ps.nb[1] * ps.nb[2];
+    {
+        StageScope sc(ST_SPREAD, s);
+        k_poly_spread<R, MC><<<dim3(ntile, nmb), 256, shm, s>>>(X, M, ps.base.as<int4>(), w1, ps.bin_start.as<int>(),
+                                                               ps.bin_end.as<int>(), ps.idx_sorted.as<int>(), t, grid);
+        MPM_LAUNCH();
+    }
+    {
+        StageScope sc(ST_FFT_FWD, s);
+        transform<R>(grid, M, false, s);
+    }
+    {
+        StageScope sc(ST_KSPACE, s);
+        const long long n = (long long)gv_.Nx * gv_.Ny * gv_.Nz * M;
+        const R* scl = sizeof(R) == 4 ? reinterpret_cast<const R*>(scale32_.p) : reinterpret_cast<const R*>(scale64_.p);
+        k_poly_scale<R><<<nblk(n, 256), 256, 0, s>>>(grid, scl, n, M);
+        MPM_LAUNCH();
+    }
+    {
+        StageScope sc(ST_FFT_INV, s);
+        transform<R>(grid, M, true, s);
+    }
+    StageScope sc(ST_CONTRACT, s);
+    const PointSet& tg = spec_.solver_ax ? sources_ : targets_;
+    const R* tw = sizeof(R) == 4 ? reinterpret_cast<const R*>(tg.w32.p) : reinterpret_cast<const R*>(tg.w64.p);
+    const double factor = pgeom_.h[0] * pgeom_.h[1] * pgeom_.h[2];
+    k_poly_contract<R, MC><<<dim3(tg.n, nmb), 128, 0, s>>>(grid, M, tg.base.as<int4>(), tw, pgeom_.P, gv_.Nx, gv_.Ny,
+                                                          gv_.Nz, factor, Y);
+    MPM_LAUNCH();
+}
+
+template void Field::poly_recip_on<float>(const double2*, double2*, int, cplx<float>*, cudaStream_t);
+template void Field::poly_recip_on<double>(const double2*, double2*, int, cplx<double>*, cudaStream_t);
+
+}  // namespace mpm

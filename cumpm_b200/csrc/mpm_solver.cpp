@@ -236,8 +236,10 @@ void DipoleSolver::compute(const std::vector<double>& x, const std::vector<doubl
             else if (field_type_ == "monodisperse") poly = false;
             else if (field_type_ == "auto") poly = !all_equal(radius_);
             else throw std::runtime_error("Unknown field_type: " + field_type_);
-            if (poly) throw std::runtime_error("polydisperse spectral Ewald field is not available in this build");
-            fs.kind = FIELD_MONO;
+            if (poly && solve_quads_)
+                throw std::runtime_error("polydisperse quadrupoles are not available in this build");
+            fs.kind = poly ? FIELD_POLY : FIELD_MONO;
+            if (poly) fs.radius = radius_;
         }
         field_ = std::make_unique<Field>(fs);
     } else if (N_ != n) {
@@ -383,8 +385,8 @@ std::vector<double> NearField::calculate() {
             else if (field_type_ == "monodisperse") poly = false;
             else if (field_type_ == "auto") poly = !all_equal(radius_);
             else throw std::runtime_error("Unknown field_type: " + field_type_);
-            if (poly) throw std::runtime_error("polydisperse spectral Ewald field is not available in this build");
-            fs.kind = FIELD_MONO;
+            fs.kind = poly ? FIELD_POLY : FIELD_MONO;
+            if (poly) fs.radius = sr;
         }
         if (!stream_) MPM_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
         field_ = std::make_unique<Field>(fs);

@@ -54,6 +54,7 @@ extern "C" {
 /* field kinds and modes (reference FieldCalcMode, electric_field.h:8-11) */
 #define MPM_FIELD_DIRECT 0
 #define MPM_FIELD_MONO 1
+#define MPM_FIELD_POLY 2    /* polydisperse Ewald, dipoles (radius per particle required) */
 #define MPM_MODE_SOLVER_AX 0
 #define MPM_MODE_INTERACTION 1
 
@@ -194,6 +195,18 @@ MPM_API int mpm_mono_tables(double xi, double* out, double* selfo, double* self_
 /* Ewald parameters for a box: grid[3], stencil, rc, h[3], eta[3] */
 MPM_API int mpm_ewald_geometry(const double box[3], double errortol, double xi, int grid[3], int* stencil, double* rc,
                        double h[3], double eta[3]);
+/* Polydisperse parameters (polydisperse_ewald_electric_field.cu:39-84,
+ * 2039-2112): grid[3], support P, eta, rc, number of radius classes and the
+ * class of each of the n radii (cls may be NULL). */
+MPM_API int mpm_poly_geometry(const double box[3], double errortol, double xi, const double* radii, int n, int grid[3],
+                              int* P, double* eta, double* rc, int* n_classes, int* cls);
+/* Polydisperse real-space pair functions of radii a <= b at the n distances
+ * r > 0 (helper_compute_pair_tables, polydisperse_ewald_electric_field.cu:
+ * 1434-1627): fd1 (perpendicular), fd2 (parallel) and the r = 0 self value;
+ * and, when lookup != 0, the reference's linear table lookup at r instead
+ * (:170-187, table nodes 0, 1, 1.001, ... for cutoff rc). */
+MPM_API int mpm_poly_pair_functions(double a, double b, double xi, double rc, int lookup, const double* r, int n,
+                                    double* fd1, double* fd2, double* self_value);
 
 #ifdef __cplusplus
 }

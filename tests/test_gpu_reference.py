@@ -115,3 +115,81 @@ def test_dipole_solver_vs_reference(ref, solver_type):
     s.compute(pos)
     d = s._solver.get_dipoles(True)
     np.testing.assert_allclose(d, dr, rtol=1e-6, atol=1e-7 * np.abs(dr).max())
+
+
+def ref_poly_field(R, box, tol, xi, pos, radii, P, sc, mode, field_points=None):
+    ef = R.Polydisperse_Ewald_Electric_Field(box[0], box[1], box[2], tol, xi, mode, list(map(float, radii)), False,
+                                             [], R.PrecisionMode.DOUBLE)
+    if field_points is not None:
+        ef.updateFieldCoordinates(*[list(field_points[:, d]) for d in range(3)])
+    ef.updateParticleCoordinates(*[list(pos[:, d]) for d in range(3)])
+    ef.updateDipolesComplex(*[list(f(P[:, d])) for d in range(3) for f in (np.real, np.imag)])
+    ef.setSelfCoef(list(sc.real), list(sc.imag))
+    ef.calculate()
+    return np.ravel(np.asarray(ef.getEPointHost()))
+
+
+def nonoverlapping(rng, n, box, rmin, rmax):
+    box = np.asarray(box, dtype=float)
+    pos, rad = [], []
+    while len(pos) < n:
+        p = rng.uniform(0, 1, 3) * box
+        a = rng.uniform(rmin, rmax)
+        if all(np.linalg.norm((p - q) - box * np.round((p - q) / box)) >= a + b for q, b in zip(pos, rad)):
+            pos.append(p)
+            rad.append(a)
+    return np.array(pos), np.array(rad)
+
+
+@pytest.mark.parametrize("seed,rmax", [(11, 1.0), (12, 2.5), (13, 4.0)])
+def test_polydisperse_operator_vs_reference(ref, seed, rmax):
+    """Mixed radii (one class per particle) against the reference's own
+    polydisperse field, fp64 reciprocal space."""
+    from cumpm_b200 import capi
+    import torch
+    rng = np.random.default_rng(seed)
+    box = (32.0, 30.0, 34.0)
+    pos, rad = nonoverlapping(rng, 30, box, 1.0, rmax)
+    P, sc = rand_c(rng, 30, 3), rand_c(rng, 30)
+    E_ref = ref_poly_field(ref, box, 1e-6, 0.5, pos, rad, P, sc, ref.FieldCalcMode.SOLVER_AX)
+    F = capi.Field(capi.FIELD_POLY, box, 1e-6, 0.5, radius=rad)
+    F.set_positions(pos)
+    Y = F.apply(torch.tensor(P.reshape(-1, 1), device="cuda"),
+                self_coef=torch.tensor(sc.reshape(-1, 1), device="cuda")).cpu().numpy()[:, 0]
+    np.testing.assert_allclose(Y, E_ref, rtol=1e-9, atol=1e-10 * np.abs(E_ref).max())
+
+
+def test_polydisperse_interaction_vs_reference(ref):
+    from cumpm_b200 import capi
+    import torch
+    rng = np.random.default_rng(14)
+    box = (30.0, 30.0, 30.0)
+    pos, rad = nonoverlapping(rng, 10, box, 1.0, 2.0)
+    fp = rng.uniform(0, 30, (14, 3))
+    P = rand_c(rng, 10, 3)
+    E_ref = ref_poly_field(ref, box, 1e-6, 0.5, pos, rad, P, np.zeros(10, complex),
+                           ref.FieldCalcMode.INTERACTION_FIELD, field_points=fp)
+    F = capi.Field(capi.FIELD_POLY, box, 1e-6, 0.5, radius=rad, mode=capi.MODE_INTERACTION)
+    F.set_field_points(fp)
+    F.set_positions(pos)
+    Y = F.apply(torch.tensor(P.reshape(-1, 1), device="cuda")).cpu().numpy()[:, 0]
+    np.testing.assert_allclose(Y, E_ref, rtol=1e-9, atol=1e-10 * np.abs(E_ref).max())
+
+
+def test_polydisperse_dipole_solver_vs_reference(ref):
+    import cumpm_b200 as cuMPM
+    rng = np.random.default_rng(15)
+    box = [60.0, 60.0, 60.0]
+    pos, rad = nonoverlapping(rng, 20, box, 2.0, 5.0)
+    omega = np.linspace(0.3, 0.9, 3)
+    eps = 4.0 - 1.8 ** 2 / (omega ** 2 + 1j * omega * 0.1)
+    args = dict(radius=list(map(float, rad)), eps_m=1.77, xi=0.5, tol=1e-9, quiet=True, guess_type="derivative",
+                solver_type="gmres", field_type="polydisperse", E0=[], solve_quadrupoles=False, quad_idxs=[])
+    R = ref.Dipole_Solver(list(box), [complex(e) for e in eps], precision=ref.PrecisionMode.DOUBLE, **args)
+    R.compute(list(pos[:, 0]), list(pos[:, 1]), list(pos[:, 2]))
+    dr = np.asarray(R.get_dipoles(True))
+    s = cuMPM.dipole_solver(box, eps, radius=list(rad), eps_m=1.77, tol=1e-9, quiet=True, field_type="polydisperse",
+                            precision="double")
+    s.compute(pos)
+    d = s._solver.get_dipoles(True)
+    np.testing.assert_allclose(d, dr, rtol=1e-6, atol=1e-7 * np.abs(dr).max())
