@@ -190,6 +190,7 @@ private:
     PolyGeom pgeom_;
     DevBuf pcls_, prad_, pself_, ptrad_;  // class per particle, class radii, self value per particle, target radii
     int pcand_cap_ = 0;                   // largest spread candidate count of a tile
+    DevBuf ptoff_, ptlist_, ptmax_;       // per-tile spread candidate lists (CSR), their largest size
 };
 
 }  // namespace mpm

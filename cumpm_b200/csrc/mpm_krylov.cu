@@ -576,7 +576,8 @@ void BatchSolver::true_residual(Field& F, const double2* b, const double2* x, in
 }
 
 void BatchSolver::gmres(Field& F, const double2* b, double2* x, int M, const double2* sc, const SolveOptions& opt,
-                        SolveStats& st, bool r32, bool re32, cudaStream_t s, bool x_zero, const double* tolv) {
+                        SolveStats& st, bool r32, bool re32, cudaStream_t s, bool x_zero, const double* tolv,
+                        bool precond_rel) {
     const int rows = F.rows_in();
     const size_t n = size_t(rows) * M;
     const int restart = std::max(1, std::min(rows, opt.restart));
@@ -613,6 +614,7 @@ void BatchSolver::gmres(Field& F, const double2* b, double2* x, int M, const dou
         k_jacobi<<<vb, 256, 0, s>>>(b, bj_.as<double2>(), F.num_particles(), F.num_quads(), M, F.quad_idx_dev(), sc);
         MPM_LAUNCH();
         bj = bj_.as<double2>();
+        if (precond_rel) norms(bj, rows, M, bnorm_.as<double>(), s);
     }
     // columns cycling at the start of the current cycle (empty: all)
     std::vector<int> begin_cols;
@@ -687,7 +689,8 @@ void BatchSolver::gmres(Field& F, const double2* b, double2* x, int M, const dou
 }
 
 void BatchSolver::bicgstab(Field& F, const double2* b, double2* x, int M, const double2* sc, const SolveOptions& opt,
-                           SolveStats& st, bool r32, bool re32, cudaStream_t s, bool x_zero, const double* tolv) {
+                           SolveStats& st, bool r32, bool re32, cudaStream_t s, bool x_zero, const double* tolv,
+                        bool precond_rel) {
     const int rows = F.rows_in();
     const size_t n = size_t(rows) * M;
     for (DevBuf* d : {&r0_, &p_, &v_, &s_, &t_, &r_, &w_, &bj_}) d->ensure(sizeof(double2) * n);
@@ -712,6 +715,7 @@ void BatchSolver::bicgstab(Field& F, const double2* b, double2* x, int M, const 
         k_jacobi<<<vb, 256, 0, s>>>(b, bj_.as<double2>(), F.num_particles(), F.num_quads(), M, F.quad_idx_dev(), sc);
         MPM_LAUNCH();
         bj = bj_.as<double2>();
+        if (precond_rel) norms(bj, rows, M, bnorm_.as<double>(), s);
     }
     double2* r = r_.as<double2>();
     if (x_zero) {
@@ -850,9 +854,9 @@ void BatchSolver::solve(Field& F, const double2* b, double2* x, int M, const dou
         SolveStats inner;
         inner.iters.assign(M, 0);
         if (opt.method == SOLVER_BICGSTAB)
-            bicgstab(F, xr_.as<double2>(), d_.as<double2>(), M, sc, in, inner, true, true, s, true, tolv);
+            bicgstab(F, xr_.as<double2>(), d_.as<double2>(), M, sc, in, inner, true, true, s, true, tolv, true);
         else
-            gmres(F, xr_.as<double2>(), d_.as<double2>(), M, sc, in, inner, true, true, s, true, tolv);
+            gmres(F, xr_.as<double2>(), d_.as<double2>(), M, sc, in, inner, true, true, s, true, tolv, true);
         k_axpy1<<<vb, 256, 0, s>>>(x, d_.as<double2>(), n);
         MPM_LAUNCH();
         for (int m = 0; m < M; ++m) st.iters[m] += inner.iters[m];

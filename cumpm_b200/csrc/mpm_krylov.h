@@ -70,9 +70,12 @@ public:
 private:
     // x_zero: x is known to be zero on entry (skips the first matvec).
     // tolv: optional device per-column tolerance replacing opt.tol.
+    // precond_rel: stop on |D^-1 r| < tol |D^-1 b| (a relative reduction of
+    // the preconditioned residual, used by the inner solves of the
+    // refinement) instead of the reference rule |D^-1 r| < tol |b|.
     void gmres(Field& F, const double2* b, double2* x, int M, const double2* sc, const SolveOptions& opt,
                SolveStats& st, bool recip32, bool real32, cudaStream_t s, bool x_zero = false,
-               const double* tolv = nullptr);
+               const double* tolv = nullptr, bool precond_rel = false);
     // Y = op(X) for the columns whose host flag is set (all when cols_ is
     // empty): gathers them into a compact batch when some are idle.
     // Returns the number of columns applied.
@@ -80,7 +83,7 @@ private:
                    bool re32, const int* active, bool compact, cudaStream_t s);
     void bicgstab(Field& F, const double2* b, double2* x, int M, const double2* sc, const SolveOptions& opt,
                   SolveStats& st, bool recip32, bool real32, cudaStream_t s, bool x_zero = false,
-                  const double* tolv = nullptr);
+                  const double* tolv = nullptr, bool precond_rel = false);
     void dots(const double2* V, size_t vstride, int nvec, const double2* w, int rows, int M, int conj,
               double2* out, cudaStream_t s);
     void norms(const double2* w, int rows, int M, double* out, cudaStream_t s);

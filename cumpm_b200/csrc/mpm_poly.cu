@@ -45,12 +45,11 @@ PolyGeom make_poly_geom(const double box[3], double errortol, double xi, const s
     // radius classes: a radius joins an existing class within 1e-5, classes
     // are sorted, each particle takes the first sorted class within 1e-5
     std::set<double> seen;
-    std::vector<double> order;
     for (double r : radii) {
         bool found = false;
         for (auto it = seen.lower_bound(r - 1e-5); it != seen.end() && *it <= r + 1e-5; ++it)
             if (std::abs(*it - r) < 1e-5) { found = true; break; }
-        if (!found) { seen.insert(r); order.push_back(r); }
+        if (!found) seen.insert(r);
     }
     g.unique.assign(seen.begin(), seen.end());
     g.cls.resize(radii.size());
@@ -155,9 +154,12 @@ __device__ int poly_tile_bins(const PolyTile& t, int bx, int by, int bz, int (&b
     return nbv[0] * nbv[1] * nbv[2];
 }
 
-// Candidate count of every tile (sets the shared-list size).
-__global__ void k_poly_count(PolyTile t, const int* __restrict__ bin_start, const int* __restrict__ bin_end,
-                             int* __restrict__ maxc) {
+// Candidate lists of the spread tiles, built once per frame: pass 0 counts
+// (and keeps the largest count), pass 1 writes each tile's list in bin
+// order at its CSR offset.
+__global__ void k_poly_cands(PolyTile t, const int* __restrict__ bin_start, const int* __restrict__ bin_end,
+                             const int* __restrict__ idx_sorted, int pass, int* __restrict__ cnt,
+                             int* __restrict__ maxc, const int* __restrict__ off, int* __restrict__ list) {
     const int tile = blockIdx.x * blockDim.x + threadIdx.x;
     const int ntile = t.nb[0] * t.nb[1] * t.nb[2];
     if (tile >= ntile) return;
@@ -165,84 +167,119 @@ __global__ void k_poly_count(PolyTile t, const int* __restrict__ bin_start, cons
     int xs[8], ys[8], zs[8], nbv[3];
     poly_tile_bins(t, bx, by, bz, xs, ys, zs, nbv);
     int c = 0;
+    int* out = pass ? list + off[tile] : nullptr;
     for (int k = 0; k < nbv[2]; ++k)
         for (int j = 0; j < nbv[1]; ++j)
             for (int i = 0; i < nbv[0]; ++i) {
                 const int b = (zs[k] * t.nb[1] + ys[j]) * t.nb[0] + xs[i];
-                if (bin_start[b] >= 0) c += bin_end[b] - bin_start[b];
+                if (bin_start[b] < 0) continue;
+                if (pass)
+                    for (int q = bin_start[b]; q < bin_end[b]; ++q) out[c++] = idx_sorted[q];
+                else
+                    c += bin_end[b] - bin_start[b];
             }
-    atomicMax(maxc, c);
+    if (!pass) {
+        cnt[tile] = c;
+        atomicMax(maxc, c);
+    }
 }
 
-// Gather spread.  CTA = one 8^3 tile x one block of up to 32*MC columns;
-// warp per voxel, lanes over columns.  grid[((x*Ny+y)*Nz+z)*M + m].
-template <typename R, int MC>
+// Spread onto one 8^3 voxel tile x CM consecutive columns per CTA.  The
+// tile's accumulators live in shared memory; the tile's candidate particles
+// are added one after another in candidate order, all threads sharing the
+// (covered voxel, column) pairs of the current particle, with a barrier
+// between particles.  So every voxel's sum has a fixed order, there are no
+// atomics, and every voxel of the grid is written exactly once.
+// grid[((x*Ny+y)*Nz+z)*M + m].
+template <typename R, int CM>
 __global__ void __launch_bounds__(256) k_poly_spread(const double2* __restrict__ X, int M, const int4* __restrict__ base,
-                                                     const R* __restrict__ w, const int* __restrict__ bin_start,
-                                                     const int* __restrict__ bin_end,
-                                                     const int* __restrict__ idx_sorted, PolyTile t,
+                                                     const R* __restrict__ w, const int* __restrict__ toff,
+                                                     const int* __restrict__ tlist, PolyTile t,
                                                      cplx<R>* __restrict__ grid) {
-    extern __shared__ int sh[];
-    int* cand = sh;                               // particle index
-    int4* corg = reinterpret_cast<int4*>(sh + ((t.cap + 3) & ~3));  // stencil origin
-    __shared__ int ncand;
+    extern __shared__ __align__(16) unsigned char shraw[];
+    cplx<R>* acc = reinterpret_cast<cplx<R>*>(shraw);              // [512][CM] tile accumulators
+    cplx<R>* pm = acc + 512 * CM;                                 // [cap][3][CM] candidate moments
+    int* runs = reinterpret_cast<int*>(pm + size_t(t.cap) * 3 * CM);  // [cap][8] covered runs
+    int* cand = runs + 8 * t.cap;                                 // [cap] particle index
     const int tile = blockIdx.x;
     const int bx = tile % t.nb[0], by = (tile / t.nb[0]) % t.nb[1], bz = tile / (t.nb[0] * t.nb[1]);
-    const int m0 = blockIdx.y * 32 * MC;
-    if (threadIdx.x == 0) {
-        int xs[8], ys[8], zs[8], nbv[3];
-        poly_tile_bins(t, bx, by, bz, xs, ys, zs, nbv);
-        int c = 0;
-        for (int k = 0; k < nbv[2]; ++k)
-            for (int j = 0; j < nbv[1]; ++j)
-                for (int i = 0; i < nbv[0]; ++i) {
-                    const int b = (zs[k] * t.nb[1] + ys[j]) * t.nb[0] + xs[i];
-                    if (bin_start[b] < 0) continue;
-                    for (int q = bin_start[b]; q < bin_end[b] && c < t.cap; ++q) cand[c++] = idx_sorted[q];
-                }
-        ncand = c;
-    }
-    __syncthreads();
-    const int nc = ncand;
-    for (int c = threadIdx.x; c < nc; c += blockDim.x) corg[c] = base[cand[c]];
-    __syncthreads();
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int t0[3] = {bx * 8, by * 8, bz * 8};
+    const int m0 = blockIdx.y * CM;
+    const int c0 = toff[tile];
+    const int nc = min(toff[tile + 1] - c0, t.cap);
     const int P = t.P, P3 = P * P * P;
-    const int T = t.T;
-    for (int v = warp; v < T * T * T; v += 8) {
-        const int vx = bx * T + v / (T * T), vy = by * T + (v / T) % T, vz = bz * T + v % T;
-        if (vx >= t.N[0] || vy >= t.N[1] || vz >= t.N[2]) continue;
-        cplx<R> acc[MC];
+    // Covered tile offsets of candidate c along each axis: the support index
+    // k = (t0 + u - origin) mod N must be < P.  Within a covered run k grows
+    // by one per voxel (P < N, so a wrap would pass N-1 >= P, which is not
+    // covered); at most two runs per axis.  Run word: u | len << 4 | k << 8.
+    for (int c = threadIdx.x; c < nc; c += blockDim.x) {
+        const int i = tlist[c0 + c];
+        cand[c] = i;
+        const int4 o = base[i];
+        const int org[3] = {o.x, o.y, o.z};
+        int nrs = 0;
 #pragma unroll
-        for (int q = 0; q < MC; ++q) acc[q] = mk<R>(0, 0);
-        for (int c = 0; c < nc; ++c) {
-            const int4 o = corg[c];
-            const int i = cand[c];
-            // every support node of particle i that lands on this voxel
-            // (more than one only when the grid is shorter than P)
-            for (int kx = pmod(vx - o.x, t.N[0]); kx < P; kx += t.N[0])
-                for (int ky = pmod(vy - o.y, t.N[1]); ky < P; ky += t.N[1])
-                    for (int kz = pmod(vz - o.z, t.N[2]); kz < P; kz += t.N[2]) {
-                        const R* wp = w + (size_t(i) * P3 + (kx * P + ky) * P + kz) * 3;
-                        const R w0 = wp[0], w1 = wp[1], w2 = wp[2];
+        for (int d = 0; d < 3; ++d) {
+            int nr = 0, open = 0, r0 = 0, r1 = 0;
+            int k = pmod(t0[d] - org[d], t.N[d]);
 #pragma unroll
-                        for (int q = 0; q < MC; ++q) {
-                            const int m = m0 + q * 32 + lane;
-                            if (m < M) {
-                                const cplx<R> p0 = to_r<R>(X[size_t(3 * i) * M + m]);
-                                const cplx<R> p1 = to_r<R>(X[size_t(3 * i + 1) * M + m]);
-                                const cplx<R> p2 = to_r<R>(X[size_t(3 * i + 2) * M + m]);
-                                acc[q] += p0 * w0 + p1 * w1 + p2 * w2;
-                            }
-                        }
+            for (int u = 0; u < 8; ++u) {
+                const int cov = (t0[d] + u < t.N[d]) && k < P;
+                if (cov && open) {
+                    if (nr == 1) r0 += 1 << 4; else r1 += 1 << 4;
+                } else if (cov && nr < 2) {
+                    const int word = u | (1 << 4) | (k << 8);
+                    if (nr == 0) r0 = word; else r1 = word;
+                    ++nr;
+                    open = 1;
+                } else {
+                    open = 0;
+                }
+                k = k + 1 == t.N[d] ? 0 : k + 1;
+            }
+            runs[c * 8 + 2 * d] = r0;
+            runs[c * 8 + 2 * d + 1] = r1;
+            nrs |= nr << (2 * d);
+        }
+        runs[c * 8 + 6] = nrs;
+    }
+    for (int k = threadIdx.x; k < nc * 3 * CM; k += blockDim.x) {
+        const int cm = k % CM, comp = (k / CM) % 3, c = k / (3 * CM);
+        const int m = m0 + cm;
+        pm[k] = m < M ? to_r<R>(X[size_t(3 * tlist[c0 + c] + comp) * M + m]) : mk<R>(0, 0);
+    }
+    for (int k = threadIdx.x; k < 512 * CM; k += blockDim.x) acc[k] = mk<R>(0, 0);
+    __syncthreads();
+    const int cm = threadIdx.x % CM;            // this thread's column
+    const int slot = threadIdx.x / CM;          // and voxel slot
+    constexpr int NSLOT = 256 / CM;
+    for (int c = 0; c < nc; ++c) {
+        const int* rr = runs + c * 8;
+        const int nrs = rr[6];
+        const cplx<R> p0 = pm[(c * 3 + 0) * CM + cm], p1 = pm[(c * 3 + 1) * CM + cm], p2 = pm[(c * 3 + 2) * CM + cm];
+        const R* wi = w + size_t(cand[c]) * P3 * 3;
+        for (int ax = 0; ax < (nrs & 3); ++ax)
+            for (int ay = 0; ay < ((nrs >> 2) & 3); ++ay)
+                for (int az = 0; az < ((nrs >> 4) & 3); ++az) {
+                    const int qx = rr[ax], qy = rr[2 + ay], qz = rr[4 + az];
+                    const int lx = (qx >> 4) & 15, ly = (qy >> 4) & 15, lz = (qz >> 4) & 15;
+                    const int nb = lx * ly * lz;
+                    for (int b = slot; b < nb; b += NSLOT) {
+                        const int iz = b % lz, iy = (b / lz) % ly, ix = b / (lz * ly);
+                        const int ux = (qx & 15) + ix, uy = (qy & 15) + iy, uz = (qz & 15) + iz;
+                        const int kx = (qx >> 8) + ix, ky = (qy >> 8) + iy, kz = (qz >> 8) + iz;
+                        const R* wp = wi + ((kx * P + ky) * P + kz) * 3;
+                        acc[((ux * 8 + uy) * 8 + uz) * CM + cm] += p0 * wp[0] + p1 * wp[1] + p2 * wp[2];
                     }
-        }
-        const size_t vo = ((size_t(vx) * t.N[1] + vy) * t.N[2] + vz) * M;
-#pragma unroll
-        for (int q = 0; q < MC; ++q) {
-            const int m = m0 + q * 32 + lane;
-            if (m < M) grid[vo + m] = acc[q];
-        }
+                }
+        __syncthreads();
+    }
+    for (int k = threadIdx.x; k < 512 * CM; k += blockDim.x) {
+        const int kc = k % CM, v = k / CM;
+        const int x = t0[0] + (v >> 6), y = t0[1] + ((v >> 3) & 7), z = t0[2] + (v & 7);
+        const int m = m0 + kc;
+        if (m < M && x < t.N[0] && y < t.N[1] && z < t.N[2])
+            grid[((size_t(x) * t.N[1] + y) * t.N[2] + z) * M + m] = acc[k];
     }
 }
 
@@ -270,15 +307,17 @@ __global__ void k_poly_scale(cplx<R>* __restrict__ grid, const R* __restrict__ s
     grid[t] = grid[t] * sc[t / M];
 }
 
-// Contraction.  CTA = one target x one block of up to 32*MC columns; its 4
-// warps take every 4th support node, lanes over columns, then a fixed-order
-// sum over the warps.  Y rows 3j+c, already scaled by h^3.
+// Contraction.  CTA = one target x one block of up to 32*MC columns; its
+// CW warps take every CW-th support node (unrolled so several grid loads are
+// in flight), lanes over columns, then a fixed-order sum over the warps.
+// Y rows 3j+c, already scaled by h^3.
 template <typename R, int MC>
-__global__ void __launch_bounds__(128) k_poly_contract(const cplx<R>* __restrict__ grid, int M,
+__global__ void __launch_bounds__(256) k_poly_contract(const cplx<R>* __restrict__ grid, int M,
                                                        const int4* __restrict__ base, const R* __restrict__ w, int P,
                                                        int Nx, int Ny, int Nz, double factor,
                                                        double2* __restrict__ Y) {
-    __shared__ cplx<R> red[4][3][32];
+    constexpr int CW = 8;
+    __shared__ cplx<R> red[CW][3][32];
     const int j = blockIdx.x;
     const int m0 = blockIdx.y * 32 * MC;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -287,7 +326,8 @@ __global__ void __launch_bounds__(128) k_poly_contract(const cplx<R>* __restrict
     cplx<R> acc[3][MC];
 #pragma unroll
     for (int q = 0; q < MC; ++q) acc[0][q] = acc[1][q] = acc[2][q] = mk<R>(0, 0);
-    for (int k = warp; k < P3; k += 4) {
+#pragma unroll 4
+    for (int k = warp; k < P3; k += CW) {
         const int kx = k / (P * P), ky = (k / P) % P, kz = k % P;
         int x = o.x + kx, y = o.y + ky, z = o.z + kz;
         x = x >= Nx ? x % Nx : x;
@@ -315,7 +355,8 @@ __global__ void __launch_bounds__(128) k_poly_contract(const cplx<R>* __restrict
             const int m = m0 + q * 32 + lane;
             if (m < M) {
                 for (int c = 0; c < 3; ++c) {
-                    const cplx<R> s = red[0][c][lane] + red[1][c][lane] + red[2][c][lane] + red[3][c][lane];
+                    cplx<R> s = red[0][c][lane];
+                    for (int q2 = 1; q2 < CW; ++q2) s += red[q2][c][lane];
                     const double2 d = to_d(s);
                     Y[size_t(3 * j + c) * M + m] = make_double2(d.x * factor, d.y * factor);
                 }
@@ -387,6 +428,8 @@ void Field::poly_init() {
     gv_.pruned = 0;
     gv_.off = 0;
     gv_.S = pgeom_.P;
+    if (gv_.Nx < 16 || gv_.Ny < 16 || gv_.Nz < 16 || pgeom_.P >= std::min(gv_.Nx, std::min(gv_.Ny, gv_.Nz)))
+        throw std::runtime_error("polydisperse grid shorter than 16 points or than the support along an axis");
     const size_t V = size_t(gv_.Nx) * gv_.Ny * gv_.Nz;
     scale64_.ensure(sizeof(double) * V);
     scale32_.ensure(sizeof(float) * V);
@@ -449,23 +492,38 @@ void Field::poly_weights(PointSet& ps, const double* radius_dev, cudaStream_t s,
     k_bin_bounds<<<nblk(n, 256), 256, 0, s>>>(ps.bin_key_sorted.as<int>(), n, ps.bin_start.as<int>(),
                                               ps.bin_end.as<int>());
     MPM_LAUNCH();
-    // size of the largest candidate list (one small read per frame)
+    // candidate list of every spread tile (CSR) and the largest one
     PolyTile t;
     for (int d = 0; d < 3; ++d) { t.N[d] = pgeom_.ng[d]; t.nb[d] = ps.nb[d]; }
     t.P = pgeom_.P;
     t.T = 8;
     t.cap = 0;
-    DevBuf mx;
-    mx.ensure(sizeof(int));
-    MPM_CUDA(cudaMemsetAsync(mx.p, 0, sizeof(int), s));
-    k_poly_count<<<nblk(nbins, 128), 128, 0, s>>>(t, ps.bin_start.as<int>(), ps.bin_end.as<int>(), mx.as<int>());
+    ptmax_.ensure(sizeof(int));
+    DevBuf& cnt = ps.bin_key;  // reuse: nbins + 1 ints needed
+    cnt.ensure(sizeof(int) * std::max(n, nbins + 1));
+    ptoff_.ensure(sizeof(int) * (nbins + 1));
+    MPM_CUDA(cudaMemsetAsync(ptmax_.p, 0, sizeof(int), s));
+    MPM_CUDA(cudaMemsetAsync(cnt.as<int>() + nbins, 0, sizeof(int), s));
+    k_poly_cands<<<nblk(nbins, 128), 128, 0, s>>>(t, ps.bin_start.as<int>(), ps.bin_end.as<int>(), nullptr, 0,
+                                                  cnt.as<int>(), ptmax_.as<int>(), nullptr, nullptr);
     MPM_LAUNCH();
-    int h = 0;
-    MPM_CUDA(cudaMemcpyAsync(&h, mx.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+    size_t need = 0;
+    cub::DeviceScan::ExclusiveSum(nullptr, need, cnt.as<int>(), ptoff_.as<int>(), nbins + 1, s);
+    ps.cub_tmp.ensure(need);
+    MPM_CUDA(cub::DeviceScan::ExclusiveSum(ps.cub_tmp.p, need, cnt.as<int>(), ptoff_.as<int>(), nbins + 1, s));
+    int hv[2] = {0, 0};
+    MPM_CUDA(cudaMemcpyAsync(&hv[0], ptmax_.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+    MPM_CUDA(cudaMemcpyAsync(&hv[1], ptoff_.as<int>() + nbins, sizeof(int), cudaMemcpyDeviceToHost, s));
     MPM_CUDA(cudaStreamSynchronize(s));
+    const int h = hv[0];
+    ptlist_.ensure(sizeof(int) * std::max(1, hv[1]));
+    k_poly_cands<<<nblk(nbins, 128), 128, 0, s>>>(t, ps.bin_start.as<int>(), ps.bin_end.as<int>(),
+                                                  ps.idx_sorted.as<int>(), 1, nullptr, nullptr, ptoff_.as<int>(),
+                                                  ptlist_.as<int>());
+    MPM_LAUNCH();
     pcand_cap_ = std::max(1, h);
-    const size_t shm = sizeof(int) * ((pcand_cap_ + 3) & ~3) + sizeof(int4) * pcand_cap_;
-    if (shm > 200 * 1024)
+    const size_t shm = 65536 + (3 * 128 + 9 * sizeof(int)) * size_t(pcand_cap_);
+    if (shm > 200 * 1024 || pgeom_.P > 255)
         throw std::runtime_error("polydisperse spread: " + std::to_string(h) +
                                  " particles reach one 8^3 voxel tile, more than the shared candidate list holds");
 }
@@ -497,22 +555,23 @@ void Field::poly_precalc(cudaStream_t s) {
 
 template <typename R>
 void Field::poly_recip_on(const double2* X, double2* Y, int M, cplx<R>* grid, cudaStream_t s) {
-    constexpr int MC = 8;
+    constexpr int MC = sizeof(R) == 4 ? 4 : 2;   // contraction column chunks of 32 per CTA
     const int nmb = (M + 32 * MC - 1) / (32 * MC);
+    constexpr int CM = sizeof(R) == 4 ? 16 : 8;   // spread columns per CTA (64 KB of accumulators)
     const PointSet& ps = sources_;
     PolyTile t;
     for (int d = 0; d < 3; ++d) { t.N[d] = pgeom_.ng[d]; t.nb[d] = ps.nb[d]; }
     t.P = pgeom_.P;
     t.T = 8;
     t.cap = pcand_cap_;
-    const size_t shm = sizeof(int) * ((t.cap + 3) & ~3) + sizeof(int4) * t.cap;
-    MPM_CUDA(cudaFuncSetAttribute(k_poly_spread<R, MC>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(shm)));
+    const size_t shm = sizeof(cplx<R>) * (512 + 3 * size_t(t.cap)) * CM + sizeof(int) * 9 * t.cap;
+    MPM_CUDA(cudaFuncSetAttribute(k_poly_spread<R, CM>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(shm)));
     const R* w1 = sizeof(R) == 4 ? reinterpret_cast<const R*>(ps.w32.p) : reinterpret_cast<const R*>(ps.w64.p);
     const int ntile = ps.nb[0] * ps.nb[1] * ps.nb[2];
     {
         StageScope sc(ST_SPREAD, s);
-        k_poly_spread<R, MC><<<dim3(ntile, nmb), 256, shm, s>>>(X, M, ps.base.as<int4>(), w1, ps.bin_start.as<int>(),
-                                                               ps.bin_end.as<int>(), ps.idx_sorted.as<int>(), t, grid);
+        k_poly_spread<R, CM><<<dim3(ntile, (M + CM - 1) / CM), 256, shm, s>>>(
+            X, M, ps.base.as<int4>(), w1, ptoff_.as<int>(), ptlist_.as<int>(), t, grid);
         MPM_LAUNCH();
     }
     {
@@ -534,7 +593,7 @@ void Field::poly_recip_on(const double2* X, double2* Y, int M, cplx<R>* grid, cu
     const PointSet& tg = spec_.solver_ax ? sources_ : targets_;
     const R* tw = sizeof(R) == 4 ? reinterpret_cast<const R*>(tg.w32.p) : reinterpret_cast<const R*>(tg.w64.p);
     const double factor = pgeom_.h[0] * pgeom_.h[1] * pgeom_.h[2];
-    k_poly_contract<R, MC><<<dim3(tg.n, nmb), 128, 0, s>>>(grid, M, tg.base.as<int4>(), tw, pgeom_.P, gv_.Nx, gv_.Ny,
+    k_poly_contract<R, MC><<<dim3(tg.n, nmb), 256, 0, s>>>(grid, M, tg.base.as<int4>(), tw, pgeom_.P, gv_.Nx, gv_.Ny,
                                                           gv_.Nz, factor, Y);
     MPM_LAUNCH();
 }
