@@ -66,6 +66,109 @@ __device__ __forceinline__ void pass_reg(const cplx<R>* __restrict__ in, cplx<R>
     }
 }
 
+// -i v (forward rotation) or +i v (inverse)
+template <typename R, bool INV>
+__device__ __forceinline__ cplx<R> rot(cplx<R> v) {
+    return INV ? mk<R>(-v.y, v.x) : mk<R>(v.y, -v.x);
+}
+
+// In-register DFT of RAD points, y_p = sum_q x_q W^(p q), W = exp(-+2 pi i/RAD),
+// written out for the radices the grid lengths use (2, 3, 4, 5, 6, 8).
+template <typename R, bool INV, int RAD>
+__device__ __forceinline__ void dft_small(cplx<R> (&x)[RAD]) {
+    if constexpr (RAD == 2) {
+        const cplx<R> a = x[0], b = x[1];
+        x[0] = a + b;
+        x[1] = a - b;
+    } else if constexpr (RAD == 3) {
+        const R h = R(0.86602540378443864676);   // sin(2 pi / 3)
+        const cplx<R> s = x[1] + x[2];
+        const cplx<R> t = x[0] - s * R(0.5);
+        const cplx<R> d = (x[1] - x[2]) * h;
+        x[0] = x[0] + s;
+        x[1] = t + rot<R, INV>(d);
+        x[2] = t - rot<R, INV>(d);
+    } else if constexpr (RAD == 4) {
+        const cplx<R> a = x[0] + x[2], b = x[0] - x[2], c = x[1] + x[3], d = rot<R, INV>(x[1] - x[3]);
+        x[0] = a + c;
+        x[2] = a - c;
+        x[1] = b + d;
+        x[3] = b - d;
+    } else if constexpr (RAD == 5) {
+        const R c1 = R(0.30901699437494742410), c2 = R(-0.80901699437494742410);
+        const R s1 = R(0.95105651629515357212), s2 = R(0.58778525229247312917);
+        const cplx<R> a1 = x[1] + x[4], b1 = x[1] - x[4], a2 = x[2] + x[3], b2 = x[2] - x[3];
+        const cplx<R> t1 = x[0] + a1 * c1 + a2 * c2, t2 = x[0] + a1 * c2 + a2 * c1;
+        const cplx<R> u1 = rot<R, INV>(b1 * s1 + b2 * s2), u2 = rot<R, INV>(b1 * s2 - b2 * s1);
+        x[0] = x[0] + a1 + a2;
+        x[1] = t1 + u1;
+        x[4] = t1 - u1;
+        x[2] = t2 + u2;
+        x[3] = t2 - u2;
+    } else if constexpr (RAD == 6) {
+        // even / odd halves as two 3-point DFTs, then W6^p between them
+        cplx<R> e[3] = {x[0], x[2], x[4]}, o[3] = {x[1], x[3], x[5]};
+        dft_small<R, INV, 3>(e);
+        dft_small<R, INV, 3>(o);
+        const R h = R(0.86602540378443864676);
+        const cplx<R> w1 = mk<R>(R(0.5), INV ? h : -h), w2 = mk<R>(R(-0.5), INV ? h : -h);
+        const cplx<R> o1 = o[1] * w1, o2 = o[2] * w2;
+        x[0] = e[0] + o[0];
+        x[3] = e[0] - o[0];
+        x[1] = e[1] + o1;
+        x[4] = e[1] - o1;
+        x[2] = e[2] + o2;
+        x[5] = e[2] - o2;
+    } else if constexpr (RAD == 8) {
+        const R q = R(0.70710678118654752440);
+        cplx<R> u[4], v[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            u[k] = x[k] + x[k + 4];
+            v[k] = x[k] - x[k + 4];
+        }
+        // v_k *= W8^k
+        v[1] = (v[1] + rot<R, INV>(v[1])) * q;
+        v[2] = rot<R, INV>(v[2]);
+        v[3] = (rot<R, INV>(v[3]) - v[3]) * q;
+        dft_small<R, INV, 4>(u);
+        dft_small<R, INV, 4>(v);
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            x[2 * k] = u[k];
+            x[2 * k + 1] = v[k];
+        }
+    }
+}
+
+// fixed small radix: twiddled inputs in registers, butterfly written out
+template <typename R, int CW, bool INV, int RAD>
+__device__ __forceinline__ void pass_fixed(const cplx<R>* __restrict__ in, cplx<R>* __restrict__ out,
+                                           const cplx<R>* __restrict__ T, const int2* __restrict__ jt, int n, int L) {
+    constexpr int ROWS = kFftThreads / CW;
+    const int c = threadIdx.x & (CW - 1);
+    const int lane = threadIdx.x / CW;
+    const int nr = n / RAD;
+    const int stepL = n / L;
+    const int Ns = L / RAD;
+    for (int j = lane; j < nr; j += ROWS) {
+        const int2 kb = jt[j];  // (k1, output base)
+        cplx<R> x[RAD];
+#pragma unroll
+        for (int q = 0; q < RAD; ++q) x[q] = in[(j + q * nr) * CW + c];
+        if (Ns > 1) {
+#pragma unroll
+            for (int q = 1; q < RAD; ++q) {
+                const cplx<R> w = T[q * kb.x * stepL];
+                x[q] = mk<R>(x[q].x * w.x - x[q].y * w.y, x[q].x * w.y + x[q].y * w.x);
+            }
+        }
+        dft_small<R, INV, RAD>(x);
+#pragma unroll
+        for (int p = 0; p < RAD; ++p) out[(kb.y + p * Ns) * CW + c] = x[p];
+    }
+}
+
 // large radices (always odd primes here): twiddle the inputs in place, then
 // stream them from shared memory.  With a_q = x_q + x_{r-q}, b_q = x_q - x_{r-q}
 // (q = 1..(r-1)/2) and W_r^(p q) = (wr, wi):
@@ -170,7 +273,13 @@ __global__ void __launch_bounds__(kFftThreads) k_fft_axis(cplx<R>* __restrict__ 
             jt[j] = make_int2(k1, (j / Ns) * L + k1);
         }
         __syncthreads();
-        if (r <= 8) pass_reg<R, CW, 8>(in, out, T, jt, n, r, L);
+        if (r == 2) pass_fixed<R, CW, INV, 2>(in, out, T, jt, n, L);
+        else if (r == 3) pass_fixed<R, CW, INV, 3>(in, out, T, jt, n, L);
+        else if (r == 4) pass_fixed<R, CW, INV, 4>(in, out, T, jt, n, L);
+        else if (r == 5) pass_fixed<R, CW, INV, 5>(in, out, T, jt, n, L);
+        else if (r == 6) pass_fixed<R, CW, INV, 6>(in, out, T, jt, n, L);
+        else if (r == 8) pass_fixed<R, CW, INV, 8>(in, out, T, jt, n, L);
+        else if (r <= 8) pass_reg<R, CW, 8>(in, out, T, jt, n, r, L);
         else if (MAXR > 8 && r <= MAXR) pass_reg<R, CW, (MAXR > 8 ? MAXR : 8)>(in, out, T, jt, n, r, L);
         else if (STREAM) pass_stream<R, CW>(in, out, T, jt, n, r, L);
         cplx<R>* tmp = in;
