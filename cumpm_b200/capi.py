@@ -33,7 +33,7 @@ EXPORTS = [
     "mpm_field_apply", "mpm_field_apply_part", "mpm_field_info_get", "mpm_batch_solve",
     "mpm_mono_tables", "mpm_ewald_geometry", "mpm_poly_geometry", "mpm_poly_pair_functions",
     "mpm_profile_enable", "mpm_profile_reset", "mpm_profile_read", "mpm_kernel_launches",
-    "mpm_field_apply_noalloc", "mpm_noalloc_scratch_bytes",
+    "mpm_field_apply_noalloc", "mpm_noalloc_scratch_bytes", "mpm_field_grad",
 ]
 
 STAGES = ["spread", "fft_fwd", "kspace", "fft_inv", "contract", "real", "direct", "krylov", "precalc"]
@@ -84,6 +84,8 @@ def lib():
         L.mpm_field_apply_noalloc.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_int,
                                               C.c_int, C.c_int, C.c_void_p]
         L.mpm_noalloc_scratch_bytes.restype = C.c_size_t
+        L.mpm_field_grad.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p,
+                                     C.c_void_p]
         L.mpm_kernel_launches.restype = C.c_longlong
         L._mpm_typed = True
     return L
@@ -234,6 +236,9 @@ class Field:
         import torch
         info = self.info()
         rows_out = 3 * info["num_targets"] + 5 * info["num_quads"]
+        if not (X.is_cuda and X.dtype == torch.complex128 and X.dim() == 2):
+            raise ValueError("X must be a 2-D complex128 CUDA tensor")
+        X = X.contiguous()
         Y = torch.zeros((rows_out, X.shape[1]), dtype=torch.complex128, device=X.device)
         sc = None if self_coef is None else self_coef.contiguous()
         check(lib().mpm_field_apply_part(self._h, C.c_void_p(X.data_ptr()), C.c_void_p(Y.data_ptr()), X.shape[1],
@@ -241,8 +246,30 @@ class Field:
                                          int(real_fp32), int(part), _stream_ptr(stream)))
         return Y
 
+    def grad(self, lam, p, stream=None):
+        """(gx [N,3], ga [N]) complex128: d/dx and d/d(radius) of sum_m lam_m^T G p_m."""
+        import torch
+        assert lam.is_cuda and p.is_cuda and lam.shape == p.shape and lam.dtype == torch.complex128
+        N = self.info()["num_particles"]
+        gx = torch.empty((N, 3), dtype=torch.complex128, device=p.device)
+        ga = torch.empty((N,), dtype=torch.complex128, device=p.device)
+        check(lib().mpm_field_grad(self._h, C.c_void_p(lam.contiguous().data_ptr()), C.c_void_p(p.contiguous().data_ptr()),
+                                   p.shape[1], C.c_void_p(gx.data_ptr()), C.c_void_p(ga.data_ptr()),
+                                   _stream_ptr(stream)))
+        return gx, ga
+
     def batch_solve(self, B, X, self_coef, tol, method=METHOD_GMRES, restart=50, maxiter=1000, jacobi=True,
                     recip_fp32=True, real_fp32=False, refine=False, inner_tol=1e-4, compact=True, stream=None):
+        import torch
+        for name, t in (("B", B), ("X", X), ("self_coef", self_coef)):
+            if not (t.is_cuda and t.dtype == torch.complex128 and t.dim() == 2):
+                raise ValueError(f"{name} must be a 2-D complex128 CUDA tensor")
+        if not X.is_contiguous():
+            raise ValueError("X is updated in place and must be contiguous")
+        if X.shape != B.shape or self_coef.shape[1] != B.shape[1]:
+            raise ValueError("B, X and self_coef must have the same number of columns")
+        B = B.contiguous()
+        self_coef = self_coef.contiguous()
         o = SolveOptions(int(method), int(restart), int(maxiter), float(tol), int(jacobi), int(recip_fp32),
                          int(real_fp32), int(refine), float(inner_tol), int(compact))
         r = SolveReport()

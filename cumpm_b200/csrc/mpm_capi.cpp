@@ -362,6 +362,19 @@ int mpm_ewald_geometry(const double box[3], double errortol, double xi, int grid
     });
 }
 
+int mpm_field_grad(mpm_field* f, const void* lam, const void* p, int M, void* gx, void* ga, void* stream) {
+    return guard([&] {
+        need(f, "field");
+        need(lam, "lam");
+        need(p, "p");
+        need(gx, "gx");
+        need(ga, "ga");
+        f->impl->grad_bilinear(static_cast<const double2*>(lam), static_cast<const double2*>(p), M,
+                               static_cast<double2*>(gx), static_cast<double2*>(ga),
+                               static_cast<cudaStream_t>(stream));
+    });
+}
+
 int mpm_poly_geometry(const double box[3], double errortol, double xi, const double* radii, int n, int grid[3],
                       int* P, double* eta, double* rc, int* n_classes, int* cls) {
     return guard([&] {

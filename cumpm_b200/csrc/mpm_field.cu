@@ -1150,6 +1150,7 @@ void Field::precalc(cudaStream_t s) {
         poly_precalc(s);
     }
     precalc_dirty_ = false;
+    ++adj_frame_;
 }
 
 cufftHandle Field::plan_for(int B, bool fp32) {

@@ -126,6 +126,12 @@ public:
     void apply_part(const double2* X, double2* Y, int M, const double2* self_coef, bool recip_fp32,
                     bool real_fp32, int part, cudaStream_t s);
 
+    // Gradients of the bilinear forms lam_m^T G p_m (G = this operator in
+    // SOLVER_AX mode, without the caller's self coefficients), summed over
+    // the M columns: gx[i][c] = sum_m d/dx_ic, ga[i] = sum_m d/da_i
+    // (complex128, device).  Polydisperse and direct fields (mpm_adjoint.cu).
+    void grad_bilinear(const double2* lam, const double2* p, int M, double2* gx, double2* ga, cudaStream_t s);
+
     int num_particles() const { return N_; }
     int num_targets() const { return spec_.solver_ax ? N_ : targets_.n; }
     int num_quads() const { return Nq_; }
@@ -159,6 +165,7 @@ private:
     void poly_precalc(cudaStream_t s);
     void poly_weights(PointSet& ps, const double* radius_dev, cudaStream_t s, bool bins);
     void poly_pair_coefs(cudaStream_t s);
+    // Y == nullptr: stop after the inverse transform (grid = potential)
     template <typename R> void poly_recip_on(const double2* X, double2* Y, int M, cplx<R>* grid, cudaStream_t s);
 
     FieldSpec spec_;
@@ -191,6 +198,10 @@ private:
     DevBuf pcls_, prad_, pself_, ptrad_;  // class per particle, class radii, self value per particle, target radii
     int pcand_cap_ = 0;                   // largest spread candidate count of a tile
     DevBuf ptoff_, ptlist_, ptmax_;       // per-tile spread candidate lists (CSR), their largest size
+    // adjoint: stacked [p | lam] columns, potential grid, per-pair table derivatives, self-value derivatives
+    DevBuf adj_x_, adj_grid_, adj_part_, pair_dT_, pself_d_;
+    long long pair_dT_for_ = -1;          // pair list the derivatives belong to
+    int adj_frame_ = 0, pair_dT_frame_ = -1;
 };
 
 }  // namespace mpm

@@ -589,6 +589,7 @@ void Field::poly_recip_on(const double2* X, double2* Y, int M, cplx<R>* grid, cu
         StageScope sc(ST_FFT_INV, s);
         transform<R>(grid, M, true, s);
     }
+    if (!Y) return;  // potential only (grid holds phi = IFFT(S FFT(rho)))
     StageScope sc(ST_CONTRACT, s);
     const PointSet& tg = spec_.solver_ax ? sources_ : targets_;
     const R* tw = sizeof(R) == 4 ? reinterpret_cast<const R*>(tg.w32.p) : reinterpret_cast<const R*>(tg.w64.p);

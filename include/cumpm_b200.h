@@ -177,6 +177,15 @@ MPM_API size_t mpm_noalloc_scratch_bytes(void);
 MPM_API int mpm_batch_solve(mpm_field* f, const void* B, void* X, int M, const void* self_coef,
                     const mpm_solve_options* opt, mpm_solve_report* report, void* stream);
 
+/* Gradient of the bilinear forms lam_m^T G p_m, summed over the M columns
+ * (G = the field operator in SOLVER_AX mode without the caller's self
+ * coefficients; polydisperse or direct field, dipoles): gx device
+ * complex128 [N][3] = d/dx, ga device complex128 [N] = d/d(radius).  The
+ * adjoint of a solve A p = b with A = G + diag(s) is complex-symmetric, so
+ * with lam solving A lam = conj(c), dIm(c^H p)/dtheta = -Im(lam^T dA/dtheta p).
+ * No counterpart in the reference (it has no gradients). */
+MPM_API int mpm_field_grad(mpm_field* f, const void* lam, const void* p, int M, void* gx, void* ga, void* stream);
+
 /* ---- measurement (no counterpart in the reference) -----------------------
  * Stage timers from CUDA events recorded on the launching stream, read
  * without adding synchronisation to the solve.  Stages: 0 spread, 1 forward
