@@ -10,7 +10,7 @@ namespace mpm {
 namespace {
 
 constexpr int kFftThreads = 256;
-constexpr size_t kFftSmemBudget = 100 * 1024;   // two CTAs per SM
+constexpr size_t kFftSmemBudget = 110 * 1024;   // two CTAs per SM (228 KB per SM)
 constexpr size_t kFftSmemMax = 220 * 1024;
 
 // Stockham autosort, mixed radix.  With Ns = product of the radices already

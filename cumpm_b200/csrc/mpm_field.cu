@@ -110,12 +110,14 @@ __global__ void __launch_bounds__(256) k_spread(const double2* __restrict__ X, i
                                                 const int4* __restrict__ base, const R* __restrict__ w1,
                                                 const int* __restrict__ bin_start, const int* __restrict__ bin_end,
                                                 const int* __restrict__ sorted_idx, GridView g, int TX, int TY,
-                                                int TZ, int nbx, int nby, int cap, int bc,
+                                                int TZ, int nbx, int nby, int nzt, int cap, int bc,
                                                 cplx<R>* __restrict__ grid) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ int bx[8], by[8], bz[8], nbxs, nbys, nbzs;
     __shared__ int rstart[512], rlen[512], rpre[513], nranges;
-    const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY, z0 = blockIdx.z * TZ;
+    // blockIdx.z = z tile + nzt * (column chunk of bc columns)
+    const int zt = blockIdx.z % nzt, chunk = blockIdx.z / nzt;
+    const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY, z0 = zt * TZ;
     const int x1 = min(x0 + TX, g.Nx), y1 = min(y0 + TY, g.Ny), z1 = min(z0 + TZ, g.Zs);
     const int B = C * M;
     if (threadIdx.x == 0) {
@@ -202,7 +204,8 @@ __global__ void __launch_bounds__(256) k_spread(const double2* __restrict__ X, i
             }
             ln[col] = n <= kSpreadListCap ? n : -1;
         }
-        for (int b0 = 0; b0 < B; b0 += bc) {
+        {
+            const int b0 = chunk * bc;
             const int nb = min(bc, B - b0);
             __syncthreads();
             for (int t = threadIdx.x; t < nc * nb; t += blockDim.x) {
@@ -384,8 +387,11 @@ __global__ void k_build_column(ScaleArgs a, int Z, double2* __restrict__ K64, fl
 }
 
 // Pruned layout: out[zo][c'][m] = sum_{zi,c} K_{c'c}(zo - zi) in[zi][c][m]
-// on one (kx, ky) column per CTA, in place.
-template <typename R>
+// on one (kx, ky) column per CTA, in place.  The column's Z x 3 inputs of a
+// right-hand side sit in registers; for each source component c the 2Z-1
+// Toeplitz coefficients K_{c'c}(.) are read once from shared memory and
+// applied to all Z outputs (ZMAX bounds Z at compile time).
+template <typename R, int ZMAX>
 __global__ void k_column(cplx<R>* __restrict__ grid, const cplx<R>* __restrict__ K, int Z, int M) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int col = blockIdx.x;
@@ -400,14 +406,26 @@ __global__ void k_column(cplx<R>* __restrict__ grid, const cplx<R>* __restrict__
     const int pairidx[3][3] = {{0, 1, 2}, {1, 3, 4}, {2, 4, 5}};
     for (int t = threadIdx.x; t < B; t += blockDim.x) {
         const int cp = t / M, m = t % M;
-        for (int zo = 0; zo < Z; ++zo) {
-            cplx<R> acc = mk<R>(0, 0);
-            for (int c = 0; c < 3; ++c) {
-                const cplx<R>* kab = kk + pairidx[cp][c] * nd + (Z - 1) + zo;
-                for (int zi = 0; zi < Z; ++zi) acc += kab[-zi] * in[zi * B + c * M + m];
+        cplx<R> acc[ZMAX];
+#pragma unroll
+        for (int zo = 0; zo < ZMAX; ++zo) acc[zo] = mk<R>(0, 0);
+        for (int c = 0; c < 3; ++c) {
+            cplx<R> x[ZMAX];
+#pragma unroll
+            for (int zi = 0; zi < ZMAX; ++zi) x[zi] = zi < Z ? in[zi * B + c * M + m] : mk<R>(0, 0);
+            const cplx<R>* kab = kk + pairidx[cp][c] * nd + (Z - 1);   // kab[d], d = zo - zi in [-(Z-1), Z-1]
+#pragma unroll
+            for (int d = -(ZMAX - 1); d <= ZMAX - 1; ++d) {
+                if (d < -(Z - 1) || d > Z - 1) continue;
+                const cplx<R> kv = kab[d];
+#pragma unroll
+                for (int zo = 0; zo < ZMAX; ++zo) {
+                    const int zi = zo - d;
+                    if (zi >= 0 && zi < ZMAX) acc[zo] += kv * x[zi];
+                }
             }
-            g[zo * B + t] = acc;
         }
+        for (int zo = 0; zo < Z; ++zo) g[zo * B + t] = acc[zo];
     }
 }
 
@@ -417,10 +435,13 @@ __global__ void k_column(cplx<R>* __restrict__ grid, const cplx<R>* __restrict__
 template <typename R>
 __global__ void k_contract(const cplx<R>* __restrict__ grid, GridView g, int M, int C, int Nt,
                            const int4* __restrict__ base, const R* __restrict__ w1, double factor,
-                           const int* __restrict__ quad_map, double2* __restrict__ Y, int negate) {
+                           const int* __restrict__ quad_map, double2* __restrict__ Y, int negate,
+                           const int* __restrict__ order) {
     __shared__ R w[3 * kMaxStencil];
     __shared__ int idx[3 * kMaxStencil];
-    const int j = blockIdx.x;
+    // targets in spatial-bin order when given: CTAs that run together share
+    // their stencils' voxels in L2
+    const int j = order ? order[blockIdx.x] : blockIdx.x;
     const int B = C * M;
     const int4 bs = base[j];
     for (int t = threadIdx.x; t < 3 * g.S; t += blockDim.x) {
@@ -1222,17 +1243,18 @@ void Field::recip_on(const double2* X, double2* Y, int M, cplx<R>* grid, cudaStr
     const PointSet& ps = sources_;
     const int TX = ps.tile[0], TY = ps.tile[1], TZ = ps.tile[2];
     const int bc = sizeof(R) == 4 ? 32 : 16;
-    const int cap = 192;
+    const int cap = 96;
     const size_t ncol = size_t(TX) * TY;
     const size_t shm = sizeof(R) * cap * (TX + TY + TZ) + sizeof(cplx<R>) * cap * bc +
                        (sizeof(R) + sizeof(int)) * ncol * kSpreadListCap + sizeof(int) * (ncol + cap);
     MPM_CUDA(cudaFuncSetAttribute(k_spread<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(shm)));
-    dim3 grd(ps.nb[0], ps.nb[1], ps.nb[2]);
+    const int nchunk = (B + bc - 1) / bc;
+    dim3 grd(ps.nb[0], ps.nb[1], ps.nb[2] * nchunk);  // one CTA per tile and column chunk
     const R* w1 = sizeof(R) == 4 ? reinterpret_cast<const R*>(ps.w32.p) : reinterpret_cast<const R*>(ps.w64.p);
     Profiler::get().begin(ST_SPREAD, s);
     k_spread<R><<<grd, 256, shm, s>>>(X, M, N_, C, quad_map_.as<int>(), ps.base.as<int4>(), w1,
                                       ps.bin_start.as<int>(), ps.bin_end.as<int>(), ps.idx_sorted.as<int>(), gv_,
-                                      TX, TY, TZ, ps.nb[0], ps.nb[1], cap, bc, grid);
+                                      TX, TY, TZ, ps.nb[0], ps.nb[1], ps.nb[2], cap, bc, grid);
     MPM_LAUNCH();
     Profiler::get().end(ST_SPREAD, s);
     // forward transform
@@ -1245,11 +1267,16 @@ void Field::recip_on(const double2* X, double2* Y, int M, cplx<R>* grid, cudaStr
         const int Z = gv_.Zs;
         const int nd = 2 * Z - 1;
         const size_t shm2 = sizeof(cplx<R>) * (size_t(Z) * B + 6 * nd);
-        MPM_CUDA(cudaFuncSetAttribute(k_column<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(shm2)));
         const int thr = std::min(1024, ((B + 31) / 32) * 32);
         const cplx<R>* K = sizeof(R) == 4 ? reinterpret_cast<const cplx<R>*>(colK32_.p)
                                           : reinterpret_cast<const cplx<R>*>(colK64_.p);
-        k_column<R><<<gv_.Nx * gv_.Ny, thr, shm2, s>>>(grid, K, Z, M);
+        auto go = [&](auto kern) {
+            MPM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(shm2)));
+            kern<<<gv_.Nx * gv_.Ny, thr, shm2, s>>>(grid, K, Z, M);
+        };
+        if (Z <= 9) go(k_column<R, 9>);
+        else if (Z <= 16) go(k_column<R, 16>);
+        else go(k_column<R, 24>);
         MPM_LAUNCH();
     } else {
         const size_t V = size_t(gv_.Nx) * gv_.Ny * gv_.Zs;
@@ -1274,7 +1301,8 @@ void Field::recip_on(const double2* X, double2* Y, int M, cplx<R>* grid, cudaStr
     const R* tw = sizeof(R) == 4 ? reinterpret_cast<const R*>(tg.w32.p) : reinterpret_cast<const R*>(tg.w64.p);
     const int thr = std::min(256, ((B + 31) / 32) * 32);
     k_contract<R><<<nt, thr, 0, s>>>(grid, gv_, M, C, nt, tg.base.as<int4>(), tw, factor,
-                                     spec_.solver_ax ? quad_map_.as<int>() : nullptr, Y, 0);
+                                     spec_.solver_ax ? quad_map_.as<int>() : nullptr, Y, 0,
+                                     spec_.solver_ax ? sources_.idx_sorted.as<int>() : nullptr);
     MPM_LAUNCH();
 }
 
