@@ -174,11 +174,13 @@ __device__ __forceinline__ void pass_fixed(const cplx<R>* __restrict__ in, cplx<
 // (q = 1..(r-1)/2) and W_r^(p q) = (wr, wi):
 //   y_p     = x_0 + sum_q (a.x wr - wi b.y, a.y wr + wi b.x)
 //   y_{r-p} = x_0 + sum_q (a.x wr + wi b.y, a.y wr - wi b.x)
-// i.e. r-1 FMAs per output; each thread accumulates PC output pairs.
-template <typename R, int CW>
+// i.e. r-1 FMAs per output; each thread accumulates PC output pairs.  The
+// W_r^(p q) of a thread's PC outputs are PC consecutive entries of row q of
+// the precomputed table `pt` (ld per row), staged in shared memory.
+template <typename R, bool INV, int CW>
 __device__ __forceinline__ void pass_stream(cplx<R>* __restrict__ in, cplx<R>* __restrict__ out,
                                             const cplx<R>* __restrict__ T, const int2* __restrict__ jt, int n, int r,
-                                            int L) {
+                                            int L, const cplx<R>* __restrict__ pt, int ld) {
     constexpr int ROWS = kFftThreads / CW;
     constexpr int PC = 8;
     const int c = threadIdx.x & (CW - 1);
@@ -205,25 +207,49 @@ __device__ __forceinline__ void pass_stream(cplx<R>* __restrict__ in, cplx<R>* _
         const int p0 = 1 + oc * PC;
         const cplx<R> x0 = in[j * CW + c];
         R px[PC], py[PC], qx[PC], qy[PC];
+#pragma unroll
+        for (int k = 0; k < PC; ++k) px[k] = py[k] = qx[k] = qy[k] = R(0);
+        R sx = R(0), sy = R(0);
+        const cplx<R>* prow = pt ? pt + (p0 - 1) : nullptr;
         int ep[PC];
 #pragma unroll
-        for (int k = 0; k < PC; ++k) { px[k] = py[k] = qx[k] = qy[k] = R(0); ep[k] = 0; }
-        R sx = R(0), sy = R(0);
+        for (int k = 0; k < PC; ++k) ep[k] = 0;
         for (int q = 1; q <= half; ++q) {
             const cplx<R> xa = in[(j + q * nr) * CW + c];
             const cplx<R> xb = in[(j + (r - q) * nr) * CW + c];
             const R ax = xa.x + xb.x, ay = xa.y + xb.y, bx = xa.x - xb.x, by = xa.y - xb.y;
             sx += ax;
             sy += ay;
+            cplx<R> wk[PC];
+            if (!prow) {
+                // W_r^(p q) from the line's twiddles, p q reduced mod r incrementally
+#pragma unroll
+                for (int k = 0; k < PC; ++k) {
+                    ep[k] += p0 + k;
+                    if (ep[k] >= r) ep[k] -= r;
+                    const cplx<R> w = T[ep[k] * stepR];
+                    wk[k] = mk<R>(w.x, INV ? -w.y : w.y);   // T is already conjugated for INV
+                }
+            } else if constexpr (sizeof(R) == 4) {
+                const float4* p4 = reinterpret_cast<const float4*>(prow);
+#pragma unroll
+                for (int k = 0; k < PC / 2; ++k) {
+                    const float4 v = p4[k];
+                    wk[2 * k] = mk<R>(v.x, v.y);
+                    wk[2 * k + 1] = mk<R>(v.z, v.w);
+                }
+            } else {
+#pragma unroll
+                for (int k = 0; k < PC; ++k) wk[k] = prow[k];
+            }
+            if (prow) prow += ld;
 #pragma unroll
             for (int k = 0; k < PC; ++k) {
-                ep[k] += p0 + k;
-                if (ep[k] >= r) ep[k] -= r;
-                const cplx<R> w = T[ep[k] * stepR];
-                px[k] = fma(ax, w.x, px[k]);
-                py[k] = fma(ay, w.x, py[k]);
-                qx[k] = fma(bx, w.y, qx[k]);
-                qy[k] = fma(by, w.y, qy[k]);
+                const R wy = INV ? -wk[k].y : wk[k].y;
+                px[k] = fma(ax, wk[k].x, px[k]);
+                py[k] = fma(ay, wk[k].x, py[k]);
+                qx[k] = fma(bx, wy, qx[k]);
+                qy[k] = fma(by, wy, qy[k]);
             }
         }
         if (oc == 0) out[base * CW + c] = mk<R>(x0.x + sx, x0.y + sy);
@@ -241,7 +267,7 @@ __device__ __forceinline__ void pass_stream(cplx<R>* __restrict__ in, cplx<R>* _
 template <typename R, bool INV, int CW, int MAXR, bool STREAM>
 __global__ void __launch_bounds__(kFftThreads) k_fft_axis(cplx<R>* __restrict__ data, FftFactors f,
                                                           const cplx<R>* __restrict__ tw, size_t es, int ncols,
-                                                          size_t os) {
+                                                          size_t os, const cplx<R>* __restrict__ ptw) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     constexpr int ROWS = kFftThreads / CW;
     const int n = f.n;
@@ -249,6 +275,12 @@ __global__ void __launch_bounds__(kFftThreads) k_fft_axis(cplx<R>* __restrict__ 
     cplx<R>* Bv = A + size_t(n) * CW;
     cplx<R>* T = Bv + size_t(n) * CW;
     int2* jt = reinterpret_cast<int2*>(T + n);
+    // streamed-pass twiddle tables after jt, at a 16-byte aligned offset
+    const size_t pt_off_bytes =
+        ((size_t(2 * n * CW + n) * sizeof(cplx<R>) + 8 * size_t(n)) + 15) & ~size_t(15);
+    cplx<R>* PT = reinterpret_cast<cplx<R>*>(smem_raw + pt_off_bytes);
+    if (STREAM)
+        for (int t = threadIdx.x; t < f.pt_total; t += kFftThreads) PT[t] = ptw[t];
     const int c = threadIdx.x & (CW - 1);
     const int lane = threadIdx.x / CW;
     const int c0 = blockIdx.y * CW;
@@ -281,7 +313,8 @@ __global__ void __launch_bounds__(kFftThreads) k_fft_axis(cplx<R>* __restrict__ 
         else if (r == 8) pass_fixed<R, CW, INV, 8>(in, out, T, jt, n, L);
         else if (r <= 8) pass_reg<R, CW, 8>(in, out, T, jt, n, r, L);
         else if (MAXR > 8 && r <= MAXR) pass_reg<R, CW, (MAXR > 8 ? MAXR : 8)>(in, out, T, jt, n, r, L);
-        else if (STREAM) pass_stream<R, CW>(in, out, T, jt, n, r, L);
+        else if (STREAM)
+            pass_stream<R, INV, CW>(in, out, T, jt, n, r, L, f.pt_total ? PT + f.pt_off[ps] : nullptr, f.pt_ld[ps]);
         cplx<R>* tmp = in;
         in = out;
         out = tmp;
@@ -292,19 +325,24 @@ __global__ void __launch_bounds__(kFftThreads) k_fft_axis(cplx<R>* __restrict__ 
         for (int e = lane; e < n; e += ROWS) line[size_t(e) * es] = in[e * CW + c];
 }
 
-int pick_cw(int n, size_t elem, int ncols) {
+size_t fft_smem(int n, int cw, size_t elem, int pt_total) {
+    const size_t pt_off_bytes = (((2 * size_t(n) * cw + n) * elem + 8 * size_t(n)) + 15) & ~size_t(15);
+    return pt_off_bytes + size_t(pt_total) * elem;
+}
+
+int pick_cw(int n, size_t elem, int ncols, int pt_total) {
     int cw = 32;
-    while (cw > 1 && ((2 * size_t(n) * cw + n) * elem + 8 * size_t(n)) > kFftSmemBudget) cw /= 2;
+    while (cw > 1 && fft_smem(n, cw, elem, pt_total) > kFftSmemBudget) cw /= 2;
     while (cw > 1 && cw / 2 >= ncols) cw /= 2;
     return cw;
 }
 
 template <typename R, bool INV, int CW>
 void launch_cw(int cls, bool stream, dim3 grd, size_t shm, cudaStream_t s, cplx<R>* data, const FftFactors& f,
-               const cplx<R>* tw, size_t es, int ncols, size_t os) {
+               const cplx<R>* tw, size_t es, int ncols, size_t os, const cplx<R>* ptw) {
     auto go = [&](auto kern) {
         MPM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(shm)));
-        kern<<<grd, kFftThreads, shm, s>>>(data, f, tw, es, ncols, os);
+        kern<<<grd, kFftThreads, shm, s>>>(data, f, tw, es, ncols, os, ptw);
     };
     if (stream) {
         if (cls == 8) go(k_fft_axis<R, INV, CW, 8, true>);
@@ -317,14 +355,14 @@ void launch_cw(int cls, bool stream, dim3 grd, size_t shm, cudaStream_t s, cplx<
 
 template <typename R, bool INV>
 void launch(int cw, int cls, bool stream, dim3 grd, size_t shm, cudaStream_t s, cplx<R>* data, const FftFactors& f,
-            const cplx<R>* tw, size_t es, int ncols, size_t os) {
+            const cplx<R>* tw, size_t es, int ncols, size_t os, const cplx<R>* ptw) {
     switch (cw) {
-        case 32: launch_cw<R, INV, 32>(cls, stream, grd, shm, s, data, f, tw, es, ncols, os); break;
-        case 16: launch_cw<R, INV, 16>(cls, stream, grd, shm, s, data, f, tw, es, ncols, os); break;
-        case 8: launch_cw<R, INV, 8>(cls, stream, grd, shm, s, data, f, tw, es, ncols, os); break;
-        case 4: launch_cw<R, INV, 4>(cls, stream, grd, shm, s, data, f, tw, es, ncols, os); break;
-        case 2: launch_cw<R, INV, 2>(cls, stream, grd, shm, s, data, f, tw, es, ncols, os); break;
-        default: launch_cw<R, INV, 1>(cls, stream, grd, shm, s, data, f, tw, es, ncols, os); break;
+        case 32: launch_cw<R, INV, 32>(cls, stream, grd, shm, s, data, f, tw, es, ncols, os, ptw); break;
+        case 16: launch_cw<R, INV, 16>(cls, stream, grd, shm, s, data, f, tw, es, ncols, os, ptw); break;
+        case 8: launch_cw<R, INV, 8>(cls, stream, grd, shm, s, data, f, tw, es, ncols, os, ptw); break;
+        case 4: launch_cw<R, INV, 4>(cls, stream, grd, shm, s, data, f, tw, es, ncols, os, ptw); break;
+        case 2: launch_cw<R, INV, 2>(cls, stream, grd, shm, s, data, f, tw, es, ncols, os, ptw); break;
+        default: launch_cw<R, INV, 1>(cls, stream, grd, shm, s, data, f, tw, es, ncols, os, ptw); break;
     }
 }
 
@@ -332,7 +370,7 @@ void launch(int cw, int cls, bool stream, dim3 grd, size_t shm, cudaStream_t s, 
 
 bool AxisFFT::fits(int n, bool fp64) {
     const size_t elem = fp64 ? sizeof(double2) : sizeof(float2);
-    return (3 * size_t(n)) * elem + 8 * size_t(n) <= kFftSmemMax;
+    return (3 * size_t(n)) * elem + 8 * size_t(n) + 16 <= kFftSmemMax;
 }
 
 void AxisFFT::init(int n) {
@@ -365,14 +403,51 @@ void AxisFFT::init(int n) {
     tw32_.ensure(sizeof(float2) * n);
     MPM_CUDA(cudaMemcpy(tw64_.p, t64.data(), sizeof(double2) * n, cudaMemcpyHostToDevice));
     MPM_CUDA(cudaMemcpy(tw32_.p, t32.data(), sizeof(float2) * n, cudaMemcpyHostToDevice));
+    // W_r^(p q) tables of the streamed (r > 16) passes, rows padded to a
+    // multiple of 8 entries (the streamed pass reads 8 outputs per thread)
+    std::vector<double2> p64;
+    for (int i = 0; i < f_.nf; ++i) {
+        const int r = f_.r[i];
+        if (r <= 16) continue;
+        const int half = (r - 1) / 2;
+        const int ld = (half + 7) / 8 * 8;
+        f_.pt_off[i] = int(p64.size());
+        f_.pt_ld[i] = ld;
+        for (int q = 1; q <= half; ++q)
+            for (int c = 0; c < ld; ++c) {
+                const int p = c + 1;
+                if (p > half) {
+                    p64.push_back(make_double2(0.0, 0.0));
+                    continue;
+                }
+                const double a = -2.0 * kPi * double((long long)p * q % r) / double(r);
+                p64.push_back(make_double2(std::cos(a), std::sin(a)));
+            }
+        // 8 spare entries so a padded row can always be read as a whole
+        for (int c = 0; c < 8; ++c) p64.push_back(make_double2(0.0, 0.0));
+    }
+    f_.pt_total = int(p64.size());
+    if (p64.empty()) p64.push_back(make_double2(0.0, 0.0));
+    std::vector<float2> p32(p64.size());
+    for (size_t k = 0; k < p64.size(); ++k) p32[k] = make_float2(float(p64[k].x), float(p64[k].y));
+    pt64_.ensure(sizeof(double2) * p64.size());
+    pt32_.ensure(sizeof(float2) * p64.size());
+    MPM_CUDA(cudaMemcpy(pt64_.p, p64.data(), sizeof(double2) * p64.size(), cudaMemcpyHostToDevice));
+    MPM_CUDA(cudaMemcpy(pt32_.p, p32.data(), sizeof(float2) * p32.size(), cudaMemcpyHostToDevice));
 }
 
 template <typename R>
 void AxisFFT::run(cplx<R>* data, size_t es, int ncols, size_t os, int nouter, bool inverse, cudaStream_t s) const {
     if (f_.n <= 1 || nouter <= 0 || ncols <= 0) return;
     const int n = f_.n;
-    const int cw = pick_cw(n, sizeof(cplx<R>), ncols);
-    const size_t shm = (2 * size_t(n) * cw + n) * sizeof(cplx<R>) + 8 * size_t(n);
+    // the prime-pass tables go to shared memory when small (else the pass
+    // indexes the line's own twiddles)
+    FftFactors f = f_;
+    const int cw = pick_cw(n, sizeof(cplx<R>), ncols, 0);
+    // (only when that costs no columns per CTA)
+    if (fft_smem(n, cw, sizeof(cplx<R>), f.pt_total) > kFftSmemBudget) f.pt_total = 0;
+    const int pt_total = f.pt_total;
+    const size_t shm = fft_smem(n, cw, sizeof(cplx<R>), pt_total);
     if (shm > kFftSmemMax) throw std::runtime_error("FFT line does not fit in shared memory");
     const cplx<R>* tw = sizeof(R) == 4 ? reinterpret_cast<const cplx<R>*>(tw32_.p)
                                        : reinterpret_cast<const cplx<R>*>(tw64_.p);
@@ -384,8 +459,10 @@ void AxisFFT::run(cplx<R>* data, size_t es, int ncols, size_t os, int nouter, bo
         else rsmall = std::max(rsmall, f_.r[i]);
     }
     const int cls = rsmall <= 8 ? 8 : 16;
-    if (inverse) launch<R, true>(cw, cls, stream, grd, shm, s, data, f_, tw, es, ncols, os);
-    else launch<R, false>(cw, cls, stream, grd, shm, s, data, f_, tw, es, ncols, os);
+    const cplx<R>* ptw = sizeof(R) == 4 ? reinterpret_cast<const cplx<R>*>(pt32_.p)
+                                        : reinterpret_cast<const cplx<R>*>(pt64_.p);
+    if (inverse) launch<R, true>(cw, cls, stream, grd, shm, s, data, f, tw, es, ncols, os, ptw);
+    else launch<R, false>(cw, cls, stream, grd, shm, s, data, f, tw, es, ncols, os, ptw);
     MPM_LAUNCH();
 }
 

@@ -21,6 +21,11 @@ struct FftFactors {
     int n = 1;
     int nf = 0;
     int r[kFftMaxFactors] = {};
+    // factors above 16 (streamed passes): offset and row length of their
+    // W_r^(p q) table, rows q = 1..(r-1)/2, columns p = 1..(r-1)/2 (padded)
+    int pt_off[kFftMaxFactors] = {};
+    int pt_ld[kFftMaxFactors] = {};
+    int pt_total = 0;     // entries of all tables together
 };
 
 class AxisFFT {
@@ -37,6 +42,7 @@ public:
 private:
     FftFactors f_;
     DevBuf tw64_, tw32_;
+    DevBuf pt64_, pt32_;   // prime-pass twiddle tables (see FftFactors)
 };
 
 }  // namespace mpm
