@@ -264,36 +264,28 @@ __device__ __forceinline__ void pass_stream(cplx<R>* __restrict__ in, cplx<R>* _
     }
 }
 
+// global -> shared copy of one element without a register round trip, so a
+// thread's whole share of the line is in flight at once (src_bytes = 0 fills
+// the element with zeros and reads nothing)
+template <typename R>
+__device__ __forceinline__ void copy_async(cplx<R>* dst, const cplx<R>* src, bool live) {
+    const unsigned d = static_cast<unsigned>(__cvta_generic_to_shared(dst));
+    const int bytes = live ? int(sizeof(cplx<R>)) : 0;
+    if constexpr (sizeof(cplx<R>) == 16)
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(d), "l"(src), "r"(bytes) : "memory");
+    else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(d), "l"(src), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ void copy_async_wait() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
+// All radix passes of one line held in shared memory (ping-pong between
+// `in` and `out`); returns the buffer that holds the result.  T holds the
+// line's twiddles, conjugated for INV.
 template <typename R, bool INV, int CW, int MAXR, bool STREAM>
-__global__ void __launch_bounds__(kFftThreads) k_fft_axis(cplx<R>* __restrict__ data, FftFactors f,
-                                                          const cplx<R>* __restrict__ tw, size_t es, int ncols,
-                                                          size_t os, const cplx<R>* __restrict__ ptw) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    constexpr int ROWS = kFftThreads / CW;
+__device__ __forceinline__ cplx<R>* line_passes(cplx<R>* in, cplx<R>* out, const cplx<R>* T, int2* jt,
+                                                const FftFactors& f, const cplx<R>* PT) {
     const int n = f.n;
-    cplx<R>* A = reinterpret_cast<cplx<R>*>(smem_raw);
-    cplx<R>* Bv = A + size_t(n) * CW;
-    cplx<R>* T = Bv + size_t(n) * CW;
-    int2* jt = reinterpret_cast<int2*>(T + n);
-    // streamed-pass twiddle tables after jt, at a 16-byte aligned offset
-    const size_t pt_off_bytes =
-        ((size_t(2 * n * CW + n) * sizeof(cplx<R>) + 8 * size_t(n)) + 15) & ~size_t(15);
-    cplx<R>* PT = reinterpret_cast<cplx<R>*>(smem_raw + pt_off_bytes);
-    if (STREAM)
-        for (int t = threadIdx.x; t < f.pt_total; t += kFftThreads) PT[t] = ptw[t];
-    const int c = threadIdx.x & (CW - 1);
-    const int lane = threadIdx.x / CW;
-    const int c0 = blockIdx.y * CW;
-    const bool live = c0 + c < ncols;
-    cplx<R>* line = data + size_t(blockIdx.x) * os + c0 + c;
-    for (int t = threadIdx.x; t < n; t += kFftThreads) {
-        cplx<R> w = tw[t];
-        if (INV) w.y = -w.y;
-        T[t] = w;
-    }
-    for (int e = lane; e < n; e += ROWS) A[e * CW + c] = live ? line[size_t(e) * es] : mk<R>(0, 0);
-    cplx<R>* in = A;
-    cplx<R>* out = Bv;
     int Ns = 1;
     for (int ps = 0; ps < f.nf; ++ps) {
         const int r = f.r[ps];
@@ -321,8 +313,68 @@ __global__ void __launch_bounds__(kFftThreads) k_fft_axis(cplx<R>* __restrict__ 
         Ns = L;
     }
     __syncthreads();
+    return in;
+}
+
+// Diagonal k-space factor of the fused transform: element e of line o,
+// column c is multiplied by sc[(e * nouter + o) * sz + c / sb].
+template <typename R>
+struct LineScale {
+    const R* sc = nullptr;
+    int nouter = 0, sz = 1, sb = 1;
+};
+
+// One CTA = CW adjacent columns of one line.  KSCALE: forward transform,
+// k-space scale, inverse transform in one round trip of the line (INV is
+// then unused); else a single transform in the direction INV.
+template <typename R, bool INV, int CW, int MAXR, bool STREAM, bool KSCALE>
+__global__ void __launch_bounds__(kFftThreads) k_fft_axis(cplx<R>* __restrict__ data, FftFactors f,
+                                                          const cplx<R>* __restrict__ tw, size_t es, int ncols,
+                                                          size_t os, const cplx<R>* __restrict__ ptw,
+                                                          LineScale<R> ks) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    constexpr int ROWS = kFftThreads / CW;
+    constexpr bool FWD_INV = KSCALE ? false : INV;
+    const int n = f.n;
+    cplx<R>* A = reinterpret_cast<cplx<R>*>(smem_raw);
+    cplx<R>* Bv = A + size_t(n) * CW;
+    cplx<R>* T = Bv + size_t(n) * CW;
+    int2* jt = reinterpret_cast<int2*>(T + n);
+    // streamed-pass twiddle tables after jt, at a 16-byte aligned offset
+    const size_t pt_off_bytes =
+        ((size_t(2 * n * CW + n) * sizeof(cplx<R>) + 8 * size_t(n)) + 15) & ~size_t(15);
+    cplx<R>* PT = reinterpret_cast<cplx<R>*>(smem_raw + pt_off_bytes);
+    const int c = threadIdx.x & (CW - 1);
+    const int lane = threadIdx.x / CW;
+    const int c0 = blockIdx.y * CW;
+    const bool live = c0 + c < ncols;
+    cplx<R>* line = data + size_t(blockIdx.x) * os + c0 + c;
+    // dead columns copy nothing; their source address is only a placeholder
+    const cplx<R>* src = live ? line : data;
+    const size_t ses = live ? es : 0;
+    for (int e = lane; e < n; e += ROWS) copy_async<R>(A + e * CW + c, src + size_t(e) * ses, live);
+    if (STREAM)
+        for (int t = threadIdx.x; t < f.pt_total; t += kFftThreads) PT[t] = ptw[t];
+    for (int t = threadIdx.x; t < n; t += kFftThreads) {
+        cplx<R> w = tw[t];
+        if (FWD_INV) w.y = -w.y;
+        T[t] = w;
+    }
+    copy_async_wait();
+    cplx<R>* res = line_passes<R, FWD_INV, CW, MAXR, STREAM>(A, Bv, T, jt, f, PT);
+    if constexpr (KSCALE) {
+        // each thread scales the elements it loaded; the inverse twiddles
+        // replace the forward ones (line_passes ends with a barrier)
+        if (live) {
+            const R* sc = ks.sc + size_t(blockIdx.x) * ks.sz + (c0 + c) / ks.sb;
+            const size_t sstep = size_t(ks.nouter) * ks.sz;
+            for (int e = lane; e < n; e += ROWS) res[e * CW + c] = res[e * CW + c] * sc[size_t(e) * sstep];
+        }
+        for (int t = threadIdx.x; t < n; t += kFftThreads) T[t].y = -T[t].y;
+        res = line_passes<R, true, CW, MAXR, STREAM>(res, res == A ? Bv : A, T, jt, f, PT);
+    }
     if (live)
-        for (int e = lane; e < n; e += ROWS) line[size_t(e) * es] = in[e * CW + c];
+        for (int e = lane; e < n; e += ROWS) line[size_t(e) * es] = res[e * CW + c];
 }
 
 size_t fft_smem(int n, int cw, size_t elem, int pt_total) {
@@ -337,32 +389,32 @@ int pick_cw(int n, size_t elem, int ncols, int pt_total) {
     return cw;
 }
 
-template <typename R, bool INV, int CW>
+template <typename R, bool INV, bool KSCALE, int CW>
 void launch_cw(int cls, bool stream, dim3 grd, size_t shm, cudaStream_t s, cplx<R>* data, const FftFactors& f,
-               const cplx<R>* tw, size_t es, int ncols, size_t os, const cplx<R>* ptw) {
+               const cplx<R>* tw, size_t es, int ncols, size_t os, const cplx<R>* ptw, const LineScale<R>& ks) {
     auto go = [&](auto kern) {
         MPM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(shm)));
-        kern<<<grd, kFftThreads, shm, s>>>(data, f, tw, es, ncols, os, ptw);
+        kern<<<grd, kFftThreads, shm, s>>>(data, f, tw, es, ncols, os, ptw, ks);
     };
     if (stream) {
-        if (cls == 8) go(k_fft_axis<R, INV, CW, 8, true>);
-        else go(k_fft_axis<R, INV, CW, 16, true>);
+        if (cls == 8) go(k_fft_axis<R, INV, CW, 8, true, KSCALE>);
+        else go(k_fft_axis<R, INV, CW, 16, true, KSCALE>);
     } else {
-        if (cls == 8) go(k_fft_axis<R, INV, CW, 8, false>);
-        else go(k_fft_axis<R, INV, CW, 16, false>);
+        if (cls == 8) go(k_fft_axis<R, INV, CW, 8, false, KSCALE>);
+        else go(k_fft_axis<R, INV, CW, 16, false, KSCALE>);
     }
 }
 
-template <typename R, bool INV>
+template <typename R, bool INV, bool KSCALE>
 void launch(int cw, int cls, bool stream, dim3 grd, size_t shm, cudaStream_t s, cplx<R>* data, const FftFactors& f,
-            const cplx<R>* tw, size_t es, int ncols, size_t os, const cplx<R>* ptw) {
+            const cplx<R>* tw, size_t es, int ncols, size_t os, const cplx<R>* ptw, const LineScale<R>& ks) {
     switch (cw) {
-        case 32: launch_cw<R, INV, 32>(cls, stream, grd, shm, s, data, f, tw, es, ncols, os, ptw); break;
-        case 16: launch_cw<R, INV, 16>(cls, stream, grd, shm, s, data, f, tw, es, ncols, os, ptw); break;
-        case 8: launch_cw<R, INV, 8>(cls, stream, grd, shm, s, data, f, tw, es, ncols, os, ptw); break;
-        case 4: launch_cw<R, INV, 4>(cls, stream, grd, shm, s, data, f, tw, es, ncols, os, ptw); break;
-        case 2: launch_cw<R, INV, 2>(cls, stream, grd, shm, s, data, f, tw, es, ncols, os, ptw); break;
-        default: launch_cw<R, INV, 1>(cls, stream, grd, shm, s, data, f, tw, es, ncols, os, ptw); break;
+        case 32: launch_cw<R, INV, KSCALE, 32>(cls, stream, grd, shm, s, data, f, tw, es, ncols, os, ptw, ks); break;
+        case 16: launch_cw<R, INV, KSCALE, 16>(cls, stream, grd, shm, s, data, f, tw, es, ncols, os, ptw, ks); break;
+        case 8: launch_cw<R, INV, KSCALE, 8>(cls, stream, grd, shm, s, data, f, tw, es, ncols, os, ptw, ks); break;
+        case 4: launch_cw<R, INV, KSCALE, 4>(cls, stream, grd, shm, s, data, f, tw, es, ncols, os, ptw, ks); break;
+        case 2: launch_cw<R, INV, KSCALE, 2>(cls, stream, grd, shm, s, data, f, tw, es, ncols, os, ptw, ks); break;
+        default: launch_cw<R, INV, KSCALE, 1>(cls, stream, grd, shm, s, data, f, tw, es, ncols, os, ptw, ks); break;
     }
 }
 
@@ -437,7 +489,8 @@ void AxisFFT::init(int n) {
 }
 
 template <typename R>
-void AxisFFT::run(cplx<R>* data, size_t es, int ncols, size_t os, int nouter, bool inverse, cudaStream_t s) const {
+void AxisFFT::launch_line(cplx<R>* data, size_t es, int ncols, size_t os, int nouter, int mode, const R* scale,
+                          int sz, int sb, cudaStream_t s) const {
     if (f_.n <= 1 || nouter <= 0 || ncols <= 0) return;
     const int n = f_.n;
     // the prime-pass tables go to shared memory when small (else the pass
@@ -461,12 +514,34 @@ void AxisFFT::run(cplx<R>* data, size_t es, int ncols, size_t os, int nouter, bo
     const int cls = rsmall <= 8 ? 8 : 16;
     const cplx<R>* ptw = sizeof(R) == 4 ? reinterpret_cast<const cplx<R>*>(pt32_.p)
                                         : reinterpret_cast<const cplx<R>*>(pt64_.p);
-    if (inverse) launch<R, true>(cw, cls, stream, grd, shm, s, data, f, tw, es, ncols, os, ptw);
-    else launch<R, false>(cw, cls, stream, grd, shm, s, data, f, tw, es, ncols, os, ptw);
+    LineScale<R> ks;
+    ks.sc = scale;
+    ks.nouter = nouter;
+    ks.sz = sz;
+    ks.sb = sb;
+    if (mode == 2) launch<R, false, true>(cw, cls, stream, grd, shm, s, data, f, tw, es, ncols, os, ptw, ks);
+    else if (mode == 1) launch<R, true, false>(cw, cls, stream, grd, shm, s, data, f, tw, es, ncols, os, ptw, ks);
+    else launch<R, false, false>(cw, cls, stream, grd, shm, s, data, f, tw, es, ncols, os, ptw, ks);
     MPM_LAUNCH();
+}
+
+template <typename R>
+void AxisFFT::run(cplx<R>* data, size_t es, int ncols, size_t os, int nouter, bool inverse, cudaStream_t s) const {
+    launch_line<R>(data, es, ncols, os, nouter, inverse ? 1 : 0, nullptr, 1, 1, s);
+}
+
+template <typename R>
+void AxisFFT::run_scaled(cplx<R>* data, size_t es, int ncols, size_t os, int nouter, const R* scale, int sz, int sb,
+                         cudaStream_t s) const {
+    if (!scale || sz <= 0 || sb <= 0) throw std::runtime_error("run_scaled: scale table and its strides required");
+    launch_line<R>(data, es, ncols, os, nouter, 2, scale, sz, sb, s);
 }
 
 template void AxisFFT::run<float>(float2*, size_t, int, size_t, int, bool, cudaStream_t) const;
 template void AxisFFT::run<double>(double2*, size_t, int, size_t, int, bool, cudaStream_t) const;
+template void AxisFFT::run_scaled<float>(float2*, size_t, int, size_t, int, const float*, int, int,
+                                         cudaStream_t) const;
+template void AxisFFT::run_scaled<double>(double2*, size_t, int, size_t, int, const double*, int, int,
+                                          cudaStream_t) const;
 
 }  // namespace mpm

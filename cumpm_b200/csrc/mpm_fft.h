@@ -36,10 +36,19 @@ public:
     // data[o*os + e*es + c], c in [0, ncols)
     template <typename R>
     void run(cplx<R>* data, size_t es, int ncols, size_t os, int nouter, bool inverse, cudaStream_t s) const;
+    // forward transform, multiplication of element e of line o, column c by
+    // scale[(e * nouter + o) * sz + c / sb], inverse transform: the k-space
+    // step of a convolution fused into one pass over the lines
+    template <typename R>
+    void run_scaled(cplx<R>* data, size_t es, int ncols, size_t os, int nouter, const R* scale, int sz, int sb,
+                    cudaStream_t s) const;
     // whether one line of this length fits in shared memory
     static bool fits(int n, bool fp64);
 
 private:
+    template <typename R>
+    void launch_line(cplx<R>* data, size_t es, int ncols, size_t os, int nouter, int mode, const R* scale, int sz,
+                     int sb, cudaStream_t s) const;
     FftFactors f_;
     DevBuf tw64_, tw32_;
     DevBuf pt64_, pt32_;   // prime-pass twiddle tables (see FftFactors)

@@ -574,20 +574,40 @@ void Field::poly_recip_on(const double2* X, double2* Y, int M, cplx<R>* grid, cu
             X, M, ps.base.as<int4>(), w1, ptoff_.as<int>(), ptlist_.as<int>(), t, grid);
         MPM_LAUNCH();
     }
-    {
-        StageScope sc(ST_FFT_FWD, s);
-        transform<R>(grid, M, false, s);
-    }
-    {
-        StageScope sc(ST_KSPACE, s);
-        const long long n = (long long)gv_.Nx * gv_.Ny * gv_.Nz * M;
-        const R* scl = sizeof(R) == 4 ? reinterpret_cast<const R*>(scale32_.p) : reinterpret_cast<const R*>(scale64_.p);
-        k_poly_scale<R><<<nblk(n, 256), 256, 0, s>>>(grid, scl, n, M);
-        MPM_LAUNCH();
-    }
-    {
-        StageScope sc(ST_FFT_INV, s);
-        transform<R>(grid, M, true, s);
+    const R* scl = sizeof(R) == 4 ? reinterpret_cast<const R*>(scale32_.p) : reinterpret_cast<const R*>(scale64_.p);
+    if (own_fft_) {
+        // z and y forward; x forward, scale and x inverse in one pass over
+        // the x lines; y and z inverse (the 1-D transforms commute)
+        const size_t Bi = size_t(gv_.Nz) * M;
+        {
+            StageScope sc(ST_FFT_FWD, s);
+            fftz_.run<R>(grid, size_t(M), M, size_t(gv_.Nz) * M, gv_.Nx * gv_.Ny, false, s);
+            ffty_.run<R>(grid, Bi, int(Bi), size_t(gv_.Ny) * Bi, gv_.Nx, false, s);
+        }
+        {
+            StageScope sc(ST_KSPACE, s);
+            fftx_.run_scaled<R>(grid, size_t(gv_.Ny) * Bi, int(Bi), Bi, gv_.Ny, scl, gv_.Nz, M, s);
+        }
+        {
+            StageScope sc(ST_FFT_INV, s);
+            ffty_.run<R>(grid, Bi, int(Bi), size_t(gv_.Ny) * Bi, gv_.Nx, true, s);
+            fftz_.run<R>(grid, size_t(M), M, size_t(gv_.Nz) * M, gv_.Nx * gv_.Ny, true, s);
+        }
+    } else {
+        {
+            StageScope sc(ST_FFT_FWD, s);
+            transform<R>(grid, M, false, s);
+        }
+        {
+            StageScope sc(ST_KSPACE, s);
+            const long long n = (long long)gv_.Nx * gv_.Ny * gv_.Nz * M;
+            k_poly_scale<R><<<nblk(n, 256), 256, 0, s>>>(grid, scl, n, M);
+            MPM_LAUNCH();
+        }
+        {
+            StageScope sc(ST_FFT_INV, s);
+            transform<R>(grid, M, true, s);
+        }
     }
     if (!Y) return;  // potential only (grid holds phi = IFFT(S FFT(rho)))
     StageScope sc(ST_CONTRACT, s);
