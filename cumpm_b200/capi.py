@@ -33,7 +33,7 @@ EXPORTS = [
     "mpm_field_apply", "mpm_field_apply_part", "mpm_field_info_get", "mpm_batch_solve",
     "mpm_mono_tables", "mpm_ewald_geometry", "mpm_poly_geometry", "mpm_poly_pair_functions",
     "mpm_profile_enable", "mpm_profile_reset", "mpm_profile_read", "mpm_kernel_launches",
-    "mpm_field_apply_noalloc", "mpm_noalloc_scratch_bytes", "mpm_field_grad",
+    "mpm_field_apply_noalloc", "mpm_noalloc_scratch_bytes", "mpm_field_grad", "mpm_line_fft",
 ]
 
 STAGES = ["spread", "fft_fwd", "kspace", "fft_inv", "contract", "real", "direct", "krylov", "precalc"]
@@ -87,6 +87,8 @@ def lib():
         L.mpm_field_grad.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_void_p,
                                      C.c_void_p]
         L.mpm_kernel_launches.restype = C.c_longlong
+        L.mpm_line_fft.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_size_t, C.c_int, C.c_size_t, C.c_int, C.c_int,
+                                   C.c_void_p, C.c_int, C.c_int, C.c_int, _ip, C.c_void_p]
         L._mpm_typed = True
     return L
 
@@ -125,6 +127,33 @@ def poly_geometry(box, errortol, xi, radii):
     check(lib().mpm_poly_geometry(bp, float(errortol), float(xi), rp, len(rr), grid, C.byref(P), C.byref(eta),
                                   C.byref(rc), C.byref(nc), cls.ctypes.data_as(C.POINTER(C.c_int))))
     return dict(grid=list(grid), P=P.value, eta=eta.value, rc=rc.value, n_classes=nc.value, cls=cls)
+
+
+def line_fft(data, n, es, ncols, os, nouter, mode=0, scale=None, sz=1, sb=1, general=False):
+    """In-place batched line DFT of a complex64/complex128 CUDA tensor (the
+    grid transform of the spectral-Ewald fields): element e of line o,
+    column c at flat index o*os + e*es + c.  mode 0 forward, 1 inverse,
+    2 forward * scale[(e*nouter + o)*sz + c//sb] then inverse (scale a real
+    CUDA tensor of the matching precision).  Returns the two-pass split
+    (r1, r2), (0, 0) when the multi-pass kernel ran."""
+    import torch
+
+    if not data.is_cuda or not data.is_contiguous() or data.dtype not in (torch.complex64, torch.complex128):
+        raise ValueError("data must be a contiguous complex64/complex128 CUDA tensor")
+    fp64 = data.dtype == torch.complex128
+    sp = None
+    if mode == 2:
+        if scale is None or not scale.is_cuda or not scale.is_contiguous():
+            raise ValueError("mode 2 needs a contiguous CUDA scale tensor")
+        if scale.dtype != (torch.float64 if fp64 else torch.float32):
+            raise ValueError("scale precision must match data")
+        sp = C.c_void_p(scale.data_ptr())
+    split = (C.c_int * 2)()
+    stream = torch.cuda.current_stream(data.device).cuda_stream
+    check(lib().mpm_line_fft(C.c_void_p(data.data_ptr()), int(fp64), int(n), int(es), int(ncols), int(os),
+                             int(nouter), int(mode), sp, int(sz), int(sb), int(bool(general)), split,
+                             C.c_void_p(stream)))
+    return split[0], split[1]
 
 
 def poly_pair_functions(a, b, xi, r, rc=None, lookup=False):

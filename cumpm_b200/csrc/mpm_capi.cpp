@@ -8,6 +8,7 @@
 #include <string>
 
 #include "mpm_field.h"
+#include "mpm_fft.h"
 #include "mpm_krylov.h"
 #include "mpm_solver.h"
 
@@ -372,6 +373,35 @@ int mpm_field_grad(mpm_field* f, const void* lam, const void* p, int M, void* gx
         f->impl->grad_bilinear(static_cast<const double2*>(lam), static_cast<const double2*>(p), M,
                                static_cast<double2*>(gx), static_cast<double2*>(ga),
                                static_cast<cudaStream_t>(stream));
+    });
+}
+
+int mpm_line_fft(void* data, int fp64, int n, size_t es, int ncols, size_t os, int nouter, int mode,
+                 const void* scale, int sz, int sb, int general, int* split, void* stream) {
+    return guard([&] {
+        need(data, "data");
+        if (n < 1 || ncols < 1 || nouter < 1) throw std::invalid_argument("empty line transform");
+        if (mode < 0 || mode > 2) throw std::invalid_argument("mode must be 0 (forward), 1 (inverse) or 2 (scaled)");
+        if (mode == 2 && (!scale || sz < 1 || sb < 1)) throw std::invalid_argument("mode 2 needs scale, sz, sb");
+        if (!mpm::AxisFFT::fits(n, true)) throw std::invalid_argument("line too long for the in-house transform");
+        mpm::AxisFFT fft;
+        fft.init(n);
+        fft.set_force_general(general != 0);
+        if (split) {
+            split[0] = fft.two_pass(ncols) ? fft.split_r1() : 0;
+            split[1] = fft.two_pass(ncols) ? fft.split_r2() : 0;
+        }
+        const auto st = static_cast<cudaStream_t>(stream);
+        if (fp64) {
+            auto* d = static_cast<double2*>(data);
+            if (mode == 2) fft.run_scaled<double>(d, es, ncols, os, nouter, static_cast<const double*>(scale), sz, sb, st);
+            else fft.run<double>(d, es, ncols, os, nouter, mode == 1, st);
+        } else {
+            auto* d = static_cast<float2*>(data);
+            if (mode == 2) fft.run_scaled<float>(d, es, ncols, os, nouter, static_cast<const float*>(scale), sz, sb, st);
+            else fft.run<float>(d, es, ncols, os, nouter, mode == 1, st);
+        }
+        MPM_CUDA(cudaStreamSynchronize(st));
     });
 }
 

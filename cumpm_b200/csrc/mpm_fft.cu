@@ -1,7 +1,10 @@
 // Batched in-place 1-D DFT along a strided axis (see mpm_fft.h).
 #include "mpm_fft.h"
+#include "mpm_fft_consts.cuh"
 
 #include <algorithm>
+#include <type_traits>
+#include <utility>
 #include <cmath>
 #include <vector>
 
@@ -72,11 +75,106 @@ __device__ __forceinline__ cplx<R> rot(cplx<R> v) {
     return INV ? mk<R>(-v.y, v.x) : mk<R>(v.y, -v.x);
 }
 
+template <typename R, bool INV, int RAD>
+__device__ __forceinline__ void dft_small(cplx<R> (&x)[RAD]);
+
+// W_N^j = exp(-2 pi i j / N) (conjugated for INV) from the constant tables
+template <typename R, bool INV, int N>
+__device__ __forceinline__ cplx<R> wconst(int j) {
+    cplx<R> w;
+    if constexpr (sizeof(R) == 8) {
+        if constexpr (N == 7) w = kW7d[j];
+        else if constexpr (N == 9) w = kW9d[j];
+        else if constexpr (N == 10) w = kW10d[j];
+        else if constexpr (N == 12) w = kW12d[j];
+        else w = kW16d[j];
+    } else {
+        if constexpr (N == 7) w = kW7f[j];
+        else if constexpr (N == 9) w = kW9f[j];
+        else if constexpr (N == 10) w = kW10f[j];
+        else if constexpr (N == 12) w = kW12f[j];
+        else w = kW16f[j];
+    }
+    if (INV) w.y = -w.y;
+    return w;
+}
+
+// Composite DFT of A*B points in registers (Cooley-Tukey, decimation in
+// time): input m = B m1 + m2, output k = k1 + A k2,
+//   y_k = sum_m2 W_B^(m2 k2) [ W_N^(m2 k1) sum_m1 x_(B m1 + m2) W_A^(m1 k1) ].
+template <typename R, bool INV, int A, int B>
+__device__ __forceinline__ void dft_ct(cplx<R> (&x)[A * B]) {
+    constexpr int N = A * B;
+    cplx<R> z[B][A];
+#pragma unroll
+    for (int m2 = 0; m2 < B; ++m2) {
+        cplx<R> t[A];
+#pragma unroll
+        for (int m1 = 0; m1 < A; ++m1) t[m1] = x[B * m1 + m2];
+        dft_small<R, INV, A>(t);
+#pragma unroll
+        for (int k1 = 0; k1 < A; ++k1) z[m2][k1] = m2 * k1 == 0 ? t[k1] : t[k1] * wconst<R, INV, N>(m2 * k1);
+    }
+#pragma unroll
+    for (int k1 = 0; k1 < A; ++k1) {
+        cplx<R> t[B];
+#pragma unroll
+        for (int m2 = 0; m2 < B; ++m2) t[m2] = z[m2][k1];
+        dft_small<R, INV, B>(t);
+#pragma unroll
+        for (int k2 = 0; k2 < B; ++k2) x[k1 + A * k2] = t[k2];
+    }
+}
+
+// Odd prime P in registers: with a_q = x_q + x_(P-q), b_q = x_q - x_(P-q),
+// y_p = x_0 + sum_q a_q cos(2 pi p q / P) -+ i sum_q b_q sin(2 pi p q / P)
+// and y_(P-p) the same with the sine term negated.
+template <typename R, bool INV, int P>
+__device__ __forceinline__ void dft_odd(cplx<R> (&x)[P]) {
+    constexpr int H = (P - 1) / 2;
+    cplx<R> a[H], b[H];
+#pragma unroll
+    for (int q = 1; q <= H; ++q) {
+        a[q - 1] = x[q] + x[P - q];
+        b[q - 1] = x[q] - x[P - q];
+    }
+    cplx<R> y0 = x[0];
+#pragma unroll
+    for (int q = 0; q < H; ++q) y0 += a[q];
+#pragma unroll
+    for (int p = 1; p <= H; ++p) {
+        cplx<R> t = x[0], u = mk<R>(R(0), R(0));
+#pragma unroll
+        for (int q = 1; q <= H; ++q) {
+            const cplx<R> w = wconst<R, false, P>((p * q) % P);   // (cos, -sin)
+            t = t + a[q - 1] * w.x;
+            u = u + b[q - 1] * (-w.y);
+        }
+        // -i u (forward) or +i u (inverse)
+        const cplx<R> ru = rot<R, INV>(u);
+        x[p] = t + ru;
+        x[P - p] = t - ru;
+    }
+    x[0] = y0;
+}
+
 // In-register DFT of RAD points, y_p = sum_q x_q W^(p q), W = exp(-+2 pi i/RAD),
-// written out for the radices the grid lengths use (2, 3, 4, 5, 6, 8).
+// written out for the radices the grid lengths use (2, 3, 4, 5, 6, 8) and
+// composed or tabulated for 7, 9, 10, 12, 16.
 template <typename R, bool INV, int RAD>
 __device__ __forceinline__ void dft_small(cplx<R> (&x)[RAD]) {
-    if constexpr (RAD == 2) {
+    if constexpr (RAD == 1) {
+    } else if constexpr (RAD == 7) {
+        dft_odd<R, INV, 7>(x);
+    } else if constexpr (RAD == 9) {
+        dft_ct<R, INV, 3, 3>(x);
+    } else if constexpr (RAD == 10) {
+        dft_ct<R, INV, 2, 5>(x);
+    } else if constexpr (RAD == 12) {
+        dft_ct<R, INV, 4, 3>(x);
+    } else if constexpr (RAD == 16) {
+        dft_ct<R, INV, 4, 4>(x);
+    } else if constexpr (RAD == 2) {
         const cplx<R> a = x[0], b = x[1];
         x[0] = a + b;
         x[1] = a - b;
@@ -331,7 +429,7 @@ template <typename R, bool INV, int CW, int MAXR, bool STREAM, bool KSCALE>
 __global__ void __launch_bounds__(kFftThreads) k_fft_axis(cplx<R>* __restrict__ data, FftFactors f,
                                                           const cplx<R>* __restrict__ tw, size_t es, int ncols,
                                                           size_t os, const cplx<R>* __restrict__ ptw,
-                                                          LineScale<R> ks) {
+                                                          int ngroups, LineScale<R> ks) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     constexpr int ROWS = kFftThreads / CW;
     constexpr bool FWD_INV = KSCALE ? false : INV;
@@ -346,9 +444,11 @@ __global__ void __launch_bounds__(kFftThreads) k_fft_axis(cplx<R>* __restrict__ 
     cplx<R>* PT = reinterpret_cast<cplx<R>*>(smem_raw + pt_off_bytes);
     const int c = threadIdx.x & (CW - 1);
     const int lane = threadIdx.x / CW;
-    const int c0 = blockIdx.y * CW;
+    // column groups of one line are adjacent in launch order
+    const int o = blockIdx.x / ngroups;
+    const int c0 = (blockIdx.x - o * ngroups) * CW;
     const bool live = c0 + c < ncols;
-    cplx<R>* line = data + size_t(blockIdx.x) * os + c0 + c;
+    cplx<R>* line = data + size_t(o) * os + c0 + c;
     // dead columns copy nothing; their source address is only a placeholder
     const cplx<R>* src = live ? line : data;
     const size_t ses = live ? es : 0;
@@ -366,7 +466,7 @@ __global__ void __launch_bounds__(kFftThreads) k_fft_axis(cplx<R>* __restrict__ 
         // each thread scales the elements it loaded; the inverse twiddles
         // replace the forward ones (line_passes ends with a barrier)
         if (live) {
-            const R* sc = ks.sc + size_t(blockIdx.x) * ks.sz + (c0 + c) / ks.sb;
+            const R* sc = ks.sc + size_t(o) * ks.sz + (c0 + c) / ks.sb;
             const size_t sstep = size_t(ks.nouter) * ks.sz;
             for (int e = lane; e < n; e += ROWS) res[e * CW + c] = res[e * CW + c] * sc[size_t(e) * sstep];
         }
@@ -375,6 +475,174 @@ __global__ void __launch_bounds__(kFftThreads) k_fft_axis(cplx<R>* __restrict__ 
     }
     if (live)
         for (int e = lane; e < n; e += ROWS) line[size_t(e) * es] = res[e * CW + c];
+}
+
+// ---------------------------------------------------------------------------
+// Two-pass line transform for n = r1 * r2 with both factors in-register
+// radices (<= 16).  Thread (lane, c) of a CTA of CW columns runs one
+// butterfly per pass, so a line makes a single round trip through shared
+// memory: pass 1 (radix r1, no twiddles) reads its r1 inputs straight from
+// global memory (all loads in flight together) and writes shared; pass 2
+// (radix r2, twiddles W_n^(q j)) reads shared and writes global.  Stockham
+// indexing as above: pass 1 butterfly j < r2 reads x[j + q r2], writes
+// S[j r1 + p]; pass 2 butterfly j < r1 reads S[j + q r1], writes y[p r1 + j].
+//
+// KSCALE (mode 2): after the forward pass 2 a thread holds y[p r1 + j],
+// p < r2, which are exactly the inputs of butterfly j of an inverse
+// transform whose first radix is r2; it scales them, runs that butterfly in
+// registers and writes S[j r2 + p]; the inverse radix-r1 pass (butterfly
+// j < r2 reads S[j + q r2] W_n^(-q j), writes x[p r2 + j]) ends in global
+// memory.  Forward, scale and inverse thus cost one global round trip and
+// two shared ones.
+
+constexpr int kFft2MaxThreads = 384;
+
+template <int CLS, typename Fn>
+__device__ __forceinline__ void radix_dispatch(int r, Fn&& fn) {
+    switch (r) {
+        case 1: fn(std::integral_constant<int, 1>{}); break;
+        case 2: fn(std::integral_constant<int, 2>{}); break;
+        case 3: fn(std::integral_constant<int, 3>{}); break;
+        case 4: fn(std::integral_constant<int, 4>{}); break;
+        case 5: fn(std::integral_constant<int, 5>{}); break;
+        case 6: fn(std::integral_constant<int, 6>{}); break;
+        case 7: fn(std::integral_constant<int, 7>{}); break;
+        case 8: fn(std::integral_constant<int, 8>{}); break;
+        default:
+            if constexpr (CLS > 8) {
+                switch (r) {
+                    case 9: fn(std::integral_constant<int, 9>{}); break;
+                    case 10: fn(std::integral_constant<int, 10>{}); break;
+                    case 12: fn(std::integral_constant<int, 12>{}); break;
+                    case 16: fn(std::integral_constant<int, 16>{}); break;
+                    default: break;
+                }
+            }
+            break;
+    }
+}
+
+template <typename R, int CW, int MODE, int CLS>
+__global__ void __launch_bounds__(kFft2MaxThreads) k_fft2(cplx<R>* __restrict__ data, const cplx<R>* __restrict__ tw,
+                                                          int r1, int r2, size_t es, int ncols, size_t os,
+                                                          int ngroups, LineScale<R> ks) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    constexpr bool INV = MODE == 1;
+    const int n = r1 * r2;
+    cplx<R>* S = reinterpret_cast<cplx<R>*>(smem_raw);
+    cplx<R>* T = S + size_t(n) * CW;
+    // column groups of one line are adjacent in launch order, so the DRAM
+    // lines their row pieces share are fetched once
+    const int o = blockIdx.x / ngroups;
+    const int g = blockIdx.x - o * ngroups;
+    const int c = threadIdx.x & (CW - 1);
+    const int lane = threadIdx.x / CW;
+    const int c0 = g * CW;
+    const bool live = c0 + c < ncols;
+    cplx<R>* line = data + size_t(o) * os + c0 + c;
+    for (int t = threadIdx.x; t < n; t += blockDim.x) T[t] = tw[t];
+    // pass 1: radix r1, butterfly lane < r2, global -> shared
+    radix_dispatch<CLS>(r1, [&](auto rc) {
+        constexpr int RAD = decltype(rc)::value;
+        if (lane < r2) {
+            cplx<R> x[RAD];
+#pragma unroll
+            for (int q = 0; q < RAD; ++q) x[q] = live ? line[size_t(lane + q * r2) * es] : mk<R>(R(0), R(0));
+            dft_small<R, INV, RAD>(x);
+#pragma unroll
+            for (int p = 0; p < RAD; ++p) S[(lane * RAD + p) * CW + c] = x[p];
+        }
+    });
+    __syncthreads();
+    // pass 2: radix r2, butterfly lane < r1, shared -> global (or on to the
+    // scale and the first inverse butterfly)
+    radix_dispatch<CLS>(r2, [&](auto rc) {
+        constexpr int RAD = decltype(rc)::value;
+        const bool act = lane < r1;
+        cplx<R> x[RAD];
+        if (act) {
+            x[0] = S[lane * CW + c];
+#pragma unroll
+            for (int q = 1; q < RAD; ++q) {
+                cplx<R> w = T[q * lane];
+                if (INV) w.y = -w.y;
+                x[q] = S[(lane + q * r1) * CW + c] * w;
+            }
+            dft_small<R, INV, RAD>(x);
+        }
+        if constexpr (MODE == 2) {
+            if (act) {
+                if (live) {
+                    const R* sc = ks.sc + size_t(o) * ks.sz + (c0 + c) / ks.sb;
+                    const size_t sstep = size_t(ks.nouter) * ks.sz;
+#pragma unroll
+                    for (int p = 0; p < RAD; ++p) x[p] = x[p] * sc[size_t(p * r1 + lane) * sstep];
+                }
+                dft_small<R, true, RAD>(x);
+            }
+            __syncthreads();   // every read of S above is done
+            if (act) {
+#pragma unroll
+                for (int p = 0; p < RAD; ++p) S[(lane * RAD + p) * CW + c] = x[p];
+            }
+        } else {
+            if (act && live) {
+#pragma unroll
+                for (int p = 0; p < RAD; ++p) line[size_t(p * r1 + lane) * es] = x[p];
+            }
+        }
+    });
+    if constexpr (MODE == 2) {
+        __syncthreads();
+        // inverse radix-r1 pass, butterfly lane < r2: shared -> global
+        radix_dispatch<CLS>(r1, [&](auto rc) {
+            constexpr int RAD = decltype(rc)::value;
+            if (lane < r2) {
+                cplx<R> x[RAD];
+                x[0] = S[lane * CW + c];
+#pragma unroll
+                for (int q = 1; q < RAD; ++q) {
+                    cplx<R> w = T[q * lane];
+                    w.y = -w.y;
+                    x[q] = S[(lane + q * r2) * CW + c] * w;
+                }
+                dft_small<R, true, RAD>(x);
+                if (live) {
+#pragma unroll
+                    for (int p = 0; p < RAD; ++p) line[size_t(p * r2 + lane) * es] = x[p];
+                }
+            }
+        });
+    }
+}
+
+// radices the two-pass kernel has butterflies for
+bool fft2_radix(int r) { return (r >= 1 && r <= 10) || r == 12 || r == 16; }
+
+// (r1, r2) with r1 * r2 = n, both in-register radices, max(r1, r2) smallest
+// (0, 0) when n has no such split
+std::pair<int, int> fft2_split(int n) {
+    std::pair<int, int> best(0, 0);
+    for (int a = 1; a <= 16 && a <= n; ++a) {
+        if (n % a) continue;
+        const int b = n / a;
+        if (!fft2_radix(a) || !fft2_radix(b) || a < b) continue;
+        if (!best.first || a < best.first) best = {a, b};
+    }
+    return best;
+}
+
+size_t fft2_smem(int n, int cw, size_t elem) { return (size_t(n) * cw + n) * elem; }
+
+template <typename R, int MODE, int CW>
+void launch2_cw(int cls, int nblocks, int nthreads, size_t shm, cudaStream_t s, cplx<R>* data, const cplx<R>* tw,
+                int r1, int r2, size_t es, int ncols, size_t os, int ngroups, const LineScale<R>& ks) {
+    auto go = [&](auto kern) {
+        MPM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(shm)));
+        kern<<<nblocks, nthreads, shm, s>>>(data, tw, r1, r2, es, ncols, os, ngroups, ks);
+    };
+    if (cls == 8) go(k_fft2<R, CW, MODE, 8>);
+    else go(k_fft2<R, CW, MODE, 16>);
 }
 
 size_t fft_smem(int n, int cw, size_t elem, int pt_total) {
@@ -390,11 +658,12 @@ int pick_cw(int n, size_t elem, int ncols, int pt_total) {
 }
 
 template <typename R, bool INV, bool KSCALE, int CW>
-void launch_cw(int cls, bool stream, dim3 grd, size_t shm, cudaStream_t s, cplx<R>* data, const FftFactors& f,
+void launch_cw(int cls, bool stream, int nouter, size_t shm, cudaStream_t s, cplx<R>* data, const FftFactors& f,
                const cplx<R>* tw, size_t es, int ncols, size_t os, const cplx<R>* ptw, const LineScale<R>& ks) {
+    const int ngroups = (ncols + CW - 1) / CW;
     auto go = [&](auto kern) {
         MPM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(shm)));
-        kern<<<grd, kFftThreads, shm, s>>>(data, f, tw, es, ncols, os, ptw, ks);
+        kern<<<nouter * ngroups, kFftThreads, shm, s>>>(data, f, tw, es, ncols, os, ptw, ngroups, ks);
     };
     if (stream) {
         if (cls == 8) go(k_fft_axis<R, INV, CW, 8, true, KSCALE>);
@@ -406,7 +675,7 @@ void launch_cw(int cls, bool stream, dim3 grd, size_t shm, cudaStream_t s, cplx<
 }
 
 template <typename R, bool INV, bool KSCALE>
-void launch(int cw, int cls, bool stream, dim3 grd, size_t shm, cudaStream_t s, cplx<R>* data, const FftFactors& f,
+void launch(int cw, int cls, bool stream, int grd, size_t shm, cudaStream_t s, cplx<R>* data, const FftFactors& f,
             const cplx<R>* tw, size_t es, int ncols, size_t os, const cplx<R>* ptw, const LineScale<R>& ks) {
     switch (cw) {
         case 32: launch_cw<R, INV, KSCALE, 32>(cls, stream, grd, shm, s, data, f, tw, es, ncols, os, ptw, ks); break;
@@ -444,6 +713,9 @@ void AxisFFT::init(int n) {
     if (int(rs.size()) > kFftMaxFactors) throw std::runtime_error("FFT length has too many factors");
     f_.nf = int(rs.size());
     for (int i = 0; i < f_.nf; ++i) f_.r[i] = rs[i];
+    const std::pair<int, int> sp = fft2_split(n);
+    r1_ = sp.first;
+    r2_ = sp.second;
     std::vector<double2> t64(n);
     std::vector<float2> t32(n);
     for (int t = 0; t < n; ++t) {
@@ -493,6 +765,35 @@ void AxisFFT::launch_line(cplx<R>* data, size_t es, int ncols, size_t os, int no
                           int sz, int sb, cudaStream_t s) const {
     if (f_.n <= 1 || nouter <= 0 || ncols <= 0) return;
     const int n = f_.n;
+    LineScale<R> ks;
+    ks.sc = scale;
+    ks.nouter = nouter;
+    ks.sz = sz;
+    ks.sb = sb;
+    const cplx<R>* tw = sizeof(R) == 4 ? reinterpret_cast<const cplx<R>*>(tw32_.p)
+                                       : reinterpret_cast<const cplx<R>*>(tw64_.p);
+    if (two_pass(ncols)) {
+        // two-pass in-register transform
+        int cw = 32;
+        while (cw > 16 && (cw * r1_ > kFft2MaxThreads || fft2_smem(n, cw, sizeof(cplx<R>)) > kFftSmemBudget)) cw /= 2;
+        if (cw * r1_ > kFft2MaxThreads) throw std::runtime_error("two-pass FFT: too many threads");
+        const size_t shm = fft2_smem(n, cw, sizeof(cplx<R>));
+        const int ngroups = (ncols + cw - 1) / cw;
+        const int nblocks = nouter * ngroups;
+        const int cls = r1_ <= 8 ? 8 : 16;
+        auto go = [&](auto modec) {
+            constexpr int MODE = decltype(modec)::value;
+            if (cw == 32)
+                launch2_cw<R, MODE, 32>(cls, nblocks, cw * r1_, shm, s, data, tw, r1_, r2_, es, ncols, os, ngroups, ks);
+            else
+                launch2_cw<R, MODE, 16>(cls, nblocks, cw * r1_, shm, s, data, tw, r1_, r2_, es, ncols, os, ngroups, ks);
+        };
+        if (mode == 2) go(std::integral_constant<int, 2>{});
+        else if (mode == 1) go(std::integral_constant<int, 1>{});
+        else go(std::integral_constant<int, 0>{});
+        MPM_LAUNCH();
+        return;
+    }
     // the prime-pass tables go to shared memory when small (else the pass
     // indexes the line's own twiddles)
     FftFactors f = f_;
@@ -502,9 +803,7 @@ void AxisFFT::launch_line(cplx<R>* data, size_t es, int ncols, size_t os, int no
     const int pt_total = f.pt_total;
     const size_t shm = fft_smem(n, cw, sizeof(cplx<R>), pt_total);
     if (shm > kFftSmemMax) throw std::runtime_error("FFT line does not fit in shared memory");
-    const cplx<R>* tw = sizeof(R) == 4 ? reinterpret_cast<const cplx<R>*>(tw32_.p)
-                                       : reinterpret_cast<const cplx<R>*>(tw64_.p);
-    dim3 grd(nouter, (ncols + cw - 1) / cw);
+    const int grd = nouter;
     int rsmall = 1;
     bool stream = false;
     for (int i = 0; i < f_.nf; ++i) {
@@ -514,11 +813,6 @@ void AxisFFT::launch_line(cplx<R>* data, size_t es, int ncols, size_t os, int no
     const int cls = rsmall <= 8 ? 8 : 16;
     const cplx<R>* ptw = sizeof(R) == 4 ? reinterpret_cast<const cplx<R>*>(pt32_.p)
                                         : reinterpret_cast<const cplx<R>*>(pt64_.p);
-    LineScale<R> ks;
-    ks.sc = scale;
-    ks.nouter = nouter;
-    ks.sz = sz;
-    ks.sb = sb;
     if (mode == 2) launch<R, false, true>(cw, cls, stream, grd, shm, s, data, f, tw, es, ncols, os, ptw, ks);
     else if (mode == 1) launch<R, true, false>(cw, cls, stream, grd, shm, s, data, f, tw, es, ncols, os, ptw, ks);
     else launch<R, false, false>(cw, cls, stream, grd, shm, s, data, f, tw, es, ncols, os, ptw, ks);

@@ -44,12 +44,21 @@ public:
                     cudaStream_t s) const;
     // whether one line of this length fits in shared memory
     static bool fits(int n, bool fp64);
+    // the two-pass split n = r1 * r2 (r1 >= r2, in-register radices), or (0, 0)
+    int split_r1() const { return r1_; }
+    int split_r2() const { return r2_; }
+    // run every length through the general multi-pass kernel (tests)
+    void set_force_general(bool v) { force_general_ = v; }
+    // whether a transform of ncols columns takes the two-pass kernel
+    bool two_pass(int ncols) const { return r1_ && ncols >= 16 && !force_general_; }
 
 private:
     template <typename R>
     void launch_line(cplx<R>* data, size_t es, int ncols, size_t os, int nouter, int mode, const R* scale, int sz,
                      int sb, cudaStream_t s) const;
     FftFactors f_;
+    int r1_ = 0, r2_ = 0;
+    bool force_general_ = false;
     DevBuf tw64_, tw32_;
     DevBuf pt64_, pt32_;   // prime-pass twiddle tables (see FftFactors)
 };

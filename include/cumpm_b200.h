@@ -186,6 +186,18 @@ MPM_API int mpm_batch_solve(mpm_field* f, const void* B, void* X, int M, const v
  * No counterpart in the reference (it has no gradients). */
 MPM_API int mpm_field_grad(mpm_field* f, const void* lam, const void* p, int M, void* gx, void* ga, void* stream);
 
+/* Batched 1-D DFT of the spectral-Ewald grids, the in-house replacement of
+ * the reference's cuFFT plans (e.g. the cufftExecC2C / cufftExecZ2Z calls of
+ * src/cpp/electric_field/polydisperse_ewald_electric_field.cu:2577-2627),
+ * exposed for testing: line o, column c, element e at data[o*os + e*es + c] (complex64 or complex128, device memory), c < ncols.
+ * mode 0 forward, 1 inverse (both unnormalised), 2 forward, multiplication of
+ * element e of line o, column c by scale[(e*nouter + o)*sz + c/sb], inverse.
+ * general != 0 forces the multi-pass kernel; split (optional, 2 ints)
+ * receives the two-pass factorisation n = r1 * r2 or (0, 0).  Synchronises
+ * the stream before returning. */
+MPM_API int mpm_line_fft(void* data, int fp64, int n, size_t es, int ncols, size_t os, int nouter, int mode,
+                         const void* scale, int sz, int sb, int general, int* split, void* stream);
+
 /* ---- measurement (no counterpart in the reference) -----------------------
  * Stage timers from CUDA events recorded on the launching stream, read
  * without adding synchronisation to the solve.  Stages: 0 spread, 1 forward
