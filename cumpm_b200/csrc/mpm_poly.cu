@@ -201,10 +201,13 @@ __global__ void __launch_bounds__(256) k_poly_spread(const double2* __restrict__
     cplx<R>* pm = acc + 512 * CM;                                 // [cap][3][CM] candidate moments
     int* runs = reinterpret_cast<int*>(pm + size_t(t.cap) * 3 * CM);  // [cap][8] covered runs
     int* cand = runs + 8 * t.cap;                                 // [cap] particle index
-    const int tile = blockIdx.x;
+    // the column blocks of one tile are adjacent in launch order, so the
+    // candidates' weights are read from DRAM once and then hit in L2
+    const int ncb = (M + CM - 1) / CM;
+    const int tile = blockIdx.x / ncb;
+    const int m0 = (blockIdx.x - tile * ncb) * CM;
     const int bx = tile % t.nb[0], by = (tile / t.nb[0]) % t.nb[1], bz = tile / (t.nb[0] * t.nb[1]);
     const int t0[3] = {bx * 8, by * 8, bz * 8};
-    const int m0 = blockIdx.y * CM;
     const int c0 = toff[tile];
     const int nc = min(toff[tile + 1] - c0, t.cap);
     const int P = t.P, P3 = P * P * P;
@@ -570,7 +573,7 @@ void Field::poly_recip_on(const double2* X, double2* Y, int M, cplx<R>* grid, cu
     const int ntile = ps.nb[0] * ps.nb[1] * ps.nb[2];
     {
         StageScope sc(ST_SPREAD, s);
-        k_poly_spread<R, CM><<<dim3(ntile, (M + CM - 1) / CM), 256, shm, s>>>(
+        k_poly_spread<R, CM><<<ntile * ((M + CM - 1) / CM), 256, shm, s>>>(
             X, M, ps.base.as<int4>(), w1, ptoff_.as<int>(), ptlist_.as<int>(), t, grid);
         MPM_LAUNCH();
     }
