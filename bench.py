@@ -46,10 +46,11 @@ TOL = 1e-6
 XI = 0.5
 N_FREQ = 10
 K_POL = 3
-# GMRES(50)+Jacobi matvecs per right-hand side of the reference algorithm on
-# this workload (fp64 operator, reference stop rule), measured on a B200 by
-# this arm's plain-fp64 leg; used to turn one timed CPU matvec into solves/s.
-PLAIN_MATVECS_PER_SOLVE = 40.0
+# GMRES(50)+Jacobi matvecs per right-hand side of the plain algorithm on each
+# workload (fp64 operator, one right-hand side per solve, tol 1e-6), as the
+# plain-fp64 leg of this script measures them on a B200; used to turn one
+# timed CPU matvec into solves/s when that leg did not run.
+PLAIN_MATVECS_PER_SOLVE = {"monolayer": 15.3, "poly3d": 19.6}
 
 
 def hex_lattice(n, spacing):
@@ -129,6 +130,8 @@ class Workload:
 
 
 METRIC = "solves/s at N=4000, res 1e-6: batched mixed-prec vs plain; matvec % HBM peak"
+METRICS = {"monolayer": METRIC,
+           "poly3d": "solves/s, polydisperse N=1000, 192 RHS, res 1e-6: batched mixed-prec vs plain; matvec % HBM peak"}
 DATA = {"monolayer": "synthetic (hexagonal monolayer generated as in the reference benchmark)",
         "poly3d": "synthetic (seeded random sequential addition of polydisperse spheres)"}
 WORKLOAD_LABEL = ("N=4000 hex monolayer a=5nm spacing 12nm, box 1542.0x332.6x1000nm, Drude "
@@ -369,11 +372,10 @@ def run_ours(args, rank, world, local_rank):
     out = None
     if rank == 0:
         e2e = run_e2e(args, torch, wl) if world == 1 and not args.no_e2e else None
-        per_solve = plain["matvecs_per_solve"] if plain else PLAIN_MATVECS_PER_SOLVE
+        per_solve = plain["matvecs_per_solve"] if plain else PLAIN_MATVECS_PER_SOLVE[args.workload]
         cpu = cpu_baseline(args, wl, per_solve) if world == 1 and not args.no_cpu else None
         out = {
-            "metric": METRIC if wl.name == "monolayer" else
-                      "solves/s, polydisperse N=1000, 192 RHS, res 1e-6: batched mixed-prec vs plain; matvec % HBM peak",
+            "metric": METRICS[wl.name],
             "value": round(value, 3),
             "unit": "solves/s",
             "n_gpus": world,
@@ -515,14 +517,14 @@ def cpu_matvec_sample(threads, wl=None, min_s=10.0, max_n=8):
     x = rng.standard_normal(3 * N) + 1j * rng.standard_normal(3 * N)
     sc = 3.0 / (4 * np.pi * (wl.eps[0] / EPS_M - 1.0)) / wl.radius ** 3
     ts = []
-    while len(ts) < max_n and sum(ts) < min_s:
+    while not ts or (len(ts) < max_n and sum(ts) < min_s):
         t0 = time.perf_counter()
         op.apply(x, sc)
         ts.append(time.perf_counter() - t0)
     return float(np.mean(ts)), len(ts)
 
 
-def cpu_baseline(args, wl, matvecs_per_solve=PLAIN_MATVECS_PER_SOLVE):
+def cpu_baseline(args, wl, matvecs_per_solve):
     threads = os.cpu_count() or 1
     t, n = cpu_matvec_sample(threads, wl)
     v = 1.0 / (t * matvecs_per_solve)
@@ -536,23 +538,28 @@ def run_reference(args, rank):
     if rank != 0:
         return
     threads = os.cpu_count() or 1
+    wl = Workload(args.workload)
+    per_solve = PLAIN_MATVECS_PER_SOLVE[args.workload]
+    # warm-up matvecs untimed, then one timed matvec per step
+    cpu_matvec_sample(threads, wl, min_s=0.0, max_n=max(1, args.warmup))
     ts = []
     for _ in range(max(1, args.steps)):
-        t, _n = cpu_matvec_sample(threads, Workload(args.workload), min_s=0.0, max_n=1)
+        t, _n = cpu_matvec_sample(threads, wl, min_s=0.0, max_n=1)
         ts.append(t)
     t = float(np.median(ts))
-    v = 1.0 / (t * PLAIN_MATVECS_PER_SOLVE)
+    v = 1.0 / (t * per_solve)
     line = {
         "impl": "reference",
-        "metric": METRIC,
+        "metric": METRICS[wl.name],
         "value": round(v, 5), "unit": "solves/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": round(t * 1e3, 1), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "c128", "data": "synthetic (hexagonal monolayer generated as in the reference benchmark)",
-        "config": {"workload": "N=4000 hex monolayer, 30 RHS, tol 1e-6, GMRES(50)+Jacobi, fp64",
-                   "step": "one fp64 matvec of the CPU port of the reference operator (bounded sample)"},
+        "dtype": "c128", "data": DATA[wl.name],
+        "config": {"workload": wl.label,
+                   "step": "one fp64 matvec of the CPU port of the reference operator (bounded sample), "
+                           "the same operator and sizes as the GPU arm's workload"},
         "cpu_baseline": {"value": round(v, 5), "unit": "solves/s", "cores": threads, "kind": "port",
                          "sample": f"1 fp64 matvec per step, median {t:.2f} s; solves/s = 1/(t x "
-                                   f"{PLAIN_MATVECS_PER_SOLVE:g} matvecs per plain fp64 solve)"},
+                                   f"{per_solve:g} matvecs per plain fp64 solve)"},
         "e2e": {"value": round(v, 5), "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
