@@ -8,7 +8,7 @@ to the last bit.  Run:  python gen_fft_consts.py > mpm_fft_consts.cuh
 import math
 from fractions import Fraction as F
 
-RADICES = (7, 9, 10, 12, 16)
+RADICES = (7, 9, 10, 11, 12, 13, 14, 15, 16)
 
 
 def cos_sin(fr):

@@ -388,8 +388,9 @@ int mpm_line_fft(void* data, int fp64, int n, size_t es, int ncols, size_t os, i
         fft.init(n);
         fft.set_force_general(general != 0);
         if (split) {
-            split[0] = fft.two_pass(ncols) ? fft.split_r1() : 0;
-            split[1] = fft.two_pass(ncols) ? fft.split_r2() : 0;
+            const bool two = fft.path(ncols, mode) != 0;
+            split[0] = two ? fft.split_r1() : 0;
+            split[1] = two ? fft.split_r2() : 0;
         }
         const auto st = static_cast<cudaStream_t>(stream);
         if (fp64) {

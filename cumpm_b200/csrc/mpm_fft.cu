@@ -82,17 +82,26 @@ __device__ __forceinline__ void dft_small(cplx<R> (&x)[RAD]);
 template <typename R, bool INV, int N>
 __device__ __forceinline__ cplx<R> wconst(int j) {
     cplx<R> w;
+    static_assert(N == 7 || (N >= 9 && N <= 16), "no constant table for this radix");
     if constexpr (sizeof(R) == 8) {
         if constexpr (N == 7) w = kW7d[j];
         else if constexpr (N == 9) w = kW9d[j];
         else if constexpr (N == 10) w = kW10d[j];
+        else if constexpr (N == 11) w = kW11d[j];
         else if constexpr (N == 12) w = kW12d[j];
+        else if constexpr (N == 13) w = kW13d[j];
+        else if constexpr (N == 14) w = kW14d[j];
+        else if constexpr (N == 15) w = kW15d[j];
         else w = kW16d[j];
     } else {
         if constexpr (N == 7) w = kW7f[j];
         else if constexpr (N == 9) w = kW9f[j];
         else if constexpr (N == 10) w = kW10f[j];
+        else if constexpr (N == 11) w = kW11f[j];
         else if constexpr (N == 12) w = kW12f[j];
+        else if constexpr (N == 13) w = kW13f[j];
+        else if constexpr (N == 14) w = kW14f[j];
+        else if constexpr (N == 15) w = kW15f[j];
         else w = kW16f[j];
     }
     if (INV) w.y = -w.y;
@@ -159,8 +168,8 @@ __device__ __forceinline__ void dft_odd(cplx<R> (&x)[P]) {
 }
 
 // In-register DFT of RAD points, y_p = sum_q x_q W^(p q), W = exp(-+2 pi i/RAD),
-// written out for the radices the grid lengths use (2, 3, 4, 5, 6, 8) and
-// composed or tabulated for 7, 9, 10, 12, 16.
+// written out for 2, 3, 4, 5, 6, 8, tabulated primes 7, 11, 13 and composed
+// 9, 10, 12, 14, 15, 16.
 template <typename R, bool INV, int RAD>
 __device__ __forceinline__ void dft_small(cplx<R> (&x)[RAD]) {
     if constexpr (RAD == 1) {
@@ -170,8 +179,16 @@ __device__ __forceinline__ void dft_small(cplx<R> (&x)[RAD]) {
         dft_ct<R, INV, 3, 3>(x);
     } else if constexpr (RAD == 10) {
         dft_ct<R, INV, 2, 5>(x);
+    } else if constexpr (RAD == 11) {
+        dft_odd<R, INV, 11>(x);
     } else if constexpr (RAD == 12) {
         dft_ct<R, INV, 4, 3>(x);
+    } else if constexpr (RAD == 13) {
+        dft_odd<R, INV, 13>(x);
+    } else if constexpr (RAD == 14) {
+        dft_ct<R, INV, 2, 7>(x);
+    } else if constexpr (RAD == 15) {
+        dft_ct<R, INV, 3, 5>(x);
     } else if constexpr (RAD == 16) {
         dft_ct<R, INV, 4, 4>(x);
     } else if constexpr (RAD == 2) {
@@ -513,7 +530,11 @@ __device__ __forceinline__ void radix_dispatch(int r, Fn&& fn) {
                 switch (r) {
                     case 9: fn(std::integral_constant<int, 9>{}); break;
                     case 10: fn(std::integral_constant<int, 10>{}); break;
+                    case 11: fn(std::integral_constant<int, 11>{}); break;
                     case 12: fn(std::integral_constant<int, 12>{}); break;
+                    case 13: fn(std::integral_constant<int, 13>{}); break;
+                    case 14: fn(std::integral_constant<int, 14>{}); break;
+                    case 15: fn(std::integral_constant<int, 15>{}); break;
                     case 16: fn(std::integral_constant<int, 16>{}); break;
                     default: break;
                 }
@@ -616,8 +637,8 @@ __global__ void __launch_bounds__(kFft2MaxThreads) k_fft2(cplx<R>* __restrict__ 
     }
 }
 
-// radices the two-pass kernel has butterflies for
-bool fft2_radix(int r) { return (r >= 1 && r <= 10) || r == 12 || r == 16; }
+// radices the two-pass kernels have in-register butterflies for
+bool fft2_radix(int r) { return r >= 1 && r <= 16; }
 
 // (r1, r2) with r1 * r2 = n, both in-register radices, max(r1, r2) smallest
 // (0, 0) when n has no such split
@@ -643,6 +664,170 @@ void launch2_cw(int cls, int nblocks, int nthreads, size_t shm, cudaStream_t s, 
     };
     if (cls == 8) go(k_fft2<R, CW, MODE, 8>);
     else go(k_fft2<R, CW, MODE, 16>);
+}
+
+// ---------------------------------------------------------------------------
+// Two-pass line transform for n = r1 * p, r1 an in-register radix and p an
+// odd prime above 16 (the monolayer x axis: 366 = 6 * 61).  Pass 1 (radix
+// r1, butterfly j1 < p) reads x[j1 + q p] straight from global memory and
+// stores S[j1 r1 + p1] already multiplied by pass 2's twiddle W_n^(j1 p1)
+// (pass 2 butterfly j reads S[j + q r1], i.e. j1 = q, p1 = j).  Pass 2 (radix
+// p, butterfly j < r1) streams its inputs from shared memory as the general
+// kernel's prime pass does (a_q = x_q + x_(p-q), b_q = x_q - x_(p-q), PC
+// output pairs per work item, W_p^(p' q) from the table PT in shared memory)
+// and writes y[p' r1 + j] straight to global memory.  One CTA = CW columns
+// of one line; L = blockDim.x / CW lanes loop over pass 1's p butterflies and
+// pass 2's r1 * ceil(((p-1)/2) / PC) work items.
+
+template <typename R, int CW, bool INV, int CLS>
+__global__ void __launch_bounds__(kFft2MaxThreads) k_fft2p(cplx<R>* __restrict__ data, const cplx<R>* __restrict__ tw,
+                                                           const cplx<R>* __restrict__ ptw, int pt_total, int pt_ld,
+                                                           int r1, int p, size_t es, int ncols, size_t os,
+                                                           int ngroups) {
+    constexpr int PC = 8;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int n = r1 * p;
+    const int L = blockDim.x / CW;
+    cplx<R>* S = reinterpret_cast<cplx<R>*>(smem_raw);   // [n][CW]
+    cplx<R>* PT = S + size_t(n) * CW;                      // [pt_total], 16-byte aligned (CW >= 2)
+    cplx<R>* T = PT + pt_total;                            // [n]
+    const int o = blockIdx.x / ngroups;
+    const int g = blockIdx.x - o * ngroups;
+    const int c = threadIdx.x & (CW - 1);
+    const int lane = threadIdx.x / CW;
+    const int c0 = g * CW;
+    const bool live = c0 + c < ncols;
+    cplx<R>* line = data + size_t(o) * os + c0 + c;
+    for (int t = threadIdx.x; t < n; t += blockDim.x) {
+        cplx<R> w = tw[t];
+        if (INV) w.y = -w.y;
+        T[t] = w;
+    }
+    for (int t = threadIdx.x; t < pt_total; t += blockDim.x) PT[t] = ptw[t];
+    __syncthreads();
+    // pass 1: radix r1, global -> shared with pass 2's twiddles applied
+    radix_dispatch<CLS>(r1, [&](auto rc) {
+        constexpr int RAD = decltype(rc)::value;
+#pragma unroll 2
+        for (int j1 = lane; j1 < p; j1 += L) {
+            cplx<R> x[RAD];
+#pragma unroll
+            for (int q = 0; q < RAD; ++q) x[q] = live ? line[size_t(j1 + q * p) * es] : mk<R>(R(0), R(0));
+            dft_small<R, INV, RAD>(x);
+            S[(j1 * RAD) * CW + c] = x[0];
+#pragma unroll
+            for (int p1 = 1; p1 < RAD; ++p1) S[(j1 * RAD + p1) * CW + c] = x[p1] * T[j1 * p1];
+        }
+    });
+    __syncthreads();
+    // pass 2: radix p streamed from shared memory, outputs to global memory
+    const int half = (p - 1) / 2;
+    const int nchunk = (half + PC - 1) / PC;
+    for (int u = lane; u < r1 * nchunk; u += L) {
+        const int ch = u / r1;
+        const int j = u - ch * r1;
+        const int p0 = 1 + ch * PC;
+        const cplx<R> x0 = S[j * CW + c];
+        R px[PC], py[PC], qx[PC], qy[PC];
+#pragma unroll
+        for (int k = 0; k < PC; ++k) px[k] = py[k] = qx[k] = qy[k] = R(0);
+        R sx = R(0), sy = R(0);
+        const cplx<R>* prow = PT + (p0 - 1);
+        for (int q = 1; q <= half; ++q, prow += pt_ld) {
+            const cplx<R> xa = S[(j + q * r1) * CW + c];
+            const cplx<R> xb = S[(j + (p - q) * r1) * CW + c];
+            const R ax = xa.x + xb.x, ay = xa.y + xb.y, bx = xa.x - xb.x, by = xa.y - xb.y;
+            sx += ax;
+            sy += ay;
+            cplx<R> wk[PC];
+            if constexpr (sizeof(R) == 4) {
+                const float4* p4 = reinterpret_cast<const float4*>(prow);
+#pragma unroll
+                for (int k = 0; k < PC / 2; ++k) {
+                    const float4 v = p4[k];
+                    wk[2 * k] = mk<R>(v.x, v.y);
+                    wk[2 * k + 1] = mk<R>(v.z, v.w);
+                }
+            } else {
+#pragma unroll
+                for (int k = 0; k < PC; ++k) wk[k] = prow[k];
+            }
+#pragma unroll
+            for (int k = 0; k < PC; ++k) {
+                const R wy = INV ? -wk[k].y : wk[k].y;
+                px[k] = fma(ax, wk[k].x, px[k]);
+                py[k] = fma(ay, wk[k].x, py[k]);
+                qx[k] = fma(bx, wy, qx[k]);
+                qy[k] = fma(by, wy, qy[k]);
+            }
+        }
+        if (!live) continue;
+        if (ch == 0) line[size_t(j) * es] = mk<R>(x0.x + sx, x0.y + sy);
+#pragma unroll
+        for (int k = 0; k < PC; ++k) {
+            const int pp = p0 + k;
+            if (pp <= half) {
+                line[size_t(pp * r1 + j) * es] = mk<R>(x0.x + px[k] - qy[k], x0.y + py[k] + qx[k]);
+                line[size_t((p - pp) * r1 + j) * es] = mk<R>(x0.x + px[k] + qy[k], x0.y + py[k] - qx[k]);
+            }
+        }
+    }
+}
+
+// W_r^(p q) table of a streamed prime pass: rows q = 1..(r-1)/2, columns
+// p = 1..(r-1)/2 padded to a multiple of 8 with zeros, plus 8 spare entries
+// so that a padded row can always be read whole.  Appended to `out`; returns
+// the row length.
+int append_prime_table(int r, std::vector<double2>& out) {
+    const int half = (r - 1) / 2;
+    const int ld = (half + 7) / 8 * 8;
+    for (int q = 1; q <= half; ++q)
+        for (int c = 0; c < ld; ++c) {
+            const int p = c + 1;
+            if (p > half) {
+                out.push_back(make_double2(0.0, 0.0));
+                continue;
+            }
+            const double a = -2.0 * kPi * double((long long)p * q % r) / double(r);
+            out.push_back(make_double2(std::cos(a), std::sin(a)));
+        }
+    for (int c = 0; c < 8; ++c) out.push_back(make_double2(0.0, 0.0));
+    return ld;
+}
+
+bool is_prime(int m) {
+    if (m < 2) return false;
+    for (int d = 2; d * d <= m; ++d)
+        if (m % d == 0) return false;
+    return true;
+}
+
+// (r1, p) with n = r1 * p, p the largest prime factor, p > 16, r1 an
+// in-register radix; (0, 0) otherwise
+std::pair<int, int> fft2p_split(int n) {
+    int p = 1, m = n;
+    for (int d = 2; d * d <= m; ++d)
+        while (m % d == 0) {
+            p = std::max(p, d);
+            m /= d;
+        }
+    if (m > 1) p = std::max(p, m);
+    if (p <= 16 || !is_prime(p) || !fft2_radix(n / p)) return {0, 0};
+    return {n / p, p};
+}
+
+size_t fft2p_smem(int n, int cw, size_t elem, int pt_total) { return (size_t(n) * cw + pt_total + n) * elem; }
+
+template <typename R, bool INV, int CW>
+void launch2p_cw(int cls, int nblocks, int nthreads, size_t shm, cudaStream_t s, cplx<R>* data, const cplx<R>* tw,
+                 const cplx<R>* ptw, int pt_total, int pt_ld, int r1, int p, size_t es, int ncols, size_t os,
+                 int ngroups) {
+    auto go = [&](auto kern) {
+        MPM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(shm)));
+        kern<<<nblocks, nthreads, shm, s>>>(data, tw, ptw, pt_total, pt_ld, r1, p, es, ncols, os, ngroups);
+    };
+    if (cls == 8) go(k_fft2p<R, CW, INV, 8>);
+    else go(k_fft2p<R, CW, INV, 16>);
 }
 
 size_t fft_smem(int n, int cw, size_t elem, int pt_total) {
@@ -713,7 +898,12 @@ void AxisFFT::init(int n) {
     if (int(rs.size()) > kFftMaxFactors) throw std::runtime_error("FFT length has too many factors");
     f_.nf = int(rs.size());
     for (int i = 0; i < f_.nf; ++i) f_.r[i] = rs[i];
-    const std::pair<int, int> sp = fft2_split(n);
+    std::pair<int, int> sp = fft2_split(n);
+    kind_ = sp.first ? 1 : 0;
+    if (!kind_) {
+        sp = fft2p_split(n);
+        kind_ = sp.first ? 2 : 0;
+    }
     r1_ = sp.first;
     r2_ = sp.second;
     std::vector<double2> t64(n);
@@ -727,37 +917,33 @@ void AxisFFT::init(int n) {
     tw32_.ensure(sizeof(float2) * n);
     MPM_CUDA(cudaMemcpy(tw64_.p, t64.data(), sizeof(double2) * n, cudaMemcpyHostToDevice));
     MPM_CUDA(cudaMemcpy(tw32_.p, t32.data(), sizeof(float2) * n, cudaMemcpyHostToDevice));
-    // W_r^(p q) tables of the streamed (r > 16) passes, rows padded to a
-    // multiple of 8 entries (the streamed pass reads 8 outputs per thread)
+    // W_r^(p q) tables of the general kernel's streamed (r > 16) passes
     std::vector<double2> p64;
     for (int i = 0; i < f_.nf; ++i) {
-        const int r = f_.r[i];
-        if (r <= 16) continue;
-        const int half = (r - 1) / 2;
-        const int ld = (half + 7) / 8 * 8;
+        if (f_.r[i] <= 16) continue;
         f_.pt_off[i] = int(p64.size());
-        f_.pt_ld[i] = ld;
-        for (int q = 1; q <= half; ++q)
-            for (int c = 0; c < ld; ++c) {
-                const int p = c + 1;
-                if (p > half) {
-                    p64.push_back(make_double2(0.0, 0.0));
-                    continue;
-                }
-                const double a = -2.0 * kPi * double((long long)p * q % r) / double(r);
-                p64.push_back(make_double2(std::cos(a), std::sin(a)));
-            }
-        // 8 spare entries so a padded row can always be read as a whole
-        for (int c = 0; c < 8; ++c) p64.push_back(make_double2(0.0, 0.0));
+        f_.pt_ld[i] = append_prime_table(f_.r[i], p64);
     }
     f_.pt_total = int(p64.size());
-    if (p64.empty()) p64.push_back(make_double2(0.0, 0.0));
-    std::vector<float2> p32(p64.size());
-    for (size_t k = 0; k < p64.size(); ++k) p32[k] = make_float2(float(p64[k].x), float(p64[k].y));
-    pt64_.ensure(sizeof(double2) * p64.size());
-    pt32_.ensure(sizeof(float2) * p64.size());
-    MPM_CUDA(cudaMemcpy(pt64_.p, p64.data(), sizeof(double2) * p64.size(), cudaMemcpyHostToDevice));
-    MPM_CUDA(cudaMemcpy(pt32_.p, p32.data(), sizeof(float2) * p32.size(), cudaMemcpyHostToDevice));
+    upload_table(p64, pt64_, pt32_);
+    // the prime-streamed two-pass kernel's table
+    pp_total_ = pp_ld_ = 0;
+    if (kind_ == 2) {
+        std::vector<double2> q64;
+        pp_ld_ = append_prime_table(r2_, q64);
+        pp_total_ = int(q64.size());
+        upload_table(q64, pp64_, pp32_);
+    }
+}
+
+void AxisFFT::upload_table(std::vector<double2> t64, DevBuf& d64, DevBuf& d32) {
+    if (t64.empty()) t64.push_back(make_double2(0.0, 0.0));
+    std::vector<float2> t32(t64.size());
+    for (size_t k = 0; k < t64.size(); ++k) t32[k] = make_float2(float(t64[k].x), float(t64[k].y));
+    d64.ensure(sizeof(double2) * t64.size());
+    d32.ensure(sizeof(float2) * t32.size());
+    MPM_CUDA(cudaMemcpy(d64.p, t64.data(), sizeof(double2) * t64.size(), cudaMemcpyHostToDevice));
+    MPM_CUDA(cudaMemcpy(d32.p, t32.data(), sizeof(float2) * t32.size(), cudaMemcpyHostToDevice));
 }
 
 template <typename R>
@@ -772,10 +958,46 @@ void AxisFFT::launch_line(cplx<R>* data, size_t es, int ncols, size_t os, int no
     ks.sb = sb;
     const cplx<R>* tw = sizeof(R) == 4 ? reinterpret_cast<const cplx<R>*>(tw32_.p)
                                        : reinterpret_cast<const cplx<R>*>(tw64_.p);
-    if (two_pass(ncols)) {
+    const int kind = path(ncols, mode);
+    if (kind == 2) {
+        // two-pass with a streamed prime pass
+        const int half = (r2_ - 1) / 2;
+        const int nitems = r1_ * ((half + 7) / 8);
+        const int L = std::min(32, std::max(16, nitems));
+        int cw = 16;
+        while (cw > 4 && (cw * L > kFft2MaxThreads ||
+                          fft2p_smem(n, cw, sizeof(cplx<R>), pp_total_) > kFftSmemBudget))
+            cw /= 2;
+        const size_t shm = fft2p_smem(n, cw, sizeof(cplx<R>), pp_total_);
+        const int ngroups = (ncols + cw - 1) / cw;
+        const int nblocks = nouter * ngroups;
+        const int cls = r1_ <= 8 ? 8 : 16;
+        const cplx<R>* ptw = sizeof(R) == 4 ? reinterpret_cast<const cplx<R>*>(pp32_.p)
+                                            : reinterpret_cast<const cplx<R>*>(pp64_.p);
+        auto go = [&](auto invc) {
+            constexpr bool INV = decltype(invc)::value;
+            if (cw == 16)
+                launch2p_cw<R, INV, 16>(cls, nblocks, cw * L, shm, s, data, tw, ptw, pp_total_, pp_ld_, r1_, r2_, es,
+                                        ncols, os, ngroups);
+            else if (cw == 8)
+                launch2p_cw<R, INV, 8>(cls, nblocks, cw * L, shm, s, data, tw, ptw, pp_total_, pp_ld_, r1_, r2_, es,
+                                       ncols, os, ngroups);
+            else
+                launch2p_cw<R, INV, 4>(cls, nblocks, cw * L, shm, s, data, tw, ptw, pp_total_, pp_ld_, r1_, r2_, es,
+                                       ncols, os, ngroups);
+        };
+        if (mode == 1) go(std::true_type{});
+        else go(std::false_type{});
+        MPM_LAUNCH();
+        return;
+    }
+    if (kind == 1) {
         // two-pass in-register transform
+        // fp64 butterflies hold twice the registers: smaller CTAs keep two
+        // of them resident per SM
+        const int maxthr = sizeof(R) == 8 ? 192 : kFft2MaxThreads;
         int cw = 32;
-        while (cw > 16 && (cw * r1_ > kFft2MaxThreads || fft2_smem(n, cw, sizeof(cplx<R>)) > kFftSmemBudget)) cw /= 2;
+        while (cw > 16 && (cw * r1_ > maxthr || fft2_smem(n, cw, sizeof(cplx<R>)) > kFftSmemBudget)) cw /= 2;
         if (cw * r1_ > kFft2MaxThreads) throw std::runtime_error("two-pass FFT: too many threads");
         const size_t shm = fft2_smem(n, cw, sizeof(cplx<R>));
         const int ngroups = (ncols + cw - 1) / cw;

@@ -13,6 +13,8 @@
 
 #include "mpm_common.cuh"
 
+#include <vector>
+
 namespace mpm {
 
 constexpr int kFftMaxFactors = 16;
@@ -44,23 +46,33 @@ public:
                     cudaStream_t s) const;
     // whether one line of this length fits in shared memory
     static bool fits(int n, bool fp64);
-    // the two-pass split n = r1 * r2 (r1 >= r2, in-register radices), or (0, 0)
+    // the two-pass split n = r1 * r2: both in-register radices (r1 >= r2), or
+    // r1 in-register and r2 a prime above 16 (streamed); (0, 0) if neither
     int split_r1() const { return r1_; }
     int split_r2() const { return r2_; }
     // run every length through the general multi-pass kernel (tests)
     void set_force_general(bool v) { force_general_ = v; }
-    // whether a transform of ncols columns takes the two-pass kernel
-    bool two_pass(int ncols) const { return r1_ && ncols >= 16 && !force_general_; }
+    // kernel a transform of ncols columns takes: 0 general multi-pass,
+    // 1 two-pass in registers, 2 two-pass with a streamed prime pass (modes
+    // 0 forward, 1 inverse, 2 forward-scale-inverse; 2 has no prime variant)
+    int path(int ncols, int mode) const {
+        if (!r1_ || ncols < 16 || force_general_) return 0;
+        if (kind_ == 2 && mode == 2) return 0;
+        return kind_;
+    }
 
 private:
     template <typename R>
     void launch_line(cplx<R>* data, size_t es, int ncols, size_t os, int nouter, int mode, const R* scale, int sz,
                      int sb, cudaStream_t s) const;
+    static void upload_table(std::vector<double2> t64, DevBuf& d64, DevBuf& d32);
     FftFactors f_;
-    int r1_ = 0, r2_ = 0;
+    int kind_ = 0, r1_ = 0, r2_ = 0;
     bool force_general_ = false;
     DevBuf tw64_, tw32_;
     DevBuf pt64_, pt32_;   // prime-pass twiddle tables (see FftFactors)
+    DevBuf pp64_, pp32_;   // the prime-streamed two-pass kernel's W_p^(p' q) table
+    int pp_total_ = 0, pp_ld_ = 0;
 };
 
 }  // namespace mpm

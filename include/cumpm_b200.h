@@ -193,7 +193,8 @@ MPM_API int mpm_field_grad(mpm_field* f, const void* lam, const void* p, int M, 
  * mode 0 forward, 1 inverse (both unnormalised), 2 forward, multiplication of
  * element e of line o, column c by scale[(e*nouter + o)*sz + c/sb], inverse.
  * general != 0 forces the multi-pass kernel; split (optional, 2 ints)
- * receives the two-pass factorisation n = r1 * r2 or (0, 0).  Synchronises
+ * receives the two-pass factorisation n = r1 * r2 that ran (r2 above 16 is
+ * a prime handled by the streamed pass) or (0, 0) for the multi-pass kernel.  Synchronises
  * the stream before returning. */
 MPM_API int mpm_line_fft(void* data, int fp64, int n, size_t es, int ncols, size_t os, int nouter, int mode,
                          const void* scale, int sz, int sb, int general, int* split, void* stream);
