@@ -103,6 +103,7 @@ __global__ void k_stencil(const double* __restrict__ xyz, int n, StencilArgs a, 
 // non-zero are listed once (in candidate order, so sums are deterministic),
 // and each voxel then loops only over its column's list.
 constexpr int kSpreadListCap = 64;
+constexpr int kSpreadZMax = 16;   // largest z extent of a spread tile
 
 template <typename R>
 __global__ void __launch_bounds__(256) k_spread(const double2* __restrict__ X, int M, int N, int C,
@@ -149,7 +150,6 @@ __global__ void __launch_bounds__(256) k_spread(const double2* __restrict__ X, i
     int* lc = reinterpret_cast<int*>(lw + size_t(ncol) * kSpreadListCap);          // [ncol][cap_l]
     int* ln = lc + size_t(ncol) * kSpreadListCap;                                  // [ncol]
     int* cid = ln + ncol;                                                          // [cap]
-    const int nvox = TX * TY * TZ;
     for (int r0 = 0; r0 < max(total, 1); r0 += cap) {
         const int nc = min(cap, total - r0);
         // candidate ids
@@ -223,30 +223,48 @@ __global__ void __launch_bounds__(256) k_spread(const double2* __restrict__ X, i
                 pv[c * bc + bb] = to_r<R>(v);
             }
             __syncthreads();
-            for (int t = threadIdx.x; t < nvox * nb; t += blockDim.x) {
-                const int bb = t % nb, vox = t / nb;
-                const int lz = vox % TZ, ly = (vox / TZ) % TY, lx = vox / (TZ * TY);
-                const int x = x0 + lx, y = y0 + ly, s = z0 + lz;
-                if (x >= g.Nx || y >= g.Ny || s >= g.Zs) continue;
-                const int col = lx * TY + ly;
+            // thread = one (x, y) column of the tile x one grid column bb,
+            // all TZ z slots in registers: a contributor's moment and x-y
+            // weight are read once for the whole z run
+            for (int t = threadIdx.x; t < ncol * nb; t += blockDim.x) {
+                const int bb = t % nb, col = t / nb;
+                const int lx = col / TY, ly = col % TY;
+                const int x = x0 + lx, y = y0 + ly;
+                if (x >= g.Nx || y >= g.Ny) continue;
                 const int nl = ln[col];
-                cplx<R> acc = mk<R>(0, 0);
+                cplx<R> acc[kSpreadZMax];
+#pragma unroll
+                for (int lz = 0; lz < kSpreadZMax; ++lz) acc[lz] = mk<R>(0, 0);
                 if (nl >= 0) {
                     const R* lwc = lw + col * kSpreadListCap;
                     const int* lcc = lc + col * kSpreadListCap;
                     for (int k = 0; k < nl; ++k) {
                         const int c = lcc[k];
-                        fma_rc(acc, lwc[k] * wT[c * wlen + TX + TY + lz], pv[c * bc + bb]);
+                        const R wxy = lwc[k];
+                        const cplx<R> pc = pv[c * bc + bb];
+                        const R* wz = wT + c * wlen + TX + TY;
+#pragma unroll
+                        for (int lz = 0; lz < kSpreadZMax; ++lz)
+                            if (lz < TZ) fma_rc(acc[lz], wxy * wz[lz], pc);
                     }
                 } else {
                     for (int c = 0; c < nc; ++c) {
                         const R* wc = wT + c * wlen;
-                        fma_rc(acc, wc[lx] * wc[TX + ly] * wc[TX + TY + lz], pv[c * bc + bb]);
+                        const R wxy = wc[lx] * wc[TX + ly];
+                        const cplx<R> pc = pv[c * bc + bb];
+#pragma unroll
+                        for (int lz = 0; lz < kSpreadZMax; ++lz)
+                            if (lz < TZ) fma_rc(acc[lz], wxy * wc[TX + TY + lz], pc);
                     }
                 }
-                const size_t o = ((size_t(x) * g.Ny + y) * g.Zs + s) * B + b0 + bb;
-                if (r0 == 0) grid[o] = acc;
-                else grid[o] += acc;
+                const size_t o0 = ((size_t(x) * g.Ny + y) * g.Zs + z0) * B + b0 + bb;
+#pragma unroll
+                for (int lz = 0; lz < kSpreadZMax; ++lz) {
+                    if (lz >= TZ || z0 + lz >= g.Zs) break;
+                    const size_t o = o0 + size_t(lz) * B;
+                    if (r0 == 0) grid[o] = acc[lz];
+                    else grid[o] += acc[lz];
+                }
             }
         }
         __syncthreads();
@@ -432,7 +450,9 @@ __global__ void k_column(cplx<R>* __restrict__ grid, const cplx<R>* __restrict__
 // Contraction: field at each target from its Gaussian stencil for all B
 // columns (contract_kernel, monodisperse_ewald_electric_field.cu:1488-1587).
 // Writes Y rows (overwrites).  C = 3 (dipoles) or 8 (plus field gradient).
-template <typename R>
+// SZ > 0: the stencil's z run (g.S <= SZ) unrolled, so that its grid loads
+// are in flight together; SZ = 0: any stencil length.
+template <typename R, int SZ>
 __global__ void k_contract(const cplx<R>* __restrict__ grid, GridView g, int M, int C, int Nt,
                            const int4* __restrict__ base, const R* __restrict__ w1, double factor,
                            const int* __restrict__ quad_map, double2* __restrict__ Y, int negate,
@@ -464,8 +484,18 @@ __global__ void k_contract(const cplx<R>* __restrict__ grid, GridView g, int M, 
                 const R wxy = wx * w[g.S + oy];
                 const size_t rxy = (rx + idx[g.S + oy]) * g.Zs;
                 cplx<R> a2 = mk<R>(0, 0);
-                for (int oz = 0; oz < g.S; ++oz) {
-                    fma_rc(a2, w[2 * g.S + oz], grid[(rxy + idx[2 * g.S + oz]) * B + b]);
+                if constexpr (SZ > 0) {
+                    cplx<R> v[SZ];
+#pragma unroll
+                    for (int oz = 0; oz < SZ; ++oz)
+                        if (oz < g.S) v[oz] = grid[(rxy + idx[2 * g.S + oz]) * B + b];
+#pragma unroll
+                    for (int oz = 0; oz < SZ; ++oz)
+                        if (oz < g.S) fma_rc(a2, w[2 * g.S + oz], v[oz]);
+                } else {
+                    for (int oz = 0; oz < g.S; ++oz) {
+                        fma_rc(a2, w[2 * g.S + oz], grid[(rxy + idx[2 * g.S + oz]) * B + b]);
+                    }
                 }
                 fma_rc(acc, wxy, a2);
             }
@@ -1300,9 +1330,14 @@ void Field::recip_on(const double2* X, double2* Y, int M, cplx<R>* grid, cudaStr
     const double factor = geom_.h[0] * geom_.h[1] * geom_.h[2];
     const R* tw = sizeof(R) == 4 ? reinterpret_cast<const R*>(tg.w32.p) : reinterpret_cast<const R*>(tg.w64.p);
     const int thr = std::min(256, ((B + 31) / 32) * 32);
-    k_contract<R><<<nt, thr, 0, s>>>(grid, gv_, M, C, nt, tg.base.as<int4>(), tw, factor,
-                                     spec_.solver_ax ? quad_map_.as<int>() : nullptr, Y, 0,
-                                     spec_.solver_ax ? sources_.idx_sorted.as<int>() : nullptr);
+    auto contract = [&](auto kern) {
+        kern<<<nt, thr, 0, s>>>(grid, gv_, M, C, nt, tg.base.as<int4>(), tw, factor,
+                                spec_.solver_ax ? quad_map_.as<int>() : nullptr, Y, 0,
+                                spec_.solver_ax ? sources_.idx_sorted.as<int>() : nullptr);
+    };
+    if (gv_.S <= 9) contract(k_contract<R, 9>);
+    else if (gv_.S <= 13) contract(k_contract<R, 13>);
+    else contract(k_contract<R, 0>);
     MPM_LAUNCH();
 }
 
