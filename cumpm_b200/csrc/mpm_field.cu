@@ -188,21 +188,26 @@ __global__ void __launch_bounds__(256) k_spread(const double2* __restrict__ X, i
             wT[c * wlen + l] = w;
         }
         __syncthreads();
-        // contributor list per (x, y) column, -1 = too many (full loop)
-        for (int col = threadIdx.x; col < ncol; col += blockDim.x) {
-            const int lx = col / TY, ly = col % TY;
-            int n = 0;
-            for (int c = 0; c < nc; ++c) {
-                const R wxy = wT[c * wlen + lx] * wT[c * wlen + TX + ly];
-                if (wxy != R(0)) {
-                    if (n < kSpreadListCap) {
-                        lw[col * kSpreadListCap + n] = wxy;
-                        lc[col * kSpreadListCap + n] = c;
+        // contributor list per (x, y) column in candidate order, -1 = too
+        // many (full loop): one warp per column, 32 candidates per ballot
+        {
+            const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+            for (int col = warp; col < ncol; col += nwarp) {
+                const int lx = col / TY, ly = col % TY;
+                int n = 0;
+                for (int cb = 0; cb < nc; cb += 32) {
+                    const int c = cb + lane;
+                    const R wxy = c < nc ? wT[c * wlen + lx] * wT[c * wlen + TX + ly] : R(0);
+                    const unsigned hit = __ballot_sync(0xffffffffu, wxy != R(0));
+                    const int at = n + __popc(hit & ((1u << lane) - 1u));
+                    if (wxy != R(0) && at < kSpreadListCap) {
+                        lw[col * kSpreadListCap + at] = wxy;
+                        lc[col * kSpreadListCap + at] = c;
                     }
-                    ++n;
+                    n += __popc(hit);
                 }
+                if (lane == 0) ln[col] = n <= kSpreadListCap ? n : -1;
             }
-            ln[col] = n <= kSpreadListCap ? n : -1;
         }
         {
             const int b0 = chunk * bc;
@@ -477,6 +482,17 @@ __global__ void k_contract(const cplx<R>* __restrict__ grid, GridView g, int M, 
         const int comp = b / M;
         if (comp >= 3 && q < 0) continue;
         cplx<R> acc = mk<R>(0, 0);
+        // the z weights and z offsets are the same for every (x, y) of the
+        // stencil: keep them in registers
+        R wz[SZ > 0 ? SZ : 1];
+        int zo[SZ > 0 ? SZ : 1];   // < Zs * B
+        if constexpr (SZ > 0) {
+#pragma unroll
+            for (int oz = 0; oz < SZ; ++oz) {
+                wz[oz] = oz < g.S ? w[2 * g.S + oz] : R(0);
+                zo[oz] = oz < g.S ? idx[2 * g.S + oz] * B + b : b;
+            }
+        }
         for (int ox = 0; ox < g.S; ++ox) {
             const R wx = w[ox];
             const size_t rx = size_t(idx[ox]) * g.Ny;
@@ -485,13 +501,14 @@ __global__ void k_contract(const cplx<R>* __restrict__ grid, GridView g, int M, 
                 const size_t rxy = (rx + idx[g.S + oy]) * g.Zs;
                 cplx<R> a2 = mk<R>(0, 0);
                 if constexpr (SZ > 0) {
+                    const cplx<R>* gp = grid + rxy * B;
                     cplx<R> v[SZ];
 #pragma unroll
                     for (int oz = 0; oz < SZ; ++oz)
-                        if (oz < g.S) v[oz] = grid[(rxy + idx[2 * g.S + oz]) * B + b];
+                        if (oz < g.S) v[oz] = gp[zo[oz]];
 #pragma unroll
                     for (int oz = 0; oz < SZ; ++oz)
-                        if (oz < g.S) fma_rc(a2, w[2 * g.S + oz], v[oz]);
+                        if (oz < g.S) fma_rc(a2, wz[oz], v[oz]);
                 } else {
                     for (int oz = 0; oz < g.S; ++oz) {
                         fma_rc(a2, w[2 * g.S + oz], grid[(rxy + idx[2 * g.S + oz]) * B + b]);
