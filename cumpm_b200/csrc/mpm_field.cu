@@ -276,6 +276,212 @@ __global__ void __launch_bounds__(256) k_spread(const double2* __restrict__ X, i
     }
 }
 
+// ---------------------------------------------------------------------------
+// Spread plan, built once per frame (positions are fixed during a solve).
+// For every tile: the candidate particles whose stencil reaches it (in bin
+// order, the order k_spread uses), their 1-D weights restricted to the tile,
+// and every (x, y) column's contributor list, so that a spread launch only
+// loads moments and accumulates.  pass 0 counts each tile's candidates (and
+// the largest count); pass 1 writes the plan at capT entries per tile.
+constexpr int kPlanCandMax = 256;   // candidates of one tile the plan kernel can hold
+
+__global__ void __launch_bounds__(256) k_spread_plan(const int4* __restrict__ base, const double* __restrict__ w1,
+                                                     const int* __restrict__ bin_start,
+                                                     const int* __restrict__ bin_end,
+                                                     const int* __restrict__ sorted_idx, GridView g, int TX, int TY,
+                                                     int TZ, int nbx, int nby, int pass, int capT,
+                                                     int* __restrict__ ncT, int* __restrict__ maxc,
+                                                     int* __restrict__ overflow, int* __restrict__ cidT,
+                                                     double* __restrict__ w64T, float* __restrict__ w32T,
+                                                     double* __restrict__ lw64, float* __restrict__ lw32,
+                                                     int* __restrict__ lcT, int* __restrict__ lnT) {
+    __shared__ int bx[8], by[8], bz[8], nbxs, nbys, nbzs;
+    __shared__ int rstart[512], rlen[512], rpre[513], nranges;
+    __shared__ int cand[kPlanCandMax];
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double* wloc = reinterpret_cast<double*>(smem_raw);   // [kPlanCandMax][wlen]
+    const int tile = blockIdx.x;
+    const int tx = tile % nbx, ty = (tile / nbx) % nby, zt = tile / (nbx * nby);
+    const int x0 = tx * TX, y0 = ty * TY, z0 = zt * TZ;
+    const int x1 = min(x0 + TX, g.Nx), y1 = min(y0 + TY, g.Ny), z1 = min(z0 + TZ, g.Zs);
+    if (threadIdx.x == 0) {
+        nbxs = reach_bins(x0 - g.off, x1 - 1 + g.off, g.Nx, TX, true, bx);
+        nbys = reach_bins(y0 - g.off, y1 - 1 + g.off, g.Ny, TY, true, by);
+        nbzs = reach_bins(z0 - g.off, z1 - 1 + g.off, g.Zs, TZ, !g.pruned, bz);
+        int k = 0;
+        rpre[0] = 0;
+        for (int a = 0; a < nbzs; ++a)
+            for (int b2 = 0; b2 < nbys; ++b2)
+                for (int c = 0; c < nbxs; ++c) {
+                    const int key = (bz[a] * nby + by[b2]) * nbx + bx[c];
+                    const int s0 = bin_start[key];
+                    if (s0 < 0 || k >= 512) continue;
+                    rstart[k] = s0;
+                    rlen[k] = bin_end[key] - s0;
+                    rpre[k + 1] = rpre[k] + rlen[k];
+                    ++k;
+                }
+        nranges = k;
+    }
+    __syncthreads();
+    const int total = rpre[nranges];
+    if (total > kPlanCandMax) {
+        if (threadIdx.x == 0) atomicOr(overflow, 1);
+        return;
+    }
+    const int wlen = TX + TY + TZ;
+    const int ncol = TX * TY;
+    for (int t = threadIdx.x; t < total; t += blockDim.x) {
+        int k = 0;
+        while (rpre[k + 1] <= t) ++k;
+        cand[t] = sorted_idx[rstart[k] + t - rpre[k]];
+    }
+    __syncthreads();
+    for (int t = threadIdx.x; t < total * wlen; t += blockDim.x) {
+        const int c = t / wlen, l = t % wlen;
+        const int i = cand[c];
+        const int4 bs = base[i];
+        double w = 0.0;
+        if (l < TX) {
+            const int x = x0 + l;
+            if (x < g.Nx) {
+                const int d = cyc_diff(x, bs.x, g.Nx);
+                if (d >= -g.off && d <= g.off) w = w1[(size_t(i) * 3 + 0) * g.S + d + g.off];
+            }
+        } else if (l < TX + TY) {
+            const int y = y0 + l - TX;
+            if (y < g.Ny) {
+                const int d = cyc_diff(y, bs.y, g.Ny);
+                if (d >= -g.off && d <= g.off) w = w1[(size_t(i) * 3 + 1) * g.S + d + g.off];
+            }
+        } else {
+            const int s = z0 + l - TX - TY;
+            if (s < g.Zs) {
+                const int d = g.pruned ? (s - bs.z) : cyc_diff(s, bs.z, g.Nz);
+                if (d >= -g.off && d <= g.off) w = w1[(size_t(i) * 3 + 2) * g.S + d + g.off];
+            }
+        }
+        wloc[c * wlen + l] = w;
+    }
+    __syncthreads();
+    if (pass == 0) {
+        if (threadIdx.x == 0) {
+            ncT[tile] = total;
+            atomicMax(maxc, total);
+        }
+        return;
+    }
+    const size_t trow = size_t(tile) * capT;
+    for (int t = threadIdx.x; t < total; t += blockDim.x) cidT[trow + t] = cand[t];
+    for (int t = threadIdx.x; t < total * wlen; t += blockDim.x) {
+        w64T[trow * wlen + t] = wloc[t];
+        w32T[trow * wlen + t] = static_cast<float>(wloc[t]);
+    }
+    // contributor list per (x, y) column in candidate order, -1 = too many
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+    for (int col = warp; col < ncol; col += nwarp) {
+        const int lx = col / TY, ly = col % TY;
+        const size_t lrow = (size_t(tile) * ncol + col) * kSpreadListCap;
+        int n = 0;
+        for (int cb = 0; cb < total; cb += 32) {
+            const int c = cb + lane;
+            const double wxy = c < total ? wloc[c * wlen + lx] * wloc[c * wlen + TX + ly] : 0.0;
+            // the fp32 kernel multiplies the fp32 weights
+            const float wxy32 = c < total ? static_cast<float>(wloc[c * wlen + lx]) *
+                                                static_cast<float>(wloc[c * wlen + TX + ly])
+                                          : 0.f;
+            const unsigned hit = __ballot_sync(0xffffffffu, wxy != 0.0);
+            const int at = n + __popc(hit & ((1u << lane) - 1u));
+            if (wxy != 0.0 && at < kSpreadListCap) {
+                lw64[lrow + at] = wxy;
+                lw32[lrow + at] = wxy32;
+                lcT[lrow + at] = c;
+            }
+            n += __popc(hit);
+        }
+        if (lane == 0) lnT[size_t(tile) * ncol + col] = n <= kSpreadListCap ? n : -1;
+    }
+}
+
+// Spread with the per-frame plan: CTA = one tile x one chunk of bc grid
+// columns; loads the tile's candidate moments, then thread = one (x, y)
+// column x one grid column with the whole z run in registers.  The same
+// contributors in the same order as k_spread.
+template <typename R>
+__global__ void __launch_bounds__(256) k_spread_planned(const double2* __restrict__ X, int M, int N, int C,
+                                                        const int* __restrict__ quad_map, GridView g, int TX,
+                                                        int TY, int TZ, int nbx, int nby, int nzt, int capT, int bc,
+                                                        const int* __restrict__ ncT, const int* __restrict__ cidT,
+                                                        const R* __restrict__ wT, const R* __restrict__ lwT,
+                                                        const int* __restrict__ lcT, const int* __restrict__ lnT,
+                                                        cplx<R>* __restrict__ grid) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    cplx<R>* pv = reinterpret_cast<cplx<R>*>(smem_raw);   // [capT][bc]
+    const int zt = blockIdx.z % nzt, chunk = blockIdx.z / nzt;
+    const int tile = (zt * nby + blockIdx.y) * nbx + blockIdx.x;
+    const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY, z0 = zt * TZ;
+    const int B = C * M;
+    const int wlen = TX + TY + TZ;
+    const int ncol = TX * TY;
+    const int nc = ncT[tile];
+    const size_t trow = size_t(tile) * capT;
+    const int b0 = chunk * bc;
+    const int nb = min(bc, B - b0);
+    for (int t = threadIdx.x; t < nc * nb; t += blockDim.x) {
+        const int c = t / nb, bb = t % nb;
+        const int i = cidT[trow + c];
+        const int b = b0 + bb;
+        const int comp = b / M;
+        double2 v;
+        if (comp < 3) {
+            v = X[size_t(3 * i) * M + b];
+        } else {
+            const int q = quad_map ? quad_map[i] : -1;
+            v = (q >= 0) ? X[size_t(3 * N + 5 * q + comp - 3) * M + (b - comp * M)] : make_double2(0, 0);
+        }
+        pv[c * bc + bb] = to_r<R>(v);
+    }
+    __syncthreads();
+    const R* wTt = wT + trow * wlen;
+    for (int t = threadIdx.x; t < ncol * nb; t += blockDim.x) {
+        const int bb = t % nb, col = t / nb;
+        const int lx = col / TY, ly = col % TY;
+        const int x = x0 + lx, y = y0 + ly;
+        if (x >= g.Nx || y >= g.Ny) continue;
+        const int nl = lnT[size_t(tile) * ncol + col];
+        cplx<R> acc[kSpreadZMax];
+#pragma unroll
+        for (int lz = 0; lz < kSpreadZMax; ++lz) acc[lz] = mk<R>(0, 0);
+        if (nl >= 0) {
+            const size_t lrow = (size_t(tile) * ncol + col) * kSpreadListCap;
+            for (int k = 0; k < nl; ++k) {
+                const int c = lcT[lrow + k];
+                const R wxy = lwT[lrow + k];
+                const cplx<R> pc = pv[c * bc + bb];
+                const R* wz = wTt + c * wlen + TX + TY;
+#pragma unroll
+                for (int lz = 0; lz < kSpreadZMax; ++lz)
+                    if (lz < TZ) fma_rc(acc[lz], wxy * wz[lz], pc);
+            }
+        } else {
+            for (int c = 0; c < nc; ++c) {
+                const R* wc = wTt + c * wlen;
+                const R wxy = wc[lx] * wc[TX + ly];
+                const cplx<R> pc = pv[c * bc + bb];
+#pragma unroll
+                for (int lz = 0; lz < kSpreadZMax; ++lz)
+                    if (lz < TZ) fma_rc(acc[lz], wxy * wc[TX + TY + lz], pc);
+            }
+        }
+        const size_t o0 = ((size_t(x) * g.Ny + y) * g.Zs + z0) * B + b0 + bb;
+#pragma unroll
+        for (int lz = 0; lz < kSpreadZMax; ++lz) {
+            if (lz >= TZ || z0 + lz >= g.Zs) break;
+            grid[o0 + size_t(lz) * B] = acc[lz];
+        }
+    }
+}
+
 // Full layout: k-space Green tensor, dipoles only (scale_kernel,
 // monodisperse_ewald_electric_field.cu:1406-1432) or joint dipole/quadrupole
 // (scale_kernel_joint, :1434-1486).  One thread per (voxel, rhs).
@@ -1038,6 +1244,53 @@ void Field::choose_layout(cudaStream_t) {
     gv_.z0 = (best_start + best_len) % Nz;
 }
 
+// The spread plan (see k_spread_plan).  Left out (plan_cap_ = 0, spread
+// builds its lists in every launch) when a tile has more candidates than the
+// plan kernel holds or the plan would take more than 512 MB.
+void Field::build_spread_plan(cudaStream_t s) {
+    plan_cap_ = 0;
+    const PointSet& ps = sources_;
+    const int TX = ps.tile[0], TY = ps.tile[1], TZ = ps.tile[2];
+    const int wlen = TX + TY + TZ;
+    const int ntile = ps.nb[0] * ps.nb[1] * ps.nb[2];
+    const int ncol = TX * TY;
+    if (TZ > kSpreadZMax || ntile < 1) return;
+    const size_t shm = sizeof(double) * kPlanCandMax * wlen;
+    MPM_CUDA(cudaFuncSetAttribute(k_spread_plan, cudaFuncAttributeMaxDynamicSharedMemorySize, int(shm)));
+    plan_nc_.ensure(sizeof(int) * ntile);
+    plan_cnt_.ensure(sizeof(int) * 2);
+    MPM_CUDA(cudaMemsetAsync(plan_cnt_.p, 0, sizeof(int) * 2, s));
+    int* cnt = plan_cnt_.as<int>();
+    auto run = [&](int pass, int cap) {
+        k_spread_plan<<<ntile, 256, shm, s>>>(ps.base.as<int4>(), ps.w64.as<double>(), ps.bin_start.as<int>(),
+                                              ps.bin_end.as<int>(), ps.idx_sorted.as<int>(), gv_, TX, TY, TZ,
+                                              ps.nb[0], ps.nb[1], pass, cap, plan_nc_.as<int>(), cnt, cnt + 1,
+                                              plan_cid_.as<int>(), plan_w64_.as<double>(), plan_w32_.as<float>(),
+                                              plan_lw64_.as<double>(), plan_lw32_.as<float>(), plan_lc_.as<int>(),
+                                              plan_ln_.as<int>());
+        MPM_LAUNCH();
+    };
+    run(0, 0);
+    int h[2] = {0, 0};
+    MPM_CUDA(cudaMemcpyAsync(h, plan_cnt_.p, sizeof(h), cudaMemcpyDeviceToHost, s));
+    MPM_CUDA(cudaStreamSynchronize(s));
+    if (h[1]) return;
+    const int cap = std::max(1, h[0]);
+    const size_t lists = size_t(ntile) * ncol * kSpreadListCap;
+    const size_t bytes = size_t(ntile) * cap * (sizeof(int) + wlen * (sizeof(double) + sizeof(float))) +
+                         lists * (sizeof(double) + sizeof(float) + sizeof(int)) + sizeof(int) * ntile * ncol;
+    if (bytes > (size_t(512) << 20)) return;
+    plan_cid_.ensure(sizeof(int) * ntile * cap);
+    plan_w64_.ensure(sizeof(double) * ntile * cap * wlen);
+    plan_w32_.ensure(sizeof(float) * ntile * cap * wlen);
+    plan_lw64_.ensure(sizeof(double) * lists);
+    plan_lw32_.ensure(sizeof(float) * lists);
+    plan_lc_.ensure(sizeof(int) * lists);
+    plan_ln_.ensure(sizeof(int) * size_t(ntile) * ncol);
+    run(1, cap);
+    plan_cap_ = cap;
+}
+
 void Field::build_stencil(PointSet& ps, cudaStream_t s, bool bins) {
     const int n = ps.n;
     const int S = gv_.S;
@@ -1207,6 +1460,7 @@ void Field::precalc(cudaStream_t s) {
             if (!gv_.pruned) fftz_.init(gv_.Nz);
         }
         build_stencil(sources_, s, true);
+        build_spread_plan(s);
         if (!spec_.solver_ax) build_stencil(targets_, s, false);  // SOLVER_AX: targets share the source stencil
         build_pairs(s);
         if (gv_.pruned) {
@@ -1299,9 +1553,21 @@ void Field::recip_on(const double2* X, double2* Y, int M, cplx<R>* grid, cudaStr
     dim3 grd(ps.nb[0], ps.nb[1], ps.nb[2] * nchunk);  // one CTA per tile and column chunk
     const R* w1 = sizeof(R) == 4 ? reinterpret_cast<const R*>(ps.w32.p) : reinterpret_cast<const R*>(ps.w64.p);
     Profiler::get().begin(ST_SPREAD, s);
-    k_spread<R><<<grd, 256, shm, s>>>(X, M, N_, C, quad_map_.as<int>(), ps.base.as<int4>(), w1,
-                                      ps.bin_start.as<int>(), ps.bin_end.as<int>(), ps.idx_sorted.as<int>(), gv_,
-                                      TX, TY, TZ, ps.nb[0], ps.nb[1], ps.nb[2], cap, bc, grid);
+    if (plan_cap_ > 0) {
+        const size_t pshm = sizeof(cplx<R>) * size_t(plan_cap_) * bc;
+        MPM_CUDA(cudaFuncSetAttribute(k_spread_planned<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(pshm)));
+        const bool f32 = sizeof(R) == 4;
+        const R* wT = f32 ? reinterpret_cast<const R*>(plan_w32_.p) : reinterpret_cast<const R*>(plan_w64_.p);
+        const R* lw = f32 ? reinterpret_cast<const R*>(plan_lw32_.p) : reinterpret_cast<const R*>(plan_lw64_.p);
+        k_spread_planned<R><<<grd, 256, pshm, s>>>(X, M, N_, C, quad_map_.as<int>(), gv_, TX, TY, TZ, ps.nb[0],
+                                                   ps.nb[1], ps.nb[2], plan_cap_, bc, plan_nc_.as<int>(),
+                                                   plan_cid_.as<int>(), wT, lw, plan_lc_.as<int>(),
+                                                   plan_ln_.as<int>(), grid);
+    } else {
+        k_spread<R><<<grd, 256, shm, s>>>(X, M, N_, C, quad_map_.as<int>(), ps.base.as<int4>(), w1,
+                                          ps.bin_start.as<int>(), ps.bin_end.as<int>(), ps.idx_sorted.as<int>(),
+                                          gv_, TX, TY, TZ, ps.nb[0], ps.nb[1], ps.nb[2], cap, bc, grid);
+    }
     MPM_LAUNCH();
     Profiler::get().end(ST_SPREAD, s);
     // forward transform

@@ -156,6 +156,7 @@ private:
     template <typename R> void recip(const double2* X, double2* Y, int M, cudaStream_t s);
     template <typename R> void recip_on(const double2* X, double2* Y, int M, cplx<R>* grid, cudaStream_t s);
     template <typename R> void transform(cplx<R>* grid, int B, bool inverse, cudaStream_t s);
+    void build_spread_plan(cudaStream_t s);
     void real_part(const double2* X, double2* Y, int M, const double2* self_coef, bool jacobi, bool real_fp32,
                    bool add_recip, cudaStream_t s);
     void direct(const double2* X, double2* Y, int M, const double2* self_coef, bool jacobi, bool fp32,
@@ -187,6 +188,10 @@ private:
     DevBuf grid_;                   // complex grid, sized for the largest use
     DevBuf scale64_, scale32_;      // full layout: per-voxel scale
     DevBuf colK64_, colK32_;        // pruned layout: per-column Toeplitz kernels
+    // per-frame spread plan (monodisperse): per tile candidates, 1-D weights,
+    // column contributor lists; plan_cap_ = 0 when the plan is not in use
+    DevBuf plan_nc_, plan_cid_, plan_w64_, plan_w32_, plan_lw64_, plan_lw32_, plan_lc_, plan_ln_, plan_cnt_;
+    int plan_cap_ = 0;
     int colK_Z_ = -1;
     int scale_built_ = 0;
     struct PlanKey { int M; bool fp32; int pruned; int Zs; cufftHandle h; };  // M: columns per voxel
