@@ -679,12 +679,17 @@ void launch2_cw(int cls, int nblocks, int nthreads, size_t shm, cudaStream_t s, 
 // of one line; L = blockDim.x / CW lanes loop over pass 1's p butterflies and
 // pass 2's r1 * ceil(((p-1)/2) / PC) work items.
 
+// fp64 work items carry half the output pairs, so that their accumulators
+// leave room for three CTAs per SM
+template <typename R>
+__host__ __device__ constexpr int fft2p_pc() { return sizeof(R) == 8 ? 4 : 8; }
+
 template <typename R, int CW, bool INV, int CLS>
 __global__ void __launch_bounds__(kFft2MaxThreads) k_fft2p(cplx<R>* __restrict__ data, const cplx<R>* __restrict__ tw,
                                                            const cplx<R>* __restrict__ ptw, int pt_total, int pt_ld,
                                                            int r1, int p, size_t es, int ncols, size_t os,
                                                            int ngroups) {
-    constexpr int PC = 8;
+    constexpr int PC = fft2p_pc<R>();   // output pairs per work item
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int n = r1 * p;
     const int L = blockDim.x / CW;
@@ -962,8 +967,9 @@ void AxisFFT::launch_line(cplx<R>* data, size_t es, int ncols, size_t os, int no
     if (kind == 2) {
         // two-pass with a streamed prime pass
         const int half = (r2_ - 1) / 2;
-        const int nitems = r1_ * ((half + 7) / 8);
-        const int L = std::min(32, std::max(16, nitems));
+        const int pc = fft2p_pc<R>();
+        const int nitems = r1_ * ((half + pc - 1) / pc);
+        const int L = std::min(sizeof(R) == 8 ? 24 : 32, std::max(16, nitems));
         int cw = 16;
         while (cw > 4 && (cw * L > kFft2MaxThreads ||
                           fft2p_smem(n, cw, sizeof(cplx<R>), pp_total_) > kFftSmemBudget))

@@ -407,7 +407,7 @@ __global__ void __launch_bounds__(256) k_spread_plan(const int4* __restrict__ ba
 // columns; loads the tile's candidate moments, then thread = one (x, y)
 // column x one grid column with the whole z run in registers.  The same
 // contributors in the same order as k_spread.
-template <typename R>
+template <typename R, int ZMAX>
 __global__ void __launch_bounds__(256) k_spread_planned(const double2* __restrict__ X, int M, int N, int C,
                                                         const int* __restrict__ quad_map, GridView g, int TX,
                                                         int TY, int TZ, int nbx, int nby, int nzt, int capT, int bc,
@@ -449,9 +449,9 @@ __global__ void __launch_bounds__(256) k_spread_planned(const double2* __restric
         const int x = x0 + lx, y = y0 + ly;
         if (x >= g.Nx || y >= g.Ny) continue;
         const int nl = lnT[size_t(tile) * ncol + col];
-        cplx<R> acc[kSpreadZMax];
+        cplx<R> acc[ZMAX];
 #pragma unroll
-        for (int lz = 0; lz < kSpreadZMax; ++lz) acc[lz] = mk<R>(0, 0);
+        for (int lz = 0; lz < ZMAX; ++lz) acc[lz] = mk<R>(0, 0);
         if (nl >= 0) {
             const size_t lrow = (size_t(tile) * ncol + col) * kSpreadListCap;
             for (int k = 0; k < nl; ++k) {
@@ -460,7 +460,7 @@ __global__ void __launch_bounds__(256) k_spread_planned(const double2* __restric
                 const cplx<R> pc = pv[c * bc + bb];
                 const R* wz = wTt + c * wlen + TX + TY;
 #pragma unroll
-                for (int lz = 0; lz < kSpreadZMax; ++lz)
+                for (int lz = 0; lz < ZMAX; ++lz)
                     if (lz < TZ) fma_rc(acc[lz], wxy * wz[lz], pc);
             }
         } else {
@@ -469,13 +469,13 @@ __global__ void __launch_bounds__(256) k_spread_planned(const double2* __restric
                 const R wxy = wc[lx] * wc[TX + ly];
                 const cplx<R> pc = pv[c * bc + bb];
 #pragma unroll
-                for (int lz = 0; lz < kSpreadZMax; ++lz)
+                for (int lz = 0; lz < ZMAX; ++lz)
                     if (lz < TZ) fma_rc(acc[lz], wxy * wc[TX + TY + lz], pc);
             }
         }
         const size_t o0 = ((size_t(x) * g.Ny + y) * g.Zs + z0) * B + b0 + bb;
 #pragma unroll
-        for (int lz = 0; lz < kSpreadZMax; ++lz) {
+        for (int lz = 0; lz < ZMAX; ++lz) {
             if (lz >= TZ || z0 + lz >= g.Zs) break;
             grid[o0 + size_t(lz) * B] = acc[lz];
         }
@@ -650,7 +650,13 @@ __global__ void k_column(cplx<R>* __restrict__ grid, const cplx<R>* __restrict__
 #pragma unroll
                 for (int zo = 0; zo < ZMAX; ++zo) {
                     const int zi = zo - d;
-                    if (zi >= 0 && zi < ZMAX) acc[zo] += kv * x[zi];
+                    if (zi >= 0 && zi < ZMAX) {
+                        // acc += kv * x, four FMAs
+                        acc[zo].x = fma(kv.x, x[zi].x, acc[zo].x);
+                        acc[zo].x = fma(-kv.y, x[zi].y, acc[zo].x);
+                        acc[zo].y = fma(kv.x, x[zi].y, acc[zo].y);
+                        acc[zo].y = fma(kv.y, x[zi].x, acc[zo].y);
+                    }
                 }
             }
         }
@@ -1555,14 +1561,18 @@ void Field::recip_on(const double2* X, double2* Y, int M, cplx<R>* grid, cudaStr
     Profiler::get().begin(ST_SPREAD, s);
     if (plan_cap_ > 0) {
         const size_t pshm = sizeof(cplx<R>) * size_t(plan_cap_) * bc;
-        MPM_CUDA(cudaFuncSetAttribute(k_spread_planned<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(pshm)));
         const bool f32 = sizeof(R) == 4;
         const R* wT = f32 ? reinterpret_cast<const R*>(plan_w32_.p) : reinterpret_cast<const R*>(plan_w64_.p);
         const R* lw = f32 ? reinterpret_cast<const R*>(plan_lw32_.p) : reinterpret_cast<const R*>(plan_lw64_.p);
-        k_spread_planned<R><<<grd, 256, pshm, s>>>(X, M, N_, C, quad_map_.as<int>(), gv_, TX, TY, TZ, ps.nb[0],
-                                                   ps.nb[1], ps.nb[2], plan_cap_, bc, plan_nc_.as<int>(),
-                                                   plan_cid_.as<int>(), wT, lw, plan_lc_.as<int>(),
-                                                   plan_ln_.as<int>(), grid);
+        auto go = [&](auto kern) {
+            MPM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(pshm)));
+            kern<<<grd, 256, pshm, s>>>(X, M, N_, C, quad_map_.as<int>(), gv_, TX, TY, TZ, ps.nb[0], ps.nb[1],
+                                        ps.nb[2], plan_cap_, bc, plan_nc_.as<int>(), plan_cid_.as<int>(), wT, lw,
+                                        plan_lc_.as<int>(), plan_ln_.as<int>(), grid);
+        };
+        // the tile's z run in registers: as many accumulators as it needs
+        if (TZ <= 9) go(k_spread_planned<R, 9>);
+        else go(k_spread_planned<R, kSpreadZMax>);
     } else {
         k_spread<R><<<grd, 256, shm, s>>>(X, M, N_, C, quad_map_.as<int>(), ps.base.as<int4>(), w1,
                                           ps.bin_start.as<int>(), ps.bin_end.as<int>(), ps.idx_sorted.as<int>(),
