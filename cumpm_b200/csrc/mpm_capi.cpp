@@ -122,7 +122,11 @@ int mpm_solver_dims(const mpm_solver* s, int64_t dims[5]) {
 }
 
 int mpm_solver_get_dipoles(const mpm_solver* s, int physical, double* out, size_t n) {
-    return guard([&] { need(s, "solver"); copy_out(s->impl->get_dipoles(physical != 0), out, n); });
+    return guard([&] {
+        need(s, "solver");
+        need(out, "out");
+        s->impl->get_dipoles_into(physical != 0, reinterpret_cast<cd*>(out), n);
+    });
 }
 int mpm_solver_get_quadrupoles(const mpm_solver* s, int physical, double* out, size_t n) {
     return guard([&] { need(s, "solver"); copy_out(s->impl->get_quadrupoles(physical != 0), out, n); });

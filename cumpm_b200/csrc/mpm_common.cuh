@@ -113,4 +113,28 @@ struct DevBuf {
     template <typename T> T* as() const { return static_cast<T*>(p); }
 };
 
+// Page-locked host buffer (reused across calls, so host<->device copies run
+// at full PCIe/C2C speed and never fault fresh pages).
+struct HostBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+    HostBuf() = default;
+    HostBuf(const HostBuf&) = delete;
+    HostBuf& operator=(const HostBuf&) = delete;
+    ~HostBuf() { release(); }
+    void release() {
+        if (p) cudaFreeHost(p);
+        p = nullptr;
+        bytes = 0;
+    }
+    void ensure(size_t n) {
+        if (n <= bytes && p) return;
+        release();
+        if (n == 0) return;
+        MPM_CUDA(cudaHostAlloc(&p, n, cudaHostAllocDefault));
+        bytes = n;
+    }
+    template <typename T> T* as() const { return static_cast<T*>(p); }
+};
+
 }  // namespace mpm

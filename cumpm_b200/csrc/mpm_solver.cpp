@@ -141,7 +141,14 @@ void DipoleSolver::solve_batch(const std::vector<size_t>& freqs, const std::vect
     const size_t K = E0_.size();
     const size_t rows = N_ * 3 + Nq_ * 5;
     const int M = int(freqs.size() * K);
-    std::vector<cdouble> hb(rows * M, 0.0), hx(rows * M, 0.0), hsc(N_ * M);
+    hB_.ensure(sizeof(cdouble) * rows * M);
+    hX_.ensure(sizeof(cdouble) * rows * M);
+    hSC_.ensure(sizeof(cdouble) * N_ * M);
+    cdouble* hb = hB_.as<cdouble>();
+    cdouble* hx = hX_.as<cdouble>();
+    cdouble* hsc = hSC_.as<cdouble>();
+    std::fill(hb, hb + rows * M, cdouble(0.0));
+    std::fill(hx, hx + rows * M, cdouble(0.0));
     for (size_t f = 0; f < freqs.size(); ++f) {
         const size_t w = freqs[f];
         // self coefficients s = -3 / (4 pi (1 - eps) a^3) (dipole_solver.cu:452-460)
@@ -173,9 +180,9 @@ void DipoleSolver::solve_batch(const std::vector<size_t>& freqs, const std::vect
     dB_.ensure(bytes);
     dX_.ensure(bytes);
     dSC_.ensure(sizeof(double2) * N_ * M);
-    MPM_CUDA(cudaMemcpyAsync(dB_.p, hb.data(), bytes, cudaMemcpyHostToDevice, stream_));
-    MPM_CUDA(cudaMemcpyAsync(dX_.p, hx.data(), bytes, cudaMemcpyHostToDevice, stream_));
-    MPM_CUDA(cudaMemcpyAsync(dSC_.p, hsc.data(), sizeof(double2) * N_ * M, cudaMemcpyHostToDevice, stream_));
+    MPM_CUDA(cudaMemcpyAsync(dB_.p, hb, bytes, cudaMemcpyHostToDevice, stream_));
+    MPM_CUDA(cudaMemcpyAsync(dX_.p, hx, bytes, cudaMemcpyHostToDevice, stream_));
+    MPM_CUDA(cudaMemcpyAsync(dSC_.p, hsc, sizeof(double2) * N_ * M, cudaMemcpyHostToDevice, stream_));
     SolveOptions so;
     so.method = solver_type_ == "bicgstab" ? SOLVER_BICGSTAB : SOLVER_GMRES;
     so.restart = opt_.restart;
@@ -188,7 +195,7 @@ void DipoleSolver::solve_batch(const std::vector<size_t>& freqs, const std::vect
     so.inner_tol = opt_.inner_tol;
     solver_->solve(*field_, dB_.as<double2>(), dX_.as<double2>(), M, dSC_.as<double2>(), so, last_stats_, stream_);
     for (int v : last_stats_.iters) iters_.push_back(v);
-    MPM_CUDA(cudaMemcpyAsync(hx.data(), dX_.p, bytes, cudaMemcpyDeviceToHost, stream_));
+    MPM_CUDA(cudaMemcpyAsync(hx, dX_.p, bytes, cudaMemcpyDeviceToHost, stream_));
     MPM_CUDA(cudaStreamSynchronize(stream_));
     for (size_t f = 0; f < freqs.size(); ++f) {
         const size_t w = freqs[f];
@@ -312,6 +319,13 @@ std::vector<cdouble> DipoleSolver::get_dipoles(bool physical) const {
     std::vector<cdouble> out = dips_;
     for (auto& v : out) v *= f;
     return out;
+}
+
+size_t DipoleSolver::get_dipoles_into(bool physical, cdouble* out, size_t cap) const {
+    if (cap < dips_.size()) throw std::invalid_argument("output buffer too small");
+    const double f = physical ? eps_scale_ * std::pow(length_scale_, 3.0) : 1.0;
+    for (size_t k = 0; k < dips_.size(); ++k) out[k] = dips_[k] * f;
+    return dips_.size();
 }
 
 std::vector<cdouble> DipoleSolver::get_quadrupoles(bool physical) const {

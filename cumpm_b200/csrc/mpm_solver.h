@@ -43,6 +43,8 @@ public:
 
     std::vector<cdouble> get_eff_polarizability(bool physical) const;
     std::vector<cdouble> get_dipoles(bool physical) const;
+    // the same values written straight into out (cap entries); returns the count
+    size_t get_dipoles_into(bool physical, cdouble* out, size_t cap) const;
     std::vector<cdouble> get_quadrupoles(bool physical) const;
 
     size_t num_frames() const { return num_frames_; }
@@ -89,6 +91,7 @@ private:
     std::unique_ptr<BatchSolver> solver_;
     cudaStream_t stream_ = nullptr;
     DevBuf dB_, dX_, dSC_;
+    HostBuf hB_, hX_, hSC_;   // pinned staging of the batch's right-hand sides, guesses / solutions, self terms
     int indent_ = 0;
 };
 
