@@ -211,13 +211,22 @@ def measured_peaks():
         return 6650.0, "fallback"
 
 
-def ncu_traffic():
-    """Per-launch DRAM bytes of the profiled kernels (profiles/traffic.json)."""
-    try:
-        with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
-            return json.load(f)
-    except Exception:
-        return {}
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per algorithmic
+# byte of a stage's kernels, from ncu --set full captures of one launch each
+# (profiles/kernels_monolayer_n4000.md: x and y transforms of a 25-column
+# matvec, 522.6 MB of DRAM traffic for 632.4 MB algorithmic;
+# profiles/kernels_poly3d_n1000.md: spread 1892 MB for 1962 MB, plain axis
+# pass 3811 MB for 3870 MB).  Traffic scales with the columns a launch
+# carries, so a stage's traffic per launch is this ratio times its
+# algorithmic bytes per launch.  Below 1: the last writes of a launch are
+# still in L2 when the kernel ends.
+TRAFFIC_PER_ALG_BYTE = {
+    ("monolayer", "fft_fwd"): 522.6 / 632.4,
+    ("monolayer", "fft_inv"): 522.2 / 632.4,
+    ("poly3d", "spread"): 1892.0 / 1962.0,
+    ("poly3d", "fft_fwd"): 3811.0 / 3870.0,
+    ("poly3d", "fft_inv"): 3811.0 / 3870.0,
+}
 
 
 def algorithmic_bytes(info, M, n_pairs, fp64, mono=True):
@@ -357,7 +366,8 @@ def run_ours(args, rank, world, local_rank):
     bytes_total = stage_bytes(dom)
     peak, peak_kind = measured_peaks()
     achieved = bytes_total / (dom_ms / 1e3) / 1e9 if dom_ms > 0 else 0.0
-    traffic = ncu_traffic().get(dom)
+    ratio = TRAFFIC_PER_ALG_BYTE.get((wl.name, dom))
+    traffic = round(ratio * bytes_total / max(1, dom_n)) if ratio else None
     mv_bytes = sum(stage_bytes(k) for k in op_stages)
     mv_ms = sum(stages[k][0] for k in op_stages)
     mv_frac = round(mv_bytes / (mv_ms / 1e3) / 1e9 / peak, 4) if mv_ms > 0 else None
@@ -418,6 +428,8 @@ def run_ours(args, rank, world, local_rank):
                 "unit": "GB/s",
                 "frac": round(achieved / peak, 4),
                 "traffic": None if traffic is None else traffic,
+                "traffic_source": ("ncu DRAM bytes per algorithmic byte of this stage's kernels (profiles/kernels_*.md)"
+                                   " x algorithmic bytes per launch") if traffic is not None else None,
                 "algorithmic_bytes_per_launch": round(bytes_total / max(1, dom_n)),
                 "algorithmic_bytes_full_batch_fp32": b32[dom],
                 "launches": dom_n,
