@@ -526,12 +526,18 @@ __device__ __forceinline__ void radix_dispatch(int r, Fn&& fn) {
         case 7: fn(std::integral_constant<int, 7>{}); break;
         case 8: fn(std::integral_constant<int, 8>{}); break;
         default:
+            // register classes: radices up to CLS only (8, 12 or 16)
             if constexpr (CLS > 8) {
                 switch (r) {
                     case 9: fn(std::integral_constant<int, 9>{}); break;
                     case 10: fn(std::integral_constant<int, 10>{}); break;
                     case 11: fn(std::integral_constant<int, 11>{}); break;
                     case 12: fn(std::integral_constant<int, 12>{}); break;
+                    default: break;
+                }
+            }
+            if constexpr (CLS > 12) {
+                switch (r) {
                     case 13: fn(std::integral_constant<int, 13>{}); break;
                     case 14: fn(std::integral_constant<int, 14>{}); break;
                     case 15: fn(std::integral_constant<int, 15>{}); break;
@@ -640,6 +646,9 @@ __global__ void __launch_bounds__(kFft2MaxThreads) k_fft2(cplx<R>* __restrict__ 
 // radices the two-pass kernels have in-register butterflies for
 bool fft2_radix(int r) { return r >= 1 && r <= 16; }
 
+// the kernel instantiation (largest radix compiled in) for a largest radix r
+int register_class(int r) { return r <= 8 ? 8 : (r <= 12 ? 12 : 16); }
+
 // (r1, r2) with r1 * r2 = n, both in-register radices, max(r1, r2) smallest
 // (0, 0) when n has no such split
 std::pair<int, int> fft2_split(int n) {
@@ -663,6 +672,7 @@ void launch2_cw(int cls, int nblocks, int nthreads, size_t shm, cudaStream_t s, 
         kern<<<nblocks, nthreads, shm, s>>>(data, tw, r1, r2, es, ncols, os, ngroups, ks);
     };
     if (cls == 8) go(k_fft2<R, CW, MODE, 8>);
+    else if (cls == 12) go(k_fft2<R, CW, MODE, 12>);
     else go(k_fft2<R, CW, MODE, 16>);
 }
 
@@ -835,6 +845,178 @@ void launch2p_cw(int cls, int nblocks, int nthreads, size_t shm, cudaStream_t s,
     else go(k_fft2p<R, CW, INV, 16>);
 }
 
+// ---------------------------------------------------------------------------
+// Two-pass line transform n = r1 * p with the prime pass done by Rader's
+// algorithm: with g a primitive root mod p, a_q = x[g^-q], b_s = W_p^(g^s),
+//   y[0] = x[0] + sum_q a_q,   y[g^m] = x[0] + (a (*) b)_m   (cyclic, length N = p-1)
+// and the cyclic convolution is IDFT_N(DFT_N(a) . Bh) with Bh = DFT_N(b) / N
+// precomputed.  N = A * B with both in-register radices, so DFT_N is one
+// Cooley-Tukey step through shared memory: R1 (thread per (j, q2)) an A-point
+// DFT over q1 of a[B q1 + q2] and the twiddles W_N^(q2 k1); R2 (thread per
+// (j, k1)) the B-point DFT over q2, the product with Bh, the B-point inverse
+// DFT and the twiddles W_N^(-m1 k1) in registers; R4 (thread per (j, m1)) the
+// A-point inverse DFT giving c[m1 + B m2], written to global memory at row
+// g^(m1 + B m2).  About a quarter of the direct prime pass's arithmetic.
+// Pass 1 is k_fft2p's (radix r1 from global memory, pass-2 twiddles fused).
+template <typename R, int CW, bool INV, int CLS>
+__global__ void __launch_bounds__(kFft2MaxThreads) k_fft2r(cplx<R>* __restrict__ data, const cplx<R>* __restrict__ tw,
+                                                           const cplx<R>* __restrict__ rtab,
+                                                           const int* __restrict__ rperm, int r1, int p, int A,
+                                                           int B, size_t es, int ncols, size_t os, int ngroups) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int n = r1 * p;
+    const int N = p - 1;
+    const int L = blockDim.x / CW;
+    cplx<R>* S = reinterpret_cast<cplx<R>*>(smem_raw);   // [n][CW] pass-1 output
+    cplx<R>* Tt = S + size_t(n) * CW;                      // [r1 * N][CW] Rader work rows
+    cplx<R>* T = Tt + size_t(r1) * N * CW;                 // [n] line twiddles
+    cplx<R>* WN = T + n;                                   // [N] W_N^t
+    cplx<R>* Bh = WN + N;                                  // [N] this direction's Bh
+    int* pin = reinterpret_cast<int*>(Bh + N);             // [N] g^-q
+    int* pout = pin + N;                                   // [N] g^m
+    const int o = blockIdx.x / ngroups;
+    const int g = blockIdx.x - o * ngroups;
+    const int c = threadIdx.x & (CW - 1);
+    const int lane = threadIdx.x / CW;
+    const int c0 = g * CW;
+    const bool live = c0 + c < ncols;
+    cplx<R>* line = data + size_t(o) * os + c0 + c;
+    for (int t = threadIdx.x; t < n; t += blockDim.x) {
+        cplx<R> w = tw[t];
+        if (INV) w.y = -w.y;
+        T[t] = w;
+    }
+    for (int t = threadIdx.x; t < N; t += blockDim.x) {
+        WN[t] = rtab[t];
+        Bh[t] = rtab[(INV ? 2 : 1) * N + t];
+        pin[t] = rperm[t];
+        pout[t] = rperm[N + t];
+    }
+    __syncthreads();
+    // pass 1: radix r1, global -> shared with pass 2's twiddles applied
+    radix_dispatch<CLS>(r1, [&](auto rc) {
+        constexpr int RAD = decltype(rc)::value;
+#pragma unroll 2
+        for (int j1 = lane; j1 < p; j1 += L) {
+            cplx<R> x[RAD];
+#pragma unroll
+            for (int q = 0; q < RAD; ++q) x[q] = live ? line[size_t(j1 + q * p) * es] : mk<R>(R(0), R(0));
+            dft_small<R, INV, RAD>(x);
+            S[(j1 * RAD) * CW + c] = x[0];
+#pragma unroll
+            for (int p1 = 1; p1 < RAD; ++p1) S[(j1 * RAD + p1) * CW + c] = x[p1] * T[j1 * p1];
+        }
+    });
+    __syncthreads();
+    // R1: A-point DFTs over q1 of a[B q1 + q2], twiddled by W_N^(q2 k1)
+    radix_dispatch<CLS>(A, [&](auto rc) {
+        constexpr int RA = decltype(rc)::value;
+        for (int u = lane; u < r1 * B; u += L) {
+            const int q2 = u / r1;
+            const int j = u - q2 * r1;
+            cplx<R> z[RA];
+#pragma unroll
+            for (int q1 = 0; q1 < RA; ++q1) z[q1] = S[(j + pin[B * q1 + q2] * r1) * CW + c];
+            dft_small<R, false, RA>(z);
+            cplx<R>* trow = Tt + (size_t(j) * N + q2 * RA) * CW + c;
+            trow[0] = z[0];
+#pragma unroll
+            for (int k1 = 1; k1 < RA; ++k1) trow[k1 * CW] = q2 ? z[k1] * WN[q2 * k1] : z[k1];
+        }
+    });
+    __syncthreads();
+    // R2: B-point DFT over q2 (-> DFT_N(a) at k1 + A k2), times Bh, B-point
+    // inverse DFT over k2, twiddles W_N^(-m1 k1); the thread rewrites the
+    // same Tt slots it read
+    radix_dispatch<CLS>(B, [&](auto rc) {
+        constexpr int RB = decltype(rc)::value;
+        for (int u = lane; u < r1 * A; u += L) {
+            const int k1 = u / r1;
+            const int j = u - k1 * r1;
+            cplx<R>* tcol = Tt + (size_t(j) * N + k1) * CW + c;
+            cplx<R> v[RB];
+#pragma unroll
+            for (int q2 = 0; q2 < RB; ++q2) v[q2] = tcol[q2 * A * CW];
+            dft_small<R, false, RB>(v);
+            if (k1 == 0 && live) {
+                const cplx<R> x0 = S[j * CW + c];
+                line[size_t(j) * es] = x0 + v[0];   // y[0] = x[0] + sum a
+            }
+#pragma unroll
+            for (int k2 = 0; k2 < RB; ++k2) v[k2] = v[k2] * Bh[k1 + A * k2];
+            dft_small<R, true, RB>(v);
+            tcol[0] = v[0];
+#pragma unroll
+            for (int m1 = 1; m1 < RB; ++m1) {
+                cplx<R> w = WN[m1 * k1];
+                w.y = -w.y;
+                tcol[m1 * A * CW] = k1 ? v[m1] * w : v[m1];
+            }
+        }
+    });
+    __syncthreads();
+    // R4: A-point inverse DFT over k1 -> c[m1 + B m2]; y[g^m] = x[0] + c[m]
+    radix_dispatch<CLS>(A, [&](auto rc) {
+        constexpr int RA = decltype(rc)::value;
+        for (int u = lane; u < r1 * B; u += L) {
+            const int m1 = u / r1;
+            const int j = u - m1 * r1;
+            const cplx<R>* trow = Tt + (size_t(j) * N + m1 * RA) * CW + c;
+            cplx<R> d[RA];
+#pragma unroll
+            for (int k1 = 0; k1 < RA; ++k1) d[k1] = trow[k1 * CW];
+            dft_small<R, true, RA>(d);
+            if (!live) continue;
+            const cplx<R> x0 = S[j * CW + c];
+#pragma unroll
+            for (int m2 = 0; m2 < RA; ++m2) line[size_t(pout[m1 + B * m2] * r1 + j) * es] = x0 + d[m2];
+        }
+    });
+}
+
+size_t fft2r_smem(int n, int r1, int N, int cw, size_t elem) {
+    return (size_t(n) * cw + size_t(r1) * N * cw + n + 2 * size_t(N)) * elem + 2 * sizeof(int) * N;
+}
+
+template <typename R, bool INV, int CW>
+void launch2r_cw(int cls, int nblocks, int nthreads, size_t shm, cudaStream_t s, cplx<R>* data, const cplx<R>* tw,
+                 const cplx<R>* rtab, const int* rperm, int r1, int p, int A, int B, size_t es, int ncols, size_t os,
+                 int ngroups) {
+    auto go = [&](auto kern) {
+        MPM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(shm)));
+        kern<<<nblocks, nthreads, shm, s>>>(data, tw, rtab, rperm, r1, p, A, B, es, ncols, os, ngroups);
+    };
+    if (cls == 8) go(k_fft2r<R, CW, INV, 8>);
+    else if (cls == 12) go(k_fft2r<R, CW, INV, 12>);
+    else go(k_fft2r<R, CW, INV, 16>);
+}
+
+// smallest primitive root of the prime p
+int primitive_root(int p) {
+    std::vector<int> f;
+    int m = p - 1;
+    for (int d = 2; d * d <= m; ++d)
+        if (m % d == 0) {
+            f.push_back(d);
+            while (m % d == 0) m /= d;
+        }
+    if (m > 1) f.push_back(m);
+    for (int g = 2; g < p; ++g) {
+        bool ok = true;
+        for (int q : f) {
+            long long e = (p - 1) / q, r = 1, b = g;
+            while (e) {
+                if (e & 1) r = r * b % p;
+                b = b * b % p;
+                e >>= 1;
+            }
+            if (r == 1) { ok = false; break; }
+        }
+        if (ok) return g;
+    }
+    return 0;
+}
+
 size_t fft_smem(int n, int cw, size_t elem, int pt_total) {
     const size_t pt_off_bytes = (((2 * size_t(n) * cw + n) * elem + 8 * size_t(n)) + 15) & ~size_t(15);
     return pt_off_bytes + size_t(pt_total) * elem;
@@ -932,6 +1114,51 @@ void AxisFFT::init(int n) {
     f_.pt_total = int(p64.size());
     upload_table(p64, pt64_, pt32_);
     // the prime-streamed two-pass kernel's table
+    // Rader tables when p - 1 splits into two in-register radices
+    ra_ = rb_ = 0;
+    if (kind_ == 2) {
+        const int pr = r2_, N = pr - 1;
+        const std::pair<int, int> ab = fft2_split(N);
+        const int g = primitive_root(pr);
+        if (ab.first && g) {
+            kind_ = 3;
+            ra_ = ab.first;
+            rb_ = ab.second;
+            std::vector<int> perm(2 * N);
+            std::vector<long long> gp(N);   // g^s mod p
+            long long v = 1;
+            for (int t = 0; t < N; ++t) {
+                gp[t] = v;
+                v = v * g % pr;
+            }
+            for (int q = 0; q < N; ++q) perm[q] = int(gp[(N - q) % N]);   // a_q = x[g^-q]
+            for (int m = 0; m < N; ++m) perm[N + m] = int(gp[m]);         // y[g^m]
+            std::vector<double2> t64(3 * size_t(N));
+            for (int t = 0; t < N; ++t) {
+                const double a = -2.0 * kPi * double(t) / double(N);
+                t64[t] = make_double2(std::cos(a), std::sin(a));
+            }
+            // Bh = DFT_N(b) / N, b_s = W_p^(g^s) (forward) or its conjugate (inverse)
+            for (int k = 0; k < N; ++k) {
+                double fr = 0, fi = 0, ir = 0, ii = 0;
+                for (int t = 0; t < N; ++t) {
+                    const double ab_ = -2.0 * kPi * double(gp[t]) / double(pr);
+                    const double br = std::cos(ab_), bi = std::sin(ab_);
+                    const double e = -2.0 * kPi * double((long long)t * k % N) / double(N);
+                    const double er = std::cos(e), ei = std::sin(e);
+                    fr += br * er - bi * ei;
+                    fi += br * ei + bi * er;
+                    ir += br * er + bi * ei;
+                    ii += br * ei - bi * er;
+                }
+                t64[N + k] = make_double2(fr / N, fi / N);
+                t64[2 * N + k] = make_double2(ir / N, ii / N);
+            }
+            upload_table(t64, rt64_, rt32_);
+            rperm_.ensure(sizeof(int) * perm.size());
+            MPM_CUDA(cudaMemcpy(rperm_.p, perm.data(), sizeof(int) * perm.size(), cudaMemcpyHostToDevice));
+        }
+    }
     pp_total_ = pp_ld_ = 0;
     if (kind_ == 2) {
         std::vector<double2> q64;
@@ -964,6 +1191,40 @@ void AxisFFT::launch_line(cplx<R>* data, size_t es, int ncols, size_t os, int no
     const cplx<R>* tw = sizeof(R) == 4 ? reinterpret_cast<const cplx<R>*>(tw32_.p)
                                        : reinterpret_cast<const cplx<R>*>(tw64_.p);
     const int kind = path(ncols, mode);
+    if (kind == 3) {
+        // two-pass with a Rader prime pass
+        const int N = r2_ - 1;
+        const int L = 24;
+        // wide butterfly classes hold more registers: smaller CTAs
+        int cw = register_class(std::max(r1_, ra_)) > 8 ? 8 : 16;
+        while (cw > 4 && (cw * L > (sizeof(R) == 8 ? 192 : kFft2MaxThreads) ||
+                          fft2r_smem(n, r1_, N, cw, sizeof(cplx<R>)) > kFftSmemBudget))
+            cw /= 2;
+        const size_t shm = fft2r_smem(n, r1_, N, cw, sizeof(cplx<R>));
+        if (shm > kFftSmemMax) throw std::runtime_error("FFT line does not fit in shared memory");
+        const int ngroups = (ncols + cw - 1) / cw;
+        const int nblocks = nouter * ngroups;
+        const int cls = register_class(std::max(r1_, ra_));
+        const cplx<R>* rt = sizeof(R) == 4 ? reinterpret_cast<const cplx<R>*>(rt32_.p)
+                                           : reinterpret_cast<const cplx<R>*>(rt64_.p);
+        const int* rp = rperm_.as<int>();
+        auto go = [&](auto invc) {
+            constexpr bool INV = decltype(invc)::value;
+            if (cw == 16)
+                launch2r_cw<R, INV, 16>(cls, nblocks, cw * L, shm, s, data, tw, rt, rp, r1_, r2_, ra_, rb_, es, ncols,
+                                        os, ngroups);
+            else if (cw == 8)
+                launch2r_cw<R, INV, 8>(cls, nblocks, cw * L, shm, s, data, tw, rt, rp, r1_, r2_, ra_, rb_, es, ncols,
+                                       os, ngroups);
+            else
+                launch2r_cw<R, INV, 4>(cls, nblocks, cw * L, shm, s, data, tw, rt, rp, r1_, r2_, ra_, rb_, es, ncols,
+                                       os, ngroups);
+        };
+        if (mode == 1) go(std::true_type{});
+        else go(std::false_type{});
+        MPM_LAUNCH();
+        return;
+    }
     if (kind == 2) {
         // two-pass with a streamed prime pass
         const int half = (r2_ - 1) / 2;
@@ -1008,7 +1269,7 @@ void AxisFFT::launch_line(cplx<R>* data, size_t es, int ncols, size_t os, int no
         const size_t shm = fft2_smem(n, cw, sizeof(cplx<R>));
         const int ngroups = (ncols + cw - 1) / cw;
         const int nblocks = nouter * ngroups;
-        const int cls = r1_ <= 8 ? 8 : 16;
+        const int cls = register_class(r1_);
         auto go = [&](auto modec) {
             constexpr int MODE = decltype(modec)::value;
             if (cw == 32)

@@ -53,13 +53,16 @@ public:
     // run every length through the general multi-pass kernel (tests)
     void set_force_general(bool v) { force_general_ = v; }
     // kernel a transform of ncols columns takes: 0 general multi-pass,
-    // 1 two-pass in registers, 2 two-pass with a streamed prime pass (modes
-    // 0 forward, 1 inverse, 2 forward-scale-inverse; 2 has no prime variant)
+    // 1 two-pass in registers, 2 two-pass with a streamed prime pass, 3
+    // two-pass with a Rader prime pass (modes 0 forward, 1 inverse, 2
+    // forward-scale-inverse; 2 has no prime variant)
     int path(int ncols, int mode) const {
         if (!r1_ || ncols < 16 || force_general_) return 0;
-        if (kind_ == 2 && mode == 2) return 0;
+        if (kind_ >= 2 && mode == 2) return 0;
         return kind_;
     }
+    // the Rader split p - 1 = A * B (0 when the prime pass is streamed)
+    int rader_a() const { return ra_; }
 
 private:
     template <typename R>
@@ -68,6 +71,9 @@ private:
     static void upload_table(std::vector<double2> t64, DevBuf& d64, DevBuf& d32);
     FftFactors f_;
     int kind_ = 0, r1_ = 0, r2_ = 0;
+    int ra_ = 0, rb_ = 0;   // Rader split of r2_ - 1
+    DevBuf rt64_, rt32_;     // Rader tables: W_N^t, forward Bh, inverse Bh
+    DevBuf rperm_;           // Rader index maps: g^-q, g^m
     bool force_general_ = false;
     DevBuf tw64_, tw32_;
     DevBuf pt64_, pt32_;   // prime-pass twiddle tables (see FftFactors)
