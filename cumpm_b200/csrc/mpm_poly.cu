@@ -259,6 +259,9 @@ __global__ void __launch_bounds__(256) k_poly_spread(const double2* __restrict__
     for (int c = 0; c < nc; ++c) {
         const int* rr = runs + c * 8;
         const int nrs = rr[6];
+        // a candidate that misses the tile along some axis adds nothing (the
+        // branch is uniform across the CTA, so its barrier goes too)
+        if (!(nrs & 3) || !(nrs & 12) || !(nrs & 48)) continue;
         const cplx<R> p0 = pm[(c * 3 + 0) * CM + cm], p1 = pm[(c * 3 + 1) * CM + cm], p2 = pm[(c * 3 + 2) * CM + cm];
         const R* wi = w + size_t(cand[c]) * P3 * 3;
         for (int ax = 0; ax < (nrs & 3); ++ax)
@@ -266,13 +269,16 @@ __global__ void __launch_bounds__(256) k_poly_spread(const double2* __restrict__
                 for (int az = 0; az < ((nrs >> 4) & 3); ++az) {
                     const int qx = rr[ax], qy = rr[2 + ay], qz = rr[4 + az];
                     const int lx = (qx >> 4) & 15, ly = (qy >> 4) & 15, lz = (qz >> 4) & 15;
-                    const int nb = lx * ly * lz;
-                    for (int b = slot; b < nb; b += NSLOT) {
-                        const int iz = b % lz, iy = (b / lz) % ly, ix = b / (lz * ly);
-                        const int ux = (qx & 15) + ix, uy = (qy & 15) + iy, uz = (qz & 15) + iz;
-                        const int kx = (qx >> 8) + ix, ky = (qy >> 8) + iy, kz = (qz >> 8) + iz;
-                        const R* wp = wi + ((kx * P + ky) * P + kz) * 3;
-                        acc[((ux * 8 + uy) * 8 + uz) * CM + cm] += p0 * wp[0] + p1 * wp[1] + p2 * wp[2];
+                    // slot = one (x, y) row of the covered box; its z run is
+                    // contiguous in both the accumulators and the weights
+                    for (int r = slot; r < lx * ly; r += NSLOT) {
+                        const int ix = r / ly, iy = r - ix * ly;
+                        const int ux = (qx & 15) + ix, uy = (qy & 15) + iy;
+                        const int kx = (qx >> 8) + ix, ky = (qy >> 8) + iy;
+                        const R* wp = wi + ((kx * P + ky) * P + (qz >> 8)) * 3;
+                        cplx<R>* ap = acc + ((ux * 8 + uy) * 8 + (qz & 15)) * CM + cm;
+                        for (int iz = 0; iz < lz; ++iz, wp += 3, ap += CM)
+                            *ap += p0 * wp[0] + p1 * wp[1] + p2 * wp[2];
                     }
                 }
         __syncthreads();
