@@ -335,25 +335,32 @@ __global__ void __launch_bounds__(256) k_poly_contract(const cplx<R>* __restrict
     cplx<R> acc[3][MC];
 #pragma unroll
     for (int q = 0; q < MC; ++q) acc[0][q] = acc[1][q] = acc[2][q] = mk<R>(0, 0);
+    // warp = (x, y) rows of the support (P < N, so a coordinate wraps at
+    // most once); each row's z run is contiguous in the weights and, up to
+    // one wrap, in the grid
+    for (int r = warp; r < P * P; r += CW) {
+        const int kx = r / P, ky = r - kx * P;
+        int x = o.x + kx, y = o.y + ky;
+        if (x >= Nx) x -= Nx;
+        if (y >= Ny) y -= Ny;
+        const size_t rowbase = (size_t(x) * Ny + y) * Nz;
+        const R* wp = w + (size_t(j) * P3 + size_t(r) * P) * 3;
+        int z = o.z;
 #pragma unroll 4
-    for (int k = warp; k < P3; k += CW) {
-        const int kx = k / (P * P), ky = (k / P) % P, kz = k % P;
-        int x = o.x + kx, y = o.y + ky, z = o.z + kz;
-        x = x >= Nx ? x % Nx : x;
-        y = y >= Ny ? y % Ny : y;
-        z = z >= Nz ? z % Nz : z;
-        const size_t vo = ((size_t(x) * Ny + y) * Nz + z) * M;
-        const R* wp = w + (size_t(j) * P3 + k) * 3;
-        const R w0 = wp[0], w1 = wp[1], w2 = wp[2];
+        for (int kz = 0; kz < P; ++kz) {
+            const size_t vo = (rowbase + z) * M;
+            const R w0 = wp[3 * kz], w1 = wp[3 * kz + 1], w2 = wp[3 * kz + 2];
 #pragma unroll
-        for (int q = 0; q < MC; ++q) {
-            const int m = m0 + q * 32 + lane;
-            if (m < M) {
-                const cplx<R> g = grid[vo + m];
-                acc[0][q] += g * w0;
-                acc[1][q] += g * w1;
-                acc[2][q] += g * w2;
+            for (int q = 0; q < MC; ++q) {
+                const int m = m0 + q * 32 + lane;
+                if (m < M) {
+                    const cplx<R> g = grid[vo + m];
+                    acc[0][q] += g * w0;
+                    acc[1][q] += g * w1;
+                    acc[2][q] += g * w2;
+                }
             }
+            z = z + 1 == Nz ? 0 : z + 1;
         }
     }
 #pragma unroll

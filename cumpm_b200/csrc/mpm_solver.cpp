@@ -147,35 +147,46 @@ void DipoleSolver::solve_batch(const std::vector<size_t>& freqs, const std::vect
     cdouble* hb = hB_.as<cdouble>();
     cdouble* hx = hX_.as<cdouble>();
     cdouble* hsc = hSC_.as<cdouble>();
-    std::fill(hb, hb + rows * M, cdouble(0.0));
-    std::fill(hx, hx + rows * M, cdouble(0.0));
-    for (size_t f = 0; f < freqs.size(); ++f) {
-        const size_t w = freqs[f];
-        // self coefficients s = -3 / (4 pi (1 - eps) a^3) (dipole_solver.cu:452-460)
-        for (size_t p = 0; p < N_; ++p) {
-            cdouble diff = 1.0 - eps_p_[w][p];
+    const size_t F = freqs.size();
+    // rows outermost so that every host array is written contiguously
+    // ([row][M] with m = f * K + k)
+    for (size_t p = 0; p < N_; ++p) {
+        cdouble* sp = hsc + p * M;
+        for (size_t f = 0; f < F; ++f) {
+            // self coefficients s = -3 / (4 pi (1 - eps) a^3) (dipole_solver.cu:452-460)
+            cdouble diff = 1.0 - eps_p_[freqs[f]][p];
             if (std::abs(diff) < 1e-12) diff = 1e-12;
-            const cdouble s = -3.0 / (4.0 * PI * diff) / std::pow(radius_[p], 3.0);
-            for (size_t k = 0; k < K; ++k) hsc[p * M + f * K + k] = s;
+            const cdouble sv = -3.0 / (4.0 * PI * diff) / std::pow(radius_[p], 3.0);
+            for (size_t k = 0; k < K; ++k) sp[f * K + k] = sv;
         }
-        const std::vector<cdouble>& gs = guesses[f];
-        for (size_t k = 0; k < K; ++k) {
-            const size_t m = f * K + k;
-            const auto& e = E0_[k];
-            if (e.size() == N_ * 3) {
-                for (size_t i = 0; i < N_ * 3; ++i) hb[i * M + m] = e[i];
-            } else if (e.size() == 3) {
-                for (size_t p = 0; p < N_; ++p)
-                    for (int c = 0; c < 3; ++c) hb[(p * 3 + c) * M + m] = e[c];
-            } else {
-                for (size_t i = 0; i < rows; ++i) hb[i * M + m] = e[i];
+        for (int c = 0; c < 3; ++c) {
+            const size_t row = p * 3 + c;
+            cdouble* br = hb + row * M;
+            cdouble* xr = hx + row * M;
+            for (size_t k = 0; k < K; ++k) {
+                const auto& e = E0_[k];
+                const cdouble ev = e.size() == 3 ? e[c] : e[row];
+                for (size_t f = 0; f < F; ++f) {
+                    br[f * K + k] = ev;
+                    xr[f * K + k] = guesses[f][p * K * 3 + k * 3 + c];
+                }
             }
-            for (size_t p = 0; p < N_; ++p)
-                for (int c = 0; c < 3; ++c) hx[(p * 3 + c) * M + m] = gs[p * K * 3 + k * 3 + c];
-            for (size_t q = 0; q < Nq_; ++q)
-                for (int c = 0; c < 5; ++c) hx[(N_ * 3 + q * 5 + c) * M + m] = gs[N_ * K * 3 + q * K * 5 + k * 5 + c];
         }
     }
+    for (size_t q = 0; q < Nq_; ++q)
+        for (int c = 0; c < 5; ++c) {
+            const size_t row = N_ * 3 + q * 5 + c;
+            cdouble* br = hb + row * M;
+            cdouble* xr = hx + row * M;
+            for (size_t k = 0; k < K; ++k) {
+                const auto& e = E0_[k];
+                const cdouble ev = (e.size() == rows) ? e[row] : cdouble(0.0);
+                for (size_t f = 0; f < F; ++f) {
+                    br[f * K + k] = ev;
+                    xr[f * K + k] = guesses[f][N_ * K * 3 + q * K * 5 + k * 5 + c];
+                }
+            }
+        }
     const size_t bytes = sizeof(double2) * rows * M;
     dB_.ensure(bytes);
     dX_.ensure(bytes);
@@ -197,23 +208,30 @@ void DipoleSolver::solve_batch(const std::vector<size_t>& freqs, const std::vect
     for (int v : last_stats_.iters) iters_.push_back(v);
     MPM_CUDA(cudaMemcpyAsync(hx, dX_.p, bytes, cudaMemcpyDeviceToHost, stream_));
     MPM_CUDA(cudaStreamSynchronize(stream_));
-    for (size_t f = 0; f < freqs.size(); ++f) {
-        const size_t w = freqs[f];
-        for (size_t k = 0; k < K; ++k) {
-            const size_t m = f * K + k;
-            cdouble avg[3] = {0.0, 0.0, 0.0};
-            for (size_t p = 0; p < N_; ++p)
-                for (int c = 0; c < 3; ++c) {
-                    const cdouble v = hx[(p * 3 + c) * M + m];
-                    frame_dip[w * N_ * K * 3 + p * K * 3 + k * 3 + c] = v;
-                    avg[c] += v;
+    std::vector<cdouble> avg(size_t(M) * 3, 0.0);
+    for (size_t p = 0; p < N_; ++p)
+        for (int c = 0; c < 3; ++c) {
+            const cdouble* xr = hx + (p * 3 + c) * M;
+            for (size_t f = 0; f < F; ++f) {
+                cdouble* dst = frame_dip.data() + freqs[f] * N_ * K * 3 + p * K * 3 + c;
+                for (size_t k = 0; k < K; ++k) {
+                    const cdouble v = xr[f * K + k];
+                    dst[k * 3] = v;
+                    avg[(f * K + k) * 3 + c] += v;
                 }
-            for (size_t q = 0; q < Nq_; ++q)
-                for (int c = 0; c < 5; ++c)
-                    frame_quad[w * Nq_ * K * 5 + q * K * 5 + k * 5 + c] = hx[(N_ * 3 + q * 5 + c) * M + m];
-            for (int c = 0; c < 3; ++c) frame_cap[w * K * 3 + k * 3 + c] = avg[c] / double(N_);
+            }
         }
-    }
+    for (size_t q = 0; q < Nq_; ++q)
+        for (int c = 0; c < 5; ++c) {
+            const cdouble* xr = hx + (N_ * 3 + q * 5 + c) * M;
+            for (size_t f = 0; f < F; ++f)
+                for (size_t k = 0; k < K; ++k)
+                    frame_quad[freqs[f] * Nq_ * K * 5 + q * K * 5 + k * 5 + c] = xr[f * K + k];
+        }
+    for (size_t f = 0; f < F; ++f)
+        for (size_t k = 0; k < K; ++k)
+            for (int c = 0; c < 3; ++c)
+                frame_cap[freqs[f] * K * 3 + k * 3 + c] = avg[(f * K + k) * 3 + c] / double(N_);
 }
 
 // dipole_solver.cu:495-607
