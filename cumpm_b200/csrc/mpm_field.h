@@ -203,6 +203,7 @@ private:
     DevBuf pcls_, prad_, pself_, ptrad_;  // class per particle, class radii, self value per particle, target radii
     int pcand_cap_ = 0;                   // largest spread candidate count of a tile
     DevBuf ptoff_, ptlist_, ptmax_;       // per-tile spread candidate lists (CSR), their largest size
+    DevBuf ptcnt_, ptclist_, ptruns_;     // per tile: candidates that cover it, their covered runs
     // adjoint: stacked [p | lam] columns, potential grid, per-pair table derivatives, self-value derivatives
     DevBuf adj_x_, adj_grid_, adj_part_, pair_dT_, pself_d_;
     long long pair_dT_for_ = -1;          // pair list the derivatives belong to

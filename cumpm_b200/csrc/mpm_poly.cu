@@ -184,6 +184,61 @@ __global__ void k_poly_cands(PolyTile t, const int* __restrict__ bin_start, cons
     }
 }
 
+// Covered runs of every tile candidate, built once per frame (thread per
+// tile, candidates in list order).  The support index along an axis is
+// k = (t0 + u - origin) mod N and a tile offset u is covered when k < P;
+// within a covered run k grows by one per voxel (P < N, so a wrap would pass
+// N-1 >= P, which is not covered): at most two runs per axis.  Run word:
+// u | len << 4 | k << 8; word 6 holds the run counts (2 bits per axis).
+// Candidates that miss the tile along an axis are dropped, the others keep
+// their order (so each voxel's sum keeps its order): cnt[tile] of them at the
+// tile's CSR offset in clist / 8 words each in cruns.
+__global__ void k_poly_runs(PolyTile t, const int4* __restrict__ base, const int* __restrict__ off,
+                            const int* __restrict__ list, int* __restrict__ cnt, int* __restrict__ clist,
+                            int* __restrict__ cruns) {
+    const int tile = blockIdx.x * blockDim.x + threadIdx.x;
+    const int ntile = t.nb[0] * t.nb[1] * t.nb[2];
+    if (tile >= ntile) return;
+    const int bx = tile % t.nb[0], by = (tile / t.nb[0]) % t.nb[1], bz = tile / (t.nb[0] * t.nb[1]);
+    const int t0[3] = {bx * 8, by * 8, bz * 8};
+    const int c0 = off[tile], c1 = off[tile + 1];
+    int kept = 0;
+    for (int c = c0; c < c1; ++c) {
+        const int i = list[c];
+        const int4 o = base[i];
+        const int org[3] = {o.x, o.y, o.z};
+        int w[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+        bool all = true;
+        for (int d = 0; d < 3; ++d) {
+            int nr = 0, open = 0, r0 = 0, r1 = 0;
+            int k = pmod(t0[d] - org[d], t.N[d]);
+            for (int u = 0; u < 8; ++u) {
+                const int cov = (t0[d] + u < t.N[d]) && k < t.P;
+                if (cov && open) {
+                    if (nr == 1) r0 += 1 << 4; else r1 += 1 << 4;
+                } else if (cov && nr < 2) {
+                    const int word = u | (1 << 4) | (k << 8);
+                    if (nr == 0) r0 = word; else r1 = word;
+                    ++nr;
+                    open = 1;
+                } else {
+                    open = 0;
+                }
+                k = k + 1 == t.N[d] ? 0 : k + 1;
+            }
+            w[2 * d] = r0;
+            w[2 * d + 1] = r1;
+            w[6] |= nr << (2 * d);
+            all = all && nr > 0;
+        }
+        if (!all) continue;
+        clist[c0 + kept] = i;
+        for (int q = 0; q < 8; ++q) cruns[size_t(c0 + kept) * 8 + q] = w[q];
+        ++kept;
+    }
+    cnt[tile] = kept;
+}
+
 // Spread onto one 8^3 voxel tile x CM consecutive columns per CTA.  The
 // tile's accumulators live in shared memory; the tile's candidate particles
 // are added one after another in candidate order, all threads sharing the
@@ -192,10 +247,10 @@ __global__ void k_poly_cands(PolyTile t, const int* __restrict__ bin_start, cons
 // atomics, and every voxel of the grid is written exactly once.
 // grid[((x*Ny+y)*Nz+z)*M + m].
 template <typename R, int CM>
-__global__ void __launch_bounds__(256) k_poly_spread(const double2* __restrict__ X, int M, const int4* __restrict__ base,
-                                                     const R* __restrict__ w, const int* __restrict__ toff,
-                                                     const int* __restrict__ tlist, PolyTile t,
-                                                     cplx<R>* __restrict__ grid) {
+__global__ void __launch_bounds__(256) k_poly_spread(const double2* __restrict__ X, int M, const R* __restrict__ w,
+                                                     const int* __restrict__ toff, const int* __restrict__ tcnt,
+                                                     const int* __restrict__ clist, const int* __restrict__ cruns,
+                                                     PolyTile t, cplx<R>* __restrict__ grid) {
     extern __shared__ __align__(16) unsigned char shraw[];
     cplx<R>* acc = reinterpret_cast<cplx<R>*>(shraw);              // [512][CM] tile accumulators
     cplx<R>* pm = acc + 512 * CM;                                 // [cap][3][CM] candidate moments
@@ -209,47 +264,15 @@ __global__ void __launch_bounds__(256) k_poly_spread(const double2* __restrict__
     const int bx = tile % t.nb[0], by = (tile / t.nb[0]) % t.nb[1], bz = tile / (t.nb[0] * t.nb[1]);
     const int t0[3] = {bx * 8, by * 8, bz * 8};
     const int c0 = toff[tile];
-    const int nc = min(toff[tile + 1] - c0, t.cap);
+    const int nc = min(tcnt[tile], t.cap);
     const int P = t.P, P3 = P * P * P;
-    // Covered tile offsets of candidate c along each axis: the support index
-    // k = (t0 + u - origin) mod N must be < P.  Within a covered run k grows
-    // by one per voxel (P < N, so a wrap would pass N-1 >= P, which is not
-    // covered); at most two runs per axis.  Run word: u | len << 4 | k << 8.
-    for (int c = threadIdx.x; c < nc; c += blockDim.x) {
-        const int i = tlist[c0 + c];
-        cand[c] = i;
-        const int4 o = base[i];
-        const int org[3] = {o.x, o.y, o.z};
-        int nrs = 0;
-#pragma unroll
-        for (int d = 0; d < 3; ++d) {
-            int nr = 0, open = 0, r0 = 0, r1 = 0;
-            int k = pmod(t0[d] - org[d], t.N[d]);
-#pragma unroll
-            for (int u = 0; u < 8; ++u) {
-                const int cov = (t0[d] + u < t.N[d]) && k < P;
-                if (cov && open) {
-                    if (nr == 1) r0 += 1 << 4; else r1 += 1 << 4;
-                } else if (cov && nr < 2) {
-                    const int word = u | (1 << 4) | (k << 8);
-                    if (nr == 0) r0 = word; else r1 = word;
-                    ++nr;
-                    open = 1;
-                } else {
-                    open = 0;
-                }
-                k = k + 1 == t.N[d] ? 0 : k + 1;
-            }
-            runs[c * 8 + 2 * d] = r0;
-            runs[c * 8 + 2 * d + 1] = r1;
-            nrs |= nr << (2 * d);
-        }
-        runs[c * 8 + 6] = nrs;
-    }
+    // the tile's covering candidates and their runs (k_poly_runs)
+    for (int c = threadIdx.x; c < nc; c += blockDim.x) cand[c] = clist[c0 + c];
+    for (int q = threadIdx.x; q < nc * 8; q += blockDim.x) runs[q] = cruns[size_t(c0) * 8 + q];
     for (int k = threadIdx.x; k < nc * 3 * CM; k += blockDim.x) {
         const int cm = k % CM, comp = (k / CM) % 3, c = k / (3 * CM);
         const int m = m0 + cm;
-        pm[k] = m < M ? to_r<R>(X[size_t(3 * tlist[c0 + c] + comp) * M + m]) : mk<R>(0, 0);
+        pm[k] = m < M ? to_r<R>(X[size_t(3 * clist[c0 + c] + comp) * M + m]) : mk<R>(0, 0);
     }
     for (int k = threadIdx.x; k < 512 * CM; k += blockDim.x) acc[k] = mk<R>(0, 0);
     __syncthreads();
@@ -537,6 +560,12 @@ void Field::poly_weights(PointSet& ps, const double* radius_dev, cudaStream_t s,
                                                   ps.idx_sorted.as<int>(), 1, nullptr, nullptr, ptoff_.as<int>(),
                                                   ptlist_.as<int>());
     MPM_LAUNCH();
+    ptcnt_.ensure(sizeof(int) * std::max(1, nbins));
+    ptclist_.ensure(sizeof(int) * std::max(1, hv[1]));
+    ptruns_.ensure(sizeof(int) * 8 * size_t(std::max(1, hv[1])));
+    k_poly_runs<<<nblk(nbins, 128), 128, 0, s>>>(t, ps.base.as<int4>(), ptoff_.as<int>(), ptlist_.as<int>(),
+                                                 ptcnt_.as<int>(), ptclist_.as<int>(), ptruns_.as<int>());
+    MPM_LAUNCH();
     pcand_cap_ = std::max(1, h);
     const size_t shm = 65536 + (3 * 128 + 9 * sizeof(int)) * size_t(pcand_cap_);
     if (shm > 200 * 1024 || pgeom_.P > 255)
@@ -587,7 +616,7 @@ void Field::poly_recip_on(const double2* X, double2* Y, int M, cplx<R>* grid, cu
     {
         StageScope sc(ST_SPREAD, s);
         k_poly_spread<R, CM><<<ntile * ((M + CM - 1) / CM), 256, shm, s>>>(
-            X, M, ps.base.as<int4>(), w1, ptoff_.as<int>(), ptlist_.as<int>(), t, grid);
+            X, M, w1, ptoff_.as<int>(), ptcnt_.as<int>(), ptclist_.as<int>(), ptruns_.as<int>(), t, grid);
         MPM_LAUNCH();
     }
     const R* scl = sizeof(R) == 4 ? reinterpret_cast<const R*>(scale32_.p) : reinterpret_cast<const R*>(scale64_.p);
