@@ -85,14 +85,24 @@ void DipoleSolver::nondimensionalize() {
 std::vector<cdouble> DipoleSolver::mean_field_guess(size_t w) const {
     const size_t K = E0_.size();
     std::vector<cdouble> g(N_ * K * 3 + Nq_ * K * 5, 0.0);
+    // complex quotient a / b written out (std::complex division guards
+    // against overflow and is several times slower; these values are O(1))
+    auto quot = [](cdouble a, cdouble b) {
+        const double d = std::norm(b);
+        return cdouble((a.real() * b.real() + a.imag() * b.imag()) / d,
+                       (a.imag() * b.real() - a.real() * b.imag()) / d);
+    };
     for (size_t p = 0; p < N_; ++p) {
-        const cdouble beta = (eps_p_[w][p] - 1.0) / (eps_p_[w][p] + 2.0);
-        const cdouble val = 4.0 * PI * std::pow(radius_[p], 3.0) * beta / (1.0 - beta * vol_frac_);
-        for (size_t d = 0; d < K; ++d)
-            for (int c = 0; c < 3; ++c) {
-                const cdouble e = E0_[d].size() > 3 ? E0_[d][p * 3 + c] : E0_[d][c];
-                g[p * K * 3 + d * 3 + c] = val * e;
-            }
+        const cdouble e = eps_p_[w][p];
+        const cdouble beta = quot(e - 1.0, e + 2.0);
+        const double r = radius_[p];
+        const cdouble val = quot(4.0 * PI * r * r * r * beta, 1.0 - beta * vol_frac_);
+        for (size_t d = 0; d < K; ++d) {
+            const std::vector<cdouble>& ed = E0_[d];
+            const cdouble* ev = ed.size() > 3 ? ed.data() + p * 3 : ed.data();
+            cdouble* gp = g.data() + p * K * 3 + d * 3;
+            for (int c = 0; c < 3; ++c) gp[c] = val * ev[c];
+        }
     }
     return g;
 }
@@ -286,11 +296,11 @@ void DipoleSolver::compute(const std::vector<double>& x, const std::vector<doubl
         // previous frame's first frequency (dipole_solver.cu:576-593)
         const size_t prev = num_frames_ - 2;
         init.assign(N_ * K * 3 + Nq_ * K * 5, 0.0);
-        const size_t off = prev * W * N_ * K * 3;
-        std::copy(dips_.begin() + off, dips_.begin() + off + N_ * K * 3, init.begin());
+        const std::vector<cdouble>& pd = dip_frames_[prev];
+        std::copy(pd.begin(), pd.begin() + N_ * K * 3, init.begin());
         if (solve_quads_ && Nq_) {
-            const size_t qo = prev * W * Nq_ * K * 5;
-            std::copy(quads_.begin() + qo, quads_.begin() + qo + Nq_ * K * 5, init.begin() + N_ * K * 3);
+            const std::vector<cdouble>& pq = quad_frames_[prev];
+            std::copy(pq.begin(), pq.begin() + Nq_ * K * 5, init.begin() + N_ * K * 3);
         }
     }
     std::vector<cdouble> frame_cap(W * K * 3, 0.0), frame_dip(W * N_ * K * 3, 0.0), frame_quad(W * Nq_ * K * 5, 0.0);
@@ -313,8 +323,8 @@ void DipoleSolver::compute(const std::vector<double>& x, const std::vector<doubl
     }
     indent_--;
     avg_dips_.insert(avg_dips_.end(), frame_cap.begin(), frame_cap.end());
-    dips_.insert(dips_.end(), frame_dip.begin(), frame_dip.end());
-    if (solve_quads_ && Nq_) quads_.insert(quads_.end(), frame_quad.begin(), frame_quad.end());
+    dip_frames_.push_back(std::move(frame_dip));
+    quad_frames_.push_back(solve_quads_ && Nq_ ? std::move(frame_quad) : std::vector<cdouble>());
 }
 
 // dipole_solver.cu:613-647
@@ -332,25 +342,37 @@ std::vector<cdouble> DipoleSolver::get_eff_polarizability(bool physical) const {
     return out;
 }
 
+namespace {
+// every frame's values, frames concatenated, times f
+std::vector<cdouble> concat_frames(const std::vector<std::vector<cdouble>>& frames, double f) {
+    size_t n = 0;
+    for (const auto& fr : frames) n += fr.size();
+    std::vector<cdouble> out;
+    out.reserve(n);
+    for (const auto& fr : frames)
+        for (const cdouble& v : fr) out.push_back(v * f);
+    return out;
+}
+}  // namespace
+
 std::vector<cdouble> DipoleSolver::get_dipoles(bool physical) const {
     const double f = physical ? eps_scale_ * std::pow(length_scale_, 3.0) : 1.0;
-    std::vector<cdouble> out = dips_;
-    for (auto& v : out) v *= f;
-    return out;
+    return concat_frames(dip_frames_, f);
 }
 
 size_t DipoleSolver::get_dipoles_into(bool physical, cdouble* out, size_t cap) const {
-    if (cap < dips_.size()) throw std::invalid_argument("output buffer too small");
+    size_t n = 0;
+    for (const auto& fr : dip_frames_) n += fr.size();
+    if (cap < n) throw std::invalid_argument("output buffer too small");
     const double f = physical ? eps_scale_ * std::pow(length_scale_, 3.0) : 1.0;
-    for (size_t k = 0; k < dips_.size(); ++k) out[k] = dips_[k] * f;
-    return dips_.size();
+    for (const auto& fr : dip_frames_)
+        for (const cdouble& v : fr) *out++ = v * f;
+    return n;
 }
 
 std::vector<cdouble> DipoleSolver::get_quadrupoles(bool physical) const {
     const double f = physical ? eps_scale_ * std::pow(length_scale_, 4.0) : 1.0;
-    std::vector<cdouble> out = quads_;
-    for (auto& v : out) v *= f;
-    return out;
+    return concat_frames(quad_frames_, f);
 }
 
 // ---------------------------------------------------------------- NearField

@@ -83,7 +83,9 @@ private:
 
     size_t N_ = 0, Nq_ = 0, num_frames_ = 0;
     double length_scale_ = 1.0, eps_scale_ = 1.0, vol_frac_ = 0.0;
-    std::vector<cdouble> avg_dips_, dips_, quads_;
+    std::vector<cdouble> avg_dips_;
+    // one vector per frame (appending a frame copies nothing already stored)
+    std::vector<std::vector<cdouble>> dip_frames_, quad_frames_;
     std::vector<int> iters_;
     SolveStats last_stats_;
 
