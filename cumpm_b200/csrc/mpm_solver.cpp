@@ -158,16 +158,21 @@ void DipoleSolver::solve_batch(const std::vector<size_t>& freqs, const std::vect
     cdouble* hx = hX_.as<cdouble>();
     cdouble* hsc = hSC_.as<cdouble>();
     const size_t F = freqs.size();
+    // the right-hand sides and self terms of a batch depend only on its
+    // frequencies: rebuilt (and copied to the device) when those change
+    const bool rebuild = freqs != dev_freqs_;
     // rows outermost so that every host array is written contiguously
     // ([row][M] with m = f * K + k)
     for (size_t p = 0; p < N_; ++p) {
-        cdouble* sp = hsc + p * M;
-        for (size_t f = 0; f < F; ++f) {
-            // self coefficients s = -3 / (4 pi (1 - eps) a^3) (dipole_solver.cu:452-460)
-            cdouble diff = 1.0 - eps_p_[freqs[f]][p];
-            if (std::abs(diff) < 1e-12) diff = 1e-12;
-            const cdouble sv = -3.0 / (4.0 * PI * diff) / std::pow(radius_[p], 3.0);
-            for (size_t k = 0; k < K; ++k) sp[f * K + k] = sv;
+        if (rebuild) {
+            cdouble* sp = hsc + p * M;
+            for (size_t f = 0; f < F; ++f) {
+                // self coefficients s = -3 / (4 pi (1 - eps) a^3) (dipole_solver.cu:452-460)
+                cdouble diff = 1.0 - eps_p_[freqs[f]][p];
+                if (std::abs(diff) < 1e-12) diff = 1e-12;
+                const cdouble sv = -3.0 / (4.0 * PI * diff) / std::pow(radius_[p], 3.0);
+                for (size_t k = 0; k < K; ++k) sp[f * K + k] = sv;
+            }
         }
         for (int c = 0; c < 3; ++c) {
             const size_t row = p * 3 + c;
@@ -177,7 +182,7 @@ void DipoleSolver::solve_batch(const std::vector<size_t>& freqs, const std::vect
                 const auto& e = E0_[k];
                 const cdouble ev = e.size() == 3 ? e[c] : e[row];
                 for (size_t f = 0; f < F; ++f) {
-                    br[f * K + k] = ev;
+                    if (rebuild) br[f * K + k] = ev;
                     xr[f * K + k] = guesses[f][p * K * 3 + k * 3 + c];
                 }
             }
@@ -192,7 +197,7 @@ void DipoleSolver::solve_batch(const std::vector<size_t>& freqs, const std::vect
                 const auto& e = E0_[k];
                 const cdouble ev = (e.size() == rows) ? e[row] : cdouble(0.0);
                 for (size_t f = 0; f < F; ++f) {
-                    br[f * K + k] = ev;
+                    if (rebuild) br[f * K + k] = ev;
                     xr[f * K + k] = guesses[f][N_ * K * 3 + q * K * 5 + k * 5 + c];
                 }
             }
@@ -201,9 +206,11 @@ void DipoleSolver::solve_batch(const std::vector<size_t>& freqs, const std::vect
     dB_.ensure(bytes);
     dX_.ensure(bytes);
     dSC_.ensure(sizeof(double2) * N_ * M);
-    MPM_CUDA(cudaMemcpyAsync(dB_.p, hb, bytes, cudaMemcpyHostToDevice, stream_));
+    if (rebuild) {
+        MPM_CUDA(cudaMemcpyAsync(dB_.p, hb, bytes, cudaMemcpyHostToDevice, stream_));
+        MPM_CUDA(cudaMemcpyAsync(dSC_.p, hsc, sizeof(double2) * N_ * M, cudaMemcpyHostToDevice, stream_));
+    }
     MPM_CUDA(cudaMemcpyAsync(dX_.p, hx, bytes, cudaMemcpyHostToDevice, stream_));
-    MPM_CUDA(cudaMemcpyAsync(dSC_.p, hsc, sizeof(double2) * N_ * M, cudaMemcpyHostToDevice, stream_));
     SolveOptions so;
     so.method = solver_type_ == "bicgstab" ? SOLVER_BICGSTAB : SOLVER_GMRES;
     so.restart = opt_.restart;
@@ -218,6 +225,7 @@ void DipoleSolver::solve_batch(const std::vector<size_t>& freqs, const std::vect
     for (int v : last_stats_.iters) iters_.push_back(v);
     MPM_CUDA(cudaMemcpyAsync(hx, dX_.p, bytes, cudaMemcpyDeviceToHost, stream_));
     MPM_CUDA(cudaStreamSynchronize(stream_));
+    dev_freqs_ = freqs;
     std::vector<cdouble> avg(size_t(M) * 3, 0.0);
     for (size_t p = 0; p < N_; ++p)
         for (int c = 0; c < 3; ++c) {

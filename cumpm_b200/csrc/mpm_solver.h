@@ -94,6 +94,9 @@ private:
     cudaStream_t stream_ = nullptr;
     DevBuf dB_, dX_, dSC_;
     HostBuf hB_, hX_, hSC_;   // pinned staging of the batch's right-hand sides, guesses / solutions, self terms
+    // frequencies whose right-hand sides and self terms dB_ / dSC_ hold (they
+    // depend on nothing that changes between frames)
+    std::vector<size_t> dev_freqs_;
     int indent_ = 0;
 };
 
