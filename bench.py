@@ -261,6 +261,23 @@ def algorithmic_bytes(info, M, n_pairs, fp64, mono=True):
     return b
 
 
+def replica_throughput(t_ms, units, dist=None, device="cpu"):
+    """Whole-job throughput of independent replicas: (slowest rank's time in
+    ms, units summed over the ranks, units per second over that time).
+    Every rank takes the same two collectives; without a process group the
+    rank's own figures."""
+    import torch
+
+    t_max, total = float(t_ms), int(units)
+    if dist is not None:
+        tt = torch.tensor([t_ms], device=device, dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        cc = torch.tensor([units], device=device, dtype=torch.float64)
+        dist.all_reduce(cc)
+        t_max, total = float(tt.item()), int(round(cc.item()))
+    return t_max, total, total / (t_max / 1e3)
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
 
@@ -324,17 +341,8 @@ def run_ours(args, rank, world, local_rank):
     R = B - F.apply(X, self_coef=S)
     rel = (torch.linalg.vector_norm(R, dim=0) / torch.linalg.vector_norm(B, dim=0)).cpu().numpy()
     converged = int(np.sum(rel <= TOL))
-    t_max = t_ms
-    conv_total = converged * args.steps
-    if dist:
-        tt = torch.tensor([t_ms], device=dev)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        t_max = float(tt.item())
-        cc = torch.tensor([conv_total], device=dev, dtype=torch.float64)
-        dist.all_reduce(cc)
-        conv_total = int(cc.item())
+    t_max, conv_total, value = replica_throughput(t_ms, converged * args.steps, dist, dev)
     ms_per_step = t_max / args.steps
-    value = conv_total / (t_max / 1e3)
 
     # 2) the same steps again with per-stage CUDA events on the launching
     #    stream: stage breakdown and the roofline of the dominant stage
