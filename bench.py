@@ -442,7 +442,7 @@ def run_ours(args, rank, world, local_rank):
                 "algorithmic_bytes_full_batch_fp32": b32[dom],
                 "launches": dom_n,
                 "timing": "per-stage CUDA events on the launching stream over a second pass of the timed steps",
-            },
+            } if dom_ms > 0 else None,   # --no-profile: no stage timings, no roofline
             "cpu_baseline": cpu,
             "e2e": e2e,
             "gpu_launches": launches,
