@@ -1,0 +1,133 @@
+"""cumpm_b200.dev (the reference's cuMPM.dev field classes on this build's
+field operator) on the GPU: field-point and solver modes, the monodisperse /
+polydisperse agreement and the real / reciprocal split the reference's
+tests/test_electric_fields.py checks, precision modes, and the monodisperse
+class against the reference build itself when it is present."""
+import os
+import sys
+
+import numpy as np
+import pytest
+
+torch = pytest.importorskip("torch")
+
+pytestmark = pytest.mark.gpu
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+REF_DIR = os.path.join(ROOT, "oracle", "_ref")
+
+
+def line_system(n, spacing):
+    pos = np.zeros((n, 3))
+    pos[:, 0] = spacing * np.arange(n)
+    return pos
+
+
+def test_direct_field_points():
+    from cumpm_b200 import capi, dev
+
+    ef = dev.DirectElectricField(np.array([1.0, 1.2, 1.5]), mode=False, precision="double")
+    ef.update_particle_coordinates([0.0, 2.0, 4.0], [0.0] * 3, [0.0] * 3)
+    ef.update_field_coordinates([1.0, 3.0], [0.0, 0.0], [0.0, 0.0])
+    ef.update_dipoles_complex(np.ones(3), np.zeros(3), np.zeros(3), np.zeros(3), np.zeros(3), np.zeros(3))
+    ef.set_self_coef(np.ones(3), np.zeros(3))
+    assert ef.num_particles == 3 and ef.num_field_points == 2
+    ef.calculate()
+    E = ef.get_epoint_host()
+    assert E.shape == (2, 3) and np.all(np.isfinite(E))
+    F = capi.Field(capi.FIELD_DIRECT, None, mode=capi.MODE_INTERACTION, radius=[1.0, 1.2, 1.5])
+    F.set_field_points(np.array([[1.0, 0, 0], [3.0, 0, 0]]))
+    F.set_positions(np.array([[0.0, 0, 0], [2.0, 0, 0], [4.0, 0, 0]]))
+    X = torch.tensor(np.array([1, 0, 0] * 3, dtype=complex).reshape(-1, 1), device="cuda")
+    np.testing.assert_allclose(E.ravel(), F.apply(X).cpu().numpy()[:, 0], rtol=1e-14, atol=0)
+
+
+def test_monodisperse_polydisperse_agreement_and_splits():
+    from cumpm_b200 import dev
+
+    pos = line_system(4, 5.0)
+    fields = []
+    for cls, extra in ((dev.MonodisperseEwaldElectricField, ()), (dev.PolydisperseEwaldElectricField, ([1.0] * 4,))):
+        ef = cls(20.0, 20.0, 20.0, 1e-6, 0.5, True, *extra, precision="double")
+        ef.update_particle_coordinates(pos[:, 0], pos[:, 1], pos[:, 2])
+        ef.update_dipoles(np.ones(4), np.zeros(4), np.zeros(4))
+        ef.set_self_coef(np.ones(4), np.zeros(4))
+        ef.calculate()
+        tot = ef.get_epoint_host()
+        real = ef.compute_real_field()
+        inv = ef.compute_inverse_field()
+        np.testing.assert_allclose(tot, real + inv, rtol=1e-12, atol=1e-12)
+        assert np.abs(inv).max() > 0 and np.abs(real).max() > 0
+        fields.append(tot)
+    np.testing.assert_allclose(fields[0], fields[1], rtol=1e-5, atol=1e-5)
+
+
+def test_monodisperse_quadrupole_splits():
+    from cumpm_b200 import dev
+
+    pos = line_system(4, 4.0)
+    ef = dev.MonodisperseEwaldElectricField(20.0, 20.0, 20.0, 1e-6, 0.5, True, solve_quadrupoles=True,
+                                            quad_idxs=[0, 2], precision="double")
+    ef.update_particle_coordinates(pos[:, 0], pos[:, 1], pos[:, 2])
+    ef.update_dipoles(np.ones(4), np.zeros(4), np.zeros(4))
+    ef.update_quadrupoles(np.ones(2), np.zeros(2), np.zeros(2), np.zeros(2), np.zeros(2))
+    ef.set_self_coef(np.ones(4), np.zeros(4))
+    ef.calculate()
+    E, G = ef.get_epoint_host()
+    assert E.shape == (4, 3) and G.shape == (2, 5)
+    Er, Gr = ef.compute_real_field()
+    Ei, Gi = ef.compute_inverse_field()
+    np.testing.assert_allclose(E, Er + Ei, rtol=1e-12, atol=1e-12)
+    np.testing.assert_allclose(G, Gr + Gi, rtol=1e-12, atol=1e-12)
+
+
+def test_precision_modes():
+    from cumpm_b200 import dev
+
+    out = {}
+    for prec in (dev.PrecisionMode.FP64, dev.PrecisionMode.FP32):
+        ef = dev.DirectElectricField(np.array([1.0, 1.2, 1.5]), mode=False, precision=prec)
+        ef.update_particle_coordinates([0.0, 2.0, 4.0], [0.0] * 3, [0.0] * 3)
+        ef.update_field_coordinates([1.0, 3.0], [0.0, 0.0], [0.0, 0.0])
+        ef.update_dipoles_complex(np.ones(3), np.zeros(3), np.zeros(3), np.zeros(3), np.zeros(3), np.zeros(3))
+        ef.calculate()
+        out[prec] = ef.get_epoint_host()
+    np.testing.assert_allclose(out[dev.PrecisionMode.FP32], out[dev.PrecisionMode.FP64], rtol=1e-5, atol=1e-5)
+    out = {}
+    for prec in ("double", "mixed"):
+        ef = dev.MonodisperseEwaldElectricField(50.0, 50.0, 50.0, 1e-4, 0.5, True, precision=prec)
+        ef.update_particle_coordinates([0.0, 2.0, 4.0], [0.0] * 3, [0.0] * 3)
+        ef.update_dipoles(np.ones(3), np.zeros(3), np.zeros(3))
+        ef.calculate()
+        out[prec] = ef.get_epoint_host()
+    np.testing.assert_allclose(out["mixed"], out["double"], rtol=1e-4, atol=1e-4)
+
+
+def test_monodisperse_class_vs_reference_build():
+    if not os.path.isdir(REF_DIR) or not any(f.startswith("_cuMPM") for f in os.listdir(REF_DIR)):
+        pytest.skip("reference build oracle/_ref not present")
+    sys.path.insert(0, REF_DIR)
+    try:
+        import _cuMPM as R
+    finally:
+        sys.path.remove(REF_DIR)
+    from cumpm_b200 import dev
+
+    rng = np.random.default_rng(5)
+    pos = rng.uniform(0, 20, (12, 3))
+    P = rng.standard_normal((12, 3)) + 1j * rng.standard_normal((12, 3))
+    sc = rng.standard_normal(12) + 1j * rng.standard_normal(12)
+    ref = R.Monodisperse_Ewald_Electric_Field(20.0, 20.0, 20.0, 1e-6, 0.5, R.FieldCalcMode.SOLVER_AX, 1.0, False, [],
+                                              R.PrecisionMode.DOUBLE)
+    ref.updateParticleCoordinates(*[list(pos[:, d]) for d in range(3)])
+    ref.updateDipolesComplex(*[list(f(P[:, d])) for d in range(3) for f in (np.real, np.imag)])
+    ref.setSelfCoef(list(sc.real), list(sc.imag))
+    ref.calculate()
+    E_ref = np.asarray(ref.getEPointHost())
+    ef = dev.MonodisperseEwaldElectricField(20.0, 20.0, 20.0, 1e-6, 0.5, True, precision="double")
+    ef.update_particle_coordinates(pos[:, 0], pos[:, 1], pos[:, 2])
+    ef.update_dipoles_complex(*[f(P[:, d]) for d in range(3) for f in (np.real, np.imag)])
+    ef.set_self_coef(sc.real, sc.imag)
+    ef.calculate()
+    np.testing.assert_allclose(ef.get_epoint_host(reshape=False), E_ref, rtol=1e-11,
+                               atol=1e-12 * np.abs(E_ref).max())
