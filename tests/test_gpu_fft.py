@@ -13,12 +13,13 @@ pytestmark = pytest.mark.gpu
 
 # two-pass splits in registers: 2 = 2x1, 16 = 4x4, 49 = 7x7, 80 = 10x8,
 # 108 = 12x9, 112 = 14x8, 143 = 13x11, 256 = 16x16; with a Rader prime pass
-# (p - 1 = A x B in registers): 97 = 1x97 (96 = 12x8), 238 = 14x17 (16 = 4x4),
-# 366 = 6x61 (60 = 10x6); with a streamed prime pass: 206 = 2x103 (102 has
-# no such split); general only: 289 = 17*17
-LENGTHS = [2, 16, 49, 80, 97, 108, 112, 143, 206, 238, 256, 289, 366]
-SPLITS = {2: (2, 1), 16: (4, 4), 49: (7, 7), 80: (10, 8), 108: (12, 9), 112: (14, 8), 143: (13, 11),
-          256: (16, 16), 97: (1, 97), 206: (2, 103), 238: (14, 17), 366: (6, 61)}
+# (p - 1 = A x B in registers): 34 = 2x17 (16 = 4x4, radix <= 8 class),
+# 97 = 1x97 (96 = 12x8), 238 = 14x17 (16 = 4x4), 366 = 6x61 (60 = 10x6); with
+# a streamed prime pass: 206 = 2x103 (102 has no such split); general only:
+# 289 = 17*17
+LENGTHS = [2, 16, 34, 49, 80, 97, 108, 112, 143, 206, 238, 256, 289, 366]
+SPLITS = {2: (2, 1), 16: (4, 4), 34: (2, 17), 49: (7, 7), 80: (10, 8), 108: (12, 9), 112: (14, 8),
+          143: (13, 11), 256: (16, 16), 97: (1, 97), 206: (2, 103), 238: (14, 17), 366: (6, 61)}
 
 
 def run_case(n, layout, ncols, nouter, fp64, mode, general, seed=0, sb=4):
