@@ -1113,14 +1113,14 @@ void AxisFFT::init(int n) {
     }
     f_.pt_total = int(p64.size());
     upload_table(p64, pt64_, pt32_);
-    // the prime-streamed two-pass kernel's table
-    // Rader tables when p - 1 splits into two in-register radices
+    // Rader tables when p - 1 splits into two in-register radices and the
+    // kernel's shared memory fits at its narrowest tile (4 fp64 columns)
     ra_ = rb_ = 0;
     if (kind_ == 2) {
         const int pr = r2_, N = pr - 1;
         const std::pair<int, int> ab = fft2_split(N);
         const int g = primitive_root(pr);
-        if (ab.first && g) {
+        if (ab.first && g && fft2r_smem(n, r1_, N, 4, sizeof(double2)) <= kFftSmemBudget) {
             kind_ = 3;
             ra_ = ab.first;
             rb_ = ab.second;
@@ -1159,12 +1159,20 @@ void AxisFFT::init(int n) {
             MPM_CUDA(cudaMemcpy(rperm_.p, perm.data(), sizeof(int) * perm.size(), cudaMemcpyHostToDevice));
         }
     }
+    // the streamed prime pass's table; lengths whose table and tile do not
+    // fit in shared memory go to the general multi-pass kernel
     pp_total_ = pp_ld_ = 0;
     if (kind_ == 2) {
         std::vector<double2> q64;
-        pp_ld_ = append_prime_table(r2_, q64);
-        pp_total_ = int(q64.size());
-        upload_table(q64, pp64_, pp32_);
+        const int ld = append_prime_table(r2_, q64);
+        if (fft2p_smem(n, 4, sizeof(double2), int(q64.size())) <= kFftSmemBudget) {
+            pp_ld_ = ld;
+            pp_total_ = int(q64.size());
+            upload_table(q64, pp64_, pp32_);
+        } else {
+            kind_ = 0;
+            r1_ = r2_ = 0;
+        }
     }
 }
 
