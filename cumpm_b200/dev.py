@@ -169,6 +169,8 @@ class _Field:
         return self._F
 
     def _inputs(self):
+        """(X, self terms) as CUDA tensors; every size is checked on the host
+        first, so a mismatch never reaches a device call."""
         import torch
 
         n = self.num_particles
@@ -182,11 +184,13 @@ class _Field:
             if q.shape != (nq, 5):
                 raise ValueError("quadrupoles must have one entry per quadrupole index")
             parts.append(q.ravel())
-        X = torch.tensor(np.concatenate(parts).reshape(-1, 1), dtype=torch.complex128, device="cuda")
-        sc = None
+        s = None
         if self._mode != FieldCalcMode.INTERACTION_FIELD:
             s = self._self if self._self is not None else np.zeros(n, complex)
-            sc = torch.tensor(np.asarray(s, dtype=complex).reshape(-1, 1), device="cuda")
+            if len(s) != n:
+                raise ValueError("self coefficients must have one entry per particle")
+        X = torch.tensor(np.concatenate(parts).reshape(-1, 1), dtype=torch.complex128, device="cuda")
+        sc = None if s is None else torch.tensor(np.asarray(s, dtype=complex).reshape(-1, 1), device="cuda")
         return X, sc
 
     def calculate(self):

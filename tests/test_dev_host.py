@@ -42,3 +42,19 @@ def test_named_gaps():
         ef.set_bloch_wavevector(0.1, 0.0)
     with pytest.raises(ValueError, match="radius"):
         dev.MonodisperseEwaldElectricField(20.0, 20.0, 20.0, 1e-6, 0.5, True, radius=2.0)
+
+
+def test_inputs_must_match_particle_count():
+    """Mismatched inputs are rejected on the host, before any device call."""
+    from cumpm_b200 import dev
+
+    ef = dev.MonodisperseEwaldElectricField(20.0, 20.0, 20.0, 1e-6, 0.5, True)
+    ef.set_self_coef(1.0)                       # no particles yet: zero entries
+    ef.update_particle_coordinates([0, 4, 8], [0, 0, 0], [0, 0, 0])
+    ef.update_dipoles(np.ones(3), np.zeros(3), np.zeros(3))
+    with pytest.raises(ValueError, match="self coefficients"):
+        ef._inputs()
+    ef.set_self_coef(np.ones(3))
+    ef.update_dipoles(np.ones(2), np.zeros(2), np.zeros(2))
+    with pytest.raises(ValueError, match="dipoles"):
+        ef._inputs()
