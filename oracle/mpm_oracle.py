@@ -25,6 +25,15 @@ What it restates (reference ``file:line``):
   table nodes and interpolation ``:170-187, 1629-1687``, spread weights
   ``:189-350``, scale ``:565-651``, contraction ``:653-693``, real space
   ``:352-441, 695-826``, stage order ``:2553-2730``
+* polydisperse quadrupoles on the same scalar grid: radius-1 quadrupole
+  tables ``:1690-2035`` (gq2 and gq3 are the polydisperse field's own
+  expressions), point-Gaussian weights ``:828-922, 2114-2278``, joint scale
+  ``:565-638, 925-962``, spread and G contraction ``:964-1146``, joint self
+  and pair terms ``:1148-1428``.  Pinned by the shared tables against the
+  reference CPU operator's fixtures and by the reference's own solver-level
+  checks (equal radii against the monodisperse quadrupole solve, mixed radii
+  in a large box against the direct sum); not yet against the reference
+  build's polydisperse quadrupole field.
 * open-boundary direct sum: ``electric_field/direct_electric_field.cu:42-324``
 * Krylov solvers: ``numerical_solver/gmres_solver.cu:56-208``,
   ``numerical_solver/bicgstab_solver.cu:58-192``, Jacobi
@@ -100,13 +109,25 @@ TABLE_STEPS = 9000
 TABLE_DR = 0.001
 
 
-def mono_real_tables(xi):
-    """Return (r_table, dict name->values) of length 9001.
+def mono_real_tables(xi, r=None, variant="mono"):
+    """Return (r_table, dict name->values, selfo, self_grad).
 
-    Entry 0 is r=0 (the self value); entries 1.. are r = 1 + k*0.001.
+    Entry 0 is r=0 (the self value); entries 1.. are r = 1 + k*0.001, 9000
+    of them unless ``r`` gives the nodes (the polydisperse field sizes its
+    table by the cutoff, polydisperse_ewald_electric_field.cu:1629-1645).
     Names: fd1 (perp), fd2 (para), fq1, fq2, fq3, gq1..gq4.
+
+    ``variant="poly"`` gives the radius-1 quadrupole tables the polydisperse
+    field builds for itself (:1697-2035): fq1-fq3, gq1 and gq4 are the
+    monodisperse expressions, gq2 is a different expression and gq3 carries
+    the opposite sign on the r^5 and r^4 terms of its exp(-(r+2)^2 xi^2)
+    coefficient.
     """
-    r = 1.0 + np.arange(TABLE_STEPS) * TABLE_DR
+    if variant not in ("mono", "poly"):
+        raise ValueError("variant must be 'mono' or 'poly'")
+    if r is None:
+        r = 1.0 + np.arange(TABLE_STEPS) * TABLE_DR
+    r = np.asarray(r, dtype=np.float64)
     x = xi
     x2, x4, x6, x8, x10 = x ** 2, x ** 4, x ** 6, x ** 8, x ** 10
     x5, x7, x9 = x ** 5, x ** 7, x ** 9
@@ -238,11 +259,30 @@ def mono_real_tables(xi):
     f0 = -base / (32768 * PI * x10 * r5)
     reg = -3.0 / (2 * PI) * (1.0 / r5 - 1.0 + 25.0 * r / 32.0 - 25.0 * r3 / 256.0 + 3.0 * r5 / 512.0)
     t["gq2"] = _combo(r, x, ep, em, e0, fp, fm, f0, reg)
+    if variant == "poly":
+        # polydisperse grad_quad_2 (:1890-1924): odd and even parts of the
+        # exp(-(r -+ 2)^2 xi^2) polynomials, one erfc polynomial
+        c = -15.0 / (16384 * sp * x7 * r3)
+        odd = (24 * x6 * r7 + (148 * x4 - 96 * x6) * r5 + (90 * x2 + 72 * x4 + 256 * x8) * r3
+               - (45 + 120 * x2 - 192 * x4 + 512 * x6) * r)
+        even = (-48 * x6 * r6 - (264 * x4 - 192 * x6) * r4 + (60 * x2 - 144 * x4 + 512 * x8) * r2
+                - 2 * (45 + 24 * x2 - 64 * x4 + 512 * x6))
+        ep, em = c * (odd + even), c * (odd - even)
+        e0 = 75.0 / (8192 * sp * x7 * r2) * (8 * x6 * r6 + (44 * x4 - 64 * x6) * r4
+                                             + (18 * x2 - 48 * x4 + 128 * x6) * r2 - 9 + 40 * x2 - 192 * x4)
+        base = (48 * x8 * r8 + (288 * x6 - 384 * x8) * r6 + (216 * x4 - 576 * x6 + 768 * x8) * r4
+                - (72 * x2 - 288 * x4 + 768 * x6) * r2 + 45 - 240 * x2 + 960 * x4)
+        fp = -15.0 / (32768 * PI * x8 * r3) * (base - 4096 * x8 * r5 - 8192 * x8)
+        fm = -15.0 / (32768 * PI * x8 * r3) * (base + 4096 * x8 * r5 - 8192 * x8)
+        f0 = 15.0 / (16384 * PI * x8 * r3) * base
+        reg = -45.0 * r / (32 * PI) * (1.0 - 5.0 * r2 / 12.0 + r4 / 16.0)
+        t["gq2"] = _combo(r, x, ep, em, e0, fp, fm, f0, reg)
 
     # grad_quad_3 (:375-416)
     c = -15.0 / (65536 * sp * x9 * r5)
+    s54 = -1.0 if variant == "poly" else 1.0
     ep = c * (48 * x8 * r9 - 96 * x8 * r8 + (336 * x6 - 288 * x8) * r7 - 576 * (x6 - x8) * r6
-              + (216 * x4 + 144 * x6 + 128 * x8) * r5 - (480 * x6 + 256 * x8) * r4
+              + s54 * ((216 * x4 + 144 * x6 + 128 * x8) * r5 - (480 * x6 + 256 * x8) * r4)
               - (180 * x2 - 120 * x4 + 640 * x6 - 512 * x8) * r3
               + (720 * x4 + 768 * x6 - 1024 * x8) * r2
               + (135 + 180 * x2 + 480 * x4 - 768 * x6 + 2048 * x8) * r
@@ -837,21 +877,103 @@ def poly_scale(params: PolyParams, bloch=(0.0, 0.0)):
     return np.where(zero, 0.0, sc)
 
 
-class PolyEwaldOperator:
-    """Polydisperse spectral-Ewald dipole field (SOLVER_AX or
-    INTERACTION_FIELD), polydisperse_ewald_electric_field.cu: scalar grid,
-    spread :443-562, scale :640-651, contract :653-693, real space
-    :695-826, stage order and INTERACTION sign :2553-2730."""
+def poly_point_weights(params: PolyParams, pos):
+    """Point-Gaussian weights of the quadrupole grid, (2 xi^2/pi)^1.5 h^3
+    exp(-2 xi^2 |g|^2) on the same stencil and voxel indices as
+    :func:`poly_weights` (spread_precalcs_kernel_point, :828-874, and
+    contract_precalcs_kernel_point, :876-922; the constant from :2145 and
+    :2227).  Returns (idx (n,P^3), w (n,P^3))."""
+    pos = np.asarray(pos, dtype=np.float64)
+    h, xi, N = params.h, params.xi, params.num_grid
+    g = c_round(pos / h)
+    d0 = g * h - pos
+    o = params.offsets
+    ox, oy, oz = np.meshgrid(o, o, o, indexing="ij")
+    off = np.stack([ox.ravel(), oy.ravel(), oz.ravel()], axis=1)
+    gd = d0[:, None, :] + off[None, :, :] * h[None, None, :]
+    const = (2.0 * xi * xi / PI) ** 1.5 * float(np.prod(h))
+    w = const * np.exp(-2.0 * xi * xi * np.sum(gd * gd, axis=-1))
+    gi = np.mod(g[:, None, :] + off[None, :, :], N[None, None, :])
+    idx = (gi[..., 0] * N[1] + gi[..., 1]) * N[2] + gi[..., 2]
+    return idx, w
 
-    def __init__(self, box, errortol, xi, radii, solver_ax=True):
+
+def poly_quad_scale(params: PolyParams, bloch=(0.0, 0.0)):
+    """k-space factors of the quadrupole coupling on the scalar grid
+    (compute_scale_coefficients_polydisperse_kernel, :565-638): with
+    e = exp(-(1-eta) k^2 / 4 xi^2) / V, sQ = -e/2, sGP = e, sGQ = -e k^2 / 2,
+    the traceless projector qf and its dot form qd, all 0 at k=0."""
+    Nx, Ny, Nz = params.num_grid
+    L = params.box
+    kx = (_freqs(Nx) * 2 * PI / L[0] - bloch[0])[:, None, None]
+    ky = (_freqs(Ny) * 2 * PI / L[1] - bloch[1])[None, :, None]
+    kz = (_freqs(Nz) * 2 * PI / L[2])[None, None, :]
+    kx, ky, kz = np.broadcast_arrays(kx, ky, kz)
+    ksq = kx * kx + ky * ky + kz * kz
+    zero = ksq < 1e-12
+    ks = np.where(zero, 1.0, ksq)
+    e = np.exp(-(1.0 - params.eta) * ks / (4.0 * params.xi * params.xi)) / float(Nx * Ny * Nz)
+    km = np.sqrt(ks)
+    k0, k1, k2 = kx / km, ky / km, kz / km
+    qf = np.stack([k0 * k0 - 1.0 / 3.0, k0 * k1, k0 * k2, k1 * k1 - 1.0 / 3.0, k1 * k2])
+    qd = np.stack([k0 * k0 - k2 * k2, 2 * k0 * k1, 2 * k0 * k2, k1 * k1 - k2 * k2, 2 * k1 * k2])
+    out = {"sQ": -0.5 * e, "sGP": e, "sGQ": -0.5 * e * ks, "qf": qf, "qd": qd}
+    for a in out.values():
+        a[..., zero] = 0.0
+    return out
+
+
+def poly_self_grad(a, xi):
+    """Quadrupole self value of radius ``a`` (computeRealSpaceTables,
+    :1690-1706): the radius-1 gradient self value at xi*a, over a^5."""
+    xa = xi * a
+    x2, x4, x5 = xa * xa, xa ** 4, xa ** 5
+    v = 0.5 / PI * (3.0 * (3.0 - 10.0 * x2 + 20.0 * x4) / (8.0 * math.sqrt(PI) * x5)
+                    - 3.0 * (3.0 + 2.0 * x2 + 4.0 * x4) * math.exp(-4.0 * x2) / (8.0 * math.sqrt(PI) * x5)
+                    + 3.0 * math.erfc(2.0 * xa))
+    return v / a ** 5
+
+
+class PolyEwaldOperator:
+    """Polydisperse spectral-Ewald field (SOLVER_AX or INTERACTION_FIELD),
+    polydisperse_ewald_electric_field.cu: scalar grid, spread :443-562, scale
+    :640-651, contract :653-693, real space :695-826, stage order and
+    INTERACTION sign :2553-2730.
+
+    With ``quad_idxs`` the quadrupoles ride along as the reference has them:
+    five point-Gaussian component grids (:964-1087), the joint k-space scale
+    coupling them with the dipole grid (:925-962), a G contraction at every
+    field point copied out at the quadrupole particles (:1090-1146), and the
+    joint self and pair terms (:1148-1428) with radius-1 quadrupole tables.
+    Quadrupole q is spread on the stencil of particle q (the spread kernel
+    indexes the particle stencils by q, :994-1005), which is particle
+    quad_idxs[q] only when every particle carries a quadrupole."""
+
+    def __init__(self, box, errortol, xi, radii, solver_ax=True, quad_idxs=None):
         self.p = PolyParams(box, errortol, xi, radii)
         self.radii = np.asarray(radii, dtype=np.float64)
         self.solver_ax = solver_ax
         self.scale = poly_scale(self.p)
         u = self.p.unique
         self.self_perp = np.array([poly_pair_functions(np.array([1.0]), a, a, xi)[2] for a in u])
+        self.quad_idxs = None if quad_idxs is None else np.asarray(quad_idxs, dtype=np.int64)
+        if self.quad_idxs is not None:
+            N = len(self.radii)
+            self.quad_map = -np.ones(N, dtype=np.int64)
+            for q, i in enumerate(self.quad_idxs):
+                if 0 <= i < N:
+                    self.quad_map[i] = q
+            self.qsc = poly_quad_scale(self.p)
+            _, tabs, _, sg = mono_real_tables(xi, self.p.r_table[1:], variant="poly")
+            self.qtables = tabs
+            self.self_G2 = np.array([poly_self_grad(a, xi) for a in u])
 
     def set_positions(self, pos, field_points=None):
+        if self.quad_idxs is not None and field_points is not None:
+            # the joint pair kernel writes quadrupole rows at an offset of
+            # 3 x (particle count) into a field laid out by the field-point
+            # count (:1265); only targets that are the particles are restated
+            raise NotImplementedError("polydisperse quadrupoles are restated for targets at the particles only")
         self.pos = np.asarray(pos, dtype=np.float64)
         self.fp = self.pos if field_points is None else np.asarray(field_points, dtype=np.float64)
         N = len(self.pos)
@@ -859,6 +981,9 @@ class PolyEwaldOperator:
         # field points beyond the particles use the first particle's radius (:297)
         frad = np.array([self.radii[j] if j < N else self.radii[0] for j in range(len(self.fp))])
         self.ct = self.sp if field_points is None else poly_weights(self.p, self.fp, frad)
+        if self.quad_idxs is not None:
+            self.sq = poly_point_weights(self.p, self.pos)
+            self.cq = self.sq if field_points is None else poly_point_weights(self.p, self.fp)
         i, j, r = neighbor_pairs(self.pos, self.fp, self.p.box, self.p.rc, self.solver_ax)
         d = np.sqrt(np.sum(r * r, axis=1))
         keep = d < self.p.rc
@@ -877,43 +1002,122 @@ class PolyEwaldOperator:
                 m = (lo == a_) & (hi == b_)
                 pp, pa = poly_table_lookup(deff[m], u[a_], u[b_], self.p.xi, self.p.r_table)
                 self.perp[m], self.para[m] = pp, pa
+        if self.quad_idxs is not None:
+            self.qpair = {k: interp_table(deff, self.p.r_table, v) for k, v in self.qtables.items()
+                          if k in ("fq1", "fq2", "fq3", "gq1", "gq2", "gq3", "gq4")}
 
-    def reciprocal(self, p):
+    def reciprocal(self, p, Q=None):
+        """(E at the field points, G at the quadrupoles or None)."""
         Nx, Ny, Nz = self.p.num_grid
+        V = Nx * Ny * Nz
         idx, w = self.sp
         vals = np.einsum("noc,nc->no", w, p)
-        grid = np.zeros(Nx * Ny * Nz, dtype=np.complex128)
+        grid = np.zeros(V, dtype=np.complex128)
         np.add.at(grid, idx.ravel(), vals.ravel())
-        F = np.fft.fftn(grid.reshape(Nx, Ny, Nz)) * self.scale
-        Es = (np.fft.ifftn(F) * float(Nx * Ny * Nz)).ravel()
+        F = np.fft.fftn(grid.reshape(Nx, Ny, Nz))
         cidx, cw = self.ct
-        return float(np.prod(self.p.h)) * np.einsum("noc,no->nc", cw, Es[cidx])
+        h3 = float(np.prod(self.p.h))
+        if Q is None:
+            Es = (np.fft.ifftn(F * self.scale) * float(V)).ravel()
+            return h3 * np.einsum("noc,no->nc", cw, Es[cidx]), None
+        Q = np.asarray(Q, dtype=np.complex128)
+        sidx, sw = self.sq
+        gq = np.zeros((5, V), dtype=np.complex128)
+        for c in range(5):
+            # quadrupole q on particle q's stencil (see the class docstring)
+            np.add.at(gq[c], sidx[:len(Q)].ravel(), (sw[:len(Q)] * Q[:, c][:, None]).ravel())
+        FG = np.fft.fftn(gq.reshape(5, Nx, Ny, Nz), axes=(1, 2, 3))
+        k = self.qsc
+        gdot = np.sum(FG * k["qd"], axis=0)
+        Fs = F * self.scale + gdot * k["sQ"]
+        Gd = -(F * k["sGP"]) - gdot * k["sGQ"]
+        Es = (np.fft.ifftn(Fs) * float(V)).ravel()
+        Gs = (np.fft.ifftn(Gd[None] * k["qf"], axes=(1, 2, 3)) * float(V)).reshape(5, V)
+        E = h3 * np.einsum("noc,no->nc", cw, Es[cidx])
+        qidx, qw = self.cq
+        Gp = np.stack([np.sum(qw * Gs[c][qidx], axis=1) for c in range(5)], axis=1)
+        G = np.zeros((len(self.quad_idxs), 5), dtype=np.complex128)
+        ok = (self.quad_idxs >= 0) & (self.quad_idxs < len(self.fp))
+        G[ok] = Gp[self.quad_idxs[ok]]
+        return E, G
 
-    def real_space(self, p, self_coef=None):
-        """Pair sum (sign +1) plus, in SOLVER_AX, the self term."""
+    def real_space(self, p, Q=None, self_coef=None):
+        """Pair sum (sign +1) plus, in SOLVER_AX, the self terms; returns
+        (E, G or None)."""
         M = len(self.fp)
         E = np.zeros((M, 3), dtype=np.complex128)
+        G = None if Q is None else np.zeros((len(self.quad_idxs), 5), dtype=np.complex128)
         if self.solver_ax and self_coef is not None:
-            sp = self.self_perp[self.p.ridx]
-            E += (np.asarray(self_coef) + sp)[:, None] * p
-        if len(self.pi_):
-            dl = self.pr / self.deff[:, None]
-            P = p[self.pi_]
-            rP = np.sum(P * dl, axis=1)
-            Ed = (P - rP[:, None] * dl) * self.perp[:, None] + (rP[:, None] * dl) * self.para[:, None]
-            np.add.at(E, self.pj, Ed)
-        return E
+            sc = np.asarray(self_coef)
+            E += (sc + self.self_perp[self.p.ridx])[:, None] * p
+            if Q is not None:
+                for q, i in enumerate(self.quad_idxs):
+                    a = self.radii[i]
+                    f = 2.5 * sc[i] / (a * a) + 0.5 * self.self_G2[self.p.ridx[i]]
+                    G[q] += f * Q[q]
+        if len(self.pi_) == 0:
+            return E, G
+        dl = self.pr / self.deff[:, None]
+        P = p[self.pi_]
+        rP = np.sum(P * dl, axis=1)
+        Ed = (P - rP[:, None] * dl) * self.perp[:, None] + (rP[:, None] * dl) * self.para[:, None]
+        if Q is not None:
+            t = self.qpair
+            qs = self.quad_map[self.pi_]
+            has = qs >= 0
+            Qs = np.zeros((len(self.pi_), 5), dtype=np.complex128)
+            Qs[has] = Q[qs[has]]
+            dx, dy, dz = dl[:, 0], dl[:, 1], dl[:, 2]
+            q0, q1, q2, q3, q4 = (Qs[:, c] for c in range(5))
+            Qr = np.stack([q0 * dx + q1 * dy + q2 * dz,
+                           q1 * dx + q3 * dy + q4 * dz,
+                           q2 * dx + q4 * dy - (q0 + q3) * dz], axis=1)
+            rr_ = np.stack([dx * dx - dz * dz, 2 * dx * dy, 2 * dx * dz, dy * dy - dz * dz, 2 * dy * dz], axis=1)
+            Qrr = np.sum(Qs * rr_, axis=1)
+            Eq = 0.5 * (Qrr[:, None] * (t["fq1"][:, None] * dl) + Qr * (2.0 * t["fq2"][:, None]))
+            Eq[~has] = 0.0
+            Ed = Ed - Eq
+            N = len(self.pos)
+            tq = np.where(self.pj < N, self.quad_map[np.minimum(self.pj, N - 1)], -1)
+            tgt = tq >= 0
+            if np.any(tgt):
+                rs = np.stack([dx * dx, dx * dy, dx * dz, dy * dy, dy * dz], axis=1)
+                I5 = np.array([1.0, 0.0, 0.0, 1.0, 0.0])
+                px, py, pz = P[:, 0], P[:, 1], P[:, 2]
+                Pr = np.stack([2 * px * dx, px * dy + py * dx, px * dz + pz * dx, 2 * py * dy,
+                               py * dz + pz * dy], axis=1)
+                Gd = (rP[:, None] * (t["fq1"][:, None] * rs + (t["fq2"] + t["fq3"])[:, None] * I5[None, :])
+                      + Pr * t["fq2"][:, None])
+                Qrr2 = np.sum(Qr * dl, axis=1)
+                QrrQ = np.stack([Qr[:, 0] * 2 * dx, Qr[:, 0] * dy + Qr[:, 1] * dx, Qr[:, 0] * dz + Qr[:, 2] * dx,
+                                 Qr[:, 1] * 2 * dy, Qr[:, 1] * dz + Qr[:, 2] * dy], axis=1)
+                Gq = 0.5 * (Qrr2[:, None] * ((t["gq1"] + t["gq3"])[:, None] * I5[None, :] + t["gq4"][:, None] * rs)
+                            + Qs * t["gq2"][:, None] + QrrQ * (2.0 * t["gq3"][:, None]))
+                Gq[~has] = 0.0
+                np.add.at(G, tq[tgt], (Gd + Gq)[tgt])
+        np.add.at(E, self.pj, Ed)
+        return E, G
 
     def apply(self, moments, self_coef=None, split=False):
+        """Full field for flat moments ``[N*3 (+ Nq*5)]``; returns flat E
+        (then G when quadrupoles are on)."""
         N = len(self.pos)
-        p = np.asarray(moments, dtype=np.complex128)[:3 * N].reshape(N, 3)
-        Er = self.reciprocal(p)
-        Es = self.real_space(p, self_coef)
+        moments = np.asarray(moments, dtype=np.complex128)
+        p = moments[:3 * N].reshape(N, 3)
+        Q = None
+        if self.quad_idxs is not None:
+            Q = moments[3 * N:3 * N + 5 * len(self.quad_idxs)].reshape(len(self.quad_idxs), 5)
+        Er, Gr = self.reciprocal(p, Q)
+        Es, Gs = self.real_space(p, Q, self_coef)
         # INTERACTION_FIELD: reciprocal part negated, pairs added with sign -1
         E = Er + Es if self.solver_ax else -(Er + Es)
+        G = None
+        if Q is not None:
+            G = Gr + Gs if self.solver_ax else -(Gr + Gs)
+        out = E.ravel() if G is None else np.concatenate([E.ravel(), G.ravel()])
         if split:
-            return E.ravel(), (Er, Es)
-        return E.ravel()
+            return out, ((Er, Es) if G is None else (Er, Es, Gr, Gs))
+        return out
 
 
 # ---------------------------------------------------------------------------
@@ -1228,9 +1432,7 @@ class DipoleSolverOracle:
             return DirectOperator(self.radius, True, qi)
         mono = all(r == self.radius[0] for r in self.radius)
         if self.field_type == "polydisperse" or (self.field_type == "auto" and not mono):
-            if self.solve_quadrupoles:
-                raise NotImplementedError("polydisperse quadrupoles are not restated")
-            return PolyEwaldOperator(self.box, self.tol, self.xi, self.radius, True)
+            return PolyEwaldOperator(self.box, self.tol, self.xi, self.radius, True, qi)
         return MonoEwaldOperator(self.box, self.tol, self.xi, True, qi)
 
     def _mean_field(self, w):
