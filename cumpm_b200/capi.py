@@ -32,6 +32,7 @@ EXPORTS = [
     "mpm_field_create", "mpm_field_destroy", "mpm_field_set_positions", "mpm_field_set_field_points",
     "mpm_field_apply", "mpm_field_apply_part", "mpm_field_info_get", "mpm_batch_solve",
     "mpm_mono_tables", "mpm_ewald_geometry", "mpm_poly_geometry", "mpm_poly_pair_functions",
+    "mpm_poly_quad_tables", "mpm_poly_quad_self",
     "mpm_profile_enable", "mpm_profile_reset", "mpm_profile_read", "mpm_kernel_launches",
     "mpm_field_apply_noalloc", "mpm_noalloc_scratch_bytes", "mpm_field_grad", "mpm_line_fft",
 ]
@@ -80,6 +81,8 @@ def lib():
         L.mpm_poly_geometry.argtypes = [_dp, C.c_double, C.c_double, _dp, C.c_int, _ip, _ip, _dp, _dp, _ip, _ip]
         L.mpm_poly_pair_functions.argtypes = [C.c_double, C.c_double, C.c_double, C.c_double, C.c_int, _dp, C.c_int,
                                               _dp, _dp, _dp]
+        L.mpm_poly_quad_tables.argtypes = [C.c_double, C.c_double, _dp, C.c_size_t, _ip]
+        L.mpm_poly_quad_self.argtypes = [C.c_double, _dp, C.c_int, _dp]
         L.mpm_profile_read.argtypes = [_dp, C.POINTER(C.c_longlong), C.c_int]
         L.mpm_field_apply_noalloc.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_void_p, C.c_int,
                                               C.c_int, C.c_int, C.c_void_p]
@@ -114,6 +117,26 @@ def mono_tables(xi):
     out = out.reshape(10, 9001)
     names = ["fd1", "fd2", "fq1", "fq2", "fq3", "gq1", "gq2", "gq3", "gq4"]
     return out[0], {n: out[i + 1] for i, n in enumerate(names)}, so.value, sg.value
+
+
+def poly_quad_tables(xi, rc):
+    """Radius-1 quadrupole tables of the polydisperse field for cutoff rc:
+    (r, {name: values}) with names fq1, fq2, fq3, gq1, gq2, gq3, gq4."""
+    n = C.c_int()
+    check(lib().mpm_poly_quad_tables(float(xi), float(rc), None, 0, C.byref(n)))
+    out = np.zeros(8 * n.value)
+    check(lib().mpm_poly_quad_tables(float(xi), float(rc), out.ctypes.data_as(_dp), out.size, C.byref(n)))
+    out = out.reshape(8, n.value)
+    names = ["fq1", "fq2", "fq3", "gq1", "gq2", "gq3", "gq4"]
+    return out[0], {k: out[i + 1] for i, k in enumerate(names)}
+
+
+def poly_quad_self(xi, radii):
+    """Quadrupole self value of each radius."""
+    rr, rp = _arr(np.atleast_1d(radii))
+    out = np.zeros(len(rr))
+    check(lib().mpm_poly_quad_self(float(xi), rp, len(rr), out.ctypes.data_as(_dp)))
+    return out
 
 
 def poly_geometry(box, errortol, xi, radii):

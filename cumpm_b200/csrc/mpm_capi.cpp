@@ -4,6 +4,7 @@
 #include "../../include/cumpm_b200.h"
 
 #include <complex>
+#include <cmath>
 #include <cstring>
 #include <string>
 
@@ -348,6 +349,36 @@ int mpm_mono_tables(double xi, double* out, double* selfo, double* self_grad) {
             std::memcpy(out + size_t(f + 1) * mpm::kTableSize, T.f[f].data(), sizeof(double) * mpm::kTableSize);
         if (selfo) *selfo = T.selfo;
         if (self_grad) *self_grad = T.self_grad;
+    });
+}
+
+int mpm_poly_quad_tables(double xi, double rc, double* out, size_t cap, int* n_nodes) {
+    return guard([&] {
+        if (!(xi > 0) || !(rc > 0)) throw std::invalid_argument("xi and rc must be positive");
+        const double rc_val = rc < 1.001 ? 1.001 : rc;
+        const int n = static_cast<int>(std::ceil((rc_val - 1.0) / mpm::kTableDr)) + 1;
+        if (n_nodes) *n_nodes = n;
+        if (!out) return;
+        if (cap < size_t(mpm::PQ_COUNT + 1) * size_t(n))
+            throw std::invalid_argument("out holds fewer than 8 x n_nodes doubles");
+        const auto T = mpm::build_poly_quad_tables(xi, n);
+        std::memcpy(out, T.r.data(), sizeof(double) * n);
+        for (int f = 0; f < mpm::PQ_COUNT; ++f)
+            std::memcpy(out + size_t(f + 1) * n, T.f[f].data(), sizeof(double) * n);
+    });
+}
+
+int mpm_poly_quad_self(double xi, const double* radii, int n, double* out) {
+    return guard([&] {
+        if (!(xi > 0)) throw std::invalid_argument("xi must be positive");
+        if (n < 0) throw std::invalid_argument("n must be non-negative");
+        if (n == 0) return;
+        need(radii, "radii");
+        need(out, "out");
+        for (int i = 0; i < n; ++i) {
+            if (!(radii[i] > 0)) throw std::invalid_argument("radii must be positive");
+            out[i] = mpm::poly_quad_self_value(radii[i], xi);
+        }
     });
 }
 

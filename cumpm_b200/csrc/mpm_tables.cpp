@@ -258,6 +258,51 @@ Terms gq4_terms(double r, const Powers& p) {
     return t;
 }
 
+// polydisperse grad_quad_2 (polydisperse_ewald_electric_field.cu:1890-1924):
+// the polydisperse field's own expression, lower in degree than gq2_terms
+Terms gq2_poly_terms(double r, const Powers& p) {
+    const double sp = std::pow(PI, 1.5);
+    const double r2 = r * r, r3 = r2 * r, r4 = r2 * r2, r5 = r4 * r, r6 = r3 * r3, r7 = r6 * r, r8 = r4 * r4;
+    const double x2 = p.x2, x4 = p.x4, x6 = p.x6, x8 = p.x8;
+    Terms t;
+    const double ce = -15.0 / (16384.0 * sp * p.x7 * r3);
+    const double odd = 24 * x6 * r7 + (148 * x4 - 96 * x6) * r5 + (90 * x2 + 72 * x4 + 256 * x8) * r3 -
+                       (45 + 120 * x2 - 192 * x4 + 512 * x6) * r;
+    const double even = -48 * x6 * r6 - (264 * x4 - 192 * x6) * r4 + (60 * x2 - 144 * x4 + 512 * x8) * r2 -
+                        2 * (45 + 24 * x2 - 64 * x4 + 512 * x6);
+    t.ep = ce * (odd + even);
+    t.em = ce * (odd - even);
+    t.e0 = 75.0 / (8192.0 * sp * p.x7 * r2) *
+           (8 * x6 * r6 + (44 * x4 - 64 * x6) * r4 + (18 * x2 - 48 * x4 + 128 * x6) * r2 - 9 + 40 * x2 - 192 * x4);
+    const double base = 48 * x8 * r8 + (288 * x6 - 384 * x8) * r6 + (216 * x4 - 576 * x6 + 768 * x8) * r4 -
+                        (72 * x2 - 288 * x4 + 768 * x6) * r2 + 45 - 240 * x2 + 960 * x4;
+    const double cf = -15.0 / (32768.0 * PI * x8 * r3);
+    t.fp = cf * (base - 4096 * x8 * r5 - 8192 * x8);
+    t.fm = cf * (base + 4096 * x8 * r5 - 8192 * x8);
+    t.f0 = 15.0 / (16384.0 * PI * x8 * r3) * base;
+    t.reg = -45.0 * r / (32 * PI) * (1.0 - 5.0 * r2 / 12.0 + r4 / 16.0);
+    return t;
+}
+
+// polydisperse grad_quad_3 (:1926-1967): gq3_terms with the r^5 and r^4
+// terms of the exp(-(r+2)^2 xi^2) coefficient taken with the opposite sign
+Terms gq3_poly_terms(double r, const Powers& p) {
+    Terms t = gq3_terms(r, p);
+    const double r2 = r * r, r4 = r2 * r2, r5 = r4 * r;
+    const double ce = -15.0 / (65536.0 * std::pow(PI, 1.5) * p.x9 * r5);
+    t.ep -= 2.0 * ce * ((216 * p.x4 + 144 * p.x6 + 128 * p.x8) * r5 - (480 * p.x6 + 256 * p.x8) * r4);
+    return t;
+}
+
+// r = 0 entry of the gradient tables for the unit sphere
+double gradient_self_value(double xi) {
+    const double x2 = xi * xi, x4 = x2 * x2, x5 = x4 * xi;
+    return 0.5 / PI *
+           (3.0 * (3.0 - 10.0 * x2 + 20.0 * x4) / (8.0 * std::sqrt(PI) * x5) -
+            3.0 * (3.0 + 2.0 * x2 + 4.0 * x4) * std::exp(-4.0 * x2) / (8.0 * std::sqrt(PI) * x5) +
+            3.0 * std::erfc(2.0 * xi));
+}
+
 }  // namespace
 
 MonoTables build_mono_tables(double xi) {
@@ -273,19 +318,40 @@ MonoTables build_mono_tables(double xi) {
         T.r[k + 1] = r;
         for (int f = 0; f < T_COUNT; ++f) T.f[f][k + 1] = combine(r, xi, fns[f](r, p));
     }
-    const double x2 = p.x2, x4 = p.x4, x5 = p.x5;
+    const double x2 = p.x2;
     T.selfo = (-1.0 + 6.0 * x2 + (1.0 - 2.0 * x2) * std::exp(-4.0 * x2)) / (16.0 * std::pow(PI, 1.5) * x2 * xi) +
               std::erfc(2.0 * xi) / (4.0 * PI);
-    T.self_grad = 0.5 / PI *
-                  (3.0 * (3.0 - 10.0 * x2 + 20.0 * x4) / (8.0 * std::sqrt(PI) * x5) -
-                   3.0 * (3.0 + 2.0 * x2 + 4.0 * x4) * std::exp(-4.0 * x2) / (8.0 * std::sqrt(PI) * x5) +
-                   3.0 * std::erfc(2.0 * xi));
+    T.self_grad = gradient_self_value(xi);
     T.r[0] = 0.0;
     T.f[T_FD1][0] = T.selfo;
     T.f[T_FD2][0] = T.selfo;
     T.f[T_FQ1][0] = T.f[T_FQ2][0] = T.f[T_FQ3][0] = 0.0;
     for (int f = T_GQ1; f <= T_GQ4; ++f) T.f[f][0] = T.self_grad;
     return T;
+}
+
+PolyQuadTables build_poly_quad_tables(double xi, int n_nodes) {
+    if (n_nodes < 2) n_nodes = 2;
+    PolyQuadTables T;
+    const Powers p(xi);
+    T.r.resize(n_nodes);
+    for (auto& v : T.f) v.resize(n_nodes);
+    using Fn = Terms (*)(double, const Powers&);
+    const Fn fns[PQ_COUNT] = {fq1_terms, fq2_terms, fq3_terms, gq1_terms, gq2_poly_terms, gq3_poly_terms, gq4_terms};
+    for (int k = 0; k + 1 < n_nodes; ++k) {
+        const double r = 1.0 + k * kTableDr;
+        T.r[k + 1] = r;
+        for (int f = 0; f < PQ_COUNT; ++f) T.f[f][k + 1] = combine(r, xi, fns[f](r, p));
+    }
+    T.self_grad = gradient_self_value(xi);
+    T.r[0] = 0.0;
+    T.f[PQ_FQ1][0] = T.f[PQ_FQ2][0] = T.f[PQ_FQ3][0] = 0.0;
+    for (int f = PQ_GQ1; f <= PQ_GQ4; ++f) T.f[f][0] = T.self_grad;
+    return T;
+}
+
+double poly_quad_self_value(double a, double xi) {
+    return gradient_self_value(xi * a) / (a * a * a * a * a);
 }
 
 double table_lookup(double r, const double* rt, const double* y, int n) {

@@ -229,6 +229,14 @@ MPM_API int mpm_poly_geometry(const double box[3], double errortol, double xi, c
  * (:170-187, table nodes 0, 1, 1.001, ... for cutoff rc). */
 MPM_API int mpm_poly_pair_functions(double a, double b, double xi, double rc, int lookup, const double* r, int n,
                                     double* fd1, double* fd2, double* self_value);
+/* Radius-1 quadrupole tables of the polydisperse field for cutoff rc
+ * (computeRealSpaceTables, polydisperse_ewald_electric_field.cu:1690-2035):
+ * n_nodes = ceil((max(rc, 1.001) - 1) / 0.001) + 1 nodes (0, 1, 1.001, ...);
+ * out (cap doubles, at least 8 x n_nodes) gets r, fq1, fq2, fq3, gq1, gq2,
+ * gq3, gq4, one row of n_nodes each.  out may be NULL to query n_nodes. */
+MPM_API int mpm_poly_quad_tables(double xi, double rc, double* out, size_t cap, int* n_nodes);
+/* Quadrupole self value of each of the n radii (:1690-1706). */
+MPM_API int mpm_poly_quad_self(double xi, const double* radii, int n, double* out);
 
 #ifdef __cplusplus
 }

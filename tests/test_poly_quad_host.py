@@ -153,3 +153,39 @@ def test_reference_check_mixed_radii_large_box_matches_direct():
     b.compute(pos)
     for f in ("get_eff_polarizability", "get_dipoles", "get_quadrupoles"):
         np.testing.assert_allclose(getattr(a, f)(), getattr(b, f)(), rtol=1e-3, atol=1e-3)
+
+
+@pytest.mark.parametrize("xi,rc", [(0.4, 9.3), (0.5, 7.43), (0.3, 12.4), (0.8, 1.0005)])
+def test_library_tables_match_oracle(xi, rc):
+    """The C++ tables behind the C-ABI (mpm_poly_quad_tables) against the
+    oracle on the same nodes."""
+    from cumpm_b200 import capi
+
+    r, T = capi.poly_quad_tables(xi, rc)
+    n = int(np.ceil((max(rc, 1.001) - 1.0) / 0.001)) + 1
+    assert len(r) == n and r[0] == 0.0
+    np.testing.assert_allclose(r[1:], 1.0 + np.arange(n - 1) * 0.001, rtol=0, atol=1e-12)
+    _, W, _, sg = O.mono_real_tables(xi, r[1:], variant="poly")
+    # the closed forms cancel terms of size xi^-10; the C++ groups them by
+    # parity, the oracle term by term, so the two agree to that rounding
+    for k in ("fq1", "fq2", "fq3", "gq1", "gq2", "gq3", "gq4"):
+        np.testing.assert_allclose(T[k], W[k], rtol=1e-10, atol=1e-11 * np.abs(W[k]).max(), err_msg=k)
+    assert T["gq1"][0] == T["gq4"][0] and abs(T["gq2"][0] - sg) <= 1e-15 * abs(sg)
+
+
+def test_library_self_values_match_oracle():
+    from cumpm_b200 import capi
+
+    radii = np.array([0.8, 1.0, 1.2, 2.5, 4.0])
+    for xi in (0.3, 0.5):
+        np.testing.assert_allclose(capi.poly_quad_self(xi, radii), [O.poly_self_grad(a, xi) for a in radii],
+                                   rtol=1e-14)
+
+
+def test_library_table_arguments_are_checked():
+    from cumpm_b200 import capi
+
+    with pytest.raises(ValueError):
+        capi.poly_quad_tables(-0.5, 7.0)
+    with pytest.raises(ValueError):
+        capi.poly_quad_self(0.5, [1.0, -1.0])
