@@ -869,6 +869,11 @@ struct RealArgs {
     double selfo, self_grad;
     int solver_ax, jacobi, add_recip, quads;
     int pairs_plus;   // pairs enter with +1 in INTERACTION_FIELD too (polydisperse, :780-826)
+    // polydisperse quadrupole self term 2.5 s / a^2 + 0.5 g(a) per target
+    // (real_space_self_kernel_polydisperse_joint, :1148-1195); null: a = 1,
+    // g = self_grad (monodisperse)
+    const double* qa2;
+    const double* qg2;
 };
 
 template <typename R>
@@ -976,7 +981,9 @@ __global__ void __launch_bounds__(128) k_real(const double2* __restrict__ X, dou
                 }
                 if (a.solver_ax) {
                     const double2 qv = X[size_t(3 * a.N + 5 * qt + c) * M + m];
-                    v += make_double2(2.5 * s.x + 0.5 * a.self_grad, 2.5 * s.y) * qv;
+                    const double qa2 = a.qa2 ? a.qa2[j] : 1.0;
+                    const double qg2 = a.qg2 ? a.qg2[j] : a.self_grad;
+                    v += make_double2(2.5 * s.x / qa2 + 0.5 * qg2, 2.5 * s.y / qa2) * qv;
                 }
                 if (a.jacobi) v = v * inv;
                 Y[o] = v;
@@ -1537,7 +1544,7 @@ void Field::recip(const double2* X, double2* Y, int M, cudaStream_t s) {
 }
 
 size_t Field::grid_bytes(int M, bool fp64) const {
-    const int C = spec_.kind == FIELD_POLY ? 1 : (Nq_ ? 8 : 3);
+    const int C = spec_.kind == FIELD_POLY ? (Nq_ ? 6 : 1) : (Nq_ ? 8 : 3);
     return (fp64 ? sizeof(double2) : sizeof(float2)) * size_t(gv_.Nx) * gv_.Ny * gv_.Zs * size_t(C) * M;
 }
 
@@ -1648,6 +1655,8 @@ void Field::real_part(const double2* X, double2* Y, int M, const double2* sc, bo
     a.add_recip = add_recip ? 1 : 0;
     a.quads = Nq_ > 0 ? 1 : 0;
     a.pairs_plus = spec_.kind == FIELD_POLY ? 1 : 0;
+    a.qa2 = (spec_.kind == FIELD_POLY && Nq_) ? pqa2_.as<double>() : nullptr;
+    a.qg2 = (spec_.kind == FIELD_POLY && Nq_) ? pqg2_.as<double>() : nullptr;
     const double* selfv = spec_.kind == FIELD_POLY ? pself_.as<double>() : nullptr;
     const int warps = a.Nt;
     const int thr = 128;

@@ -179,6 +179,10 @@ private:
     std::vector<double> host_z_;    // source z coordinates (layout choice)
 
     DevBuf quad_idx_, quad_map_, radius_;
+    // polydisperse quadrupoles: point weights of the sources, radius-1
+    // quadrupole tables (r then 7 rows of table_n), per particle a^2 and
+    // quadrupole self value
+    DevBuf pqw64_, pqw32_, pqtab_, pqa2_, pqg2_;
     DevBuf tab_r_, tab_f_;          // double[kTableSize], double[T_COUNT][kTableSize]
     // CSR pairs by target
     DevBuf pair_off_, pair_cnt_, pair_src_, pair_T64_, pair_T32_, pair_Q_, cell_key_, cell_idx_, cell_key_s_,

@@ -432,12 +432,191 @@ __global__ void k_poly_pair_coefs(const double* __restrict__ pgeo, const int* __
     }
 }
 
+// Reference table lookup with n nodes 0, 1, 1.001, ...
+// (interpolate_table_gpu_polydisperse, :161-187).
+__device__ double poly_table_at(double r, const double* __restrict__ rt, const double* __restrict__ y, int n) {
+    if (r <= 0.0) return y[0];
+    if (r >= rt[n - 1]) return y[n - 1];
+    if (r < 1.0) return y[0] * (1.0 - r) + y[1] * r;
+    const size_t k = 1 + static_cast<size_t>((r - 1.0) / kTableDr);
+    if (k >= size_t(n - 1)) return y[n - 1];
+    const double t = (r - rt[k]) / (rt[k + 1] - rt[k]);
+    return y[k] * (1.0 - t) + y[k + 1] * t;
+}
+
+// Quadrupole pair coefficients: the seven radius-1 quadrupole tables at
+// max(d, 1e-6) (real_space_precalcs_kernel_polydisperse, :421-429).  Same
+// per-pair layout as the monodisperse Q[8] = {Q1,Q2,Q3,G1,G2,G3,G4,0}.
+__global__ void k_poly_pair_quad(const double* __restrict__ pgeo, long long np, const double* __restrict__ qtab,
+                                 int qn, double* __restrict__ Q) {
+    const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= np) return;
+    const double d = pgeo[4 * p + 3];
+    const double de = d < 1e-6 ? 1e-6 : d;
+    double* qq = Q + 8 * p;
+    for (int k = 0; k < 7; ++k) qq[k] = poly_table_at(de, qtab, qtab + size_t(k + 1) * qn, qn);
+    qq[7] = 0.0;
+}
+
+// Point-Gaussian weight of the quadrupole grids per (point, support node):
+// c exp(-2 xi^2 |g|^2) with c = (2 xi^2/pi)^1.5 h^3
+// (spread_precalcs_kernel_point / contract_precalcs_kernel_point, :828-922;
+// the constant from :2145).  Node order as k_poly_weights.
+__global__ void k_poly_point_weights(const double* __restrict__ xyz, int n, PolyArgs a, double c,
+                                     double* __restrict__ w64, float* __restrict__ w32) {
+    const int P3 = a.P * a.P * a.P;
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long long)n * P3) return;
+    const int i = int(t / P3), o = int(t - (long long)i * P3);
+    const int oo[3] = {o / (a.P * a.P), (o / a.P) % a.P, o % a.P};
+    double d2 = 0.0;
+    for (int d = 0; d < 3; ++d) {
+        const double p = xyz[size_t(d) * n + i];
+        const int g = static_cast<int>(round(p / a.h[d]));
+        const double gd = (g * a.h[d] - p) + double(a.off_min + oo[d]) * a.h[d];
+        d2 += gd * gd;
+    }
+    const double w = c * exp(-2.0 * a.xi * a.xi * d2);
+    w64[t] = w;
+    w32[t] = static_cast<float>(w);
+}
+
+// Quadrupole grids, five planes gq[c][V][M]: quadrupole q adds Q_qc w_o on
+// the support of particle q (spread_quadrupoles_kernel_polydisperse,
+// :964-1087, indexes the particle stencils by q, which is particle
+// quad_idxs[q] only when every particle carries a quadrupole).  Thread per
+// (quadrupole, node), atomics: the quadrupole grids are zeroed first.
+template <typename R>
+__global__ void k_poly_quad_spread(const double2* __restrict__ X, int M, int N, int Nq,
+                                   const int4* __restrict__ base, const R* __restrict__ w, int P, int Nx, int Ny,
+                                   int Nz, cplx<R>* __restrict__ gq) {
+    const int P3 = P * P * P;
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long long)Nq * P3) return;
+    const int q = int(t / P3), o = int(t - (long long)q * P3);
+    if (q >= N) return;   // more quadrupoles than particle stencils: nothing to spread on
+    const int4 b = base[q];
+    // P < N along every axis, so a coordinate wraps at most once
+    int x = b.x + o / (P * P), y = b.y + (o / P) % P, z = b.z + o % P;
+    if (x >= Nx) x -= Nx;
+    if (y >= Ny) y -= Ny;
+    if (z >= Nz) z -= Nz;
+    const size_t V = size_t(Nx) * Ny * Nz;
+    const size_t v = (size_t(x) * Ny + y) * Nz + z;
+    const R wo = w[size_t(q) * P3 + o];
+    for (int c = 0; c < 5; ++c)
+        for (int m = 0; m < M; ++m) {
+            const cplx<R> qv = to_r<R>(X[size_t(3 * N + 5 * q + c) * M + m]) * wo;
+            R* dst = reinterpret_cast<R*>(gq + (size_t(c) * V + v) * M + m);
+            atomicAdd(dst, qv.x);
+            atomicAdd(dst + 1, qv.y);
+        }
+}
+
+// Joint k-space step of the dipole grid phi and the quadrupole grids G_c
+// (compute_scale_coefficients_polydisperse_kernel, :565-638, and
+// scale_kernel_joint_polydisperse, :925-962).  With e = exp(-(1-eta) k^2 /
+// 4 xi^2) / V and gdot = sum_c qd_c G_c:
+//   phi <- (e/k^2) phi - (e/2) gdot,   G_c <- qf_c (-e phi + (e k^2/2) gdot),
+// all zero at k = 0; the coefficients are rounded to R as stored there.
+template <typename R>
+__global__ void k_poly_quad_scale(cplx<R>* __restrict__ grid, cplx<R>* __restrict__ gq, int M, int Nx, int Ny,
+                                  int Nz, double Lx, double Ly, double Lz, double xi, double eta) {
+    const long long V = (long long)Nx * Ny * Nz;
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= V) return;
+    const int ix = int(t / ((long long)Ny * Nz)), iy = int((t / Nz) % Ny), iz = int(t % Nz);
+    const double fx = ix <= (Nx - 1) / 2 ? ix : ix - Nx;
+    const double fy = iy <= (Ny - 1) / 2 ? iy : iy - Ny;
+    const double fz = iz <= (Nz - 1) / 2 ? iz : iz - Nz;
+    const double kx = fx * 2.0 * kPi / Lx, ky = fy * 2.0 * kPi / Ly, kz = fz * 2.0 * kPi / Lz;
+    const double k2 = kx * kx + ky * ky + kz * kz;
+    double sc = 0.0, sQ = 0.0, sGP = 0.0, sGQ = 0.0;
+    double qf[5] = {0, 0, 0, 0, 0}, qd[5] = {0, 0, 0, 0, 0};
+    if (!(k2 < 1e-12)) {
+        const double e = exp(-(1.0 - eta) * k2 / (4.0 * xi * xi));
+        const double inv = 1.0 / double(V);
+        sc = (e / k2) * inv;
+        sQ = (-0.5 * e) * inv;
+        sGP = e * inv;
+        sGQ = (-0.5 * e * k2) * inv;
+        const double km = sqrt(k2);
+        const double h0 = kx / km, h1 = ky / km, h2 = kz / km;
+        qf[0] = h0 * h0 - 1.0 / 3.0; qf[1] = h0 * h1; qf[2] = h0 * h2; qf[3] = h1 * h1 - 1.0 / 3.0; qf[4] = h1 * h2;
+        qd[0] = h0 * h0 - h2 * h2; qd[1] = 2.0 * h0 * h1; qd[2] = 2.0 * h0 * h2; qd[3] = h1 * h1 - h2 * h2;
+        qd[4] = 2.0 * h1 * h2;
+    }
+    const R rsc = R(sc), rsQ = R(sQ), rsGP = R(sGP), rsGQ = R(sGQ);
+    for (int m = 0; m < M; ++m) {
+        const cplx<R> e = grid[size_t(t) * M + m];
+        cplx<R> gd = mk<R>(0, 0);
+        for (int c = 0; c < 5; ++c) gd += gq[(size_t(c) * V + t) * M + m] * R(qd[c]);
+        grid[size_t(t) * M + m] = e * rsc + gd * rsQ;
+        const cplx<R> G = e * (-rsGP) - gd * rsGQ;
+        for (int c = 0; c < 5; ++c) gq[(size_t(c) * V + t) * M + m] = G * R(qf[c]);
+    }
+}
+
+// G at the quadrupole particles: the sum over the support of particle
+// quad_idxs[q] of w_o G_c (contract_kernel_G_polydisperse and
+// copy_G_to_E_kernel_polydisperse, :1090-1146; no h^3 factor, the point
+// weights carry it).  CTA per quadrupole, threads over the support nodes,
+// fixed-order tree sum per column.  Y rows 3*Nt + 5q + c; rows of a
+// quadrupole whose particle index is out of range are zero.
+template <typename R>
+__global__ void __launch_bounds__(128) k_poly_quad_contract(const cplx<R>* __restrict__ gq, int M,
+                                                            const int4* __restrict__ base, const R* __restrict__ w,
+                                                            int P, int Nx, int Ny, int Nz,
+                                                            const int* __restrict__ qidx, int Nt,
+                                                            double2* __restrict__ Y) {
+    __shared__ double2 red[5][128];
+    const int q = blockIdx.x;
+    const int i = qidx[q];
+    if (i < 0 || i >= Nt) {   // uniform across the CTA
+        for (int k = threadIdx.x; k < 5 * M; k += blockDim.x)
+            Y[size_t(3 * Nt + 5 * q + k / M) * M + (k % M)] = make_double2(0.0, 0.0);
+        return;
+    }
+    const int P3 = P * P * P;
+    const size_t V = size_t(Nx) * Ny * Nz;
+    const int4 b = base[i];
+    for (int m = 0; m < M; ++m) {
+        double2 acc[5];
+        for (int c = 0; c < 5; ++c) acc[c] = make_double2(0.0, 0.0);
+        for (int o = threadIdx.x; o < P3; o += blockDim.x) {
+            int x = b.x + o / (P * P), y = b.y + (o / P) % P, z = b.z + o % P;
+            if (x >= Nx) x -= Nx;
+            if (y >= Ny) y -= Ny;
+            if (z >= Nz) z -= Nz;
+            const size_t v = (size_t(x) * Ny + y) * Nz + z;
+            const R wo = w[size_t(i) * P3 + o];
+            for (int c = 0; c < 5; ++c) acc[c] += to_d(gq[(size_t(c) * V + v) * M + m] * wo);
+        }
+        for (int c = 0; c < 5; ++c) red[c][threadIdx.x] = acc[c];
+        __syncthreads();
+        for (int h = blockDim.x / 2; h > 0; h >>= 1) {
+            if (threadIdx.x < h)
+                for (int c = 0; c < 5; ++c) red[c][threadIdx.x] += red[c][threadIdx.x + h];
+            __syncthreads();
+        }
+        if (threadIdx.x < 5) Y[size_t(3 * Nt + 5 * q + threadIdx.x) * M + m] = red[threadIdx.x][0];
+        __syncthreads();
+    }
+}
+
 }  // namespace
 
 // ------------------------------------------------------------------ host
 
 void Field::poly_init() {
-    if (spec_.quads) throw std::runtime_error("polydisperse quadrupoles are not available in this build");
+    // The quadrupole path below (point-Gaussian grids, joint scale, G
+    // contraction, joint pair and self terms) stays closed until its parity
+    // with the oracle has been checked on a GPU.
+    if (spec_.quads)
+        throw std::runtime_error("polydisperse quadrupoles are not enabled in this build (device path not yet "
+                                 "checked on a GPU)");
+    if (spec_.quads && !spec_.solver_ax)
+        throw std::runtime_error("polydisperse quadrupoles are computed at the particles (SOLVER_AX) only");
     pgeom_ = make_poly_geom(spec_.box, spec_.errortol, spec_.xi, spec_.radius);
     geom_ = EwaldGeom{};
     geom_.rc = pgeom_.rc;
@@ -459,6 +638,25 @@ void Field::poly_init() {
     MPM_CUDA(cudaMemcpy(prad_.p, pgeom_.unique.data(), sizeof(double) * nu, cudaMemcpyHostToDevice));
     MPM_CUDA(cudaMemcpy(pself_.p, selfv.data(), sizeof(double) * n, cudaMemcpyHostToDevice));
     MPM_CUDA(cudaMemcpy(radius_.p, spec_.radius.data(), sizeof(double) * n, cudaMemcpyHostToDevice));
+    if (spec_.quads) {
+        const int qn = pgeom_.table_n;
+        const auto QT = build_poly_quad_tables(spec_.xi, qn);
+        pqtab_.ensure(sizeof(double) * 8 * size_t(qn));
+        MPM_CUDA(cudaMemcpy(pqtab_.p, QT.r.data(), sizeof(double) * qn, cudaMemcpyHostToDevice));
+        for (int f = 0; f < PQ_COUNT; ++f)
+            MPM_CUDA(cudaMemcpy(pqtab_.as<double>() + size_t(f + 1) * qn, QT.f[f].data(), sizeof(double) * qn,
+                                cudaMemcpyHostToDevice));
+        // a from the particle, the self value from its radius class (:1171-1177)
+        std::vector<double> a2(n), g2(n);
+        for (int i = 0; i < n; ++i) {
+            a2[i] = spec_.radius[i] * spec_.radius[i];
+            g2[i] = poly_quad_self_value(pgeom_.unique[pgeom_.cls[i]], spec_.xi);
+        }
+        pqa2_.ensure(sizeof(double) * n);
+        pqg2_.ensure(sizeof(double) * n);
+        MPM_CUDA(cudaMemcpy(pqa2_.p, a2.data(), sizeof(double) * n, cudaMemcpyHostToDevice));
+        MPM_CUDA(cudaMemcpy(pqg2_.p, g2.data(), sizeof(double) * n, cudaMemcpyHostToDevice));
+    }
     gv_.Nx = pgeom_.ng[0];
     gv_.Ny = pgeom_.ng[1];
     gv_.Nz = pgeom_.ng[2];
@@ -580,10 +778,32 @@ void Field::poly_pair_coefs(cudaStream_t s) {
                                                     nt, N_, pcls_.as<int>(), prad_.as<double>(), spec_.xi,
                                                     pgeom_.table_n, pair_T64_.as<double>(), pair_T32_.as<float>());
     MPM_LAUNCH();
+    if (Nq_) {
+        k_poly_pair_quad<<<nblk(num_pairs_, 256), 256, 0, s>>>(pair_geo_.as<double>(), num_pairs_,
+                                                               pqtab_.as<double>(), pgeom_.table_n,
+                                                               pair_Q_.as<double>());
+        MPM_LAUNCH();
+    }
 }
 
 void Field::poly_precalc(cudaStream_t s) {
     poly_weights(sources_, radius_.as<double>(), s, true);
+    if (Nq_) {
+        // point weights of the quadrupole grids (targets are the particles)
+        const int P3 = pgeom_.P * pgeom_.P * pgeom_.P;
+        pqw64_.ensure(sizeof(double) * size_t(N_) * P3);
+        pqw32_.ensure(sizeof(float) * size_t(N_) * P3);
+        PolyArgs a;
+        for (int d = 0; d < 3; ++d) { a.h[d] = pgeom_.h[d]; a.N[d] = pgeom_.ng[d]; }
+        a.P = pgeom_.P;
+        a.off_min = pgeom_.off_min;
+        a.eta = pgeom_.eta;
+        a.xi = spec_.xi;
+        const double c = std::pow(2.0 * spec_.xi * spec_.xi / kPi, 1.5) * pgeom_.h[0] * pgeom_.h[1] * pgeom_.h[2];
+        k_poly_point_weights<<<nblk((long long)N_ * P3, 256), 256, 0, s>>>(sources_.xyz.as<double>(), N_, a, c,
+                                                                           pqw64_.as<double>(), pqw32_.as<float>());
+        MPM_LAUNCH();
+    }
     if (!spec_.solver_ax) {
         // field points past the particles take the first particle's radius (:297)
         const int nt = targets_.n;
@@ -620,7 +840,36 @@ void Field::poly_recip_on(const double2* X, double2* Y, int M, cplx<R>* grid, cu
         MPM_LAUNCH();
     }
     const R* scl = sizeof(R) == 4 ? reinterpret_cast<const R*>(scale32_.p) : reinterpret_cast<const R*>(scale64_.p);
-    if (own_fft_) {
+    const size_t V = size_t(gv_.Nx) * gv_.Ny * gv_.Nz;
+    cplx<R>* gq = grid + V * M;   // quadrupole grids [5][V][M] (grid_bytes holds six grids then)
+    const R* qw = sizeof(R) == 4 ? reinterpret_cast<const R*>(pqw32_.p) : reinterpret_cast<const R*>(pqw64_.p);
+    if (Nq_) {
+        // the quadrupole grids couple with phi in k space, so the forward,
+        // joint scale and inverse run as separate passes over six grids
+        const int P3 = pgeom_.P * pgeom_.P * pgeom_.P;
+        {
+            StageScope sc(ST_SPREAD, s);
+            MPM_CUDA(cudaMemsetAsync(gq, 0, sizeof(cplx<R>) * 5 * V * M, s));
+            k_poly_quad_spread<R><<<nblk((long long)Nq_ * P3, 128), 128, 0, s>>>(
+                X, M, N_, Nq_, ps.base.as<int4>(), qw, pgeom_.P, gv_.Nx, gv_.Ny, gv_.Nz, gq);
+            MPM_LAUNCH();
+        }
+        {
+            StageScope sc(ST_FFT_FWD, s);
+            for (int c = 0; c < 6; ++c) transform<R>(c == 0 ? grid : gq + size_t(c - 1) * V * M, M, false, s);
+        }
+        {
+            StageScope sc(ST_KSPACE, s);
+            k_poly_quad_scale<R><<<nblk((long long)V, 128), 128, 0, s>>>(grid, gq, M, gv_.Nx, gv_.Ny, gv_.Nz,
+                                                                          spec_.box[0], spec_.box[1], spec_.box[2],
+                                                                          spec_.xi, pgeom_.eta);
+            MPM_LAUNCH();
+        }
+        {
+            StageScope sc(ST_FFT_INV, s);
+            for (int c = 0; c < 6; ++c) transform<R>(c == 0 ? grid : gq + size_t(c - 1) * V * M, M, true, s);
+        }
+    } else if (own_fft_) {
         // z and y forward; x forward, scale and x inverse in one pass over
         // the x lines; y and z inverse (the 1-D transforms commute)
         const size_t Bi = size_t(gv_.Nz) * M;
@@ -662,6 +911,11 @@ void Field::poly_recip_on(const double2* X, double2* Y, int M, cplx<R>* grid, cu
     k_poly_contract<R, MC><<<dim3(tg.n, nmb), 256, 0, s>>>(grid, M, tg.base.as<int4>(), tw, pgeom_.P, gv_.Nx, gv_.Ny,
                                                           gv_.Nz, factor, Y);
     MPM_LAUNCH();
+    if (Nq_) {
+        k_poly_quad_contract<R><<<Nq_, 128, 0, s>>>(gq, M, tg.base.as<int4>(), qw, pgeom_.P, gv_.Nx, gv_.Ny, gv_.Nz,
+                                                   quad_idx_.as<int>(), tg.n, Y);
+        MPM_LAUNCH();
+    }
 }
 
 template void Field::poly_recip_on<float>(const double2*, double2*, int, cplx<float>*, cudaStream_t);
