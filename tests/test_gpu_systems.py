@@ -1,0 +1,54 @@
+"""Several independent systems solved through cumpm_b200.systems give, system
+by system, what a dipole_solver of each gives on its own."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _packing(rng, n, box, a):
+    pos = []
+    while len(pos) < n:
+        p = rng.uniform(0, box, 3)
+        if all(np.linalg.norm((p - q) - box * np.round((p - q) / box)) >= 2.2 * a for q in pos):
+            pos.append(p)
+    return np.array(pos)
+
+
+def _hex(rows, cols, d):
+    return np.array([[(i + 0.5 * (j % 2)) * d, j * np.sqrt(3) / 2 * d, 0.0] for j in range(rows) for i in range(cols)])
+
+
+def _systems():
+    from cumpm_b200.systems import System
+
+    rng = np.random.default_rng(41)
+    omega = np.linspace(0.3, 0.9, 3)
+    eps = 4.0 - 1.8 ** 2 / (omega ** 2 + 1j * omega * 0.1)
+    # 10 x 8 monolayer; every box edge above twice the real-space cutoff
+    # (about 8 radii at tol 1e-7)
+    hexa = _hex(10, 8, 12.0)
+    box_h = [8 * 12.0, 10 * np.sqrt(3) / 2 * 12.0, 200.0]
+    out = [
+        System(box=box_h, positions=hexa, eps_p=eps, radius=5.0, eps_m=1.77, tol=1e-7, quadrupoles=True,
+               precision="double"),
+        System(box=[40.0] * 3, positions=_packing(rng, 24, 40.0, 2.0), eps_p=eps, radius=2.0, eps_m=1.77, tol=1e-7,
+               quadrupoles=[0, 5, 7], precision="double"),
+        System(box=[50.0] * 3, positions=_packing(rng, 20, 50.0, 3.0), eps_p=eps,
+               radius=list(rng.uniform(1.0, 3.0, 20)), eps_m=1.77, tol=1e-7, field_type="polydisperse",
+               precision="double"),
+    ]
+    return out
+
+
+def test_systems_match_their_own_solvers():
+    from cumpm_b200 import systems as S
+
+    syst = _systems()
+    res = S.solve_systems(syst)
+    for s, r in zip(syst, res):
+        ref = S.solve_one(s)
+        assert set(r) == set(ref)
+        for k in ref:
+            np.testing.assert_allclose(r[k], ref[k], rtol=1e-12, atol=1e-14 * np.abs(ref[k]).max())
+    assert "quadrupoles" in res[0] and res[1]["quadrupoles"].shape[-1] == 5 and "quadrupoles" not in res[2]
