@@ -189,3 +189,29 @@ def test_library_table_arguments_are_checked():
         capi.poly_quad_tables(-0.5, 7.0)
     with pytest.raises(ValueError):
         capi.poly_quad_self(0.5, [1.0, -1.0])
+
+
+def _line_of_four():
+    """The reference's field-level subset case: four unit spheres in a line
+    10 apart, box 50, xi 0.4, quadrupoles on particles 0 and 2, self
+    coefficient 1.5 + 0.1i, moments from the legacy seed 42."""
+    d = 10.0
+    pos = np.array([[0.0, 0, 0], [d, 0, 0], [2 * d, 0, 0], [3 * d, 0, 0]])
+    rs = np.random.RandomState(42)
+    P = rs.rand(4, 3) + 1j * rs.rand(4, 3)
+    Q = rs.rand(2, 5) + 1j * rs.rand(2, 5)
+    return pos, [5 * d] * 3, [0, 2], np.concatenate([P.ravel(), Q.ravel()]), np.full(4, 1.5 + 0.1j)
+
+
+def test_reference_check_subset_field_matches_monodisperse():
+    """Reference KAT at the field level: the polydisperse field with a
+    quadrupole subset matches the monodisperse one to 1e-3
+    (tests/test_electric_fields.py:158-223)."""
+    pos, box, qi, X, sc = _line_of_four()
+    m = O.MonoEwaldOperator(box, 1e-6, 0.4, True, qi)
+    m.set_positions(pos)
+    p = O.PolyEwaldOperator(box, 1e-6, 0.4, [1.0] * 4, True, qi)
+    p.set_positions(pos)
+    a, b = m.apply(X, sc), p.apply(X, sc)
+    np.testing.assert_allclose(b[:12], a[:12], rtol=1e-3, atol=1e-3)
+    np.testing.assert_allclose(b[12:], a[12:], rtol=1e-3, atol=1e-3)
