@@ -841,7 +841,8 @@ void Field::poly_recip_on(const double2* X, double2* Y, int M, cplx<R>* grid, cu
     }
     const R* scl = sizeof(R) == 4 ? reinterpret_cast<const R*>(scale32_.p) : reinterpret_cast<const R*>(scale64_.p);
     const size_t V = size_t(gv_.Nx) * gv_.Ny * gv_.Nz;
-    cplx<R>* gq = grid + V * M;   // quadrupole grids [5][V][M] (grid_bytes holds six grids then)
+    // quadrupole grids [5][V][M] after phi (grid_bytes holds six grids then)
+    cplx<R>* gq = Nq_ ? grid + V * M : nullptr;
     const R* qw = sizeof(R) == 4 ? reinterpret_cast<const R*>(pqw32_.p) : reinterpret_cast<const R*>(pqw64_.p);
     if (Nq_) {
         // the quadrupole grids couple with phi in k space, so the forward,
