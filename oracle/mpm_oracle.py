@@ -34,6 +34,12 @@ What it restates (reference ``file:line``):
   checks (equal radii against the monodisperse quadrupole solve, mixed radii
   in a large box against the direct sum); not yet against the reference
   build's polydisperse quadrupole field.
+* Bloch wavevector (k_x, k_y) in both Ewald operators: shifted k in the
+  scales (``monodisperse...cu:1329-1330``, ``polydisperse...cu:592-593``)
+  and a phase exp(-i(k_x r_x + k_y r_y)) on every pair term
+  (``monodisperse...cu:1749-1858``, ``polydisperse...cu:799-806,
+  1339-1419``); pinned by the reference's mono/poly Bloch check
+  (``tests/test_electric_fields.py:226-284``)
 * open-boundary direct sum: ``electric_field/direct_electric_field.cu:42-324``
 * Krylov solvers: ``numerical_solver/gmres_solver.cu:56-208``,
   ``numerical_solver/bicgstab_solver.cu:58-192``, Jacobi
@@ -490,6 +496,16 @@ def neighbor_pairs(src, tgt, box, rc, exclude_self):
 # ---------------------------------------------------------------------------
 
 
+def _bloch_phase(bloch, r):
+    """exp(i phase), phase = -(k_x r_x + k_y r_y) per pair (r = source -
+    target, minimum image); None without a Bloch wavevector."""
+    kx, ky = bloch
+    if kx == 0.0 and ky == 0.0:
+        return None
+    ph = -(kx * r[:, 0] + ky * r[:, 1])
+    return np.cos(ph) + 1j * np.sin(ph)
+
+
 class MonoEwaldOperator:
     """Monodisperse spectral-Ewald field (SOLVER_AX or INTERACTION_FIELD).
 
@@ -497,13 +513,17 @@ class MonoEwaldOperator:
     (``base_electric_field.cu:235``).
     """
 
-    def __init__(self, box, errortol, xi, solver_ax=True, quad_idxs=None, fft_workers=None):
+    def __init__(self, box, errortol, xi, solver_ax=True, quad_idxs=None, fft_workers=None, bloch=(0.0, 0.0)):
         self.fft_workers = fft_workers
         self.p = MonoParams(box, errortol, xi)
         self.solver_ax = solver_ax
         self.quad_idxs = None if quad_idxs is None else np.asarray(quad_idxs, dtype=int)
         self.r_table, self.tables, self.selfo, self.self_grad = mono_real_tables(xi)
-        self.sc = mono_scale(self.p, quads=self.quad_idxs is not None)
+        # Bloch wavevector (k_x, k_y): shifted k in the scale, a phase on
+        # every pair term (monodisperse_ewald_electric_field.cu:1329-1330,
+        # 1749-1756, 1778-1785, 1851-1858)
+        self.bloch = (float(bloch[0]), float(bloch[1]))
+        self.sc = mono_scale(self.p, quads=self.quad_idxs is not None, bloch=self.bloch)
 
     def set_positions(self, pos, field_points=None):
         self.pos = np.asarray(pos, dtype=np.float64)
@@ -519,6 +539,7 @@ class MonoEwaldOperator:
         d = np.sqrt(np.sum(r * r, axis=1))
         keep = d < self.p.rc
         self.pi_, self.pj, self.pr, self.pd = i[keep], j[keep], r[keep], d[keep]
+        self.phase = _bloch_phase(self.bloch, self.pr)
 
     # -- stages --------------------------------------------------------------
     def _fftn(self, a):
@@ -605,6 +626,8 @@ class MonoEwaldOperator:
             Eq = 0.5 * (Qrr[:, None] * (Q1[:, None] * dl) + Qr * (2.0 * Q2[:, None]))
             Eq[~has] = 0.0
             Ed = Ed - Eq
+            if self.phase is not None:
+                Ed = Ed * self.phase[:, None]
             # contributions to G of quadrupole targets
             tq = qm[self.pj] if self.pj.max(initial=-1) < len(qm) else -np.ones_like(self.pj)
             tgt = tq >= 0
@@ -626,7 +649,11 @@ class MonoEwaldOperator:
                             + Qs * G2[:, None] + QrrQ * (2.0 * G3[:, None]))
                 Gq[~has] = 0.0
                 Gt = (Gd + Gq) * sign
+                if self.phase is not None:
+                    Gt = Gt * self.phase[:, None]
                 np.add.at(G, tq[tgt], Gt[tgt])
+        elif self.phase is not None:
+            Ed = Ed * self.phase[:, None]
         np.add.at(E, self.pj, Ed * sign)
         return E, G
 
@@ -949,11 +976,14 @@ class PolyEwaldOperator:
     indexes the particle stencils by q, :994-1005), which is particle
     quad_idxs[q] only when every particle carries a quadrupole."""
 
-    def __init__(self, box, errortol, xi, radii, solver_ax=True, quad_idxs=None):
+    def __init__(self, box, errortol, xi, radii, solver_ax=True, quad_idxs=None, bloch=(0.0, 0.0)):
         self.p = PolyParams(box, errortol, xi, radii)
         self.radii = np.asarray(radii, dtype=np.float64)
         self.solver_ax = solver_ax
-        self.scale = poly_scale(self.p)
+        # Bloch wavevector: shifted k in the scales, a phase on every pair
+        # term (:592-593, 799-806, 1339-1346, 1414-1419)
+        self.bloch = (float(bloch[0]), float(bloch[1]))
+        self.scale = poly_scale(self.p, self.bloch)
         u = self.p.unique
         self.self_perp = np.array([poly_pair_functions(np.array([1.0]), a, a, xi)[2] for a in u])
         self.quad_idxs = None if quad_idxs is None else np.asarray(quad_idxs, dtype=np.int64)
@@ -963,7 +993,7 @@ class PolyEwaldOperator:
             for q, i in enumerate(self.quad_idxs):
                 if 0 <= i < N:
                     self.quad_map[i] = q
-            self.qsc = poly_quad_scale(self.p)
+            self.qsc = poly_quad_scale(self.p, self.bloch)
             _, tabs, _, sg = mono_real_tables(xi, self.p.r_table[1:], variant="poly")
             self.qtables = tabs
             self.self_G2 = np.array([poly_self_grad(a, xi) for a in u])
@@ -988,6 +1018,7 @@ class PolyEwaldOperator:
         d = np.sqrt(np.sum(r * r, axis=1))
         keep = d < self.p.rc
         self.pi_, self.pj, self.pr, self.pd = i[keep], j[keep], r[keep], d[keep]
+        self.phase = _bloch_phase(self.bloch, self.pr)
         # per-pair table values (real_space_precalcs_kernel_polydisperse, :352-441)
         u, ridx = self.p.unique, self.p.ridx
         deff = np.maximum(self.pd, 1e-6)
@@ -1094,7 +1125,12 @@ class PolyEwaldOperator:
                 Gq = 0.5 * (Qrr2[:, None] * ((t["gq1"] + t["gq3"])[:, None] * I5[None, :] + t["gq4"][:, None] * rs)
                             + Qs * t["gq2"][:, None] + QrrQ * (2.0 * t["gq3"][:, None]))
                 Gq[~has] = 0.0
-                np.add.at(G, tq[tgt], (Gd + Gq)[tgt])
+                Gt = Gd + Gq
+                if self.phase is not None:
+                    Gt = Gt * self.phase[:, None]
+                np.add.at(G, tq[tgt], Gt[tgt])
+        if self.phase is not None:
+            Ed = Ed * self.phase[:, None]
         np.add.at(E, self.pj, Ed)
         return E, G
 

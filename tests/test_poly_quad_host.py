@@ -215,3 +215,26 @@ def test_reference_check_subset_field_matches_monodisperse():
     a, b = m.apply(X, sc), p.apply(X, sc)
     np.testing.assert_allclose(b[:12], a[:12], rtol=1e-3, atol=1e-3)
     np.testing.assert_allclose(b[12:], a[12:], rtol=1e-3, atol=1e-3)
+
+
+def test_reference_check_bloch_wavevector_matches_monodisperse():
+    """Reference KAT: with the Bloch wavevector (0.15, -0.22) the
+    polydisperse field with quadrupoles on particles 0 and 2 matches the
+    monodisperse one to 1e-3 (tests/test_electric_fields.py:226-284)."""
+    pos = np.array([[0.0, 0, 0], [4.5, 0, 0], [9.0, 0, 0], [13.5, 0, 0]])
+    box, qi, k = [18.0] * 3, [0, 2], (0.15, -0.22)
+    rs = np.random.RandomState(123)
+    P = rs.rand(4, 3) + 1j * rs.rand(4, 3)
+    Q = rs.rand(2, 5) + 1j * rs.rand(2, 5)
+    X, sc = np.concatenate([P.ravel(), Q.ravel()]), np.ones(4, complex)
+    m = O.MonoEwaldOperator(box, 1e-6, 0.5, True, qi, bloch=k)
+    m.set_positions(pos)
+    p = O.PolyEwaldOperator(box, 1e-6, 0.5, [1.0] * 4, True, qi, bloch=k)
+    p.set_positions(pos)
+    a, b = m.apply(X, sc), p.apply(X, sc)
+    np.testing.assert_allclose(b[:12], a[:12], rtol=1e-3, atol=1e-3)
+    np.testing.assert_allclose(b[12:], a[12:], rtol=1e-3, atol=1e-3)
+    # the wavevector is felt: without it the field moves by about 1.7e-3
+    m0 = O.MonoEwaldOperator(box, 1e-6, 0.5, True, qi)
+    m0.set_positions(pos)
+    assert np.abs(m0.apply(X, sc) - a).max() > 5e-4
