@@ -4,8 +4,9 @@ It exists for callers that cannot allocate device memory while they solve
 (their GPU memory belongs to another allocator, or their loop must not call
 into the driver's allocator): its reciprocal-space grid is a static device
 array of the library.  It must give the same fields as mpm_field_apply.
-This file is collected last so that a failure here leaves every other test
-already run; it passes alone in a fresh process and after the other tests.
+This file is collected after the operator and solver tests so that a
+failure here leaves them already run; it passes alone in a fresh process and
+after the other tests.
 """
 import ctypes as C
 
