@@ -11,6 +11,10 @@ the tests need).
   10th entry, at xi = 0.4 and 0.5.
 * refcpu_operator.npz: field E and field gradient G from that CPU operator
   for seeded random dipoles and quadrupoles on a 6-particle periodic box.
+* ref_eels_vs_python_module.npz: the reference's EELS golden vector
+  (tests/data/ref_eels_vs_python_module.npz) with the inputs of the test
+  that reads it (tests/test_eels_solver.py:114-173): loss spectra of two
+  beam positions at five frequencies and the scaled dipoles.
 
 Usage: python tests/golden/make_golden.py [/path/to/reference]
 """
@@ -47,6 +51,14 @@ def main():
              dip_pos=np.array([[0, 0, 0], [10, 0, 0], [0, 10, 0], [0, 0, 10.0]]),
              dipoles=np.array([[0.1 + 0.05j, 0, 0], [-0.1, 0.02j, 0], [0, 0.05, -0.01j], [0.01, 0, 0.1j]]),
              field_points=np.array([[5.0, 0, 0], [0, 5, 0], [2.5, 2.5, 2.5]]))
+    g = np.load(os.path.join(data, "ref_eels_vs_python_module.npz"))
+    d = 25.0 + 2.6
+    omega = np.linspace(2000.0, 9000.0, 5)
+    np.savez(os.path.join(HERE, "ref_eels_vs_python_module.npz"), ref_eels=g["ref_eels"],
+             ref_dips_stacked=g["ref_dips_stacked"], box=np.full(3, 10.0 * d),
+             points=np.array([[-0.5, 0.0, 0.0], [0.5, 0.0, 0.0]]) * d, e_pos=np.array([[0.0, 0.0], [1.0, 0.0]]) * d,
+             radius=0.5 * 25.0, omega_cm=omega, eps_p=drude(omega, 845.0, 11886.0, 2.25), omega_nm=omega / 1e7,
+             v=0.45, eps_m=1.0)
     # --- reference CPU operator
     sys.path.insert(0, os.path.join(REF, "tests"))
     from quadrupole_field import Electric_Field
