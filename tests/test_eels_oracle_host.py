@@ -50,3 +50,20 @@ def test_loss_is_the_reciprocity_sum():
         want = np.sum(np.imag(np.sum(dips[w] * np.conj(Einc), axis=1))) / (2 * np.pi ** 2)
         assert eels[w] == pytest.approx(want, rel=1e-12)
         assert eels[w] > 0.0   # a lossy particle absorbs
+
+
+def test_zone_sum_in_a_large_box_is_the_isolated_pair():
+    """The Brillouin-zone sum (beam images with Bloch phases on the Ewald
+    operator with the Bloch wavevector, eels_solver.cu:491-509, 847-859) of
+    a pair in a box much larger than the beam's decay length gives the loss
+    of the isolated pair under one beam (direct field), closer with more
+    zone points."""
+    box, pts = np.full(3, 60.0), np.array([[0.0, 0, 0], [9.0, 0, 0]])
+    kw = dict(radius=3.0, xi=0.5, tol=1e-6)
+    iso, _ = E.EELSOracle(box, [4.0 + 0.3j], [0.05], 0.4, field_type="direct", **kw).compute([5.0, 3.0], pts)
+    errs = []
+    for n in (1, 2):
+        z, _ = E.EELSOracle(box, [4.0 + 0.3j], [0.05], 0.4, field_type="monodisperse", asm=True, asm_n=(n, n),
+                            **kw).compute([5.0, 3.0], pts)
+        errs.append(abs(z[0] - iso[0]) / iso[0])
+    assert errs[0] < 2e-3 and errs[1] < errs[0]
