@@ -1,0 +1,211 @@
+"""Electron energy loss (EELS) of a particle assembly under a moving
+electron beam, on the device batched solve.
+
+Drop-in for the reference's ``cuMPM.EELS`` (``src/cuMPM/eels.py``,
+``src/cpp/eels_solver.cu``) for dipoles.  Per beam position, every
+frequency is one right-hand side of one batched Krylov solve on the GPU:
+
+* host: non-dimensionalisation by the smallest radius and by eps_m
+  (eels_solver.cu:241-263), the beam field at each particle (:519-578):
+  soft-core distance sqrt(r_perp^2 + sigma^2) with sigma = 0.5 nm, K1 across
+  and K0 along the beam, phase exp(2 pi i omega z / v), Lorentz factor
+  1/sqrt(1 - v^2) (taken after eps_m is scaled to 1, :482); self
+  coefficients -3 / (4 pi (1 - eps)) without the radius factor (:638-642);
+* device: ``capi.Field.batch_solve`` of A(omega_w) p_w = E_inc(omega_w)
+  for all w at once (the field and its precalcs built once per frame);
+* host: the loss by reciprocity, sum_p Im(p . conj(E_inc)) / (2 pi^2)
+  (:796-838).
+
+Not available yet (they raise ``RuntimeError`` naming the gap): the
+Brillouin-zone sum (``asm_flag``, it needs the Bloch wavevector in the
+device operator), particle splitting near the beam (``split_dist`` with
+``N_split``) and quadrupoles.
+"""
+import math
+
+import numpy as np
+
+from . import capi
+
+_PI = math.pi
+
+
+def _bessel_k(n, z):
+    """K_n(z), n in {0, 1}, by the reference's rules (eels_solver.cu:56-93):
+    the real-argument function unless z lies on the imaginary axis, where
+    the Hankel form applies."""
+    from scipy import special
+
+    z = np.asarray(z, dtype=np.complex128)
+    out = special.kv(n, z.real).astype(np.complex128)
+    axis = (np.abs(z.imag) >= 1e-12) & (np.abs(z.real) < 1e-12)
+    if np.any(axis):
+        y = np.abs(z.imag[axis])
+        j, yn = special.jv(n, y), special.yv(n, y)
+        v = (-_PI / 2 * yn - 1j * _PI / 2 * j) if n == 0 else (-_PI / 2 * j + 1j * _PI / 2 * yn)
+        out[axis] = np.where(z.imag[axis] < 0.0, np.conj(v), v)
+    return out
+
+
+def beam_field(pos, epos, omega, v, gamma, length_scale):
+    """Beam field (N, 3) at scaled positions, for one scaled frequency."""
+    pos = np.asarray(pos, dtype=np.float64)
+    dx = pos[:, 0] - epos[0]
+    dy = pos[:, 1] - epos[1]
+    sigma = 0.5 / length_scale
+    r = np.sqrt(dx * dx + dy * dy + sigma * sigma)
+    x = (2.0 * _PI * omega * r) / (v * gamma)
+    pref = omega / (v * v * gamma) * np.exp(1j * 2.0 * _PI * omega * pos[:, 2] / v)
+    k0, k1 = _bessel_k(0, x), _bessel_k(1, x)
+    return np.stack([-pref * k1 * dx / r, -pref * k1 * dy / r, pref * 1j / gamma * k0], axis=1)
+
+
+class EELS:
+    """EELS probability spectrum and induced dipoles (see the module
+    docstring); same constructor, ``compute``, ``get_eels``,
+    ``get_dipoles`` and ``get_positions`` as the reference's class."""
+
+    def __init__(self, box, eps_p, omega, v, eps_m=1.0, radius=1.0, xi=0.5, tol=1e-3, quiet=False,
+                 guess_type="derivative", solver_type="gmres", field_type="auto", split_dist=None, N_split=None,
+                 integration_step=0.05, split_method="cubic", solve_quadrupoles=False, quad_idxs=None,
+                 asm_flag=False, asm_Nx=1, asm_Ny=1, precision=None):
+        if split_method not in ("cubic", "fibonacci", "fcc"):
+            raise ValueError("split_method must be 'cubic', 'fibonacci', or 'fcc', got " + repr(split_method))
+        if (split_dist is None) != (N_split is None):
+            raise ValueError("Both split_dist and N_split must be specified, or both left as None.")
+        if field_type not in ("auto", "monodisperse", "polydisperse", "direct"):
+            raise ValueError(f"field_type must be 'auto', 'monodisperse', 'polydisperse', or 'direct', got {field_type}")
+        if len(np.atleast_1d(box)) != 3:
+            raise ValueError("box must have length 3")
+        if solver_type not in ("gmres", "bicgstab"):
+            raise ValueError(f"Unknown solver_type: {solver_type}")
+        if split_dist is not None and float(split_dist) > 0.0 and int(N_split) > 1:
+            raise RuntimeError("EELS particle splitting near the beam is not available in this build")
+        if solve_quadrupoles or (quad_idxs is not None and len(quad_idxs)):
+            raise RuntimeError("EELS quadrupoles are not available in this build")
+        if asm_flag:
+            raise RuntimeError("the EELS Brillouin-zone sum (asm_flag) is not available in this build")
+        from .solver import _parse_precision
+
+        prec = _parse_precision(precision)
+        self._fp64 = str(prec).upper().endswith("DOUBLE")
+        self.box = np.asarray(box, dtype=np.float64)
+        self.omega = np.atleast_1d(np.asarray(omega, dtype=np.float64))
+        self.eps_p = eps_p
+        self.v, self.eps_m, self.radius = float(v), float(eps_m), radius
+        self.xi, self.tol, self.quiet = float(xi), float(tol), bool(quiet)
+        self.solver_type, self.field_type = solver_type, field_type
+        self.use_jacobi_precond = True
+        self._N = 0
+        self._F = None
+        self._eels, self._dips = [], []
+        self.positions = None
+
+    # -- set-up (eels_solver.cu:202-263) -----------------------------------
+    def _eps_matrix(self, N):
+        W = len(self.omega)
+        e = np.asarray(self.eps_p, dtype=np.complex128)
+        if e.ndim == 0 or e.size == 1:
+            return np.full((W, N), complex(e.ravel()[0]))
+        if e.ndim == 1:
+            if e.size != W:
+                raise ValueError("1D eps_p must have length equal to num_wavevectors")
+            return np.repeat(e[:, None], N, axis=1)
+        if e.shape[0] != W:
+            raise ValueError("First dimension of 2D eps_p must be equal to num_wavevectors")
+        if e.shape[1] == 1:
+            return np.repeat(e, N, axis=1)
+        if e.shape[1] != N:
+            raise RuntimeError("The number of particles is inconsistent with eps_p provided.")
+        return e.copy()
+
+    def _setup(self, N):
+        rad = np.atleast_1d(np.asarray(self.radius, dtype=np.float64))
+        if rad.size == 1:
+            rad = np.full(N, float(rad[0]))
+        elif rad.size != N:
+            raise RuntimeError("The number of particles is inconsistent with the number of radii provided.")
+        mono = bool(np.all(rad == rad[0]))
+        if self.field_type == "monodisperse" and not mono:
+            raise RuntimeError("field_type was set to 'monodisperse' but radii are not identical.")
+        self._ls = float(rad.min())
+        self._eps = self._eps_matrix(N) / self.eps_m
+        self._rad_s = rad / self._ls
+        box_s = self.box / self._ls
+        if self.field_type == "direct":
+            self._F = capi.Field(capi.FIELD_DIRECT, radius=self._rad_s)
+        elif self.field_type == "polydisperse" or (self.field_type == "auto" and not mono):
+            self._F = capi.Field(capi.FIELD_POLY, box_s, self.tol, self.xi, radius=self._rad_s)
+        else:
+            self._F = capi.Field(capi.FIELD_MONO, box_s, self.tol, self.xi)
+        self._N = N
+
+    # -- one beam position (eels_solver.cu:386-881, without the zone sum) ---
+    def _frame(self, epos, pos_s):
+        import torch
+
+        N, W = self._N, len(self.omega)
+        om = self.omega * self._ls
+        gamma = 1.0 / math.sqrt(1.0 - self.v * self.v)
+        e_s = np.asarray(epos, dtype=np.float64) / self._ls
+        B = np.empty((3 * N, W), dtype=np.complex128)
+        for w in range(W):
+            B[:, w] = beam_field(pos_s, e_s, om[w], self.v, gamma, self._ls).ravel()
+        S = (-3.0 / (4.0 * _PI * (1.0 - self._eps))).T.copy()          # (N, W)
+        dev = torch.device("cuda")
+        Bt = torch.tensor(B, device=dev)
+        X = torch.zeros_like(Bt)
+        St = torch.tensor(S, device=dev)
+        method = capi.METHOD_BICGSTAB if self.solver_type == "bicgstab" else capi.METHOD_GMRES
+        self._F.batch_solve(Bt, X, St, tol=self.tol, method=method, jacobi=self.use_jacobi_precond,
+                            recip_fp32=not self._fp64, refine=not self._fp64)
+        p = X.cpu().numpy()
+        eels = np.imag(np.sum(p * np.conj(B), axis=0)) / (2.0 * _PI * _PI)
+        dips = p.T.reshape(W, N, 3)
+        return eels, dips
+
+    def compute(self, epos, positions):
+        positions = np.asarray(positions, dtype=np.float64)
+        if positions.ndim != 2 or positions.shape[1] != 3:
+            raise ValueError("positions must be of shape (num_particles, 3)")
+        epos = np.asarray(epos, dtype=np.float64)
+        if epos.ndim == 1:
+            if epos.shape[0] != 2:
+                raise ValueError("epos must be of shape (2,) or (num_epos, 2)")
+            epos = epos[np.newaxis, :]
+        elif epos.ndim != 2 or epos.shape[1] != 2:
+            raise ValueError("epos must be of shape (2,) or (num_epos, 2)")
+        N = len(positions)
+        if N == 0:
+            return
+        if self._N == 0:
+            self._setup(N)
+        elif N != self._N:
+            raise RuntimeError("The number of particles has changed!")
+        self.positions = positions
+        pos_s = positions / self._ls
+        self._F.set_positions(pos_s)
+        for e in epos:
+            if not self.quiet:
+                print("  [EELS] impact parameter", e)
+            eels, dips = self._frame(e, pos_s)
+            self._eels.append(eels)
+            self._dips.append(dips)
+
+    def get_eels(self):
+        """Loss probability, (num_epos, num_wavelengths), squeezed."""
+        return np.squeeze(np.array(self._eels))
+
+    def get_dipoles(self, physical=True):
+        """Induced dipoles, (num_epos, num_wavelengths, N, 3), squeezed;
+        physical units multiply by eps_m * a_min^3 (eels_solver.h:155-160)."""
+        d = np.array(self._dips)
+        if physical:
+            d = d * (self.eps_m * self._ls ** 3)
+        return np.squeeze(d)
+
+    def get_quadrupoles(self, physical=True):
+        raise RuntimeError("EELS quadrupoles are not available in this build")
+
+    def get_positions(self):
+        return self.positions

@@ -11,6 +11,16 @@ GOLDEN = os.path.join(ROOT, "tests", "golden")
 
 def pytest_configure(config):
     config.addinivalue_line("markers", "gpu: needs a CUDA GPU (B200)")
+    config.addinivalue_line("markers", "first_gpu_run: a GPU path whose first run on a B200 is still to come; "
+                                       "collected after every other test")
+
+
+def pytest_collection_modifyitems(config, items):
+    """Tests of paths that have not run on a GPU yet go last (stable order
+    otherwise), so that under -x a failure among them leaves every
+    established test already run."""
+    items[:] = ([it for it in items if it.get_closest_marker("first_gpu_run") is None]
+                + [it for it in items if it.get_closest_marker("first_gpu_run") is not None])
 
 
 @pytest.fixture

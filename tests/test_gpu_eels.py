@@ -1,0 +1,47 @@
+"""EELS on the device batched solve (cumpm_b200.eels) against the reference's
+golden vector and the EELS oracle."""
+import numpy as np
+import pytest
+
+from oracle import mpm_eels as E
+
+pytestmark = [pytest.mark.gpu, pytest.mark.first_gpu_run]
+
+
+def test_reference_golden_two_beams_five_frequencies(golden):
+    """tests/test_eels_solver.py:114-173 of the reference, through the
+    drop-in class: loss / (omega R) * (4 pi)^2 and the scaled dipoles to the
+    reference test's 2e-2."""
+    import cumpm_b200.eels as eels
+
+    g = golden("ref_eels_vs_python_module.npz")
+    R = float(g["radius"])
+    s = eels.EELS(box=g["box"], eps_p=g["eps_p"], omega=g["omega_nm"], v=float(g["v"]), eps_m=float(g["eps_m"]),
+                  radius=R, xi=0.5, tol=1e-3, field_type="direct", solver_type="bicgstab", quiet=True,
+                  precision="double")
+    s.compute(g["e_pos"], g["points"])
+    loss = s.get_eels() / (g["omega_nm"] * R) * (4.0 * np.pi) ** 2
+    np.testing.assert_allclose(loss, g["ref_eels"], rtol=2e-2, atol=1e-5)
+    np.testing.assert_allclose(s.get_dipoles(physical=False), g["ref_dips_stacked"], rtol=2e-2, atol=1e-5)
+
+
+@pytest.mark.parametrize("field_type,radius", [("direct", 3.0), ("monodisperse", 3.0),
+                                               ("polydisperse", [3.0, 3.6, 2.5])])
+def test_matches_oracle(field_type, radius):
+    import cumpm_b200.eels as eels
+
+    box = np.array([80.0, 80.0, 80.0])
+    pts = np.array([[0.0, 0.0, 0.0], [9.0, 1.0, -2.0], [-3.0, 8.5, 4.0]])
+    omega = np.array([0.04, 0.06, 0.09])
+    eps = 4.0 - 1.5 ** 2 / (omega ** 2 * 100 + 0.05j)
+    beams = np.array([[4.0, -5.0], [12.0, 3.0]])
+    s = eels.EELS(box, eps, omega, 0.5, eps_m=1.3, radius=radius, tol=1e-9, field_type=field_type, quiet=True,
+                  precision="double")
+    s.compute(beams, pts)
+    o = E.EELSOracle(box, eps, omega, 0.5, eps_m=1.3, radius=radius, tol=1e-9, field_type=field_type)
+    for b in beams:
+        o.compute(b, pts)
+    ref = np.array(o.eels)
+    np.testing.assert_allclose(s.get_eels(), ref, rtol=1e-6, atol=1e-9 * np.abs(ref).max())
+    np.testing.assert_allclose(s.get_dipoles(physical=False), np.array(o.dipoles), rtol=1e-6,
+                               atol=1e-8 * np.abs(np.array(o.dipoles)).max())

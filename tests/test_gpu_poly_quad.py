@@ -8,7 +8,7 @@ import pytest
 
 from oracle import mpm_oracle as O
 
-pytestmark = pytest.mark.gpu
+pytestmark = [pytest.mark.gpu, pytest.mark.first_gpu_run]
 
 BOX = (26.0, 24.0, 28.0)
 POS = np.array([[2, 2, 2], [8, 3, 4], [14, 9, 5], [3, 15, 12], [18, 18, 18], [10, 20, 7.0]])

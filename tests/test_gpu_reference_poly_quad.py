@@ -3,8 +3,8 @@ itself (oracle/_ref, the reference's Polydisperse_Ewald_Electric_Field with
 quadrupoles, run on the GPU).  This pins the oracle's restatement of the
 polydisperse quadrupole tables, the point-Gaussian grids, the joint scale and
 the spread of quadrupole q on particle q's stencil.  Skipped when the
-reference build is not present.  Collected after every other test, so a
-mismatch here leaves the rest already run."""
+reference build is not present.  Marked first_gpu_run: collected after every
+other test, so a mismatch here leaves the rest already run."""
 import glob
 import os
 import sys
@@ -14,7 +14,7 @@ import pytest
 
 from oracle import mpm_oracle as O
 
-pytestmark = pytest.mark.gpu
+pytestmark = [pytest.mark.gpu, pytest.mark.first_gpu_run]
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 REF_DIR = os.path.join(ROOT, "oracle", "_ref")
