@@ -16,10 +16,14 @@ frequency is one right-hand side of one batched Krylov solve on the GPU:
 * host: the loss by reciprocity, sum_p Im(p . conj(E_inc)) / (2 pi^2)
   (:796-838).
 
+Particles closer to the beam than ``split_dist`` (with ``N_split`` > 1) are
+split into sub-dipoles on a cubic, Fibonacci or fcc lattice in the unit
+sphere that keep the particle's volume (``eels.py:177-320``); each beam
+position then solves its own split system.
+
 Not available yet (they raise ``RuntimeError`` naming the gap): the
 Brillouin-zone sum (``asm_flag``, it needs the Bloch wavevector in the
-device operator), particle splitting near the beam (``split_dist`` with
-``N_split``) and quadrupoles.
+device operator) and quadrupoles.
 """
 import math
 
@@ -60,6 +64,80 @@ def beam_field(pos, epos, omega, v, gamma, length_scale):
     return np.stack([-pref * k1 * dx / r, -pref * k1 * dy / r, pref * 1j / gamma * k0], axis=1)
 
 
+def unit_offsets(method, n_split):
+    """Sub-dipole offsets inside the unit sphere (eels.py:177-258).
+
+    * cubic: the n^3 cell centres of [-1, 1]^3, n the smallest integer with
+      n^3 >= n_split, those within distance 1 kept;
+    * fibonacci: n_split golden-angle directions on the sphere times
+      cube-root shell radii ((i + 1/2)/n)^(1/3), the radii shuffled by the
+      generator of seed 0;
+    * fcc: points of even index sum on a cubic lattice of step h within
+      distance 1, h = (2 pi / 3n)^(1/3) shrunk by 2 % until at least n_split
+      points fit.
+    """
+    if method == "cubic":
+        n = int(np.ceil(n_split ** (1.0 / 3.0)))
+        while n ** 3 < n_split:
+            n += 1
+        h = 2.0 / n
+        c = np.linspace(-1.0 + h / 2.0, 1.0 - h / 2.0, n)
+        g = np.stack([a.ravel() for a in np.meshgrid(c, c, c, indexing="ij")], axis=1)
+        return g[np.linalg.norm(g, axis=1) <= 1.0]
+    if method == "fibonacci":
+        n = int(n_split)
+        i = np.arange(n, dtype=np.float64)
+        y = 1.0 - (i / float(n - 1)) * 2.0
+        t = np.pi * (3.0 - np.sqrt(5.0)) * i
+        s = np.sqrt(np.maximum(0.0, 1.0 - y * y))
+        dirs = np.stack([np.cos(t) * s, y, np.sin(t) * s], axis=1)
+        shells = ((i + 0.5) / n) ** (1.0 / 3.0)
+        np.random.default_rng(0).shuffle(shells)
+        return shells[:, None] * dirs
+    if method == "fcc":
+        n = max(1, int(n_split))
+
+        def lattice(step):
+            m = int(np.ceil(1.0 / step))
+            k = np.arange(-m, m + 1)
+            gx, gy, gz = np.meshgrid(k, k, k, indexing="ij")
+            even = (gx + gy + gz) % 2 == 0
+            g = np.stack([gx[even], gy[even], gz[even]], axis=1) * step
+            return g[np.linalg.norm(g, axis=1) <= 1.0]
+
+        h = ((2.0 * np.pi) / (3.0 * n)) ** (1.0 / 3.0)
+        pts = lattice(h)
+        while len(pts) < n and h > 1e-4:
+            h *= 0.98
+            pts = lattice(h)
+        return pts
+    raise ValueError(f"Unknown split_method: {method}")
+
+
+def split_near_beam(positions, e_pos, radii, eps, split_dist, offsets):
+    """Particles within split_dist of the beam (in the plane across it)
+    replaced by sub-dipoles at position + R * offset of radius
+    R / M^(1/3), M = len(offsets), each with its particle's permittivity;
+    the others first, in order (eels.py:261-320).  eps is (W, N)."""
+    positions = np.asarray(positions, dtype=np.float64)
+    d = np.linalg.norm(positions[:, :2] - np.asarray(e_pos, dtype=np.float64)[None, :], axis=1)
+    close = d < split_dist
+    if not np.any(close):
+        return positions.copy(), np.asarray(radii, dtype=np.float64).copy(), np.asarray(eps).copy()
+    keep = np.nonzero(~close)[0]
+    M = len(offsets)
+    frac = 1.0 / (M ** (1.0 / 3.0))
+    pos_out = [positions[keep]]
+    rad_out = [np.asarray(radii, dtype=np.float64)[keep]]
+    eps_out = [np.asarray(eps)[:, keep]]
+    for i in np.nonzero(close)[0]:
+        R = float(radii[i])
+        pos_out.append(positions[i] + offsets * R)
+        rad_out.append(np.full(M, R * frac))
+        eps_out.append(np.repeat(np.asarray(eps)[:, i:i + 1], M, axis=1))
+    return np.concatenate(pos_out), np.concatenate(rad_out), np.concatenate(eps_out, axis=1)
+
+
 class EELS:
     """EELS probability spectrum and induced dipoles (see the module
     docstring); same constructor, ``compute``, ``get_eels``,
@@ -79,8 +157,9 @@ class EELS:
             raise ValueError("box must have length 3")
         if solver_type not in ("gmres", "bicgstab"):
             raise ValueError(f"Unknown solver_type: {solver_type}")
-        if split_dist is not None and float(split_dist) > 0.0 and int(N_split) > 1:
-            raise RuntimeError("EELS particle splitting near the beam is not available in this build")
+        self.split_dist = 0.0 if split_dist is None else float(split_dist)
+        self.N_split = 0 if N_split is None else int(N_split)
+        self.split_method = split_method
         if solve_quadrupoles or (quad_idxs is not None and len(quad_idxs)):
             raise RuntimeError("EELS quadrupoles are not available in this build")
         if asm_flag:
@@ -99,6 +178,8 @@ class EELS:
         self._N = 0
         self._F = None
         self._eels, self._dips = [], []
+        self._split_pos, self._dip_scale = [], []
+        self._precision = precision
         self.positions = None
 
     # -- set-up (eels_solver.cu:202-263) -----------------------------------
@@ -178,6 +259,9 @@ class EELS:
         N = len(positions)
         if N == 0:
             return
+        if self._splitting():
+            self._compute_split(epos, positions)
+            return
         if self._N == 0:
             self._setup(N)
         elif N != self._N:
@@ -192,13 +276,58 @@ class EELS:
             self._eels.append(eels)
             self._dips.append(dips)
 
+    # -- splitting near the beam (eels.py:381-478) --------------------------
+    def _splitting(self):
+        return self.split_dist > 0.0 and self.N_split > 1
+
+    def _compute_split(self, epos, positions):
+        N, W = len(positions), len(self.omega)
+        rad = np.atleast_1d(np.asarray(self.radius, dtype=np.float64))
+        if rad.size == 1:
+            rad = np.full(N, float(rad[0]))
+        elif rad.size != N:
+            raise ValueError("The number of particles is inconsistent with the number of radii provided.")
+        eps = self._eps_matrix(N)
+        offsets = unit_offsets(self.split_method, self.N_split)
+        self.positions = positions
+        for e in epos:
+            if not self.quiet:
+                print("  [EELS] impact parameter", e)
+            sp, sr, se = split_near_beam(positions, e, rad, eps, self.split_dist, offsets)
+            sub = EELS(self.box, se, self.omega, self.v, eps_m=self.eps_m, radius=sr, xi=self.xi, tol=self.tol,
+                       quiet=True, solver_type=self.solver_type, field_type=self.field_type,
+                       precision=self._precision)
+            sub.use_jacobi_precond = self.use_jacobi_precond
+            sub.compute(e, sp)
+            self._eels.append(sub._eels[0])
+            self._dips.append(sub._dips[0])
+            self._split_pos.append(sp)
+            # physical dipoles of a split system scale by the first particle's
+            # radius, as the reference does (eels.py:469)
+            self._dip_scale.append(self.eps_m * sr[0] ** 3)
+
+    @staticmethod
+    def _stack(items):
+        if len(items) == 1:
+            return np.squeeze(items[0])
+        try:
+            return np.squeeze(np.stack(items))
+        except ValueError:
+            return [np.squeeze(a) for a in items]
+
     def get_eels(self):
         """Loss probability, (num_epos, num_wavelengths), squeezed."""
         return np.squeeze(np.array(self._eels))
 
     def get_dipoles(self, physical=True):
-        """Induced dipoles, (num_epos, num_wavelengths, N, 3), squeezed;
-        physical units multiply by eps_m * a_min^3 (eels_solver.h:155-160)."""
+        """Induced dipoles, (num_epos, num_wavelengths, N, 3), squeezed
+        (a list when split systems differ in size); physical units multiply
+        by eps_m * a_min^3 (eels_solver.h:155-160)."""
+        if self._splitting():
+            if not self._dips:
+                return []
+            d = [a * f for a, f in zip(self._dips, self._dip_scale)] if physical else list(self._dips)
+            return self._stack(d)
         d = np.array(self._dips)
         if physical:
             d = d * (self.eps_m * self._ls ** 3)
@@ -208,4 +337,8 @@ class EELS:
         raise RuntimeError("EELS quadrupoles are not available in this build")
 
     def get_positions(self):
+        """Positions used: the split systems of every beam position when
+        splitting, else the particles."""
+        if self._splitting():
+            return self._stack(self._split_pos) if self._split_pos else []
         return self.positions

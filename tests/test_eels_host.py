@@ -38,7 +38,7 @@ def test_constructor_checks():
         eels.EELS([50.0] * 3, [4.0], [0.1], 0.3, field_type="fast")
     with pytest.raises(ValueError, match="box must have length 3"):
         eels.EELS([50.0] * 2, [4.0], [0.1], 0.3)
-    for kw in (dict(split_dist=4.0, N_split=27), dict(solve_quadrupoles=True), dict(asm_flag=True)):
+    for kw in (dict(solve_quadrupoles=True), dict(asm_flag=True)):
         with pytest.raises(RuntimeError, match="not available in this build"):
             eels.EELS([50.0] * 3, [4.0], [0.1], 0.3, **kw)
 
@@ -51,3 +51,46 @@ def test_positions_and_beams_are_checked():
         s.compute([0.0, 0.0], np.zeros((3, 2)))
     with pytest.raises(ValueError, match="epos must be of shape"):
         s.compute([0.0, 0.0, 1.0], np.zeros((3, 3)))
+
+
+@pytest.mark.parametrize("method", ["cubic", "fibonacci", "fcc"])
+@pytest.mark.parametrize("n", [8, 27, 50, 100])
+def test_unit_offsets_match_reference(golden, method, n):
+    """Sub-dipole lattices against the reference's own Python
+    (src/cuMPM/eels.py:177-258; fixture script
+    tests/golden/make_eels_split_golden.py)."""
+    from cumpm_b200 import eels
+
+    ref = golden("ref_eels_split.npz")[f"offsets_{method}_{n}"]
+    got = eels.unit_offsets(method, n)
+    assert got.shape == ref.shape
+    np.testing.assert_allclose(got, ref, rtol=1e-14, atol=1e-15)
+
+
+@pytest.mark.parametrize("method,n", [("cubic", 27), ("fibonacci", 20), ("fcc", 50)])
+def test_split_near_beam_matches_reference(golden, method, n):
+    """Particles 0 and 2 lie within 4 of the beam at (1, 0) (particle 3 just
+    outside, at 4.03): they become sub-dipoles after the untouched particles
+    1 and 3 (eels.py:261-320)."""
+    from cumpm_b200 import eels
+
+    g = golden("ref_eels_split.npz")
+    off = eels.unit_offsets(method, n)
+    p, r, e = eels.split_near_beam(g["split_pos_in"], g["split_epos"], g["split_radii_in"], g["split_eps_in"],
+                                   float(g["split_dist"]), off)
+    np.testing.assert_allclose(p, g[f"split_{method}_{n}_pos"], rtol=1e-14, atol=1e-14)
+    np.testing.assert_allclose(r, g[f"split_{method}_{n}_radii"], rtol=1e-14)
+    np.testing.assert_array_equal(e, g[f"split_{method}_{n}_eps"])
+    assert len(p) == 2 + 2 * len(off)
+    # the sub-dipoles keep each particle's volume
+    vol = np.sum(r ** 3)
+    assert vol == pytest.approx(np.sum(g["split_radii_in"] ** 3), rel=1e-12)
+
+
+def test_split_with_no_particle_near_the_beam_is_a_copy():
+    from cumpm_b200 import eels
+
+    pos = np.array([[10.0, 0, 0], [0, 12.0, 0]])
+    p, r, e = eels.split_near_beam(pos, [0.0, 0.0], [1.0, 2.0], np.ones((3, 2)), 4.0, eels.unit_offsets("cubic", 8))
+    np.testing.assert_array_equal(p, pos)
+    assert r.tolist() == [1.0, 2.0] and e.shape == (3, 2)

@@ -45,3 +45,32 @@ def test_matches_oracle(field_type, radius):
     np.testing.assert_allclose(s.get_eels(), ref, rtol=1e-6, atol=1e-9 * np.abs(ref).max())
     np.testing.assert_allclose(s.get_dipoles(physical=False), np.array(o.dipoles), rtol=1e-6,
                                atol=1e-8 * np.abs(np.array(o.dipoles)).max())
+
+
+def test_split_systems_match_oracle():
+    """Splitting near the beam (cubic, 27 -> 19 sub-dipoles): each beam
+    position solves its own split system; the oracle solves the same split
+    systems (built by the splitting that tests/test_eels_host.py pins
+    against the reference's Python)."""
+    import cumpm_b200.eels as eels
+
+    box = np.array([80.0, 80.0, 80.0])
+    pts = np.array([[0.0, 0.0, 0.0], [12.0, 0.0, 0.0], [0.0, 13.0, 2.0]])
+    omega = np.array([0.05, 0.08])
+    eps = 4.0 - 1.5 ** 2 / (omega ** 2 * 100 + 0.05j)
+    beams = np.array([[2.0, 1.0], [11.0, -2.0]])
+    s = eels.EELS(box, eps, omega, 0.5, radius=3.0, tol=1e-9, field_type="direct", quiet=True, split_dist=5.0,
+                  N_split=27, precision="double")
+    s.compute(beams, pts)
+    off = eels.unit_offsets("cubic", 27)
+    ref_eels, ref_dips = [], []
+    for b in beams:
+        sp, sr, se = eels.split_near_beam(pts, b, np.full(3, 3.0), np.repeat(eps[:, None], 3, axis=1), 5.0, off)
+        o = E.EELSOracle(box, se, omega, 0.5, radius=sr, tol=1e-9, field_type="direct")
+        l, d = o.compute(b, sp)
+        ref_eels.append(l)
+        ref_dips.append(d)
+    np.testing.assert_allclose(s.get_eels(), np.array(ref_eels), rtol=1e-6)
+    np.testing.assert_allclose(s.get_dipoles(physical=False), np.array(ref_dips), rtol=1e-6,
+                               atol=1e-8 * np.abs(np.array(ref_dips)).max())
+    assert len(s.get_positions()) == 2 and len(s.get_positions()[0]) == 2 + 19
