@@ -94,3 +94,15 @@ def test_split_with_no_particle_near_the_beam_is_a_copy():
     p, r, e = eels.split_near_beam(pos, [0.0, 0.0], [1.0, 2.0], np.ones((3, 2)), 4.0, eels.unit_offsets("cubic", 8))
     np.testing.assert_array_equal(p, pos)
     assert r.tolist() == [1.0, 2.0] and e.shape == (3, 2)
+
+
+@pytest.mark.parametrize("method,n", [("cubic", 27), ("cubic", 64), ("fcc", 50), ("fcc", 13)])
+def test_symmetric_lattices_keep_the_centre(method, n):
+    """The cubic and fcc sub-dipole lattices are symmetric about the centre,
+    so a split particle's sub-dipoles keep its centre (the reference checks
+    this for fcc, tests/test_eels_solver.py:229-230) and its volume."""
+    from cumpm_b200 import eels
+
+    off = eels.unit_offsets(method, n)
+    assert np.linalg.norm(off.mean(axis=0)) < 1e-12
+    assert np.all(np.linalg.norm(off, axis=1) <= 1.0)

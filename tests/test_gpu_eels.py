@@ -74,3 +74,19 @@ def test_split_systems_match_oracle():
     np.testing.assert_allclose(s.get_dipoles(physical=False), np.array(ref_dips), rtol=1e-6,
                                atol=1e-8 * np.abs(np.array(ref_dips)).max())
     assert len(s.get_positions()) == 2 and len(s.get_positions()[0]) == 2 + 19
+
+
+@pytest.mark.parametrize("method,n", [("cubic", 27), ("fcc", 50)])
+def test_reference_splitting_checks(method, n):
+    """tests/test_eels_solver.py:176-230 of the reference: particle 0 near
+    the beam is split; with fcc the sub-dipoles keep its centre."""
+    import cumpm_b200 as cuMPM
+
+    s = cuMPM.EELS(box=[100, 100, 100], eps_p=[4.0], omega=[0.15], v=0.3, radius=2.0, split_dist=4.0, N_split=n,
+                   split_method=method, field_type="direct", precision="double", quiet=True)
+    s.compute(np.array([1.0, 0.0]), np.array([[0.0, 0.0, 0.0], [10.0, 0.0, 0.0]]))
+    split_pos = s.get_positions()
+    assert len(split_pos) > 2
+    if method == "fcc":
+        assert np.linalg.norm(np.mean(split_pos[1:], axis=0)) < 1e-12
+    assert np.all(np.isfinite(s.get_eels()))
