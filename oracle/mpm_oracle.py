@@ -1631,8 +1631,12 @@ def near_field_intensity(box, E0, radius, dip, dip_pos, field_points, xi=0.5, er
     srad = np.asarray(rad) / ls
     pos = np.asarray(dip_pos, dtype=np.float64) / ls
     fp = np.asarray(field_points, dtype=np.float64) / ls
+    mono = all(r == rad[0] for r in rad)
     if field_type == "direct":
         op = DirectOperator(srad, solver_ax=False)
+    elif field_type == "polydisperse" or (field_type == "auto" and not mono):
+        # polydisperse field on the radii scaled by the first one (:98-135)
+        op = PolyEwaldOperator(sbox, errortol, xi, srad, solver_ax=False)
     else:
         op = MonoEwaldOperator(sbox, errortol, xi, solver_ax=False)
     op.set_positions(pos, fp)

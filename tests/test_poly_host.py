@@ -133,3 +133,23 @@ def test_oracle_poly_solver_matches_direct_in_large_box():
     b.compute(pos)
     np.testing.assert_allclose(a.get_eff_polarizability(), b.get_eff_polarizability(), rtol=1e-3, atol=1e-3)
     np.testing.assert_allclose(a.get_dipoles(), b.get_dipoles(), rtol=1e-3, atol=1e-3)
+
+
+def test_near_field_polydisperse_branch():
+    """Near field with field_type polydisperse (near_field.cu:98-135): at
+    equal radii it is the monodisperse near field (the mono/poly
+    equivalence at radius 1 holds for field points too), and "auto" with
+    unequal radii takes it."""
+    rng = np.random.default_rng(17)
+    box = [30.0, 28.0, 32.0]
+    dip_pos = np.array([[3.0, 4.0, 5.0], [12.0, 14.0, 9.0], [20.0, 6.0, 25.0]])
+    dip = rng.standard_normal((3, 3)) + 1j * rng.standard_normal((3, 3))
+    fp = rng.uniform(0, 28, (6, 3))
+    E0 = [1.0, 0.0, 0.0]
+    a = O.near_field_intensity(box, E0, 1.0, dip, dip_pos, fp, errortol=1e-6, field_type="monodisperse")
+    b = O.near_field_intensity(box, E0, 1.0, dip, dip_pos, fp, errortol=1e-6, field_type="polydisperse")
+    np.testing.assert_allclose(b, a, rtol=1e-5)
+    c = O.near_field_intensity(box, E0, [1.0, 1.3, 1.1], dip, dip_pos, fp, errortol=1e-6, field_type="auto")
+    d = O.near_field_intensity(box, E0, [1.0, 1.3, 1.1], dip, dip_pos, fp, errortol=1e-6, field_type="polydisperse")
+    np.testing.assert_array_equal(c, d)
+    assert np.abs(c - a).max() > 0
