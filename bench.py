@@ -14,10 +14,16 @@ one converged right-hand side.
 This arm: all 30 right-hand sides in one batch, fp32 operator inside fp64
 iterative refinement.  `value` is device-timed with device-resident inputs;
 `e2e` runs the same workload through the public drop-in API
-(cumpm_b200.dipole_solver) with host inputs and outputs.
+(cumpm_b200.dipole_solver) with host inputs and outputs.  Beside it the line
+carries: the plain per-system fp64 solve on this build's kernels, every
+dipole's error against an fp64 solve of the same system, the reference
+build's own GPU solve of the same workload (when it was compiled into
+oracle/_ref), the CPU port's full solve, and the other benchmark workloads
+(BiCGSTAB on the monolayer, the polydisperse packing, the small random
+packing) as extra keys.
 
-`--impl reference` times the CPU port of the reference algorithm (oracle/)
-on the host cores, per the measurement rules of this project.
+`--impl reference` times full single-right-hand-side GMRES solves of the CPU
+port of the reference algorithm (oracle/) on the host cores.
 
 Multi-GPU (torchrun): every rank solves an independent replica (the same
 geometry at its own frequency set); no collective on the data path.
@@ -30,6 +36,7 @@ import math
 import os
 import subprocess
 import sys
+import tempfile
 import threading
 import time
 
@@ -46,11 +53,9 @@ TOL = 1e-6
 XI = 0.5
 N_FREQ = 10
 K_POL = 3
-# GMRES(50)+Jacobi matvecs per right-hand side of the plain algorithm on each
-# workload (fp64 operator, one right-hand side per solve, tol 1e-6), as the
-# plain-fp64 leg of this script measures them on a B200; used to turn one
-# timed CPU matvec into solves/s when that leg did not run.
-PLAIN_MATVECS_PER_SOLVE = {"monolayer": 15.3, "poly3d": 19.6}
+# the fp64 solve every dipole is compared with (same operator, GMRES to this
+# preconditioned residual)
+REF_SOLVE_TOL = 1e-11
 
 
 def hex_lattice(n, spacing):
@@ -97,6 +102,7 @@ class Workload:
 
     def __init__(self, name, rank=0):
         self.name = name
+        self.restart = 50
         if name == "monolayer":
             pos, box, eps = workload(rank)
             self.radius_nm = np.full(len(pos), RADIUS)
@@ -113,6 +119,17 @@ class Workload:
             self.label = ("N=1000 polydisperse 3D packing, radii U[1,4] nm (seeded), phi 0.15, periodic box "
                           f"{box[0]:.1f} nm, Drude (eps_inf 4, wp 1.8 eV, gamma 0.1 eV), eps_m 1.77, 64 freqs "
                           "0.2-1.2 eV x 3 pols = 192 RHS, tol 1e-6, GMRES(50)+Jacobi, fp32 inner + fp64 refinement")
+        elif name == "c1":
+            rad = np.full(500, RADIUS)
+            pos, box = rsa_packing(500, rad, 0.10, 500 + rank)
+            omega = np.array([0.5 + 0.01 * rank])
+            eps = 4.0 - 1.8 ** 2 / (omega ** 2 + 1j * omega * 0.1)
+            self.radius_nm = rad
+            self.K = 1
+            self.restart = 30
+            self.label = (f"N=500 random packing a=5nm, phi 0.10, periodic cube {box[0]:.1f} nm, Drude "
+                          "(eps_inf 4, wp 1.8 eV, gamma 0.1 eV) at 0.5 eV, eps_m 1.77, x-polarised (1 RHS), "
+                          "tol 1e-6, GMRES(30)+Jacobi")
         else:
             raise ValueError(f"unknown workload {name}")
         self.unit = float(self.radius_nm.min())
@@ -131,17 +148,20 @@ class Workload:
 
 METRIC = "solves/s at N=4000, res 1e-6: batched mixed-prec vs plain; matvec % HBM peak"
 METRICS = {"monolayer": METRIC,
-           "poly3d": "solves/s, polydisperse N=1000, 192 RHS, res 1e-6: batched mixed-prec vs plain; matvec % HBM peak"}
+           "poly3d": "solves/s, polydisperse N=1000, 192 RHS, res 1e-6: batched mixed-prec vs plain; matvec % HBM peak",
+           "c1": "solves/s, N=500 random packing, 1 RHS, res 1e-6"}
 DATA = {"monolayer": "synthetic (hexagonal monolayer generated as in the reference benchmark)",
-        "poly3d": "synthetic (seeded random sequential addition of polydisperse spheres)"}
+        "poly3d": "synthetic (seeded random sequential addition of polydisperse spheres)",
+        "c1": "synthetic (seeded random sequential addition of equal spheres)"}
 WORKLOAD_LABEL = ("N=4000 hex monolayer a=5nm spacing 12nm, box 1542.0x332.6x1000nm, Drude "
                   "(eps_inf 4, wp 1.8 eV, gamma 0.1 eV), eps_m 1.77, 10 freqs 0.2-1.0 eV x 3 pols = 30 RHS, "
                   "tol 1e-6 (Ewald and true fp64 residual), GMRES(50)+Jacobi, fp32 inner + fp64 refinement")
 
 
-def device_problem(wl, torch, dev):
+def problem_arrays(wl):
     """Right-hand sides, mean-field initial guesses and self coefficients in
-    the [row][M] layout (dipole_solver.cu:233-257, 438-489)."""
+    the [row][M] layout (dipole_solver.cu:233-257, 438-489), host arrays.
+    Column m is frequency m // K, polarisation m % K."""
     N = len(wl.pos)
     M = wl.M
     K = wl.K
@@ -155,8 +175,37 @@ def device_problem(wl, torch, dev):
     beta = (e - 1) / (e + 2)
     g = 4 * np.pi * beta / (1 - beta * phi)                   # per column, radius 1
     X0 = B * g[None, :] * np.repeat(a3, 3)[:, None]
+    return B, X0, sc
+
+
+def device_problem(wl, torch, dev):
+    B, X0, sc = problem_arrays(wl)
     t = lambda a: torch.tensor(a, dtype=torch.complex128, device=dev)
     return t(B), t(X0), t(sc)
+
+
+def fp64_reference_solution(F, B, X0, S, capi, tol=REF_SOLVE_TOL):
+    """The fp64 solution every dipole is compared with: GMRES(50)+Jacobi on
+    the fp64 operator (fp64 spread/FFT/contraction and real space) from X0,
+    to a preconditioned residual of `tol`, all columns in one batch."""
+    X = X0.clone()
+    F.batch_solve(B, X, S, tol=tol, method=capi.METHOD_GMRES, restart=50, maxiter=4000, recip_fp32=False,
+                  real_fp32=False, refine=False)
+    return X
+
+
+def dipole_errors(X, Xref, N):
+    """Per-dipole error of X against Xref ([3N][M] complex): the largest
+    |p_i - p_i^ref| / |p_i^ref| over particles and columns (3-vector norms),
+    and the largest column-normwise |X - Xref| / |Xref|."""
+    import torch
+    D = (X - Xref)[:3 * N].reshape(N, 3, -1)
+    R = Xref[:3 * N].reshape(N, 3, -1)
+    dn = torch.linalg.vector_norm(D, dim=1)
+    rn = torch.linalg.vector_norm(R, dim=1)
+    per = (dn / rn.clamp_min(1e-300)).max().item()
+    col = (torch.linalg.vector_norm(X - Xref, dim=0) / torch.linalg.vector_norm(Xref, dim=0)).max().item()
+    return {"max_dipole_rel_err": per, "max_normwise_rel_err": col}
 
 
 class ClockSampler:
@@ -212,14 +261,13 @@ def measured_peaks():
 
 
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per algorithmic
-# byte of a stage's kernels, from ncu --set full captures of one launch each
-# (profiles/kernels_monolayer_n4000.md: x and y transforms of a 25-column
-# matvec, 522.6 MB of DRAM traffic for 632.4 MB algorithmic;
-# profiles/kernels_poly3d_n1000.md: spread 1892 MB for 1962 MB, plain axis
-# pass 3811 MB for 3870 MB).  Traffic scales with the columns a launch
-# carries, so a stage's traffic per launch is this ratio times its
-# algorithmic bytes per launch.  Below 1: the last writes of a launch are
-# still in L2 when the kernel ends.
+# byte of a stage's kernels, from ncu captures of one launch of each kernel
+# on the same workload (monolayer: x and y transforms of a 25-column matvec,
+# 522.6 MB of DRAM traffic for 632.4 MB algorithmic; polydisperse packing:
+# spread 1892 MB for 1962 MB, plain axis pass 3811 MB for 3870 MB).  Traffic
+# scales with the columns a launch carries, so a stage's traffic per launch
+# is this ratio times its algorithmic bytes per launch.  Below 1: the last
+# writes of a launch are still in L2 when the kernel ends.
 TRAFFIC_PER_ALG_BYTE = {
     ("monolayer", "fft_fwd"): 522.6 / 632.4,
     ("monolayer", "fft_inv"): 522.2 / 632.4,
@@ -278,6 +326,60 @@ def replica_throughput(t_ms, units, dist=None, device="cpu"):
     return t_max, total, total / (t_max / 1e3)
 
 
+class Timed:
+    """The batched mixed-precision solve of one workload, its steps timed
+    with CUDA events after an L2 flush (a 256 MB write outside the timed
+    interval)."""
+
+    def __init__(self, wl, capi, torch, dev, args, method, flush, dist=None):
+        self.wl, self.capi, self.torch, self.dist, self.flush = wl, capi, torch, dist, flush
+        self.F = wl.field(capi)
+        self.B, self.X0, self.S = device_problem(wl, torch, dev)
+        self.X = torch.empty_like(self.X0)
+        self.M = self.B.shape[1]
+        self.opts = dict(tol=TOL, method=method, restart=wl.restart, maxiter=1000, refine=True,
+                         inner_tol=args.inner_tol, compact=not args.no_compact)
+        self.reports = []
+
+    def step(self):
+        self.F.set_positions(self.wl.pos)
+        self.X.copy_(self.X0)
+        self.reports.append(self.F.batch_solve(self.B, self.X, self.S, **self.opts))
+
+    def timed(self, nsteps):
+        torch = self.torch
+        if self.dist:
+            self.dist.barrier()
+        torch.cuda.synchronize()
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(nsteps)]
+        for k in range(nsteps):
+            self.flush.fill_(float(k))  # L2 flush outside the timed interval
+            ev[k][0].record()
+            self.step()
+            ev[k][1].record()
+        torch.cuda.synchronize()
+        if self.dist:
+            self.dist.barrier()
+        return sum(a.elapsed_time(b) for a, b in ev)
+
+    def warm(self, n):
+        for _ in range(n):
+            self.step()
+        self.torch.cuda.synchronize()
+
+    def true_residuals(self):
+        torch = self.torch
+        R = self.B - self.F.apply(self.X, self_coef=self.S)
+        return (torch.linalg.vector_norm(R, dim=0) / torch.linalg.vector_norm(self.B, dim=0)).cpu().numpy()
+
+    def accuracy(self):
+        Xref = fp64_reference_solution(self.F, self.B, self.X0, self.S, self.capi)
+        e = dipole_errors(self.X, Xref, len(self.wl.pos))
+        e["reference"] = (f"fp64 GMRES(50)+Jacobi on the same fp64 operator to preconditioned residual "
+                          f"{REF_SOLVE_TOL:g}, every column")
+        return e, Xref
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
 
@@ -292,66 +394,108 @@ def run_ours(args, rank, world, local_rank):
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     wl = Workload(args.workload, rank)
-    pos = wl.pos
-    F = wl.field(capi)
-    B, X0, S = device_problem(wl, torch, dev)
-    X = torch.empty_like(X0)
-    M = B.shape[1]
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
-    opts = dict(tol=TOL, method=capi.METHOD_GMRES, restart=50, maxiter=1000, refine=True, inner_tol=args.inner_tol,
-                compact=not args.no_compact)
-    reports = []
-
-    def step():
-        F.set_positions(pos)
-        X.copy_(X0)
-        reports.append(F.batch_solve(B, X, S, **opts))
-
-    def timed(nsteps):
-        """nsteps steps, each bracketed by CUDA events after a 256 MB L2 flush."""
-        if dist:
-            dist.barrier()
-        torch.cuda.synchronize()
-        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(nsteps)]
-        for k in range(nsteps):
-            flush.fill_(float(k))  # L2 flush outside the timed interval
-            ev[k][0].record()
-            step()
-            ev[k][1].record()
-        torch.cuda.synchronize()
-        if dist:
-            dist.barrier()
-        return sum(a.elapsed_time(b) for a, b in ev)
-
-    for _ in range(args.warmup):
-        step()
-    torch.cuda.synchronize()
+    method = capi.METHOD_BICGSTAB if args.method == "bicgstab" else capi.METHOD_GMRES
+    T = Timed(wl, capi, torch, dev, args, method, flush, dist)
+    F, B, X0, S, M = T.F, T.B, T.X0, T.S, T.M
+    T.warm(args.warmup)
     info = F.info()
 
     # 1) the timed region: no stage timers
-    reports.clear()
+    T.reports.clear()
     launches0 = capi.kernel_launches()
     clocks = ClockSampler(local_rank)
     clocks.start()
-    t_ms = timed(args.steps)
+    t_ms = T.timed(args.steps)
     clk = clocks.stop()
     launches = capi.kernel_launches() - launches0
-    timed_reports = list(reports)
+    timed_reports = list(T.reports)
     # correctness of the timed result: fp64 true residual of every column
-    R = B - F.apply(X, self_coef=S)
-    rel = (torch.linalg.vector_norm(R, dim=0) / torch.linalg.vector_norm(B, dim=0)).cpu().numpy()
+    rel = T.true_residuals()
     converged = int(np.sum(rel <= TOL))
     t_max, conv_total, value = replica_throughput(t_ms, converged * args.steps, dist, dev)
     ms_per_step = t_max / args.steps
 
     # 2) the same steps again with per-stage CUDA events on the launching
     #    stream: stage breakdown and the roofline of the dominant stage
-    reports.clear()
+    T.reports.clear()
     capi.profile_reset()
     capi.profile_enable(not args.no_profile)
-    t_prof = timed(args.steps)
+    t_prof = T.timed(args.steps)
     capi.profile_enable(False)
     stages = capi.profile_read()
+    rl, mv_frac = stage_roofline(wl, info, M, T.reports, stages, args.steps)
+
+    out = None
+    if rank == 0:
+        # every dipole of the timed solve against an fp64 solve of the same system
+        acc, Xref = T.accuracy() if world == 1 and not args.no_accuracy else (None, None)
+        # 3) the plain per-system fp64 solve on the same operator: one
+        #    right-hand side per solve, fp64 reciprocal and real space
+        plain = run_plain(args, F, B, X0, S, M, torch, capi, wl) if not args.no_plain else None
+        iters = [r["total_iterations"] / M for r in timed_reports]
+        mv_per_step = sum(r["matvecs"] for r in timed_reports) / max(1, len(timed_reports))
+        colmv_per_step = sum(r["column_matvecs"] for r in timed_reports) / max(1, len(timed_reports))
+        solo = world == 1
+        e2e = run_e2e(args, torch, wl) if solo and not args.no_e2e else None
+        extras = run_extras(args, capi, torch, dev, flush) if solo and not args.no_extras else None
+        ref_gpu = reference_gpu_leg(args, wl, F, B, S, Xref, torch) if solo and not args.no_reference_gpu else None
+        cpu = cpu_baseline(args, wl) if solo and not args.no_cpu else None
+        out = {
+            "metric": METRICS[wl.name],
+            "value": round(value, 3),
+            "unit": "solves/s",
+            "n_gpus": world,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": round(ms_per_step, 3),
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "c64 operator / c128 refinement",
+            "data": DATA[wl.name],
+            "config": {
+                "workload": wl.label,
+                "method": args.method,
+                "rhs_per_step": M,
+                "converged_per_step": converged,
+                "max_true_rel_resid": float(rel.max()),
+                "krylov_steps_per_rhs": round(float(np.mean(iters)), 2),
+                "matvecs_per_step": mv_per_step,
+                "column_matvecs_per_step": colmv_per_step,
+                "inner_tol": f"max({args.inner_tol:g}, 0.5 tol |b_m| / |r_m|) per column",
+                "compact_batch": not args.no_compact,
+                "grid": info["grid"], "pruned_z_slots": info["z_slots"] if info["pruned"] else None,
+                "support": info["stencil"],
+                "real_space_pairs": info["num_pairs"],
+                "l2": "inputs larger than L2 (grid + Krylov basis > 126 MB) and a 256 MB L2 flush before each step",
+                "parallelism": f"replicas x{world}",
+                "profiled_ms_per_step": round(t_prof / args.steps, 3),
+                "stage_ms_per_step": {k: round(v[0] / args.steps, 3) for k, v in stages.items()},
+                "stage_launches_per_step": {k: v[1] / args.steps for k, v in stages.items()},
+            },
+            "accuracy": acc,
+            "matvec_hbm_frac": mv_frac,
+            "plain_fp64": plain,
+            "batched_vs_plain": round(value / plain["value"], 2) if plain else None,
+            "roofline": rl,
+            "reference_gpu": ref_gpu,
+            "extra_workloads": extras,
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "gpu_launches": launches,
+            "clocks": clk,
+        }
+        print(json.dumps(out), flush=True)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    return out
+
+
+def stage_roofline(wl, info, M, reports, stages, nsteps):
+    """Roofline of the dominant operator stage and the whole matvec's HBM
+    fraction, from the per-stage CUDA-event times of a profiled pass."""
     matvecs = sum(r["matvecs"] for r in reports)
     mv64 = sum(r["refine_steps"] + 1 for r in reports)  # fp64 true-residual matvecs, all M columns
     mv32 = matvecs - mv64
@@ -371,101 +515,46 @@ def run_ours(args, rank, world, local_rank):
     b32 = algorithmic_bytes(info, M, info["num_pairs"], False, wl.mono)
     dom = max(op_stages, key=lambda k: stages[k][0])
     dom_ms, dom_n = stages[dom]
+    if dom_ms <= 0:   # --no-profile: no stage timings, no roofline
+        return None, None
     bytes_total = stage_bytes(dom)
     peak, peak_kind = measured_peaks()
-    achieved = bytes_total / (dom_ms / 1e3) / 1e9 if dom_ms > 0 else 0.0
+    achieved = bytes_total / (dom_ms / 1e3) / 1e9
     ratio = TRAFFIC_PER_ALG_BYTE.get((wl.name, dom))
     traffic = round(ratio * bytes_total / max(1, dom_n)) if ratio else None
     mv_bytes = sum(stage_bytes(k) for k in op_stages)
     mv_ms = sum(stages[k][0] for k in op_stages)
     mv_frac = round(mv_bytes / (mv_ms / 1e3) / 1e9 / peak, 4) if mv_ms > 0 else None
-
-    # 3) the plain per-system fp64 solve on the same operator: one right-hand
-    #    side per solve, fp64 reciprocal and real space, no refinement
-    plain = run_plain(args, F, B, X0, S, M, torch, capi, wl) if not args.no_plain else None
-    iters = [r["total_iterations"] / M for r in timed_reports]
-    mv_per_step = sum(r["matvecs"] for r in timed_reports) / max(1, len(timed_reports))
-    colmv_per_step = sum(r["column_matvecs"] for r in timed_reports) / max(1, len(timed_reports))
-
-    out = None
-    if rank == 0:
-        e2e = run_e2e(args, torch, wl) if world == 1 and not args.no_e2e else None
-        per_solve = plain["matvecs_per_solve"] if plain else PLAIN_MATVECS_PER_SOLVE[args.workload]
-        cpu = cpu_baseline(args, wl, per_solve) if world == 1 and not args.no_cpu else None
-        out = {
-            "metric": METRICS[wl.name],
-            "value": round(value, 3),
-            "unit": "solves/s",
-            "n_gpus": world,
-            "steps": args.steps,
-            "warmup": args.warmup,
-            "ms_per_step": round(ms_per_step, 3),
-            "higher_is_better": True,
-            "scaling": "weak",
-            "vs_baseline": None,
-            "dtype": "c64 operator / c128 refinement",
-            "data": DATA[wl.name],
-            "config": {
-                "workload": wl.label,
-                "rhs_per_step": M,
-                "converged_per_step": converged,
-                "max_true_rel_resid": float(rel.max()),
-                "krylov_steps_per_rhs": round(float(np.mean(iters)), 2),
-                "matvecs_per_step": mv_per_step,
-                "column_matvecs_per_step": colmv_per_step,
-                "inner_tol": f"max({args.inner_tol:g}, 0.5 tol |b_m| / |r_m|) per column",
-                "compact_batch": not args.no_compact,
-                "grid": info["grid"], "pruned_z_slots": info["z_slots"] if info["pruned"] else None,
-                "support": info["stencil"],
-                "real_space_pairs": info["num_pairs"],
-                "l2": "inputs larger than L2 (grid + Krylov basis > 126 MB) and a 256 MB L2 flush before each step",
-                "parallelism": f"replicas x{world}",
-                "profiled_ms_per_step": round(t_prof / args.steps, 3),
-                "stage_ms_per_step": {k: round(v[0] / args.steps, 3) for k, v in stages.items()},
-                "stage_launches_per_step": {k: v[1] / args.steps for k, v in stages.items()},
-            },
-            "matvec_hbm_frac": mv_frac,
-            "plain_fp64": plain,
-            "batched_vs_plain": round(value / plain["value"], 2) if plain else None,
-            "roofline": {
-                "kernel": dom,
-                "bound": "hbm",
-                "achieved": round(achieved, 1),
-                "peak": peak,
-                "peak_source": peak_kind,
-                "unit": "GB/s",
-                "frac": round(achieved / peak, 4),
-                "traffic": None if traffic is None else traffic,
-                "traffic_source": ("ncu DRAM bytes per algorithmic byte of this stage's kernels (profiles/kernels_*.md)"
-                                   " x algorithmic bytes per launch") if traffic is not None else None,
-                "algorithmic_bytes_per_launch": round(bytes_total / max(1, dom_n)),
-                "algorithmic_bytes_full_batch_fp32": b32[dom],
-                "launches": dom_n,
-                "timing": "per-stage CUDA events on the launching stream over a second pass of the timed steps",
-            } if dom_ms > 0 else None,   # --no-profile: no stage timings, no roofline
-            "cpu_baseline": cpu,
-            "e2e": e2e,
-            "gpu_launches": launches,
-            "clocks": clk,
-        }
-        print(json.dumps(out), flush=True)
-    if dist:
-        dist.barrier()
-        dist.destroy_process_group()
-    return out
+    rl = {
+        "kernel": dom,
+        "bound": "hbm",
+        "achieved": round(achieved, 1),
+        "peak": peak,
+        "peak_source": peak_kind,
+        "unit": "GB/s",
+        "frac": round(achieved / peak, 4),
+        "traffic": traffic,
+        "traffic_source": ("ncu DRAM bytes per algorithmic byte of this stage's kernels (one captured launch each)"
+                           " x algorithmic bytes per launch") if traffic is not None else None,
+        "algorithmic_bytes_per_launch": round(bytes_total / max(1, dom_n)),
+        "algorithmic_bytes_full_batch_fp32": b32[dom],
+        "launches": dom_n,
+        "timing": "per-stage CUDA events on the launching stream over a second pass of the timed steps",
+    }
+    return rl, mv_frac
 
 
 def run_plain(args, F, B, X0, S, M, torch, capi, wl):
     """Plain per-system fp64 solves: one right-hand side at a time.
 
-    Right-hand sides are solved one by one with GMRES(50)+Jacobi on the fp64
+    Right-hand sides are solved one by one with GMRES+Jacobi on the fp64
     operator (the reference's plain method), each timed with CUDA events;
-    their count over the summed time gives plain solves/s.  All 30 columns
-    of the monolayer; every 8th of the 192 polydisperse columns.
+    their count over the summed time gives plain solves/s.  All columns up to
+    32; every 8th of the 192 polydisperse columns.
     """
     cols = list(range(0, M, 1 if M <= 32 else 8))
     Xp = torch.empty((B.shape[0], 1), dtype=B.dtype, device=B.device)
-    o = dict(tol=TOL, method=capi.METHOD_GMRES, restart=50, maxiter=1000, recip_fp32=False, refine=False)
+    o = dict(tol=TOL, method=capi.METHOD_GMRES, restart=wl.restart, maxiter=1000, recip_fp32=False, refine=False)
     # warm-up: plans and buffers for M=1
     Xp.copy_(X0[:, :1])
     F.batch_solve(B[:, :1].contiguous(), Xp, S[:, :1].contiguous(), **o)
@@ -488,7 +577,45 @@ def run_plain(args, F, B, X0, S, M, torch, capi, wl):
     n = len(cols)
     return {"value": round(n / (tot_ms / 1e3), 3), "unit": "solves/s", "rhs_sampled": n, "converged": ok,
             "ms_per_solve": round(tot_ms / n, 3), "matvecs_per_solve": mvs / n,
-            "method": f"GMRES(50)+Jacobi, fp64 operator, 1 RHS per solve, no refinement, {len(cols)} of {M} RHS"}
+            "method": f"GMRES({wl.restart})+Jacobi, fp64 operator, 1 RHS per solve, no refinement, "
+                      f"{len(cols)} of {M} RHS"}
+
+
+def run_extras(args, capi, torch, dev, flush):
+    """The other benchmark workloads, each timed like the headline step
+    (warm-up, CUDA events after an L2 flush): BiCGSTAB on the monolayer, the
+    N=1000 polydisperse packing (192 RHS) and the N=500 random packing
+    (1 RHS); with the plain fp64 leg and per-dipole accuracy."""
+    out = {}
+    steps = max(2, min(args.steps, 5))
+    warm = max(1, min(args.warmup, 3))
+    todo = [("monolayer_bicgstab", "monolayer", capi.METHOD_BICGSTAB), ("poly3d", "poly3d", capi.METHOD_GMRES),
+            ("c1", "c1", capi.METHOD_GMRES)]
+    for key, name, method in todo:
+        if name == args.workload and (method == capi.METHOD_GMRES) == (args.method == "gmres"):
+            continue
+        wl = Workload(name)
+        T = Timed(wl, capi, torch, dev, args, method, flush)
+        T.warm(warm)
+        T.reports.clear()
+        t = T.timed(steps)
+        rel = T.true_residuals()
+        conv = int(np.sum(rel <= TOL))
+        acc, _ = T.accuracy()
+        plain = run_plain(args, T.F, T.B, T.X0, T.S, T.M, torch, capi, wl)
+        value = conv * steps / (t / 1e3)
+        info = T.F.info()
+        out[key] = {
+            "workload": wl.label, "method": "bicgstab" if method == capi.METHOD_BICGSTAB else "gmres",
+            "value": round(value, 3), "unit": "solves/s", "ms_per_step": round(t / steps, 3), "steps": steps,
+            "rhs_per_step": T.M, "converged_per_step": conv, "max_true_rel_resid": float(rel.max()),
+            "krylov_steps_per_rhs": round(float(np.mean([r["total_iterations"] / T.M for r in T.reports])), 2),
+            "grid": info["grid"], "accuracy": acc, "plain_fp64": plain,
+            "batched_vs_plain": round(value / plain["value"], 2),
+        }
+        del T
+        torch.cuda.empty_cache()
+    return out
 
 
 def run_e2e(args, torch, wl):
@@ -497,7 +624,8 @@ def run_e2e(args, torch, wl):
 
     rad = wl.radius_nm if not wl.mono else float(wl.radius_nm[0])
     E0 = None if wl.K == 3 else [[1.0, 0.0, 0.0]]
-    mk = lambda: cuMPM.dipole_solver(wl.box_nm, wl.eps, radius=rad, eps_m=EPS_M, tol=TOL, quiet=True, E0=E0)
+    mk = lambda: cuMPM.dipole_solver(wl.box_nm, wl.eps, radius=rad, eps_m=EPS_M, tol=TOL, quiet=True, E0=E0,
+                                     solver_type=args.method)
     s = mk()
     s.set_solver_options(batch_all=True, refine=True, inner_tol=args.inner_tol)
     s.compute(wl.pos_nm)  # warm-up (plans, precalc buffers)
@@ -529,56 +657,165 @@ def run_e2e(args, torch, wl):
                       "memory out), median of steps; get_dipoles() read once after the loop"}
 
 
-def cpu_matvec_sample(threads, wl=None, min_s=10.0, max_n=8):
-    """Mean time of fp64 matvecs (1 RHS) of the CPU port of the reference operator.
+# ---------------------------------------------------------------- baselines
 
-    Repeats the matvec on the full workload until about min_s seconds of CPU
-    work (at most max_n matvecs); the per-frame precalculation is excluded.
-    """
+REF_DIR = os.path.join(ROOT, "oracle", "_ref")
+
+
+def reference_gpu_child(args):
+    """Runs in a child process (an error exit of the reference build cannot
+    take the benchmark down): the reference build's own Dipole_Solver on the
+    monolayer workload, timed as the reference's benchmark times it
+    (benchmarks/benchmark_cumpm_vs_pympm.py:35-89: a small warm-up solve,
+    then wall clock around one compute() of all frequencies and
+    polarisations), for fp64 ("double") and the default AUTO precision, with
+    GMRES and BiCGSTAB.  Writes the dipoles of each run to args.ref_out and
+    prints one JSON line."""
+    import glob
+
+    if not glob.glob(os.path.join(REF_DIR, "_cuMPM*.so")):
+        print(json.dumps({"unavailable": "reference build oracle/_ref not present"}))
+        return
+    sys.path.insert(0, REF_DIR)
+    import _cuMPM as R
+
+    wl = Workload("monolayer")
+    pos, box = wl.pos_nm, wl.box_nm
+    eps = [complex(e) for e in wl.eps]
+
+    def solver(prec, method, p, e, tol):
+        return R.Dipole_Solver(list(map(float, box)), e, radius=[RADIUS], eps_m=EPS_M, xi=XI, tol=tol, quiet=True,
+                               guess_type="derivative", solver_type=method, field_type="monodisperse", E0=[],
+                               solve_quadrupoles=False, quad_idxs=[], precision=p)
+
+    w = solver(R.PrecisionMode.AUTO, "gmres", None, eps[:2], 1e-3)   # warm-up: context, cuFFT
+    w.compute(list(pos[:100, 0]), list(pos[:100, 1]), list(pos[:100, 2]))
+    res = {}
+    dips = {}
+    for pname, prec in (("double", R.PrecisionMode.DOUBLE), ("auto", R.PrecisionMode.AUTO)):
+        for method in ("gmres", "bicgstab"):
+            s = solver(prec, method, None, eps, TOL)
+            t0 = time.perf_counter()
+            s.compute(list(pos[:, 0]), list(pos[:, 1]), list(pos[:, 2]))
+            t = time.perf_counter() - t0
+            d = np.asarray(s.get_dipoles(True))
+            key = f"{pname}_{method}"
+            dips[key] = d.reshape(-1)
+            res[key] = {"s_per_compute": round(t, 4), "rhs": wl.M, "rhs_per_s": round(wl.M / t, 3)}
+            del s
+    np.savez(args.ref_out, **dips)
+    print(json.dumps(res), flush=True)
+
+
+def reference_gpu_leg(args, wl, F, B, S, Xref, torch):
+    """The reference build (oracle/_ref) solving the same monolayer on this
+    GPU, in a child process; its dipoles are checked here with this build's
+    fp64 operator (true residual) and against the fp64 solution."""
+    if wl.name != "monolayer" or wl.K != 3:
+        return None
+    with tempfile.TemporaryDirectory() as td:
+        outp = os.path.join(td, "ref_dipoles.npz")
+        cmd = [sys.executable, os.path.abspath(__file__), "--_reference-gpu-child", "--ref-out", outp]
+        try:
+            r = subprocess.run(cmd, capture_output=True, text=True, timeout=600, cwd=ROOT)
+        except subprocess.TimeoutExpired:
+            return {"unavailable": "reference build run exceeded 600 s"}
+        lines = [ln for ln in r.stdout.strip().splitlines() if ln.startswith("{")]
+        if r.returncode != 0 or not lines:
+            return {"unavailable": f"reference build run failed (rc {r.returncode}): {r.stderr.strip()[-300:]}"}
+        res = json.loads(lines[-1])
+        if "unavailable" in res:
+            return res
+        dz = np.load(outp)
+        N, K, W = len(wl.pos), wl.K, len(wl.eps)
+        scale = EPS_M * wl.unit ** 3
+        for key, v in res.items():
+            d = dz[key].reshape(-1, W, N, K, 3)[-1] / scale           # (W, N, K, 3), solver units
+            X = np.transpose(d, (1, 3, 0, 2)).reshape(3 * N, W * K)  # row 3i+c, column w*K+k
+            X = np.ascontiguousarray(X)
+            Xt = torch.tensor(X, dtype=torch.complex128, device=B.device)
+            R = B - F.apply(Xt, self_coef=S)
+            rel = (torch.linalg.vector_norm(R, dim=0) / torch.linalg.vector_norm(B, dim=0)).cpu().numpy()
+            v["max_true_rel_resid"] = float(rel.max())
+            v["rhs_within_true_resid_tol"] = int(np.sum(rel <= TOL))
+            if Xref is not None:
+                v.update(dipole_errors(Xt, Xref, N))
+    return {"runs": res,
+            "protocol": "reference build (oracle/_ref, compiled from the reference sources for sm_100a) Dipole_Solver "
+                        "on the same workload: wall clock around one compute() of 10 freqs x 3 pols after a small "
+                        "warm-up solve, as benchmarks/benchmark_cumpm_vs_pympm.py times it; one RHS at a time, "
+                        "its own stop rule |D^-1 r| < tol |b|; residuals and errors computed here with this "
+                        "build's fp64 operator"}
+
+
+def _cpu_operator(wl, threads):
     from oracle import mpm_oracle as O
 
-    wl = wl or Workload("monolayer")
     if wl.mono:
         op = O.MonoEwaldOperator(wl.box, TOL, XI, True, fft_workers=threads)
     else:
         op = O.PolyEwaldOperator(wl.box, TOL, XI, wl.radius, True)
     op.set_positions(wl.pos)
+    return op
+
+
+def cpu_solve(op, wl, B, X0, S, m):
+    """One full fp64 GMRES+Jacobi solve of column m on the CPU port (the
+    reference's plain method: restart 50, stop rule |D^-1 r| < tol |b|);
+    (seconds, matvecs)."""
+    from oracle import mpm_oracle as O
+
     N = len(wl.pos)
-    rng = np.random.default_rng(0)
-    x = rng.standard_normal(3 * N) + 1j * rng.standard_normal(3 * N)
-    sc = 3.0 / (4 * np.pi * (wl.eps[0] / EPS_M - 1.0)) / wl.radius ** 3
-    ts = []
-    while not ts or (len(ts) < max_n and sum(ts) < min_s):
-        t0 = time.perf_counter()
-        op.apply(x, sc)
-        ts.append(time.perf_counter() - t0)
-    return float(np.mean(ts)), len(ts)
+    count = [0]
+
+    def A(v):
+        count[0] += 1
+        return op.apply(v, S[:, m])
+
+    Mj = O.jacobi_inverse(S[:, m], N)
+    t0 = time.perf_counter()
+    O.gmres(A, B[:, m], X0[:, m], TOL, Mj, restart=wl.restart)
+    return time.perf_counter() - t0, count[0]
 
 
-def cpu_baseline(args, wl, matvecs_per_solve):
+def cpu_baseline(args, wl, min_s=10.0):
+    """Full fp64 single-right-hand-side solves of the CPU port (oracle/) on
+    the full workload, on all host threads (FFTs), until about min_s seconds
+    of CPU work: solves/s = solves / time."""
     threads = os.cpu_count() or 1
-    t, n = cpu_matvec_sample(threads, wl)
-    v = 1.0 / (t * matvecs_per_solve)
-    return {"value": round(v, 5), "unit": "solves/s", "cores": threads, "kind": "port",
-            "sample": f"{n} fp64 matvecs of the CPU port (oracle/) on the full workload, mean {t:.2f} s each, "
-                      f"FFT on {threads} threads; solves/s = 1/(t x {matvecs_per_solve:g} matvecs per plain fp64 solve)"}
+    op = _cpu_operator(wl, threads)
+    B, X0, S = problem_arrays(wl)
+    ts, mvs = [], []
+    while not ts or (sum(ts) < min_s and len(ts) < wl.M):
+        t, n = cpu_solve(op, wl, B, X0, S, len(ts))
+        ts.append(t)
+        mvs.append(n)
+    return {"value": round(len(ts) / sum(ts), 5), "unit": "solves/s", "cores": threads, "kind": "port",
+            "sample": f"{len(ts)} full fp64 GMRES({wl.restart})+Jacobi solves (columns 0..{len(ts) - 1}) of the CPU "
+                      f"port (oracle/) on the full workload, {np.mean(ts):.2f} s and {np.mean(mvs):.1f} matvecs "
+                      f"each, FFTs on {threads} threads"}
 
 
 def run_reference(args, rank):
-    """CPU port of the reference operator on the host cores (rank 0 only)."""
+    """CPU port of the reference solve on the host cores (rank 0 only): each
+    timed step is one full fp64 single-right-hand-side GMRES solve (column
+    step mod M of the workload); warm-up steps are one operator application
+    each."""
     if rank != 0:
         return
     threads = os.cpu_count() or 1
     wl = Workload(args.workload)
-    per_solve = PLAIN_MATVECS_PER_SOLVE[args.workload]
-    # warm-up matvecs untimed, then one timed matvec per step
-    cpu_matvec_sample(threads, wl, min_s=0.0, max_n=max(1, args.warmup))
-    ts = []
-    for _ in range(max(1, args.steps)):
-        t, _n = cpu_matvec_sample(threads, wl, min_s=0.0, max_n=1)
+    op = _cpu_operator(wl, threads)
+    B, X0, S = problem_arrays(wl)
+    for _ in range(max(1, args.warmup)):
+        op.apply(X0[:, 0], S[:, 0])
+    ts, mvs = [], []
+    for k in range(max(1, args.steps)):
+        t, n = cpu_solve(op, wl, B, X0, S, k % wl.M)
         ts.append(t)
+        mvs.append(n)
     t = float(np.median(ts))
-    v = 1.0 / (t * per_solve)
+    v = 1.0 / t
     line = {
         "impl": "reference",
         "metric": METRICS[wl.name],
@@ -586,11 +823,11 @@ def run_reference(args, rank):
         "ms_per_step": round(t * 1e3, 1), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "c128", "data": DATA[wl.name],
         "config": {"workload": wl.label,
-                   "step": "one fp64 matvec of the CPU port of the reference operator (bounded sample), "
-                           "the same operator and sizes as the GPU arm's workload"},
+                   "step": f"one full fp64 GMRES({wl.restart})+Jacobi solve of one right-hand side (column step mod "
+                           f"{wl.M}) with the CPU port of the reference algorithm, stop rule |D^-1 r| < tol |b|; "
+                           f"{np.mean(mvs):.1f} matvecs per solve"},
         "cpu_baseline": {"value": round(v, 5), "unit": "solves/s", "cores": threads, "kind": "port",
-                         "sample": f"1 fp64 matvec per step, median {t:.2f} s; solves/s = 1/(t x "
-                                   f"{per_solve:g} matvecs per plain fp64 solve)"},
+                         "sample": f"{len(ts)} full solves, median {t:.2f} s each, FFTs on {threads} threads"},
         "e2e": {"value": round(v, 5), "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -602,15 +839,25 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--method", default="gmres", choices=["gmres", "bicgstab"])
     ap.add_argument("--inner-tol", type=float, default=1e-4, help="floor of one inner solve's reduction")
     ap.add_argument("--no-compact", action="store_true", help="idle columns still go through the operator")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-profile", action="store_true", help="skip the stage-timer pass")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain per-system fp64 leg")
-    ap.add_argument("--workload", default="monolayer", choices=["monolayer", "poly3d"],
-                    help="monolayer: the headline N=4000 case; poly3d: the N=1000 polydisperse 192-RHS case")
+    ap.add_argument("--no-accuracy", action="store_true", help="skip the per-dipole fp64 comparison")
+    ap.add_argument("--no-extras", action="store_true", help="skip the other workloads")
+    ap.add_argument("--no-reference-gpu", action="store_true", help="skip the reference build's GPU solve")
+    ap.add_argument("--workload", default="monolayer", choices=["monolayer", "poly3d", "c1"],
+                    help="monolayer: the headline N=4000 case; poly3d: the N=1000 polydisperse 192-RHS case; "
+                         "c1: the N=500 single-RHS case")
+    ap.add_argument("--_reference-gpu-child", dest="ref_child", action="store_true", help=argparse.SUPPRESS)
+    ap.add_argument("--ref-out", default=None, help=argparse.SUPPRESS)
     args = ap.parse_args()
+    if args.ref_child:
+        reference_gpu_child(args)
+        return
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))

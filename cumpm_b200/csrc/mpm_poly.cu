@@ -609,12 +609,6 @@ __global__ void __launch_bounds__(128) k_poly_quad_contract(const cplx<R>* __res
 // ------------------------------------------------------------------ host
 
 void Field::poly_init() {
-    // The quadrupole path below (point-Gaussian grids, joint scale, G
-    // contraction, joint pair and self terms) stays closed until its parity
-    // with the oracle has been checked on a GPU.
-    if (spec_.quads)
-        throw std::runtime_error("polydisperse quadrupoles are not enabled in this build (device path not yet "
-                                 "checked on a GPU)");
     if (spec_.quads && !spec_.solver_ax)
         throw std::runtime_error("polydisperse quadrupoles are computed at the particles (SOLVER_AX) only");
     pgeom_ = make_poly_geom(spec_.box, spec_.errortol, spec_.xi, spec_.radius);

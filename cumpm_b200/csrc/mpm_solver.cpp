@@ -279,8 +279,6 @@ void DipoleSolver::compute(const std::vector<double>& x, const std::vector<doubl
             else if (field_type_ == "monodisperse") poly = false;
             else if (field_type_ == "auto") poly = !all_equal(radius_);
             else throw std::runtime_error("Unknown field_type: " + field_type_);
-            if (poly && solve_quads_)
-                throw std::runtime_error("polydisperse quadrupoles are not available in this build");
             fs.kind = poly ? FIELD_POLY : FIELD_MONO;
             if (poly) fs.radius = radius_;
         }

@@ -67,8 +67,6 @@ class _Field:
         self._solve_quads = bool(solve_quadrupoles)
         self._quad_idxs = [int(i) for i in (quad_idxs or [])]
         self._prec = _parse_precision(precision)
-        if self._solve_quads and kind == capi.FIELD_POLY:
-            raise RuntimeError("polydisperse quadrupoles are not available in this build")
         self._pos = np.zeros((0, 3))
         self._fpts = None
         self._dip = None

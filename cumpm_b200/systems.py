@@ -15,6 +15,7 @@ assignment without communicating.
 from __future__ import annotations
 
 import math
+import os
 from dataclasses import dataclass, field
 from typing import Callable, Dict, List, Optional, Sequence
 
@@ -81,30 +82,74 @@ def solve_one(system: System) -> Dict[str, np.ndarray]:
     return out
 
 
+def local_device_ordinal(rank: int, env=None, device_count: Optional[int] = None) -> int:
+    """The GPU a rank binds to: LOCAL_RANK when the launcher sets it
+    (torchrun does), else the rank modulo the visible device count."""
+    env = os.environ if env is None else env
+    if "LOCAL_RANK" in env:
+        return int(env["LOCAL_RANK"])
+    if device_count is None:
+        import torch
+
+        device_count = torch.cuda.device_count()
+    return rank % max(1, int(device_count))
+
+
+def _bind_device(ordinal: int) -> None:
+    import torch
+
+    if torch.cuda.is_available():
+        torch.cuda.set_device(ordinal)
+
+
+class SystemSolveError(RuntimeError):
+    """One or more systems failed on some rank; raised on every rank after
+    the results have been exchanged, so no rank is left waiting."""
+
+
 def solve_systems(systems: Sequence[System], *, dist=None,
-                  solve_fn: Callable[[System], Dict[str, np.ndarray]] = solve_one) -> List[Dict[str, np.ndarray]]:
+                  solve_fn: Callable[[System], Dict[str, np.ndarray]] = solve_one,
+                  bind_device: Optional[Callable[[int], None]] = _bind_device) -> List[Dict[str, np.ndarray]]:
     """Solve every system once across the ranks of ``dist`` (an initialised
     ``torch.distributed``, or None for one process) and return all results,
     in system order, on every rank.
 
-    Each rank solves its own share (:func:`partition`); the only exchange is
-    one ``all_gather_object`` of the results at the end, which every rank
-    joins, whether its share is empty or not.
+    Each rank first binds its own GPU (``local_device_ordinal``; pass
+    ``bind_device=None`` when the caller has done so), then solves its
+    share (:func:`partition`); the only exchange is one
+    ``all_gather_object`` of the results at the end, which every rank joins,
+    whether its share is empty or not and whether its solves succeeded or
+    not.  A solve that raises is caught and its message travels in the
+    gather; afterwards every rank raises :class:`SystemSolveError` naming the
+    failed systems.
     """
     sizes = [s.num_particles for s in systems]
     if dist is None or not dist.is_initialized():
         return [solve_fn(s) for s in systems]
     rank, world = dist.get_rank(), dist.get_world_size()
+    if bind_device is not None:
+        bind_device(local_device_ordinal(rank))
     mine = partition(sizes, world)[rank]
-    local = [(i, solve_fn(systems[i])) for i in mine]
+    local = []
+    for i in mine:
+        try:
+            local.append((i, True, solve_fn(systems[i])))
+        except Exception as e:  # reported on every rank after the gather
+            local.append((i, False, f"rank {rank}: {type(e).__name__}: {e}"))
     gathered: List[object] = [None] * world
     dist.all_gather_object(gathered, local)
     out: List[Optional[Dict[str, np.ndarray]]] = [None] * len(systems)
+    errors = []
     for part in gathered:
-        for i, res in part:
+        for i, ok, res in part:
+            if not ok:
+                errors.append(f"system {i} ({res})")
+                continue
             if out[i] is not None:
                 raise RuntimeError(f"system {i} solved on two ranks")
             out[i] = res
+    if errors:
+        raise SystemSolveError("; ".join(errors))
     missing = [i for i, r in enumerate(out) if r is None]
     if missing:
         raise RuntimeError(f"systems {missing} were not solved")

@@ -16,11 +16,16 @@ def pytest_configure(config):
 
 
 def pytest_collection_modifyitems(config, items):
-    """Tests of paths that have not run on a GPU yet go last (stable order
-    otherwise), so that under -x a failure among them leaves every
-    established test already run."""
-    items[:] = ([it for it in items if it.get_closest_marker("first_gpu_run") is None]
-                + [it for it in items if it.get_closest_marker("first_gpu_run") is not None])
+    """Tests of paths that have not run on a GPU yet go after the established
+    ones (stable order otherwise), so that under -x a failure among them
+    leaves every established test already run; the allocation-free entry
+    point's file (test_zz_no_alloc.py) stays the very last."""
+    def rank(it):
+        if os.path.basename(str(it.fspath)) == "test_zz_no_alloc.py":
+            return 2
+        return 1 if it.get_closest_marker("first_gpu_run") is not None else 0
+
+    items[:] = sorted(items, key=rank)
 
 
 @pytest.fixture

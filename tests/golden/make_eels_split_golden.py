@@ -5,7 +5,7 @@ the particles near the beam, from the reference's own Python
 :261-320).  Its compiled module is replaced by a stub that only carries the
 precision enum, which the splitting code never calls into.
 
-Usage: python tests/golden/make_eels_split_golden.py [/path/to/reference]
+Usage: python tests/golden/make_eels_split_golden.py <reference source tree>
 """
 import importlib.util
 import os
@@ -15,7 +15,9 @@ import types
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+if len(sys.argv) != 2:
+    sys.exit(f"usage: python {os.path.relpath(__file__)} <reference source tree>")
+REF = sys.argv[1]
 
 METHODS = ("cubic", "fibonacci", "fcc")
 NSPLIT = (8, 27, 50, 100)

@@ -16,7 +16,7 @@ the tests need).
   that reads it (tests/test_eels_solver.py:114-173): loss spectra of two
   beam positions at five frequencies and the scaled dipoles.
 
-Usage: python tests/golden/make_golden.py [/path/to/reference]
+Usage: python tests/golden/make_golden.py <reference source tree>
 """
 import os
 import sys
@@ -24,7 +24,9 @@ import sys
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+if len(sys.argv) != 2:
+    sys.exit(f"usage: python {os.path.relpath(__file__)} <reference source tree>")
+REF = sys.argv[1]
 
 
 def drude(omega, gamma, omega_p, eps_inf):

@@ -35,8 +35,6 @@ def test_inputs_and_sizes():
 def test_named_gaps():
     from cumpm_b200 import dev
 
-    with pytest.raises(RuntimeError, match="polydisperse quadrupoles"):
-        dev.PolydisperseEwaldElectricField(20.0, 20.0, 20.0, 1e-6, 0.5, True, [1.0, 1.2], solve_quadrupoles=True)
     ef = dev.PolydisperseEwaldElectricField(20.0, 20.0, 20.0, 1e-6, 0.5, True, [1.0, 1.2])
     with pytest.raises(RuntimeError, match="Bloch"):
         ef.set_bloch_wavevector(0.1, 0.0)

@@ -5,7 +5,7 @@ import pytest
 
 from oracle import mpm_eels as E
 
-pytestmark = [pytest.mark.gpu, pytest.mark.first_gpu_run]
+pytestmark = pytest.mark.gpu
 
 
 def test_reference_golden_two_beams_five_frequencies(golden):

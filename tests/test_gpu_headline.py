@@ -1,0 +1,176 @@
+"""Parity at the benchmark configurations themselves, not only at small sizes.
+
+* The N=4000 hexagonal monolayer (box 1542.0 x 332.6 x 1000 nm, 366x80x238
+  grid stored as 9 occupied z planes, support 9) applied to M=30 right-hand
+  sides -- the batch the benchmark solves -- in fp64, against the oracle
+  column by column, and three columns against the reference build's
+  monodisperse field (PrecisionMode.DOUBLE); the fp32 reciprocal space of
+  the same batch against the same oracle columns.  M=30 puts 90 grid
+  columns per voxel through the multi-chunk spread (32-column fp32 / 16-column
+  fp64 chunks), the M=30 Toeplitz column kernel and the contraction.
+* The N=1000 polydisperse packing (radii U[1,4] nm, 108^3 scalar grid,
+  support 12) with M=192, a quarter of the columns against the oracle and
+  two against the reference build's polydisperse field.
+* The batched mixed-precision solve of the 30 monolayer right-hand sides
+  (fp32 operator inside fp64 refinement, true residual 1e-6) against an
+  fp64 solve of the same system to 1e-11: every dipole within 1e-6 of it.
+"""
+import glob
+import os
+import sys
+
+import numpy as np
+import pytest
+
+import bench
+from oracle import mpm_oracle as O
+
+pytestmark = pytest.mark.gpu
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+REF_DIR = os.path.join(ROOT, "oracle", "_ref")
+THREADS = os.cpu_count() or 1
+
+
+def _ref_module():
+    if not glob.glob(os.path.join(REF_DIR, "_cuMPM*.so")):
+        return None
+    sys.path.insert(0, REF_DIR)
+    try:
+        import _cuMPM as R
+    finally:
+        sys.path.remove(REF_DIR)
+    return R
+
+
+def _inputs(seed, rows, N, M):
+    rng = np.random.default_rng(seed)
+    X = rng.standard_normal((rows, M)) + 1j * rng.standard_normal((rows, M))
+    sc = rng.standard_normal((N, M)) + 1j * rng.standard_normal((N, M))
+    return X, sc
+
+
+def _gpu(F, X, sc, **kw):
+    import torch
+    return F.apply(torch.tensor(X, device="cuda"), self_coef=torch.tensor(sc, device="cuda"), **kw).cpu().numpy()
+
+
+def _colrel(a, b):
+    return float(np.max(np.abs(a - b)) / np.max(np.abs(b)))
+
+
+@pytest.fixture(scope="module")
+def monolayer():
+    from cumpm_b200 import capi
+    wl = bench.Workload("monolayer")
+    F = wl.field(capi)
+    F.set_positions(wl.pos)
+    return wl, F
+
+
+def test_monolayer_operator_m30_matches_oracle(monolayer):
+    wl, F = monolayer
+    info = F.info()
+    assert info["grid"] == [366, 80, 238] and info["pruned"] == 1 and info["z_slots"] == 9
+    N, M = len(wl.pos), 30
+    X, sc = _inputs(40, 3 * N, N, M)
+    Y64 = _gpu(F, X, sc)
+    Y32 = _gpu(F, X, sc, recip_fp32=True, real_fp32=True)
+    op = O.MonoEwaldOperator(wl.box, bench.TOL, bench.XI, True, fft_workers=THREADS)
+    op.set_positions(wl.pos)
+    worst64 = worst32 = 0.0
+    for m in range(M):
+        ref = op.apply(X[:, m], sc[:, m])
+        worst64 = max(worst64, _colrel(Y64[:, m], ref))
+        worst32 = max(worst32, _colrel(Y32[:, m], ref))
+    assert worst64 < 1e-12, worst64
+    assert worst32 < 2e-6, worst32
+
+
+def test_monolayer_operator_matches_reference_build(monolayer):
+    R = _ref_module()
+    if R is None:
+        pytest.skip("reference build oracle/_ref not present")
+    wl, F = monolayer
+    N, M = len(wl.pos), 3
+    X, sc = _inputs(41, 3 * N, N, M)
+    Y = _gpu(F, X, sc)
+    pos = wl.pos
+    for m in range(M):
+        ef = R.Monodisperse_Ewald_Electric_Field(wl.box[0], wl.box[1], wl.box[2], bench.TOL, bench.XI,
+                                                 R.FieldCalcMode.SOLVER_AX, 1.0, False, [], R.PrecisionMode.DOUBLE)
+        ef.updateParticleCoordinates(*[list(pos[:, d]) for d in range(3)])
+        P = X[:, m].reshape(N, 3)
+        ef.updateDipolesComplex(*[list(f(P[:, d])) for d in range(3) for f in (np.real, np.imag)])
+        ef.setSelfCoef(list(sc[:, m].real), list(sc[:, m].imag))
+        ef.calculate()
+        E_ref = np.ravel(np.asarray(ef.getEPointHost()))
+        np.testing.assert_allclose(Y[:, m], E_ref, rtol=1e-10, atol=1e-11 * np.abs(E_ref).max())
+
+
+@pytest.fixture(scope="module")
+def poly3d():
+    from cumpm_b200 import capi
+    wl = bench.Workload("poly3d")
+    F = wl.field(capi)
+    F.set_positions(wl.pos)
+    return wl, F
+
+
+def test_poly3d_operator_m192_matches_oracle(poly3d):
+    wl, F = poly3d
+    info = F.info()
+    assert info["grid"] == [108, 108, 108]
+    N, M = len(wl.pos), 192
+    X, sc = _inputs(42, 3 * N, N, M)
+    Y64 = _gpu(F, X, sc)
+    Y32 = _gpu(F, X, sc, recip_fp32=True, real_fp32=True)
+    op = O.PolyEwaldOperator(wl.box, bench.TOL, bench.XI, wl.radius, True)
+    op.set_positions(wl.pos)
+    worst64 = worst32 = 0.0
+    for m in range(0, M, 4):
+        ref = op.apply(X[:, m], sc[:, m])
+        worst64 = max(worst64, _colrel(Y64[:, m], ref))
+        worst32 = max(worst32, _colrel(Y32[:, m], ref))
+    assert worst64 < 1e-11, worst64
+    assert worst32 < 5e-6, worst32
+
+
+def test_poly3d_operator_matches_reference_build(poly3d):
+    R = _ref_module()
+    if R is None:
+        pytest.skip("reference build oracle/_ref not present")
+    wl, F = poly3d
+    N, M = len(wl.pos), 2
+    X, sc = _inputs(43, 3 * N, N, M)
+    Y = _gpu(F, X, sc)
+    pos = wl.pos
+    for m in range(M):
+        ef = R.Polydisperse_Ewald_Electric_Field(wl.box[0], wl.box[1], wl.box[2], bench.TOL, bench.XI,
+                                                 R.FieldCalcMode.SOLVER_AX, list(map(float, wl.radius)), False, [],
+                                                 R.PrecisionMode.DOUBLE)
+        ef.updateParticleCoordinates(*[list(pos[:, d]) for d in range(3)])
+        P = X[:, m].reshape(N, 3)
+        ef.updateDipolesComplex(*[list(f(P[:, d])) for d in range(3) for f in (np.real, np.imag)])
+        ef.setSelfCoef(list(sc[:, m].real), list(sc[:, m].imag))
+        ef.calculate()
+        E_ref = np.ravel(np.asarray(ef.getEPointHost()))
+        np.testing.assert_allclose(Y[:, m], E_ref, rtol=1e-9, atol=1e-10 * np.abs(E_ref).max())
+
+
+def test_monolayer_batched_mixed_solve_every_dipole_within_1e6_of_fp64(monolayer):
+    """The benchmark's solve: every dipole of the 30 right-hand sides within
+    1e-6 (relative to that dipole) of the fp64 solution of the same system."""
+    import torch
+    from cumpm_b200 import capi
+    wl, F = monolayer
+    B, X0, S = bench.device_problem(wl, torch, torch.device("cuda"))
+    X = X0.clone()
+    rep = F.batch_solve(B, X, S, tol=bench.TOL, method=capi.METHOD_GMRES, restart=50, refine=True, inner_tol=1e-4)
+    assert rep["num_converged"] == B.shape[1]
+    Xref = bench.fp64_reference_solution(F, B, X0, S, capi)
+    err = bench.dipole_errors(X, Xref, len(wl.pos))
+    assert err["max_dipole_rel_err"] <= 1e-6, err
+    R = B - F.apply(X, self_coef=S)
+    rel = (torch.linalg.vector_norm(R, dim=0) / torch.linalg.vector_norm(B, dim=0)).max().item()
+    assert rel <= bench.TOL, rel

@@ -5,7 +5,7 @@ import pytest
 
 from oracle import mpm_oracle as O
 
-pytestmark = [pytest.mark.gpu, pytest.mark.first_gpu_run]
+pytestmark = pytest.mark.gpu
 
 
 @pytest.mark.parametrize("field_type", ["auto", "polydisperse"])

@@ -2,9 +2,10 @@
 itself (oracle/_ref, the reference's Polydisperse_Ewald_Electric_Field with
 quadrupoles, run on the GPU).  This pins the oracle's restatement of the
 polydisperse quadrupole tables, the point-Gaussian grids, the joint scale and
-the spread of quadrupole q on particle q's stencil.  Skipped when the
-reference build is not present.  Marked first_gpu_run: collected after every
-other test, so a mismatch here leaves the rest already run."""
+the spread of quadrupole q on particle q's stencil; the device field is
+compared with the same reference field directly (first run of that device
+path: marked first_gpu_run).  Skipped when the
+reference build is not present."""
 import glob
 import os
 import sys
@@ -59,6 +60,15 @@ def test_polydisperse_quadrupole_field_vs_reference(ref, radii, qi):
     E_ref = _flat(ef.getEPointHost())
     op = O.PolyEwaldOperator(box, 1e-6, 0.5, radii, True, qi)
     op.set_positions(pos)
-    E = op.apply(np.concatenate([P.ravel(), Q.ravel()]), sc)
+    X = np.concatenate([P.ravel(), Q.ravel()])
+    E = op.apply(X, sc)
     assert E_ref.shape == E.shape
     np.testing.assert_allclose(E, E_ref, rtol=1e-8, atol=1e-9 * np.abs(E_ref).max())
+    # the device operator against the reference build
+    import torch
+    from cumpm_b200 import capi
+    F = capi.Field(capi.FIELD_POLY, box, 1e-6, 0.5, radius=radii, quad_idxs=qi, solve_quads=True)
+    F.set_positions(pos)
+    Y = F.apply(torch.tensor(X.reshape(-1, 1), device="cuda"),
+                self_coef=torch.tensor(sc.reshape(-1, 1), device="cuda")).cpu().numpy()[:, 0]
+    np.testing.assert_allclose(Y, E_ref, rtol=1e-8, atol=1e-9 * np.abs(E_ref).max())

@@ -3,7 +3,7 @@ by system, what a dipole_solver of each gives on its own."""
 import numpy as np
 import pytest
 
-pytestmark = [pytest.mark.gpu, pytest.mark.first_gpu_run]
+pytestmark = pytest.mark.gpu
 
 
 def _packing(rng, n, box, a):

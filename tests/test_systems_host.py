@@ -118,6 +118,62 @@ def test_gloo_ranks_share_the_systems_and_gather_once(world):
         assert solved == [sizes[i] for i in parts[r]]   # each rank solved its own share only
 
 
+def _rank_fail(rank, world, port, q):
+    """Rank 1's solve of its first system raises; every rank must come back
+    from the gather and raise the same error (none waits forever)."""
+    sys.path.insert(0, ROOT)
+    from cumpm_b200 import systems as S2
+
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), LOCAL_RANK=str(rank))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    bound = []
+    try:
+        calls = []
+
+        def solve(system):
+            calls.append(system.num_particles)
+            if rank == 1 and len(calls) == 1:
+                raise ValueError("injected failure")
+            return _fake_solve(system)
+
+        try:
+            S2.solve_systems(_systems(), dist=dist, solve_fn=solve, bind_device=bound.append)
+            q.put((rank, "no error", bound))
+        except S2.SystemSolveError as e:
+            q.put((rank, str(e), bound))
+        dist.barrier()
+    finally:
+        dist.destroy_process_group()
+
+
+def test_a_failing_solve_raises_on_every_rank_without_a_hang():
+    world = 3
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = 29950 + (os.getpid() % 40)
+    procs = [ctx.Process(target=_rank_fail, args=(r, world, port, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    out = {}
+    for _ in range(world):
+        r, msg, bound = q.get(timeout=120)
+        out[r] = (msg, bound)
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    first_of_rank1 = S.partition([s.num_particles for s in _systems()], world)[1][0]
+    for r in range(world):
+        msg, bound = out[r]
+        assert f"system {first_of_rank1} (rank 1: ValueError: injected failure)" == msg
+        assert bound == [r]   # each rank bound the GPU of its LOCAL_RANK before solving
+
+
+def test_local_device_ordinal():
+    assert S.local_device_ordinal(5, env={"LOCAL_RANK": "1"}) == 1
+    assert S.local_device_ordinal(5, env={}, device_count=4) == 1
+    assert S.local_device_ordinal(3, env={}, device_count=0) == 0
+
+
 def test_solve_one_calls_dipole_solver_with_its_own_arguments(monkeypatch):
     """solve_one's call binds to the real dipole_solver signature and reads
     back the three results (quadrupoles only when asked for)."""
