@@ -298,6 +298,7 @@ int mpm_field_info_get(const mpm_field* f, mpm_field_info* info) {
         info->num_pairs = st.num_pairs;
         info->rc = g.rc;
         info->selfo = F.selfo();
+        info->slab_fused = st.slab_fused;
     });
 }
 

@@ -677,6 +677,195 @@ void launch2_cw(int cls, int nblocks, int nthreads, size_t shm, cudaStream_t s, 
 }
 
 // ---------------------------------------------------------------------------
+// The z-slab k-space step fused with the y transforms (AxisFFT::run_slab).
+//
+// One CTA owns one kx plane and MC right-hand sides: the tile
+// S[y][col], col = (z * 3 + c) * MC + mi, NCOL = Zs * 3 * MC columns of
+// n = Ny points, lives in shared memory for the whole step.  The y
+// transforms are the two-pass (r1, r2) split of k_fft2, run in place: the
+// butterflies of a round cover whole columns, every thread reads its
+// butterfly's inputs into registers, the block synchronises, then writes
+// (the next round's columns are disjoint, so one barrier per round).
+// Between the transforms, thread (ky, mi) reads the 3 x Zs values of its
+// (kx, ky, mi) column, synchronises and writes the Green-tensor product
+// back (four Toeplitz products of Zs x Zs).
+
+template <typename R> __host__ __device__ constexpr int slab_mc() { return sizeof(R) == 8 ? 2 : 4; }
+template <typename R> __host__ __device__ constexpr int slab_threads() { return sizeof(R) == 8 ? 160 : 320; }
+
+struct SlabArgs {
+    int Nx, Zs, M, nchunk;
+    double kxu, kyu;
+};
+
+// one in-place radix pass over all NCOL columns: butterfly j < nb of radix
+// RAD reads elements (j + q nb) (twiddled by W_n^(q j) when TW), writes
+// (j RAD + p) for pass 1 or (p nb' + j) for pass 2 -- see the callers
+template <typename R, bool INV, int RAD, int NT, bool PASS2>
+__device__ __forceinline__ void slab_pass(cplx<R>* __restrict__ S, const cplx<R>* __restrict__ T, int n, int NCOL) {
+    const int nb = n / RAD;            // butterflies per column
+    const int cpr = NT / nb;           // columns per round
+    const int rounds = (NCOL + cpr - 1) / cpr;
+    const int cl = threadIdx.x % cpr;
+    const int j = threadIdx.x / cpr;   // butterfly index; < nb for active threads
+    const bool act0 = j < nb;
+    for (int rd = 0; rd < rounds; ++rd) {
+        const int col = rd * cpr + cl;
+        const bool act = act0 && col < NCOL;
+        cplx<R> x[RAD];
+        if (act) {
+            if constexpr (!PASS2) {
+                // radix r1, butterfly j < r2 reads x[j + q r2]
+#pragma unroll
+                for (int q = 0; q < RAD; ++q) x[q] = S[(j + q * nb) * NCOL + col];
+            } else {
+                // radix r2, butterfly j < r1 reads S[j + q r1] W_n^(q j)
+                x[0] = S[j * NCOL + col];
+#pragma unroll
+                for (int q = 1; q < RAD; ++q) {
+                    cplx<R> w = T[q * j];
+                    if (INV) w.y = -w.y;
+                    x[q] = S[(j + q * nb) * NCOL + col] * w;
+                }
+            }
+            dft_small<R, INV, RAD>(x);
+        }
+        __syncthreads();
+        if (act) {
+            if constexpr (!PASS2) {
+#pragma unroll
+                for (int p = 0; p < RAD; ++p) S[(j * RAD + p) * NCOL + col] = x[p];
+            } else {
+#pragma unroll
+                for (int p = 0; p < RAD; ++p) S[(p * nb + j) * NCOL + col] = x[p];
+            }
+        }
+    }
+    __syncthreads();
+}
+
+template <typename R, bool INV, int CLS, int NT>
+__device__ __forceinline__ void slab_ytransform(cplx<R>* S, const cplx<R>* T, int r1, int r2, int NCOL) {
+    const int n = r1 * r2;
+    radix_dispatch<CLS>(r1, [&](auto rc) { slab_pass<R, INV, decltype(rc)::value, NT, false>(S, T, n, NCOL); });
+    radix_dispatch<CLS>(r2, [&](auto rc) { slab_pass<R, INV, decltype(rc)::value, NT, true>(S, T, n, NCOL); });
+}
+
+template <typename R, int ZMAX, int CLS>
+__global__ void __launch_bounds__(slab_threads<R>()) k_slab(cplx<R>* __restrict__ data, const cplx<R>* __restrict__ tw,
+                                                            const cplx<R>* __restrict__ taps, int r1, int r2,
+                                                            SlabArgs a) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    constexpr int MC = slab_mc<R>();
+    constexpr int NT = slab_threads<R>();
+    const int n = r1 * r2;
+    const int Zs = a.Zs, M = a.M, B = 3 * M;
+    const int NCOL = Zs * 3 * MC;
+    cplx<R>* S = reinterpret_cast<cplx<R>*>(smem_raw);
+    cplx<R>* T = S + size_t(n) * NCOL;
+    // the right-hand-side chunks of one kx plane are adjacent in launch order
+    const int ix = blockIdx.x / a.nchunk;
+    const int m0 = (blockIdx.x - ix * a.nchunk) * MC;
+    const int mc = min(MC, M - m0);
+    cplx<R>* g = data + size_t(ix) * n * Zs * B;
+    const int tot = n * NCOL;
+    // tile element t = ((y Zs + z) 3 + c) MC + mi  <-  g[(y Zs + z) B + c M + m0 + mi]
+    for (int t = threadIdx.x; t < tot; t += NT) {
+        const int mi = t % MC;
+        const int r = t / MC;
+        const bool live = mi < mc;
+        const cplx<R>* src = live ? g + size_t(r / 3) * B + (r % 3) * M + m0 + mi : data;
+        copy_async<R>(S + t, src, live);
+    }
+    for (int t = threadIdx.x; t < n; t += NT) T[t] = tw[t];
+    copy_async_wait();
+    __syncthreads();
+    slab_ytransform<R, false, CLS, NT>(S, T, r1, r2, NCOL);
+    // Green tensor per (ky, mi): a = kx E_x + ky E_y, E_z in registers
+    const double fx = (ix <= (a.Nx - 1) / 2) ? ix : ix - a.Nx;
+    const R kx = R(fx * a.kxu);
+    const int nd = 2 * Zs - 1;
+    const int ntask = n * MC;
+    for (int r0 = 0; r0 < ntask; r0 += NT) {
+        const int t = r0 + threadIdx.x;
+        const bool act = t < ntask;
+        const int ky_i = act ? t / MC : 0;
+        const int mi = t - ky_i * MC;
+        cplx<R> av[ZMAX], zv[ZMAX];
+        R ky = R(0);
+        if (act) {
+            const double fy = (ky_i <= (n - 1) / 2) ? ky_i : ky_i - n;
+            ky = R(fy * a.kyu);
+            const cplx<R>* b = S + size_t(ky_i) * NCOL + mi;
+#pragma unroll
+            for (int z = 0; z < ZMAX; ++z) {
+                if (z < Zs) {
+                    const cplx<R> ex = b[(z * 3 + 0) * MC], ey = b[(z * 3 + 1) * MC];
+                    av[z] = ex * kx + ey * ky;
+                    zv[z] = b[(z * 3 + 2) * MC];
+                } else {
+                    av[z] = mk<R>(R(0), R(0));
+                    zv[z] = mk<R>(R(0), R(0));
+                }
+            }
+        }
+        __syncthreads();
+        if (act) {
+            const cplx<R>* tp = taps + (size_t(ix) * n + ky_i) * 3 * nd + (Zs - 1);   // tp[k nd + d]
+            cplx<R>* b = S + size_t(ky_i) * NCOL + mi;
+            // u = t0 * a + t1 * E_z  ->  E_x = kx u, E_y = ky u;  then E_z = t1 * a + t2 * E_z
+#pragma unroll
+            for (int part = 0; part < 2; ++part) {
+                const cplx<R>* ta = tp + part * nd;         // t0 | t1 on a
+                const cplx<R>* tb = tp + (part + 1) * nd;   // t1 | t2 on E_z
+                cplx<R> acc[ZMAX];
+#pragma unroll
+                for (int zo = 0; zo < ZMAX; ++zo) acc[zo] = mk<R>(R(0), R(0));
+#pragma unroll
+                for (int d = -(ZMAX - 1); d <= ZMAX - 1; ++d) {
+                    if (d < -(Zs - 1) || d > Zs - 1) continue;
+                    const cplx<R> ka = ta[d], kb = tb[d];
+#pragma unroll
+                    for (int zo = 0; zo < ZMAX; ++zo) {
+                        const int zi = zo - d;
+                        if (zi >= 0 && zi < ZMAX) {
+                            acc[zo].x = fma(ka.x, av[zi].x, acc[zo].x);
+                            acc[zo].x = fma(-ka.y, av[zi].y, acc[zo].x);
+                            acc[zo].y = fma(ka.x, av[zi].y, acc[zo].y);
+                            acc[zo].y = fma(ka.y, av[zi].x, acc[zo].y);
+                            acc[zo].x = fma(kb.x, zv[zi].x, acc[zo].x);
+                            acc[zo].x = fma(-kb.y, zv[zi].y, acc[zo].x);
+                            acc[zo].y = fma(kb.x, zv[zi].y, acc[zo].y);
+                            acc[zo].y = fma(kb.y, zv[zi].x, acc[zo].y);
+                        }
+                    }
+                }
+#pragma unroll
+                for (int zo = 0; zo < ZMAX; ++zo) {
+                    if (zo < Zs) {
+                        if (part == 0) {
+                            b[(zo * 3 + 0) * MC] = acc[zo] * kx;
+                            b[(zo * 3 + 1) * MC] = acc[zo] * ky;
+                        } else {
+                            b[(zo * 3 + 2) * MC] = acc[zo];
+                        }
+                    }
+                }
+            }
+        }
+        __syncthreads();
+    }
+    slab_ytransform<R, true, CLS, NT>(S, T, r1, r2, NCOL);
+    for (int t = threadIdx.x; t < tot; t += NT) {
+        const int mi = t % MC;
+        if (mi < mc) {
+            const int r = t / MC;
+            g[size_t(r / 3) * B + (r % 3) * M + m0 + mi] = S[t];
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
 // Two-pass line transform for n = r1 * p, r1 an in-register radix and p an
 // odd prime above 16 (the monolayer x axis: 366 = 6 * 61).  Pass 1 (radix
 // r1, butterfly j1 < p) reads x[j1 + q p] straight from global memory and
@@ -1328,6 +1517,53 @@ void AxisFFT::run_scaled(cplx<R>* data, size_t es, int ncols, size_t os, int nou
     launch_line<R>(data, es, ncols, os, nouter, 2, scale, sz, sb, s);
 }
 
+bool AxisFFT::slab_ok(int Zs, bool fp64) const {
+    if (kind_ != 1 || force_general_ || Zs < 1 || Zs > 16) return false;
+    const int mc = fp64 ? slab_mc<double>() : slab_mc<float>();
+    const size_t elem = fp64 ? sizeof(double2) : sizeof(float2);
+    const size_t shm = (size_t(f_.n) * Zs * 3 * mc + f_.n) * elem;
+    // both passes need at least one column per round
+    const int nt = fp64 ? slab_threads<double>() : slab_threads<float>();
+    return shm <= kFftSmemBudget && nt >= std::max(r1_, r2_) && register_class(r1_) <= 16;
+}
+
+template <typename R>
+void AxisFFT::run_slab(cplx<R>* data, int nx, int Zs, int M, const cplx<R>* taps, double kxu, double kyu,
+                       cudaStream_t s) const {
+    if (!slab_ok(Zs, sizeof(R) == 8)) throw std::runtime_error("run_slab: slab not supported by this axis");
+    if (nx <= 0 || M <= 0) return;
+    constexpr int MC = slab_mc<R>();
+    constexpr int NT = slab_threads<R>();
+    const int n = f_.n;
+    const size_t shm = (size_t(n) * Zs * 3 * MC + n) * sizeof(cplx<R>);
+    SlabArgs a;
+    a.Nx = nx;
+    a.Zs = Zs;
+    a.M = M;
+    a.nchunk = (M + MC - 1) / MC;
+    a.kxu = kxu;
+    a.kyu = kyu;
+    const cplx<R>* tw = sizeof(R) == 4 ? reinterpret_cast<const cplx<R>*>(tw32_.p)
+                                       : reinterpret_cast<const cplx<R>*>(tw64_.p);
+    const int cls = register_class(r1_);
+    auto go = [&](auto kern) {
+        MPM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(shm)));
+        kern<<<nx * a.nchunk, NT, shm, s>>>(data, tw, taps, r1_, r2_, a);
+    };
+    if (Zs <= 9) {
+        if (cls == 8) go(k_slab<R, 9, 8>);
+        else if (cls == 12) go(k_slab<R, 9, 12>);
+        else go(k_slab<R, 9, 16>);
+    } else {
+        if (cls == 8) go(k_slab<R, 16, 8>);
+        else if (cls == 12) go(k_slab<R, 16, 12>);
+        else go(k_slab<R, 16, 16>);
+    }
+    MPM_LAUNCH();
+}
+
+template void AxisFFT::run_slab<float>(float2*, int, int, int, const float2*, double, double, cudaStream_t) const;
+template void AxisFFT::run_slab<double>(double2*, int, int, int, const double2*, double, double, cudaStream_t) const;
 template void AxisFFT::run<float>(float2*, size_t, int, size_t, int, bool, cudaStream_t) const;
 template void AxisFFT::run<double>(double2*, size_t, int, size_t, int, bool, cudaStream_t) const;
 template void AxisFFT::run_scaled<float>(float2*, size_t, int, size_t, int, const float*, int, int,

@@ -64,6 +64,26 @@ public:
     // the Rader split p - 1 = A * B (0 when the prime pass is streamed)
     int rader_a() const { return ra_; }
 
+    // The k-space step of the pruned (z-slab) monodisperse grid fused with
+    // this axis's transforms, for the y axis: data is the grid
+    // [x][y][slot][c][m] (Zs slots, 3 components, M right-hand sides), already
+    // transformed along x.  For every (kx, chunk of right-hand sides) one CTA
+    // loads its Ny x Zs x 3 x chunk values into shared memory, transforms
+    // along y, applies the slab Green tensor of every (kx, ky) column as
+    // three scalar Toeplitz kernels in z (taps [x][y][3][2 Zs - 1]:
+    // t_n(d) = sum_kz kz^n S(k) / |k|^2 exp(2 pi i kz d / Nz), n = 0, 1, 2),
+    //   a = kx E_x + ky E_y,  u = t0 * a + t1 * E_z,
+    //   E_x <- kx u,  E_y <- ky u,  E_z <- t1 * a + t2 * E_z,
+    // transforms back along y and stores: one HBM round trip for the y
+    // transforms and the Green tensor.  kxu, kyu: the wavenumber of one
+    // grid frequency along x and y (2 pi / L); nx: grid points along x.
+    template <typename R>
+    void run_slab(cplx<R>* data, int nx, int Zs, int M, const cplx<R>* taps, double kxu, double kyu,
+                  cudaStream_t s) const;
+    // whether run_slab handles this slab (two-pass in-register y transform,
+    // Zs <= 16 slots, tile within the shared-memory budget)
+    bool slab_ok(int Zs, bool fp64) const;
+
 private:
     template <typename R>
     void launch_line(cplx<R>* data, size_t es, int ncols, size_t os, int nouter, int mode, const R* scale, int sz,

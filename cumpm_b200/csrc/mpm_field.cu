@@ -615,6 +615,53 @@ __global__ void k_build_column(ScaleArgs a, int Z, double2* __restrict__ K64, fl
     }
 }
 
+// Pruned layout, fused path: the three scalar Toeplitz kernels of each
+// (kx, ky) column, t_n(d) = sum_kz exp(+2 pi i kz d / Nz) kz^n S(k) / |k|^2
+// (kz the signed wavenumber, zero at k = 0), d in [-(Z-1), Z-1], so that
+// K_ab(d) above is kx^2 t0, kx ky t0, kx t1, ky^2 t0, ky t1, t2 for
+// ab = xx, xy, xz, yy, yz, zz.  Computed in float64.
+__global__ void k_build_slab_taps(ScaleArgs a, int Z, double2* __restrict__ T64, float2* __restrict__ T32) {
+    extern __shared__ double sh[];
+    const int col = blockIdx.x;
+    const int ix = col / a.Ny, iy = col % a.Ny;
+    const int Nz = a.Nz;
+    double* C3 = sh;                 // [Nz][3]: S/|k|^2 times kz^0, kz^1, kz^2
+    double* tw = sh + 3 * Nz;        // [Nz][2] twiddles
+    const double V = double(a.Nx) * a.Ny * a.Nz;
+    for (int iz = threadIdx.x; iz < Nz; iz += blockDim.x) {
+        double o[4];
+        scale_coefs(ix, iy, iz, a.Nx, a.Ny, Nz, a.Lx, a.Ly, a.Lz, a.xi, a.eta, V, o);
+        const double fx = (ix <= (a.Nx - 1) / 2) ? ix : ix - a.Nx;
+        const double fy = (iy <= (a.Ny - 1) / 2) ? iy : iy - a.Ny;
+        const double fz = (iz <= (Nz - 1) / 2) ? iz : iz - Nz;
+        const double gx = fx * 2.0 * kPi / a.Lx, gy = fy * 2.0 * kPi / a.Ly, gz = fz * 2.0 * kPi / a.Lz;
+        const double k2 = gx * gx + gy * gy + gz * gz;
+        const double t = k2 < 1e-24 ? 0.0 : o[0] / k2;
+        C3[iz * 3 + 0] = t;
+        C3[iz * 3 + 1] = t * gz;
+        C3[iz * 3 + 2] = t * gz * gz;
+        double sn, cs;
+        sincospi(2.0 * iz / Nz, &sn, &cs);
+        tw[2 * iz] = cs; tw[2 * iz + 1] = sn;
+    }
+    __syncthreads();
+    const int nd = 2 * Z - 1;
+    for (int t = threadIdx.x; t < 3 * nd; t += blockDim.x) {
+        const int k = t / nd, di = t % nd;
+        const int d = di - (Z - 1);
+        double re = 0.0, im = 0.0;
+        for (int iz = 0; iz < Nz; ++iz) {
+            const int e = pmod(iz * d, Nz);
+            const double c = C3[iz * 3 + k];
+            re += c * tw[2 * e];
+            im += c * tw[2 * e + 1];
+        }
+        const size_t o = (size_t(col) * 3 + k) * nd + di;
+        T64[o] = make_double2(re, im);
+        T32[o] = make_float2(float(re), float(im));
+    }
+}
+
 // Pruned layout: out[zo][c'][m] = sum_{zi,c} K_{c'c}(zo - zi) in[zi][c][m]
 // on one (kx, ky) column per CTA, in place.  The column's Z x 3 inputs of a
 // right-hand side sit in registers; for each source component c the 2Z-1
@@ -1157,6 +1204,7 @@ FieldStats Field::stats() const {
     s.num_pairs = num_pairs_;
     for (int d = 0; d < 3; ++d) s.grid[d] = geom_.ng[d];
     s.stencil = gv_.S;
+    s.slab_fused = (spec_.kind == FIELD_MONO && use_slab()) ? 1 : 0;
     return s;
 }
 
@@ -1461,6 +1509,29 @@ void Field::build_column_kernel(cudaStream_t s) {
     colK_Z_ = Z;
 }
 
+bool Field::use_slab() const {
+    return gv_.pruned && own_fft_ && ffty_.slab_ok(gv_.Zs, true) && ffty_.slab_ok(gv_.Zs, false);
+}
+
+void Field::build_slab_taps(cudaStream_t s) {
+    const int Z = gv_.Zs;
+    const int ncol = gv_.Nx * gv_.Ny;
+    const int nd = 2 * Z - 1;
+    slabT64_.ensure(sizeof(double2) * size_t(ncol) * 3 * nd);
+    slabT32_.ensure(sizeof(float2) * size_t(ncol) * 3 * nd);
+    ScaleArgs a;
+    a.Nx = gv_.Nx; a.Ny = gv_.Ny; a.Nz = gv_.Nz;
+    a.Lx = spec_.box[0]; a.Ly = spec_.box[1]; a.Lz = spec_.box[2];
+    a.xi = spec_.xi;
+    for (int d = 0; d < 3; ++d) a.eta[d] = geom_.eta[d];
+    const size_t shm = sizeof(double) * 5 * gv_.Nz;
+    if (shm > 48 * 1024)
+        MPM_CUDA(cudaFuncSetAttribute(k_build_slab_taps, cudaFuncAttributeMaxDynamicSharedMemorySize, int(shm)));
+    k_build_slab_taps<<<ncol, 128, shm, s>>>(a, Z, slabT64_.as<double2>(), slabT32_.as<float2>());
+    MPM_LAUNCH();
+    slab_Z_ = Z;
+}
+
 void Field::precalc(cudaStream_t s) {
     if (!precalc_dirty_) return;
     StageScope scope(ST_PRECALC, s);
@@ -1476,7 +1547,9 @@ void Field::precalc(cudaStream_t s) {
         build_spread_plan(s);
         if (!spec_.solver_ax) build_stencil(targets_, s, false);  // SOLVER_AX: targets share the source stencil
         build_pairs(s);
-        if (gv_.pruned) {
+        if (use_slab()) {
+            if (slab_Z_ != gv_.Zs) build_slab_taps(s);
+        } else if (gv_.pruned) {
             if (colK_Z_ != gv_.Zs) build_column_kernel(s);
         } else if (scale_built_ != (Nq_ ? 4 : 1)) {
             build_scale(s);
@@ -1587,42 +1660,59 @@ void Field::recip_on(const double2* X, double2* Y, int M, cplx<R>* grid, cudaStr
     }
     MPM_LAUNCH();
     Profiler::get().end(ST_SPREAD, s);
-    // forward transform
-    Profiler::get().begin(ST_FFT_FWD, s);
-    transform<R>(grid, B, false, s);
-    Profiler::get().end(ST_FFT_FWD, s);
-    Profiler::get().begin(ST_KSPACE, s);
-    // k-space Green tensor
-    if (gv_.pruned) {
-        const int Z = gv_.Zs;
-        const int nd = 2 * Z - 1;
-        const size_t shm2 = sizeof(cplx<R>) * (size_t(Z) * B + 6 * nd);
-        const int thr = std::min(1024, ((B + 31) / 32) * 32);
-        const cplx<R>* K = sizeof(R) == 4 ? reinterpret_cast<const cplx<R>*>(colK32_.p)
-                                          : reinterpret_cast<const cplx<R>*>(colK64_.p);
-        auto go = [&](auto kern) {
-            MPM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(shm2)));
-            kern<<<gv_.Nx * gv_.Ny, thr, shm2, s>>>(grid, K, Z, M);
-        };
-        if (Z <= 9) go(k_column<R, 9>);
-        else if (Z <= 16) go(k_column<R, 16>);
-        else go(k_column<R, 24>);
-        MPM_LAUNCH();
+    if (use_slab()) {
+        // x forward; y forward, slab Green tensor and y inverse in one pass;
+        // x inverse (the axis transforms commute)
+        const size_t Bi = size_t(gv_.Zs) * B;
+        const cplx<R>* taps = sizeof(R) == 4 ? reinterpret_cast<const cplx<R>*>(slabT32_.p)
+                                             : reinterpret_cast<const cplx<R>*>(slabT64_.p);
+        Profiler::get().begin(ST_FFT_FWD, s);
+        fftx_.run<R>(grid, size_t(gv_.Ny) * Bi, int(Bi), Bi, gv_.Ny, false, s);
+        Profiler::get().end(ST_FFT_FWD, s);
+        Profiler::get().begin(ST_KSPACE, s);
+        ffty_.run_slab<R>(grid, gv_.Nx, gv_.Zs, M, taps, 2.0 * kPi / spec_.box[0], 2.0 * kPi / spec_.box[1], s);
+        Profiler::get().end(ST_KSPACE, s);
+        Profiler::get().begin(ST_FFT_INV, s);
+        fftx_.run<R>(grid, size_t(gv_.Ny) * Bi, int(Bi), Bi, gv_.Ny, true, s);
+        Profiler::get().end(ST_FFT_INV, s);
     } else {
-        const size_t V = size_t(gv_.Nx) * gv_.Ny * gv_.Zs;
-        const R* sc = sizeof(R) == 4 ? reinterpret_cast<const R*>(scale32_.p) : reinterpret_cast<const R*>(scale64_.p);
-        if (Nq_)
-            k_scale<R, true><<<nblk((long long)(V * M), 256), 256, 0, s>>>(grid, sc, gv_.Nx, gv_.Ny, gv_.Nz, spec_.box[0],
-                                                                           spec_.box[1], spec_.box[2], M);
-        else
-            k_scale<R, false><<<nblk((long long)(V * M), 256), 256, 0, s>>>(grid, sc, gv_.Nx, gv_.Ny, gv_.Nz, spec_.box[0],
-                                                                            spec_.box[1], spec_.box[2], M);
-        MPM_LAUNCH();
+        // forward transform
+        Profiler::get().begin(ST_FFT_FWD, s);
+        transform<R>(grid, B, false, s);
+        Profiler::get().end(ST_FFT_FWD, s);
+        Profiler::get().begin(ST_KSPACE, s);
+        // k-space Green tensor
+        if (gv_.pruned) {
+            const int Z = gv_.Zs;
+            const int nd = 2 * Z - 1;
+            const size_t shm2 = sizeof(cplx<R>) * (size_t(Z) * B + 6 * nd);
+            const int thr = std::min(1024, ((B + 31) / 32) * 32);
+            const cplx<R>* K = sizeof(R) == 4 ? reinterpret_cast<const cplx<R>*>(colK32_.p)
+                                              : reinterpret_cast<const cplx<R>*>(colK64_.p);
+            auto go = [&](auto kern) {
+                MPM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(shm2)));
+                kern<<<gv_.Nx * gv_.Ny, thr, shm2, s>>>(grid, K, Z, M);
+            };
+            if (Z <= 9) go(k_column<R, 9>);
+            else if (Z <= 16) go(k_column<R, 16>);
+            else go(k_column<R, 24>);
+            MPM_LAUNCH();
+        } else {
+            const size_t V = size_t(gv_.Nx) * gv_.Ny * gv_.Zs;
+            const R* sc = sizeof(R) == 4 ? reinterpret_cast<const R*>(scale32_.p) : reinterpret_cast<const R*>(scale64_.p);
+            if (Nq_)
+                k_scale<R, true><<<nblk((long long)(V * M), 256), 256, 0, s>>>(grid, sc, gv_.Nx, gv_.Ny, gv_.Nz, spec_.box[0],
+                                                                               spec_.box[1], spec_.box[2], M);
+            else
+                k_scale<R, false><<<nblk((long long)(V * M), 256), 256, 0, s>>>(grid, sc, gv_.Nx, gv_.Ny, gv_.Nz, spec_.box[0],
+                                                                                spec_.box[1], spec_.box[2], M);
+            MPM_LAUNCH();
+        }
+        Profiler::get().end(ST_KSPACE, s);
+        Profiler::get().begin(ST_FFT_INV, s);
+        transform<R>(grid, B, true, s);
+        Profiler::get().end(ST_FFT_INV, s);
     }
-    Profiler::get().end(ST_KSPACE, s);
-    Profiler::get().begin(ST_FFT_INV, s);
-    transform<R>(grid, B, true, s);
-    Profiler::get().end(ST_FFT_INV, s);
     StageScope scope(ST_CONTRACT, s);
     // contract
     const PointSet& tg = spec_.solver_ax ? sources_ : targets_;

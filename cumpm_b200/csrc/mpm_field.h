@@ -96,6 +96,7 @@ struct FieldStats {
     long long num_pairs = 0;
     int grid[3] = {0, 0, 0};
     int stencil = 0;
+    int slab_fused = 0;
 };
 
 class Field {
@@ -151,6 +152,8 @@ private:
     void build_pairs(cudaStream_t s);
     void choose_layout(cudaStream_t s);
     void build_column_kernel(cudaStream_t s);
+    void build_slab_taps(cudaStream_t s);
+    bool use_slab() const;   // pruned layout through AxisFFT::run_slab
     void build_scale(cudaStream_t s);
     cufftHandle plan_for(int B, bool fp32);  // B columns per voxel
     template <typename R> void recip(const double2* X, double2* Y, int M, cudaStream_t s);
@@ -191,7 +194,9 @@ private:
     // reciprocal space
     DevBuf grid_;                   // complex grid, sized for the largest use
     DevBuf scale64_, scale32_;      // full layout: per-voxel scale
-    DevBuf colK64_, colK32_;        // pruned layout: per-column Toeplitz kernels
+    DevBuf colK64_, colK32_;        // pruned layout: per-column Toeplitz kernels (unfused path)
+    DevBuf slabT64_, slabT32_;      // pruned layout: per-column scalar Toeplitz taps t0, t1, t2 (fused path)
+    int slab_Z_ = -1;
     // per-frame spread plan (monodisperse): per tile candidates, 1-D weights,
     // column contributor lists; plan_cap_ = 0 when the plan is not in use
     DevBuf plan_nc_, plan_cid_, plan_w64_, plan_w32_, plan_lw64_, plan_lw32_, plan_lc_, plan_ln_, plan_cnt_;

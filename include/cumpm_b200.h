@@ -98,6 +98,7 @@ typedef struct mpm_field_info {
     int z_slots;           /* stored z planes */
     long long num_pairs;   /* real-space (target, source) pairs */
     double rc, h[3], eta[3], selfo;
+    int slab_fused;        /* 1: pruned layout whose y transforms and k-space step run as one fused pass */
 } mpm_field_info;
 
 MPM_API const char* mpm_last_error(void);

@@ -62,6 +62,10 @@ def test_mono_solver_ax_fp64(case, M):
     info = F.info()
     if case.startswith("slab") or case == "bilayer":
         assert info["pruned"] == 1
+        # slab and slab_wrap (y lines of 32 and 33 points) take the fused
+        # y-transform / Green-tensor pass; the bilayer's 37-point y lines
+        # (prime) take the separate transforms and Toeplitz column kernel
+        assert info["slab_fused"] == (0 if case == "bilayer" else 1)
     Y = gpu_apply(F, X, sc)
     assert rel(Y, ref) < 1e-12, rel(Y, ref)
     # fp32 reciprocal / fp32 real space: single-precision agreement
