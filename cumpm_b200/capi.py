@@ -56,7 +56,8 @@ class FieldInfo(C.Structure):
     _fields_ = [("kind", C.c_int), ("mode", C.c_int), ("num_particles", C.c_int), ("num_targets", C.c_int),
                 ("num_quads", C.c_int), ("grid", C.c_int * 3), ("stencil", C.c_int), ("pruned", C.c_int),
                 ("z_slots", C.c_int), ("num_pairs", C.c_longlong), ("rc", C.c_double), ("h", C.c_double * 3),
-                ("eta", C.c_double * 3), ("selfo", C.c_double), ("slab_fused", C.c_int)]
+                ("eta", C.c_double * 3), ("selfo", C.c_double), ("slab_fused", C.c_int),
+                ("single_layer", C.c_int)]
 
 
 def lib():

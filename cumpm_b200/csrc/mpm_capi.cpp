@@ -299,6 +299,7 @@ int mpm_field_info_get(const mpm_field* f, mpm_field_info* info) {
         info->rc = g.rc;
         info->selfo = F.selfo();
         info->slab_fused = st.slab_fused;
+        info->single_layer = st.single_layer;
     });
 }
 

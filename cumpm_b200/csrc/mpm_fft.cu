@@ -690,7 +690,11 @@ void launch2_cw(int cls, int nblocks, int nthreads, size_t shm, cudaStream_t s, 
 // (kx, ky, mi) column, synchronises and writes the Green-tensor product
 // back (four Toeplitz products of Zs x Zs).
 
-template <typename R> __host__ __device__ constexpr int slab_mc() { return sizeof(R) == 8 ? 2 : 4; }
+// right-hand sides per CTA: a few for a Zs-slot slab, many for one slot
+// (a single layer), so that the tile stays near 60-70 KB
+template <typename R> __host__ __device__ constexpr int slab_mc(bool one_slot) {
+    return one_slot ? (sizeof(R) == 8 ? 16 : 32) : (sizeof(R) == 8 ? 2 : 4);
+}
 template <typename R> __host__ __device__ constexpr int slab_threads() { return sizeof(R) == 8 ? 160 : 320; }
 
 struct SlabArgs {
@@ -751,12 +755,11 @@ __device__ __forceinline__ void slab_ytransform(cplx<R>* S, const cplx<R>* T, in
     radix_dispatch<CLS>(r2, [&](auto rc) { slab_pass<R, INV, decltype(rc)::value, NT, true>(S, T, n, NCOL); });
 }
 
-template <typename R, int ZMAX, int CLS>
+template <typename R, int MC, int ZMAX, int CLS>
 __global__ void __launch_bounds__(slab_threads<R>()) k_slab(cplx<R>* __restrict__ data, const cplx<R>* __restrict__ tw,
                                                             const cplx<R>* __restrict__ taps, int r1, int r2,
                                                             SlabArgs a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    constexpr int MC = slab_mc<R>();
     constexpr int NT = slab_threads<R>();
     const int n = r1 * r2;
     const int Zs = a.Zs, M = a.M, B = 3 * M;
@@ -1519,7 +1522,7 @@ void AxisFFT::run_scaled(cplx<R>* data, size_t es, int ncols, size_t os, int nou
 
 bool AxisFFT::slab_ok(int Zs, bool fp64) const {
     if (kind_ != 1 || force_general_ || Zs < 1 || Zs > 16) return false;
-    const int mc = fp64 ? slab_mc<double>() : slab_mc<float>();
+    const int mc = fp64 ? slab_mc<double>(Zs == 1) : slab_mc<float>(Zs == 1);
     const size_t elem = fp64 ? sizeof(double2) : sizeof(float2);
     const size_t shm = (size_t(f_.n) * Zs * 3 * mc + f_.n) * elem;
     // both passes need at least one column per round
@@ -1532,8 +1535,9 @@ void AxisFFT::run_slab(cplx<R>* data, int nx, int Zs, int M, const cplx<R>* taps
                        cudaStream_t s) const {
     if (!slab_ok(Zs, sizeof(R) == 8)) throw std::runtime_error("run_slab: slab not supported by this axis");
     if (nx <= 0 || M <= 0) return;
-    constexpr int MC = slab_mc<R>();
+    constexpr int MC1 = slab_mc<R>(true), MCS = slab_mc<R>(false);
     constexpr int NT = slab_threads<R>();
+    const int MC = Zs == 1 ? MC1 : MCS;
     const int n = f_.n;
     const size_t shm = (size_t(n) * Zs * 3 * MC + n) * sizeof(cplx<R>);
     SlabArgs a;
@@ -1550,14 +1554,18 @@ void AxisFFT::run_slab(cplx<R>* data, int nx, int Zs, int M, const cplx<R>* taps
         MPM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(shm)));
         kern<<<nx * a.nchunk, NT, shm, s>>>(data, tw, taps, r1_, r2_, a);
     };
-    if (Zs <= 9) {
-        if (cls == 8) go(k_slab<R, 9, 8>);
-        else if (cls == 12) go(k_slab<R, 9, 12>);
-        else go(k_slab<R, 9, 16>);
+    if (Zs == 1) {
+        if (cls == 8) go(k_slab<R, MC1, 1, 8>);
+        else if (cls == 12) go(k_slab<R, MC1, 1, 12>);
+        else go(k_slab<R, MC1, 1, 16>);
+    } else if (Zs <= 9) {
+        if (cls == 8) go(k_slab<R, MCS, 9, 8>);
+        else if (cls == 12) go(k_slab<R, MCS, 9, 12>);
+        else go(k_slab<R, MCS, 9, 16>);
     } else {
-        if (cls == 8) go(k_slab<R, 16, 8>);
-        else if (cls == 12) go(k_slab<R, 16, 12>);
-        else go(k_slab<R, 16, 16>);
+        if (cls == 8) go(k_slab<R, MCS, 16, 8>);
+        else if (cls == 12) go(k_slab<R, MCS, 16, 12>);
+        else go(k_slab<R, MCS, 16, 16>);
     }
     MPM_LAUNCH();
 }

@@ -69,6 +69,7 @@ struct StencilArgs {
     int N[3];
     int off, S;
     int z0, pruned, Zs;
+    int layer;     // single layer: unit z weight at the centre (the real ones live in the k-space taps)
 };
 
 // Per point: nearest grid node (C round, halves away from zero), 1-D
@@ -87,7 +88,8 @@ __global__ void k_stencil(const double* __restrict__ xyz, int n, StencilArgs a, 
         const double c = (d == 0) ? a.cfac : 1.0;
         for (int o = 0; o < a.S; ++o) {
             const double gd = dd + (o - a.off) * a.h[d];
-            const double w = c * exp(-2.0 * a.xi * a.xi * gd * gd / a.eta[d]);
+            const double w = (d == 2 && a.layer) ? (o == a.off ? 1.0 : 0.0)
+                                                 : c * exp(-2.0 * a.xi * a.xi * gd * gd / a.eta[d]);
             w64[(size_t(i) * 3 + d) * a.S + o] = w;
             w32[(size_t(i) * 3 + d) * a.S + o] = static_cast<float>(w);
         }
@@ -662,6 +664,53 @@ __global__ void k_build_slab_taps(ScaleArgs a, int Z, double2* __restrict__ T64,
     }
 }
 
+// Single layer: the taps of one z slot, tau_n = sum_{o,o'} w_o w_o' t_n(o - o')
+// = sum_kz kz^n S(k) / |k|^2 |sum_o w_o exp(-2 pi i kz o / Nz)|^2 (real), with
+// the layer's common z weights w_o; w2[kz] holds the squared modulus.
+// Stored as the taps of a one-slot slab ([col][3][1]).  Float64, one thread
+// per column, kz summed in order.
+__global__ void k_layer_w2(const double* __restrict__ w, int S, int Nz, double* __restrict__ w2) {
+    const int iz = blockIdx.x * blockDim.x + threadIdx.x;
+    if (iz >= Nz) return;
+    double re = 0.0, im = 0.0;
+    for (int o = 0; o < S; ++o) {
+        double sn, cs;
+        sincospi(2.0 * double((long long)iz * o % Nz) / Nz, &sn, &cs);
+        re += w[o] * cs;
+        im -= w[o] * sn;
+    }
+    w2[iz] = re * re + im * im;
+}
+
+__global__ void k_build_layer_taps(ScaleArgs a, const double* __restrict__ w2, double2* __restrict__ T64,
+                                   float2* __restrict__ T32) {
+    const int col = blockIdx.x * blockDim.x + threadIdx.x;
+    if (col >= a.Nx * a.Ny) return;
+    const int ix = col / a.Ny, iy = col % a.Ny;
+    const int Nz = a.Nz;
+    const double V = double(a.Nx) * a.Ny * a.Nz;
+    const double fx = (ix <= (a.Nx - 1) / 2) ? ix : ix - a.Nx;
+    const double fy = (iy <= (a.Ny - 1) / 2) ? iy : iy - a.Ny;
+    const double gx = fx * 2.0 * kPi / a.Lx, gy = fy * 2.0 * kPi / a.Ly;
+    double t0 = 0.0, t1 = 0.0, t2 = 0.0;
+    for (int iz = 0; iz < Nz; ++iz) {
+        double o[4];
+        scale_coefs(ix, iy, iz, a.Nx, a.Ny, Nz, a.Lx, a.Ly, a.Lz, a.xi, a.eta, V, o);
+        const double fz = (iz <= (Nz - 1) / 2) ? iz : iz - Nz;
+        const double gz = fz * 2.0 * kPi / a.Lz;
+        const double k2 = gx * gx + gy * gy + gz * gz;
+        const double t = k2 < 1e-24 ? 0.0 : o[0] / k2 * w2[iz];
+        t0 += t;
+        t1 += t * gz;
+        t2 += t * gz * gz;
+    }
+    const double tv[3] = {t0, t1, t2};
+    for (int k = 0; k < 3; ++k) {
+        T64[size_t(col) * 3 + k] = make_double2(tv[k], 0.0);
+        T32[size_t(col) * 3 + k] = make_float2(float(tv[k]), 0.f);
+    }
+}
+
 // Pruned layout: out[zo][c'][m] = sum_{zi,c} K_{c'c}(zo - zi) in[zi][c][m]
 // on one (kx, ky) column per CTA, in place.  The column's Z x 3 inputs of a
 // right-hand side sit in registers; for each source component c the 2Z-1
@@ -714,7 +763,7 @@ __global__ void k_column(cplx<R>* __restrict__ grid, const cplx<R>* __restrict__
 // Contraction: field at each target from its Gaussian stencil for all B
 // columns (contract_kernel, monodisperse_ewald_electric_field.cu:1488-1587).
 // Writes Y rows (overwrites).  C = 3 (dipoles) or 8 (plus field gradient).
-// SZ > 0: the stencil's z run (g.S <= SZ) unrolled, so that its grid loads
+// SZ > 0: the stencil's z run (g.Sz <= SZ) unrolled, so that its grid loads
 // are in flight together; SZ = 0: any stencil length.
 template <typename R, int SZ>
 __global__ void k_contract(const cplx<R>* __restrict__ grid, GridView g, int M, int C, int Nt,
@@ -736,6 +785,9 @@ __global__ void k_contract(const cplx<R>* __restrict__ grid, GridView g, int M, 
                  : (g.pruned ? bs.z + dd : pmod(bs.z + dd, g.Nz));
     }
     __syncthreads();
+    // the z window on the stored grid: entries zb .. zb + Sz - 1 of the z
+    // stencil (all of it, or the single layer's centre)
+    const int zb = 2 * g.S + g.off - g.offz;
     const int q = (C > 3 && quad_map) ? quad_map[j] : -1;
     for (int b = threadIdx.x; b < B; b += blockDim.x) {
         const int comp = b / M;
@@ -748,8 +800,8 @@ __global__ void k_contract(const cplx<R>* __restrict__ grid, GridView g, int M, 
         if constexpr (SZ > 0) {
 #pragma unroll
             for (int oz = 0; oz < SZ; ++oz) {
-                wz[oz] = oz < g.S ? w[2 * g.S + oz] : R(0);
-                zo[oz] = oz < g.S ? idx[2 * g.S + oz] * B + b : b;
+                wz[oz] = oz < g.Sz ? w[zb + oz] : R(0);
+                zo[oz] = oz < g.Sz ? idx[zb + oz] * B + b : b;
             }
         }
         for (int ox = 0; ox < g.S; ++ox) {
@@ -764,13 +816,13 @@ __global__ void k_contract(const cplx<R>* __restrict__ grid, GridView g, int M, 
                     cplx<R> v[SZ];
 #pragma unroll
                     for (int oz = 0; oz < SZ; ++oz)
-                        if (oz < g.S) v[oz] = gp[zo[oz]];
+                        if (oz < g.Sz) v[oz] = gp[zo[oz]];
 #pragma unroll
                     for (int oz = 0; oz < SZ; ++oz)
-                        if (oz < g.S) fma_rc(a2, wz[oz], v[oz]);
+                        if (oz < g.Sz) fma_rc(a2, wz[oz], v[oz]);
                 } else {
-                    for (int oz = 0; oz < g.S; ++oz) {
-                        fma_rc(a2, w[2 * g.S + oz], grid[(rxy + idx[2 * g.S + oz]) * B + b]);
+                    for (int oz = 0; oz < g.Sz; ++oz) {
+                        fma_rc(a2, w[zb + oz], grid[(rxy + idx[zb + oz]) * B + b]);
                     }
                 }
                 fma_rc(acc, wxy, a2);
@@ -1205,6 +1257,7 @@ FieldStats Field::stats() const {
     for (int d = 0; d < 3; ++d) s.grid[d] = geom_.ng[d];
     s.stencil = gv_.S;
     s.slab_fused = (spec_.kind == FIELD_MONO && use_slab()) ? 1 : 0;
+    s.single_layer = (spec_.kind == FIELD_MONO && gv_.layer) ? 1 : 0;
     return s;
 }
 
@@ -1275,11 +1328,49 @@ void Field::choose_layout(cudaStream_t) {
     gv_.Nz = Nz;
     gv_.off = geom_.off;
     gv_.S = 2 * geom_.off + 1;
+    gv_.Sz = gv_.S;
+    gv_.offz = gv_.off;
+    gv_.layer = 0;
     gv_.pruned = 0;
     gv_.z0 = 0;
     gv_.Zs = Nz;
     // Pruned slab layout only for the dipole matvec with targets == sources.
     if (!spec_.solver_ax || Nq_ > 0) return;
+    // A single layer: every particle has the same nearest z node and the
+    // same offset from it (a planar monolayer), so every z stencil is the
+    // same weight vector w_o.  The grid then keeps one z slot and the
+    // k-space step carries sum_{o,o'} w_o w_o' K(o - o') (the same
+    // discretisation, z summed first).
+    if (!host_z_.empty()) {
+        const double hz = geom_.h[2];
+        const long g0 = std::lround(host_z_[0] / hz);
+        const double d0 = double(g0) * hz - host_z_[0];
+        bool same = true;
+        for (double zv : host_z_) {
+            const long g = std::lround(zv / hz);
+            if (pmod(int(g), Nz) != pmod(int(g0), Nz) || double(g) * hz - zv != d0) {
+                same = false;
+                break;
+            }
+        }
+        if (same) {
+            gv_.pruned = 1;
+            gv_.layer = 1;
+            gv_.Zs = 1;
+            gv_.z0 = pmod(int(g0), Nz);
+            gv_.Sz = 1;
+            gv_.offz = 0;
+            layer_w_.resize(gv_.S);
+            for (int o = 0; o < gv_.S; ++o) {
+                const double gd = d0 + (o - gv_.off) * hz;
+                layer_w_[o] = std::exp(-2.0 * spec_.xi * spec_.xi * gd * gd / geom_.eta[2]);
+            }
+            if (pmod(int(g0), Nz) != layer_key_g_ || d0 != layer_key_d_) layer_taps_ = false;
+            layer_key_g_ = pmod(int(g0), Nz);
+            layer_key_d_ = d0;
+            return;
+        }
+    }
     std::vector<char> occ(Nz, 0);
     for (double zv : host_z_) {
         const long g = std::lround(zv / geom_.h[2]);  // C round, halves away from zero
@@ -1367,6 +1458,7 @@ void Field::build_stencil(PointSet& ps, cudaStream_t s, bool bins) {
     a.z0 = gv_.z0;
     a.pruned = gv_.pruned;
     a.Zs = gv_.Zs;
+    a.layer = gv_.layer;
     k_stencil<<<nblk(n, 128), 128, 0, s>>>(ps.xyz.as<double>(), n, a, ps.base.as<int4>(), ps.w64.as<double>(),
                                             ps.w32.as<float>());
     MPM_LAUNCH();
@@ -1524,6 +1616,22 @@ void Field::build_slab_taps(cudaStream_t s) {
     a.Lx = spec_.box[0]; a.Ly = spec_.box[1]; a.Lz = spec_.box[2];
     a.xi = spec_.xi;
     for (int d = 0; d < 3; ++d) a.eta[d] = geom_.eta[d];
+    if (gv_.layer) {
+        // |sum_o w_o exp(-2 pi i kz o / Nz)|^2 per kz, then the taps
+        layer_wd_.ensure(sizeof(double) * (gv_.S + gv_.Nz));
+        double* wd = layer_wd_.as<double>();
+        MPM_CUDA(cudaMemcpyAsync(wd, layer_w_.data(), sizeof(double) * gv_.S, cudaMemcpyHostToDevice, s));
+        k_layer_w2<<<nblk(gv_.Nz, 128), 128, 0, s>>>(wd, gv_.S, gv_.Nz, wd + gv_.S);
+        MPM_LAUNCH();
+        k_build_layer_taps<<<nblk(ncol, 128), 128, 0, s>>>(a, wd + gv_.S, slabT64_.as<double2>(),
+                                                           slabT32_.as<float2>());
+        MPM_LAUNCH();
+        MPM_CUDA(cudaStreamSynchronize(s));   // layer_w_ is read by the copy above
+        layer_taps_ = true;
+        slab_Z_ = -1;
+        return;
+    }
+    layer_taps_ = false;
     const size_t shm = sizeof(double) * 5 * gv_.Nz;
     if (shm > 48 * 1024)
         MPM_CUDA(cudaFuncSetAttribute(k_build_slab_taps, cudaFuncAttributeMaxDynamicSharedMemorySize, int(shm)));
@@ -1548,7 +1656,7 @@ void Field::precalc(cudaStream_t s) {
         if (!spec_.solver_ax) build_stencil(targets_, s, false);  // SOLVER_AX: targets share the source stencil
         build_pairs(s);
         if (use_slab()) {
-            if (slab_Z_ != gv_.Zs) build_slab_taps(s);
+            if (gv_.layer ? !layer_taps_ : slab_Z_ != gv_.Zs) build_slab_taps(s);
         } else if (gv_.pruned) {
             if (colK_Z_ != gv_.Zs) build_column_kernel(s);
         } else if (scale_built_ != (Nq_ ? 4 : 1)) {
@@ -1651,7 +1759,8 @@ void Field::recip_on(const double2* X, double2* Y, int M, cplx<R>* grid, cudaStr
                                         plan_lc_.as<int>(), plan_ln_.as<int>(), grid);
         };
         // the tile's z run in registers: as many accumulators as it needs
-        if (TZ <= 9) go(k_spread_planned<R, 9>);
+        if (TZ == 1) go(k_spread_planned<R, 1>);
+        else if (TZ <= 9) go(k_spread_planned<R, 9>);
         else go(k_spread_planned<R, kSpreadZMax>);
     } else {
         k_spread<R><<<grd, 256, shm, s>>>(X, M, N_, C, quad_map_.as<int>(), ps.base.as<int4>(), w1,
@@ -1725,8 +1834,9 @@ void Field::recip_on(const double2* X, double2* Y, int M, cplx<R>* grid, cudaStr
                                 spec_.solver_ax ? quad_map_.as<int>() : nullptr, Y, 0,
                                 spec_.solver_ax ? sources_.idx_sorted.as<int>() : nullptr);
     };
-    if (gv_.S <= 9) contract(k_contract<R, 9>);
-    else if (gv_.S <= 13) contract(k_contract<R, 13>);
+    if (gv_.Sz == 1) contract(k_contract<R, 1>);
+    else if (gv_.Sz <= 9) contract(k_contract<R, 9>);
+    else if (gv_.Sz <= 13) contract(k_contract<R, 13>);
     else contract(k_contract<R, 0>);
     MPM_LAUNCH();
 }

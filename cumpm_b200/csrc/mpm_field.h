@@ -76,6 +76,11 @@ struct GridView {
     int pruned;    // 1: slots are the occupied planes z0..z0+Zs-1 (mod Nz)
     int off;       // stencil half width
     int S;         // stencil width
+    // z extent of the stencils on the stored grid: S and off, or 1 and 0 for
+    // a single layer (every particle the same z stencil, folded into the
+    // k-space taps; the grid then holds one z slot)
+    int Sz, offz;
+    int layer;
 };
 
 struct PointSet {
@@ -97,6 +102,7 @@ struct FieldStats {
     int grid[3] = {0, 0, 0};
     int stencil = 0;
     int slab_fused = 0;
+    int single_layer = 0;
 };
 
 class Field {
@@ -197,6 +203,13 @@ private:
     DevBuf colK64_, colK32_;        // pruned layout: per-column Toeplitz kernels (unfused path)
     DevBuf slabT64_, slabT32_;      // pruned layout: per-column scalar Toeplitz taps t0, t1, t2 (fused path)
     int slab_Z_ = -1;
+    // single layer: the common z weights of every stencil (planes z0 ..
+    // z0 + S - 1) and the (plane, offset) they were built for
+    std::vector<double> layer_w_;
+    long layer_key_g_ = -1;
+    double layer_key_d_ = 0.0;
+    bool layer_taps_ = false;
+    DevBuf layer_wd_;               // device copy of layer_w_ and its |DFT|^2 per kz
     // per-frame spread plan (monodisperse): per tile candidates, 1-D weights,
     // column contributor lists; plan_cap_ = 0 when the plan is not in use
     DevBuf plan_nc_, plan_cid_, plan_w64_, plan_w32_, plan_lw64_, plan_lw32_, plan_lc_, plan_ln_, plan_cnt_;

@@ -659,6 +659,9 @@ void Field::poly_init() {
     gv_.pruned = 0;
     gv_.off = 0;
     gv_.S = pgeom_.P;
+    gv_.Sz = gv_.S;
+    gv_.offz = 0;
+    gv_.layer = 0;
     if (gv_.Nx < 16 || gv_.Ny < 16 || gv_.Nz < 16 || pgeom_.P >= std::min(gv_.Nx, std::min(gv_.Ny, gv_.Nz)))
         throw std::runtime_error("polydisperse grid shorter than 16 points or than the support along an axis");
     const size_t V = size_t(gv_.Nx) * gv_.Ny * gv_.Nz;

@@ -99,6 +99,7 @@ typedef struct mpm_field_info {
     long long num_pairs;   /* real-space (target, source) pairs */
     double rc, h[3], eta[3], selfo;
     int slab_fused;        /* 1: pruned layout whose y transforms and k-space step run as one fused pass */
+    int single_layer;      /* 1: every particle has the same z stencil; the grid keeps one z slot */
 } mpm_field_info;
 
 MPM_API const char* mpm_last_error(void);

@@ -1,13 +1,14 @@
 """Parity at the benchmark configurations themselves, not only at small sizes.
 
 * The N=4000 hexagonal monolayer (box 1542.0 x 332.6 x 1000 nm, 366x80x238
-  grid stored as 9 occupied z planes, support 9) applied to M=30 right-hand
+  grid; a planar layer, so stored as one z slot; support 9) applied to M=30 right-hand
   sides -- the batch the benchmark solves -- in fp64, against the oracle
   column by column, and three columns against the reference build's
   monodisperse field (PrecisionMode.DOUBLE); the fp32 reciprocal space of
   the same batch against the same oracle columns.  M=30 puts 90 grid
   columns per voxel through the multi-chunk spread (32-column fp32 / 16-column
-  fp64 chunks), the M=30 Toeplitz column kernel and the contraction.
+  fp64 chunks), the fused y-transform / Green-tensor pass and the
+  contraction.
 * The N=1000 polydisperse packing (radii U[1,4] nm, 108^3 scalar grid,
   support 12) with M=192, a quarter of the columns against the oracle, and
   the same positions with four radius classes against the reference build's
@@ -73,8 +74,9 @@ def monolayer():
 def test_monolayer_operator_m30_matches_oracle(monolayer):
     wl, F = monolayer
     info = F.info()
-    assert info["grid"] == [366, 80, 238] and info["pruned"] == 1 and info["z_slots"] == 9
-    assert info["slab_fused"] == 1
+    # a planar layer: one z slot, the z weights in the fused k-space pass
+    assert info["grid"] == [366, 80, 238] and info["pruned"] == 1 and info["z_slots"] == 1
+    assert info["slab_fused"] == 1 and info["single_layer"] == 1
     N, M = len(wl.pos), 30
     X, sc = _inputs(40, 3 * N, N, M)
     Y64 = _gpu(F, X, sc)

@@ -66,6 +66,10 @@ def test_mono_solver_ax_fp64(case, M):
         # y-transform / Green-tensor pass; the bilayer's 37-point y lines
         # (prime) take the separate transforms and Toeplitz column kernel
         assert info["slab_fused"] == (0 if case == "bilayer" else 1)
+        # the slab case is one plane (z = 0.3 for every particle): a single
+        # layer, one stored z slot; slab_wrap spreads z over several planes
+        assert info["single_layer"] == (1 if case == "slab" else 0)
+        assert (info["z_slots"] == 1) == (case == "slab")
     Y = gpu_apply(F, X, sc)
     assert rel(Y, ref) < 1e-12, rel(Y, ref)
     # fp32 reciprocal / fp32 real space: single-precision agreement
