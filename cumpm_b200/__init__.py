@@ -9,8 +9,9 @@ from .near_field import Near_Field  # noqa: F401
 from .eels import EELS  # noqa: F401
 from . import capi  # noqa: F401
 from . import dev  # noqa: F401
+from . import io  # noqa: F401
 from ._load import extension as _extension
 
 _cuMPM = _extension()
 
-__all__ = ["dipole_solver", "drude_dielectric", "Near_Field", "EELS", "dev", "capi"]
+__all__ = ["dipole_solver", "drude_dielectric", "Near_Field", "EELS", "dev", "capi", "io"]

@@ -975,7 +975,47 @@ struct RealArgs {
     const double* qg2;
 };
 
+// Dipole pairs of one target, kPairBatch pairs at a time: the source
+// indices, pair coefficients and moments of a batch are all loaded before
+// any is used, so the pair loop waits on one memory latency per batch
+// rather than two per pair.  Accumulation order is the pair order.
+constexpr int kPairBatch = 4;
+
 template <typename R>
+__device__ __forceinline__ void real_dipole_pairs(const double2* __restrict__ X, int M, int m, int p0, int p1,
+                                                  const int* __restrict__ src, const R* __restrict__ T,
+                                                  cplx<R>& e0, cplx<R>& e1, cplx<R>& e2) {
+    for (int p = p0; p < p1; p += kPairBatch) {
+        int ii[kPairBatch];
+        R dx[kPairBatch], dy[kPairBatch], dz[kPairBatch], pe[kPairBatch], pa[kPairBatch];
+        cplx<R> px[kPairBatch], py[kPairBatch], pz[kPairBatch];
+#pragma unroll
+        for (int u = 0; u < kPairBatch; ++u) ii[u] = (p + u < p1) ? src[p + u] : -1;
+#pragma unroll
+        for (int u = 0; u < kPairBatch; ++u) {
+            if (ii[u] >= 0) {
+                const R* t = T + 8 * size_t(p + u);
+                dx[u] = t[0]; dy[u] = t[1]; dz[u] = t[2]; pe[u] = t[3]; pa[u] = t[4];
+                const double2* xi = X + size_t(3 * ii[u]) * M + m;
+                px[u] = to_r<R>(xi[0]);
+                py[u] = to_r<R>(xi[size_t(M)]);
+                pz[u] = to_r<R>(xi[size_t(2) * M]);
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < kPairBatch; ++u) {
+            if (ii[u] >= 0) {
+                const cplx<R> rp = px[u] * dx[u] + py[u] * dy[u] + pz[u] * dz[u];
+                const cplx<R> k = rp * (pa[u] - pe[u]);
+                e0 += px[u] * pe[u] + k * dx[u];
+                e1 += py[u] * pe[u] + k * dy[u];
+                e2 += pz[u] * pe[u] + k * dz[u];
+            }
+        }
+    }
+}
+
+template <typename R, bool QUADS>
 __global__ void __launch_bounds__(128) k_real(const double2* __restrict__ X, double2* __restrict__ Y, RealArgs a,
                                               const int* __restrict__ off, const int* __restrict__ src,
                                               const R* __restrict__ T, const double* __restrict__ Qt,
@@ -989,12 +1029,13 @@ __global__ void __launch_bounds__(128) k_real(const double2* __restrict__ X, dou
     const int M = a.M;
     const double sign = (a.solver_ax || a.pairs_plus) ? 1.0 : -1.0;
     const double selfc = selfv ? selfv[j] : a.selfo;  // polydisperse: self value of the particle's radius class
-    const int qt = (a.quads && quad_map && j < a.N) ? quad_map[j] : -1;
+    const int qt = (QUADS && quad_map && j < a.N) ? quad_map[j] : -1;
     for (int m = lane; m < M; m += 32) {
         cplx<R> e0 = mk<R>(0, 0), e1 = e0, e2 = e0;
         double2 G[5] = {make_double2(0, 0), make_double2(0, 0), make_double2(0, 0), make_double2(0, 0),
                         make_double2(0, 0)};
-        for (int p = p0; p < p1; ++p) {
+        if constexpr (!QUADS) real_dipole_pairs<R>(X, M, m, p0, p1, src, T, e0, e1, e2);
+        for (int p = p0; QUADS && p < p1; ++p) {
             const int i = src[p];
             const R* t = T + 8 * size_t(p);
             const R dx = t[0], dy = t[1], dz = t[2], perp = t[3], para = t[4];
@@ -1006,7 +1047,7 @@ __global__ void __launch_bounds__(128) k_real(const double2* __restrict__ X, dou
             e0 += px * perp + k * dx;
             e1 += py * perp + k * dy;
             e2 += pz * perp + k * dz;
-            if (a.quads) {
+            {
                 // quadrupole couplings in float64 (reference :1758-1866)
                 const double* qc = Qt + 8 * size_t(p);
                 const double Q1 = qc[0], Q2 = qc[1], Q3 = qc[2];
@@ -1862,13 +1903,17 @@ void Field::real_part(const double2* X, double2* Y, int M, const double2* sc, bo
     const int thr = 128;
     const int blocks = nblk((long long)warps * 32, thr);
     StageScope scope(ST_REAL, s);
-    if (fp32)
-        k_real<float><<<blocks, thr, 0, s>>>(X, Y, a, pair_off_.as<int>(), pair_src_.as<int>(), pair_T32_.as<float>(),
-                                             pair_Q_.as<double>(), quad_map_.as<int>(), sc, selfv);
-    else
-        k_real<double><<<blocks, thr, 0, s>>>(X, Y, a, pair_off_.as<int>(), pair_src_.as<int>(),
-                                              pair_T64_.as<double>(), pair_Q_.as<double>(), quad_map_.as<int>(), sc,
-                                              selfv);
+    auto go = [&](auto kern, const auto* T) {
+        kern<<<blocks, thr, 0, s>>>(X, Y, a, pair_off_.as<int>(), pair_src_.as<int>(), T, pair_Q_.as<double>(),
+                                    quad_map_.as<int>(), sc, selfv);
+    };
+    if (fp32) {
+        if (a.quads) go(k_real<float, true>, pair_T32_.as<float>());
+        else go(k_real<float, false>, pair_T32_.as<float>());
+    } else {
+        if (a.quads) go(k_real<double, true>, pair_T64_.as<double>());
+        else go(k_real<double, false>, pair_T64_.as<double>());
+    }
     MPM_LAUNCH();
 }
 

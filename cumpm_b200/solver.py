@@ -114,6 +114,10 @@ class dipole_solver:
         else:
             raise TypeError("quadrupoles must be a boolean or a list/iterable of particle indices")
         eps = _to_numpy(eps_p)
+        # the run's inputs, kept for result files (cumpm_b200.io.save_solution)
+        self._args = {"box": np.array(box_list), "eps_p": np.asarray(eps, dtype=np.complex128),
+                      "radius": np.array(radius_list), "eps_m": float(eps_m), "xi": float(xi), "tol": float(tol),
+                      "E0": np.array(E0_list, dtype=np.complex128) if E0_list else np.eye(3, dtype=np.complex128)}
         args = (radius_list, float(eps_m), float(xi), float(tol), bool(quiet), guess_type, solver_type,
                 field_type, E0_list, solve_q, quad_idxs, prec)
         if eps.ndim == 0 or (eps.ndim == 1 and eps.size == 1):

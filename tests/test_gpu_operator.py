@@ -229,6 +229,7 @@ def test_hex_monolayer_operator_fp64():
     F = capi.Field(capi.FIELD_MONO, box, 1e-6, 0.5)
     F.set_positions(pos)
     info = F.info()
-    assert info["pruned"] == 1 and info["z_slots"] == 9
+    # every particle at z = 0: a single layer (one stored z slot)
+    assert info["pruned"] == 1 and info["z_slots"] == 1 and info["single_layer"] == 1
     assert info["num_pairs"] == len(op.pi_)
     assert rel(gpu_apply(F, X, sc), ref) < 1e-12
