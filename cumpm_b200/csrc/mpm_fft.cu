@@ -681,91 +681,80 @@ void launch2_cw(int cls, int nblocks, int nthreads, size_t shm, cudaStream_t s, 
 //
 // One CTA owns one kx plane and MC right-hand sides: the tile
 // S[y][col], col = (z * 3 + c) * MC + mi, NCOL = Zs * 3 * MC columns of
-// n = Ny points, lives in shared memory for the whole step.  The y
-// transforms are the two-pass (r1, r2) split of k_fft2, run in place: the
-// butterflies of a round cover whole columns, every thread reads its
-// butterfly's inputs into registers, the block synchronises, then writes
-// (the next round's columns are disjoint, so one barrier per round).
-// Between the transforms, thread (ky, mi) reads the 3 x Zs values of its
-// (kx, ky, mi) column, synchronises and writes the Green-tensor product
-// back (four Toeplitz products of Zs x Zs).
+// n = Ny points, lives in shared memory for the whole step, with a second
+// tile of the same size for the transforms.  The y transforms are the
+// two-pass (r1, r2) split of k_fft2 between the two tiles (pass 1 S -> S2,
+// pass 2 S2 -> S), so a pass needs one barrier, not one per group of
+// columns.  Between the transforms thread (ky, mi) reads the 3 x Zs values
+// of its (kx, ky, mi) column and writes the Green-tensor product back in
+// place (four Toeplitz products of Zs x Zs); no other thread touches them.
 
-// right-hand sides per CTA: a few for a Zs-slot slab, many for one slot
-// (a single layer), so that the tile stays near 60-70 KB
+// right-hand sides per CTA: two tiles of n x Zs x 3 x MC within ~70 KB
 template <typename R> __host__ __device__ constexpr int slab_mc(bool one_slot) {
-    return one_slot ? (sizeof(R) == 8 ? 16 : 32) : (sizeof(R) == 8 ? 2 : 4);
+    return one_slot ? (sizeof(R) == 8 ? 4 : 8) : (sizeof(R) == 8 ? 1 : 2);
 }
-template <typename R> __host__ __device__ constexpr int slab_threads() { return sizeof(R) == 8 ? 160 : 320; }
+constexpr int kSlabThreads = 128;
 
 struct SlabArgs {
     int Nx, Zs, M, nchunk;
     double kxu, kyu;
 };
 
-// one in-place radix pass over all NCOL columns: butterfly j < nb of radix
-// RAD reads elements (j + q nb) (twiddled by W_n^(q j) when TW), writes
-// (j RAD + p) for pass 1 or (p nb' + j) for pass 2 -- see the callers
-template <typename R, bool INV, int RAD, int NT, bool PASS2>
-__device__ __forceinline__ void slab_pass(cplx<R>* __restrict__ S, const cplx<R>* __restrict__ T, int n, int NCOL) {
-    const int nb = n / RAD;            // butterflies per column
-    const int cpr = NT / nb;           // columns per round
-    const int rounds = (NCOL + cpr - 1) / cpr;
-    const int cl = threadIdx.x % cpr;
-    const int j = threadIdx.x / cpr;   // butterfly index; < nb for active threads
-    const bool act0 = j < nb;
-    for (int rd = 0; rd < rounds; ++rd) {
-        const int col = rd * cpr + cl;
-        const bool act = act0 && col < NCOL;
+// one radix pass over all NCOL columns, src -> dst, thread task t =
+// (butterfly j, column col), col fastest.  Pass 1 (radix r1, butterfly
+// j < r2) reads src[j + q r2] and writes dst[j r1 + p]; pass 2 (radix r2,
+// butterfly j < r1) reads src[j + q r1] W_n^(q j) and writes dst[p r1 + j].
+template <typename R, bool INV, int RAD, bool PASS2>
+__device__ __forceinline__ void slab_pass(const cplx<R>* __restrict__ src, cplx<R>* __restrict__ dst,
+                                          const cplx<R>* __restrict__ T, int n, int NCOL) {
+    const int nb = n / RAD;   // butterflies per column
+    for (int t = threadIdx.x; t < nb * NCOL; t += kSlabThreads) {
+        const int j = t / NCOL, col = t - j * NCOL;
         cplx<R> x[RAD];
-        if (act) {
-            if constexpr (!PASS2) {
-                // radix r1, butterfly j < r2 reads x[j + q r2]
+        if constexpr (!PASS2) {
 #pragma unroll
-                for (int q = 0; q < RAD; ++q) x[q] = S[(j + q * nb) * NCOL + col];
-            } else {
-                // radix r2, butterfly j < r1 reads S[j + q r1] W_n^(q j)
-                x[0] = S[j * NCOL + col];
+            for (int q = 0; q < RAD; ++q) x[q] = src[(j + q * nb) * NCOL + col];
+        } else {
+            x[0] = src[j * NCOL + col];
 #pragma unroll
-                for (int q = 1; q < RAD; ++q) {
-                    cplx<R> w = T[q * j];
-                    if (INV) w.y = -w.y;
-                    x[q] = S[(j + q * nb) * NCOL + col] * w;
-                }
+            for (int q = 1; q < RAD; ++q) {
+                cplx<R> w = T[q * j];
+                if (INV) w.y = -w.y;
+                x[q] = src[(j + q * nb) * NCOL + col] * w;
             }
-            dft_small<R, INV, RAD>(x);
         }
-        __syncthreads();
-        if (act) {
-            if constexpr (!PASS2) {
+        dft_small<R, INV, RAD>(x);
+        if constexpr (!PASS2) {
 #pragma unroll
-                for (int p = 0; p < RAD; ++p) S[(j * RAD + p) * NCOL + col] = x[p];
-            } else {
+            for (int p = 0; p < RAD; ++p) dst[(j * RAD + p) * NCOL + col] = x[p];
+        } else {
 #pragma unroll
-                for (int p = 0; p < RAD; ++p) S[(p * nb + j) * NCOL + col] = x[p];
-            }
+            for (int p = 0; p < RAD; ++p) dst[(p * nb + j) * NCOL + col] = x[p];
         }
     }
     __syncthreads();
 }
 
-template <typename R, bool INV, int CLS, int NT>
-__device__ __forceinline__ void slab_ytransform(cplx<R>* S, const cplx<R>* T, int r1, int r2, int NCOL) {
+// y transform of every column of S (result back in S; S2 is scratch)
+template <typename R, bool INV, int CLS>
+__device__ __forceinline__ void slab_ytransform(cplx<R>* S, cplx<R>* S2, const cplx<R>* T, int r1, int r2,
+                                                int NCOL) {
     const int n = r1 * r2;
-    radix_dispatch<CLS>(r1, [&](auto rc) { slab_pass<R, INV, decltype(rc)::value, NT, false>(S, T, n, NCOL); });
-    radix_dispatch<CLS>(r2, [&](auto rc) { slab_pass<R, INV, decltype(rc)::value, NT, true>(S, T, n, NCOL); });
+    radix_dispatch<CLS>(r1, [&](auto rc) { slab_pass<R, INV, decltype(rc)::value, false>(S, S2, T, n, NCOL); });
+    radix_dispatch<CLS>(r2, [&](auto rc) { slab_pass<R, INV, decltype(rc)::value, true>(S2, S, T, n, NCOL); });
 }
 
 template <typename R, int MC, int ZMAX, int CLS>
-__global__ void __launch_bounds__(slab_threads<R>()) k_slab(cplx<R>* __restrict__ data, const cplx<R>* __restrict__ tw,
-                                                            const cplx<R>* __restrict__ taps, int r1, int r2,
-                                                            SlabArgs a) {
+__global__ void __launch_bounds__(kSlabThreads) k_slab(cplx<R>* __restrict__ data, const cplx<R>* __restrict__ tw,
+                                                       const cplx<R>* __restrict__ taps, int r1, int r2,
+                                                       SlabArgs a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    constexpr int NT = slab_threads<R>();
     const int n = r1 * r2;
     const int Zs = a.Zs, M = a.M, B = 3 * M;
     const int NCOL = Zs * 3 * MC;
     cplx<R>* S = reinterpret_cast<cplx<R>*>(smem_raw);
-    cplx<R>* T = S + size_t(n) * NCOL;
+    cplx<R>* S2 = S + size_t(n) * NCOL;
+    cplx<R>* T = S2 + size_t(n) * NCOL;
     // the right-hand-side chunks of one kx plane are adjacent in launch order
     const int ix = blockIdx.x / a.nchunk;
     const int m0 = (blockIdx.x - ix * a.nchunk) * MC;
@@ -773,93 +762,83 @@ __global__ void __launch_bounds__(slab_threads<R>()) k_slab(cplx<R>* __restrict_
     cplx<R>* g = data + size_t(ix) * n * Zs * B;
     const int tot = n * NCOL;
     // tile element t = ((y Zs + z) 3 + c) MC + mi  <-  g[(y Zs + z) B + c M + m0 + mi]
-    for (int t = threadIdx.x; t < tot; t += NT) {
+    for (int t = threadIdx.x; t < tot; t += kSlabThreads) {
         const int mi = t % MC;
         const int r = t / MC;
         const bool live = mi < mc;
         const cplx<R>* src = live ? g + size_t(r / 3) * B + (r % 3) * M + m0 + mi : data;
         copy_async<R>(S + t, src, live);
     }
-    for (int t = threadIdx.x; t < n; t += NT) T[t] = tw[t];
+    for (int t = threadIdx.x; t < n; t += kSlabThreads) T[t] = tw[t];
     copy_async_wait();
     __syncthreads();
-    slab_ytransform<R, false, CLS, NT>(S, T, r1, r2, NCOL);
-    // Green tensor per (ky, mi): a = kx E_x + ky E_y, E_z in registers
+    slab_ytransform<R, false, CLS>(S, S2, T, r1, r2, NCOL);
+    // Green tensor per (ky, mi), in place: a = kx E_x + ky E_y,
+    // u = t0 * a + t1 * E_z  ->  E_x = kx u, E_y = ky u;  E_z = t1 * a + t2 * E_z
     const double fx = (ix <= (a.Nx - 1) / 2) ? ix : ix - a.Nx;
     const R kx = R(fx * a.kxu);
     const int nd = 2 * Zs - 1;
-    const int ntask = n * MC;
-    for (int r0 = 0; r0 < ntask; r0 += NT) {
-        const int t = r0 + threadIdx.x;
-        const bool act = t < ntask;
-        const int ky_i = act ? t / MC : 0;
+    for (int t = threadIdx.x; t < n * MC; t += kSlabThreads) {
+        const int ky_i = t / MC;
         const int mi = t - ky_i * MC;
+        const double fy = (ky_i <= (n - 1) / 2) ? ky_i : ky_i - n;
+        const R ky = R(fy * a.kyu);
+        cplx<R>* b = S + size_t(ky_i) * NCOL + mi;
         cplx<R> av[ZMAX], zv[ZMAX];
-        R ky = R(0);
-        if (act) {
-            const double fy = (ky_i <= (n - 1) / 2) ? ky_i : ky_i - n;
-            ky = R(fy * a.kyu);
-            const cplx<R>* b = S + size_t(ky_i) * NCOL + mi;
 #pragma unroll
-            for (int z = 0; z < ZMAX; ++z) {
-                if (z < Zs) {
-                    const cplx<R> ex = b[(z * 3 + 0) * MC], ey = b[(z * 3 + 1) * MC];
-                    av[z] = ex * kx + ey * ky;
-                    zv[z] = b[(z * 3 + 2) * MC];
-                } else {
-                    av[z] = mk<R>(R(0), R(0));
-                    zv[z] = mk<R>(R(0), R(0));
-                }
+        for (int z = 0; z < ZMAX; ++z) {
+            if (z < Zs) {
+                const cplx<R> ex = b[(z * 3 + 0) * MC], ey = b[(z * 3 + 1) * MC];
+                av[z] = ex * kx + ey * ky;
+                zv[z] = b[(z * 3 + 2) * MC];
+            } else {
+                av[z] = mk<R>(R(0), R(0));
+                zv[z] = mk<R>(R(0), R(0));
             }
         }
-        __syncthreads();
-        if (act) {
-            const cplx<R>* tp = taps + (size_t(ix) * n + ky_i) * 3 * nd + (Zs - 1);   // tp[k nd + d]
-            cplx<R>* b = S + size_t(ky_i) * NCOL + mi;
-            // u = t0 * a + t1 * E_z  ->  E_x = kx u, E_y = ky u;  then E_z = t1 * a + t2 * E_z
+        const cplx<R>* tp = taps + (size_t(ix) * n + ky_i) * 3 * nd + (Zs - 1);   // tp[k nd + d]
 #pragma unroll
-            for (int part = 0; part < 2; ++part) {
-                const cplx<R>* ta = tp + part * nd;         // t0 | t1 on a
-                const cplx<R>* tb = tp + (part + 1) * nd;   // t1 | t2 on E_z
-                cplx<R> acc[ZMAX];
+        for (int part = 0; part < 2; ++part) {
+            const cplx<R>* ta = tp + part * nd;         // t0 | t1 on a
+            const cplx<R>* tb = tp + (part + 1) * nd;   // t1 | t2 on E_z
+            cplx<R> acc[ZMAX];
 #pragma unroll
-                for (int zo = 0; zo < ZMAX; ++zo) acc[zo] = mk<R>(R(0), R(0));
+            for (int zo = 0; zo < ZMAX; ++zo) acc[zo] = mk<R>(R(0), R(0));
 #pragma unroll
-                for (int d = -(ZMAX - 1); d <= ZMAX - 1; ++d) {
-                    if (d < -(Zs - 1) || d > Zs - 1) continue;
-                    const cplx<R> ka = ta[d], kb = tb[d];
-#pragma unroll
-                    for (int zo = 0; zo < ZMAX; ++zo) {
-                        const int zi = zo - d;
-                        if (zi >= 0 && zi < ZMAX) {
-                            acc[zo].x = fma(ka.x, av[zi].x, acc[zo].x);
-                            acc[zo].x = fma(-ka.y, av[zi].y, acc[zo].x);
-                            acc[zo].y = fma(ka.x, av[zi].y, acc[zo].y);
-                            acc[zo].y = fma(ka.y, av[zi].x, acc[zo].y);
-                            acc[zo].x = fma(kb.x, zv[zi].x, acc[zo].x);
-                            acc[zo].x = fma(-kb.y, zv[zi].y, acc[zo].x);
-                            acc[zo].y = fma(kb.x, zv[zi].y, acc[zo].y);
-                            acc[zo].y = fma(kb.y, zv[zi].x, acc[zo].y);
-                        }
-                    }
-                }
+            for (int d = -(ZMAX - 1); d <= ZMAX - 1; ++d) {
+                if (d < -(Zs - 1) || d > Zs - 1) continue;
+                const cplx<R> ka = ta[d], kb = tb[d];
 #pragma unroll
                 for (int zo = 0; zo < ZMAX; ++zo) {
-                    if (zo < Zs) {
-                        if (part == 0) {
-                            b[(zo * 3 + 0) * MC] = acc[zo] * kx;
-                            b[(zo * 3 + 1) * MC] = acc[zo] * ky;
-                        } else {
-                            b[(zo * 3 + 2) * MC] = acc[zo];
-                        }
+                    const int zi = zo - d;
+                    if (zi >= 0 && zi < ZMAX) {
+                        acc[zo].x = fma(ka.x, av[zi].x, acc[zo].x);
+                        acc[zo].x = fma(-ka.y, av[zi].y, acc[zo].x);
+                        acc[zo].y = fma(ka.x, av[zi].y, acc[zo].y);
+                        acc[zo].y = fma(ka.y, av[zi].x, acc[zo].y);
+                        acc[zo].x = fma(kb.x, zv[zi].x, acc[zo].x);
+                        acc[zo].x = fma(-kb.y, zv[zi].y, acc[zo].x);
+                        acc[zo].y = fma(kb.x, zv[zi].y, acc[zo].y);
+                        acc[zo].y = fma(kb.y, zv[zi].x, acc[zo].y);
+                    }
+                }
+            }
+#pragma unroll
+            for (int zo = 0; zo < ZMAX; ++zo) {
+                if (zo < Zs) {
+                    if (part == 0) {
+                        b[(zo * 3 + 0) * MC] = acc[zo] * kx;
+                        b[(zo * 3 + 1) * MC] = acc[zo] * ky;
+                    } else {
+                        b[(zo * 3 + 2) * MC] = acc[zo];
                     }
                 }
             }
         }
-        __syncthreads();
     }
-    slab_ytransform<R, true, CLS, NT>(S, T, r1, r2, NCOL);
-    for (int t = threadIdx.x; t < tot; t += NT) {
+    __syncthreads();
+    slab_ytransform<R, true, CLS>(S, S2, T, r1, r2, NCOL);
+    for (int t = threadIdx.x; t < tot; t += kSlabThreads) {
         const int mi = t % MC;
         if (mi < mc) {
             const int r = t / MC;
@@ -1520,14 +1499,12 @@ void AxisFFT::run_scaled(cplx<R>* data, size_t es, int ncols, size_t os, int nou
     launch_line<R>(data, es, ncols, os, nouter, 2, scale, sz, sb, s);
 }
 
+size_t slab_smem(int n, int Zs, int mc, size_t elem) { return (2 * size_t(n) * Zs * 3 * mc + n) * elem; }
+
 bool AxisFFT::slab_ok(int Zs, bool fp64) const {
     if (kind_ != 1 || force_general_ || Zs < 1 || Zs > 16) return false;
     const int mc = fp64 ? slab_mc<double>(Zs == 1) : slab_mc<float>(Zs == 1);
-    const size_t elem = fp64 ? sizeof(double2) : sizeof(float2);
-    const size_t shm = (size_t(f_.n) * Zs * 3 * mc + f_.n) * elem;
-    // both passes need at least one column per round
-    const int nt = fp64 ? slab_threads<double>() : slab_threads<float>();
-    return shm <= kFftSmemBudget && nt >= std::max(r1_, r2_) && register_class(r1_) <= 16;
+    return slab_smem(f_.n, Zs, mc, fp64 ? sizeof(double2) : sizeof(float2)) <= kFftSmemBudget;
 }
 
 template <typename R>
@@ -1536,10 +1513,9 @@ void AxisFFT::run_slab(cplx<R>* data, int nx, int Zs, int M, const cplx<R>* taps
     if (!slab_ok(Zs, sizeof(R) == 8)) throw std::runtime_error("run_slab: slab not supported by this axis");
     if (nx <= 0 || M <= 0) return;
     constexpr int MC1 = slab_mc<R>(true), MCS = slab_mc<R>(false);
-    constexpr int NT = slab_threads<R>();
     const int MC = Zs == 1 ? MC1 : MCS;
     const int n = f_.n;
-    const size_t shm = (size_t(n) * Zs * 3 * MC + n) * sizeof(cplx<R>);
+    const size_t shm = slab_smem(n, Zs, MC, sizeof(cplx<R>));
     SlabArgs a;
     a.Nx = nx;
     a.Zs = Zs;
@@ -1552,7 +1528,7 @@ void AxisFFT::run_slab(cplx<R>* data, int nx, int Zs, int M, const cplx<R>* taps
     const int cls = register_class(r1_);
     auto go = [&](auto kern) {
         MPM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(shm)));
-        kern<<<nx * a.nchunk, NT, shm, s>>>(data, tw, taps, r1_, r2_, a);
+        kern<<<nx * a.nchunk, kSlabThreads, shm, s>>>(data, tw, taps, r1_, r2_, a);
     };
     if (Zs == 1) {
         if (cls == 8) go(k_slab<R, MC1, 1, 8>);

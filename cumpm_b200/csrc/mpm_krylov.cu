@@ -152,78 +152,206 @@ __global__ void k_normalize(const double2* __restrict__ src, double2* __restrict
     dst[t] = (st[m].cyc && d > 0.0) ? src[t] * (1.0 / d) : make_double2(0, 0);
 }
 
-// h += h2
-__global__ void k_addto(double2* __restrict__ a, const double2* __restrict__ b, int n) {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t < n) a[t] += b[t];
-}
+// ----------------------------------------------- fused Arnoldi-step kernels --
+//
+// CGS2 with the per-step reductions fused into the passes that produce their
+// inputs: (1) h = V^H w (k_dots1 + k_dots2); (2) w -= V h and the partial
+// sums of h2 = V^H w over the same rows (k_arn_update_dots) + k_dots2;
+// (3) w -= V h2 and the partial sums of |w|^2 (k_arn_update_norm); (4) one
+// CTA per step (k_arn_finish): |w|, h += h2, the Givens update of every
+// column and the count of columns still cycling.  Row blocks of
+// 8 x kArnRows rows by 32 columns; every sum is taken in a fixed order.
+constexpr int kArnRows = 4;   // rows per thread
 
-// Hessenberg column k, previous rotations, new rotation, residual estimate
-// (gmres_solver.cu:120-184), one thread per RHS.
-__global__ void k_gm_givens(GState* __restrict__ st, const double2* __restrict__ h, const double* __restrict__ wn,
-                            double2* __restrict__ H, double2* __restrict__ g, double* __restrict__ cs,
-                            double2* __restrict__ sn, int k, int restart, int M, const double* __restrict__ bn,
-                            double tol, const double* __restrict__ tolv, int maxiter, int* __restrict__ flag) {
-    const int m = blockIdx.x * blockDim.x + threadIdx.x;
-    if (m >= M) return;
-    GState s = st[m];
-    if (!s.cyc) {
-        flag[1 + m] = 0;
-        return;
-    }
-    const int ld = restart + 1;
-    double2* Hm = H + size_t(m) * ld * restart;   // column-major: Hm[col*ld + row]
-    double2* gm = g + size_t(m) * ld;
-    double* csm = cs + size_t(m) * restart;
-    double2* snm = sn + size_t(m) * restart;
-    double2* col = Hm + size_t(k) * ld;
-    for (int i = 0; i <= k; ++i) col[i] = h[size_t(i) * M + m];
-    col[k + 1] = make_double2(wn[m], 0.0);
-    for (int i = 0; i < k; ++i) {
-        const double2 h1 = col[i], h2 = col[i + 1];
-        const double c = csm[i];
-        const double2 sv = snm[i];
-        const double2 cs_ = make_double2(sv.x, -sv.y);
-        col[i] = h1 * c + cs_ * h2;
-        col[i + 1] = (sv * h1) * -1.0 + h2 * c;
-    }
-    const double2 h1 = col[k], h2 = col[k + 1];
-    double c = 1.0;
-    double2 sv = make_double2(0, 0);
-    if (h2.x != 0.0 || h2.y != 0.0) {
-        const double a1 = hypot(h1.x, h1.y);
-        if (a1 == 0.0) {
-            c = 0.0;
-            sv = make_double2(1.0, 0.0);
-        } else {
-            const double a2 = hypot(h2.x, h2.y);
-            const double sc = a1 + a2;
-            const double n1 = a1 / sc, n2 = a2 / sc;
-            const double hh = sc * sqrt(n1 * n1 + n2 * n2);
-            c = a1 / hh;
-            // (conj(h1)/|h1|) * (h2/hh)
-            const double2 u = make_double2(h1.x / a1, -h1.y / a1);
-            sv = u * make_double2(h2.x / hh, h2.y / hh);
+__device__ __forceinline__ int arn_rows(int rows, int bx) { return bx * 8 * kArnRows; }
+
+// w[row][m] -= sum_{i < nvec} V_i[row][m] h[i][m] over this CTA's rows, kept
+// in registers; then partial[bx][i][m] = sum over those rows of
+// conj(V_i) w (NORM = false) or partial[bx][m] = sum |w|^2 (NORM = true)
+template <bool NORM>
+__global__ void __launch_bounds__(256, 2) k_arn_update(double2* __restrict__ w, const double2* __restrict__ V,
+                                                    size_t vstride, int nvec, const double2* __restrict__ h,
+                                                    int rows, int M, double2* __restrict__ partial) {
+    __shared__ double2 red[8][8][32];
+    const int m = blockIdx.y * 32 + threadIdx.x;
+    const int r0 = arn_rows(rows, blockIdx.x) + threadIdx.y;
+    double2 wr[kArnRows];
+#pragma unroll
+    for (int j = 0; j < kArnRows; ++j) {
+        const int row = r0 + 8 * j;
+        wr[j] = make_double2(0, 0);
+        if (m < M && row < rows) {
+            const size_t o = size_t(row) * M + m;
+            double2 acc = make_double2(0, 0);
+            for (int i = 0; i < nvec; ++i) acc += V[size_t(i) * vstride + o] * h[size_t(i) * M + m];
+            wr[j] = w[o] - acc;
+            w[o] = wr[j];
         }
     }
-    csm[k] = c;
-    snm[k] = sv;
-    const double2 scj = make_double2(sv.x, -sv.y);
-    col[k] = h1 * c + scj * h2;
-    col[k + 1] = make_double2(0, 0);
-    const double2 g1 = gm[k], g2 = gm[k + 1];
-    gm[k] = g1 * c + scj * g2;
-    gm[k + 1] = (sv * g1) * -1.0 + g2 * c;
-    s.iters += 1;
-    const double resid = hypot(gm[k + 1].x, gm[k + 1].y);
-    if (resid < col_tol(tol, tolv, m) * bn[m] || k + 1 >= restart || s.iters >= maxiter) {
-        s.cyc = 0;
-        s.kcount = k + 1;
+    if constexpr (NORM) {
+        double s = 0.0;
+#pragma unroll
+        for (int j = 0; j < kArnRows; ++j) s += wr[j].x * wr[j].x + wr[j].y * wr[j].y;
+        red[0][threadIdx.y][threadIdx.x] = make_double2(s, 0.0);
+        __syncthreads();
+        if (threadIdx.y == 0 && m < M) {
+            double t = 0.0;
+            for (int r = 0; r < 8; ++r) t += red[0][r][threadIdx.x].x;
+            partial[size_t(blockIdx.x) * M + m] = make_double2(t, 0.0);
+        }
     } else {
-        atomicAdd(flag, 1);
+        for (int i0 = 0; i0 < nvec; i0 += 8) {
+            const int nv = min(8, nvec - i0);
+            double2 acc[8];
+#pragma unroll
+            for (int k = 0; k < 8; ++k) acc[k] = make_double2(0, 0);
+#pragma unroll
+            for (int j = 0; j < kArnRows; ++j) {
+                const int row = r0 + 8 * j;
+                if (m < M && row < rows) {
+                    const size_t o = size_t(row) * M + m;
+#pragma unroll
+                    for (int k = 0; k < 8; ++k)
+                        if (k < nv) acc[k] += conjmul(V[size_t(i0 + k) * vstride + o], wr[j]);
+                }
+            }
+#pragma unroll
+            for (int k = 0; k < 8; ++k) red[k][threadIdx.y][threadIdx.x] = acc[k];
+            __syncthreads();
+            if (threadIdx.y < nv && m < M) {
+                double2 t = make_double2(0, 0);
+                for (int r = 0; r < 8; ++r) t += red[threadIdx.y][r][threadIdx.x];
+                partial[(size_t(blockIdx.x) * nvec + i0 + threadIdx.y) * M + m] = t;
+            }
+            __syncthreads();
+        }
     }
-    flag[1 + m] = s.cyc;
-    st[m] = s;
+}
+
+// partial[bx][i][m] = sum over the CTA's rows of conj(V_i) w (no update)
+__global__ void __launch_bounds__(256, 2) k_arn_dots(const double2* __restrict__ V, size_t vstride, int nvec,
+                                                  const double2* __restrict__ w, int rows, int M,
+                                                  double2* __restrict__ partial) {
+    __shared__ double2 red[8][8][32];
+    const int m = blockIdx.y * 32 + threadIdx.x;
+    const int r0 = arn_rows(rows, blockIdx.x) + threadIdx.y;
+    double2 wr[kArnRows];
+#pragma unroll
+    for (int j = 0; j < kArnRows; ++j) {
+        const int row = r0 + 8 * j;
+        wr[j] = (m < M && row < rows) ? w[size_t(row) * M + m] : make_double2(0, 0);
+    }
+    for (int i0 = 0; i0 < nvec; i0 += 8) {
+        const int nv = min(8, nvec - i0);
+        double2 acc[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) acc[k] = make_double2(0, 0);
+#pragma unroll
+        for (int j = 0; j < kArnRows; ++j) {
+            const int row = r0 + 8 * j;
+            if (m < M && row < rows) {
+                const size_t o = size_t(row) * M + m;
+#pragma unroll
+                for (int k = 0; k < 8; ++k)
+                    if (k < nv) acc[k] += conjmul(V[size_t(i0 + k) * vstride + o], wr[j]);
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < 8; ++k) red[k][threadIdx.y][threadIdx.x] = acc[k];
+        __syncthreads();
+        if (threadIdx.y < nv && m < M) {
+            double2 t = make_double2(0, 0);
+            for (int r = 0; r < 8; ++r) t += red[threadIdx.y][r][threadIdx.x];
+            partial[(size_t(blockIdx.x) * nvec + i0 + threadIdx.y) * M + m] = t;
+        }
+        __syncthreads();
+    }
+}
+
+// One CTA: |w| from the row-block partials, h += h2, the Givens update of
+// every column (Hessenberg column k, the previous rotations, a new rotation
+// and the residual estimate, gmres_solver.cu:120-184) and flag[0] = the
+// number of columns still cycling.
+__global__ void __launch_bounds__(1024) k_arn_finish(GState* __restrict__ st, double2* __restrict__ h,
+                                                     const double2* __restrict__ h2,
+                                                     const double2* __restrict__ pnorm, int gx,
+                                                     double* __restrict__ wn, double2* __restrict__ H,
+                                                     double2* __restrict__ g, double* __restrict__ cs,
+                                                     double2* __restrict__ sn, int k, int restart, int M,
+                                                     const double* __restrict__ bn, double tol,
+                                                     const double* __restrict__ tolv, int maxiter,
+                                                     int* __restrict__ flag) {
+    __shared__ int total;
+    if (threadIdx.x == 0) total = 0;
+    __syncthreads();
+    int cycling = 0;
+    for (int m = threadIdx.x; m < M; m += blockDim.x) {
+        double ss = 0.0;
+        for (int b = 0; b < gx; ++b) ss += pnorm[size_t(b) * M + m].x;
+        const double wnm = sqrt(fmax(ss, 0.0));
+        wn[m] = wnm;
+        for (int i = 0; i <= k; ++i) h[size_t(i) * M + m] += h2[size_t(i) * M + m];
+        GState s = st[m];
+        if (!s.cyc) {
+            flag[1 + m] = 0;
+            continue;
+        }
+        const int ld = restart + 1;
+        double2* Hm = H + size_t(m) * ld * restart;
+        double2* gm = g + size_t(m) * ld;
+        double* csm = cs + size_t(m) * restart;
+        double2* snm = sn + size_t(m) * restart;
+        double2* col = Hm + size_t(k) * ld;
+        for (int i = 0; i <= k; ++i) col[i] = h[size_t(i) * M + m];
+        col[k + 1] = make_double2(wnm, 0.0);
+        for (int i = 0; i < k; ++i) {
+            const double2 h1 = col[i], hh2 = col[i + 1];
+            const double c = csm[i];
+            const double2 sv = snm[i];
+            const double2 cs_ = make_double2(sv.x, -sv.y);
+            col[i] = h1 * c + cs_ * hh2;
+            col[i + 1] = (sv * h1) * -1.0 + hh2 * c;
+        }
+        const double2 h1 = col[k], hh2 = col[k + 1];
+        double c = 1.0;
+        double2 sv = make_double2(0, 0);
+        if (hh2.x != 0.0 || hh2.y != 0.0) {
+            const double a1 = hypot(h1.x, h1.y);
+            if (a1 == 0.0) {
+                c = 0.0;
+                sv = make_double2(1.0, 0.0);
+            } else {
+                const double a2 = hypot(hh2.x, hh2.y);
+                const double sc = a1 + a2;
+                const double n1 = a1 / sc, n2 = a2 / sc;
+                const double hh = sc * sqrt(n1 * n1 + n2 * n2);
+                c = a1 / hh;
+                const double2 u = make_double2(h1.x / a1, -h1.y / a1);
+                sv = u * make_double2(hh2.x / hh, hh2.y / hh);
+            }
+        }
+        csm[k] = c;
+        snm[k] = sv;
+        const double2 scj = make_double2(sv.x, -sv.y);
+        col[k] = h1 * c + scj * hh2;
+        col[k + 1] = make_double2(0, 0);
+        const double2 g1 = gm[k], g2 = gm[k + 1];
+        gm[k] = g1 * c + scj * g2;
+        gm[k + 1] = (sv * g1) * -1.0 + g2 * c;
+        s.iters += 1;
+        const double resid = hypot(gm[k + 1].x, gm[k + 1].y);
+        if (resid < col_tol(tol, tolv, m) * bn[m] || k + 1 >= restart || s.iters >= maxiter) {
+            s.cyc = 0;
+            s.kcount = k + 1;
+        } else {
+            ++cycling;
+        }
+        flag[1 + m] = s.cyc;
+        st[m] = s;
+    }
+    if (cycling) atomicAdd(&total, cycling);
+    __syncthreads();
+    if (threadIdx.x == 0) flag[0] = total;
 }
 
 // back substitution H y = g, y stored [i][m]
@@ -603,6 +731,9 @@ void BatchSolver::gmres(Field& F, const double2* b, double2* x, int M, const dou
     int* dflag = flagdev_.as<int>();
     const int mb = nblk(M, 128);
     const int vb = nblk((long long)n, 256);
+    // fused Arnoldi kernels: row blocks of 8 x kArnRows rows
+    const int agx = std::max(1, (rows + 8 * kArnRows - 1) / (8 * kArnRows));
+    partial_.ensure(sizeof(double2) * size_t(agx) * (restart + 1) * M);
 
     norms(b, rows, M, bnorm_.as<double>(), s);
     k_gm_init<<<mb, 128, 0, s>>>(gs, bnorm_.as<double>(), M);
@@ -646,29 +777,30 @@ void BatchSolver::gmres(Field& F, const double2* b, double2* x, int M, const dou
             double2* w = w_.as<double2>();
             st.column_matvecs += apply_cols(F, Vk, w, M, sc, opt.jacobi, r32, re32, cyc.data(), opt.compact, s);
             st.matvecs++;
-            // CGS2
-            dots(V, n, k + 1, w, rows, M, 1, h_.as<double2>(), s);
+            // CGS2, the reductions fused into the passes that feed them
             {
                 StageScope sc1(ST_KRYLOV, s);
-                k_vupdate<<<vb, 256, 0, s>>>(w, V, n, k + 1, h_.as<double2>(), rows, M, -1.0, nullptr);
+                const dim3 grd(agx, (M + 31) / 32), blk(32, 8);
+                double2* part = partial_.as<double2>();
+                k_arn_dots<<<grd, blk, 0, s>>>(V, n, k + 1, w, rows, M, part);
+                MPM_LAUNCH();
+                k_dots2<<<nblk((long long)(k + 1) * M * 32, 256), 256, 0, s>>>(part, agx, k + 1, M, h_.as<double2>());
+                MPM_LAUNCH();
+                k_arn_update<false><<<grd, blk, 0, s>>>(w, V, n, k + 1, h_.as<double2>(), rows, M, part);
+                MPM_LAUNCH();
+                k_dots2<<<nblk((long long)(k + 1) * M * 32, 256), 256, 0, s>>>(part, agx, k + 1, M,
+                                                                              h2_.as<double2>());
+                MPM_LAUNCH();
+                k_arn_update<true><<<grd, blk, 0, s>>>(w, V, n, k + 1, h2_.as<double2>(), rows, M, part);
+                MPM_LAUNCH();
+                k_arn_finish<<<1, std::min(1024, ((M + 31) / 32) * 32), 0, s>>>(
+                    gs, h_.as<double2>(), h2_.as<double2>(), part, agx, rnorm_.as<double>(), H_.as<double2>(),
+                    g_.as<double2>(), cs_.as<double>(), sn_.as<double2>(), k, restart, M, bnorm_.as<double>(), opt.tol,
+                    tolv, opt.maxiter, dflag);
+                MPM_LAUNCH();
+                k_normalize<<<vb, 256, 0, s>>>(w, V + size_t(k + 1) * n, rnorm_.as<double>(), gs, n, M);
                 MPM_LAUNCH();
             }
-            dots(V, n, k + 1, w, rows, M, 1, h2_.as<double2>(), s);
-            {
-                StageScope sc2(ST_KRYLOV, s);
-                k_vupdate<<<vb, 256, 0, s>>>(w, V, n, k + 1, h2_.as<double2>(), rows, M, -1.0, nullptr);
-                MPM_LAUNCH();
-                k_addto<<<nblk((k + 1) * M, 128), 128, 0, s>>>(h_.as<double2>(), h2_.as<double2>(), (k + 1) * M);
-                MPM_LAUNCH();
-            }
-            norms(w, rows, M, rnorm_.as<double>(), s);
-            k_normalize<<<vb, 256, 0, s>>>(w, V + size_t(k + 1) * n, rnorm_.as<double>(), gs, n, M);
-            MPM_LAUNCH();
-            MPM_CUDA(cudaMemsetAsync(dflag, 0, sizeof(int), s));
-            k_gm_givens<<<mb, 128, 0, s>>>(gs, h_.as<double2>(), rnorm_.as<double>(), H_.as<double2>(),
-                                           g_.as<double2>(), cs_.as<double>(), sn_.as<double2>(), k, restart, M,
-                                           bnorm_.as<double>(), opt.tol, tolv, opt.maxiter, dflag);
-            MPM_LAUNCH();
             if (read_flags(dflag, M, s) == 0) break;
             cyc.assign(flag_ + 1, flag_ + 1 + M);
         }

@@ -12,7 +12,7 @@ def test_solution_file_rebuilds_the_run(tmp_path):
 
     sp = 12.0
     pos = np.array([[(i + 0.5 * (j % 2)) * sp, j * np.sqrt(3) / 2 * sp, 0.0] for j in range(4) for i in range(6)])
-    box = np.array([6 * sp, 4 * sp * np.sqrt(3) / 2, 200.0])
+    box = np.array([100.0, 100.0, 200.0])
     omega = np.array([0.5, 0.7])
     eps = cuMPM.drude_dielectric(omega, 0.1, 1.8, 4.0)
     s = cuMPM.dipole_solver(box, eps, radius=5.0, eps_m=1.77, tol=1e-8, quiet=True, precision="double")
