@@ -491,6 +491,7 @@ def run_ours(args, rank, world, local_rank):
                 "krylov_steps_per_rhs": round(float(np.mean(iters)), 2),
                 "matvecs_per_step": mv_per_step,
                 "column_matvecs_per_step": colmv_per_step,
+                "reorth_steps_per_step": sum(r["reorth_steps"] for r in timed_reports) / max(1, len(timed_reports)),
                 "inner_tol": f"max({args.inner_tol:g}, 0.5 tol |b_m| / |r_m|) per column",
                 "compact_batch": not args.no_compact,
                 "grid": info["grid"], "pruned_z_slots": info["z_slots"] if info["pruned"] else None,

@@ -49,7 +49,7 @@ class SolveOptions(C.Structure):
 class SolveReport(C.Structure):
     _fields_ = [("matvecs", C.c_int), ("refine_steps", C.c_int), ("total_iterations", C.c_int),
                 ("max_iterations", C.c_int), ("num_converged", C.c_int), ("max_rel_resid", C.c_double),
-                ("column_matvecs", C.c_longlong)]
+                ("column_matvecs", C.c_longlong), ("reorth_steps", C.c_int)]
 
 
 class FieldInfo(C.Structure):

@@ -330,6 +330,7 @@ int mpm_batch_solve(mpm_field* f, const void* B, void* X, int M, const void* sc,
             rep->matvecs = st.matvecs;
             rep->refine_steps = st.refine_steps;
             rep->column_matvecs = st.column_matvecs;
+            rep->reorth_steps = st.reorth_steps;
             for (int m = 0; m < M; ++m) {
                 rep->total_iterations += st.iters[m];
                 rep->max_iterations = std::max(rep->max_iterations, st.iters[m]);

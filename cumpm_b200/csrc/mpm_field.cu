@@ -578,8 +578,11 @@ __global__ void k_build_scale(ScaleArgs a, int quads, double* __restrict__ s64, 
 
 // Pruned layout: Toeplitz kernel over the occupied planes for each (kx, ky)
 // column, K_ab(d) = sum_kz exp(+2 pi i kz d / Nz) S(k) khat_a khat_b for the
-// six symmetric ab pairs and d in [-(Z-1), Z-1].  Computed in float64.
-__global__ void k_build_column(ScaleArgs a, int Z, double2* __restrict__ K64, float2* __restrict__ K32) {
+// six symmetric ab pairs and d in [-(Z-1), Z-1]; for a single layer
+// (Z = 1, w2 given) the z-weighted K_ab = sum_kz |W(kz)|^2 S khat_a khat_b.
+// Computed in float64.
+__global__ void k_build_column(ScaleArgs a, int Z, const double* __restrict__ w2, double2* __restrict__ K64,
+                               float2* __restrict__ K32) {
     extern __shared__ double sh[];
     const int col = blockIdx.x;
     const int ix = col / a.Ny, iy = col % a.Ny;
@@ -592,7 +595,8 @@ __global__ void k_build_column(ScaleArgs a, int Z, double2* __restrict__ K64, fl
         scale_coefs(ix, iy, iz, a.Nx, a.Ny, Nz, a.Lx, a.Ly, a.Lz, a.xi, a.eta, V, o);
         double kx, ky, kz;
         khat_at<double>(ix, iy, iz, a.Nx, a.Ny, Nz, a.Lx, a.Ly, a.Lz, kx, ky, kz);
-        const double s = o[0];
+        // single layer (Z = 1): weighted by |sum_o w_o exp(-2 pi i kz o / Nz)|^2
+        const double s = w2 ? o[0] * w2[iz] : o[0];
         C6[iz * 6 + 0] = s * kx * kx; C6[iz * 6 + 1] = s * kx * ky; C6[iz * 6 + 2] = s * kx * kz;
         C6[iz * 6 + 3] = s * ky * ky; C6[iz * 6 + 4] = s * ky * kz; C6[iz * 6 + 5] = s * kz * kz;
         double sn, cs;
@@ -762,14 +766,17 @@ __global__ void k_column(cplx<R>* __restrict__ grid, const cplx<R>* __restrict__
 
 // Contraction: field at each target from its Gaussian stencil for all B
 // columns (contract_kernel, monodisperse_ewald_electric_field.cu:1488-1587).
-// Writes Y rows (overwrites).  C = 3 (dipoles) or 8 (plus field gradient).
-// SZ > 0: the stencil's z run (g.Sz <= SZ) unrolled, so that its grid loads
-// are in flight together; SZ = 0: any stencil length.
+// Writes Y rows (overwrites), or with `accumulate` adds to the dipole rows
+// already in Y (the real-space part, computed concurrently) and, when jsc
+// is given, scales the sum by the Jacobi factor 1/s of the target and
+// column.  C = 3 (dipoles) or 8 (plus field gradient).  SZ > 0: the
+// stencil's z run (g.Sz <= SZ) unrolled, so that its grid loads are in
+// flight together; SZ = 0: any stencil length.
 template <typename R, int SZ>
 __global__ void k_contract(const cplx<R>* __restrict__ grid, GridView g, int M, int C, int Nt,
                            const int4* __restrict__ base, const R* __restrict__ w1, double factor,
                            const int* __restrict__ quad_map, double2* __restrict__ Y, int negate,
-                           const int* __restrict__ order) {
+                           const int* __restrict__ order, int accumulate, const double2* __restrict__ jsc) {
     __shared__ R w[3 * kMaxStencil];
     __shared__ int idx[3 * kMaxStencil];
     // targets in spatial-bin order when given: CTAs that run together share
@@ -833,6 +840,14 @@ __global__ void k_contract(const cplx<R>* __restrict__ grid, GridView g, int M, 
         if (negate) { v.x = -v.x; v.y = -v.y; }
         const int m = b - comp * M;
         const size_t row = (comp < 3) ? size_t(3 * j + comp) : size_t(3 * Nt + 5 * q + comp - 3);
+        if (accumulate && comp < 3) {
+            v += Y[row * M + m];
+            if (jsc) {
+                const double2 sv = jsc[size_t(j) * M + m];
+                const double den = sv.x * sv.x + sv.y * sv.y;
+                if (den > 1e-30) v = v * make_double2(sv.x / den, -sv.y / den);
+            }
+        }
         Y[row * M + m] = v;
     }
 }
@@ -1288,6 +1303,9 @@ Field::Field(const FieldSpec& spec) : spec_(spec) {
 
 Field::~Field() {
     for (auto& p : plans_) cufftDestroy(p.h);
+    if (ev_fork_) cudaEventDestroy(ev_fork_);
+    if (ev_join_) cudaEventDestroy(ev_join_);
+    if (aux_) cudaStreamDestroy(aux_);
 }
 
 FieldStats Field::stats() const {
@@ -1406,7 +1424,7 @@ void Field::choose_layout(cudaStream_t) {
                 const double gd = d0 + (o - gv_.off) * hz;
                 layer_w_[o] = std::exp(-2.0 * spec_.xi * spec_.xi * gd * gd / geom_.eta[2]);
             }
-            if (pmod(int(g0), Nz) != layer_key_g_ || d0 != layer_key_d_) layer_taps_ = false;
+            if (pmod(int(g0), Nz) != layer_key_g_ || d0 != layer_key_d_) layer_taps_ = layer_colK_ = false;
             layer_key_g_ = pmod(int(g0), Nz);
             layer_key_d_ = d0;
             return;
@@ -1637,9 +1655,25 @@ void Field::build_column_kernel(cudaStream_t s) {
     const size_t shm = sizeof(double) * 8 * gv_.Nz;
     if (shm > 48 * 1024)
         MPM_CUDA(cudaFuncSetAttribute(k_build_column, cudaFuncAttributeMaxDynamicSharedMemorySize, int(shm)));
-    k_build_column<<<ncol, 128, shm, s>>>(a, Z, colK64_.as<double2>(), colK32_.as<float2>());
+    const double* w2 = nullptr;
+    if (gv_.layer) {
+        layer_wd_.ensure(sizeof(double) * (gv_.S + gv_.Nz));
+        double* wd = layer_wd_.as<double>();
+        MPM_CUDA(cudaMemcpyAsync(wd, layer_w_.data(), sizeof(double) * gv_.S, cudaMemcpyHostToDevice, s));
+        k_layer_w2<<<nblk(gv_.Nz, 128), 128, 0, s>>>(wd, gv_.S, gv_.Nz, wd + gv_.S);
+        MPM_LAUNCH();
+        w2 = wd + gv_.S;
+    }
+    k_build_column<<<ncol, 128, shm, s>>>(a, Z, w2, colK64_.as<double2>(), colK32_.as<float2>());
     MPM_LAUNCH();
-    colK_Z_ = Z;
+    if (gv_.layer) {
+        MPM_CUDA(cudaStreamSynchronize(s));   // layer_w_ is read by the copy above
+        layer_colK_ = true;
+        colK_Z_ = -1;
+    } else {
+        layer_colK_ = false;
+        colK_Z_ = Z;
+    }
 }
 
 bool Field::use_slab() const {
@@ -1699,7 +1733,7 @@ void Field::precalc(cudaStream_t s) {
         if (use_slab()) {
             if (gv_.layer ? !layer_taps_ : slab_Z_ != gv_.Zs) build_slab_taps(s);
         } else if (gv_.pruned) {
-            if (colK_Z_ != gv_.Zs) build_column_kernel(s);
+            if (gv_.layer ? !layer_colK_ : colK_Z_ != gv_.Zs) build_column_kernel(s);
         } else if (scale_built_ != (Nq_ ? 4 : 1)) {
             build_scale(s);
         }
@@ -1759,10 +1793,10 @@ template void Field::transform<float>(cplx<float>*, int, bool, cudaStream_t);
 template void Field::transform<double>(cplx<double>*, int, bool, cudaStream_t);
 
 template <typename R>
-void Field::recip(const double2* X, double2* Y, int M, cudaStream_t s) {
+void Field::recip(const double2* X, double2* Y, int M, cudaStream_t s, const RealOverlap* ov) {
     grid_.ensure(grid_bytes(M, sizeof(R) == 8));
     if (spec_.kind == FIELD_POLY) poly_recip_on<R>(X, Y, M, grid_.as<cplx<R>>(), s);
-    else recip_on<R>(X, Y, M, grid_.as<cplx<R>>(), s);
+    else recip_on<R>(X, Y, M, grid_.as<cplx<R>>(), s, ov);
 }
 
 size_t Field::grid_bytes(int M, bool fp64) const {
@@ -1772,7 +1806,7 @@ size_t Field::grid_bytes(int M, bool fp64) const {
 
 // Reciprocal-space part on a caller-provided grid of grid_bytes(M) bytes.
 template <typename R>
-void Field::recip_on(const double2* X, double2* Y, int M, cplx<R>* grid, cudaStream_t s) {
+void Field::recip_on(const double2* X, double2* Y, int M, cplx<R>* grid, cudaStream_t s, const RealOverlap* ov) {
     const int C = Nq_ ? 8 : 3;
     const int B = C * M;
     // spread
@@ -1870,10 +1904,12 @@ void Field::recip_on(const double2* X, double2* Y, int M, cplx<R>* grid, cudaStr
     const double factor = geom_.h[0] * geom_.h[1] * geom_.h[2];
     const R* tw = sizeof(R) == 4 ? reinterpret_cast<const R*>(tg.w32.p) : reinterpret_cast<const R*>(tg.w64.p);
     const int thr = std::min(256, ((B + 31) / 32) * 32);
+    if (ov) MPM_CUDA(cudaStreamWaitEvent(s, ov->join, 0));   // the real-space part is in Y
     auto contract = [&](auto kern) {
         kern<<<nt, thr, 0, s>>>(grid, gv_, M, C, nt, tg.base.as<int4>(), tw, factor,
                                 spec_.solver_ax ? quad_map_.as<int>() : nullptr, Y, 0,
-                                spec_.solver_ax ? sources_.idx_sorted.as<int>() : nullptr);
+                                spec_.solver_ax ? sources_.idx_sorted.as<int>() : nullptr, ov ? 1 : 0,
+                                ov ? ov->jacobi_sc : nullptr);
     };
     if (gv_.Sz == 1) contract(k_contract<R, 1>);
     else if (gv_.Sz <= 9) contract(k_contract<R, 9>);
@@ -1937,6 +1973,25 @@ void Field::apply(const double2* X, double2* Y, int M, const double2* sc, bool j
     if (!spec_.solver_ax && targets_.n == 0) throw std::runtime_error("Field::apply without field points");
     if (spec_.kind == FIELD_DIRECT) {
         direct(X, Y, M, sc, jacobi, recip_fp32, s);
+        return;
+    }
+    if (spec_.kind == FIELD_MONO && spec_.solver_ax && Nq_ == 0) {
+        // the real-space sum runs on a second stream while the reciprocal
+        // chain (spread, transforms, k-space step) runs on s; it writes the
+        // pairs and self terms into Y, and the contraction, after waiting
+        // for it, adds the reciprocal part and applies the Jacobi scaling
+        if (!aux_) {
+            MPM_CUDA(cudaStreamCreateWithFlags(&aux_, cudaStreamNonBlocking));
+            MPM_CUDA(cudaEventCreateWithFlags(&ev_fork_, cudaEventDisableTiming));
+            MPM_CUDA(cudaEventCreateWithFlags(&ev_join_, cudaEventDisableTiming));
+        }
+        MPM_CUDA(cudaEventRecord(ev_fork_, s));
+        MPM_CUDA(cudaStreamWaitEvent(aux_, ev_fork_, 0));
+        real_part(X, Y, M, sc, false, real_fp32, false, aux_);
+        MPM_CUDA(cudaEventRecord(ev_join_, aux_));
+        const RealOverlap ov{ev_join_, jacobi ? sc : nullptr};
+        if (recip_fp32) recip<float>(X, Y, M, s, &ov);
+        else recip<double>(X, Y, M, s, &ov);
         return;
     }
     if (recip_fp32) recip<float>(X, Y, M, s);

@@ -162,8 +162,17 @@ private:
     bool use_slab() const;   // pruned layout through AxisFFT::run_slab
     void build_scale(cudaStream_t s);
     cufftHandle plan_for(int B, bool fp32);  // B columns per voxel
-    template <typename R> void recip(const double2* X, double2* Y, int M, cudaStream_t s);
-    template <typename R> void recip_on(const double2* X, double2* Y, int M, cplx<R>* grid, cudaStream_t s);
+    // the real-space part already written into Y on another stream: the
+    // contraction waits for `join`, adds, and scales by 1/s (jacobi_sc)
+    struct RealOverlap {
+        cudaEvent_t join;
+        const double2* jacobi_sc;
+    };
+    template <typename R>
+    void recip(const double2* X, double2* Y, int M, cudaStream_t s, const RealOverlap* ov = nullptr);
+    template <typename R>
+    void recip_on(const double2* X, double2* Y, int M, cplx<R>* grid, cudaStream_t s,
+                  const RealOverlap* ov = nullptr);
     template <typename R> void transform(cplx<R>* grid, int B, bool inverse, cudaStream_t s);
     void build_spread_plan(cudaStream_t s);
     void real_part(const double2* X, double2* Y, int M, const double2* self_coef, bool jacobi, bool real_fp32,
@@ -208,8 +217,11 @@ private:
     std::vector<double> layer_w_;
     long layer_key_g_ = -1;
     double layer_key_d_ = 0.0;
-    bool layer_taps_ = false;
+    bool layer_taps_ = false, layer_colK_ = false;   // layer taps / column kernel built for that key
     DevBuf layer_wd_;               // device copy of layer_w_ and its |DFT|^2 per kz
+    // second stream for the real-space sum alongside the reciprocal chain
+    cudaStream_t aux_ = nullptr;
+    cudaEvent_t ev_fork_ = nullptr, ev_join_ = nullptr;
     // per-frame spread plan (monodisperse): per tile candidates, 1-D weights,
     // column contributor lists; plan_cap_ = 0 when the plan is not in use
     DevBuf plan_nc_, plan_cid_, plan_w64_, plan_w32_, plan_lw64_, plan_lw32_, plan_lc_, plan_ln_, plan_cnt_;

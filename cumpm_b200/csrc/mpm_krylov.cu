@@ -110,7 +110,8 @@ struct GState {
     int kcount;      // Arnoldi columns of the current cycle
     int iters;       // total Arnoldi steps
     int converged;
-    int pad[3];
+    int reorth;      // this Arnoldi step: 0 one projection, 1 second pass pending, 2 second pass done
+    int pad[2];
 };
 
 __device__ __forceinline__ double col_tol(double tol, const double* tolv, int m) { return tolv ? tolv[m] : tol; }
@@ -152,206 +153,155 @@ __global__ void k_normalize(const double2* __restrict__ src, double2* __restrict
     dst[t] = (st[m].cyc && d > 0.0) ? src[t] * (1.0 / d) : make_double2(0, 0);
 }
 
-// ----------------------------------------------- fused Arnoldi-step kernels --
+// ------------------------------------------------- Arnoldi step kernels --
 //
-// CGS2 with the per-step reductions fused into the passes that produce their
-// inputs: (1) h = V^H w (k_dots1 + k_dots2); (2) w -= V h and the partial
-// sums of h2 = V^H w over the same rows (k_arn_update_dots) + k_dots2;
-// (3) w -= V h2 and the partial sums of |w|^2 (k_arn_update_norm); (4) one
-// CTA per step (k_arn_finish): |w|, h += h2, the Givens update of every
-// column and the count of columns still cycling.  Row blocks of
-// 8 x kArnRows rows by 32 columns; every sum is taken in a fixed order.
-constexpr int kArnRows = 4;   // rows per thread
+// The operator writes A V_k straight into V_{k+1}, so one pass of k_dots1 over
+// the k+2 vectors V_0..V_{k+1} gives h_i = V_i^H w (i <= k) and |w|^2 (i =
+// k+1).  Classical Gram-Schmidt with selective re-orthogonalisation: after
+// the projection |w'|^2 = |w|^2 - |h|^2 (Pythagoras, V orthonormal); a column
+// whose norm dropped below 0.7 |w| (|w'|^2 <= 0.49 |w|^2, where that
+// difference loses digits and orthogonality may suffer) takes a second
+// projection (Kahan and Parlett's "twice is enough" test); the others are
+// finished after one.  The Givens rotation of a column uses the final h and
+// |w'|; k_arn_update projects and normalises V_{k+1} in place.
 
-__device__ __forceinline__ int arn_rows(int rows, int bx) { return bx * 8 * kArnRows; }
-
-// w[row][m] -= sum_{i < nvec} V_i[row][m] h[i][m] over this CTA's rows, kept
-// in registers; then partial[bx][i][m] = sum over those rows of
-// conj(V_i) w (NORM = false) or partial[bx][m] = sum |w|^2 (NORM = true)
-template <bool NORM>
-__global__ void __launch_bounds__(256, 2) k_arn_update(double2* __restrict__ w, const double2* __restrict__ V,
-                                                    size_t vstride, int nvec, const double2* __restrict__ h,
-                                                    int rows, int M, double2* __restrict__ partial) {
-    __shared__ double2 red[8][8][32];
-    const int m = blockIdx.y * 32 + threadIdx.x;
-    const int r0 = arn_rows(rows, blockIdx.x) + threadIdx.y;
-    double2 wr[kArnRows];
-#pragma unroll
-    for (int j = 0; j < kArnRows; ++j) {
-        const int row = r0 + 8 * j;
-        wr[j] = make_double2(0, 0);
-        if (m < M && row < rows) {
-            const size_t o = size_t(row) * M + m;
-            double2 acc = make_double2(0, 0);
-            for (int i = 0; i < nvec; ++i) acc += V[size_t(i) * vstride + o] * h[size_t(i) * M + m];
-            wr[j] = w[o] - acc;
-            w[o] = wr[j];
+// Givens update of Hessenberg column k of one right-hand side (the previous
+// rotations, a new rotation, the residual estimate; gmres_solver.cu:120-184)
+__device__ void gm_givens(GState& s, const double2* __restrict__ h, double wn, double2* __restrict__ Hm,
+                          double2* __restrict__ gm, double* __restrict__ csm, double2* __restrict__ snm, int k,
+                          int ld, int M, int m, int restart, double tolm, double bnm, int maxiter) {
+    double2* col = Hm + size_t(k) * ld;
+    for (int i = 0; i <= k; ++i) col[i] = h[size_t(i) * M + m];
+    col[k + 1] = make_double2(wn, 0.0);
+    for (int i = 0; i < k; ++i) {
+        const double2 h1 = col[i], h2 = col[i + 1];
+        const double c = csm[i];
+        const double2 sv = snm[i];
+        const double2 cs_ = make_double2(sv.x, -sv.y);
+        col[i] = h1 * c + cs_ * h2;
+        col[i + 1] = (sv * h1) * -1.0 + h2 * c;
+    }
+    const double2 h1 = col[k], h2 = col[k + 1];
+    double c = 1.0;
+    double2 sv = make_double2(0, 0);
+    if (h2.x != 0.0 || h2.y != 0.0) {
+        const double a1 = hypot(h1.x, h1.y);
+        if (a1 == 0.0) {
+            c = 0.0;
+            sv = make_double2(1.0, 0.0);
+        } else {
+            const double a2 = hypot(h2.x, h2.y);
+            const double sc = a1 + a2;
+            const double n1 = a1 / sc, n2 = a2 / sc;
+            const double hh = sc * sqrt(n1 * n1 + n2 * n2);
+            c = a1 / hh;
+            // (conj(h1)/|h1|) * (h2/hh)
+            const double2 u = make_double2(h1.x / a1, -h1.y / a1);
+            sv = u * make_double2(h2.x / hh, h2.y / hh);
         }
     }
-    if constexpr (NORM) {
-        double s = 0.0;
-#pragma unroll
-        for (int j = 0; j < kArnRows; ++j) s += wr[j].x * wr[j].x + wr[j].y * wr[j].y;
-        red[0][threadIdx.y][threadIdx.x] = make_double2(s, 0.0);
-        __syncthreads();
-        if (threadIdx.y == 0 && m < M) {
-            double t = 0.0;
-            for (int r = 0; r < 8; ++r) t += red[0][r][threadIdx.x].x;
-            partial[size_t(blockIdx.x) * M + m] = make_double2(t, 0.0);
-        }
-    } else {
-        for (int i0 = 0; i0 < nvec; i0 += 8) {
-            const int nv = min(8, nvec - i0);
-            double2 acc[8];
-#pragma unroll
-            for (int k = 0; k < 8; ++k) acc[k] = make_double2(0, 0);
-#pragma unroll
-            for (int j = 0; j < kArnRows; ++j) {
-                const int row = r0 + 8 * j;
-                if (m < M && row < rows) {
-                    const size_t o = size_t(row) * M + m;
-#pragma unroll
-                    for (int k = 0; k < 8; ++k)
-                        if (k < nv) acc[k] += conjmul(V[size_t(i0 + k) * vstride + o], wr[j]);
-                }
-            }
-#pragma unroll
-            for (int k = 0; k < 8; ++k) red[k][threadIdx.y][threadIdx.x] = acc[k];
-            __syncthreads();
-            if (threadIdx.y < nv && m < M) {
-                double2 t = make_double2(0, 0);
-                for (int r = 0; r < 8; ++r) t += red[threadIdx.y][r][threadIdx.x];
-                partial[(size_t(blockIdx.x) * nvec + i0 + threadIdx.y) * M + m] = t;
-            }
-            __syncthreads();
-        }
+    csm[k] = c;
+    snm[k] = sv;
+    const double2 scj = make_double2(sv.x, -sv.y);
+    col[k] = h1 * c + scj * h2;
+    col[k + 1] = make_double2(0, 0);
+    const double2 g1 = gm[k], g2 = gm[k + 1];
+    gm[k] = g1 * c + scj * g2;
+    gm[k + 1] = (sv * g1) * -1.0 + g2 * c;
+    s.iters += 1;
+    const double resid = hypot(gm[k + 1].x, gm[k + 1].y);
+    if (resid < tolm * bnm || k + 1 >= restart || s.iters >= maxiter) {
+        s.cyc = 0;
+        s.kcount = k + 1;
     }
 }
 
-// partial[bx][i][m] = sum over the CTA's rows of conj(V_i) w (no update)
-__global__ void __launch_bounds__(256, 2) k_arn_dots(const double2* __restrict__ V, size_t vstride, int nvec,
-                                                  const double2* __restrict__ w, int rows, int M,
-                                                  double2* __restrict__ partial) {
-    __shared__ double2 red[8][8][32];
-    const int m = blockIdx.y * 32 + threadIdx.x;
-    const int r0 = arn_rows(rows, blockIdx.x) + threadIdx.y;
-    double2 wr[kArnRows];
-#pragma unroll
-    for (int j = 0; j < kArnRows; ++j) {
-        const int row = r0 + 8 * j;
-        wr[j] = (m < M && row < rows) ? w[size_t(row) * M + m] : make_double2(0, 0);
-    }
-    for (int i0 = 0; i0 < nvec; i0 += 8) {
-        const int nv = min(8, nvec - i0);
-        double2 acc[8];
-#pragma unroll
-        for (int k = 0; k < 8; ++k) acc[k] = make_double2(0, 0);
-#pragma unroll
-        for (int j = 0; j < kArnRows; ++j) {
-            const int row = r0 + 8 * j;
-            if (m < M && row < rows) {
-                const size_t o = size_t(row) * M + m;
-#pragma unroll
-                for (int k = 0; k < 8; ++k)
-                    if (k < nv) acc[k] += conjmul(V[size_t(i0 + k) * vstride + o], wr[j]);
-            }
-        }
-#pragma unroll
-        for (int k = 0; k < 8; ++k) red[k][threadIdx.y][threadIdx.x] = acc[k];
-        __syncthreads();
-        if (threadIdx.y < nv && m < M) {
-            double2 t = make_double2(0, 0);
-            for (int r = 0; r < 8; ++r) t += red[threadIdx.y][r][threadIdx.x];
-            partial[(size_t(blockIdx.x) * nvec + i0 + threadIdx.y) * M + m] = t;
-        }
-        __syncthreads();
-    }
-}
-
-// One CTA: |w| from the row-block partials, h += h2, the Givens update of
-// every column (Hessenberg column k, the previous rotations, a new rotation
-// and the residual estimate, gmres_solver.cu:120-184) and flag[0] = the
-// number of columns still cycling.
+// pass 1: hh = [V_0..V_k, w]^H w.  Columns whose projection keeps |w'| >
+// 0.7 |w| get |w'| by Pythagoras and their Givens update now; the others are
+// marked for a second pass.  pass 2 (marked columns, hh2 = [V_0..V_k, w']^H w'
+// after the first projection): h += h2, |w''| likewise, Givens.  Thread per
+// column; one CTA: flag[0] = columns still cycling, flag[1 + m] = column m
+// cycling, flag[1 + M] = columns marked for the second pass.
 __global__ void __launch_bounds__(1024) k_arn_finish(GState* __restrict__ st, double2* __restrict__ h,
-                                                     const double2* __restrict__ h2,
-                                                     const double2* __restrict__ pnorm, int gx,
-                                                     double* __restrict__ wn, double2* __restrict__ H,
+                                                     const double2* __restrict__ h2, int pass,
+                                                     double* __restrict__ inv_nu, double2* __restrict__ H,
                                                      double2* __restrict__ g, double* __restrict__ cs,
                                                      double2* __restrict__ sn, int k, int restart, int M,
                                                      const double* __restrict__ bn, double tol,
                                                      const double* __restrict__ tolv, int maxiter,
                                                      int* __restrict__ flag) {
-    __shared__ int total;
-    if (threadIdx.x == 0) total = 0;
+    __shared__ int ncyc, nreo;
+    if (threadIdx.x == 0) ncyc = nreo = 0;
     __syncthreads();
-    int cycling = 0;
+    const int ld = restart + 1;
+    int c_cyc = 0, c_reo = 0;
     for (int m = threadIdx.x; m < M; m += blockDim.x) {
-        double ss = 0.0;
-        for (int b = 0; b < gx; ++b) ss += pnorm[size_t(b) * M + m].x;
-        const double wnm = sqrt(fmax(ss, 0.0));
-        wn[m] = wnm;
-        for (int i = 0; i <= k; ++i) h[size_t(i) * M + m] += h2[size_t(i) * M + m];
         GState s = st[m];
-        if (!s.cyc) {
-            flag[1 + m] = 0;
-            continue;
-        }
-        const int ld = restart + 1;
-        double2* Hm = H + size_t(m) * ld * restart;
-        double2* gm = g + size_t(m) * ld;
-        double* csm = cs + size_t(m) * restart;
-        double2* snm = sn + size_t(m) * restart;
-        double2* col = Hm + size_t(k) * ld;
-        for (int i = 0; i <= k; ++i) col[i] = h[size_t(i) * M + m];
-        col[k + 1] = make_double2(wnm, 0.0);
-        for (int i = 0; i < k; ++i) {
-            const double2 h1 = col[i], hh2 = col[i + 1];
-            const double c = csm[i];
-            const double2 sv = snm[i];
-            const double2 cs_ = make_double2(sv.x, -sv.y);
-            col[i] = h1 * c + cs_ * hh2;
-            col[i + 1] = (sv * h1) * -1.0 + hh2 * c;
-        }
-        const double2 h1 = col[k], hh2 = col[k + 1];
-        double c = 1.0;
-        double2 sv = make_double2(0, 0);
-        if (hh2.x != 0.0 || hh2.y != 0.0) {
-            const double a1 = hypot(h1.x, h1.y);
-            if (a1 == 0.0) {
-                c = 0.0;
-                sv = make_double2(1.0, 0.0);
+        if (pass == 1) s.reorth = 0;
+        bool go = s.cyc && (pass == 1 || s.reorth == 1);
+        if (go) {
+            double wn2, hs = 0.0;
+            if (pass == 1) {
+                wn2 = h[size_t(k + 1) * M + m].x;
+                for (int i = 0; i <= k; ++i) {
+                    const double2 v = h[size_t(i) * M + m];
+                    hs += v.x * v.x + v.y * v.y;
+                }
             } else {
-                const double a2 = hypot(hh2.x, hh2.y);
-                const double sc = a1 + a2;
-                const double n1 = a1 / sc, n2 = a2 / sc;
-                const double hh = sc * sqrt(n1 * n1 + n2 * n2);
-                c = a1 / hh;
-                const double2 u = make_double2(h1.x / a1, -h1.y / a1);
-                sv = u * make_double2(hh2.x / hh, hh2.y / hh);
+                wn2 = h2[size_t(k + 1) * M + m].x;
+                for (int i = 0; i <= k; ++i) {
+                    const double2 v = h2[size_t(i) * M + m];
+                    hs += v.x * v.x + v.y * v.y;
+                    h[size_t(i) * M + m] += v;
+                }
             }
+            const double nu2 = wn2 - hs;
+            if (pass == 1 && !(nu2 > 0.49 * wn2)) {
+                s.reorth = 1;   // second projection before the Givens update
+            } else {
+                const double nu = sqrt(fmax(nu2, 0.0));
+                inv_nu[m] = nu > 0.0 ? 1.0 / nu : 0.0;
+                gm_givens(s, h, nu, H + size_t(m) * ld * restart, g + size_t(m) * ld, cs + size_t(m) * restart,
+                          sn + size_t(m) * restart, k, ld, M, m, restart, col_tol(tol, tolv, m), bn[m], maxiter);
+                if (pass == 2) s.reorth = 2;
+            }
+            st[m] = s;
         }
-        csm[k] = c;
-        snm[k] = sv;
-        const double2 scj = make_double2(sv.x, -sv.y);
-        col[k] = h1 * c + scj * hh2;
-        col[k + 1] = make_double2(0, 0);
-        const double2 g1 = gm[k], g2 = gm[k + 1];
-        gm[k] = g1 * c + scj * g2;
-        gm[k + 1] = (sv * g1) * -1.0 + g2 * c;
-        s.iters += 1;
-        const double resid = hypot(gm[k + 1].x, gm[k + 1].y);
-        if (resid < col_tol(tol, tolv, m) * bn[m] || k + 1 >= restart || s.iters >= maxiter) {
-            s.cyc = 0;
-            s.kcount = k + 1;
-        } else {
-            ++cycling;
-        }
+        c_cyc += s.cyc;
+        c_reo += s.reorth == 1;
         flag[1 + m] = s.cyc;
-        st[m] = s;
     }
-    if (cycling) atomicAdd(&total, cycling);
+    if (c_cyc) atomicAdd(&ncyc, c_cyc);
+    if (c_reo) atomicAdd(&nreo, c_reo);
     __syncthreads();
-    if (threadIdx.x == 0) flag[0] = total;
+    if (threadIdx.x == 0) {
+        flag[0] = ncyc;
+        flag[1 + M] = nreo;
+    }
+}
+
+// V_{k+1} -= sum_{i <= k} V_i h_i for the columns of this pass (pass 1: the
+// columns still cycling; pass 2: those whose second projection was just
+// finished), then scaled by 1/|w'| unless a second pass is pending; the
+// other columns of V_{k+1} (ended cycles, unused) are zeroed in pass 1.
+__global__ void k_arn_update(double2* __restrict__ V, size_t vstride, int k, const double2* __restrict__ h,
+                             const GState* __restrict__ st, const double* __restrict__ inv_nu, int rows, int M,
+                             int pass) {
+    const size_t t = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (t >= size_t(rows) * M) return;
+    const int m = int(t % M);
+    const GState s = st[m];
+    double2* w = V + size_t(k + 1) * vstride + t;
+    const bool mine = pass == 1 ? s.cyc != 0 : s.reorth == 2;
+    if (!mine) {
+        if (pass == 1) *w = make_double2(0, 0);
+        return;
+    }
+    double2 acc = make_double2(0, 0);
+    for (int i = 0; i <= k; ++i) acc += V[size_t(i) * vstride + t] * h[size_t(i) * M + m];
+    double2 v = *w - acc;
+    if (s.reorth != 1) v = v * inv_nu[m];
+    *w = v;
 }
 
 // back substitution H y = g, y stored [i][m]
@@ -723,7 +673,7 @@ void BatchSolver::gmres(Field& F, const double2* b, double2* x, int M, const dou
     w_.ensure(sizeof(double2) * n);
     r_.ensure(sizeof(double2) * n);
     bj_.ensure(sizeof(double2) * n);
-    flagdev_.ensure(sizeof(int) * (M + 1));
+    flagdev_.ensure(sizeof(int) * (M + 2));   // count, M column flags, second-pass count
     cur_cols_.clear();  // self coefficients may differ from the previous call
     double2* V = V_.as<double2>();
     GState* gs = state_.as<GState>();
@@ -731,9 +681,6 @@ void BatchSolver::gmres(Field& F, const double2* b, double2* x, int M, const dou
     int* dflag = flagdev_.as<int>();
     const int mb = nblk(M, 128);
     const int vb = nblk((long long)n, 256);
-    // fused Arnoldi kernels: row blocks of 8 x kArnRows rows
-    const int agx = std::max(1, (rows + 8 * kArnRows - 1) / (8 * kArnRows));
-    partial_.ensure(sizeof(double2) * size_t(agx) * (restart + 1) * M);
 
     norms(b, rows, M, bnorm_.as<double>(), s);
     k_gm_init<<<mb, 128, 0, s>>>(gs, bnorm_.as<double>(), M);
@@ -774,34 +721,42 @@ void BatchSolver::gmres(Field& F, const double2* b, double2* x, int M, const dou
         std::vector<int> cyc = begin_cols;
         for (int k = 0; k < restart; ++k) {
             double2* Vk = V + size_t(k) * n;
-            double2* w = w_.as<double2>();
+            double2* w = V + size_t(k + 1) * n;   // A V_k lands in V_{k+1}, projected and normalised in place
             st.column_matvecs += apply_cols(F, Vk, w, M, sc, opt.jacobi, r32, re32, cyc.data(), opt.compact, s);
             st.matvecs++;
-            // CGS2, the reductions fused into the passes that feed them
+            const int fthr = std::min(1024, ((M + 31) / 32) * 32);
+            auto finish = [&](int pass) {
+                k_arn_finish<<<1, fthr, 0, s>>>(gs, h_.as<double2>(), h2_.as<double2>(), pass, rnorm_.as<double>(),
+                                                H_.as<double2>(), g_.as<double2>(), cs_.as<double>(),
+                                                sn_.as<double2>(), k, restart, M, bnorm_.as<double>(), opt.tol, tolv,
+                                                opt.maxiter, dflag);
+                MPM_LAUNCH();
+            };
+            auto update = [&](const double2* hv, int pass) {
+                k_arn_update<<<vb, 256, 0, s>>>(V, n, k, hv, gs, rnorm_.as<double>(), rows, M, pass);
+                MPM_LAUNCH();
+            };
+            // [V_0..V_k, w]^H w: the projection and |w|^2 in one pass
+            dots(V, n, k + 2, w, rows, M, 1, h_.as<double2>(), s);
             {
                 StageScope sc1(ST_KRYLOV, s);
-                const dim3 grd(agx, (M + 31) / 32), blk(32, 8);
-                double2* part = partial_.as<double2>();
-                k_arn_dots<<<grd, blk, 0, s>>>(V, n, k + 1, w, rows, M, part);
-                MPM_LAUNCH();
-                k_dots2<<<nblk((long long)(k + 1) * M * 32, 256), 256, 0, s>>>(part, agx, k + 1, M, h_.as<double2>());
-                MPM_LAUNCH();
-                k_arn_update<false><<<grd, blk, 0, s>>>(w, V, n, k + 1, h_.as<double2>(), rows, M, part);
-                MPM_LAUNCH();
-                k_dots2<<<nblk((long long)(k + 1) * M * 32, 256), 256, 0, s>>>(part, agx, k + 1, M,
-                                                                              h2_.as<double2>());
-                MPM_LAUNCH();
-                k_arn_update<true><<<grd, blk, 0, s>>>(w, V, n, k + 1, h2_.as<double2>(), rows, M, part);
-                MPM_LAUNCH();
-                k_arn_finish<<<1, std::min(1024, ((M + 31) / 32) * 32), 0, s>>>(
-                    gs, h_.as<double2>(), h2_.as<double2>(), part, agx, rnorm_.as<double>(), H_.as<double2>(),
-                    g_.as<double2>(), cs_.as<double>(), sn_.as<double2>(), k, restart, M, bnorm_.as<double>(), opt.tol,
-                    tolv, opt.maxiter, dflag);
-                MPM_LAUNCH();
-                k_normalize<<<vb, 256, 0, s>>>(w, V + size_t(k + 1) * n, rnorm_.as<double>(), gs, n, M);
-                MPM_LAUNCH();
+                finish(1);
+                update(h_.as<double2>(), 1);
             }
-            if (read_flags(dflag, M, s) == 0) break;
+            // the count, the M column flags and the second-pass count
+            int left = read_flags(dflag, M + 1, s);
+            if (flag_[1 + M] > 0) {
+                // second projection of the columns that lost most of their norm
+                dots(V, n, k + 2, w, rows, M, 1, h2_.as<double2>(), s);
+                {
+                    StageScope sc2(ST_KRYLOV, s);
+                    finish(2);
+                    update(h2_.as<double2>(), 2);
+                }
+                left = read_flags(dflag, M + 1, s);
+                st.reorth_steps++;
+            }
+            if (left == 0) break;
             cyc.assign(flag_ + 1, flag_ + 1 + M);
         }
         k_gm_backsub<<<mb, 128, 0, s>>>(gs, H_.as<double2>(), g_.as<double2>(), y_.as<double2>(), restart, M, kper);
@@ -925,6 +880,7 @@ void BatchSolver::solve(Field& F, const double2* b, double2* x, int M, const dou
     st.matvecs = 0;
     st.column_matvecs = 0;
     st.refine_steps = 0;
+    st.reorth_steps = 0;
     if (!opt.refine) {
         if (opt.method == SOLVER_BICGSTAB) bicgstab(F, b, x, M, sc, opt, st, opt.recip_fp32, opt.real_fp32, s);
         else gmres(F, b, x, M, sc, opt, st, opt.recip_fp32, opt.real_fp32, s);
@@ -994,6 +950,7 @@ void BatchSolver::solve(Field& F, const double2* b, double2* x, int M, const dou
         for (int m = 0; m < M; ++m) st.iters[m] += inner.iters[m];
         st.matvecs += inner.matvecs;
         st.column_matvecs += inner.column_matvecs;
+        st.reorth_steps += inner.reorth_steps;
         st.refine_steps++;
     }
     for (int m = 0; m < M; ++m) st.converged[m] = conv[m];

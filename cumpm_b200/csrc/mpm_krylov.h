@@ -51,6 +51,7 @@ struct SolveStats {
     int matvecs = 0;                 // batched operator applications
     long long column_matvecs = 0;    // columns that went through the operator
     int refine_steps = 0;
+    int reorth_steps = 0;            // GMRES steps that needed a second projection pass
 };
 
 class BatchSolver {
@@ -88,8 +89,8 @@ private:
               double2* out, cudaStream_t s);
     void norms(const double2* w, int rows, int M, double* out, cudaStream_t s);
 
-    // reads the count and the M per-column flags that follow it
-    int read_flags(const int* dflag, int M, cudaStream_t s);
+    // reads the count and the nflags words that follow it into flag_
+    int read_flags(const int* dflag, int nflags, cudaStream_t s);
 
     DevBuf V_, H_, g_, cs_, sn_, y_, h_, h2_, partial_, bnorm_, rnorm_, state_, w_, r_, bj_;
     DevBuf r0_, p_, v_, s_, t_, scal_, d_, rr_, xr_, flagdev_, tolv_;

@@ -87,6 +87,7 @@ typedef struct mpm_solve_report {
     int num_converged;
     double max_rel_resid;  /* true fp64 |b-Ax|/|b| (refinement mode), else -1 */
     long long column_matvecs; /* right-hand-side columns that went through the operator */
+    int reorth_steps;      /* GMRES steps that took a second projection pass */
 } mpm_solve_report;
 
 typedef struct mpm_field_info {

@@ -229,7 +229,9 @@ def test_hex_monolayer_operator_fp64():
     F = capi.Field(capi.FIELD_MONO, box, 1e-6, 0.5)
     F.set_positions(pos)
     info = F.info()
-    # every particle at z = 0: a single layer (one stored z slot)
+    # every particle at z = 0: a single layer (one stored z slot); the 31-point
+    # y lines (prime) take the column kernel, with the layer's z weights
     assert info["pruned"] == 1 and info["z_slots"] == 1 and info["single_layer"] == 1
+    assert info["slab_fused"] == 0
     assert info["num_pairs"] == len(op.pi_)
     assert rel(gpu_apply(F, X, sc), ref) < 1e-12
