@@ -484,6 +484,86 @@ __global__ void __launch_bounds__(256) k_spread_planned(const double2* __restric
     }
 }
 
+// Spread with the per-frame plan for one-slot tiles (a single layer): a
+// warp per (x, y) column of the tile, lanes over the chunk's grid columns.
+// The column's contributor list (candidate, x-y weight times the
+// candidate's z weight) is read once per warp, 32 entries at a time, and
+// broadcast by shuffles, so a contribution costs two shuffles, a shared
+// load and an FMA; the warp's stores are one contiguous row.  Same
+// contributors in the same order as k_spread_planned.
+template <typename R>
+__global__ void __launch_bounds__(256) k_spread_planned_1z(const double2* __restrict__ X, int M, int N, int C,
+                                                           const int* __restrict__ quad_map, GridView g, int TX,
+                                                           int TY, int nbx, int nby, int capT, int bc,
+                                                           const int* __restrict__ ncT, const int* __restrict__ cidT,
+                                                           const R* __restrict__ wT, const R* __restrict__ lwT,
+                                                           const int* __restrict__ lcT, const int* __restrict__ lnT,
+                                                           cplx<R>* __restrict__ grid) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    cplx<R>* pv = reinterpret_cast<cplx<R>*>(smem_raw);   // [capT][bc]
+    const int chunk = blockIdx.z;
+    const int tile = blockIdx.y * nbx + blockIdx.x;
+    const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
+    const int B = C * M;
+    const int wlen = TX + TY + 1;
+    const int ncol = TX * TY;
+    const int nc = ncT[tile];
+    const size_t trow = size_t(tile) * capT;
+    const int b0 = chunk * bc;
+    const int nb = min(bc, B - b0);
+    for (int t = threadIdx.x; t < nc * nb; t += blockDim.x) {
+        const int c = t / nb, bb = t % nb;
+        const int i = cidT[trow + c];
+        const int b = b0 + bb;
+        const int comp = b / M;
+        double2 v;
+        if (comp < 3) {
+            v = X[size_t(3 * i) * M + b];
+        } else {
+            const int q = quad_map ? quad_map[i] : -1;
+            v = (q >= 0) ? X[size_t(3 * N + 5 * q + comp - 3) * M + (b - comp * M)] : make_double2(0, 0);
+        }
+        pv[c * bc + bb] = to_r<R>(v);
+    }
+    __syncthreads();
+    const R* wTt = wT + trow * wlen;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+    for (int col = warp; col < ncol; col += nwarp) {
+        const int lx = col / TY, ly = col % TY;
+        const int x = x0 + lx, y = y0 + ly;
+        if (x >= g.Nx || y >= g.Ny) continue;   // uniform over the warp
+        const int nl = lnT[size_t(tile) * ncol + col];
+        const size_t lrow = (size_t(tile) * ncol + col) * kSpreadListCap;
+        for (int bb0 = 0; bb0 < nb; bb0 += 32) {
+            const int bb = bb0 + lane;
+            cplx<R> acc = mk<R>(0, 0);
+            const int n = nl >= 0 ? nl : nc;   // full candidate loop when the list overflowed
+            for (int k0 = 0; k0 < n; k0 += 32) {
+                int ck = 0;
+                R wk = R(0);
+                if (k0 + lane < n) {
+                    if (nl >= 0) {
+                        ck = lcT[lrow + k0 + lane];
+                        wk = lwT[lrow + k0 + lane];
+                    } else {
+                        ck = k0 + lane;
+                        const R* wc = wTt + ck * wlen;
+                        wk = wc[lx] * wc[TX + ly];
+                    }
+                    wk *= wTt[ck * wlen + TX + TY];   // the candidate's z weight (1 for a layer)
+                }
+                const int kn = min(32, n - k0);
+                for (int k = 0; k < kn; ++k) {
+                    const int c = __shfl_sync(0xffffffffu, ck, k);
+                    const R w = __shfl_sync(0xffffffffu, wk, k);
+                    if (bb < nb) fma_rc(acc, w, pv[c * bc + bb]);
+                }
+            }
+            if (bb < nb) grid[(size_t(x) * g.Ny + y) * B + b0 + bb] = acc;
+        }
+    }
+}
+
 // Full layout: k-space Green tensor, dipoles only (scale_kernel,
 // monodisperse_ewald_electric_field.cu:1406-1432) or joint dipole/quadrupole
 // (scale_kernel_joint, :1434-1486).  One thread per (voxel, rhs).
@@ -1834,7 +1914,14 @@ void Field::recip_on(const double2* X, double2* Y, int M, cplx<R>* grid, cudaStr
                                         plan_lc_.as<int>(), plan_ln_.as<int>(), grid);
         };
         // the tile's z run in registers: as many accumulators as it needs
-        if (TZ == 1) go(k_spread_planned<R, 1>);
+        if (TZ == 1 && gv_.Zs == 1) {
+            MPM_CUDA(cudaFuncSetAttribute(k_spread_planned_1z<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          int(pshm)));
+            k_spread_planned_1z<R><<<grd, 256, pshm, s>>>(X, M, N_, C, quad_map_.as<int>(), gv_, TX, TY, ps.nb[0],
+                                                          ps.nb[1], plan_cap_, bc, plan_nc_.as<int>(),
+                                                          plan_cid_.as<int>(), wT, lw, plan_lc_.as<int>(),
+                                                          plan_ln_.as<int>(), grid);
+        }
         else if (TZ <= 9) go(k_spread_planned<R, 9>);
         else go(k_spread_planned<R, kSpreadZMax>);
     } else {

@@ -14,10 +14,12 @@ inline int nblk(long long n, int b) { return int((n + b - 1) / b); }
 // ----------------------------------------------------------- reductions --
 
 // out[i][m] = sum_row op(V_i[row][m]) * w[row][m], op = conj or identity.
-// Stage 1 writes per-CTA partials; stage 2 sums them.
+// Stage 1 writes per-CTA partials; stage 2 sums them.  shift >= 0 (the
+// GMRES step, w = V_{nvec-1} = A V_shift): the sums are taken with
+// u = w - V_shift in place of w, and the last vector's entry is |u|^2.
 __global__ void __launch_bounds__(256) k_dots1(const double2* __restrict__ V, size_t vstride, int nvec,
                                                const double2* __restrict__ w, int rows, int M, int conj,
-                                               double2* __restrict__ partial) {
+                                               double2* __restrict__ partial, int shift) {
     __shared__ double2 red[8][8][32];
     const int m = blockIdx.y * 32 + threadIdx.x;
     const int i0 = blockIdx.z * 8;
@@ -26,9 +28,11 @@ __global__ void __launch_bounds__(256) k_dots1(const double2* __restrict__ V, si
     const int nv = min(8, nvec - i0);
     if (m < M) {
         for (int row = blockIdx.x * 8 + threadIdx.y; row < rows; row += gridDim.x * 8) {
-            const double2 wv = w[size_t(row) * M + m];
+            double2 wv = w[size_t(row) * M + m];
+            if (shift >= 0) wv -= V[size_t(shift) * vstride + size_t(row) * M + m];
             for (int k = 0; k < nv; ++k) {
-                const double2 v = V[size_t(i0 + k) * vstride + size_t(row) * M + m];
+                const double2 v = (shift >= 0 && i0 + k == nvec - 1) ? wv
+                                                                       : V[size_t(i0 + k) * vstride + size_t(row) * M + m];
                 if (conj) acc[k] += conjmul(v, wv);
                 else acc[k] += v * wv;
             }
@@ -156,13 +160,14 @@ __global__ void k_normalize(const double2* __restrict__ src, double2* __restrict
 // ------------------------------------------------- Arnoldi step kernels --
 //
 // The operator writes A V_k straight into V_{k+1}, so one pass of k_dots1 over
-// the k+2 vectors V_0..V_{k+1} gives h_i = V_i^H w (i <= k) and |w|^2 (i =
-// k+1).  Classical Gram-Schmidt with selective re-orthogonalisation: after
-// the projection |w'|^2 = |w|^2 - |h|^2 (Pythagoras, V orthonormal); a column
-// whose norm dropped below 0.7 |w| (|w'|^2 <= 0.49 |w|^2, where that
-// difference loses digits and orthogonality may suffer) takes a second
-// projection (Kahan and Parlett's "twice is enough" test); the others are
-// finished after one.  The Givens rotation of a column uses the final h and
+// the k+2 vectors V_0..V_{k+1} gives h_i = V_i^H u (i <= k) and |u|^2 (i =
+// k+1) for u = w - V_k (then h_k(w) = h_k(u) + 1; u has the same projection
+// remainder w' as w).  Classical Gram-Schmidt with selective
+// re-orthogonalisation: after the projection |w'|^2 = |u|^2 - |h(u)|^2
+// (Pythagoras, V orthonormal); a column whose norm dropped below 0.7 |u|
+// (|w'|^2 <= 0.49 |u|^2, where that difference loses digits and
+// orthogonality may suffer) takes a second projection (Kahan and Parlett's
+// "twice is enough" test); the others are finished after one.  The Givens rotation of a column uses the final h and
 // |w'|; k_arn_update projects and normalises V_{k+1} in place.
 
 // Givens update of Hessenberg column k of one right-hand side (the previous
@@ -242,11 +247,13 @@ __global__ void __launch_bounds__(1024) k_arn_finish(GState* __restrict__ st, do
         if (go) {
             double wn2, hs = 0.0;
             if (pass == 1) {
+                // h holds V^H u and |u|^2 for u = w - V_k: h_k(w) = h_k(u) + 1
                 wn2 = h[size_t(k + 1) * M + m].x;
                 for (int i = 0; i <= k; ++i) {
                     const double2 v = h[size_t(i) * M + m];
                     hs += v.x * v.x + v.y * v.y;
                 }
+                h[size_t(k) * M + m].x += 1.0;
             } else {
                 wn2 = h2[size_t(k + 1) * M + m].x;
                 for (int i = 0; i <= k; ++i) {
@@ -616,12 +623,12 @@ int BatchSolver::apply_cols(Field& F, const double2* X, double2* Y, int M, const
 }
 
 void BatchSolver::dots(const double2* V, size_t vstride, int nvec, const double2* w, int rows, int M, int conj,
-                       double2* out, cudaStream_t s) {
+                       double2* out, cudaStream_t s, int shift) {
     StageScope scope(ST_KRYLOV, s);
     const int gx = std::max(1, std::min(296, (rows + 7) / 8));
     partial_.ensure(sizeof(double2) * size_t(gx) * nvec * M);
     dim3 grd(gx, (M + 31) / 32, (nvec + 7) / 8);
-    k_dots1<<<grd, dim3(32, 8), 0, s>>>(V, vstride, nvec, w, rows, M, conj, partial_.as<double2>());
+    k_dots1<<<grd, dim3(32, 8), 0, s>>>(V, vstride, nvec, w, rows, M, conj, partial_.as<double2>(), shift);
     MPM_LAUNCH();
     k_dots2<<<nblk((long long)nvec * M * 32, 256), 256, 0, s>>>(partial_.as<double2>(), gx, nvec, M, out);
     MPM_LAUNCH();
@@ -736,8 +743,11 @@ void BatchSolver::gmres(Field& F, const double2* b, double2* x, int M, const dou
                 k_arn_update<<<vb, 256, 0, s>>>(V, n, k, hv, gs, rnorm_.as<double>(), rows, M, pass);
                 MPM_LAUNCH();
             };
-            // [V_0..V_k, w]^H w: the projection and |w|^2 in one pass
-            dots(V, n, k + 2, w, rows, M, 1, h_.as<double2>(), s);
+            // [V_0..V_k, u]^H u with u = w - V_k: the projection and |u|^2 in one
+            // pass.  The preconditioned operator is close to the identity, so w
+            // is mostly V_k; projecting u instead leaves the same w' but tests the
+            // cancellation on the part that is not, and a second pass is rare.
+            dots(V, n, k + 2, w, rows, M, 1, h_.as<double2>(), s, k);
             {
                 StageScope sc1(ST_KRYLOV, s);
                 finish(1);

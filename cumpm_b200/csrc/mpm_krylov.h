@@ -86,7 +86,7 @@ private:
                   SolveStats& st, bool recip32, bool real32, cudaStream_t s, bool x_zero = false,
                   const double* tolv = nullptr, bool precond_rel = false);
     void dots(const double2* V, size_t vstride, int nvec, const double2* w, int rows, int M, int conj,
-              double2* out, cudaStream_t s);
+              double2* out, cudaStream_t s, int shift = -1);
     void norms(const double2* w, int rows, int M, double* out, cudaStream_t s);
 
     // reads the count and the nflags words that follow it into flag_
