@@ -491,7 +491,7 @@ def run_ours(args, rank, world, local_rank):
                 "krylov_steps_per_rhs": round(float(np.mean(iters)), 2),
                 "matvecs_per_step": mv_per_step,
                 "column_matvecs_per_step": colmv_per_step,
-                "reorth_steps_per_step": sum(r["reorth_steps"] for r in timed_reports) / max(1, len(timed_reports)),
+                "shifted_seed_columns": timed_reports[-1]["shift_seeds"] if timed_reports else 0,
                 "inner_tol": f"max({args.inner_tol:g}, 0.5 tol |b_m| / |r_m|) per column",
                 "compact_batch": not args.no_compact,
                 "grid": info["grid"], "pruned_z_slots": info["z_slots"] if info["pruned"] else None,
@@ -548,10 +548,10 @@ def stage_roofline(wl, info, M, reports, stages, nsteps):
     """Roofline of the dominant operator stage and the whole matvec's HBM
     fraction, from the per-stage CUDA-event times of a profiled pass."""
     matvecs = sum(r["matvecs"] for r in reports)
-    mv64 = sum(r["refine_steps"] + 1 for r in reports)  # fp64 true-residual matvecs, all M columns
+    mv64 = sum(r["fp64_matvecs"] for r in reports)  # fp64 true-residual matvecs (at most M columns each)
     mv32 = matvecs - mv64
     col64 = mv64 * M
-    col32 = sum(r["column_matvecs"] for r in reports) - col64
+    col32 = max(0, sum(r["column_matvecs"] for r in reports) - col64)
     op_stages = ["spread", "fft_fwd", "kspace", "fft_inv", "contract", "real"]
 
     def stage_bytes(k):

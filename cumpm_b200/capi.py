@@ -43,13 +43,14 @@ STAGES = ["spread", "fft_fwd", "kspace", "fft_inv", "contract", "real", "direct"
 class SolveOptions(C.Structure):
     _fields_ = [("method", C.c_int), ("restart", C.c_int), ("maxiter", C.c_int), ("tol", C.c_double),
                 ("jacobi", C.c_int), ("recip_fp32", C.c_int), ("real_fp32", C.c_int), ("refine", C.c_int),
-                ("inner_tol", C.c_double), ("compact", C.c_int)]
+                ("inner_tol", C.c_double), ("compact", C.c_int), ("shifted", C.c_int)]
 
 
 class SolveReport(C.Structure):
     _fields_ = [("matvecs", C.c_int), ("refine_steps", C.c_int), ("total_iterations", C.c_int),
                 ("max_iterations", C.c_int), ("num_converged", C.c_int), ("max_rel_resid", C.c_double),
-                ("column_matvecs", C.c_longlong), ("reorth_steps", C.c_int)]
+                ("column_matvecs", C.c_longlong), ("reorth_steps", C.c_int), ("shift_seeds", C.c_int),
+                ("fp64_matvecs", C.c_int)]
 
 
 class FieldInfo(C.Structure):
@@ -312,7 +313,8 @@ class Field:
         return gx, ga
 
     def batch_solve(self, B, X, self_coef, tol, method=METHOD_GMRES, restart=50, maxiter=1000, jacobi=True,
-                    recip_fp32=True, real_fp32=False, refine=False, inner_tol=1e-4, compact=True, stream=None):
+                    recip_fp32=True, real_fp32=False, refine=False, inner_tol=1e-4, compact=True, shifted=True,
+                    stream=None):
         import torch
         for name, t in (("B", B), ("X", X), ("self_coef", self_coef)):
             if not (t.is_cuda and t.dtype == torch.complex128 and t.dim() == 2):
@@ -324,7 +326,7 @@ class Field:
         B = B.contiguous()
         self_coef = self_coef.contiguous()
         o = SolveOptions(int(method), int(restart), int(maxiter), float(tol), int(jacobi), int(recip_fp32),
-                         int(real_fp32), int(refine), float(inner_tol), int(compact))
+                         int(real_fp32), int(refine), float(inner_tol), int(compact), int(shifted))
         r = SolveReport()
         check(lib().mpm_batch_solve(self._h, C.c_void_p(B.data_ptr()), C.c_void_p(X.data_ptr()), B.shape[1],
                                     C.c_void_p(self_coef.data_ptr()), C.byref(o), C.byref(r), _stream_ptr(stream)))

@@ -321,6 +321,7 @@ int mpm_batch_solve(mpm_field* f, const void* B, void* X, int M, const void* sc,
         o.refine = opt->refine != 0;
         o.inner_tol = opt->inner_tol;
         o.compact = opt->compact != 0;
+        o.shifted = opt->shifted != 0;
         if (!(o.inner_tol >= 0.0)) throw std::invalid_argument("inner_tol must be >= 0");
         mpm::SolveStats st;
         f->solver->solve(*f->impl, static_cast<const double2*>(B), static_cast<double2*>(X), M,
@@ -331,6 +332,8 @@ int mpm_batch_solve(mpm_field* f, const void* B, void* X, int M, const void* sc,
             rep->refine_steps = st.refine_steps;
             rep->column_matvecs = st.column_matvecs;
             rep->reorth_steps = st.reorth_steps;
+            rep->shift_seeds = st.shift_seeds;
+            rep->fp64_matvecs = st.fp64_matvecs;
             for (int m = 0; m < M; ++m) {
                 rep->total_iterations += st.iters[m];
                 rep->max_iterations = std::max(rep->max_iterations, st.iters[m]);

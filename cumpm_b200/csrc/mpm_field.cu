@@ -484,13 +484,14 @@ __global__ void __launch_bounds__(256) k_spread_planned(const double2* __restric
     }
 }
 
-// Spread with the per-frame plan for one-slot tiles (a single layer): a
-// warp per (x, y) column of the tile, lanes over the chunk's grid columns.
-// The column's contributor list (candidate, x-y weight times the
-// candidate's z weight) is read once per warp, 32 entries at a time, and
-// broadcast by shuffles, so a contribution costs two shuffles, a shared
-// load and an FMA; the warp's stores are one contiguous row.  Same
-// contributors in the same order as k_spread_planned.
+// Spread with the per-frame plan for one-slot tiles (a single layer): the
+// tile's candidate moments and every (x, y) column's contributor list
+// (candidate, x-y weight times the candidate's z weight -- 1 for a layer)
+// are staged in shared memory first, all loads in flight together; then a
+// warp per column, lanes over the chunk's grid columns, walks the list by
+// broadcast reads: a contribution costs three shared loads and an FMA, and
+// the warp's stores are one contiguous row.  Same contributors in the same
+// order as k_spread_planned.
 template <typename R>
 __global__ void __launch_bounds__(256) k_spread_planned_1z(const double2* __restrict__ X, int M, int N, int C,
                                                            const int* __restrict__ quad_map, GridView g, int TX,
@@ -500,17 +501,21 @@ __global__ void __launch_bounds__(256) k_spread_planned_1z(const double2* __rest
                                                            const int* __restrict__ lcT, const int* __restrict__ lnT,
                                                            cplx<R>* __restrict__ grid) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    cplx<R>* pv = reinterpret_cast<cplx<R>*>(smem_raw);   // [capT][bc]
+    const int ncol = TX * TY;
+    cplx<R>* pv = reinterpret_cast<cplx<R>*>(smem_raw);             // [capT][bc]
+    R* lwS = reinterpret_cast<R*>(pv + size_t(capT) * bc);           // [ncol][kSpreadListCap]
+    int* lcS = reinterpret_cast<int*>(lwS + size_t(ncol) * kSpreadListCap);
+    int* lnS = lcS + size_t(ncol) * kSpreadListCap;                   // [ncol]
     const int chunk = blockIdx.z;
     const int tile = blockIdx.y * nbx + blockIdx.x;
     const int x0 = blockIdx.x * TX, y0 = blockIdx.y * TY;
     const int B = C * M;
     const int wlen = TX + TY + 1;
-    const int ncol = TX * TY;
     const int nc = ncT[tile];
     const size_t trow = size_t(tile) * capT;
     const int b0 = chunk * bc;
     const int nb = min(bc, B - b0);
+    const R* wTt = wT + trow * wlen;
     for (int t = threadIdx.x; t < nc * nb; t += blockDim.x) {
         const int c = t / nb, bb = t % nb;
         const int i = cidT[trow + c];
@@ -525,41 +530,37 @@ __global__ void __launch_bounds__(256) k_spread_planned_1z(const double2* __rest
         }
         pv[c * bc + bb] = to_r<R>(v);
     }
+    for (int t = threadIdx.x; t < ncol; t += blockDim.x) lnS[t] = lnT[size_t(tile) * ncol + t];
     __syncthreads();
-    const R* wTt = wT + trow * wlen;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+    for (int col = warp; col < ncol; col += nwarp) {
+        const int nl = lnS[col];
+        const size_t lrow = (size_t(tile) * ncol + col) * kSpreadListCap;
+        for (int k = lane; k < nl; k += 32) {
+            const int c = lcT[lrow + k];
+            lcS[col * kSpreadListCap + k] = c;
+            lwS[col * kSpreadListCap + k] = lwT[lrow + k] * wTt[c * wlen + TX + TY];
+        }
+    }
+    __syncthreads();
     for (int col = warp; col < ncol; col += nwarp) {
         const int lx = col / TY, ly = col % TY;
         const int x = x0 + lx, y = y0 + ly;
         if (x >= g.Nx || y >= g.Ny) continue;   // uniform over the warp
-        const int nl = lnT[size_t(tile) * ncol + col];
-        const size_t lrow = (size_t(tile) * ncol + col) * kSpreadListCap;
-        for (int bb0 = 0; bb0 < nb; bb0 += 32) {
-            const int bb = bb0 + lane;
+        const int nl = lnS[col];
+        const int* lc = lcS + col * kSpreadListCap;
+        const R* lw = lwS + col * kSpreadListCap;
+        for (int bb = lane; bb < nb; bb += 32) {
             cplx<R> acc = mk<R>(0, 0);
-            const int n = nl >= 0 ? nl : nc;   // full candidate loop when the list overflowed
-            for (int k0 = 0; k0 < n; k0 += 32) {
-                int ck = 0;
-                R wk = R(0);
-                if (k0 + lane < n) {
-                    if (nl >= 0) {
-                        ck = lcT[lrow + k0 + lane];
-                        wk = lwT[lrow + k0 + lane];
-                    } else {
-                        ck = k0 + lane;
-                        const R* wc = wTt + ck * wlen;
-                        wk = wc[lx] * wc[TX + ly];
-                    }
-                    wk *= wTt[ck * wlen + TX + TY];   // the candidate's z weight (1 for a layer)
-                }
-                const int kn = min(32, n - k0);
-                for (int k = 0; k < kn; ++k) {
-                    const int c = __shfl_sync(0xffffffffu, ck, k);
-                    const R w = __shfl_sync(0xffffffffu, wk, k);
-                    if (bb < nb) fma_rc(acc, w, pv[c * bc + bb]);
+            if (nl >= 0) {
+                for (int k = 0; k < nl; ++k) fma_rc(acc, lw[k], pv[lc[k] * bc + bb]);
+            } else {   // list overflowed: every candidate, in order
+                for (int c = 0; c < nc; ++c) {
+                    const R* wc = wTt + c * wlen;
+                    fma_rc(acc, (wc[lx] * wc[TX + ly]) * wc[TX + TY], pv[c * bc + bb]);
                 }
             }
-            if (bb < nb) grid[(size_t(x) * g.Ny + y) * B + b0 + bb] = acc;
+            grid[(size_t(x) * g.Ny + y) * B + b0 + bb] = acc;
         }
     }
 }
@@ -851,14 +852,17 @@ __global__ void k_column(cplx<R>* __restrict__ grid, const cplx<R>* __restrict__
 // is given, scales the sum by the Jacobi factor 1/s of the target and
 // column.  C = 3 (dipoles) or 8 (plus field gradient).  SZ > 0: the
 // stencil's z run (g.Sz <= SZ) unrolled, so that its grid loads are in
-// flight together; SZ = 0: any stencil length.
-template <typename R, int SZ>
+// flight together; SZ = 0: any stencil length.  SXY > 0: the stencil width
+// g.S == SXY at compile time, its y run unrolled as well.  Grid offsets of
+// the stencil's x and y indices are precomputed once per target.
+template <typename R, int SZ, int SXY>
 __global__ void k_contract(const cplx<R>* __restrict__ grid, GridView g, int M, int C, int Nt,
                            const int4* __restrict__ base, const R* __restrict__ w1, double factor,
                            const int* __restrict__ quad_map, double2* __restrict__ Y, int negate,
                            const int* __restrict__ order, int accumulate, const double2* __restrict__ jsc) {
     __shared__ R w[3 * kMaxStencil];
     __shared__ int idx[3 * kMaxStencil];
+    __shared__ long long offxy[2 * kMaxStencil];   // x then y stencil offsets into the grid (elements)
     // targets in spatial-bin order when given: CTAs that run together share
     // their stencils' voxels in L2
     const int j = order ? order[blockIdx.x] : blockIdx.x;
@@ -870,6 +874,8 @@ __global__ void k_contract(const cplx<R>* __restrict__ grid, GridView g, int M, 
         const int dd = o - g.off;
         idx[t] = (d == 0) ? pmod(bs.x + dd, g.Nx) : (d == 1) ? pmod(bs.y + dd, g.Ny)
                  : (g.pruned ? bs.z + dd : pmod(bs.z + dd, g.Nz));
+        if (d == 0) offxy[o] = (long long)idx[t] * g.Ny * g.Zs * B;
+        else if (d == 1) offxy[g.S + o] = (long long)idx[t] * g.Zs * B;
     }
     __syncthreads();
     // the z window on the stored grid: entries zb .. zb + Sz - 1 of the z
@@ -891,28 +897,31 @@ __global__ void k_contract(const cplx<R>* __restrict__ grid, GridView g, int M, 
                 zo[oz] = oz < g.Sz ? idx[zb + oz] * B + b : b;
             }
         }
-        for (int ox = 0; ox < g.S; ++ox) {
+        const int S = SXY > 0 ? SXY : g.S;
+        // one stencil column (x, y): its z run from gp (the grid at (x, y), slot 0)
+        auto column = [&](const cplx<R>* gp) {
+            cplx<R> a2 = mk<R>(0, 0);
+            if constexpr (SZ > 0) {
+                cplx<R> v[SZ];
+#pragma unroll
+                for (int oz = 0; oz < SZ; ++oz)
+                    if (oz < g.Sz) v[oz] = gp[zo[oz]];
+#pragma unroll
+                for (int oz = 0; oz < SZ; ++oz)
+                    if (oz < g.Sz) fma_rc(a2, wz[oz], v[oz]);
+            } else {
+                for (int oz = 0; oz < g.Sz; ++oz) fma_rc(a2, w[zb + oz], gp[size_t(idx[zb + oz]) * B + b]);
+            }
+            return a2;
+        };
+        for (int ox = 0; ox < S; ++ox) {
             const R wx = w[ox];
-            const size_t rx = size_t(idx[ox]) * g.Ny;
-            for (int oy = 0; oy < g.S; ++oy) {
-                const R wxy = wx * w[g.S + oy];
-                const size_t rxy = (rx + idx[g.S + oy]) * g.Zs;
-                cplx<R> a2 = mk<R>(0, 0);
-                if constexpr (SZ > 0) {
-                    const cplx<R>* gp = grid + rxy * B;
-                    cplx<R> v[SZ];
+            const cplx<R>* gx = grid + offxy[ox];
+            if constexpr (SXY > 0) {
 #pragma unroll
-                    for (int oz = 0; oz < SZ; ++oz)
-                        if (oz < g.Sz) v[oz] = gp[zo[oz]];
-#pragma unroll
-                    for (int oz = 0; oz < SZ; ++oz)
-                        if (oz < g.Sz) fma_rc(a2, wz[oz], v[oz]);
-                } else {
-                    for (int oz = 0; oz < g.Sz; ++oz) {
-                        fma_rc(a2, w[zb + oz], grid[(rxy + idx[zb + oz]) * B + b]);
-                    }
-                }
-                fma_rc(acc, wxy, a2);
+                for (int oy = 0; oy < SXY; ++oy) fma_rc(acc, wx * w[SXY + oy], column(gx + offxy[SXY + oy]));
+            } else {
+                for (int oy = 0; oy < S; ++oy) fma_rc(acc, wx * w[S + oy], column(gx + offxy[S + oy]));
             }
         }
         double2 v = to_d(acc);
@@ -1915,9 +1924,10 @@ void Field::recip_on(const double2* X, double2* Y, int M, cplx<R>* grid, cudaStr
         };
         // the tile's z run in registers: as many accumulators as it needs
         if (TZ == 1 && gv_.Zs == 1) {
+            const size_t lshm = pshm + (sizeof(R) + sizeof(int)) * ncol * kSpreadListCap + sizeof(int) * ncol;
             MPM_CUDA(cudaFuncSetAttribute(k_spread_planned_1z<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                          int(pshm)));
-            k_spread_planned_1z<R><<<grd, 256, pshm, s>>>(X, M, N_, C, quad_map_.as<int>(), gv_, TX, TY, ps.nb[0],
+                                          int(lshm)));
+            k_spread_planned_1z<R><<<grd, 256, lshm, s>>>(X, M, N_, C, quad_map_.as<int>(), gv_, TX, TY, ps.nb[0],
                                                           ps.nb[1], plan_cap_, bc, plan_nc_.as<int>(),
                                                           plan_cid_.as<int>(), wT, lw, plan_lc_.as<int>(),
                                                           plan_ln_.as<int>(), grid);
@@ -1998,10 +2008,17 @@ void Field::recip_on(const double2* X, double2* Y, int M, cplx<R>* grid, cudaStr
                                 spec_.solver_ax ? sources_.idx_sorted.as<int>() : nullptr, ov ? 1 : 0,
                                 ov ? ov->jacobi_sc : nullptr);
     };
-    if (gv_.Sz == 1) contract(k_contract<R, 1>);
-    else if (gv_.Sz <= 9) contract(k_contract<R, 9>);
-    else if (gv_.Sz <= 13) contract(k_contract<R, 13>);
-    else contract(k_contract<R, 0>);
+    if (gv_.Sz == 1) {
+        if (gv_.S == 9) contract(k_contract<R, 1, 9>);
+        else contract(k_contract<R, 1, 0>);
+    } else if (gv_.Sz <= 9) {
+        if (gv_.S == 9) contract(k_contract<R, 9, 9>);
+        else contract(k_contract<R, 9, 0>);
+    } else if (gv_.Sz <= 13) {
+        contract(k_contract<R, 13, 0>);
+    } else {
+        contract(k_contract<R, 0, 0>);
+    }
     MPM_LAUNCH();
 }
 

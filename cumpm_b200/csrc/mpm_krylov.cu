@@ -27,6 +27,7 @@ __global__ void __launch_bounds__(256) k_dots1(const double2* __restrict__ V, si
     for (int k = 0; k < 8; ++k) acc[k] = make_double2(0, 0);
     const int nv = min(8, nvec - i0);
     if (m < M) {
+#pragma unroll 4
         for (int row = blockIdx.x * 8 + threadIdx.y; row < rows; row += gridDim.x * 8) {
             double2 wv = w[size_t(row) * M + m];
             if (shift >= 0) wv -= V[size_t(shift) * vstride + size_t(row) * M + m];
@@ -176,17 +177,18 @@ __device__ void gm_givens(GState& s, const double2* __restrict__ h, double wn, d
                           double2* __restrict__ gm, double* __restrict__ csm, double2* __restrict__ snm, int k,
                           int ld, int M, int m, int restart, double tolm, double bnm, int maxiter) {
     double2* col = Hm + size_t(k) * ld;
-    for (int i = 0; i <= k; ++i) col[i] = h[size_t(i) * M + m];
-    col[k + 1] = make_double2(wn, 0.0);
+    // the previous rotations applied down the column, the running entry in
+    // a register (the column's inputs and the rotations are independent loads)
+    double2 carry = h[m];
     for (int i = 0; i < k; ++i) {
-        const double2 h1 = col[i], h2 = col[i + 1];
+        const double2 h2 = h[size_t(i + 1) * M + m];
         const double c = csm[i];
         const double2 sv = snm[i];
         const double2 cs_ = make_double2(sv.x, -sv.y);
-        col[i] = h1 * c + cs_ * h2;
-        col[i + 1] = (sv * h1) * -1.0 + h2 * c;
+        col[i] = carry * c + cs_ * h2;
+        carry = (sv * carry) * -1.0 + h2 * c;
     }
-    const double2 h1 = col[k], h2 = col[k + 1];
+    const double2 h1 = carry, h2 = make_double2(wn, 0.0);
     double c = 1.0;
     double2 sv = make_double2(0, 0);
     if (h2.x != 0.0 || h2.y != 0.0) {
@@ -221,6 +223,10 @@ __device__ void gm_givens(GState& s, const double2* __restrict__ h, double wn, d
     }
 }
 
+// givens = 0 (the seeds of a shifted solve): |w'| and the normalisation
+// only; the Givens updates are the members' (k_shift_givens).  always2:
+// every column takes the second projection (CGS2); else only those that
+// fail the 0.7 test.
 // pass 1: hh = [V_0..V_k, w]^H w.  Columns whose projection keeps |w'| >
 // 0.7 |w| get |w'| by Pythagoras and their Givens update now; the others are
 // marked for a second pass.  pass 2 (marked columns, hh2 = [V_0..V_k, w']^H w'
@@ -228,7 +234,8 @@ __device__ void gm_givens(GState& s, const double2* __restrict__ h, double wn, d
 // column; one CTA: flag[0] = columns still cycling, flag[1 + m] = column m
 // cycling, flag[1 + M] = columns marked for the second pass.
 __global__ void __launch_bounds__(1024) k_arn_finish(GState* __restrict__ st, double2* __restrict__ h,
-                                                     const double2* __restrict__ h2, int pass,
+                                                     const double2* __restrict__ h2, int pass, int givens, int always2,
+                                                     double* __restrict__ nu_out,
                                                      double* __restrict__ inv_nu, double2* __restrict__ H,
                                                      double2* __restrict__ g, double* __restrict__ cs,
                                                      double2* __restrict__ sn, int k, int restart, int M,
@@ -263,13 +270,16 @@ __global__ void __launch_bounds__(1024) k_arn_finish(GState* __restrict__ st, do
                 }
             }
             const double nu2 = wn2 - hs;
-            if (pass == 1 && !(nu2 > 0.49 * wn2)) {
+            if (pass == 1 && (always2 || !(nu2 > 0.49 * wn2))) {
                 s.reorth = 1;   // second projection before the Givens update
             } else {
                 const double nu = sqrt(fmax(nu2, 0.0));
                 inv_nu[m] = nu > 0.0 ? 1.0 / nu : 0.0;
-                gm_givens(s, h, nu, H + size_t(m) * ld * restart, g + size_t(m) * ld, cs + size_t(m) * restart,
-                          sn + size_t(m) * restart, k, ld, M, m, restart, col_tol(tol, tolv, m), bn[m], maxiter);
+                if (nu_out) nu_out[m] = nu;
+                if (givens)
+                    gm_givens(s, h, nu, H + size_t(m) * ld * restart, g + size_t(m) * ld, cs + size_t(m) * restart,
+                              sn + size_t(m) * restart, k, ld, M, m, restart, col_tol(tol, tolv, m), bn[m],
+                              maxiter);
                 if (pass == 2) s.reorth = 2;
             }
             st[m] = s;
@@ -311,6 +321,132 @@ __global__ void k_arn_update(double2* __restrict__ V, size_t vstride, int k, con
     *w = v;
 }
 
+// ---------------------------------------------------------- shifted solve --
+//
+// Columns m whose self coefficients are one particle profile c times a
+// scalar, sc[:, m] = f_m c, have operators A_m = G + f_m diag(c) (G the
+// interactions and the self value common to all columns); scaled by
+// diag(c)^-1 they are the shifted family A0 + (f_m - 1) I with A0 = diag(c)^-1
+// G + I, the operator apply gives with self coefficients c and Jacobi
+// scaling.  Columns with the same right-hand side share one Krylov space of
+// A0: one seed column per distinct right-hand side is iterated, and every
+// member m of a seed's group runs its own Givens QR on the seed's Hessenberg
+// column with sigma_m = f_m - 1 added to the diagonal (GMRES for shifted
+// systems with x0 = 0, whose residuals stay collinear).
+
+// f_m = sc[0][m] / sc[0][0]; bad[m] = 1 unless sc[i][m] = f_m sc[i][0] for
+// every particle i (relative 1e-12)
+__global__ void k_shift_ratio(const double2* __restrict__ sc, int N, int M, double2* __restrict__ f,
+                              int* __restrict__ bad) {
+    const int m = blockIdx.x;
+    const double2 a = sc[m], c0 = sc[0];
+    const double den = c0.x * c0.x + c0.y * c0.y;
+    const double2 fm = den > 0.0 ? make_double2((a.x * c0.x + a.y * c0.y) / den, (a.y * c0.x - a.x * c0.y) / den)
+                                 : make_double2(0, 0);
+    int miss = den > 0.0 ? 0 : 1;
+    for (int i = threadIdx.x; i < N && !miss; i += blockDim.x) {
+        const double2 v = sc[size_t(i) * M + m], r = sc[size_t(i) * M] * fm;
+        const double dx = v.x - r.x, dy = v.y - r.y;
+        if (dx * dx + dy * dy > 1e-24 * (v.x * v.x + v.y * v.y) || (v.x == 0.0 && v.y == 0.0)) miss = 1;
+    }
+    miss = __syncthreads_or(miss);
+    if (threadIdx.x == 0) {
+        f[m] = fm;
+        bad[m] = miss;
+    }
+}
+
+// eq[m][m2] = 1 if right-hand-side columns m and m2 < m are equal
+__global__ void k_col_equal(const double2* __restrict__ b, int rows, int M, int* __restrict__ eq) {
+    const int m = blockIdx.x, m2 = blockIdx.y;
+    if (m2 >= m) return;
+    int diff = 0;
+    for (int r = threadIdx.x; r < rows && !diff; r += blockDim.x) {
+        const double2 u = b[size_t(r) * M + m], v = b[size_t(r) * M + m2];
+        if (u.x != v.x || u.y != v.y) diff = 1;
+    }
+    diff = __syncthreads_or(diff);
+    if (threadIdx.x == 0) eq[size_t(m) * M + m2] = !diff;
+}
+
+// member m of seed grp[m]: Hessenberg column k of the seed plus sigma_m on
+// the diagonal, then its Givens update (gm_givens).  pass 1 takes the members
+// of seeds finished after one projection, pass 2 those of seeds whose second
+// projection just finished (reorth 2); members of a seed still waiting for
+// its second projection keep it cycling.  A seed cycles while any member
+// does (written back to its state).  One CTA: flag[0] = seeds cycling,
+// flag[1 + g] = seed g cycling.
+__global__ void __launch_bounds__(1024) k_shift_givens(GState* __restrict__ mst, GState* __restrict__ sst,
+                                                       const double2* __restrict__ hs, const double* __restrict__ nu,
+                                                       const double2* __restrict__ sigma, const int* __restrict__ grp,
+                                                       int G, int pass, double2* __restrict__ hm,
+                                                       double2* __restrict__ H, double2* __restrict__ g,
+                                                       double* __restrict__ cs, double2* __restrict__ sn, int k,
+                                                       int restart, int M, const double* __restrict__ bs,
+                                                       const double* __restrict__ tolv, int maxiter,
+                                                       int* __restrict__ seed_cyc, int* __restrict__ flag) {
+    __shared__ int n;
+    if (threadIdx.x == 0) n = 0;
+    for (int t = threadIdx.x; t < G; t += blockDim.x) seed_cyc[t] = 0;
+    __syncthreads();
+    const int ld = restart + 1;
+    for (int m = threadIdx.x; m < M; m += blockDim.x) {
+        GState s = mst[m];
+        if (!s.cyc) continue;
+        const int gi = grp[m];
+        const int sr = sst[gi].reorth;
+        if (sr == 1) {              // second projection pending
+            atomicOr(&seed_cyc[gi], 1);
+            continue;
+        }
+        if (sr == (pass == 1 ? 0 : 2)) {
+            for (int i = 0; i <= k; ++i) hm[size_t(i) * M + m] = hs[size_t(i) * G + gi];
+            hm[size_t(k) * M + m] += sigma[m];
+            gm_givens(s, hm, nu[gi], H + size_t(m) * ld * restart, g + size_t(m) * ld, cs + size_t(m) * restart,
+                      sn + size_t(m) * restart, k, ld, M, m, restart, tolv[m], bs[gi], maxiter);
+            mst[m] = s;
+        }
+        if (s.cyc) atomicOr(&seed_cyc[gi], 1);
+    }
+    __syncthreads();
+    for (int t = threadIdx.x; t < G; t += blockDim.x) {
+        flag[1 + t] = seed_cyc[t];
+        sst[t].cyc = seed_cyc[t];
+        if (seed_cyc[t]) atomicAdd(&n, 1);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) flag[0] = n;
+}
+
+// member states: active and cycling from the start, x0 = 0; g_m = (beta, 0..)
+__global__ void k_shift_init(GState* __restrict__ mst, const int* __restrict__ grp, const double* __restrict__ bs,
+                             double2* __restrict__ g, int restart, int M) {
+    const int m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= M) return;
+    GState s{};
+    const double beta = bs[grp[m]];
+    s.active = beta > 0.0;
+    s.cyc = s.active;
+    s.converged = !s.active;
+    mst[m] = s;
+    g[size_t(m) * (restart + 1)] = make_double2(beta, 0.0);
+    for (int i = 1; i <= restart; ++i) g[size_t(m) * (restart + 1) + i] = make_double2(0, 0);
+}
+
+// x[row][m] = sum_{i < kper[m]} V_i[row][grp[m]] y[i][m]
+__global__ void k_shift_x(double2* __restrict__ x, const double2* __restrict__ V, size_t vstride, int G,
+                          const double2* __restrict__ y, const int* __restrict__ grp, const int* __restrict__ kper,
+                          int rows, int M) {
+    const size_t t = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (t >= size_t(rows) * M) return;
+    const size_t row = t / M;
+    const int m = int(t - row * M);
+    const int gi = grp[m];
+    double2 acc = make_double2(0, 0);
+    for (int i = 0; i < kper[m]; ++i) acc += V[size_t(i) * vstride + row * G + gi] * y[size_t(i) * M + m];
+    x[t] = acc;
+}
+
 // back substitution H y = g, y stored [i][m]
 __global__ void k_gm_backsub(const GState* __restrict__ st, const double2* __restrict__ H,
                              const double2* __restrict__ g, double2* __restrict__ y, int restart, int M,
@@ -329,6 +465,15 @@ __global__ void k_gm_backsub(const GState* __restrict__ st, const double2* __res
         const double den = d.x * d.x + d.y * d.y;
         y[size_t(i) * M + m] = make_double2((v.x * d.x + v.y * d.y) / den, (v.y * d.x - v.x * d.y) / den);
     }
+}
+
+// seeds: cycling from the start unless their right-hand side is zero
+__global__ void k_seed_init(GState* __restrict__ st, const double* __restrict__ bn, int G) {
+    const int m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= G) return;
+    GState s{};
+    s.active = s.cyc = bn[m] > 0.0;
+    st[m] = s;
 }
 
 __global__ void k_zero_rhs_cols(double2* __restrict__ x, const double* __restrict__ bn, size_t n, int M) {
@@ -625,7 +770,8 @@ int BatchSolver::apply_cols(Field& F, const double2* X, double2* Y, int M, const
 void BatchSolver::dots(const double2* V, size_t vstride, int nvec, const double2* w, int rows, int M, int conj,
                        double2* out, cudaStream_t s, int shift) {
     StageScope scope(ST_KRYLOV, s);
-    const int gx = std::max(1, std::min(296, (rows + 7) / 8));
+    // four CTAs per SM: the sums are latency-bound, not bandwidth-bound
+    const int gx = std::max(1, std::min(592, (rows + 7) / 8));
     partial_.ensure(sizeof(double2) * size_t(gx) * nvec * M);
     dim3 grd(gx, (M + 31) / 32, (nvec + 7) / 8);
     k_dots1<<<grd, dim3(32, 8), 0, s>>>(V, vstride, nvec, w, rows, M, conj, partial_.as<double2>(), shift);
@@ -733,8 +879,8 @@ void BatchSolver::gmres(Field& F, const double2* b, double2* x, int M, const dou
             st.matvecs++;
             const int fthr = std::min(1024, ((M + 31) / 32) * 32);
             auto finish = [&](int pass) {
-                k_arn_finish<<<1, fthr, 0, s>>>(gs, h_.as<double2>(), h2_.as<double2>(), pass, rnorm_.as<double>(),
-                                                H_.as<double2>(), g_.as<double2>(), cs_.as<double>(),
+                k_arn_finish<<<1, fthr, 0, s>>>(gs, h_.as<double2>(), h2_.as<double2>(), pass, 1, 1, nullptr,
+                                                rnorm_.as<double>(), H_.as<double2>(), g_.as<double2>(), cs_.as<double>(),
                                                 sn_.as<double2>(), k, restart, M, bnorm_.as<double>(), opt.tol, tolv,
                                                 opt.maxiter, dflag);
                 MPM_LAUNCH();
@@ -743,29 +889,25 @@ void BatchSolver::gmres(Field& F, const double2* b, double2* x, int M, const dou
                 k_arn_update<<<vb, 256, 0, s>>>(V, n, k, hv, gs, rnorm_.as<double>(), rows, M, pass);
                 MPM_LAUNCH();
             };
-            // [V_0..V_k, u]^H u with u = w - V_k: the projection and |u|^2 in one
-            // pass.  The preconditioned operator is close to the identity, so w
-            // is mostly V_k; projecting u instead leaves the same w' but tests the
-            // cancellation on the part that is not, and a second pass is rare.
+            // CGS2: [V_0..V_k, u]^H u with u = w - V_k (the preconditioned
+            // operator is close to the identity, so w is mostly V_k: the
+            // first projection then works on the part that is not), w -= V h;
+            // then [V_0..V_k, w']^H w', w' -= V h2, normalised; one flag read
             dots(V, n, k + 2, w, rows, M, 1, h_.as<double2>(), s, k);
             {
                 StageScope sc1(ST_KRYLOV, s);
                 finish(1);
                 update(h_.as<double2>(), 1);
             }
-            // the count, the M column flags and the second-pass count
-            int left = read_flags(dflag, M + 1, s);
-            if (flag_[1 + M] > 0) {
-                // second projection of the columns that lost most of their norm
-                dots(V, n, k + 2, w, rows, M, 1, h2_.as<double2>(), s);
-                {
-                    StageScope sc2(ST_KRYLOV, s);
-                    finish(2);
-                    update(h2_.as<double2>(), 2);
-                }
-                left = read_flags(dflag, M + 1, s);
-                st.reorth_steps++;
+            dots(V, n, k + 2, w, rows, M, 1, h2_.as<double2>(), s);
+            {
+                StageScope sc2(ST_KRYLOV, s);
+                finish(2);
+                update(h2_.as<double2>(), 2);
             }
+            st.reorth_steps++;
+            // the count and the M column flags
+            const int left = read_flags(dflag, M, s);
             if (left == 0) break;
             cyc.assign(flag_ + 1, flag_ + 1 + M);
         }
@@ -783,6 +925,159 @@ void BatchSolver::gmres(Field& F, const double2* b, double2* x, int M, const dou
         st.iters[m] += h[m].iters;
         st.converged[m] = h[m].converged;
     }
+}
+
+bool BatchSolver::detect_shifts(const double2* b, const double2* sc, int rows, int N, int M, cudaStream_t s,
+                                std::vector<int>& grp, std::vector<double2>& f) {
+    if (M < 2 || M > 1024 || !sc) return false;
+    shf_.ensure(sizeof(double2) * M);
+    shflag_.ensure(sizeof(int) * (size_t(M) + size_t(M) * M));
+    int* bad = shflag_.as<int>();
+    int* eq = bad + M;
+    MPM_CUDA(cudaMemsetAsync(eq, 0, sizeof(int) * size_t(M) * M, s));
+    k_shift_ratio<<<M, 256, 0, s>>>(sc, N, M, shf_.as<double2>(), bad);
+    MPM_LAUNCH();
+    k_col_equal<<<dim3(M, M), 256, 0, s>>>(b, rows, M, eq);
+    MPM_LAUNCH();
+    std::vector<int> h(size_t(M) + size_t(M) * M);
+    f.resize(M);
+    MPM_CUDA(cudaMemcpyAsync(h.data(), bad, sizeof(int) * h.size(), cudaMemcpyDeviceToHost, s));
+    MPM_CUDA(cudaMemcpyAsync(f.data(), shf_.p, sizeof(double2) * M, cudaMemcpyDeviceToHost, s));
+    MPM_CUDA(cudaStreamSynchronize(s));
+    for (int m = 0; m < M; ++m)
+        if (h[m]) return false;
+    grp.assign(M, -1);
+    int G = 0;
+    for (int m = 0; m < M; ++m) {
+        for (int m2 = 0; m2 < m && grp[m] < 0; ++m2)
+            if (h[M + size_t(m) * M + m2]) grp[m] = grp[m2];
+        if (grp[m] < 0) grp[m] = G++;
+    }
+    return G < M;   // no shared right-hand side: nothing to gain
+}
+
+void BatchSolver::gmres_shifted(Field& F, const double2* b, double2* x, int M, const double2* sc,
+                                const SolveOptions& opt, SolveStats& st, bool r32, bool re32, cudaStream_t s,
+                                const double* tolv, const std::vector<int>& grp, const std::vector<double2>& f) {
+    const int rows = F.rows_in(), N = F.num_particles();
+    const int G = 1 + *std::max_element(grp.begin(), grp.end());
+    const int restart = std::max(1, std::min(rows, opt.restart));
+    const size_t ns = size_t(rows) * G;
+    std::vector<int> seed(G, -1), zeros(G, 0);
+    for (int m = 0; m < M; ++m)
+        if (seed[grp[m]] < 0) seed[grp[m]] = m;
+    std::vector<double2> sigma(M);
+    for (int m = 0; m < M; ++m) sigma[m] = make_double2(f[m].x - 1.0, f[m].y);
+    // device copies: member -> seed, seed columns, zero indices (ints), then
+    // sigma (double2) at a 16-byte aligned offset
+    const size_t sig_off = (sizeof(int) * (size_t(M) + 2 * G) + 15) & ~size_t(15);
+    shmeta_.ensure(sig_off + sizeof(double2) * M);
+    int* dgrp = shmeta_.as<int>();
+    int* dseed = dgrp + M;
+    int* dzero = dseed + G;
+    double2* dsig = reinterpret_cast<double2*>(shmeta_.as<char>() + sig_off);
+    MPM_CUDA(cudaMemcpyAsync(dgrp, grp.data(), sizeof(int) * M, cudaMemcpyHostToDevice, s));
+    MPM_CUDA(cudaMemcpyAsync(dseed, seed.data(), sizeof(int) * G, cudaMemcpyHostToDevice, s));
+    MPM_CUDA(cudaMemcpyAsync(dzero, zeros.data(), sizeof(int) * G, cudaMemcpyHostToDevice, s));
+    MPM_CUDA(cudaMemcpyAsync(dsig, sigma.data(), sizeof(double2) * M, cudaMemcpyHostToDevice, s));
+    // seed operator: self coefficients c = sc[:, 0] for every seed, Jacobi
+    // scaling: A0 = diag(c)^-1 G + I; seed right-hand sides diag(c)^-1 b
+    shsc_.ensure(sizeof(double2) * size_t(N) * G);
+    shb_.ensure(sizeof(double2) * ns * 2);
+    double2* scs = shsc_.as<double2>();
+    double2* sb = shb_.as<double2>();
+    double2* sbj = sb + ns;
+    k_gather_cols<<<nblk((long long)N * G, 256), 256, 0, s>>>(sc, M, scs, G, dzero, N);
+    MPM_LAUNCH();
+    k_gather_cols<<<nblk((long long)ns, 256), 256, 0, s>>>(b, M, sb, G, dseed, rows);
+    MPM_LAUNCH();
+    k_jacobi<<<nblk((long long)ns, 256), 256, 0, s>>>(sb, sbj, N, F.num_quads(), G, F.quad_idx_dev(), scs);
+    MPM_LAUNCH();
+    V_.ensure(sizeof(double2) * ns * (restart + 1));
+    H_.ensure(sizeof(double2) * size_t(M) * (restart + 1) * restart);
+    g_.ensure(sizeof(double2) * size_t(M) * (restart + 1));
+    cs_.ensure(sizeof(double) * size_t(M) * restart);
+    sn_.ensure(sizeof(double2) * size_t(M) * restart);
+    y_.ensure(sizeof(double2) * size_t(M) * restart);
+    h_.ensure(sizeof(double2) * size_t(G) * (restart + 1));
+    h2_.ensure(sizeof(double2) * size_t(G) * (restart + 1));
+    hm_.ensure(sizeof(double2) * size_t(M) * (restart + 1));
+    state_.ensure(sizeof(GState) * M + sizeof(int) * M);
+    // seed states, seed cycling flags, then |b~| and |w'| per seed (8-byte aligned)
+    const size_t bs_off = (sizeof(GState) * G + sizeof(int) * G + 7) & ~size_t(7);
+    shst_.ensure(bs_off + 2 * sizeof(double) * G);
+    rnorm_.ensure(sizeof(double) * std::max(M, G) * 2);
+    flagdev_.ensure(sizeof(int) * (G + 2));
+    cur_cols_.clear();
+    double2* V = V_.as<double2>();
+    GState* mst = state_.as<GState>();
+    int* kper = reinterpret_cast<int*>(mst + M);
+    GState* sst = shst_.as<GState>();
+    int* scyc = reinterpret_cast<int*>(sst + G);
+    double* bs = reinterpret_cast<double*>(shst_.as<char>() + bs_off);
+    double* nu = bs + G;
+    int* dflag = flagdev_.as<int>();
+    norms(sbj, rows, G, bs, s);
+    k_seed_init<<<nblk(G, 128), 128, 0, s>>>(sst, bs, G);
+    MPM_LAUNCH();
+    k_shift_init<<<nblk(M, 128), 128, 0, s>>>(mst, dgrp, bs, g_.as<double2>(), restart, M);
+    MPM_LAUNCH();
+    k_normalize<<<nblk((long long)ns, 256), 256, 0, s>>>(sbj, V, bs, sst, ns, G);
+    MPM_LAUNCH();
+    std::vector<double> hbs(G);
+    MPM_CUDA(cudaMemcpyAsync(hbs.data(), bs, sizeof(double) * G, cudaMemcpyDeviceToHost, s));
+    MPM_CUDA(cudaStreamSynchronize(s));
+    std::vector<int> cyc(G);
+    for (int gi = 0; gi < G; ++gi) cyc[gi] = hbs[gi] > 0.0;
+    const int vb = nblk((long long)ns, 256);
+    const int fthr = std::min(1024, ((std::max(M, G) + 31) / 32) * 32);
+    for (int k = 0; k < restart; ++k) {
+        if (std::count(cyc.begin(), cyc.end(), 1) == 0) break;
+        double2* Vk = V + size_t(k) * ns;
+        double2* w = V + size_t(k + 1) * ns;
+        st.column_matvecs += apply_cols(F, Vk, w, G, scs, true, r32, re32, cyc.data(), opt.compact, s);
+        st.matvecs++;
+        auto seed_pass = [&](int pass, const double2* hv) {
+            // (every seed takes both projections: the members' Givens updates
+            // follow the second)
+            StageScope sc1(ST_KRYLOV, s);
+            k_arn_finish<<<1, fthr, 0, s>>>(sst, h_.as<double2>(), h2_.as<double2>(), pass, 0, 1, nu,
+                                            rnorm_.as<double>(), nullptr, nullptr, nullptr, nullptr, k, restart, G,
+                                            bs, opt.tol, nullptr, opt.maxiter, dflag);
+            MPM_LAUNCH();
+            k_arn_update<<<vb, 256, 0, s>>>(V, ns, k, hv, sst, rnorm_.as<double>(), rows, G, pass);
+            MPM_LAUNCH();
+            if (pass == 1) return;
+            k_shift_givens<<<1, fthr, 0, s>>>(mst, sst, h_.as<double2>(), nu, dsig, dgrp, G, pass,
+                                              hm_.as<double2>(), H_.as<double2>(), g_.as<double2>(),
+                                              cs_.as<double>(), sn_.as<double2>(), k, restart, M, bs, tolv,
+                                              opt.maxiter, scyc, dflag);
+            MPM_LAUNCH();
+        };
+        dots(V, ns, k + 2, w, rows, G, 1, h_.as<double2>(), s, k);
+        seed_pass(1, h_.as<double2>());
+        dots(V, ns, k + 2, w, rows, G, 1, h2_.as<double2>(), s);
+        seed_pass(2, h2_.as<double2>());
+        st.reorth_steps++;
+        const int left = read_flags(dflag, G, s);
+        if (left == 0) break;
+        cyc.assign(flag_ + 1, flag_ + 1 + G);
+    }
+    k_gm_backsub<<<nblk(M, 128), 128, 0, s>>>(mst, H_.as<double2>(), g_.as<double2>(), y_.as<double2>(), restart, M,
+                                              kper);
+    MPM_LAUNCH();
+    k_shift_x<<<nblk((long long)rows * M, 256), 256, 0, s>>>(x, V, ns, G, y_.as<double2>(), dgrp, kper, rows, M);
+    MPM_LAUNCH();
+    std::vector<GState> h(M);
+    MPM_CUDA(cudaMemcpyAsync(h.data(), mst, sizeof(GState) * M, cudaMemcpyDeviceToHost, s));
+    MPM_CUDA(cudaStreamSynchronize(s));
+    st.iters.resize(M);
+    st.converged.resize(M);
+    for (int m = 0; m < M; ++m) {
+        st.iters[m] += h[m].iters;
+        st.converged[m] = h[m].converged;
+    }
+    st.shift_seeds = G;
 }
 
 void BatchSolver::bicgstab(Field& F, const double2* b, double2* x, int M, const double2* sc, const SolveOptions& opt,
@@ -891,6 +1186,8 @@ void BatchSolver::solve(Field& F, const double2* b, double2* x, int M, const dou
     st.column_matvecs = 0;
     st.refine_steps = 0;
     st.reorth_steps = 0;
+    st.shift_seeds = 0;
+    st.fp64_matvecs = 0;
     if (!opt.refine) {
         if (opt.method == SOLVER_BICGSTAB) bicgstab(F, b, x, M, sc, opt, st, opt.recip_fp32, opt.real_fp32, s);
         else gmres(F, b, x, M, sc, opt, st, opt.recip_fp32, opt.real_fp32, s);
@@ -919,12 +1216,23 @@ void BatchSolver::solve(Field& F, const double2* b, double2* x, int M, const dou
     std::vector<int> conv(M, 0), act(M, 1);
     st.rel_resid.assign(M, 0.0);
     cur_cols_.clear();
+    // Shifted structure (one particle profile of self coefficients, shared
+    // right-hand sides: a frequency sweep of one material): the first
+    // correction is solved from x = 0 for all columns at once on the seeds'
+    // Krylov spaces; later corrections are per column.
+    std::vector<int> grp;
+    std::vector<double2> fsh;
+    const bool shifted = opt.shifted && opt.method == SOLVER_GMRES &&
+                         detect_shifts(b, sc, rows, F.num_particles(), M, s, grp, fsh);
+    bool reset = false;   // x replaced by the shifted solve from zero: every column active again
     for (int step = 0; step < opt.max_refine; ++step) {
         // fp64 true residual of the columns not yet converged (a converged
         // column's x no longer changes)
         st.column_matvecs += apply_cols(F, x, xr_.as<double2>(), M, sc, false, false, false,
-                                        step == 0 ? nullptr : act.data(), opt.compact, s);
+                                        step == 0 || reset ? nullptr : act.data(), opt.compact, s);
+        reset = false;
         st.matvecs++;
+        st.fp64_matvecs++;
         k_sub<<<vb, 256, 0, s>>>(b, xr_.as<double2>(), xr_.as<double2>(), n);
         MPM_LAUNCH();
         norms(xr_.as<double2>(), rows, M, rn2, s);
@@ -943,6 +1251,28 @@ void BatchSolver::solve(Field& F, const double2* b, double2* x, int M, const dou
             left += act[m];
         }
         if (!left) break;
+        double worst = 0.0;
+        for (int m = 0; m < M; ++m)
+            if (act[m]) worst = std::max(worst, st.rel_resid[m]);
+        if (step == 0 && shifted && left == M && worst >= 0.05) {
+            // a poor initial guess (every column's residual at least 5% of
+            // |b|): start again from x = 0 and solve the first correction of
+            // all columns on the seeds' Krylov spaces
+            MPM_CUDA(cudaMemsetAsync(x, 0, sizeof(double2) * n, s));
+            k_inner_tol<<<nblk(M, 128), 128, 0, s>>>(bn2, bn2, opt.tol, floor, tolv_.as<double>(), M);
+            MPM_LAUNCH();
+            SolveStats inner;
+            inner.iters.assign(M, 0);
+            gmres_shifted(F, b, x, M, sc, in, inner, true, true, s, tolv_.as<double>(), grp, fsh);
+            for (int m = 0; m < M; ++m) st.iters[m] += inner.iters[m];
+            st.matvecs += inner.matvecs;
+            st.column_matvecs += inner.column_matvecs;
+            st.reorth_steps += inner.reorth_steps;
+            st.shift_seeds = inner.shift_seeds;
+            st.refine_steps++;
+            reset = true;
+            continue;
+        }
         k_mask_conv<<<vb, 256, 0, s>>>(xr_.as<double2>(), convd, n, M);
         MPM_LAUNCH();
         MPM_CUDA(cudaMemsetAsync(d_.p, 0, sizeof(double2) * n, s));

@@ -42,6 +42,12 @@ struct SolveOptions {
     // Only the columns still iterating go through the field operator
     // (gathered into a compact batch); converged columns cost nothing.
     bool compact = true;
+    // Refinement with GMRES: when every column's self coefficients are one
+    // particle profile times a scalar and right-hand sides repeat (a
+    // frequency sweep of one material), solve the first correction of all
+    // columns from x = 0 on one Krylov space per distinct right-hand side
+    // (shifted systems).  The initial guess is then not used.
+    bool shifted = true;
 };
 
 struct SolveStats {
@@ -52,6 +58,8 @@ struct SolveStats {
     long long column_matvecs = 0;    // columns that went through the operator
     int refine_steps = 0;
     int reorth_steps = 0;            // GMRES steps that needed a second projection pass
+    int shift_seeds = 0;             // seed columns of the shifted first correction (0: not used)
+    int fp64_matvecs = 0;            // true-residual (fp64 operator) matvecs of the refinement
 };
 
 class BatchSolver {
@@ -85,6 +93,16 @@ private:
     void bicgstab(Field& F, const double2* b, double2* x, int M, const double2* sc, const SolveOptions& opt,
                   SolveStats& st, bool recip32, bool real32, cudaStream_t s, bool x_zero = false,
                   const double* tolv = nullptr, bool precond_rel = false);
+    // grp[m]: the seed (distinct right-hand side) of column m; f[m]: its
+    // self-coefficient scale, sc[:, m] = f[m] sc[:, 0].  False when the
+    // columns have no such structure or no repeated right-hand side.
+    bool detect_shifts(const double2* b, const double2* sc, int rows, int N, int M, cudaStream_t s,
+                       std::vector<int>& grp, std::vector<double2>& f);
+    // x (all M columns) from x0 = 0 by GMRES on the seeds' Krylov spaces;
+    // stops each column at |D^-1 r| < tolv[m] |D^-1 b|
+    void gmres_shifted(Field& F, const double2* b, double2* x, int M, const double2* sc, const SolveOptions& opt,
+                       SolveStats& st, bool recip32, bool real32, cudaStream_t s, const double* tolv,
+                       const std::vector<int>& grp, const std::vector<double2>& f);
     void dots(const double2* V, size_t vstride, int nvec, const double2* w, int rows, int M, int conj,
               double2* out, cudaStream_t s, int shift = -1);
     void norms(const double2* w, int rows, int M, double* out, cudaStream_t s);
@@ -96,6 +114,7 @@ private:
     DevBuf r0_, p_, v_, s_, t_, scal_, d_, rr_, xr_, flagdev_, tolv_;
     DevBuf cidx_, xc_, yc_, scc_;        // compact-batch gather buffers
     DevBuf bn2_, rn2_, convd_;           // refinement: |b|, true |r|, converged flags
+    DevBuf shf_, shflag_, shmeta_, shsc_, shb_, shst_, hm_;   // shifted solve: detection, seeds, members
     int* flag_ = nullptr;                // pinned host words: count + per-column flags
     int flag_cap_ = 0;
     int* hidx_ = nullptr;                // pinned host column list for the gather

@@ -77,6 +77,10 @@ typedef struct mpm_solve_options {
     double inner_tol;  /* smallest relative reduction asked of one inner solve (0: 1e-4); a column's
                           inner solve also stops once its residual is below 0.5 tol |b| */
     int compact;       /* only still-iterating columns go through the operator (gathered batch) */
+    int shifted;       /* refinement with GMRES: when the columns are one material's frequency sweep
+                          (self coefficients one particle profile times a scalar, repeated right-hand
+                          sides), solve the first correction on one Krylov space per distinct
+                          right-hand side (shifted systems, from x = 0) */
 } mpm_solve_options;
 
 typedef struct mpm_solve_report {
@@ -88,6 +92,8 @@ typedef struct mpm_solve_report {
     double max_rel_resid;  /* true fp64 |b-Ax|/|b| (refinement mode), else -1 */
     long long column_matvecs; /* right-hand-side columns that went through the operator */
     int reorth_steps;      /* GMRES steps that took a second projection pass */
+    int shift_seeds;       /* seed columns of the shifted first correction (0: not used) */
+    int fp64_matvecs;      /* fp64 true-residual matvecs of the refinement */
 } mpm_solve_report;
 
 typedef struct mpm_field_info {
