@@ -418,13 +418,14 @@ __global__ void __launch_bounds__(1024) k_shift_givens(GState* __restrict__ mst,
     if (threadIdx.x == 0) flag[0] = n;
 }
 
-// member states: active and cycling from the start, x0 = 0; g_m = (beta, 0..)
+// member states: active and cycling from the start, x0 = 0; g_m = (beta, 0..);
+// members already converged (skip[m], may be null) take no part
 __global__ void k_shift_init(GState* __restrict__ mst, const int* __restrict__ grp, const double* __restrict__ bs,
-                             double2* __restrict__ g, int restart, int M) {
+                             const int* __restrict__ skip, double2* __restrict__ g, int restart, int M) {
     const int m = blockIdx.x * blockDim.x + threadIdx.x;
     if (m >= M) return;
     GState s{};
-    const double beta = bs[grp[m]];
+    const double beta = (skip && skip[m]) ? 0.0 : bs[grp[m]];
     s.active = beta > 0.0;
     s.cyc = s.active;
     s.converged = !s.active;
@@ -433,14 +434,16 @@ __global__ void k_shift_init(GState* __restrict__ mst, const int* __restrict__ g
     for (int i = 1; i <= restart; ++i) g[size_t(m) * (restart + 1) + i] = make_double2(0, 0);
 }
 
-// x[row][m] = sum_{i < kper[m]} V_i[row][grp[m]] y[i][m]
+// x[row][m] = sum_{i < kper[m]} V_i[row][grp[m]] y[i][m] (columns skipped
+// as converged keep their x)
 __global__ void k_shift_x(double2* __restrict__ x, const double2* __restrict__ V, size_t vstride, int G,
                           const double2* __restrict__ y, const int* __restrict__ grp, const int* __restrict__ kper,
-                          int rows, int M) {
+                          const int* __restrict__ skip, int rows, int M) {
     const size_t t = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
     if (t >= size_t(rows) * M) return;
     const size_t row = t / M;
     const int m = int(t - row * M);
+    if (skip && skip[m]) return;
     const int gi = grp[m];
     double2 acc = make_double2(0, 0);
     for (int i = 0; i < kper[m]; ++i) acc += V[size_t(i) * vstride + row * G + gi] * y[size_t(i) * M + m];
@@ -958,7 +961,8 @@ bool BatchSolver::detect_shifts(const double2* b, const double2* sc, int rows, i
 
 void BatchSolver::gmres_shifted(Field& F, const double2* b, double2* x, int M, const double2* sc,
                                 const SolveOptions& opt, SolveStats& st, bool r32, bool re32, cudaStream_t s,
-                                const double* tolv, const std::vector<int>& grp, const std::vector<double2>& f) {
+                                const double* tolv, const std::vector<int>& grp, const std::vector<double2>& f,
+                                const int* skip, const int* live) {
     const int rows = F.rows_in(), N = F.num_particles();
     const int G = 1 + *std::max_element(grp.begin(), grp.end());
     const int restart = std::max(1, std::min(rows, opt.restart));
@@ -1020,7 +1024,7 @@ void BatchSolver::gmres_shifted(Field& F, const double2* b, double2* x, int M, c
     norms(sbj, rows, G, bs, s);
     k_seed_init<<<nblk(G, 128), 128, 0, s>>>(sst, bs, G);
     MPM_LAUNCH();
-    k_shift_init<<<nblk(M, 128), 128, 0, s>>>(mst, dgrp, bs, g_.as<double2>(), restart, M);
+    k_shift_init<<<nblk(M, 128), 128, 0, s>>>(mst, dgrp, bs, skip, g_.as<double2>(), restart, M);
     MPM_LAUNCH();
     k_normalize<<<nblk((long long)ns, 256), 256, 0, s>>>(sbj, V, bs, sst, ns, G);
     MPM_LAUNCH();
@@ -1028,7 +1032,9 @@ void BatchSolver::gmres_shifted(Field& F, const double2* b, double2* x, int M, c
     MPM_CUDA(cudaMemcpyAsync(hbs.data(), bs, sizeof(double) * G, cudaMemcpyDeviceToHost, s));
     MPM_CUDA(cudaStreamSynchronize(s));
     std::vector<int> cyc(G);
-    for (int gi = 0; gi < G; ++gi) cyc[gi] = hbs[gi] > 0.0;
+    std::vector<int> used(G, live ? 0 : 1);
+    for (int m = 0; m < M && live; ++m) used[grp[m]] |= live[m] != 0;
+    for (int gi = 0; gi < G; ++gi) cyc[gi] = hbs[gi] > 0.0 && used[gi];
     const int vb = nblk((long long)ns, 256);
     const int fthr = std::min(1024, ((std::max(M, G) + 31) / 32) * 32);
     for (int k = 0; k < restart; ++k) {
@@ -1066,7 +1072,8 @@ void BatchSolver::gmres_shifted(Field& F, const double2* b, double2* x, int M, c
     k_gm_backsub<<<nblk(M, 128), 128, 0, s>>>(mst, H_.as<double2>(), g_.as<double2>(), y_.as<double2>(), restart, M,
                                               kper);
     MPM_LAUNCH();
-    k_shift_x<<<nblk((long long)rows * M, 256), 256, 0, s>>>(x, V, ns, G, y_.as<double2>(), dgrp, kper, rows, M);
+    k_shift_x<<<nblk((long long)rows * M, 256), 256, 0, s>>>(x, V, ns, G, y_.as<double2>(), dgrp, kper, skip, rows,
+                                                             M);
     MPM_LAUNCH();
     std::vector<GState> h(M);
     MPM_CUDA(cudaMemcpyAsync(h.data(), mst, sizeof(GState) * M, cudaMemcpyDeviceToHost, s));
@@ -1251,19 +1258,20 @@ void BatchSolver::solve(Field& F, const double2* b, double2* x, int M, const dou
             left += act[m];
         }
         if (!left) break;
-        double worst = 0.0;
+        double best = 1e300;
         for (int m = 0; m < M; ++m)
-            if (act[m]) worst = std::max(worst, st.rel_resid[m]);
-        if (step == 0 && shifted && left == M && worst >= 0.05) {
-            // a poor initial guess (every column's residual at least 5% of
-            // |b|): start again from x = 0 and solve the first correction of
-            // all columns on the seeds' Krylov spaces
-            MPM_CUDA(cudaMemsetAsync(x, 0, sizeof(double2) * n, s));
+            if (act[m]) best = std::min(best, st.rel_resid[m]);
+        if (step == 0 && shifted && best >= 0.05) {
+            // a poor initial guess (every unconverged column's residual at
+            // least 5% of |b|): those columns start again from x = 0 and
+            // their first correction is solved on the seeds' Krylov spaces;
+            // converged columns (a warm start) keep their x
             k_inner_tol<<<nblk(M, 128), 128, 0, s>>>(bn2, bn2, opt.tol, floor, tolv_.as<double>(), M);
             MPM_LAUNCH();
             SolveStats inner;
             inner.iters.assign(M, 0);
-            gmres_shifted(F, b, x, M, sc, in, inner, true, true, s, tolv_.as<double>(), grp, fsh);
+            gmres_shifted(F, b, x, M, sc, in, inner, true, true, s, tolv_.as<double>(), grp, fsh, convd,
+                          act.data());
             for (int m = 0; m < M; ++m) st.iters[m] += inner.iters[m];
             st.matvecs += inner.matvecs;
             st.column_matvecs += inner.column_matvecs;

@@ -98,11 +98,14 @@ private:
     // columns have no such structure or no repeated right-hand side.
     bool detect_shifts(const double2* b, const double2* sc, int rows, int N, int M, cudaStream_t s,
                        std::vector<int>& grp, std::vector<double2>& f);
-    // x (all M columns) from x0 = 0 by GMRES on the seeds' Krylov spaces;
-    // stops each column at |D^-1 r| < tolv[m] |D^-1 b|
+    // x (the M columns but those with skip[m] set, device, may be null) from
+    // x0 = 0 by GMRES on the seeds' Krylov spaces; stops each column at
+    // |D^-1 r| < tolv[m] |D^-1 b|.  live (host, may be null) = !skip: seeds
+    // with no live member are not iterated.
     void gmres_shifted(Field& F, const double2* b, double2* x, int M, const double2* sc, const SolveOptions& opt,
                        SolveStats& st, bool recip32, bool real32, cudaStream_t s, const double* tolv,
-                       const std::vector<int>& grp, const std::vector<double2>& f);
+                       const std::vector<int>& grp, const std::vector<double2>& f, const int* skip,
+                       const int* live);
     void dots(const double2* V, size_t vstride, int nvec, const double2* w, int rows, int M, int conj,
               double2* out, cudaStream_t s, int shift = -1);
     void norms(const double2* w, int rows, int M, double* out, cudaStream_t s);
