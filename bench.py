@@ -143,10 +143,17 @@ class Workload:
         self.mono = bool(np.all(self.radius == self.radius[0]))
         self.M = len(eps) * self.K
 
-    def field(self, capi):
+    def field(self, capi, tuning=None):
         if self.mono:
-            return capi.Field(capi.FIELD_MONO, self.box, TOL, XI)
-        return capi.Field(capi.FIELD_POLY, self.box, TOL, XI, radius=self.radius)
+            return capi.Field(capi.FIELD_MONO, self.box, TOL, XI, tuning=tuning)
+        return capi.Field(capi.FIELD_POLY, self.box, TOL, XI, radius=self.radius, tuning=tuning)
+
+    def autotune(self, capi):
+        """The field autotuner's pick for this workload (batch of M columns,
+        fp32 reciprocal space as the inner solves run it)."""
+        kind = capi.FIELD_MONO if self.mono else capi.FIELD_POLY
+        return capi.autotune(kind, self.box, TOL, XI, self.pos, self.M, radius=None if self.mono else self.radius,
+                             recip_fp32=True, real_fp32=False)
 
 
 METRIC = "solves/s at N=4000, res 1e-6: batched mixed-prec vs plain; matvec % HBM peak"
@@ -357,9 +364,9 @@ class Timed:
     with CUDA events after an L2 flush (a 256 MB write outside the timed
     interval)."""
 
-    def __init__(self, wl, capi, torch, dev, args, method, flush, dist=None):
+    def __init__(self, wl, capi, torch, dev, args, method, flush, dist=None, field=None):
         self.wl, self.capi, self.torch, self.dist, self.flush = wl, capi, torch, dist, flush
-        self.F = wl.field(capi)
+        self.F = wl.field(capi) if field is None else field
         self.B, self.X0, self.S = device_problem(wl, torch, dev)
         self.X = torch.empty_like(self.X0)
         self.M = self.B.shape[1]
@@ -671,6 +678,48 @@ def run_extras(args, capi, torch, dev, flush):
         del T
         torch.cuda.empty_cache()
     out["c4_adjoint"] = run_c4(args, torch)
+    out["autotuned"] = {name: run_autotuned(args, capi, torch, dev, flush, name) for name in ("monolayer", "poly3d")}
+    return out
+
+
+def run_autotuned(args, capi, torch, dev, flush, name):
+    """The workload with the field autotuner's pick (xi, grid, support,
+    spread tile measured on this GPU) in place of the reference's rule:
+    tuning time, the pick, the batched solve timed like the headline, and
+    per-dipole errors against the fp64 solutions of both the tuned operator
+    and the rule's operator."""
+    wl = Workload(name)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    pick = wl.autotune(capi)
+    torch.cuda.synchronize()
+    tune_s = time.perf_counter() - t0
+    steps = max(2, min(args.steps, 5))
+    T = Timed(wl, capi, torch, dev, args, capi.METHOD_GMRES, flush, field=wl.field(capi, tuning=pick))
+    T.warm(max(1, min(args.warmup, 3)))
+    T.reports.clear()
+    t = T.timed(steps)
+    rel = T.true_residuals()
+    conv = int(np.sum(rel <= TOL))
+    acc, _ = T.accuracy()
+    rule = wl.field(capi)
+    rule.set_positions(wl.pos)
+    Xrule = fp64_reference_solution(rule, T.B, T.X0, T.S, capi)
+    vs_rule = dipole_errors(T.X, Xrule, len(wl.pos))
+    info = T.F.info()
+    out = {
+        "workload": wl.label, "tune_s": round(tune_s, 3),
+        "pick": {"xi": pick["xi"], "grid": list(info["grid"]), "support": info["stencil"], "tile": list(pick["tile"])},
+        "rule": {"xi": XI, "grid": list(rule.info()["grid"]), "support": rule.info()["stencil"], "tile": [8, 8]},
+        "apply_ms": round(pick["apply_ms"], 4), "apply_ms_rule": round(pick["apply_ms_rule"], 4),
+        "operator_error": pick["error"], "operator_error_rule": pick["error_rule"],
+        "error_bound": pick["error_bound"], "candidates": pick["candidates"], "accepted": pick["accepted"],
+        "value": round(conv * steps / (t / 1e3), 3), "unit": "solves/s", "ms_per_step": round(t / steps, 3),
+        "converged_per_step": conv, "rhs_per_step": T.M, "max_true_rel_resid": float(rel.max()),
+        "accuracy": acc, "vs_rule_fp64": vs_rule,
+    }
+    del T, rule
+    torch.cuda.empty_cache()
     return out
 
 

@@ -27,7 +27,8 @@ NVCC = os.environ.get("NVCC", "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 LIB = os.path.join(HERE, "libcumpm_b200.so")
 
-LIB_SOURCES = ["mpm_tables.cpp", "mpm_profile.cpp", "mpm_fft.cu", "mpm_field.cu", "mpm_poly.cu", "mpm_adjoint.cu", "mpm_krylov.cu", "mpm_solver.cpp", "mpm_capi.cpp", "mpm_noalloc.cu"]
+LIB_SOURCES = ["mpm_tables.cpp", "mpm_profile.cpp", "mpm_fft.cu", "mpm_field.cu", "mpm_poly.cu", "mpm_adjoint.cu",
+               "mpm_krylov.cu", "mpm_solver.cpp", "mpm_capi.cpp", "mpm_noalloc.cu", "mpm_tune.cpp"]
 NVFLAGS = ["-O3", "-std=c++17", "-lineinfo", "--expt-relaxed-constexpr", "-Xcompiler", "-fPIC",
            "-Xcompiler", "-fvisibility=hidden", "-I" + CSRC, "-I" + INCLUDE] + ARCH
 

@@ -35,6 +35,8 @@ EXPORTS = [
     "mpm_poly_quad_tables", "mpm_poly_quad_self",
     "mpm_profile_enable", "mpm_profile_reset", "mpm_profile_read", "mpm_kernel_launches",
     "mpm_field_apply_noalloc", "mpm_noalloc_scratch_bytes", "mpm_field_grad", "mpm_line_fft",
+    "mpm_field_create_tuned", "mpm_field_autotune", "mpm_tune_xi_candidates", "mpm_tune_next_size",
+    "mpm_solver_set_tuning", "mpm_solver_autotune",
 ]
 
 STAGES = ["spread", "fft_fwd", "kspace", "fft_inv", "contract", "real", "direct", "krylov", "precalc"]
@@ -59,6 +61,29 @@ class FieldInfo(C.Structure):
                 ("z_slots", C.c_int), ("num_pairs", C.c_longlong), ("rc", C.c_double), ("h", C.c_double * 3),
                 ("eta", C.c_double * 3), ("selfo", C.c_double), ("slab_fused", C.c_int),
                 ("single_layer", C.c_int)]
+
+
+class FieldTuning(C.Structure):
+    _fields_ = [("xi", C.c_double), ("grid", C.c_int * 3), ("support", C.c_int), ("tile", C.c_int * 2)]
+
+    def as_dict(self):
+        return {"xi": self.xi, "grid": tuple(self.grid), "support": self.support, "tile": tuple(self.tile)}
+
+
+class TuneReport(C.Structure):
+    _fields_ = [("apply_ms", C.c_double), ("apply_ms_rule", C.c_double), ("error", C.c_double),
+                ("error_rule", C.c_double), ("error_bound", C.c_double), ("candidates", C.c_int),
+                ("accepted", C.c_int)]
+
+
+def make_tuning(xi, grid=(0, 0, 0), support=0, tile=(0, 0)):
+    t = FieldTuning()
+    t.xi = float(xi)
+    for d in range(3):
+        t.grid[d] = int(grid[d])
+    t.support = int(support)
+    t.tile[0], t.tile[1] = int(tile[0]), int(tile[1])
+    return t
 
 
 def lib():
@@ -94,6 +119,17 @@ def lib():
         L.mpm_kernel_launches.restype = C.c_longlong
         L.mpm_line_fft.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_size_t, C.c_int, C.c_size_t, C.c_int, C.c_int,
                                    C.c_void_p, C.c_int, C.c_int, C.c_int, _ip, C.c_void_p]
+        L.mpm_field_create_tuned.argtypes = [C.POINTER(C.c_void_p), C.c_int, C.c_int, _dp, C.c_double,
+                                             C.POINTER(FieldTuning), _dp, C.c_int, C.c_int, _ip, C.c_int]
+        L.mpm_field_autotune.argtypes = [C.c_int, _dp, C.c_double, C.c_double, _dp, C.c_int, C.c_int, _ip, C.c_int,
+                                         _dp, _dp, _dp, C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(FieldTuning),
+                                         C.POINTER(TuneReport), C.c_void_p]
+        L.mpm_tune_xi_candidates.argtypes = [C.c_int, _dp, C.c_double, C.c_double, _dp, C.c_int, _dp, _ip, _ip, _dp,
+                                             C.c_int, _ip]
+        L.mpm_tune_next_size.argtypes = [C.c_int, C.c_int]
+        L.mpm_solver_set_tuning.argtypes = [C.c_void_p, C.POINTER(FieldTuning)]
+        L.mpm_solver_autotune.argtypes = [C.c_void_p, _dp, _dp, _dp, C.c_int, C.POINTER(FieldTuning),
+                                          C.POINTER(TuneReport)]
         L._mpm_typed = True
     return L
 
@@ -235,16 +271,24 @@ class Field:
     """Batched field operator A(omega) on CUDA tensors (see module docstring)."""
 
     def __init__(self, kind, box=None, errortol=1e-3, xi=0.5, mode=MODE_SOLVER_AX, radius=None, quad_idxs=None,
-                 solve_quads=False):
+                 solve_quads=False, tuning=None):
+        """tuning: a dict as ``autotune`` returns (xi, grid, support, tile;
+        zeros keep the rule); its xi replaces ``xi``."""
         L = lib()
         self._h = C.c_void_p()
         bx, bp = _arr(box if box is not None else [0.0, 0.0, 0.0])
         rad = None if radius is None else np.ascontiguousarray(radius, dtype=np.float64)
         qi = None if quad_idxs is None else np.ascontiguousarray(quad_idxs, dtype=np.int32)
-        check(L.mpm_field_create(C.byref(self._h), int(kind), int(mode), bp, float(errortol), float(xi),
-                                 None if rad is None else rad.ctypes.data_as(_dp), 0 if rad is None else len(rad),
-                                 int(bool(solve_quads) or qi is not None),
-                                 None if qi is None else qi.ctypes.data_as(_ip), 0 if qi is None else len(qi)))
+        tail = (None if rad is None else rad.ctypes.data_as(_dp), 0 if rad is None else len(rad),
+                int(bool(solve_quads) or qi is not None),
+                None if qi is None else qi.ctypes.data_as(_ip), 0 if qi is None else len(qi))
+        if tuning is None:
+            check(L.mpm_field_create(C.byref(self._h), int(kind), int(mode), bp, float(errortol), float(xi), *tail))
+        else:
+            t = make_tuning(tuning["xi"], tuning.get("grid", (0, 0, 0)), tuning.get("support", 0),
+                            tuning.get("tile", (0, 0)))
+            check(L.mpm_field_create_tuned(C.byref(self._h), int(kind), int(mode), bp, float(errortol),
+                                           C.byref(t), *tail))
         self.kind = kind
 
     def __del__(self):
@@ -331,3 +375,51 @@ class Field:
         check(lib().mpm_batch_solve(self._h, C.c_void_p(B.data_ptr()), C.c_void_p(X.data_ptr()), B.shape[1],
                                     C.c_void_p(self_coef.data_ptr()), C.byref(o), C.byref(r), _stream_ptr(stream)))
         return {k: getattr(r, k) for k, _ in r._fields_}
+
+
+def autotune(kind, box, errortol, xi, pos, M, radius=None, quad_idxs=None, solve_quads=False, recip_fp32=True,
+             real_fp32=False, stream=None):
+    """Tune a SOLVER_AX field (xi, grid, support, spread tile) for the
+    positions pos (N, 3, non-dimensional) and a batch of M columns; returns
+    the pick and the report as one dict (see mpm_field_autotune)."""
+    L = lib()
+    bx, bp = _arr(box)
+    p = np.ascontiguousarray(np.asarray(pos, dtype=np.float64))
+    x, y, z = (np.ascontiguousarray(p[:, d]) for d in range(3))
+    rad = None if radius is None else np.ascontiguousarray(radius, dtype=np.float64)
+    qi = None if quad_idxs is None else np.ascontiguousarray(quad_idxs, dtype=np.int32)
+    t, r = FieldTuning(), TuneReport()
+    check(L.mpm_field_autotune(int(kind), bp, float(errortol), float(xi),
+                               None if rad is None else rad.ctypes.data_as(_dp), 0 if rad is None else len(rad),
+                               int(bool(solve_quads) or qi is not None),
+                               None if qi is None else qi.ctypes.data_as(_ip), 0 if qi is None else len(qi),
+                               x.ctypes.data_as(_dp), y.ctypes.data_as(_dp), z.ctypes.data_as(_dp), len(p), int(M),
+                               int(bool(recip_fp32)), int(bool(real_fp32)), C.byref(t), C.byref(r),
+                               _stream_ptr(stream)))
+    out = t.as_dict()
+    out.update({k: getattr(r, k) for k, _ in r._fields_})
+    return out
+
+
+def tune_xi_candidates(kind, box, errortol, xi, radius=None):
+    """Host only: the tuner's first-stage xi candidates as a list of dicts
+    (xi, grid, support, rc)."""
+    L = lib()
+    bx, bp = _arr(box)
+    rad = None if radius is None else np.ascontiguousarray(radius, dtype=np.float64)
+    n = C.c_int()
+    args = (int(kind), bp, float(errortol), float(xi), None if rad is None else rad.ctypes.data_as(_dp),
+            0 if rad is None else len(rad))
+    check(L.mpm_tune_xi_candidates(*args, None, None, None, None, 0, C.byref(n)))
+    k = n.value
+    xs, gs, ps, rs = np.zeros(k), np.zeros(3 * k, np.int32), np.zeros(k, np.int32), np.zeros(k)
+    check(L.mpm_tune_xi_candidates(*args, xs.ctypes.data_as(_dp), gs.ctypes.data_as(_ip), ps.ctypes.data_as(_ip),
+                                   rs.ctypes.data_as(_dp), k, C.byref(n)))
+    return [{"xi": xs[i], "grid": tuple(int(g) for g in gs[3 * i:3 * i + 3]), "support": int(ps[i]), "rc": rs[i]}
+            for i in range(k)]
+
+
+def tune_next_size(n, smooth23=False):
+    """Host only: smallest length >= n with prime factors 2, 3, 5, 7 (or
+    2, 3 with smooth23)."""
+    return lib().mpm_tune_next_size(int(n), int(bool(smooth23)))

@@ -12,6 +12,7 @@
 #include "mpm_fft.h"
 #include "mpm_krylov.h"
 #include "mpm_solver.h"
+#include "mpm_tune.h"
 
 #include "mpm_capi_internal.h"
 #include "mpm_poly.cuh"
@@ -59,6 +60,66 @@ void copy_out(const std::vector<cd>& v, double* out, size_t cap) {
     if (cap < v.size()) throw std::invalid_argument("output buffer too small");
     std::memcpy(out, v.data(), v.size() * sizeof(cd));
 }
+
+mpm::FieldSpec field_spec(int kind, int mode, const double box[3], double errortol, double xi, const double* radius,
+                          int n_radius, int solve_quads, const int* quad_idxs, int n_quad_idxs) {
+    mpm::FieldSpec fs;
+    if (kind != MPM_FIELD_DIRECT && kind != MPM_FIELD_MONO && kind != MPM_FIELD_POLY)
+        throw std::invalid_argument("unknown field kind");
+    fs.kind = kind == MPM_FIELD_DIRECT ? mpm::FIELD_DIRECT : kind == MPM_FIELD_POLY ? mpm::FIELD_POLY : mpm::FIELD_MONO;
+    if (fs.kind == mpm::FIELD_POLY && (!radius || n_radius < 1))
+        throw std::invalid_argument("polydisperse field needs one radius per particle");
+    fs.solver_ax = mode == MPM_MODE_SOLVER_AX;
+    if (box) for (int d = 0; d < 3; ++d) fs.box[d] = box[d];
+    if (fs.kind != mpm::FIELD_DIRECT) need(box, "box");
+    fs.errortol = errortol;
+    fs.xi = xi;
+    if (radius) fs.radius.assign(radius, radius + n_radius);
+    fs.quads = solve_quads != 0;
+    if (quad_idxs) fs.quad_idxs.assign(quad_idxs, quad_idxs + n_quad_idxs);
+    return fs;
+}
+
+mpm::FieldTuning from_c(const mpm_field_tuning& t) {
+    mpm::FieldTuning r;
+    if (!(t.xi > 0)) throw std::invalid_argument("tuning: xi must be > 0");
+    r.xi = t.xi;
+    for (int d = 0; d < 3; ++d) {
+        if (t.grid[d] < 0 || (t.grid[d] > 0 && t.grid[d] < 8)) throw std::invalid_argument("tuning: grid sizes must be 0 or >= 8");
+        r.grid[d] = t.grid[d];
+    }
+    if (t.support < 0) throw std::invalid_argument("tuning: support must be >= 0");
+    r.support = t.support;
+    for (int d = 0; d < 2; ++d) {
+        if (t.tile[d] != 0 && t.tile[d] != 4 && t.tile[d] != 8 && t.tile[d] != 16)
+            throw std::invalid_argument("tuning: tile sizes must be 0, 4, 8 or 16");
+        r.tile[d] = t.tile[d];
+    }
+    if (r.tile[0] && r.tile[1] && r.tile[0] * r.tile[1] > 128)
+        throw std::invalid_argument("tuning: a spread tile has at most 128 columns");
+    return r;
+}
+
+void to_c(const mpm::FieldTuning& t, mpm_field_tuning* out) {
+    std::memset(out, 0, sizeof(*out));
+    out->xi = t.xi;
+    for (int d = 0; d < 3; ++d) out->grid[d] = t.grid[d];
+    out->support = t.support;
+    out->tile[0] = t.tile[0];
+    out->tile[1] = t.tile[1];
+}
+
+void to_c(const mpm::TuneReport& r, mpm_tune_report* out) {
+    std::memset(out, 0, sizeof(*out));
+    out->apply_ms = r.apply_ms;
+    out->apply_ms_rule = r.apply_ms_rule;
+    out->error = r.error;
+    out->error_rule = r.error_rule;
+    out->error_bound = r.error_bound;
+    out->candidates = r.candidates;
+    out->accepted = r.accepted;
+}
+
 
 }  // namespace
 
@@ -155,6 +216,28 @@ int mpm_solver_set_options(mpm_solver* s, int restart, int maxiter, int batch_al
         o.real_fp32 = real_fp32 != 0;
     });
 }
+int mpm_solver_set_tuning(mpm_solver* s, const mpm_field_tuning* tuning) {
+    return guard([&] {
+        need(s, "solver");
+        need(tuning, "tuning");
+        s->impl->set_tuning(from_c(*tuning));
+    });
+}
+int mpm_solver_autotune(mpm_solver* s, const double* x, const double* y, const double* z, int n,
+                        mpm_field_tuning* out, mpm_tune_report* report) {
+    return guard([&] {
+        need(s, "solver");
+        need(x, "x");
+        need(y, "y");
+        need(z, "z");
+        if (n <= 0) throw std::invalid_argument("autotune: empty coordinate set");
+        mpm::TuneReport rep;
+        const mpm::FieldTuning t = s->impl->autotune(std::vector<double>(x, x + n), std::vector<double>(y, y + n),
+                                                     std::vector<double>(z, z + n), &rep);
+        if (out) to_c(t, out);
+        if (report) to_c(rep, report);
+    });
+}
 int mpm_solver_iterations(const mpm_solver* s, int* out, size_t cap, size_t* n_out) {
     return guard([&] {
         need(s, "solver");
@@ -204,27 +287,70 @@ int mpm_near_calculate(mpm_near* nf, double* intensity, int n) {
     });
 }
 
+
 int mpm_field_create(mpm_field** out, int kind, int mode, const double box[3], double errortol, double xi,
                      const double* radius, int n_radius, int solve_quads, const int* quad_idxs, int n_quad_idxs) {
     return guard([&] {
         need(out, "out");
-        mpm::FieldSpec fs;
-        if (kind != MPM_FIELD_DIRECT && kind != MPM_FIELD_MONO && kind != MPM_FIELD_POLY)
-            throw std::invalid_argument("unknown field kind");
-        fs.kind = kind == MPM_FIELD_DIRECT ? mpm::FIELD_DIRECT : kind == MPM_FIELD_POLY ? mpm::FIELD_POLY : mpm::FIELD_MONO;
-        if (fs.kind == mpm::FIELD_POLY && (!radius || n_radius < 1))
-            throw std::invalid_argument("polydisperse field needs one radius per particle");
-        fs.solver_ax = mode == MPM_MODE_SOLVER_AX;
-        if (box) for (int d = 0; d < 3; ++d) fs.box[d] = box[d];
-        if (fs.kind != mpm::FIELD_DIRECT) need(box, "box");
-        fs.errortol = errortol;
-        fs.xi = xi;
-        if (radius) fs.radius.assign(radius, radius + n_radius);
-        fs.quads = solve_quads != 0;
-        if (quad_idxs) fs.quad_idxs.assign(quad_idxs, quad_idxs + n_quad_idxs);
+        const mpm::FieldSpec fs =
+            field_spec(kind, mode, box, errortol, xi, radius, n_radius, solve_quads, quad_idxs, n_quad_idxs);
         auto* f = new mpm::Field(fs);
         *out = new mpm_field{f, nullptr};
     });
+}
+int mpm_field_create_tuned(mpm_field** out, int kind, int mode, const double box[3], double errortol,
+                           const mpm_field_tuning* tuning, const double* radius, int n_radius, int solve_quads,
+                           const int* quad_idxs, int n_quad_idxs) {
+    return guard([&] {
+        need(out, "out");
+        need(tuning, "tuning");
+        const mpm::FieldTuning t = from_c(*tuning);
+        const mpm::FieldSpec fs = mpm::apply_tuning(
+            field_spec(kind, mode, box, errortol, t.xi, radius, n_radius, solve_quads, quad_idxs, n_quad_idxs), t);
+        auto* f = new mpm::Field(fs);
+        *out = new mpm_field{f, nullptr};
+    });
+}
+int mpm_field_autotune(int kind, const double box[3], double errortol, double xi, const double* radius, int n_radius,
+                       int solve_quads, const int* quad_idxs, int n_quad_idxs, const double* x, const double* y,
+                       const double* z, int n, int M, int recip_fp32, int real_fp32, mpm_field_tuning* out,
+                       mpm_tune_report* report, void* stream) {
+    return guard([&] {
+        need(out, "out");
+        need(x, "x");
+        need(y, "y");
+        need(z, "z");
+        if (!(errortol > 0 && errortol < 1) || !(xi > 0)) throw std::invalid_argument("invalid Ewald parameters");
+        const mpm::FieldSpec fs = field_spec(kind, MPM_MODE_SOLVER_AX, box, errortol, xi, radius, n_radius,
+                                             solve_quads, quad_idxs, n_quad_idxs);
+        mpm::TuneReport rep;
+        const mpm::FieldTuning t = mpm::autotune(fs, x, y, z, n, M, recip_fp32 != 0, real_fp32 != 0,
+                                                 static_cast<cudaStream_t>(stream), &rep);
+        to_c(t, out);
+        if (report) to_c(rep, report);
+    });
+}
+int mpm_tune_xi_candidates(int kind, const double box[3], double errortol, double xi, const double* radius,
+                           int n_radius, double* xi_out, int* grid_out, int* support_out, double* rc_out, int cap,
+                           int* n_out) {
+    return guard([&] {
+        need(n_out, "n_out");
+        if (!(errortol > 0 && errortol < 1) || !(xi > 0)) throw std::invalid_argument("invalid Ewald parameters");
+        const mpm::FieldSpec fs =
+            field_spec(kind, MPM_MODE_SOLVER_AX, box, errortol, xi, radius, n_radius, 0, nullptr, 0);
+        const auto c = mpm::tune_xi_candidates(fs);
+        *n_out = int(c.size());
+        for (int i = 0; i < int(c.size()) && i < cap; ++i) {
+            if (xi_out) xi_out[i] = c[i].xi;
+            if (grid_out) for (int d = 0; d < 3; ++d) grid_out[3 * i + d] = c[i].grid[d];
+            if (support_out) support_out[i] = c[i].support;
+            if (rc_out) rc_out[i] = c[i].rc;
+        }
+    });
+}
+int mpm_tune_next_size(int n, int smooth23) {
+    if (n < 1 || n > (1 << 24)) return -1;
+    return smooth23 ? mpm::tune_next_smooth23(n) : mpm::tune_next_fast(n);
 }
 void mpm_field_destroy(mpm_field* f) {
     if (!f) return;

@@ -35,7 +35,7 @@ namespace mpm {
 
 // ---------------------------------------------------------------- geometry
 
-EwaldGeom make_ewald_geom(const double box[3], double errortol, double xi) {
+EwaldGeom make_ewald_geom(const double box[3], double errortol, double xi, const int* grid, int support) {
     EwaldGeom g;
     double rc = std::sqrt(-std::log(errortol)) / xi;
     if (rc < 2.0) rc = 2.0;
@@ -46,9 +46,11 @@ EwaldGeom make_ewald_geom(const double box[3], double errortol, double xi) {
     g.kcut = 2.0 * xi * xi * rc;
     for (int d = 0; d < 3; ++d) {
         g.ng[d] = static_cast<int>(std::ceil(1.0 + box[d] * g.kcut / kPi));
+        if (grid && grid[d] > 0) g.ng[d] = grid[d];
         g.h[d] = box[d] / g.ng[d];
     }
     g.P = static_cast<int>(std::ceil(-2.0 * std::log(errortol) / kPi));
+    if (support > 0) g.P = support;
     g.off = g.P / 2;
     for (int d = 0; d < 3; ++d) g.eta[d] = g.P * std::pow(g.h[d] * xi, 2) / kPi;
     g.spread_const = std::pow(2.0 * xi * xi / kPi, 1.5) * std::sqrt(1.0 / (g.eta[0] * g.eta[1] * g.eta[2]));
@@ -379,7 +381,10 @@ __global__ void __launch_bounds__(256) k_spread_plan(const int4* __restrict__ ba
         w64T[trow * wlen + t] = wloc[t];
         w32T[trow * wlen + t] = static_cast<float>(wloc[t]);
     }
-    // contributor list per (x, y) column in candidate order, -1 = too many
+    // contributor list per (x, y) column in candidate order, -1 = too many.
+    // A one-slot tile (TZ = Zs = 1) stores the x-y weight times the
+    // candidate's z weight, the factor its spread kernel applies.
+    const bool premul = TZ == 1 && g.Zs == 1;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
     for (int col = warp; col < ncol; col += nwarp) {
         const int lx = col / TY, ly = col % TY;
@@ -395,8 +400,9 @@ __global__ void __launch_bounds__(256) k_spread_plan(const int4* __restrict__ ba
             const unsigned hit = __ballot_sync(0xffffffffu, wxy != 0.0);
             const int at = n + __popc(hit & ((1u << lane) - 1u));
             if (wxy != 0.0 && at < kSpreadListCap) {
-                lw64[lrow + at] = wxy;
-                lw32[lrow + at] = wxy32;
+                const double wz = premul ? wloc[c * wlen + TX + TY] : 1.0;
+                lw64[lrow + at] = premul ? wxy * wz : wxy;
+                lw32[lrow + at] = premul ? wxy32 * static_cast<float>(wz) : wxy32;
                 lcT[lrow + at] = c;
             }
             n += __popc(hit);
@@ -486,12 +492,14 @@ __global__ void __launch_bounds__(256) k_spread_planned(const double2* __restric
 
 // Spread with the per-frame plan for one-slot tiles (a single layer): the
 // tile's candidate moments and every (x, y) column's contributor list
-// (candidate, x-y weight times the candidate's z weight -- 1 for a layer)
-// are staged in shared memory first, all loads in flight together; then a
-// warp per column, lanes over the chunk's grid columns, walks the list by
-// broadcast reads: a contribution costs three shared loads and an FMA, and
-// the warp's stores are one contiguous row.  Same contributors in the same
-// order as k_spread_planned.
+// (candidate, x-y weight times the candidate's z weight, premultiplied by
+// the plan) are staged in shared memory first, a warp's loads for eight
+// columns in flight together; then a group of gsz lanes per column (gsz =
+// the chunk's grid columns rounded up to a power of two, at most 32), lanes
+// over those grid columns, walks the list by broadcast reads: a
+// contribution costs three shared loads and an FMA, and a group's stores are
+// one contiguous row.  Same contributors in the same order as
+// k_spread_planned.
 template <typename R>
 __global__ void __launch_bounds__(256) k_spread_planned_1z(const double2* __restrict__ X, int M, int N, int C,
                                                            const int* __restrict__ quad_map, GridView g, int TX,
@@ -533,24 +541,43 @@ __global__ void __launch_bounds__(256) k_spread_planned_1z(const double2* __rest
     for (int t = threadIdx.x; t < ncol; t += blockDim.x) lnS[t] = lnT[size_t(tile) * ncol + t];
     __syncthreads();
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
-    for (int col = warp; col < ncol; col += nwarp) {
-        const int nl = lnS[col];
-        const size_t lrow = (size_t(tile) * ncol + col) * kSpreadListCap;
-        for (int k = lane; k < nl; k += 32) {
-            const int c = lcT[lrow + k];
-            lcS[col * kSpreadListCap + k] = c;
-            lwS[col * kSpreadListCap + k] = lwT[lrow + k] * wTt[c * wlen + TX + TY];
+    constexpr int kCPW = 8;   // columns whose list loads a warp issues together
+    for (int col0 = warp; col0 < ncol; col0 += nwarp * kCPW) {
+        for (int k0 = 0; k0 < kSpreadListCap; k0 += 32) {
+            int cc[kCPW];
+            R ww[kCPW];
+#pragma unroll
+            for (int u = 0; u < kCPW; ++u) {
+                const int col = col0 + u * nwarp, k = k0 + lane;
+                cc[u] = -1;
+                if (col < ncol && k < lnS[col]) {
+                    const size_t lrow = (size_t(tile) * ncol + col) * kSpreadListCap;
+                    cc[u] = lcT[lrow + k];
+                    ww[u] = lwT[lrow + k];
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < kCPW; ++u) {
+                if (cc[u] < 0) continue;
+                const int col = col0 + u * nwarp, k = k0 + lane;
+                lcS[col * kSpreadListCap + k] = cc[u];
+                lwS[col * kSpreadListCap + k] = ww[u];
+            }
         }
     }
     __syncthreads();
-    for (int col = warp; col < ncol; col += nwarp) {
+    const int gsz = nb > 16 ? 32 : nb > 8 ? 16 : nb > 4 ? 8 : 4;
+    const int per = 32 / gsz, sub = lane / gsz, sl = lane % gsz;
+    for (int col0 = warp * per; col0 < ncol; col0 += nwarp * per) {
+        const int col = col0 + sub;
+        if (col >= ncol) continue;
         const int lx = col / TY, ly = col % TY;
         const int x = x0 + lx, y = y0 + ly;
-        if (x >= g.Nx || y >= g.Ny) continue;   // uniform over the warp
+        if (x >= g.Nx || y >= g.Ny) continue;
         const int nl = lnS[col];
         const int* lc = lcS + col * kSpreadListCap;
         const R* lw = lwS + col * kSpreadListCap;
-        for (int bb = lane; bb < nb; bb += 32) {
+        for (int bb = sl; bb < nb; bb += gsz) {
             cplx<R> acc = mk<R>(0, 0);
             if (nl >= 0) {
                 for (int k = 0; k < nl; ++k) fma_rc(acc, lw[k], pv[lc[k] * bc + bb]);
@@ -941,6 +968,88 @@ __global__ void k_contract(const cplx<R>* __restrict__ grid, GridView g, int M, 
     }
 }
 
+// k_contract for one stored z slot (single layer) and few grid columns
+// (B = 3M <= 16, dipoles only): a CTA holds 128 / gsz targets, gsz = B
+// rounded up to a power of two lanes each, instead of one target per CTA
+// with B of its 32 lanes busy.  Same arithmetic, in the same order, as
+// k_contract<R, 1, SXY>.
+constexpr int kContractSmallMaxT = 32;   // targets per CTA (gsz >= 4)
+
+template <typename R, int SXY>
+__global__ void __launch_bounds__(128) k_contract_small(const cplx<R>* __restrict__ grid, GridView g, int M, int Nt,
+                                                        const int4* __restrict__ base, const R* __restrict__ w1,
+                                                        double factor, double2* __restrict__ Y, int negate,
+                                                        const int* __restrict__ order, int accumulate,
+                                                        const double2* __restrict__ jsc, int gsz) {
+    __shared__ R wxy[kContractSmallMaxT][2 * kMaxStencil];
+    __shared__ long long offxy[kContractSmallMaxT][2 * kMaxStencil];
+    __shared__ R wzs[kContractSmallMaxT];
+    __shared__ int zos[kContractSmallMaxT];
+    const int B = 3 * M;
+    const int per = blockDim.x / gsz;
+    const int slot = threadIdx.x / gsz, sl = threadIdx.x % gsz;
+    const int jj = blockIdx.x * per + slot;
+    const bool live = jj < Nt;
+    const int j = live ? (order ? order[jj] : jj) : 0;
+    if (live) {
+        const int4 bs = base[j];
+        const int zc = g.off - g.offz;   // the stored slot's entry of the z stencil
+        for (int t = sl; t < 2 * g.S + 1; t += gsz) {
+            if (t < 2 * g.S) {
+                const int d = t / g.S, o = t % g.S;
+                wxy[slot][t] = w1[(size_t(j) * 3 + d) * g.S + o];
+                const int dd = o - g.off;
+                if (d == 0) offxy[slot][t] = (long long)pmod(bs.x + dd, g.Nx) * g.Ny * g.Zs * B;
+                else offxy[slot][t] = (long long)pmod(bs.y + dd, g.Ny) * g.Zs * B;
+            } else {
+                wzs[slot] = w1[(size_t(j) * 3 + 2) * g.S + zc];
+                const int dz = zc - g.off;
+                zos[slot] = g.pruned ? bs.z + dz : pmod(bs.z + dz, g.Nz);
+            }
+        }
+    }
+    __syncthreads();
+    if (!live) return;
+    const int S = SXY > 0 ? SXY : g.S;
+    const R* w = wxy[slot];
+    const long long* off = offxy[slot];
+    const R wz = wzs[slot];
+    for (int b = sl; b < B; b += gsz) {
+        const int comp = b / M;
+        const int zo = zos[slot] * B + b;
+        cplx<R> acc = mk<R>(0, 0);
+        for (int ox = 0; ox < S; ++ox) {
+            const R wx = w[ox];
+            const cplx<R>* gx = grid + off[ox];
+            auto cell = [&](int oy) {
+                cplx<R> a2 = mk<R>(0, 0);
+                fma_rc(a2, wz, gx[off[S + oy] + zo]);
+                fma_rc(acc, wx * w[S + oy], a2);
+            };
+            if constexpr (SXY > 0) {
+#pragma unroll
+                for (int oy = 0; oy < SXY; ++oy) cell(oy);
+            } else {
+                for (int oy = 0; oy < S; ++oy) cell(oy);
+            }
+        }
+        double2 v = to_d(acc);
+        v.x *= factor; v.y *= factor;
+        if (negate) { v.x = -v.x; v.y = -v.y; }
+        const int m = b - comp * M;
+        const size_t row = size_t(3 * j + comp);
+        if (accumulate) {
+            v += Y[row * M + m];
+            if (jsc) {
+                const double2 sv = jsc[size_t(j) * M + m];
+                const double den = sv.x * sv.x + sv.y * sv.y;
+                if (den > 1e-30) v = v * make_double2(sv.x / den, -sv.y / den);
+            }
+        }
+        Y[row * M + m] = v;
+    }
+}
+
 // ------------------------------------------------------------ neighbours
 
 struct CellArgs {
@@ -1085,20 +1194,22 @@ struct RealArgs {
 // rather than two per pair.  Accumulation order is the pair order.
 constexpr int kPairBatch = 4;
 
+// pairs p0, p0 + stride, p0 + 2 stride, ... below p1 (stride 1: all of
+// them in order)
 template <typename R>
 __device__ __forceinline__ void real_dipole_pairs(const double2* __restrict__ X, int M, int m, int p0, int p1,
-                                                  const int* __restrict__ src, const R* __restrict__ T,
-                                                  cplx<R>& e0, cplx<R>& e1, cplx<R>& e2) {
-    for (int p = p0; p < p1; p += kPairBatch) {
+                                                  int stride, const int* __restrict__ src,
+                                                  const R* __restrict__ T, cplx<R>& e0, cplx<R>& e1, cplx<R>& e2) {
+    for (int p = p0; p < p1; p += kPairBatch * stride) {
         int ii[kPairBatch];
         R dx[kPairBatch], dy[kPairBatch], dz[kPairBatch], pe[kPairBatch], pa[kPairBatch];
         cplx<R> px[kPairBatch], py[kPairBatch], pz[kPairBatch];
 #pragma unroll
-        for (int u = 0; u < kPairBatch; ++u) ii[u] = (p + u < p1) ? src[p + u] : -1;
+        for (int u = 0; u < kPairBatch; ++u) ii[u] = (p + u * stride < p1) ? src[p + u * stride] : -1;
 #pragma unroll
         for (int u = 0; u < kPairBatch; ++u) {
             if (ii[u] >= 0) {
-                const R* t = T + 8 * size_t(p + u);
+                const R* t = T + 8 * size_t(p + u * stride);
                 dx[u] = t[0]; dy[u] = t[1]; dz[u] = t[2]; pe[u] = t[3]; pa[u] = t[4];
                 const double2* xi = X + size_t(3 * ii[u]) * M + m;
                 px[u] = to_r<R>(xi[0]);
@@ -1134,11 +1245,29 @@ __global__ void __launch_bounds__(128) k_real(const double2* __restrict__ X, dou
     const double sign = (a.solver_ax || a.pairs_plus) ? 1.0 : -1.0;
     const double selfc = selfv ? selfv[j] : a.selfo;  // polydisperse: self value of the particle's radius class
     const int qt = (QUADS && quad_map && j < a.N) ? quad_map[j] : -1;
-    for (int m = lane; m < M; m += 32) {
+    // fewer than 32 columns (dipoles only): the warp splits into 32 / gsz
+    // groups of gsz lanes (gsz = M rounded up to a power of two); group g
+    // takes pairs p0 + g, p0 + g + 32/gsz, ... and the groups' sums meet in a
+    // fixed shuffle tree
+    const int gsz = (!QUADS && M < 32) ? (M <= 1 ? 1 : M <= 2 ? 2 : M <= 4 ? 4 : M <= 8 ? 8 : 16) : 32;
+    const int ng = 32 / gsz, grp = lane / gsz;
+    for (int m0 = 0; m0 < M; m0 += gsz) {
+        const int m = m0 + lane % gsz;
         cplx<R> e0 = mk<R>(0, 0), e1 = e0, e2 = e0;
         double2 G[5] = {make_double2(0, 0), make_double2(0, 0), make_double2(0, 0), make_double2(0, 0),
                         make_double2(0, 0)};
-        if constexpr (!QUADS) real_dipole_pairs<R>(X, M, m, p0, p1, src, T, e0, e1, e2);
+        if constexpr (!QUADS) {
+            if (m < M) real_dipole_pairs<R>(X, M, m, p0 + grp, p1, ng, src, T, e0, e1, e2);
+            for (int o = gsz; o < 32; o <<= 1) {
+                e0.x += __shfl_xor_sync(0xffffffffu, e0.x, o);
+                e0.y += __shfl_xor_sync(0xffffffffu, e0.y, o);
+                e1.x += __shfl_xor_sync(0xffffffffu, e1.x, o);
+                e1.y += __shfl_xor_sync(0xffffffffu, e1.y, o);
+                e2.x += __shfl_xor_sync(0xffffffffu, e2.x, o);
+                e2.y += __shfl_xor_sync(0xffffffffu, e2.y, o);
+            }
+        }
+        if (m >= M || grp != 0) continue;
         for (int p = p0; QUADS && p < p1; ++p) {
             const int i = src[p];
             const R* t = T + 8 * size_t(p);
@@ -1374,8 +1503,19 @@ inline int nblk(long long n, int b) { return int((n + b - 1) / b); }
 
 Field::Field(const FieldSpec& spec) : spec_(spec) {
     if (spec_.kind == FIELD_MONO) {
-        geom_ = make_ewald_geom(spec_.box, spec_.errortol, spec_.xi);
+        geom_ = make_ewald_geom(spec_.box, spec_.errortol, spec_.xi, spec_.grid, spec_.support);
         if (2 * geom_.off + 1 > kMaxStencil) throw std::runtime_error("Ewald stencil wider than supported (errortol too small)");
+        // a spread tile reaches at most 8 bins per axis (the spread kernels'
+        // bin lists) and holds at most 128 (x, y) columns
+        for (int d = 0; d < 2; ++d) {
+            const int t = spec_.tile[d];
+            if (t != 0 && (t < 1 || (t + 2 * geom_.off + t - 1) / t + 1 > 8))
+                throw std::invalid_argument("spread tile " + std::to_string(t) + " too small for stencil half width " +
+                                            std::to_string(geom_.off));
+        }
+        if (spec_.tile[0] * spec_.tile[1] > 128 || (spec_.tile[0] == 0 ? 8 : spec_.tile[0]) *
+                                                           (spec_.tile[1] == 0 ? 8 : spec_.tile[1]) > 128)
+            throw std::invalid_argument("a spread tile holds at most 128 columns");
         tables_ = build_mono_tables(spec_.xi);
         tab_r_.ensure(sizeof(double) * kTableSize);
         tab_f_.ensure(sizeof(double) * kTableSize * T_COUNT);
@@ -1611,8 +1751,8 @@ void Field::build_stencil(PointSet& ps, cudaStream_t s, bool bins) {
                                             ps.w32.as<float>());
     MPM_LAUNCH();
     if (!bins) return;
-    ps.tile[0] = 8;
-    ps.tile[1] = 8;
+    ps.tile[0] = spec_.tile[0] > 0 ? spec_.tile[0] : 8;
+    ps.tile[1] = spec_.tile[1] > 0 ? spec_.tile[1] : 8;
     ps.tile[2] = (gv_.pruned && gv_.Zs <= 16) ? gv_.Zs : 8;
     ps.nb[0] = (gv_.Nx + ps.tile[0] - 1) / ps.tile[0];
     ps.nb[1] = (gv_.Ny + ps.tile[1] - 1) / ps.tile[1];
@@ -2008,7 +2148,17 @@ void Field::recip_on(const double2* X, double2* Y, int M, cplx<R>* grid, cudaStr
                                 spec_.solver_ax ? sources_.idx_sorted.as<int>() : nullptr, ov ? 1 : 0,
                                 ov ? ov->jacobi_sc : nullptr);
     };
-    if (gv_.Sz == 1) {
+    if (gv_.Sz == 1 && C == 3 && B <= 16) {
+        const int gsz = B <= 4 ? 4 : B <= 8 ? 8 : 16;
+        const int per = 128 / gsz;
+        auto small = [&](auto kern) {
+            kern<<<nblk(nt, per), 128, 0, s>>>(grid, gv_, M, nt, tg.base.as<int4>(), tw, factor, Y, 0,
+                                               spec_.solver_ax ? sources_.idx_sorted.as<int>() : nullptr,
+                                               ov ? 1 : 0, ov ? ov->jacobi_sc : nullptr, gsz);
+        };
+        if (gv_.S == 9) small(k_contract_small<R, 9>);
+        else small(k_contract_small<R, 0>);
+    } else if (gv_.Sz == 1) {
         if (gv_.S == 9) contract(k_contract<R, 1, 9>);
         else contract(k_contract<R, 1, 0>);
     } else if (gv_.Sz <= 9) {

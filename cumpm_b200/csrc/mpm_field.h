@@ -37,6 +37,12 @@ struct FieldSpec {
     std::vector<double> radius;       // per particle (direct, polydisperse) or empty
     bool quads = false;
     std::vector<int> quad_idxs;       // empty + quads => all particles
+    // overrides of the spectral-Ewald rules (0: the rule), set by the
+    // autotuner (mpm_tune.cu): grid points per axis, Gaussian support P,
+    // spread tile in x and y (monodisperse)
+    int grid[3] = {0, 0, 0};
+    int support = 0;
+    int tile[2] = {0, 0};
 };
 
 // Spectral-Ewald parameters (monodisperse_ewald_electric_field.cu:546-616).
@@ -50,7 +56,9 @@ struct EwaldGeom {
     double spread_const = 0;  // (2 xi^2/pi)^1.5 / sqrt(eta_x eta_y eta_z)
 };
 
-EwaldGeom make_ewald_geom(const double box[3], double errortol, double xi);
+// grid / support: overrides of the rules (null / 0: the rule)
+EwaldGeom make_ewald_geom(const double box[3], double errortol, double xi, const int* grid = nullptr,
+                          int support = 0);
 
 // Polydisperse parameters (polydisperse_ewald_electric_field.cu:2039-2112)
 // and radius classes (:39-84).
@@ -66,7 +74,8 @@ struct PolyGeom {
     std::vector<int> cls;        // class of each particle
 };
 
-PolyGeom make_poly_geom(const double box[3], double errortol, double xi, const std::vector<double>& radii);
+PolyGeom make_poly_geom(const double box[3], double errortol, double xi, const std::vector<double>& radii,
+                        const int* grid = nullptr, int support = 0);
 
 // Device-side description of the stored part of the grid.
 struct GridView {

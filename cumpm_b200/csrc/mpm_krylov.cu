@@ -48,6 +48,43 @@ __global__ void __launch_bounds__(256) k_dots1(const double2* __restrict__ V, si
     }
 }
 
+// k_dots1 for few columns (M < 16): threads run over the flat [row][M]
+// elements, (256 / M) * M of them per CTA, so that each thread keeps one
+// column m for the whole grid-stride loop (the stride is a multiple of M);
+// the CTA's per-column sums are then taken over the threads of that column
+// in a fixed order.  Same partial layout as k_dots1.
+__global__ void __launch_bounds__(256) k_dots1s(const double2* __restrict__ V, size_t vstride, int nvec,
+                                                const double2* __restrict__ w, int rows, int M, int conj,
+                                                double2* __restrict__ partial, int shift) {
+    __shared__ double2 red[8][256];
+    const int L = (256 / M) * M;
+    const int j = threadIdx.x;
+    const int i0 = blockIdx.z * 8;
+    const int nv = min(8, nvec - i0);
+    const size_t n = size_t(rows) * M;
+    double2 acc[8];
+    for (int k = 0; k < 8; ++k) acc[k] = make_double2(0, 0);
+    if (j < L) {
+        for (size_t t = size_t(blockIdx.x) * L + j; t < n; t += size_t(gridDim.x) * L) {
+            double2 wv = w[t];
+            if (shift >= 0) wv -= V[size_t(shift) * vstride + t];
+            for (int k = 0; k < nv; ++k) {
+                const double2 v = (shift >= 0 && i0 + k == nvec - 1) ? wv : V[size_t(i0 + k) * vstride + t];
+                if (conj) acc[k] += conjmul(v, wv);
+                else acc[k] += v * wv;
+            }
+        }
+    }
+    for (int k = 0; k < 8; ++k) red[k][j] = acc[k];
+    __syncthreads();
+    if (j < nv * M) {
+        const int k = j / M, m = j % M;
+        double2 sum = make_double2(0, 0);
+        for (int q = m; q < L; q += M) sum += red[k][q];
+        partial[(size_t(blockIdx.x) * nvec + i0 + k) * M + m] = sum;
+    }
+}
+
 // one warp per output: lanes stride over the per-CTA partials, then a fixed
 // shuffle tree (deterministic order)
 __global__ void k_dots2(const double2* __restrict__ partial, int gx, int nvec, int M, double2* __restrict__ out) {
@@ -774,6 +811,17 @@ void BatchSolver::dots(const double2* V, size_t vstride, int nvec, const double2
                        double2* out, cudaStream_t s, int shift) {
     StageScope scope(ST_KRYLOV, s);
     // four CTAs per SM: the sums are latency-bound, not bandwidth-bound
+    if (M < 16) {
+        const long long L = (256 / M) * M;
+        const int gx = int(std::max(1LL, std::min(592LL, (1LL * rows * M + L - 1) / L)));
+        partial_.ensure(sizeof(double2) * size_t(gx) * nvec * M);
+        k_dots1s<<<dim3(gx, 1, (nvec + 7) / 8), 256, 0, s>>>(V, vstride, nvec, w, rows, M, conj,
+                                                             partial_.as<double2>(), shift);
+        MPM_LAUNCH();
+        k_dots2<<<nblk((long long)nvec * M * 32, 256), 256, 0, s>>>(partial_.as<double2>(), gx, nvec, M, out);
+        MPM_LAUNCH();
+        return;
+    }
     const int gx = std::max(1, std::min(592, (rows + 7) / 8));
     partial_.ensure(sizeof(double2) * size_t(gx) * nvec * M);
     dim3 grd(gx, (M + 31) / 32, (nvec + 7) / 8);
@@ -1259,13 +1307,24 @@ void BatchSolver::solve(Field& F, const double2* b, double2* x, int M, const dou
         }
         if (!left) break;
         double best = 1e300;
+        int live_seeds = 0;
+        if (shifted) {
+            std::vector<char> seen(M, 0);
+            for (int m = 0; m < M; ++m)
+                if (act[m] && !seen[grp[m]]) {
+                    seen[grp[m]] = 1;
+                    ++live_seeds;
+                }
+        }
         for (int m = 0; m < M; ++m)
             if (act[m]) best = std::min(best, st.rel_resid[m]);
-        if (step == 0 && shifted && best >= 0.05) {
+        if (step == 0 && shifted && (best >= 0.05 || left >= 8 * live_seeds)) {
             // a poor initial guess (every unconverged column's residual at
-            // least 5% of |b|): those columns start again from x = 0 and
-            // their first correction is solved on the seeds' Krylov spaces;
-            // converged columns (a warm start) keep their x
+            // least 5% of |b|), or at least eight unconverged columns per
+            // seed (the seeds' Krylov spaces cost a small part of per-column
+            // solves even from x = 0): those columns start again from x = 0
+            // and their first correction is solved on the seeds' Krylov
+            // spaces; converged columns (a warm start) keep their x
             k_inner_tol<<<nblk(M, 128), 128, 0, s>>>(bn2, bn2, opt.tol, floor, tolv_.as<double>(), M);
             MPM_LAUNCH();
             SolveStats inner;

@@ -39,7 +39,8 @@ namespace mpm {
 
 // ------------------------------------------------------------ parameters
 
-PolyGeom make_poly_geom(const double box[3], double errortol, double xi, const std::vector<double>& radii) {
+PolyGeom make_poly_geom(const double box[3], double errortol, double xi, const std::vector<double>& radii,
+                        const int* grid, int support) {
     if (radii.empty()) throw std::invalid_argument("polydisperse field needs one radius per particle");
     PolyGeom g;
     // radius classes: a radius joins an existing class within 1e-5, classes
@@ -69,10 +70,12 @@ PolyGeom make_poly_geom(const double box[3], double errortol, double xi, const s
     const double kcut = 2.0 * xi * xi * rc;
     for (int d = 0; d < 3; ++d) {
         g.ng[d] = static_cast<int>(std::ceil(1.0 + box[d] * kcut / kPi));
+        if (grid && grid[d] > 0) g.ng[d] = grid[d];
         g.h[d] = box[d] / g.ng[d];
     }
     const double mean_h = (g.h[0] + g.h[1] + g.h[2]) / 3.0;
     g.P = static_cast<int>(std::ceil(2.0 / mean_h - 2.0 * std::log(errortol) / kPi));
+    if (support > 0) g.P = support;
     g.eta = g.P * std::pow(mean_h * xi, 2.0) / kPi;
     g.off_min = -static_cast<int>(std::floor((g.P - 1) / 2.0));
     const double rc_val = rc < 1.001 ? 1.001 : rc;
@@ -611,7 +614,7 @@ __global__ void __launch_bounds__(128) k_poly_quad_contract(const cplx<R>* __res
 void Field::poly_init() {
     if (spec_.quads && !spec_.solver_ax)
         throw std::runtime_error("polydisperse quadrupoles are computed at the particles (SOLVER_AX) only");
-    pgeom_ = make_poly_geom(spec_.box, spec_.errortol, spec_.xi, spec_.radius);
+    pgeom_ = make_poly_geom(spec_.box, spec_.errortol, spec_.xi, spec_.radius, spec_.grid, spec_.support);
     geom_ = EwaldGeom{};
     geom_.rc = pgeom_.rc;
     for (int d = 0; d < 3; ++d) {

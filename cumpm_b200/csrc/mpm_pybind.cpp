@@ -8,6 +8,7 @@
 #include <pybind11/pybind11.h>
 #include <pybind11/stl.h>
 
+#include <array>
 #include <complex>
 #include <string>
 #include <vector>
@@ -101,6 +102,40 @@ public:
     void set_jacobi(bool on) { check(mpm_solver_set_jacobi(s_, on)); }
     void set_options(int restart, int maxiter, bool batch_all, bool refine, double inner_tol, bool real_fp32) {
         check(mpm_solver_set_options(s_, restart, maxiter, batch_all, refine, inner_tol, real_fp32));
+    }
+    py::dict autotune(const std::vector<double>& x, const std::vector<double>& y, const std::vector<double>& z) {
+        if (x.size() != y.size() || x.size() != z.size())
+            throw py::value_error("Input coordinate vectors must have the exact same size.");
+        mpm_field_tuning t{};
+        mpm_tune_report r{};
+        int st;
+        {
+            py::gil_scoped_release nogil;
+            st = mpm_solver_autotune(s_, x.data(), y.data(), z.data(), int(x.size()), &t, &r);
+        }
+        check(st);
+        py::dict d;
+        d["xi"] = t.xi;
+        d["grid"] = py::make_tuple(t.grid[0], t.grid[1], t.grid[2]);
+        d["support"] = t.support;
+        d["tile"] = py::make_tuple(t.tile[0], t.tile[1]);
+        d["apply_ms"] = r.apply_ms;
+        d["apply_ms_rule"] = r.apply_ms_rule;
+        d["error"] = r.error;
+        d["error_rule"] = r.error_rule;
+        d["error_bound"] = r.error_bound;
+        d["candidates"] = r.candidates;
+        d["accepted"] = r.accepted;
+        return d;
+    }
+    void set_tuning(double xi, const std::array<int, 3>& grid, int support, const std::array<int, 2>& tile) {
+        mpm_field_tuning t{};
+        t.xi = xi;
+        for (int d = 0; d < 3; ++d) t.grid[d] = grid[d];
+        t.support = support;
+        t.tile[0] = tile[0];
+        t.tile[1] = tile[1];
+        check(mpm_solver_set_tuning(s_, &t));
     }
     std::vector<int> iterations() const {
         size_t n = 0;
@@ -216,7 +251,10 @@ PYBIND11_MODULE(_cuMPM, m) {
         .def("set_solver_options", &PyDipoleSolver::set_options, py::arg("restart") = 50, py::arg("maxiter") = 1000,
              py::arg("batch_all") = false, py::arg("refine") = false, py::arg("inner_tol") = 1e-4,
              py::arg("real_fp32") = false)
-        .def("get_iterations", &PyDipoleSolver::iterations);
+        .def("get_iterations", &PyDipoleSolver::iterations)
+        .def("autotune", &PyDipoleSolver::autotune)
+        .def("set_tuning", &PyDipoleSolver::set_tuning, py::arg("xi"), py::arg("grid") = std::array<int, 3>{0, 0, 0},
+             py::arg("support") = 0, py::arg("tile") = std::array<int, 2>{0, 0});
 
     py::class_<PyNearField>(m, "Near_Field")
         .def(py::init<const std::vector<double>&, const std::vector<cd>&, const std::vector<double>&, double, double,

@@ -252,47 +252,75 @@ void DipoleSolver::solve_batch(const std::vector<size_t>& freqs, const std::vect
                 frame_cap[freqs[f] * K * 3 + k * 3 + c] = avg[(f * K + k) * 3 + c] / double(N_);
 }
 
+void DipoleSolver::setup(size_t n) {
+    set_dims(n);
+    nondimensionalize();
+    if (!stream_) MPM_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+    solver_ = std::make_unique<BatchSolver>();
+}
+
+FieldSpec DipoleSolver::field_spec() const {
+    FieldSpec fs;
+    fs.solver_ax = true;
+    fs.quads = solve_quads_;
+    fs.quad_idxs = quad_idxs_;
+    for (int d = 0; d < 3; ++d) fs.box[d] = box_[d];
+    fs.errortol = tol_;
+    fs.xi = xi_;
+    if (field_type_ == "direct") {
+        fs.kind = FIELD_DIRECT;
+        fs.radius = radius_;
+    } else {
+        bool poly;
+        if (field_type_ == "polydisperse") poly = true;
+        else if (field_type_ == "monodisperse") poly = false;
+        else if (field_type_ == "auto") poly = !all_equal(radius_);
+        else throw std::runtime_error("Unknown field_type: " + field_type_);
+        fs.kind = poly ? FIELD_POLY : FIELD_MONO;
+        if (poly) fs.radius = radius_;
+    }
+    return fs;
+}
+
+std::vector<double> DipoleSolver::scaled(const std::vector<double>& v) const {
+    std::vector<double> out(v.size());
+    for (size_t i = 0; i < v.size(); ++i) out[i] = v[i] / length_scale_;
+    return out;
+}
+
+void DipoleSolver::set_tuning(const FieldTuning& t) {
+    tuning_ = t;
+    tuned_ = true;
+    field_.reset();
+}
+
+FieldTuning DipoleSolver::autotune(const std::vector<double>& x, const std::vector<double>& y,
+                                   const std::vector<double>& z, TuneReport* report) {
+    if (x.size() != y.size() || x.size() != z.size())
+        throw std::invalid_argument("Input coordinate vectors must have the exact same size.");
+    const size_t n = x.size();
+    if (n == 0) throw std::invalid_argument("autotune: empty coordinate set");
+    if (N_ == 0) setup(n);
+    else if (N_ != n) throw std::runtime_error("The number of particles has changed!");
+    const int M = int(opt_.batch_all ? eps_p_.size() * E0_.size() : E0_.size());
+    const std::vector<double> sx = scaled(x), sy = scaled(y), sz = scaled(z);
+    const FieldTuning t = mpm::autotune(field_spec(), sx.data(), sy.data(), sz.data(), int(n), M,
+                                        precision_ != PREC_DOUBLE, opt_.real_fp32, stream_, report);
+    set_tuning(t);
+    return t;
+}
+
 // dipole_solver.cu:495-607
 void DipoleSolver::compute(const std::vector<double>& x, const std::vector<double>& y, const std::vector<double>& z) {
     if (x.size() != y.size() || x.size() != z.size())
         throw std::invalid_argument("Input coordinate vectors must have the exact same size.");
     const size_t n = x.size();
     if (n == 0) return;
-    if (N_ == 0) {
-        set_dims(n);
-        nondimensionalize();
-        if (!stream_) MPM_CUDA(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
-        solver_ = std::make_unique<BatchSolver>();
-        FieldSpec fs;
-        fs.solver_ax = true;
-        fs.quads = solve_quads_;
-        fs.quad_idxs = quad_idxs_;
-        for (int d = 0; d < 3; ++d) fs.box[d] = box_[d];
-        fs.errortol = tol_;
-        fs.xi = xi_;
-        if (field_type_ == "direct") {
-            fs.kind = FIELD_DIRECT;
-            fs.radius = radius_;
-        } else {
-            bool poly;
-            if (field_type_ == "polydisperse") poly = true;
-            else if (field_type_ == "monodisperse") poly = false;
-            else if (field_type_ == "auto") poly = !all_equal(radius_);
-            else throw std::runtime_error("Unknown field_type: " + field_type_);
-            fs.kind = poly ? FIELD_POLY : FIELD_MONO;
-            if (poly) fs.radius = radius_;
-        }
-        field_ = std::make_unique<Field>(fs);
-    } else if (N_ != n) {
-        throw std::runtime_error("The number of particles has changed!");
-    }
+    if (N_ == 0) setup(n);
+    else if (N_ != n) throw std::runtime_error("The number of particles has changed!");
+    if (!field_) field_ = std::make_unique<Field>(tuned_ ? apply_tuning(field_spec(), tuning_) : field_spec());
     num_frames_++;
-    std::vector<double> sx(N_), sy(N_), sz(N_);
-    for (size_t i = 0; i < N_; ++i) {
-        sx[i] = x[i] / length_scale_;
-        sy[i] = y[i] / length_scale_;
-        sz[i] = z[i] / length_scale_;
-    }
+    const std::vector<double> sx = scaled(x), sy = scaled(y), sz = scaled(z);
     field_->set_positions(sx.data(), sy.data(), sz.data(), int(N_), stream_);
     const size_t K = E0_.size(), W = eps_p_.size();
     std::vector<cdouble> init;

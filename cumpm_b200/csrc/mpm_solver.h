@@ -15,6 +15,7 @@
 
 #include "mpm_field.h"
 #include "mpm_krylov.h"
+#include "mpm_tune.h"
 
 namespace mpm {
 
@@ -41,6 +42,15 @@ public:
 
     void compute(const std::vector<double>& x, const std::vector<double>& y, const std::vector<double>& z);
 
+    // Field tuning (mpm_tune.h): a given one, or one measured on these
+    // positions (physical units) for this solver's batch width and
+    // arithmetic.  Either replaces the field; later frames use it.
+    void set_tuning(const FieldTuning& t);
+    FieldTuning autotune(const std::vector<double>& x, const std::vector<double>& y, const std::vector<double>& z,
+                         TuneReport* report);
+    bool tuned() const { return tuned_; }
+    const FieldTuning& tuning() const { return tuning_; }
+
     std::vector<cdouble> get_eff_polarizability(bool physical) const;
     std::vector<cdouble> get_dipoles(bool physical) const;
     // the same values written straight into out (cap entries); returns the count
@@ -62,6 +72,9 @@ public:
 private:
     void set_dims(size_t n);
     void nondimensionalize();
+    void setup(size_t n);               // first frame: dimensions, units, stream, batch solver
+    FieldSpec field_spec() const;       // the field the reference's rules give
+    std::vector<double> scaled(const std::vector<double>& v) const;
     std::vector<cdouble> mean_field_guess(size_t w) const;
     std::vector<cdouble> guess(const std::vector<cdouble>& fd, const std::vector<cdouble>& fq, size_t w) const;
     void solve_batch(const std::vector<size_t>& freqs, const std::vector<std::vector<cdouble>>& guesses,
@@ -89,6 +102,8 @@ private:
     std::vector<int> iters_;
     SolveStats last_stats_;
 
+    FieldTuning tuning_;
+    bool tuned_ = false;
     std::unique_ptr<Field> field_;
     std::unique_ptr<BatchSolver> solver_;
     cudaStream_t stream_ = nullptr;
@@ -120,6 +135,8 @@ private:
     std::vector<cdouble> dips_;
     std::vector<double> px_, py_, pz_, fx_, fy_, fz_;
     double length_scale_ = 1.0;
+    FieldTuning tuning_;
+    bool tuned_ = false;
     std::unique_ptr<Field> field_;
     cudaStream_t stream_ = nullptr;
     DevBuf dX_, dY_;

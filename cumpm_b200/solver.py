@@ -137,6 +137,8 @@ class dipole_solver:
         if pos.ndim != 3 or pos.shape[-1] != 3:
             raise ValueError("positions must be of shape (num_particles, 3) or (num_frames, num_particles, 3)")
         pos = np.ascontiguousarray(pos, dtype=np.float64)
+        if getattr(self, "_autotune_pending", False):
+            self.autotune(pos[0])
         for frame in pos:
             self._solver.compute(frame[:, 0].tolist(), frame[:, 1].tolist(), frame[:, 2].tolist())
 
@@ -166,14 +168,36 @@ class dipole_solver:
 
     # ---- extensions beyond the reference API --------------------------------
     def set_solver_options(self, restart=50, maxiter=1000, batch_all=False, refine=False, inner_tol=1e-4,
-                           real_fp32=False):
+                           real_fp32=False, autotune=False):
         """GMRES restart/maxiter, all-frequency batching, mixed-precision refinement.
 
         Each fp32 inner solve of the refinement reduces a column's residual by
         at most inner_tol and stops earlier once that column's residual is
-        below half the outer tolerance.
+        below half the outer tolerance.  ``autotune=True`` tunes the field on
+        the next frame's positions before solving it (see ``autotune``).
         """
         self._solver.set_solver_options(restart, maxiter, batch_all, refine, inner_tol, real_fp32)
+        self._autotune_pending = bool(autotune)
+
+    def autotune(self, positions):
+        """Tune the Ewald field for these positions (N, 3) and this solver's
+        batch width and arithmetic: the splitting parameter xi, the grid, the
+        Gaussian support and the spread tile are measured on the device and
+        the fastest setting whose operator error stays within
+        max(tol, 1.1 x the error of the reference's rule setting) is kept for
+        every later frame.  Returns the pick (xi non-dimensional, zeros =
+        the rule) with its timings and errors."""
+        pos = np.ascontiguousarray(_to_numpy(positions), dtype=np.float64)
+        if pos.ndim != 2 or pos.shape[-1] != 3:
+            raise ValueError("positions must be of shape (num_particles, 3)")
+        out = self._solver.autotune(pos[:, 0].tolist(), pos[:, 1].tolist(), pos[:, 2].tolist())
+        self._autotune_pending = False
+        return dict(out)
+
+    def set_tuning(self, xi, grid=(0, 0, 0), support=0, tile=(0, 0)):
+        """Use this field setting (xi non-dimensional; zeros keep the rule)."""
+        self._solver.set_tuning(float(xi), tuple(int(g) for g in grid), int(support), tuple(int(t) for t in tile))
+        self._autotune_pending = False
 
     def get_iterations(self):
         """Krylov steps of every right-hand side solved so far (solve order)."""

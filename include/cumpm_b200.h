@@ -182,6 +182,56 @@ MPM_API int mpm_field_apply_noalloc(mpm_field* f, const void* X, void* Y, int M,
                                     int recip_fp32, int real_fp32, void* stream);
 MPM_API size_t mpm_noalloc_scratch_bytes(void);
 
+/* ---- field autotuner ---------------------------------------------------
+ * No counterpart in the reference, which fixes these by rule from xi and the
+ * tolerance (grid N = ceil(1 + L kcut / pi): monodisperse_ewald_electric_
+ * field.cu:546-616, polydisperse_ewald_electric_field.cu:2039-2112; spread
+ * tile 8 x 8).  A tuning overrides them; zeros keep the rule. */
+typedef struct mpm_field_tuning {
+    double xi;             /* Ewald splitting parameter (non-dimensional) */
+    int grid[3];           /* grid points per axis, 0: the rule */
+    int support;           /* Gaussian support P, 0: the rule */
+    int tile[2];           /* spread tile in x and y (monodisperse), 0: 8 */
+} mpm_field_tuning;
+
+typedef struct mpm_tune_report {
+    double apply_ms;       /* M-column apply of the pick (caller's arithmetic) */
+    double apply_ms_rule;  /* the same for the rule configuration */
+    double error;          /* relative operator error of the pick against a field of tolerance errortol/1000 */
+    double error_rule;     /* the same for the rule configuration */
+    double error_bound;    /* acceptance bound: max(errortol, 1.1 * error_rule) */
+    int candidates, accepted;
+} mpm_tune_report;
+
+/* mpm_field_create with the tuning's xi and overrides */
+MPM_API int mpm_field_create_tuned(mpm_field** out, int kind, int mode, const double box[3], double errortol,
+                                   const mpm_field_tuning* tuning, const double* radius, int n_radius,
+                                   int solve_quads, const int* quad_idxs, int n_quad_idxs);
+/* Measures candidate (xi, grid, support, tile) settings of a SOLVER_AX
+ * field on the device for the n positions (non-dimensional host arrays) and
+ * a batch of M columns in the given arithmetic, and writes the fastest one
+ * whose operator error stays within max(errortol, 1.1 x the rule's own
+ * error).  Direct fields: the rule (nothing to tune). */
+MPM_API int mpm_field_autotune(int kind, const double box[3], double errortol, double xi, const double* radius,
+                               int n_radius, int solve_quads, const int* quad_idxs, int n_quad_idxs, const double* x,
+                               const double* y, const double* z, int n, int M, int recip_fp32, int real_fp32,
+                               mpm_field_tuning* out, mpm_tune_report* report, void* stream);
+/* Host only: the xi candidates of the tuner's first stage (xi times fixed
+ * factors, those whose rule geometry is valid), with their rule grid,
+ * support and cutoff; n_out = count (at most cap written). */
+MPM_API int mpm_tune_xi_candidates(int kind, const double box[3], double errortol, double xi, const double* radius,
+                                   int n_radius, double* xi_out, int* grid_out, int* support_out, double* rc_out,
+                                   int cap, int* n_out);
+/* Host only: smallest length >= n with prime factors in {2, 3, 5, 7}
+ * (smooth23 = 0) or {2, 3} (smooth23 = 1). */
+MPM_API int mpm_tune_next_size(int n, int smooth23);
+/* Dipole solver: use this tuning for its field (before the first compute),
+ * or tune it on the given positions (physical units, as compute takes them)
+ * for the solver's batch width and arithmetic and keep the pick. */
+MPM_API int mpm_solver_set_tuning(mpm_solver* s, const mpm_field_tuning* tuning);
+MPM_API int mpm_solver_autotune(mpm_solver* s, const double* x, const double* y, const double* z, int n,
+                                mpm_field_tuning* out, mpm_tune_report* report);
+
 /* batched Krylov solve A X = B on device buffers (X holds the guess) */
 MPM_API int mpm_batch_solve(mpm_field* f, const void* B, void* X, int M, const void* self_coef,
                     const mpm_solve_options* opt, mpm_solve_report* report, void* stream);

@@ -69,6 +69,21 @@ def test_line_fft_matches_numpy(n, fp64):
                 assert split == want, (split, want)
 
 
+# grid lengths the field autotuner proposes for the benchmark geometries
+# (rule sizes rounded up to prime factors 2, 3, 5, 7 or to 2^a 3^b)
+TUNER_LENGTHS = [81, 84, 90, 96, 120, 375, 378, 384]
+
+
+@pytest.mark.parametrize("n", TUNER_LENGTHS)
+def test_line_fft_tuner_lengths(n):
+    for fp64 in (False, True):
+        tol = 1e-12 if fp64 else 2e-6
+        for layout in ("z", "x"):
+            for mode in (0, 1, 2):
+                err, _ = run_case(n, layout, 40, 3, fp64, mode, False)
+                assert err < tol, (fp64, layout, mode, err)
+
+
 @pytest.mark.parametrize("ncols", [1, 5, 17, 33, 70])
 def test_line_fft_ragged_column_groups(ncols):
     """Column counts that leave the last CTA's column group partly empty, and
