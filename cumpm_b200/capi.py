@@ -36,7 +36,7 @@ EXPORTS = [
     "mpm_profile_enable", "mpm_profile_reset", "mpm_profile_read", "mpm_kernel_launches",
     "mpm_field_apply_noalloc", "mpm_noalloc_scratch_bytes", "mpm_field_grad", "mpm_line_fft",
     "mpm_field_create_tuned", "mpm_field_autotune", "mpm_tune_xi_candidates", "mpm_tune_next_size",
-    "mpm_solver_set_tuning", "mpm_solver_autotune",
+    "mpm_solver_set_tuning", "mpm_solver_autotune", "mpm_field_set_bloch",
 ]
 
 STAGES = ["spread", "fft_fwd", "kspace", "fft_inv", "contract", "real", "direct", "krylov", "precalc"]
@@ -127,6 +127,7 @@ def lib():
         L.mpm_tune_xi_candidates.argtypes = [C.c_int, _dp, C.c_double, C.c_double, _dp, C.c_int, _dp, _ip, _ip, _dp,
                                              C.c_int, _ip]
         L.mpm_tune_next_size.argtypes = [C.c_int, C.c_int]
+        L.mpm_field_set_bloch.argtypes = [C.c_void_p, C.c_double, C.c_double]
         L.mpm_solver_set_tuning.argtypes = [C.c_void_p, C.POINTER(FieldTuning)]
         L.mpm_solver_autotune.argtypes = [C.c_void_p, _dp, _dp, _dp, C.c_int, C.POINTER(FieldTuning),
                                           C.POINTER(TuneReport)]
@@ -305,6 +306,12 @@ class Field:
         x, y, z = (np.ascontiguousarray(p[:, d]) for d in range(3))
         check(lib().mpm_field_set_positions(self._h, x.ctypes.data_as(_dp), y.ctypes.data_as(_dp),
                                             z.ctypes.data_as(_dp), len(p), _stream_ptr(stream)))
+
+    def set_bloch(self, kx, ky):
+        """Bloch wavevector (non-dimensional) of the periodic images: k-space
+        at k - (kx, ky, 0), a phase on every real-space pair (dipoles only;
+        (0, 0) is the plain operator)."""
+        check(lib().mpm_field_set_bloch(self._h, float(kx), float(ky)))
 
     def set_field_points(self, pts, stream=None):
         p = np.ascontiguousarray(np.asarray(pts, dtype=np.float64))

@@ -377,6 +377,7 @@ void Field::grad_bilinear(const double2* lam, const double2* p, int M, double2* 
     if (N_ == 0) throw std::runtime_error("gradient before set_positions");
     if (!spec_.solver_ax) throw std::runtime_error("gradients need the SOLVER_AX operator");
     if (Nq_ > 0) throw std::runtime_error("gradients are available for dipoles only");
+    if (bloch_on()) throw std::runtime_error("gradients are available without a Bloch wavevector only");
     if (M < 1) throw std::invalid_argument("M must be >= 1");
     if (spec_.kind == FIELD_DIRECT) {
         if (int(spec_.radius.size()) != N_) throw std::runtime_error("direct gradient needs one radius per particle");

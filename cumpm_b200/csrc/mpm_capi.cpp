@@ -397,6 +397,13 @@ int mpm_field_apply_part(mpm_field* f, const void* X, void* Y, int M, const void
                             static_cast<cudaStream_t>(stream));
     });
 }
+int mpm_field_set_bloch(mpm_field* f, double kx, double ky) {
+    return guard([&] {
+        need(f, "field");
+        if (!std::isfinite(kx) || !std::isfinite(ky)) throw std::invalid_argument("Bloch wavevector must be finite");
+        f->impl->set_bloch(kx, ky);
+    });
+}
 int mpm_field_info_get(const mpm_field* f, mpm_field_info* info) {
     return guard([&] {
         need(f, "field");

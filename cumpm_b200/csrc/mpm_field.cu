@@ -597,11 +597,13 @@ __global__ void __launch_bounds__(256) k_spread_planned_1z(const double2* __rest
 // (scale_kernel_joint, :1434-1486).  One thread per (voxel, rhs).
 template <typename R>
 __device__ __forceinline__ void khat_at(int ix, int iy, int iz, int Nx, int Ny, int Nz, double Lx, double Ly,
-                                        double Lz, R& kx, R& ky, R& kz) {
+                                        double Lz, R& kx, R& ky, R& kz, double bx = 0.0, double by = 0.0) {
     const double fx = (ix <= (Nx - 1) / 2) ? ix : ix - Nx;
     const double fy = (iy <= (Ny - 1) / 2) ? iy : iy - Ny;
     const double fz = (iz <= (Nz - 1) / 2) ? iz : iz - Nz;
-    const double ax = fx * 2.0 * kPi / Lx, ay = fy * 2.0 * kPi / Ly, az = fz * 2.0 * kPi / Lz;
+    // Bloch wavevector (bx, by): the direction of k - b
+    // (monodisperse_ewald_electric_field.cu:1329-1331)
+    const double ax = fx * 2.0 * kPi / Lx - bx, ay = fy * 2.0 * kPi / Ly - by, az = fz * 2.0 * kPi / Lz;
     const double km = sqrt(ax * ax + ay * ay + az * az);
     if (km < 1e-12) { kx = ky = kz = R(0); return; }
     kx = R(ax / km); ky = R(ay / km); kz = R(az / km);
@@ -609,7 +611,7 @@ __device__ __forceinline__ void khat_at(int ix, int iy, int iz, int Nx, int Ny, 
 
 template <typename R, bool QUADS>
 __global__ void k_scale(cplx<R>* __restrict__ grid, const R* __restrict__ sc, int Nx, int Ny, int Nz, double Lx,
-                        double Ly, double Lz, int M) {
+                        double Ly, double Lz, int M, double bx, double by) {
     const size_t V = size_t(Nx) * Ny * Nz;
     const size_t t = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
     if (t >= V * M) return;
@@ -617,7 +619,7 @@ __global__ void k_scale(cplx<R>* __restrict__ grid, const R* __restrict__ sc, in
     const int m = int(t % M);
     const int iz = int(v % Nz), iy = int((v / Nz) % Ny), ix = int(v / (size_t(Nz) * Ny));
     R kx, ky, kz;
-    khat_at<R>(ix, iy, iz, Nx, Ny, Nz, Lx, Ly, Lz, kx, ky, kz);
+    khat_at<R>(ix, iy, iz, Nx, Ny, Nz, Lx, Ly, Lz, kx, ky, kz, bx, by);
     constexpr int C = QUADS ? 8 : 3;
     cplx<R>* f = grid + v * (size_t(C) * M) + m;
     const cplx<R> f0 = f[0], f1 = f[size_t(M)], f2 = f[size_t(2) * M];
@@ -643,13 +645,18 @@ __global__ void k_scale(cplx<R>* __restrict__ grid, const R* __restrict__ sc, in
 
 // Per-voxel scale coefficients (compute_scale_coefficients_kernel,
 // monodisperse_ewald_electric_field.cu:1300-1404), float64.
+// With a Bloch wavevector (bx, by): |k - b| in the Green function, the
+// window deconvolution on the grid wavevector g itself
+// (monodisperse_ewald_electric_field.cu:1329-1331).
 __device__ void scale_coefs(int ix, int iy, int iz, int Nx, int Ny, int Nz, double Lx, double Ly, double Lz,
-                            double xi, const double* eta, double V, double out[4]) {
+                            double xi, const double* eta, double V, double out[4], double bx = 0.0,
+                            double by = 0.0) {
     const double fx = (ix <= (Nx - 1) / 2) ? ix : ix - Nx;
     const double fy = (iy <= (Ny - 1) / 2) ? iy : iy - Ny;
     const double fz = (iz <= (Nz - 1) / 2) ? iz : iz - Nz;
     const double gx = fx * 2.0 * kPi / Lx, gy = fy * 2.0 * kPi / Ly, gz = fz * 2.0 * kPi / Lz;
-    const double ks = gx * gx + gy * gy + gz * gz;
+    const double qx = gx - bx, qy = gy - by;
+    const double ks = qx * qx + qy * qy + gz * gz;
     const double km = sqrt(ks);
     if (km < 1e-12) { out[0] = out[1] = out[2] = out[3] = 0.0; return; }
     const double etaksq = ks - (gx * gx * eta[0] + gy * gy * eta[1] + gz * gz * eta[2]);
@@ -667,6 +674,7 @@ __device__ void scale_coefs(int ix, int iy, int iz, int Nx, int Ny, int Nz, doub
 struct ScaleArgs {
     int Nx, Ny, Nz;
     double Lx, Ly, Lz, xi, eta[3];
+    double bx = 0.0, by = 0.0;   // Bloch wavevector (full layout and column kernel)
 };
 
 __global__ void k_build_scale(ScaleArgs a, int quads, double* __restrict__ s64, float* __restrict__ s32) {
@@ -675,7 +683,7 @@ __global__ void k_build_scale(ScaleArgs a, int quads, double* __restrict__ s64, 
     if (v >= V) return;
     const int iz = int(v % a.Nz), iy = int((v / a.Nz) % a.Ny), ix = int(v / (size_t(a.Nz) * a.Ny));
     double o[4];
-    scale_coefs(ix, iy, iz, a.Nx, a.Ny, a.Nz, a.Lx, a.Ly, a.Lz, a.xi, a.eta, double(V), o);
+    scale_coefs(ix, iy, iz, a.Nx, a.Ny, a.Nz, a.Lx, a.Ly, a.Lz, a.xi, a.eta, double(V), o, a.bx, a.by);
     if (quads) {
         for (int c = 0; c < 4; ++c) { s64[4 * v + c] = o[c]; s32[4 * v + c] = float(o[c]); }
     } else {
@@ -700,9 +708,9 @@ __global__ void k_build_column(ScaleArgs a, int Z, const double* __restrict__ w2
     const double V = double(a.Nx) * a.Ny * a.Nz;
     for (int iz = threadIdx.x; iz < Nz; iz += blockDim.x) {
         double o[4];
-        scale_coefs(ix, iy, iz, a.Nx, a.Ny, Nz, a.Lx, a.Ly, a.Lz, a.xi, a.eta, V, o);
+        scale_coefs(ix, iy, iz, a.Nx, a.Ny, Nz, a.Lx, a.Ly, a.Lz, a.xi, a.eta, V, o, a.bx, a.by);
         double kx, ky, kz;
-        khat_at<double>(ix, iy, iz, a.Nx, a.Ny, Nz, a.Lx, a.Ly, a.Lz, kx, ky, kz);
+        khat_at<double>(ix, iy, iz, a.Nx, a.Ny, Nz, a.Lx, a.Ly, a.Lz, kx, ky, kz, a.bx, a.by);
         // single layer (Z = 1): weighted by |sum_o w_o exp(-2 pi i kz o / Nz)|^2
         const double s = w2 ? o[0] * w2[iz] : o[0];
         C6[iz * 6 + 0] = s * kx * kx; C6[iz * 6 + 1] = s * kx * ky; C6[iz * 6 + 2] = s * kx * kz;
@@ -1170,6 +1178,19 @@ __global__ void k_pair_coefs(const double* __restrict__ pgeo, long long np, cons
     }
 }
 
+// Bloch phase of every pair, exp(i phi) with phi = -(bx r_x + by r_y), r =
+// source - target (minimum image) (monodisperse_ewald_electric_field.cu:
+// 1749-1756).
+__global__ void k_pair_phase(const double* __restrict__ pgeo, long long np, double bx, double by,
+                             double2* __restrict__ P64, float2* __restrict__ P32) {
+    const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= np) return;
+    double sn, cs;
+    sincos(-(bx * pgeo[4 * p + 0] + by * pgeo[4 * p + 1]), &sn, &cs);
+    P64[p] = make_double2(cs, sn);
+    P32[p] = make_float2(float(cs), float(sn));
+}
+
 // ------------------------------------------------------------ real space
 
 // Gather by target (warp per target, lanes over right-hand sides) of the
@@ -1196,14 +1217,17 @@ constexpr int kPairBatch = 4;
 
 // pairs p0, p0 + stride, p0 + 2 stride, ... below p1 (stride 1: all of
 // them in order)
+// ph (may be null): the pairs' Bloch phases, each pair's term multiplied
+// by its phase.
 template <typename R>
 __device__ __forceinline__ void real_dipole_pairs(const double2* __restrict__ X, int M, int m, int p0, int p1,
                                                   int stride, const int* __restrict__ src,
-                                                  const R* __restrict__ T, cplx<R>& e0, cplx<R>& e1, cplx<R>& e2) {
+                                                  const R* __restrict__ T, const cplx<R>* __restrict__ ph,
+                                                  cplx<R>& e0, cplx<R>& e1, cplx<R>& e2) {
     for (int p = p0; p < p1; p += kPairBatch * stride) {
         int ii[kPairBatch];
         R dx[kPairBatch], dy[kPairBatch], dz[kPairBatch], pe[kPairBatch], pa[kPairBatch];
-        cplx<R> px[kPairBatch], py[kPairBatch], pz[kPairBatch];
+        cplx<R> px[kPairBatch], py[kPairBatch], pz[kPairBatch], pf[kPairBatch];
 #pragma unroll
         for (int u = 0; u < kPairBatch; ++u) ii[u] = (p + u * stride < p1) ? src[p + u * stride] : -1;
 #pragma unroll
@@ -1211,6 +1235,7 @@ __device__ __forceinline__ void real_dipole_pairs(const double2* __restrict__ X,
             if (ii[u] >= 0) {
                 const R* t = T + 8 * size_t(p + u * stride);
                 dx[u] = t[0]; dy[u] = t[1]; dz[u] = t[2]; pe[u] = t[3]; pa[u] = t[4];
+                if (ph) pf[u] = ph[p + u * stride];
                 const double2* xi = X + size_t(3 * ii[u]) * M + m;
                 px[u] = to_r<R>(xi[0]);
                 py[u] = to_r<R>(xi[size_t(M)]);
@@ -1222,9 +1247,15 @@ __device__ __forceinline__ void real_dipole_pairs(const double2* __restrict__ X,
             if (ii[u] >= 0) {
                 const cplx<R> rp = px[u] * dx[u] + py[u] * dy[u] + pz[u] * dz[u];
                 const cplx<R> k = rp * (pa[u] - pe[u]);
-                e0 += px[u] * pe[u] + k * dx[u];
-                e1 += py[u] * pe[u] + k * dy[u];
-                e2 += pz[u] * pe[u] + k * dz[u];
+                if (ph) {
+                    e0 += (px[u] * pe[u] + k * dx[u]) * pf[u];
+                    e1 += (py[u] * pe[u] + k * dy[u]) * pf[u];
+                    e2 += (pz[u] * pe[u] + k * dz[u]) * pf[u];
+                } else {
+                    e0 += px[u] * pe[u] + k * dx[u];
+                    e1 += py[u] * pe[u] + k * dy[u];
+                    e2 += pz[u] * pe[u] + k * dz[u];
+                }
             }
         }
     }
@@ -1235,7 +1266,8 @@ __global__ void __launch_bounds__(128) k_real(const double2* __restrict__ X, dou
                                               const int* __restrict__ off, const int* __restrict__ src,
                                               const R* __restrict__ T, const double* __restrict__ Qt,
                                               const int* __restrict__ quad_map,
-                                              const double2* __restrict__ sc, const double* __restrict__ selfv) {
+                                              const double2* __restrict__ sc, const double* __restrict__ selfv,
+                                              const cplx<R>* __restrict__ ph) {
     const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     if (warp >= a.Nt) return;
@@ -1257,7 +1289,7 @@ __global__ void __launch_bounds__(128) k_real(const double2* __restrict__ X, dou
         double2 G[5] = {make_double2(0, 0), make_double2(0, 0), make_double2(0, 0), make_double2(0, 0),
                         make_double2(0, 0)};
         if constexpr (!QUADS) {
-            if (m < M) real_dipole_pairs<R>(X, M, m, p0 + grp, p1, ng, src, T, e0, e1, e2);
+            if (m < M) real_dipole_pairs<R>(X, M, m, p0 + grp, p1, ng, src, T, ph, e0, e1, e2);
             for (int o = gsz; o < 32; o <<= 1) {
                 e0.x += __shfl_xor_sync(0xffffffffu, e0.x, o);
                 e0.y += __shfl_xor_sync(0xffffffffu, e0.y, o);
@@ -1847,12 +1879,41 @@ void Field::build_pairs(cudaStream_t s) {
     pair_T64_.ensure(sizeof(double) * 8 * np);
     pair_T32_.ensure(sizeof(float) * 8 * np);
     if (Nq_) pair_Q_.ensure(sizeof(double) * 8 * np);
+    if (bloch_on()) build_pair_phases(s);
     if (num_pairs_ > 0 && spec_.kind == FIELD_MONO) {  // polydisperse: poly_pair_coefs
         k_pair_coefs<<<nblk(num_pairs_, 256), 256, 0, s>>>(geo.as<double>(), num_pairs_, tab_r_.as<double>(),
                                                             tab_f_.as<double>(), Nq_ > 0, pair_T64_.as<double>(),
                                                             pair_T32_.as<float>(), pair_Q_.as<double>());
         MPM_LAUNCH();
     }
+}
+
+void Field::build_pair_phases(cudaStream_t s) {
+    const size_t np = std::max<long long>(1, num_pairs_);
+    pair_ph64_.ensure(sizeof(double2) * np);
+    pair_ph32_.ensure(sizeof(float2) * np);
+    if (num_pairs_ <= 0) return;
+    k_pair_phase<<<nblk(num_pairs_, 256), 256, 0, s>>>(pair_geo_.as<double>(), num_pairs_, spec_.bloch[0],
+                                                        spec_.bloch[1], pair_ph64_.as<double2>(),
+                                                        pair_ph32_.as<float2>());
+    MPM_LAUNCH();
+}
+
+void Field::set_bloch(double bx, double by) {
+    if (spec_.kind == FIELD_DIRECT && (bx != 0.0 || by != 0.0))
+        throw std::invalid_argument("a Bloch wavevector needs a periodic (Ewald) field");
+    if ((bx != 0.0 || by != 0.0) && spec_.quads)
+        throw std::invalid_argument("a Bloch wavevector is supported for dipoles only");
+    if (bx == spec_.bloch[0] && by == spec_.bloch[1]) return;
+    spec_.bloch[0] = bx;
+    spec_.bloch[1] = by;
+    // every k-space table and the pair phases follow the wavevector
+    scale_built_ = 0;
+    colK_Z_ = -1;
+    slab_Z_ = -1;
+    layer_colK_ = layer_taps_ = false;
+    if (spec_.kind == FIELD_POLY) poly_build_scale();
+    precalc_dirty_ = true;
 }
 
 void Field::build_scale(cudaStream_t s) {
@@ -1865,6 +1926,8 @@ void Field::build_scale(cudaStream_t s) {
     a.Lx = spec_.box[0]; a.Ly = spec_.box[1]; a.Lz = spec_.box[2];
     a.xi = spec_.xi;
     for (int d = 0; d < 3; ++d) a.eta[d] = geom_.eta[d];
+    a.bx = spec_.bloch[0];
+    a.by = spec_.bloch[1];
     k_build_scale<<<nblk((long long)V, 256), 256, 0, s>>>(a, Nq_ ? 1 : 0, scale64_.as<double>(), scale32_.as<float>());
     MPM_LAUNCH();
     scale_built_ = per;
@@ -1881,6 +1944,8 @@ void Field::build_column_kernel(cudaStream_t s) {
     a.Lx = spec_.box[0]; a.Ly = spec_.box[1]; a.Lz = spec_.box[2];
     a.xi = spec_.xi;
     for (int d = 0; d < 3; ++d) a.eta[d] = geom_.eta[d];
+    a.bx = spec_.bloch[0];
+    a.by = spec_.bloch[1];
     const size_t shm = sizeof(double) * 8 * gv_.Nz;
     if (shm > 48 * 1024)
         MPM_CUDA(cudaFuncSetAttribute(k_build_column, cudaFuncAttributeMaxDynamicSharedMemorySize, int(shm)));
@@ -1906,7 +1971,9 @@ void Field::build_column_kernel(cudaStream_t s) {
 }
 
 bool Field::use_slab() const {
-    return gv_.pruned && own_fft_ && ffty_.slab_ok(gv_.Zs, true) && ffty_.slab_ok(gv_.Zs, false);
+    // the fused pass's taps assume the grid wavevectors themselves (no Bloch
+    // shift); with one the pruned layout takes the column kernel
+    return gv_.pruned && own_fft_ && ffty_.slab_ok(gv_.Zs, true) && ffty_.slab_ok(gv_.Zs, false) && !bloch_on();
 }
 
 void Field::build_slab_taps(cudaStream_t s) {
@@ -2123,10 +2190,10 @@ void Field::recip_on(const double2* X, double2* Y, int M, cplx<R>* grid, cudaStr
             const R* sc = sizeof(R) == 4 ? reinterpret_cast<const R*>(scale32_.p) : reinterpret_cast<const R*>(scale64_.p);
             if (Nq_)
                 k_scale<R, true><<<nblk((long long)(V * M), 256), 256, 0, s>>>(grid, sc, gv_.Nx, gv_.Ny, gv_.Nz, spec_.box[0],
-                                                                               spec_.box[1], spec_.box[2], M);
+                                                                               spec_.box[1], spec_.box[2], M, spec_.bloch[0], spec_.bloch[1]);
             else
                 k_scale<R, false><<<nblk((long long)(V * M), 256), 256, 0, s>>>(grid, sc, gv_.Nx, gv_.Ny, gv_.Nz, spec_.box[0],
-                                                                                spec_.box[1], spec_.box[2], M);
+                                                                                spec_.box[1], spec_.box[2], M, spec_.bloch[0], spec_.bloch[1]);
             MPM_LAUNCH();
         }
         Profiler::get().end(ST_KSPACE, s);
@@ -2193,16 +2260,19 @@ void Field::real_part(const double2* X, double2* Y, int M, const double2* sc, bo
     const int thr = 128;
     const int blocks = nblk((long long)warps * 32, thr);
     StageScope scope(ST_REAL, s);
-    auto go = [&](auto kern, const auto* T) {
+    const bool ph = bloch_on();
+    auto go = [&](auto kern, const auto* T, const auto* P) {
         kern<<<blocks, thr, 0, s>>>(X, Y, a, pair_off_.as<int>(), pair_src_.as<int>(), T, pair_Q_.as<double>(),
-                                    quad_map_.as<int>(), sc, selfv);
+                                    quad_map_.as<int>(), sc, selfv, P);
     };
     if (fp32) {
-        if (a.quads) go(k_real<float, true>, pair_T32_.as<float>());
-        else go(k_real<float, false>, pair_T32_.as<float>());
+        const float2* P = ph ? pair_ph32_.as<float2>() : nullptr;
+        if (a.quads) go(k_real<float, true>, pair_T32_.as<float>(), P);
+        else go(k_real<float, false>, pair_T32_.as<float>(), P);
     } else {
-        if (a.quads) go(k_real<double, true>, pair_T64_.as<double>());
-        else go(k_real<double, false>, pair_T64_.as<double>());
+        const double2* P = ph ? pair_ph64_.as<double2>() : nullptr;
+        if (a.quads) go(k_real<double, true>, pair_T64_.as<double>(), P);
+        else go(k_real<double, false>, pair_T64_.as<double>(), P);
     }
     MPM_LAUNCH();
 }

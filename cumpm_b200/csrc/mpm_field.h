@@ -43,6 +43,9 @@ struct FieldSpec {
     int grid[3] = {0, 0, 0};
     int support = 0;
     int tile[2] = {0, 0};
+    // Bloch wavevector (x, y) of the periodic images (EELS zone sum):
+    // k-space at k - b, a phase on every real-space pair; dipoles only
+    double bloch[2] = {0.0, 0.0};
 };
 
 // Spectral-Ewald parameters (monodisperse_ewald_electric_field.cu:546-616).
@@ -148,6 +151,11 @@ public:
     // (complex128, device).  Polydisperse and direct fields (mpm_adjoint.cu).
     void grad_bilinear(const double2* lam, const double2* p, int M, double2* gx, double2* ga, cudaStream_t s);
 
+    // Bloch wavevector (non-dimensional): rebuilds the k-space tables and
+    // pair phases at the next apply (Ewald fields, dipoles only)
+    void set_bloch(double bx, double by);
+    bool bloch_on() const { return spec_.bloch[0] != 0.0 || spec_.bloch[1] != 0.0; }
+
     int num_particles() const { return N_; }
     int num_targets() const { return spec_.solver_ax ? N_ : targets_.n; }
     int num_quads() const { return Nq_; }
@@ -170,6 +178,8 @@ private:
     void build_slab_taps(cudaStream_t s);
     bool use_slab() const;   // pruned layout through AxisFFT::run_slab
     void build_scale(cudaStream_t s);
+    void build_pair_phases(cudaStream_t s);
+    void poly_build_scale();
     cufftHandle plan_for(int B, bool fp32);  // B columns per voxel
     // the real-space part already written into Y on another stream: the
     // contraction waits for `join`, adds, and scales by 1/s (jacobi_sc)
@@ -213,7 +223,7 @@ private:
     DevBuf tab_r_, tab_f_;          // double[kTableSize], double[T_COUNT][kTableSize]
     // CSR pairs by target
     DevBuf pair_off_, pair_cnt_, pair_src_, pair_T64_, pair_T32_, pair_Q_, cell_key_, cell_idx_, cell_key_s_,
-        cell_idx_s_, cell_start_, cell_end_, cub_tmp_, pair_geo_;
+        cell_idx_s_, cell_start_, cell_end_, cub_tmp_, pair_geo_, pair_ph64_, pair_ph32_;
     long long num_pairs_ = 0;
     // reciprocal space
     DevBuf grid_;                   // complex grid, sized for the largest use

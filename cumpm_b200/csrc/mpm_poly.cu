@@ -318,8 +318,9 @@ __global__ void __launch_bounds__(256) k_poly_spread(const double2* __restrict__
     }
 }
 
+// (bx, by): Bloch wavevector, the scale taken at k - b
 __global__ void k_poly_build_scale(int Nx, int Ny, int Nz, double Lx, double Ly, double Lz, double xi, double eta,
-                                   double* __restrict__ s64, float* __restrict__ s32) {
+                                   double bx, double by, double* __restrict__ s64, float* __restrict__ s32) {
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     const long long V = (long long)Nx * Ny * Nz;
     if (t >= V) return;
@@ -327,7 +328,7 @@ __global__ void k_poly_build_scale(int Nx, int Ny, int Nz, double Lx, double Ly,
     const double fx = ix <= (Nx - 1) / 2 ? ix : ix - Nx;
     const double fy = iy <= (Ny - 1) / 2 ? iy : iy - Ny;
     const double fz = iz <= (Nz - 1) / 2 ? iz : iz - Nz;
-    const double kx = fx * 2.0 * kPi / Lx, ky = fy * 2.0 * kPi / Ly, kz = fz * 2.0 * kPi / Lz;
+    const double kx = fx * 2.0 * kPi / Lx - bx, ky = fy * 2.0 * kPi / Ly - by, kz = fz * 2.0 * kPi / Lz;
     const double k2 = kx * kx + ky * ky + kz * kz;
     double v = 0.0;
     if (!(k2 < 1e-12)) v = (exp(-(1.0 - eta) * k2 / (4.0 * xi * xi)) / k2) * (1.0 / double(V));
@@ -667,20 +668,24 @@ void Field::poly_init() {
     gv_.layer = 0;
     if (gv_.Nx < 16 || gv_.Ny < 16 || gv_.Nz < 16 || pgeom_.P >= std::min(gv_.Nx, std::min(gv_.Ny, gv_.Nz)))
         throw std::runtime_error("polydisperse grid shorter than 16 points or than the support along an axis");
-    const size_t V = size_t(gv_.Nx) * gv_.Ny * gv_.Nz;
-    scale64_.ensure(sizeof(double) * V);
-    scale32_.ensure(sizeof(float) * V);
-    k_poly_build_scale<<<nblk((long long)V, 256), 256>>>(gv_.Nx, gv_.Ny, gv_.Nz, spec_.box[0], spec_.box[1],
-                                                         spec_.box[2], spec_.xi, pgeom_.eta, scale64_.as<double>(),
-                                                         scale32_.as<float>());
-    MPM_LAUNCH();
-    MPM_CUDA(cudaDeviceSynchronize());
+    poly_build_scale();
     own_fft_ = AxisFFT::fits(gv_.Nx, true) && AxisFFT::fits(gv_.Ny, true) && AxisFFT::fits(gv_.Nz, true);
     if (own_fft_) {
         fftx_.init(gv_.Nx);
         ffty_.init(gv_.Ny);
         fftz_.init(gv_.Nz);
     }
+}
+
+void Field::poly_build_scale() {
+    const size_t V = size_t(gv_.Nx) * gv_.Ny * gv_.Nz;
+    scale64_.ensure(sizeof(double) * V);
+    scale32_.ensure(sizeof(float) * V);
+    k_poly_build_scale<<<nblk((long long)V, 256), 256>>>(gv_.Nx, gv_.Ny, gv_.Nz, spec_.box[0], spec_.box[1],
+                                                         spec_.box[2], spec_.xi, pgeom_.eta, spec_.bloch[0],
+                                                         spec_.bloch[1], scale64_.as<double>(), scale32_.as<float>());
+    MPM_LAUNCH();
+    MPM_CUDA(cudaDeviceSynchronize());
 }
 
 void Field::poly_weights(PointSet& ps, const double* radius_dev, cudaStream_t s, bool bins) {

@@ -276,7 +276,7 @@ FieldTuning autotune(const FieldSpec& base_in, const double* x, const double* y,
     if (!best.ok) throw std::runtime_error("autotune: the rule configuration does not fit in device memory");
     rep.error_rule = best.err;
     rep.apply_ms_rule = best.ms;
-    bound = std::max(base.errortol, 1.1 * best.err);
+    bound = std::max(base.errortol, best.err);
     std::vector<Eval> xs{best};
     for (const XiCandidate& c : tune_xi_candidates(base)) {
         if (c.xi == base.xi) continue;

@@ -10,7 +10,7 @@
 // the grid up to sizes the line transforms handle fastest, trim the support
 // and change the spread tile, and keeps a candidate only if its operator
 // error, measured against a field of 1000x tighter tolerance on the same
-// positions, stays within max(errortol, 1.1 x the rule's own error).
+// positions, stays within max(errortol, the rule's own error).
 #pragma once
 
 #include <vector>

@@ -21,9 +21,15 @@ split into sub-dipoles on a cubic, Fibonacci or fcc lattice in the unit
 sphere that keep the particle's volume (``eels.py:177-320``); each beam
 position then solves its own split system.
 
-Not available yet (they raise ``RuntimeError`` naming the gap): the
-Brillouin-zone sum (``asm_flag``, it needs the Bloch wavevector in the
-device operator) and quadrupoles.
+With ``asm_flag`` (an infinite array: the Brillouin-zone sum,
+eels_solver.cu:495-881) the solve runs once per point of an asm_Nx x
+asm_Ny midpoint grid over the zone: the device field takes the point's
+Bloch wavevector (``capi.Field.set_bloch``; a direct field has none, as in
+the reference), the beam field sums the periodic images within 12 decay
+lengths with the Bloch phase, and loss and dipoles are averaged over the
+points (the sum times dk_x dk_y over the zone area).
+
+Not available yet (it raises ``RuntimeError`` naming the gap): quadrupoles.
 """
 import math
 
@@ -51,17 +57,34 @@ def _bessel_k(n, z):
     return out
 
 
-def beam_field(pos, epos, omega, v, gamma, length_scale):
-    """Beam field (N, 3) at scaled positions, for one scaled frequency."""
+def beam_field(pos, epos, omega, v, gamma, length_scale, box=None, k=(0.0, 0.0), asm=False):
+    """Beam field (N, 3) at scaled positions, for one scaled frequency.
+    With ``asm``: the sum over the beam's periodic images (R_x, R_y) within
+    12 decay lengths |v gamma / (2 pi omega)|, each times the Bloch phase
+    exp(i (k_x (x - R_x) + k_y (y - R_y))) (eels_solver.cu:519-578)."""
     pos = np.asarray(pos, dtype=np.float64)
-    dx = pos[:, 0] - epos[0]
-    dy = pos[:, 1] - epos[1]
     sigma = 0.5 / length_scale
-    r = np.sqrt(dx * dx + dy * dy + sigma * sigma)
-    x = (2.0 * _PI * omega * r) / (v * gamma)
     pref = omega / (v * v * gamma) * np.exp(1j * 2.0 * _PI * omega * pos[:, 2] / v)
-    k0, k1 = _bessel_k(0, x), _bessel_k(1, x)
-    return np.stack([-pref * k1 * dx / r, -pref * k1 * dy / r, pref * 1j / gamma * k0], axis=1)
+    nx = ny = 0
+    if asm:
+        r_decay = 12.0 * abs((v * gamma) / (2.0 * _PI * omega))
+        nx = int(math.ceil(r_decay / box[0]))
+        ny = int(math.ceil(r_decay / box[1]))
+    E = np.zeros((len(pos), 3), dtype=np.complex128)
+    for ix in range(-nx, nx + 1):
+        for iy in range(-ny, ny + 1):
+            Rx = ix * box[0] if asm else 0.0
+            Ry = iy * box[1] if asm else 0.0
+            dx = pos[:, 0] - epos[0] - Rx
+            dy = pos[:, 1] - epos[1] - Ry
+            r = np.sqrt(dx * dx + dy * dy + sigma * sigma)
+            x = (2.0 * _PI * omega * r) / (v * gamma)
+            k0, k1 = _bessel_k(0, x), _bessel_k(1, x)
+            e = np.stack([-pref * k1 * dx / r, -pref * k1 * dy / r, pref * 1j / gamma * k0], axis=1)
+            if asm:
+                e = e * np.exp(1j * (k[0] * (pos[:, 0] - Rx) + k[1] * (pos[:, 1] - Ry)))[:, None]
+            E += e
+    return E
 
 
 def unit_offsets(method, n_split):
@@ -162,8 +185,10 @@ class EELS:
         self.split_method = split_method
         if solve_quadrupoles or (quad_idxs is not None and len(quad_idxs)):
             raise RuntimeError("EELS quadrupoles are not available in this build")
-        if asm_flag:
-            raise RuntimeError("the EELS Brillouin-zone sum (asm_flag) is not available in this build")
+        self.asm = bool(asm_flag)
+        self.asm_n = (int(asm_Nx), int(asm_Ny)) if self.asm else (1, 1)
+        if self.asm and min(self.asm_n) < 1:
+            raise ValueError("asm_Nx and asm_Ny must be at least 1")
         from .solver import _parse_precision
 
         prec = _parse_precision(precision)
@@ -221,7 +246,7 @@ class EELS:
             self._F = capi.Field(capi.FIELD_MONO, box_s, self.tol, self.xi)
         self._N = N
 
-    # -- one beam position (eels_solver.cu:386-881, without the zone sum) ---
+    # -- one beam position (eels_solver.cu:386-881) ------------------------
     def _frame(self, epos, pos_s):
         import torch
 
@@ -229,20 +254,37 @@ class EELS:
         om = self.omega * self._ls
         gamma = 1.0 / math.sqrt(1.0 - self.v * self.v)
         e_s = np.asarray(epos, dtype=np.float64) / self._ls
-        B = np.empty((3 * N, W), dtype=np.complex128)
-        for w in range(W):
-            B[:, w] = beam_field(pos_s, e_s, om[w], self.v, gamma, self._ls).ravel()
+        box_s = self.box / self._ls
         S = (-3.0 / (4.0 * _PI * (1.0 - self._eps))).T.copy()          # (N, W)
         dev = torch.device("cuda")
-        Bt = torch.tensor(B, device=dev)
-        X = torch.zeros_like(Bt)
         St = torch.tensor(S, device=dev)
         method = capi.METHOD_BICGSTAB if self.solver_type == "bicgstab" else capi.METHOD_GMRES
-        self._F.batch_solve(Bt, X, St, tol=self.tol, method=method, jacobi=self.use_jacobi_precond,
-                            recip_fp32=not self._fp64, refine=not self._fp64)
-        p = X.cpu().numpy()
-        eels = np.imag(np.sum(p * np.conj(B), axis=0)) / (2.0 * _PI * _PI)
-        dips = p.T.reshape(W, N, 3)
+        nx, ny = self.asm_n
+        dkx = 2.0 * _PI / (box_s[0] * nx) if self.asm else 0.0
+        dky = 2.0 * _PI / (box_s[1] * ny) if self.asm else 0.0
+        eels = np.zeros(W)
+        dips = np.zeros((W, N, 3), dtype=np.complex128)
+        for ix in range(nx):
+            for iy in range(ny):
+                k = ((-_PI / box_s[0] + (ix + 0.5) * dkx, -_PI / box_s[1] + (iy + 0.5) * dky) if self.asm
+                     else (0.0, 0.0))
+                if self.asm and self._F.kind != capi.FIELD_DIRECT:
+                    self._F.set_bloch(*k)
+                B = np.empty((3 * N, W), dtype=np.complex128)
+                for w in range(W):
+                    B[:, w] = beam_field(pos_s, e_s, om[w], self.v, gamma, self._ls, box_s, k, self.asm).ravel()
+                Bt = torch.tensor(B, device=dev)
+                X = torch.zeros_like(Bt)
+                self._F.batch_solve(Bt, X, St, tol=self.tol, method=method, jacobi=self.use_jacobi_precond,
+                                    recip_fp32=not self._fp64, refine=not self._fp64)
+                p = X.cpu().numpy()
+                eels += np.imag(np.sum(p * np.conj(B), axis=0)) / (2.0 * _PI * _PI)
+                dips += p.T.reshape(W, N, 3)
+        if self.asm:
+            # the average over the zone points (eels_solver.cu:847-862)
+            frac = (dkx * dky) / ((2.0 * _PI / box_s[0]) * (2.0 * _PI / box_s[1]))
+            eels *= frac
+            dips *= frac
         return eels, dips
 
     def compute(self, epos, positions):
@@ -296,7 +338,7 @@ class EELS:
             sp, sr, se = split_near_beam(positions, e, rad, eps, self.split_dist, offsets)
             sub = EELS(self.box, se, self.omega, self.v, eps_m=self.eps_m, radius=sr, xi=self.xi, tol=self.tol,
                        quiet=True, solver_type=self.solver_type, field_type=self.field_type,
-                       precision=self._precision)
+                       asm_flag=self.asm, asm_Nx=self.asm_n[0], asm_Ny=self.asm_n[1], precision=self._precision)
             sub.use_jacobi_precond = self.use_jacobi_precond
             sub.compute(e, sp)
             self._eels.append(sub._eels[0])

@@ -184,7 +184,7 @@ class dipole_solver:
         batch width and arithmetic: the splitting parameter xi, the grid, the
         Gaussian support and the spread tile are measured on the device and
         the fastest setting whose operator error stays within
-        max(tol, 1.1 x the error of the reference's rule setting) is kept for
+        max(tol, the error of the reference's rule setting) is kept for
         every later frame.  Returns the pick (xi non-dimensional, zeros =
         the rule) with its timings and errors."""
         pos = np.ascontiguousarray(_to_numpy(positions), dtype=np.float64)

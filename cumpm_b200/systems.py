@@ -1,4 +1,5 @@
-"""Many independent periodic systems across the ranks of one job.
+"""Many independent periodic systems across the ranks of one job, and one
+system's frequencies across the ranks (``solve_sharded``).
 
 Systems (different sizes, boxes, materials, with or without quadrupoles)
 share nothing but the code: each is a ``dipole_solver`` of its own.  Across
@@ -39,6 +40,7 @@ class System:
     E0: object = None
     precision: Optional[str] = None
     extra: Dict[str, object] = field(default_factory=dict)
+    options: Dict[str, object] = field(default_factory=dict)   # set_solver_options keywords
 
     @property
     def num_particles(self) -> int:
@@ -67,19 +69,68 @@ def partition(sizes: Sequence[int], world_size: int) -> List[List[int]]:
     return [sorted(s) for s in out]
 
 
-def solve_one(system: System) -> Dict[str, np.ndarray]:
-    """Solve one system with ``dipole_solver``; its physical results."""
+def _solver_for(system: System):
     from .solver import dipole_solver
 
     s = dipole_solver(system.box, system.eps_p, radius=system.radius, eps_m=system.eps_m, xi=system.xi,
                       tol=system.tol, quiet=True, solver_type=system.solver_type, field_type=system.field_type,
                       E0=system.E0, quadrupoles=system.quadrupoles, precision=system.precision, **system.extra)
+    if system.options:
+        s.set_solver_options(**system.options)
     s.compute(np.asarray(system.positions, dtype=np.float64))
+    return s
+
+
+def _has_quads(system: System) -> bool:
+    return system.quadrupoles is not False and system.quadrupoles is not None
+
+
+def solve_one(system: System) -> Dict[str, np.ndarray]:
+    """Solve one system with ``dipole_solver``; its physical results."""
+    s = _solver_for(system)
     out = {"eff_polarizability": np.asarray(s.get_eff_polarizability()),
            "dipoles": np.asarray(s.get_dipoles())}
-    if system.quadrupoles is not False and system.quadrupoles is not None:
+    if _has_quads(system):
         out["quadrupoles"] = np.asarray(s.get_quadrupoles())
     return out
+
+
+def solve_one_unsqueezed(system: System) -> Dict[str, np.ndarray]:
+    """``solve_one`` with every axis kept: eff_polarizability (W, K, 3),
+    dipoles (frames, W, N, K, 3), quadrupoles (frames, W, Nq, K, 5)."""
+    s = _solver_for(system)
+    raw = s._solver
+    out = {"eff_polarizability": np.asarray(raw.get_eff_polarizability(True)),
+           "dipoles": np.asarray(raw.get_dipoles(True))}
+    if _has_quads(system):
+        out["quadrupoles"] = np.asarray(raw.get_quadrupoles(True))
+    return out
+
+
+# the frequency axis of each unsqueezed result
+_FREQ_AXIS = {"eff_polarizability": 0, "dipoles": 1, "quadrupoles": 1}
+
+
+def frequency_shards(num_freqs: int, world_size: int) -> List[List[int]]:
+    """Contiguous, balanced blocks of frequency indices, one per rank (the
+    first num_freqs % world_size ranks take one more; ranks beyond
+    num_freqs take none)."""
+    if world_size < 1:
+        raise ValueError("world_size must be at least 1")
+    return [list(map(int, b)) for b in np.array_split(np.arange(int(num_freqs)), world_size)]
+
+
+def _eps_rows(eps_p) -> np.ndarray:
+    """eps_p as (W, 1) or (W, N): a scalar is one frequency, a 1-D array one
+    value per frequency, a 2-D array one row per frequency."""
+    e = np.asarray(eps_p, dtype=np.complex128)
+    if e.ndim == 0:
+        return e.reshape(1, 1)
+    if e.ndim == 1:
+        return e.reshape(-1, 1)
+    if e.ndim == 2:
+        return e
+    raise ValueError("eps_p must be a scalar, 1D array, or 2D array")
 
 
 def local_device_ordinal(rank: int, env=None, device_count: Optional[int] = None) -> int:
@@ -154,3 +205,50 @@ def solve_systems(systems: Sequence[System], *, dist=None,
     if missing:
         raise RuntimeError(f"systems {missing} were not solved")
     return out  # type: ignore[return-value]
+
+
+def solve_sharded(system: System, *, dist=None,
+                  solve_fn: Callable[[System], Dict[str, np.ndarray]] = solve_one_unsqueezed,
+                  bind_device: Optional[Callable[[int], None]] = _bind_device) -> Dict[str, np.ndarray]:
+    """One system, its frequencies split across the ranks of ``dist``
+    (strong scaling of one solve): every rank solves the same positions for
+    its contiguous block of frequencies (:func:`frequency_shards`) with its
+    own ``dipole_solver``, and one ``all_gather_object`` returns the results,
+    concatenated along the frequency axis in frequency order and squeezed
+    as ``dipole_solver``'s getters squeeze, on every rank.  The frequencies
+    are independent solves (the warm start of each block begins from the
+    mean-field guess).  A rank whose share is empty, or whose solve raises,
+    still joins the gather; a failure raises :class:`SystemSolveError` on
+    every rank."""
+    rows = _eps_rows(system.eps_p)
+    W = rows.shape[0]
+
+    def part(idx):
+        if not idx:
+            return None
+        sub = System(**{**system.__dict__, "eps_p": rows[idx] if rows.shape[1] > 1 else rows[idx, 0]})
+        return solve_fn(sub)
+
+    if dist is None or not dist.is_initialized():
+        parts = [part(list(range(W)))]
+    else:
+        rank, world = dist.get_rank(), dist.get_world_size()
+        if bind_device is not None:
+            bind_device(local_device_ordinal(rank))
+        mine = frequency_shards(W, world)[rank]
+        try:
+            local = (True, part(mine))
+        except Exception as e:  # reported on every rank after the gather
+            local = (False, f"rank {rank}: {type(e).__name__}: {e}")
+        gathered: List[object] = [None] * world
+        dist.all_gather_object(gathered, local)
+        errors = [res for ok, res in gathered if not ok]
+        if errors:
+            raise SystemSolveError("; ".join(errors))
+        parts = [res for ok, res in gathered]
+    parts = [p for p in parts if p is not None]
+    out = {}
+    for key, axis in _FREQ_AXIS.items():
+        if key in parts[0]:
+            out[key] = np.squeeze(np.concatenate([p[key] for p in parts], axis=axis))
+    return out

@@ -165,6 +165,15 @@ MPM_API int mpm_field_apply(mpm_field* f, const void* X, void* Y, int M, const v
 MPM_API int mpm_field_apply_part(mpm_field* f, const void* X, void* Y, int M, const void* self_coef, int recip_fp32,
                          int real_fp32, int part, void* stream);
 MPM_API int mpm_field_info_get(const mpm_field* f, mpm_field_info* info);
+/* Bloch wavevector (kx, ky), non-dimensional, of the periodic images for
+ * the EELS Brillouin-zone sum (the reference's Ewald base sets it,
+ * ewald_electric_field_base.h:132-138): the k-space Green tensor at k - b
+ * with the window deconvolution at k (monodisperse_ewald_electric_field.cu:
+ * 1329-1331; the polydisperse scale likewise), and a phase
+ * exp(-i (kx r_x + ky r_y)) on every real-space pair, r = source - target
+ * (:1749-1756).  Ewald fields with dipoles only; (0, 0) restores the plain
+ * operator.  Takes effect at the next apply. */
+MPM_API int mpm_field_set_bloch(mpm_field* f, double kx, double ky);
 
 /* Same result as mpm_field_apply, but this call allocates nothing.  No
  * counterpart in the reference.  For callers that cannot allocate device
@@ -199,7 +208,7 @@ typedef struct mpm_tune_report {
     double apply_ms_rule;  /* the same for the rule configuration */
     double error;          /* relative operator error of the pick against a field of tolerance errortol/1000 */
     double error_rule;     /* the same for the rule configuration */
-    double error_bound;    /* acceptance bound: max(errortol, 1.1 * error_rule) */
+    double error_bound;    /* acceptance bound: max(errortol, error_rule) */
     int candidates, accepted;
 } mpm_tune_report;
 
@@ -210,8 +219,7 @@ MPM_API int mpm_field_create_tuned(mpm_field** out, int kind, int mode, const do
 /* Measures candidate (xi, grid, support, tile) settings of a SOLVER_AX
  * field on the device for the n positions (non-dimensional host arrays) and
  * a batch of M columns in the given arithmetic, and writes the fastest one
- * whose operator error stays within max(errortol, 1.1 x the rule's own
- * error).  Direct fields: the rule (nothing to tune). */
+ * whose operator error stays within max(errortol, the rule's own error).  Direct fields: the rule (nothing to tune). */
 MPM_API int mpm_field_autotune(int kind, const double box[3], double errortol, double xi, const double* radius,
                                int n_radius, int solve_quads, const int* quad_idxs, int n_quad_idxs, const double* x,
                                const double* y, const double* z, int n, int M, int recip_fp32, int real_fp32,

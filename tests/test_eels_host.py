@@ -38,9 +38,27 @@ def test_constructor_checks():
         eels.EELS([50.0] * 3, [4.0], [0.1], 0.3, field_type="fast")
     with pytest.raises(ValueError, match="box must have length 3"):
         eels.EELS([50.0] * 2, [4.0], [0.1], 0.3)
-    for kw in (dict(solve_quadrupoles=True), dict(asm_flag=True)):
-        with pytest.raises(RuntimeError, match="not available in this build"):
-            eels.EELS([50.0] * 3, [4.0], [0.1], 0.3, **kw)
+    with pytest.raises(RuntimeError, match="not available in this build"):
+        eels.EELS([50.0] * 3, [4.0], [0.1], 0.3, solve_quadrupoles=True)
+    with pytest.raises(ValueError, match="asm_Nx and asm_Ny"):
+        eels.EELS([50.0] * 3, [4.0], [0.1], 0.3, asm_flag=True, asm_Nx=0)
+    s = eels.EELS([50.0] * 3, [4.0], [0.1], 0.3, asm_flag=True, asm_Nx=3, asm_Ny=2)
+    assert s.asm_n == (3, 2)
+
+
+def test_beam_field_images_match_the_oracle():
+    """The zone sum's beam field (periodic images with the Bloch phase)
+    agrees with the oracle's restatement term by term."""
+    from cumpm_b200 import eels
+    from oracle import mpm_eels as E
+
+    rng = np.random.default_rng(2)
+    pos = rng.uniform(0, 20, (7, 3))
+    box = np.array([20.0, 18.0, 30.0])
+    for k, asm in (((0.0, 0.0), False), ((0.07, -0.11), True)):
+        a = eels.beam_field(pos, [3.0, 4.0], 0.05, 0.4, 1.0 / np.sqrt(1 - 0.16), 2.0, box, k, asm)
+        b = E.beam_field(pos, [3.0, 4.0], 0.05, 0.4, 1.0 / np.sqrt(1 - 0.16), 2.0, box, k, asm)
+        np.testing.assert_allclose(a, b, rtol=1e-12, atol=1e-15 * np.abs(b).max())
 
 
 def test_positions_and_beams_are_checked():

@@ -52,3 +52,29 @@ def test_systems_match_their_own_solvers():
         for k in ref:
             np.testing.assert_allclose(r[k], ref[k], rtol=1e-12, atol=1e-14 * np.abs(ref[k]).max())
     assert "quadrupoles" in res[0] and res[1]["quadrupoles"].shape[-1] == 5 and "quadrupoles" not in res[2]
+
+
+def test_frequency_blocks_concatenate_to_the_whole_sweep():
+    """solve_sharded's pieces: the sweep solved as two frequency blocks
+    (what two ranks would each solve) and concatenated equals the whole
+    sweep solved at once, to the solves' tolerance; one process is the whole
+    sweep itself."""
+    from cumpm_b200 import systems as S
+
+    syst = _systems()[0]
+    omega = np.linspace(0.3, 0.9, 5)
+    syst.eps_p = 4.0 - 1.8 ** 2 / (omega ** 2 + 1j * omega * 0.1)
+    syst.options = {"batch_all": True, "refine": True}
+    syst.precision = None
+    whole = S.solve_one_unsqueezed(syst)
+    blocks = []
+    for idx in S.frequency_shards(5, 2):
+        sub = S.System(**{**syst.__dict__, "eps_p": np.asarray(syst.eps_p)[idx]})
+        blocks.append(S.solve_one_unsqueezed(sub))
+    for key, axis in (("dipoles", 1), ("eff_polarizability", 0), ("quadrupoles", 1)):
+        cat = np.concatenate([b[key] for b in blocks], axis=axis)
+        assert cat.shape == whole[key].shape
+        err = np.linalg.norm(cat - whole[key]) / np.linalg.norm(whole[key])
+        assert err < 1e-5, (key, err)
+    one = S.solve_sharded(syst)
+    assert one["dipoles"].shape == np.squeeze(whole["dipoles"]).shape

@@ -73,7 +73,7 @@ def test_autotune_pick_meets_its_bound(case):
     pick = capi.autotune(capi.FIELD_MONO, box, 1e-6, 0.5, pos, M)
     assert pick["candidates"] >= 5 and pick["accepted"] >= 1
     assert pick["error"] <= pick["error_bound"]
-    assert pick["error_bound"] == pytest.approx(max(1e-6, 1.1 * pick["error_rule"]))
+    assert pick["error_bound"] == pytest.approx(max(1e-6, pick["error_rule"]))
     assert pick["apply_ms"] <= pick["apply_ms_rule"] * 1.0000001
     op = O.MonoEwaldOperator(box, 1e-6, 0.5, True)
     op.set_positions(pos)

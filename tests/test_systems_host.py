@@ -209,3 +209,89 @@ def test_solve_one_calls_dipole_solver_with_its_own_arguments(monkeypatch):
     assert seen[-1]["quadrupoles"] == [0, 2] and seen[-1]["guess_type"] == "previous" and seen[-1]["quiet"] is True
     res = S.solve_one(S.System(box=[20.0] * 3, positions=np.zeros((4, 3)), eps_p=[3.0]))
     assert set(res) == {"eff_polarizability", "dipoles"}
+
+
+# ---- one system's frequencies across ranks (solve_sharded) -----------------
+
+@pytest.mark.parametrize("W,world", [(10, 1), (10, 3), (10, 4), (2, 3), (64, 8)])
+def test_frequency_shards_are_contiguous_and_balanced(W, world):
+    sh = S.frequency_shards(W, world)
+    assert len(sh) == world
+    assert [i for b in sh for i in b] == list(range(W))
+    sizes = [len(b) for b in sh]
+    assert max(sizes) - min(sizes) <= 1
+    assert sizes == sorted(sizes, reverse=True)
+
+
+def _fake_unsqueezed(system):
+    """Results whose values name their frequency: eff (W, K, 3) and dipoles
+    (1, W, N, K, 3) filled with eps_p of each frequency."""
+    e = np.atleast_1d(np.asarray(system.eps_p, dtype=np.complex128))
+    W, N = len(e), system.num_particles
+    return {"eff_polarizability": np.broadcast_to(e[:, None, None], (W, 3, 3)).copy(),
+            "dipoles": np.broadcast_to(e[None, :, None, None, None], (1, W, N, 3, 3)).copy()}
+
+
+def _sharded_system():
+    rng = np.random.default_rng(4)
+    return S.System(box=[10.0, 10.0, 10.0], positions=rng.uniform(0, 10, (6, 3)),
+                    eps_p=np.arange(10) + 2.0 + 0.5j)
+
+
+def test_sharded_single_process_is_the_whole_sweep():
+    out = S.solve_sharded(_sharded_system(), solve_fn=_fake_unsqueezed)
+    e = np.arange(10) + 2.0 + 0.5j
+    np.testing.assert_array_equal(out["eff_polarizability"][:, 0, 0], e)
+    assert out["dipoles"].shape == (10, 6, 3, 3)
+
+
+def _rank_sharded(rank, world, port, q, fail):
+    sys.path.insert(0, ROOT)
+    from cumpm_b200 import systems as S2
+
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), LOCAL_RANK=str(rank))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        seen, bound = [], []
+
+        def solve(system):
+            seen.append(np.atleast_1d(system.eps_p).real.tolist())
+            if fail and rank == 1:
+                raise RuntimeError("injected")
+            return _fake_unsqueezed(system)
+
+        try:
+            out = S2.solve_sharded(_sharded_system(), dist=dist, solve_fn=solve, bind_device=bound.append)
+            q.put((rank, out["eff_polarizability"][:, 0, 0].tolist(), out["dipoles"].shape, seen, bound))
+        except S2.SystemSolveError as e:
+            q.put((rank, str(e), None, seen, bound))
+        dist.barrier()
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("world,fail", [(3, False), (2, True)])
+def test_gloo_ranks_shard_the_frequencies(world, fail):
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = 30150 + world * 20 + int(fail) * 7 + (os.getpid() % 40)
+    procs = [ctx.Process(target=_rank_sharded, args=(r, world, port, q, fail)) for r in range(world)]
+    for p in procs:
+        p.start()
+    out = {}
+    for _ in range(world):
+        r, *rest = q.get(timeout=120)
+        out[r] = rest
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    shards = S.frequency_shards(10, world)
+    e = (np.arange(10) + 2.0 + 0.5j).tolist()
+    for r in range(world):
+        res, shape, seen, bound = out[r]
+        assert bound == [r]
+        assert seen == [[2.0 + i for i in shards[r]]]   # each rank solved its own block only
+        if fail:
+            assert res == "rank 1: RuntimeError: injected"
+        else:
+            assert res == e and shape == (10, 6, 3, 3)
