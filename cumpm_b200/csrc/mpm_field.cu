@@ -1913,7 +1913,13 @@ void Field::set_bloch(double bx, double by) {
     slab_Z_ = -1;
     layer_colK_ = layer_taps_ = false;
     if (spec_.kind == FIELD_POLY) poly_build_scale();
+    // the tables and pair phases are per-frame state: rebuilt now (applies
+    // use what the last set_positions / set_bloch built)
     precalc_dirty_ = true;
+    if (N_ > 0) {
+        precalc(nullptr);
+        MPM_CUDA(cudaStreamSynchronize(nullptr));
+    }
 }
 
 void Field::build_scale(cudaStream_t s) {
@@ -2158,6 +2164,8 @@ void Field::recip_on(const double2* X, double2* Y, int M, cplx<R>* grid, cudaStr
         fftx_.run<R>(grid, size_t(gv_.Ny) * Bi, int(Bi), Bi, gv_.Ny, false, s);
         Profiler::get().end(ST_FFT_FWD, s);
         Profiler::get().begin(ST_KSPACE, s);
+        if (!(gv_.layer ? layer_taps_ : slab_Z_ == gv_.Zs) || !taps)
+            throw std::runtime_error("slab taps not built for the current layout");
         ffty_.run_slab<R>(grid, gv_.Nx, gv_.Zs, M, taps, 2.0 * kPi / spec_.box[0], 2.0 * kPi / spec_.box[1], s);
         Profiler::get().end(ST_KSPACE, s);
         Profiler::get().begin(ST_FFT_INV, s);
@@ -2177,6 +2185,8 @@ void Field::recip_on(const double2* X, double2* Y, int M, cplx<R>* grid, cudaStr
             const int thr = std::min(1024, ((B + 31) / 32) * 32);
             const cplx<R>* K = sizeof(R) == 4 ? reinterpret_cast<const cplx<R>*>(colK32_.p)
                                               : reinterpret_cast<const cplx<R>*>(colK64_.p);
+            if (!(gv_.layer ? layer_colK_ : colK_Z_ == gv_.Zs) || !K)
+                throw std::runtime_error("column kernel not built for the current layout");
             auto go = [&](auto kern) {
                 MPM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(shm2)));
                 kern<<<gv_.Nx * gv_.Ny, thr, shm2, s>>>(grid, K, Z, M);
@@ -2188,6 +2198,7 @@ void Field::recip_on(const double2* X, double2* Y, int M, cplx<R>* grid, cudaStr
         } else {
             const size_t V = size_t(gv_.Nx) * gv_.Ny * gv_.Zs;
             const R* sc = sizeof(R) == 4 ? reinterpret_cast<const R*>(scale32_.p) : reinterpret_cast<const R*>(scale64_.p);
+            if (scale_built_ != (Nq_ ? 4 : 1) || !sc) throw std::runtime_error("k-space scale not built");
             if (Nq_)
                 k_scale<R, true><<<nblk((long long)(V * M), 256), 256, 0, s>>>(grid, sc, gv_.Nx, gv_.Ny, gv_.Nz, spec_.box[0],
                                                                                spec_.box[1], spec_.box[2], M, spec_.bloch[0], spec_.bloch[1]);
@@ -2261,6 +2272,8 @@ void Field::real_part(const double2* X, double2* Y, int M, const double2* sc, bo
     const int blocks = nblk((long long)warps * 32, thr);
     StageScope scope(ST_REAL, s);
     const bool ph = bloch_on();
+    if (ph && num_pairs_ > 0 && pair_ph64_.bytes < sizeof(double2) * size_t(num_pairs_))
+        throw std::runtime_error("Bloch pair phases not built for the current pairs");
     auto go = [&](auto kern, const auto* T, const auto* P) {
         kern<<<blocks, thr, 0, s>>>(X, Y, a, pair_off_.as<int>(), pair_src_.as<int>(), T, pair_Q_.as<double>(),
                                     quad_map_.as<int>(), sc, selfv, P);

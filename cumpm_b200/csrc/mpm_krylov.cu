@@ -687,6 +687,18 @@ __global__ void k_mask_conv(double2* __restrict__ r, const int* __restrict__ con
     if (conv[t % M]) r[t] = make_double2(0, 0);
 }
 
+// columns with sel[m] set take the fp64 residual (r, its norm) in place of
+// the fp32 screen's
+__global__ void k_take_cols(double2* __restrict__ r, const double2* __restrict__ r64, double* __restrict__ rn,
+                            const double* __restrict__ rn64, const int* __restrict__ sel, size_t n, int M) {
+    const size_t t = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    const int m = int(t % M);
+    if (!sel[m]) return;
+    r[t] = r64[t];
+    if (t < size_t(M)) rn[t] = rn64[t];
+}
+
 __global__ void k_axpy1(double2* __restrict__ x, const double2* __restrict__ d, size_t n) {
     const size_t t = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
     if (t < n) x[t] += d[t];
@@ -1280,20 +1292,52 @@ void BatchSolver::solve(Field& F, const double2* b, double2* x, int M, const dou
     const bool shifted = opt.shifted && opt.method == SOLVER_GMRES &&
                          detect_shifts(b, sc, rows, F.num_particles(), M, s, grp, fsh);
     bool reset = false;   // x replaced by the shifted solve from zero: every column active again
+    std::vector<double> hb(M), hr(M);
     for (int step = 0; step < opt.max_refine; ++step) {
-        // fp64 true residual of the columns not yet converged (a converged
-        // column's x no longer changes)
-        st.column_matvecs += apply_cols(F, x, xr_.as<double2>(), M, sc, false, false, false,
+        // true residual of the columns not yet converged (a converged
+        // column's x no longer changes).  The initial guess is screened with
+        // the fp32 operator first: a column whose fp32 residual is above
+        // 4 tol is not converged whatever the fp32 operator's error (about
+        // 1e-7 relative), so only the columns below that take the fp64
+        // residual; every later check is fp64 for all unconverged columns.
+        const bool screen = step == 0 && !reset && opt.tol < 0.25;
+        st.column_matvecs += apply_cols(F, x, xr_.as<double2>(), M, sc, false, screen, screen,
                                         step == 0 || reset ? nullptr : act.data(), opt.compact, s);
         reset = false;
         st.matvecs++;
-        st.fp64_matvecs++;
+        if (!screen) st.fp64_matvecs++;
         k_sub<<<vb, 256, 0, s>>>(b, xr_.as<double2>(), xr_.as<double2>(), n);
         MPM_LAUNCH();
         norms(xr_.as<double2>(), rows, M, rn2, s);
+        if (screen) {
+            MPM_CUDA(cudaMemcpyAsync(hb.data(), bn2, sizeof(double) * M, cudaMemcpyDeviceToHost, s));
+            MPM_CUDA(cudaMemcpyAsync(hr.data(), rn2, sizeof(double) * M, cudaMemcpyDeviceToHost, s));
+            MPM_CUDA(cudaStreamSynchronize(s));
+            std::vector<int> near(M, 0);
+            int nnear = 0;
+            for (int m = 0; m < M; ++m) {
+                near[m] = hr[m] <= 4.0 * opt.tol * hb[m];
+                nnear += near[m];
+            }
+            if (nnear) {
+                // fp64 residual of those columns into d_, swapped in
+                st.column_matvecs += apply_cols(F, x, d_.as<double2>(), M, sc, false, false, false, near.data(),
+                                                opt.compact, s);
+                st.matvecs++;
+                st.fp64_matvecs++;
+                k_sub<<<vb, 256, 0, s>>>(b, d_.as<double2>(), d_.as<double2>(), n);
+                MPM_LAUNCH();
+                sel_.ensure(sizeof(int) * M);
+                rn64_.ensure(sizeof(double) * M);
+                norms(d_.as<double2>(), rows, M, rn64_.as<double>(), s);
+                MPM_CUDA(cudaMemcpyAsync(sel_.p, near.data(), sizeof(int) * M, cudaMemcpyHostToDevice, s));
+                k_take_cols<<<vb, 256, 0, s>>>(xr_.as<double2>(), d_.as<double2>(), rn2, rn64_.as<double>(),
+                                               sel_.as<int>(), n, M);
+                MPM_LAUNCH();
+            }
+        }
         k_conv_update<<<nblk(M, 128), 128, 0, s>>>(rn2, bn2, opt.tol, convd, M);
         MPM_LAUNCH();
-        std::vector<double> hb(M), hr(M);
         MPM_CUDA(cudaMemcpyAsync(hb.data(), bn2, sizeof(double) * M, cudaMemcpyDeviceToHost, s));
         MPM_CUDA(cudaMemcpyAsync(hr.data(), rn2, sizeof(double) * M, cudaMemcpyDeviceToHost, s));
         MPM_CUDA(cudaStreamSynchronize(s));
@@ -1324,8 +1368,13 @@ void BatchSolver::solve(Field& F, const double2* b, double2* x, int M, const dou
             // seed (the seeds' Krylov spaces cost a small part of per-column
             // solves even from x = 0): those columns start again from x = 0
             // and their first correction is solved on the seeds' Krylov
-            // spaces; converged columns (a warm start) keep their x
-            k_inner_tol<<<nblk(M, 128), 128, 0, s>>>(bn2, bn2, opt.tol, floor, tolv_.as<double>(), M);
+            // spaces; converged columns (a warm start) keep their x.  The
+            // target is the outer one (half of it, no inner floor): the
+            // seeds' GMRES works in fp64 on the fp32 operator, so its
+            // residual estimate keeps falling below the fp32 operator error,
+            // and a first correction this tight usually leaves nothing for
+            // the per-column corrections but the fp64 check
+            k_inner_tol<<<nblk(M, 128), 128, 0, s>>>(bn2, bn2, opt.tol, 0.0, tolv_.as<double>(), M);
             MPM_LAUNCH();
             SolveStats inner;
             inner.iters.assign(M, 0);

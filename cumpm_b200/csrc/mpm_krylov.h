@@ -117,6 +117,7 @@ private:
     DevBuf r0_, p_, v_, s_, t_, scal_, d_, rr_, xr_, flagdev_, tolv_;
     DevBuf cidx_, xc_, yc_, scc_;        // compact-batch gather buffers
     DevBuf bn2_, rn2_, convd_;           // refinement: |b|, true |r|, converged flags
+    DevBuf sel_, rn64_;                  // refinement: columns re-checked in fp64, their |r|
     DevBuf shf_, shflag_, shmeta_, shsc_, shb_, shst_, hm_;   // shifted solve: detection, seeds, members
     int* flag_ = nullptr;                // pinned host words: count + per-column flags
     int flag_cap_ = 0;

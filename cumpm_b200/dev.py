@@ -12,7 +12,8 @@ SOLVER_AX mode the interaction field plus the self terms set by
 The reference's accessors of its internal device buffers (`dev_*`,
 `get_*_precalcs_host`, neighbour-list and table getters) have no
 counterpart: this build's data layout is different.  Bloch wavevectors
-(EELS) and polydisperse quadrupoles raise RuntimeError naming the gap.
+(`set_bloch_wavevector`, ewald_electric_field_base.h:132-138) are taken for
+dipoles; with quadrupoles they raise RuntimeError naming the gap.
 """
 from __future__ import annotations
 
@@ -75,6 +76,7 @@ class _Field:
         self._F = None
         self._built_for = None
         self._E = None
+        self._bloch = (0.0, 0.0)
 
     # ---------------------------------------------------------- inputs --
     def update_particle_coordinates(self, x_part, y_part, z_part):
@@ -108,7 +110,14 @@ class _Field:
         self._self = r + 1j * i
 
     def set_bloch_wavevector(self, kx, ky):
-        raise RuntimeError("Bloch wavevectors (EELS) are not available in this build")
+        """Bloch wavevector (k_x, k_y) of the periodic images: the k-space
+        Green tensor at k - b and a phase on every real-space pair
+        (dipoles only in this build)."""
+        if self._kind == capi.FIELD_DIRECT:
+            raise RuntimeError("a direct field has no Bloch wavevector")
+        if self._solve_quads and (kx != 0.0 or ky != 0.0):
+            raise RuntimeError("Bloch wavevectors with quadrupoles are not available in this build")
+        self._bloch = (float(kx), float(ky))
 
     # ------------------------------------------------------------ sizes --
     @property
@@ -164,6 +173,7 @@ class _Field:
                 raise RuntimeError("update_field_coordinates before calculate in INTERACTION_FIELD mode")
             self._F.set_field_points(self._fpts)
         self._F.set_positions(self._pos)
+        self._F.set_bloch(*self._bloch)
         return self._F
 
     def _inputs(self):

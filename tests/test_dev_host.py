@@ -35,9 +35,12 @@ def test_inputs_and_sizes():
 def test_named_gaps():
     from cumpm_b200 import dev
 
-    ef = dev.PolydisperseEwaldElectricField(20.0, 20.0, 20.0, 1e-6, 0.5, True, [1.0, 1.2])
+    ef = dev.PolydisperseEwaldElectricField(20.0, 20.0, 20.0, 1e-6, 0.5, True, [1.0, 1.2], solve_quadrupoles=True)
     with pytest.raises(RuntimeError, match="Bloch"):
         ef.set_bloch_wavevector(0.1, 0.0)
+    ef = dev.PolydisperseEwaldElectricField(20.0, 20.0, 20.0, 1e-6, 0.5, True, [1.0, 1.2])
+    ef.set_bloch_wavevector(0.1, 0.0)   # dipoles: taken (applied at the next calculate)
+    assert ef._bloch == (0.1, 0.0)
     with pytest.raises(ValueError, match="radius"):
         dev.MonodisperseEwaldElectricField(20.0, 20.0, 20.0, 1e-6, 0.5, True, radius=2.0)
 
