@@ -679,6 +679,8 @@ def run_extras(args, capi, torch, dev, flush):
         torch.cuda.empty_cache()
     out["c4_adjoint"] = run_c4(args, torch)
     out["autotuned"] = {name: run_autotuned(args, capi, torch, dev, flush, name) for name in ("monolayer", "poly3d")}
+    if not args.no_c5:
+        out["c5_systems"] = run_c5(args, torch)
     return out
 
 
@@ -720,6 +722,75 @@ def run_autotuned(args, capi, torch, dev, flush, name):
     }
     del T, rule
     torch.cuda.empty_cache()
+    return out
+
+
+C5_FREQS = np.linspace(0.2, 1.0, 8)
+
+
+def c5_systems(seed=5, total=250_000, lo=1000, hi=64000):
+    """The uneven multi-system workload: 16 periodic systems, N log-uniform
+    in [1k, 64k] (seeded) scaled to about 250k particles in all; even
+    systems hexagonal monolayers (a = 5 nm, spacing 12 nm, 80 nm box height),
+    odd ones random packings at phi in [0.05, 0.2] (a jittered simple-cubic
+    lattice: spacing (4 pi a^3 / 3 phi)^(1/3), each particle displaced
+    uniformly by less than half the gap, so none overlap); Drude spheres in
+    eps_m 1.77, 8 frequencies 0.2-1.0 eV x 3 polarisations, dipoles and
+    quadrupoles, tol 1e-6.  Returns cumpm_b200.systems.System objects (nm)."""
+    from cumpm_b200.systems import System
+
+    rng = np.random.default_rng(seed)
+    n = np.exp(rng.uniform(math.log(lo), math.log(hi), 16))
+    n = np.clip(np.round(n * total / n.sum()), lo, hi).astype(int)
+    eps = 4.0 - 1.8 ** 2 / (C5_FREQS ** 2 + 1j * C5_FREQS * 0.1)
+    out = []
+    for i, N in enumerate(n):
+        if i % 2 == 0:
+            cols = max(2, int(round(math.sqrt(N / (math.sqrt(3) / 2)))))
+            rows = max(2, int(math.ceil(N / cols)))
+            rows += rows % 2
+            pos = np.array([[(c + 0.5 * (r % 2)) * 12.0, r * math.sqrt(3) / 2 * 12.0, 0.0]
+                            for r in range(rows) for c in range(cols)])[:N]
+            box = [cols * 12.0, rows * math.sqrt(3) / 2 * 12.0, 80.0]
+        else:
+            phi = rng.uniform(0.05, 0.2)
+            sp = (4.0 * math.pi * RADIUS ** 3 / (3.0 * phi)) ** (1.0 / 3.0)
+            m = int(math.ceil(N ** (1.0 / 3.0)))
+            g = np.stack(np.meshgrid(*(np.arange(m),) * 3, indexing="ij"), axis=-1).reshape(-1, 3)
+            g = g[rng.permutation(len(g))[:N]]
+            jit = (sp - 2.0 * RADIUS) / 2.0 * 0.98
+            pos = (g + 0.5) * sp + rng.uniform(-jit, jit, (N, 3))
+            box = [m * sp] * 3
+        out.append(System(box=box, positions=pos, eps_p=eps, radius=RADIUS, eps_m=EPS_M, tol=TOL, xi=XI,
+                          quadrupoles=True, field_type="monodisperse",
+                          options={"batch_all": True, "refine": True}))
+    return out
+
+
+def run_c5(args, torch):
+    """The 16 uneven systems solved on this GPU through
+    cumpm_b200.systems.solve_systems: one after another, and two at a time
+    from host threads (each system its own device stream); wall clock with
+    the device synchronised on both sides."""
+    from cumpm_b200 import systems as S
+
+    syst = c5_systems()
+    out = {"workload": ("16 periodic systems, N log-uniform [1k, 64k] (seeded), sum N = "
+                        f"{sum(s.num_particles for s in syst)}; hex monolayers and random packings "
+                        "phi U[0.05, 0.2]; a = 5 nm Drude spheres, eps_m 1.77; dipoles + quadrupoles; "
+                        "8 freqs 0.2-1.0 eV x 3 pols; tol 1e-6; batched mixed precision per system"),
+           "sizes": [s.num_particles for s in syst], "rhs": 24 * len(syst)}
+    for conc in (1, 2):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        res = S.solve_systems(syst, concurrency=conc)
+        torch.cuda.synchronize()
+        t = time.perf_counter() - t0
+        ok = all(np.all(np.isfinite(r["dipoles"])) for r in res)
+        out[f"concurrency_{conc}"] = {"s": round(t, 3), "solves_per_s": round(out["rhs"] / t, 2),
+                                      "systems_per_s": round(len(syst) / t, 3), "finite": bool(ok)}
+        del res
+        torch.cuda.empty_cache()
     return out
 
 
@@ -1066,6 +1137,8 @@ def main():
     ap.add_argument("--no-accuracy", action="store_true", help="skip the per-dipole fp64 comparison")
     ap.add_argument("--no-extras", action="store_true", help="skip the other workloads")
     ap.add_argument("--no-reference-gpu", action="store_true", help="skip the reference build's GPU solve")
+    ap.add_argument("--no-c5", action="store_true", help="skip the 16-system workload")
+    ap.add_argument("--c5-only", action="store_true", help="run only the 16-system workload and print its line")
     ap.add_argument("--workload", default="monolayer", choices=["monolayer", "poly3d", "c1"],
                     help="monolayer: the headline N=4000 case; poly3d: the N=1000 polydisperse 192-RHS case; "
                          "c1: the N=500 single-RHS case")
@@ -1079,6 +1152,11 @@ def main():
         return
     if args.apply_only:
         run_apply_only(args)
+        return
+    if args.c5_only:
+        import torch
+
+        print(json.dumps({"c5_systems": run_c5(args, torch)}))
         return
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))

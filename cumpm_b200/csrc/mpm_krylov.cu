@@ -1289,7 +1289,9 @@ void BatchSolver::solve(Field& F, const double2* b, double2* x, int M, const dou
     // Krylov spaces; later corrections are per column.
     std::vector<int> grp;
     std::vector<double2> fsh;
-    const bool shifted = opt.shifted && opt.method == SOLVER_GMRES &&
+    // (quadrupole rows carry 2.5 s / a^2 + 0.5 g on the diagonal, which is
+    // not a multiple of s: no shifted family with quadrupoles)
+    const bool shifted = opt.shifted && opt.method == SOLVER_GMRES && F.num_quads() == 0 &&
                          detect_shifts(b, sc, rows, F.num_particles(), M, s, grp, fsh);
     bool reset = false;   // x replaced by the shifted solve from zero: every column active again
     std::vector<double> hb(M), hr(M);

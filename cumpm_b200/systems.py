@@ -158,9 +158,33 @@ class SystemSolveError(RuntimeError):
     the results have been exchanged, so no rank is left waiting."""
 
 
+def _solve_share(systems: Sequence[System], idx: Sequence[int], solve_fn, concurrency: int,
+                 bind: Optional[Callable[[], None]], rank: int):
+    """(index, ok, result or message) for each system of idx, solved one
+    after another or, with concurrency > 1, by that many host threads at
+    once (each solve has its own device stream, so small systems overlap on
+    the GPU; the native solve releases the interpreter lock)."""
+    def one(i):
+        try:
+            return (i, True, solve_fn(systems[i]))
+        except Exception as e:  # reported on every rank after the gather
+            return (i, False, f"rank {rank}: {type(e).__name__}: {e}")
+
+    if concurrency <= 1 or len(idx) <= 1:
+        return [one(i) for i in idx]
+    from concurrent.futures import ThreadPoolExecutor
+
+    # largest first, so that the long solves start early; results in idx order
+    order = sorted(idx, key=lambda i: -system_cost(systems[i].num_particles))
+    with ThreadPoolExecutor(max_workers=int(concurrency), initializer=bind) as ex:
+        done = dict(zip(order, ex.map(one, order)))
+    return [done[i] for i in idx]
+
+
 def solve_systems(systems: Sequence[System], *, dist=None,
                   solve_fn: Callable[[System], Dict[str, np.ndarray]] = solve_one,
-                  bind_device: Optional[Callable[[int], None]] = _bind_device) -> List[Dict[str, np.ndarray]]:
+                  bind_device: Optional[Callable[[int], None]] = _bind_device,
+                  concurrency: int = 1) -> List[Dict[str, np.ndarray]]:
     """Solve every system once across the ranks of ``dist`` (an initialised
     ``torch.distributed``, or None for one process) and return all results,
     in system order, on every rank.
@@ -173,20 +197,27 @@ def solve_systems(systems: Sequence[System], *, dist=None,
     not.  A solve that raises is caught and its message travels in the
     gather; afterwards every rank raises :class:`SystemSolveError` naming the
     failed systems.
+
+    ``concurrency`` > 1 solves up to that many of a rank's systems at once
+    from host threads (each bound to the rank's GPU), so that systems too
+    small to fill the GPU overlap; results do not depend on it.
     """
     sizes = [s.num_particles for s in systems]
     if dist is None or not dist.is_initialized():
-        return [solve_fn(s) for s in systems]
+        if concurrency <= 1:
+            return [solve_fn(s) for s in systems]
+        res = _solve_share(systems, range(len(systems)), solve_fn, concurrency, None, 0)
+        bad = [f"system {i} ({r})" for i, ok, r in res if not ok]
+        if bad:
+            raise SystemSolveError("; ".join(bad))
+        return [r for _, _, r in res]
     rank, world = dist.get_rank(), dist.get_world_size()
+    ordinal = local_device_ordinal(rank)
     if bind_device is not None:
-        bind_device(local_device_ordinal(rank))
+        bind_device(ordinal)
     mine = partition(sizes, world)[rank]
-    local = []
-    for i in mine:
-        try:
-            local.append((i, True, solve_fn(systems[i])))
-        except Exception as e:  # reported on every rank after the gather
-            local.append((i, False, f"rank {rank}: {type(e).__name__}: {e}"))
+    bind = (lambda: bind_device(ordinal)) if bind_device is not None else None
+    local = _solve_share(systems, mine, solve_fn, concurrency, bind, rank)
     gathered: List[object] = [None] * world
     dist.all_gather_object(gathered, local)
     out: List[Optional[Dict[str, np.ndarray]]] = [None] * len(systems)

@@ -97,12 +97,12 @@ def test_eels_zone_sum_matches_oracle():
     from cumpm_b200 import eels
     from oracle import mpm_eels as E
     rng = np.random.default_rng(3)
-    box = np.array([40.0, 36.0, 60.0])
-    pos = np.c_[rng.uniform(0, 40, 6), rng.uniform(0, 36, 6), np.zeros(6)]
+    box = np.array([60.0, 54.0, 60.0])   # every edge above twice the cutoff (8 radii at tol 1e-7)
+    pos = np.c_[rng.uniform(0, 60, 6), rng.uniform(0, 54, 6), np.zeros(6)]
     pos = pos[np.argsort(pos[:, 0])]
     omega = [0.03, 0.05, 0.08]
     eps = 4.0 - 1.8 ** 2 / (np.array([0.6, 0.9, 1.2]) ** 2 + 0.1j * np.array([0.6, 0.9, 1.2]))
-    kw = dict(eps_m=1.0, radius=3.0, xi=0.5, tol=1e-8)
+    kw = dict(eps_m=1.0, radius=3.0, xi=0.5, tol=1e-7)
     ref = E.EELSOracle(box, eps, omega, 0.5, field_type="monodisperse", asm=True, asm_n=(2, 2), **kw)
     z_ref, d_ref = ref.compute([11.0, 7.0], pos)
     s = eels.EELS(box, eps, omega, 0.5, field_type="monodisperse", asm_flag=True, asm_Nx=2, asm_Ny=2, quiet=True,
@@ -110,5 +110,5 @@ def test_eels_zone_sum_matches_oracle():
     s.compute([11.0, 7.0], pos)
     z = s.get_eels()
     d = np.asarray(s.get_dipoles(physical=False))
-    assert rel(z, z_ref) < 1e-6, (z, z_ref)
-    assert rel(d, d_ref) < 1e-6
+    assert rel(z, z_ref) < 1e-5, (z, z_ref)
+    assert rel(d, d_ref) < 1e-5

@@ -80,3 +80,18 @@ def test_frequency_blocks_concatenate_to_the_whole_sweep():
         assert err < lim, (key, err)
     one = S.solve_sharded(syst)
     assert one["dipoles"].shape == np.squeeze(whole["dipoles"]).shape
+
+
+@pytest.mark.first_gpu_run
+def test_concurrent_systems_match_serial():
+    """Three systems solved at once from host threads (each with its own
+    device stream) give what they give one after another."""
+    from cumpm_b200 import systems as S
+
+    syst = _systems()
+    serial = S.solve_systems(syst)
+    conc = S.solve_systems(syst, concurrency=3)
+    for a, b in zip(conc, serial):
+        assert set(a) == set(b)
+        for k in b:
+            np.testing.assert_allclose(a[k], b[k], rtol=1e-12, atol=1e-14 * np.abs(b[k]).max())

@@ -295,3 +295,22 @@ def test_gloo_ranks_shard_the_frequencies(world, fail):
             assert res == "rank 1: RuntimeError: injected"
         else:
             assert res == e and shape == (10, 6, 3, 3)
+
+
+def test_concurrent_share_gives_the_serial_results():
+    """Threads within a rank: same results in the same order, a failing
+    system raises SystemSolveError naming it, others still solved."""
+    serial = S.solve_systems(_systems(), solve_fn=_fake_solve)
+    conc = S.solve_systems(_systems(), solve_fn=_fake_solve, concurrency=3)
+    assert [int(r["n"][0]) for r in conc] == [int(r["n"][0]) for r in serial]
+    calls = []
+
+    def solve(system):
+        calls.append(system.num_particles)
+        if system.num_particles == 11:
+            raise ValueError("boom")
+        return _fake_solve(system)
+
+    with pytest.raises(S.SystemSolveError, match=r"system 3 \(rank 0: ValueError: boom\)"):
+        S.solve_systems(_systems(), solve_fn=solve, concurrency=2)
+    assert sorted(calls) == sorted(s.num_particles for s in _systems())
