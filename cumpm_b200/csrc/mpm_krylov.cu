@@ -48,14 +48,18 @@ __global__ void __launch_bounds__(256) k_dots1(const double2* __restrict__ V, si
     }
 }
 
-// k_dots1 for few columns (M < 16): threads run over the flat [row][M]
-// elements, (256 / M) * M of them per CTA, so that each thread keeps one
-// column m for the whole grid-stride loop (the stride is a multiple of M);
-// the CTA's per-column sums are then taken over the threads of that column
-// in a fixed order.  Same partial layout as k_dots1.
+// k_dots1 + k_dots2 for few columns (M < 16): threads run over the flat
+// [row][M] elements, (256 / M) * M of them per CTA, so that each thread
+// keeps one column m for the whole grid-stride loop (the stride is a
+// multiple of M); the CTA's per-column sums are taken over the threads of
+// that column in a fixed order and written as k_dots1's partials.  The last
+// CTA of each vector group to finish (a counter per group, no waiting) then
+// reduces the partials exactly as k_dots2 does (lanes over CTAs, fixed
+// shuffle tree) into out, and resets its counter.
 __global__ void __launch_bounds__(256) k_dots1s(const double2* __restrict__ V, size_t vstride, int nvec,
                                                 const double2* __restrict__ w, int rows, int M, int conj,
-                                                double2* __restrict__ partial, int shift) {
+                                                double2* __restrict__ partial, int shift,
+                                                double2* __restrict__ out, unsigned int* __restrict__ done) {
     __shared__ double2 red[8][256];
     const int L = (256 / M) * M;
     const int j = threadIdx.x;
@@ -83,6 +87,25 @@ __global__ void __launch_bounds__(256) k_dots1s(const double2* __restrict__ V, s
         for (int q = m; q < L; q += M) sum += red[k][q];
         partial[(size_t(blockIdx.x) * nvec + i0 + k) * M + m] = sum;
     }
+    __threadfence();
+    __syncthreads();
+    __shared__ int last;
+    if (j == 0) last = atomicAdd(&done[blockIdx.z], 1u) == gridDim.x - 1;
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    const int lane = j & 31, warp = j >> 5;
+    for (int o = warp; o < nv * M; o += 8) {
+        const int t = (i0 + o / M) * M + o % M;
+        double2 sum = make_double2(0, 0);
+        for (int b = lane; b < int(gridDim.x); b += 32) sum += __ldcg(&partial[size_t(b) * nvec * M + t]);
+        for (int off = 16; off > 0; off >>= 1) {
+            sum.x += __shfl_xor_sync(0xffffffffu, sum.x, off);
+            sum.y += __shfl_xor_sync(0xffffffffu, sum.y, off);
+        }
+        if (lane == 0) out[t] = sum;
+    }
+    if (j == 0) done[blockIdx.z] = 0u;
 }
 
 // one warp per output: lanes stride over the per-CTA partials, then a fixed
@@ -826,11 +849,14 @@ void BatchSolver::dots(const double2* V, size_t vstride, int nvec, const double2
     if (M < 16) {
         const long long L = (256 / M) * M;
         const int gx = int(std::max(1LL, std::min(592LL, (1LL * rows * M + L - 1) / L)));
+        const int nz = (nvec + 7) / 8;
         partial_.ensure(sizeof(double2) * size_t(gx) * nvec * M);
-        k_dots1s<<<dim3(gx, 1, (nvec + 7) / 8), 256, 0, s>>>(V, vstride, nvec, w, rows, M, conj,
-                                                             partial_.as<double2>(), shift);
-        MPM_LAUNCH();
-        k_dots2<<<nblk((long long)nvec * M * 32, 256), 256, 0, s>>>(partial_.as<double2>(), gx, nvec, M, out);
+        if (!dots_done_.p || dots_done_.bytes < sizeof(unsigned int) * size_t(nz)) {
+            dots_done_.ensure(sizeof(unsigned int) * std::max<size_t>(size_t(nz), 64));
+            MPM_CUDA(cudaMemsetAsync(dots_done_.p, 0, dots_done_.bytes, s));
+        }
+        k_dots1s<<<dim3(gx, 1, nz), 256, 0, s>>>(V, vstride, nvec, w, rows, M, conj, partial_.as<double2>(), shift,
+                                                 out, dots_done_.as<unsigned int>());
         MPM_LAUNCH();
         return;
     }

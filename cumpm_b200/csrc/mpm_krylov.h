@@ -118,6 +118,7 @@ private:
     DevBuf cidx_, xc_, yc_, scc_;        // compact-batch gather buffers
     DevBuf bn2_, rn2_, convd_;           // refinement: |b|, true |r|, converged flags
     DevBuf sel_, rn64_;                  // refinement: columns re-checked in fp64, their |r|
+    DevBuf dots_done_;                   // finished-CTA counters of the fused small dot kernel
     DevBuf shf_, shflag_, shmeta_, shsc_, shb_, shst_, hm_;   // shifted solve: detection, seeds, members
     int* flag_ = nullptr;                // pinned host words: count + per-column flags
     int flag_cap_ = 0;
