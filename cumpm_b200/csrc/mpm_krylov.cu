@@ -284,7 +284,7 @@ __device__ void gm_givens(GState& s, const double2* __restrict__ h, double wn, d
 }
 
 // givens = 0 (the seeds of a shifted solve): |w'| and the normalisation
-// only; the Givens updates are the members' (k_shift_givens).  always2:
+// only; the Givens updates are the members' (shift_givens_body).  always2:
 // every column takes the second projection (CGS2); else only those that
 // fail the 0.7 test.
 // pass 1: hh = [V_0..V_k, w]^H w.  Columns whose projection keeps |w'| >
@@ -293,15 +293,14 @@ __device__ void gm_givens(GState& s, const double2* __restrict__ h, double wn, d
 // after the first projection): h += h2, |w''| likewise, Givens.  Thread per
 // column; one CTA: flag[0] = columns still cycling, flag[1 + m] = column m
 // cycling, flag[1 + M] = columns marked for the second pass.
-__global__ void __launch_bounds__(1024) k_arn_finish(GState* __restrict__ st, double2* __restrict__ h,
-                                                     const double2* __restrict__ h2, int pass, int givens, int always2,
-                                                     double* __restrict__ nu_out,
-                                                     double* __restrict__ inv_nu, double2* __restrict__ H,
-                                                     double2* __restrict__ g, double* __restrict__ cs,
-                                                     double2* __restrict__ sn, int k, int restart, int M,
-                                                     const double* __restrict__ bn, double tol,
-                                                     const double* __restrict__ tolv, int maxiter,
-                                                     int* __restrict__ flag) {
+__device__ __forceinline__ void arn_finish_body(GState* __restrict__ st, double2* __restrict__ h,
+                                                const double2* __restrict__ h2, int pass, int givens, int always2,
+                                                double* __restrict__ nu_out, double* __restrict__ inv_nu,
+                                                double2* __restrict__ H, double2* __restrict__ g,
+                                                double* __restrict__ cs, double2* __restrict__ sn, int k, int restart,
+                                                int M, const double* __restrict__ bn, double tol,
+                                                const double* __restrict__ tolv, int maxiter,
+                                                int* __restrict__ flag) {
     __shared__ int ncyc, nreo;
     if (threadIdx.x == 0) ncyc = nreo = 0;
     __syncthreads();
@@ -355,6 +354,19 @@ __global__ void __launch_bounds__(1024) k_arn_finish(GState* __restrict__ st, do
         flag[0] = ncyc;
         flag[1 + M] = nreo;
     }
+}
+
+__global__ void __launch_bounds__(1024) k_arn_finish(GState* __restrict__ st, double2* __restrict__ h,
+                                                     const double2* __restrict__ h2, int pass, int givens, int always2,
+                                                     double* __restrict__ nu_out,
+                                                     double* __restrict__ inv_nu, double2* __restrict__ H,
+                                                     double2* __restrict__ g, double* __restrict__ cs,
+                                                     double2* __restrict__ sn, int k, int restart, int M,
+                                                     const double* __restrict__ bn, double tol,
+                                                     const double* __restrict__ tolv, int maxiter,
+                                                     int* __restrict__ flag) {
+    arn_finish_body(st, h, h2, pass, givens, always2, nu_out, inv_nu, H, g, cs, sn, k, restart, M, bn, tol, tolv,
+                    maxiter, flag);
 }
 
 // V_{k+1} -= sum_{i <= k} V_i h_i for the columns of this pass (pass 1: the
@@ -436,15 +448,14 @@ __global__ void k_col_equal(const double2* __restrict__ b, int rows, int M, int*
 // its second projection keep it cycling.  A seed cycles while any member
 // does (written back to its state).  One CTA: flag[0] = seeds cycling,
 // flag[1 + g] = seed g cycling.
-__global__ void __launch_bounds__(1024) k_shift_givens(GState* __restrict__ mst, GState* __restrict__ sst,
-                                                       const double2* __restrict__ hs, const double* __restrict__ nu,
-                                                       const double2* __restrict__ sigma, const int* __restrict__ grp,
-                                                       int G, int pass, double2* __restrict__ hm,
-                                                       double2* __restrict__ H, double2* __restrict__ g,
-                                                       double* __restrict__ cs, double2* __restrict__ sn, int k,
-                                                       int restart, int M, const double* __restrict__ bs,
-                                                       const double* __restrict__ tolv, int maxiter,
-                                                       int* __restrict__ seed_cyc, int* __restrict__ flag) {
+__device__ __forceinline__ void shift_givens_body(GState* __restrict__ mst, GState* __restrict__ sst,
+                                                  const double2* __restrict__ hs, const double* __restrict__ nu,
+                                                  const double2* __restrict__ sigma, const int* __restrict__ grp,
+                                                  int G, int pass, double2* __restrict__ hm, double2* __restrict__ H,
+                                                  double2* __restrict__ g, double* __restrict__ cs,
+                                                  double2* __restrict__ sn, int k, int restart, int M,
+                                                  const double* __restrict__ bs, const double* __restrict__ tolv,
+                                                  int maxiter, int* __restrict__ seed_cyc, int* __restrict__ flag) {
     __shared__ int n;
     if (threadIdx.x == 0) n = 0;
     for (int t = threadIdx.x; t < G; t += blockDim.x) seed_cyc[t] = 0;
@@ -476,6 +487,28 @@ __global__ void __launch_bounds__(1024) k_shift_givens(GState* __restrict__ mst,
     }
     __syncthreads();
     if (threadIdx.x == 0) flag[0] = n;
+}
+
+// The seeds' second projection (k_arn_finish pass 2, no Givens) and the
+// members' Givens updates (shift_givens_body, pass 2) in one CTA: the members
+// read only the seeds' Hessenberg column and norm, which the first part
+// writes, so the seeds' normalisation of V_{k+1} can follow.
+__global__ void __launch_bounds__(1024) k_seed_finish_givens(GState* __restrict__ sst, double2* __restrict__ h,
+                                                             const double2* __restrict__ h2,
+                                                             double* __restrict__ nu, double* __restrict__ inv_nu,
+                                                             int k, int restart, int G, const double* __restrict__ bs,
+                                                             double tol, int maxiter, GState* __restrict__ mst,
+                                                             const double2* __restrict__ sigma,
+                                                             const int* __restrict__ grp, double2* __restrict__ hm,
+                                                             double2* __restrict__ H, double2* __restrict__ g,
+                                                             double* __restrict__ cs, double2* __restrict__ sn, int M,
+                                                             const double* __restrict__ tolv,
+                                                             int* __restrict__ seed_cyc, int* __restrict__ flag) {
+    arn_finish_body(sst, h, h2, 2, 0, 1, nu, inv_nu, nullptr, nullptr, nullptr, nullptr, k, restart, G, bs, tol,
+                    nullptr, maxiter, flag);
+    __syncthreads();
+    shift_givens_body(mst, sst, h, nu, sigma, grp, G, 2, hm, H, g, cs, sn, k, restart, M, bs, tolv, maxiter,
+                      seed_cyc, flag);
 }
 
 // member states: active and cycling from the start, x0 = 0; g_m = (beta, 0..);
@@ -1131,19 +1164,21 @@ void BatchSolver::gmres_shifted(Field& F, const double2* b, double2* x, int M, c
         st.matvecs++;
         auto seed_pass = [&](int pass, const double2* hv) {
             // (every seed takes both projections: the members' Givens updates
-            // follow the second)
+            // follow the second, in the same one-CTA kernel)
             StageScope sc1(ST_KRYLOV, s);
-            k_arn_finish<<<1, fthr, 0, s>>>(sst, h_.as<double2>(), h2_.as<double2>(), pass, 0, 1, nu,
-                                            rnorm_.as<double>(), nullptr, nullptr, nullptr, nullptr, k, restart, G,
-                                            bs, opt.tol, nullptr, opt.maxiter, dflag);
+            if (pass == 1) {
+                k_arn_finish<<<1, fthr, 0, s>>>(sst, h_.as<double2>(), h2_.as<double2>(), pass, 0, 1, nu,
+                                                rnorm_.as<double>(), nullptr, nullptr, nullptr, nullptr, k, restart,
+                                                G, bs, opt.tol, nullptr, opt.maxiter, dflag);
+            } else {
+                k_seed_finish_givens<<<1, fthr, 0, s>>>(sst, h_.as<double2>(), h2_.as<double2>(), nu,
+                                                        rnorm_.as<double>(), k, restart, G, bs, opt.tol,
+                                                        opt.maxiter, mst, dsig, dgrp, hm_.as<double2>(),
+                                                        H_.as<double2>(), g_.as<double2>(), cs_.as<double>(),
+                                                        sn_.as<double2>(), M, tolv, scyc, dflag);
+            }
             MPM_LAUNCH();
             k_arn_update<<<vb, 256, 0, s>>>(V, ns, k, hv, sst, rnorm_.as<double>(), rows, G, pass);
-            MPM_LAUNCH();
-            if (pass == 1) return;
-            k_shift_givens<<<1, fthr, 0, s>>>(mst, sst, h_.as<double2>(), nu, dsig, dgrp, G, pass,
-                                              hm_.as<double2>(), H_.as<double2>(), g_.as<double2>(),
-                                              cs_.as<double>(), sn_.as<double2>(), k, restart, M, bs, tolv,
-                                              opt.maxiter, scyc, dflag);
             MPM_LAUNCH();
         };
         dots(V, ns, k + 2, w, rows, G, 1, h_.as<double2>(), s, k);

@@ -61,13 +61,17 @@ public:
     }
     ~PyDipoleSolver() { mpm_solver_destroy(s_); }
 
-    void compute(const std::vector<double>& x, const std::vector<double>& y, const std::vector<double>& z) {
-        if (x.size() != y.size() || x.size() != z.size())
+    // coordinates as float64 arrays (lists and other sequences are converted)
+    using darr = py::array_t<double, py::array::c_style | py::array::forcecast>;
+    void compute(const darr& x, const darr& y, const darr& z) {
+        if (x.ndim() != 1 || y.ndim() != 1 || z.ndim() != 1 || x.size() != y.size() || x.size() != z.size())
             throw py::value_error("Input coordinate vectors must have the exact same size.");
+        const double *px = x.data(), *py_ = y.data(), *pz = z.data();
+        const int n = int(x.size());
         int st;
         {
             py::gil_scoped_release nogil;
-            st = mpm_solver_compute(s_, x.data(), y.data(), z.data(), int(x.size()));
+            st = mpm_solver_compute(s_, px, py_, pz, n);
         }
         check(st);
     }

@@ -142,6 +142,148 @@ std::vector<cdouble> DipoleSolver::guess(const std::vector<cdouble>& fd, const s
     return g;
 }
 
+namespace {
+
+inline int nblk_s(long long n, int b) { return int((n + b - 1) / b); }
+
+// X[row][m] (row 3p + c, m = f K + k) of the all-frequency batch: frequency
+// 0 from init (frame layout [p][k][c]) when given, the others the
+// mean-field guess 4 pi a^3 beta / (1 - beta phi) E0_k, beta = (e-1)/(e+2)
+// (the same quotients as DipoleSolver::mean_field_guess)
+__global__ void k_batch_guess(double2* __restrict__ X, int M, int N, int K, const double2* __restrict__ eps,
+                              const double* __restrict__ rad, double phi, const double2* __restrict__ E0,
+                              const double2* __restrict__ init) {
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long long)N * 3 * M) return;
+    const int m = int(t % M);
+    const int row = int(t / M);
+    const int p = row / 3, c = row % 3;
+    const int f = m / K, k = m % K;
+    if (f == 0 && init) {
+        X[t] = init[(size_t(p) * K + k) * 3 + c];
+        return;
+    }
+    const double2 e = eps[size_t(f) * N + p];
+    auto quot = [](double2 a, double2 b) {
+        const double d = b.x * b.x + b.y * b.y;
+        return make_double2((a.x * b.x + a.y * b.y) / d, (a.y * b.x - a.x * b.y) / d);
+    };
+    const double2 beta = quot(make_double2(e.x - 1.0, e.y), make_double2(e.x + 2.0, e.y));
+    const double r3 = rad[p] * rad[p] * rad[p];
+    const double2 num = make_double2(4.0 * kPi * r3 * beta.x, 4.0 * kPi * r3 * beta.y);
+    const double2 den = make_double2(1.0 - beta.x * phi, -beta.y * phi);
+    const double2 val = quot(num, den);
+    const double2 ev = E0[size_t(k) * 3 + c];
+    X[t] = make_double2(val.x * ev.x - val.y * ev.y, val.x * ev.y + val.y * ev.x);
+}
+
+// frame[f][p][k][c] = X[3p + c][f K + k]
+__global__ void k_to_frame(const double2* __restrict__ X, int M, int N, int K, double2* __restrict__ frame) {
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long long)N * 3 * M) return;
+    const int c = int(t % 3);
+    const long long r = t / 3;
+    const int k = int(r % K);
+    const long long r2 = r / K;
+    const int p = int(r2 % N);
+    const int f = int(r2 / N);
+    frame[t] = X[size_t(3 * p + c) * M + size_t(f) * K + k];
+}
+
+}  // namespace
+
+bool DipoleSolver::device_batch_ok() const {
+    if (!opt_.batch_all || (solve_quads_ && Nq_)) return false;
+    for (const auto& e : E0_)
+        if (e.size() != 3) return false;
+    return true;
+}
+
+// The all-frequency batch with its guesses and results on the device: the
+// same solve as solve_batch over every frequency, without the host loops
+// over the [row][M] layout.
+void DipoleSolver::solve_all_device(const std::vector<cdouble>& init, std::vector<cdouble>& frame_cap,
+                                    std::vector<cdouble>& frame_dip) {
+    const size_t K = E0_.size(), W = eps_p_.size();
+    const size_t rows = N_ * 3;
+    const int M = int(W * K);
+    std::vector<size_t> freqs(W);
+    for (size_t w = 0; w < W; ++w) freqs[w] = w;
+    const size_t bytes = sizeof(double2) * rows * M;
+    dB_.ensure(bytes);
+    dX_.ensure(bytes);
+    dSC_.ensure(sizeof(double2) * N_ * M);
+    if (freqs != dev_freqs_) {
+        // right-hand sides and self terms (dipole_solver.cu:452-460), once
+        hB_.ensure(sizeof(cdouble) * rows * M);
+        hSC_.ensure(sizeof(cdouble) * N_ * M);
+        cdouble* hb = hB_.as<cdouble>();
+        cdouble* hsc = hSC_.as<cdouble>();
+        for (size_t p = 0; p < N_; ++p) {
+            for (size_t f = 0; f < W; ++f) {
+                cdouble diff = 1.0 - eps_p_[f][p];
+                if (std::abs(diff) < 1e-12) diff = 1e-12;
+                const cdouble sv = -3.0 / (4.0 * PI * diff) / std::pow(radius_[p], 3.0);
+                for (size_t k = 0; k < K; ++k) hsc[p * M + f * K + k] = sv;
+            }
+            for (int c = 0; c < 3; ++c)
+                for (size_t f = 0; f < W; ++f)
+                    for (size_t k = 0; k < K; ++k) hb[(p * 3 + c) * M + f * K + k] = E0_[k][c];
+        }
+        MPM_CUDA(cudaMemcpyAsync(dB_.p, hb, bytes, cudaMemcpyHostToDevice, stream_));
+        MPM_CUDA(cudaMemcpyAsync(dSC_.p, hsc, sizeof(double2) * N_ * M, cudaMemcpyHostToDevice, stream_));
+        dev_freqs_ = freqs;
+    }
+    if (!dev_eps_) {
+        std::vector<cdouble> e(W * N_), e0(K * 3);
+        for (size_t w = 0; w < W; ++w)
+            for (size_t p = 0; p < N_; ++p) e[w * N_ + p] = eps_p_[w][p];
+        for (size_t k = 0; k < K; ++k)
+            for (int c = 0; c < 3; ++c) e0[k * 3 + c] = E0_[k][c];
+        dEps_.ensure(sizeof(double2) * W * N_);
+        dRad_.ensure(sizeof(double) * N_);
+        dE0_.ensure(sizeof(double2) * K * 3);
+        MPM_CUDA(cudaMemcpy(dEps_.p, e.data(), sizeof(double2) * W * N_, cudaMemcpyHostToDevice));
+        MPM_CUDA(cudaMemcpy(dRad_.p, radius_.data(), sizeof(double) * N_, cudaMemcpyHostToDevice));
+        MPM_CUDA(cudaMemcpy(dE0_.p, e0.data(), sizeof(double2) * K * 3, cudaMemcpyHostToDevice));
+        dev_eps_ = true;
+    }
+    dInit_.ensure(sizeof(double2) * N_ * K * 3);
+    hX_.ensure(sizeof(cdouble) * N_ * K * 3);
+    std::copy(init.begin(), init.begin() + N_ * K * 3, hX_.as<cdouble>());
+    MPM_CUDA(cudaMemcpyAsync(dInit_.p, hX_.p, sizeof(double2) * N_ * K * 3, cudaMemcpyHostToDevice, stream_));
+    const long long n = (long long)rows * M;
+    k_batch_guess<<<nblk_s(n, 256), 256, 0, stream_>>>(dX_.as<double2>(), M, int(N_), int(K), dEps_.as<double2>(),
+                                                        dRad_.as<double>(), vol_frac_, dE0_.as<double2>(),
+                                                        dInit_.as<double2>());
+    MPM_LAUNCH();
+    SolveOptions so;
+    so.method = solver_type_ == "bicgstab" ? SOLVER_BICGSTAB : SOLVER_GMRES;
+    so.restart = opt_.restart;
+    so.maxiter = opt_.maxiter;
+    so.tol = tol_;
+    so.jacobi = jacobi_;
+    so.recip_fp32 = precision_ != PREC_DOUBLE;
+    so.real_fp32 = opt_.real_fp32;
+    so.refine = opt_.refine;
+    so.inner_tol = opt_.inner_tol;
+    solver_->solve(*field_, dB_.as<double2>(), dX_.as<double2>(), M, dSC_.as<double2>(), so, last_stats_, stream_);
+    for (int v : last_stats_.iters) iters_.push_back(v);
+    dFrame_.ensure(bytes);
+    k_to_frame<<<nblk_s(n, 256), 256, 0, stream_>>>(dX_.as<double2>(), M, int(N_), int(K), dFrame_.as<double2>());
+    MPM_LAUNCH();
+    MPM_CUDA(cudaMemcpyAsync(frame_dip.data(), dFrame_.p, bytes, cudaMemcpyDeviceToHost, stream_));
+    MPM_CUDA(cudaStreamSynchronize(stream_));
+    // particle averages per (frequency, polarisation, component)
+    for (size_t f = 0; f < W; ++f) {
+        const cdouble* src = frame_dip.data() + f * N_ * K * 3;
+        cdouble* cap = frame_cap.data() + f * K * 3;
+        for (size_t p = 0; p < N_; ++p)
+            for (size_t j = 0; j < K * 3; ++j) cap[j] += src[p * K * 3 + j];
+        for (size_t j = 0; j < K * 3; ++j) cap[j] /= double(N_);
+    }
+}
+
 // One batched device solve for the given frequencies (each with K
 // polarisations); results scattered into the frame arrays
 // (dipole_solver.cu:361-436 per polarisation, here all at once).
@@ -340,7 +482,9 @@ void DipoleSolver::compute(const std::vector<double>& x, const std::vector<doubl
     std::vector<cdouble> frame_cap(W * K * 3, 0.0), frame_dip(W * N_ * K * 3, 0.0), frame_quad(W * Nq_ * K * 5, 0.0);
     print("Wavenumber:");
     indent_++;
-    if (opt_.batch_all) {
+    if (device_batch_ok()) {
+        solve_all_device(init, frame_cap, frame_dip);
+    } else if (opt_.batch_all) {
         std::vector<size_t> fr(W);
         std::vector<std::vector<cdouble>> gs(W);
         for (size_t w = 0; w < W; ++w) {

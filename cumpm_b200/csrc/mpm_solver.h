@@ -79,6 +79,12 @@ private:
     std::vector<cdouble> guess(const std::vector<cdouble>& fd, const std::vector<cdouble>& fq, size_t w) const;
     void solve_batch(const std::vector<size_t>& freqs, const std::vector<std::vector<cdouble>>& guesses,
                      std::vector<cdouble>& frame_cap, std::vector<cdouble>& frame_dip, std::vector<cdouble>& frame_quad);
+    // batch_all with dipoles and uniform incident fields: the mean-field
+    // guesses of frequencies 1..W-1 (and frequency 0's, from init) are built
+    // on the device and the solution is written into the frame layout there
+    bool device_batch_ok() const;
+    void solve_all_device(const std::vector<cdouble>& init, std::vector<cdouble>& frame_cap,
+                          std::vector<cdouble>& frame_dip);
     void print(const std::string& msg) const;
 
     std::vector<double> box_;
@@ -108,6 +114,8 @@ private:
     std::unique_ptr<BatchSolver> solver_;
     cudaStream_t stream_ = nullptr;
     DevBuf dB_, dX_, dSC_;
+    DevBuf dEps_, dRad_, dE0_, dInit_, dFrame_;   // device batch: eps (W x N), radii, E0 (K x 3), init, frame
+    bool dev_eps_ = false;
     HostBuf hB_, hX_, hSC_;   // pinned staging of the batch's right-hand sides, guesses / solutions, self terms
     // frequencies whose right-hand sides and self terms dB_ / dSC_ hold (they
     // depend on nothing that changes between frames)

@@ -140,7 +140,8 @@ class dipole_solver:
         if getattr(self, "_autotune_pending", False):
             self.autotune(pos[0])
         for frame in pos:
-            self._solver.compute(frame[:, 0].tolist(), frame[:, 1].tolist(), frame[:, 2].tolist())
+            self._solver.compute(np.ascontiguousarray(frame[:, 0]), np.ascontiguousarray(frame[:, 1]),
+                                 np.ascontiguousarray(frame[:, 2]))
 
     def get_eff_polarizability(self, physical=True):
         """Frame- and particle-averaged dipole per polarisation, (W, K, 3) squeezed."""
