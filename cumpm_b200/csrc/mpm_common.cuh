@@ -28,6 +28,16 @@ inline void cuda_check(cudaError_t e, const char* what, const char* file, int li
     }
 }
 #define MPM_CUDA(x) ::mpm::cuda_check((x), #x, __FILE__, __LINE__)
+
+// Raises a kernel's dynamic shared-memory limit to at least `bytes` and never
+// lowers it.  The limit is one attribute per kernel for the whole process:
+// fields solved at once from several host threads share it, and a lower
+// value set for one would make another's larger launch fail.
+void raise_smem_limit(const void* kernel, size_t bytes);
+template <typename K>
+inline void set_smem_limit(K* kernel, size_t bytes) {
+    raise_smem_limit(reinterpret_cast<const void*>(kernel), bytes);
+}
 // count one of this library's kernel launches and check it
 void note_launch();
 #define MPM_LAUNCH() (::mpm::note_launch(), ::mpm::cuda_check(cudaGetLastError(), "kernel launch", __FILE__, __LINE__))

@@ -668,7 +668,7 @@ template <typename R, int MODE, int CW>
 void launch2_cw(int cls, int nblocks, int nthreads, size_t shm, cudaStream_t s, cplx<R>* data, const cplx<R>* tw,
                 int r1, int r2, size_t es, int ncols, size_t os, int ngroups, const LineScale<R>& ks) {
     auto go = [&](auto kern) {
-        MPM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(shm)));
+        set_smem_limit(kern, shm);
         kern<<<nblocks, nthreads, shm, s>>>(data, tw, r1, r2, es, ncols, os, ngroups, ks);
     };
     if (cls == 8) go(k_fft2<R, CW, MODE, 8>);
@@ -1009,7 +1009,7 @@ void launch2p_cw(int cls, int nblocks, int nthreads, size_t shm, cudaStream_t s,
                  const cplx<R>* ptw, int pt_total, int pt_ld, int r1, int p, size_t es, int ncols, size_t os,
                  int ngroups) {
     auto go = [&](auto kern) {
-        MPM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(shm)));
+        set_smem_limit(kern, shm);
         kern<<<nblocks, nthreads, shm, s>>>(data, tw, ptw, pt_total, pt_ld, r1, p, es, ncols, os, ngroups);
     };
     if (cls == 8) go(k_fft2p<R, CW, INV, 8>);
@@ -1154,7 +1154,7 @@ void launch2r_cw(int cls, int nblocks, int nthreads, size_t shm, cudaStream_t s,
                  const cplx<R>* rtab, const int* rperm, int r1, int p, int A, int B, size_t es, int ncols, size_t os,
                  int ngroups) {
     auto go = [&](auto kern) {
-        MPM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(shm)));
+        set_smem_limit(kern, shm);
         kern<<<nblocks, nthreads, shm, s>>>(data, tw, rtab, rperm, r1, p, A, B, es, ncols, os, ngroups);
     };
     if (cls == 8) go(k_fft2r<R, CW, INV, 8>);
@@ -1205,7 +1205,7 @@ void launch_cw(int cls, bool stream, int nouter, size_t shm, cudaStream_t s, cpl
                const cplx<R>* tw, size_t es, int ncols, size_t os, const cplx<R>* ptw, const LineScale<R>& ks) {
     const int ngroups = (ncols + CW - 1) / CW;
     auto go = [&](auto kern) {
-        MPM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(shm)));
+        set_smem_limit(kern, shm);
         kern<<<nouter * ngroups, kFftThreads, shm, s>>>(data, f, tw, es, ncols, os, ptw, ngroups, ks);
     };
     if (stream) {
@@ -1527,7 +1527,7 @@ void AxisFFT::run_slab(cplx<R>* data, int nx, int Zs, int M, const cplx<R>* taps
                                        : reinterpret_cast<const cplx<R>*>(tw64_.p);
     const int cls = register_class(r1_);
     auto go = [&](auto kern) {
-        MPM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(shm)));
+        set_smem_limit(kern, shm);
         kern<<<nx * a.nchunk, kSlabThreads, shm, s>>>(data, tw, taps, r1_, r2_, a);
     };
     if (Zs == 1) {

@@ -1728,7 +1728,7 @@ void Field::build_spread_plan(cudaStream_t s) {
     const int ncol = TX * TY;
     if (TZ > kSpreadZMax || ntile < 1) return;
     const size_t shm = sizeof(double) * kPlanCandMax * wlen;
-    MPM_CUDA(cudaFuncSetAttribute(k_spread_plan, cudaFuncAttributeMaxDynamicSharedMemorySize, int(shm)));
+    set_smem_limit(k_spread_plan, shm);
     plan_nc_.ensure(sizeof(int) * ntile);
     plan_cnt_.ensure(sizeof(int) * 2);
     MPM_CUDA(cudaMemsetAsync(plan_cnt_.p, 0, sizeof(int) * 2, s));
@@ -1954,7 +1954,7 @@ void Field::build_column_kernel(cudaStream_t s) {
     a.by = spec_.bloch[1];
     const size_t shm = sizeof(double) * 8 * gv_.Nz;
     if (shm > 48 * 1024)
-        MPM_CUDA(cudaFuncSetAttribute(k_build_column, cudaFuncAttributeMaxDynamicSharedMemorySize, int(shm)));
+        set_smem_limit(k_build_column, shm);
     const double* w2 = nullptr;
     if (gv_.layer) {
         layer_wd_.ensure(sizeof(double) * (gv_.S + gv_.Nz));
@@ -2011,7 +2011,7 @@ void Field::build_slab_taps(cudaStream_t s) {
     layer_taps_ = false;
     const size_t shm = sizeof(double) * 5 * gv_.Nz;
     if (shm > 48 * 1024)
-        MPM_CUDA(cudaFuncSetAttribute(k_build_slab_taps, cudaFuncAttributeMaxDynamicSharedMemorySize, int(shm)));
+        set_smem_limit(k_build_slab_taps, shm);
     k_build_slab_taps<<<ncol, 128, shm, s>>>(a, Z, slabT64_.as<double2>(), slabT32_.as<float2>());
     MPM_LAUNCH();
     slab_Z_ = Z;
@@ -2119,7 +2119,7 @@ void Field::recip_on(const double2* X, double2* Y, int M, cplx<R>* grid, cudaStr
     const size_t ncol = size_t(TX) * TY;
     const size_t shm = sizeof(R) * cap * (TX + TY + TZ) + sizeof(cplx<R>) * cap * bc +
                        (sizeof(R) + sizeof(int)) * ncol * kSpreadListCap + sizeof(int) * (ncol + cap);
-    MPM_CUDA(cudaFuncSetAttribute(k_spread<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(shm)));
+    set_smem_limit(k_spread<R>, shm);
     const int nchunk = (B + bc - 1) / bc;
     dim3 grd(ps.nb[0], ps.nb[1], ps.nb[2] * nchunk);  // one CTA per tile and column chunk
     const R* w1 = sizeof(R) == 4 ? reinterpret_cast<const R*>(ps.w32.p) : reinterpret_cast<const R*>(ps.w64.p);
@@ -2130,7 +2130,7 @@ void Field::recip_on(const double2* X, double2* Y, int M, cplx<R>* grid, cudaStr
         const R* wT = f32 ? reinterpret_cast<const R*>(plan_w32_.p) : reinterpret_cast<const R*>(plan_w64_.p);
         const R* lw = f32 ? reinterpret_cast<const R*>(plan_lw32_.p) : reinterpret_cast<const R*>(plan_lw64_.p);
         auto go = [&](auto kern) {
-            MPM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(pshm)));
+            set_smem_limit(kern, pshm);
             kern<<<grd, 256, pshm, s>>>(X, M, N_, C, quad_map_.as<int>(), gv_, TX, TY, TZ, ps.nb[0], ps.nb[1],
                                         ps.nb[2], plan_cap_, bc, plan_nc_.as<int>(), plan_cid_.as<int>(), wT, lw,
                                         plan_lc_.as<int>(), plan_ln_.as<int>(), grid);
@@ -2138,8 +2138,7 @@ void Field::recip_on(const double2* X, double2* Y, int M, cplx<R>* grid, cudaStr
         // the tile's z run in registers: as many accumulators as it needs
         if (TZ == 1 && gv_.Zs == 1) {
             const size_t lshm = pshm + (sizeof(R) + sizeof(int)) * ncol * kSpreadListCap + sizeof(int) * ncol;
-            MPM_CUDA(cudaFuncSetAttribute(k_spread_planned_1z<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                          int(lshm)));
+            set_smem_limit(k_spread_planned_1z<R>, lshm);
             k_spread_planned_1z<R><<<grd, 256, lshm, s>>>(X, M, N_, C, quad_map_.as<int>(), gv_, TX, TY, ps.nb[0],
                                                           ps.nb[1], plan_cap_, bc, plan_nc_.as<int>(),
                                                           plan_cid_.as<int>(), wT, lw, plan_lc_.as<int>(),
@@ -2188,7 +2187,7 @@ void Field::recip_on(const double2* X, double2* Y, int M, cplx<R>* grid, cudaStr
             if (!(gv_.layer ? layer_colK_ : colK_Z_ == gv_.Zs) || !K)
                 throw std::runtime_error("column kernel not built for the current layout");
             auto go = [&](auto kern) {
-                MPM_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, int(shm2)));
+                set_smem_limit(kern, shm2);
                 kern<<<gv_.Nx * gv_.Ny, thr, shm2, s>>>(grid, K, Z, M);
             };
             if (Z <= 9) go(k_column<R, 9>);

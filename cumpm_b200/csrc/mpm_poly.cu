@@ -835,7 +835,7 @@ void Field::poly_recip_on(const double2* X, double2* Y, int M, cplx<R>* grid, cu
     t.T = 8;
     t.cap = pcand_cap_;
     const size_t shm = sizeof(cplx<R>) * (512 + 3 * size_t(t.cap)) * CM + sizeof(int) * 9 * t.cap;
-    MPM_CUDA(cudaFuncSetAttribute(k_poly_spread<R, CM>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(shm)));
+    set_smem_limit(k_poly_spread<R, CM>, shm);
     const R* w1 = sizeof(R) == 4 ? reinterpret_cast<const R*>(ps.w32.p) : reinterpret_cast<const R*>(ps.w64.p);
     const int ntile = ps.nb[0] * ps.nb[1] * ps.nb[2];
     {

@@ -3,9 +3,22 @@
 
 #include "mpm_common.cuh"
 
+#include <mutex>
+#include <unordered_map>
+
 namespace mpm {
 
 void note_launch() { Profiler::get().count_launch(); }
+
+void raise_smem_limit(const void* kernel, size_t bytes) {
+    static std::mutex mu;
+    static std::unordered_map<const void*, size_t> set;
+    std::lock_guard<std::mutex> g(mu);
+    size_t& cur = set[kernel];
+    if (bytes <= cur) return;
+    MPM_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(bytes)));
+    cur = bytes;
+}
 
 Profiler& Profiler::get() {
     static Profiler p;
