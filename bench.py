@@ -272,15 +272,16 @@ def measured_peaks():
 
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) per algorithmic
 # byte of a stage's kernels, from ncu captures of one launch of each kernel
-# on the same workload (monolayer: x and y transforms of a 25-column matvec,
-# 522.6 MB of DRAM traffic for 632.4 MB algorithmic; polydisperse packing:
-# spread 1892 MB for 1962 MB, plain axis pass 3811 MB for 3870 MB).  Traffic
-# scales with the columns a launch carries, so a stage's traffic per launch
-# is this ratio times its algorithmic bytes per launch.  Below 1: the last
-# writes of a launch are still in L2 when the kernel ends.
+# on the same workload (monolayer: the x transform of a 9-column seed apply,
+# 2.164 MB of DRAM traffic for 4.216 MB algorithmic, the grid's writes
+# absorbed by L2; polydisperse packing: spread 1892 MB for 1962 MB, plain
+# axis pass 3811 MB for 3870 MB).  Traffic scales with the columns a launch
+# carries, so a stage's traffic per launch is this ratio times its
+# algorithmic bytes per launch.  Below 1: the last writes of a launch are
+# still in L2 when the kernel ends.
 TRAFFIC_PER_ALG_BYTE = {
-    ("monolayer", "fft_fwd"): 522.6 / 632.4,
-    ("monolayer", "fft_inv"): 522.2 / 632.4,
+    ("monolayer", "fft_fwd"): 2.164 / 4.216,
+    ("monolayer", "fft_inv"): 2.164 / 4.216,
     ("poly3d", "spread"): 1892.0 / 1962.0,
     ("poly3d", "fft_fwd"): 3811.0 / 3870.0,
     ("poly3d", "fft_inv"): 3811.0 / 3870.0,

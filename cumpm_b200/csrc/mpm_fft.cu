@@ -1465,7 +1465,20 @@ void AxisFFT::launch_line(cplx<R>* data, size_t es, int ncols, size_t os, int no
     // the prime-pass tables go to shared memory when small (else the pass
     // indexes the line's own twiddles)
     FftFactors f = f_;
-    const int cw = pick_cw(n, sizeof(cplx<R>), ncols, 0);
+    int cw = pick_cw(n, sizeof(cplx<R>), ncols, 0);
+    {
+        // few lines in all (a batch of a few grid columns): fewer columns per
+        // CTA, so that at least two CTAs per SM share the lines (a heuristic
+        // on the first device's SM count)
+        static const int sms = [] {
+            int d = 0, v = 148;
+            if (cudaGetDevice(&d) != cudaSuccess ||
+                cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, d) != cudaSuccess)
+                v = 148;
+            return v;
+        }();
+        while (cw > 4 && (long long)nouter * ((ncols + cw - 1) / cw) < 2LL * sms) cw /= 2;
+    }
     // (only when that costs no columns per CTA)
     if (fft_smem(n, cw, sizeof(cplx<R>), f.pt_total) > kFftSmemBudget) f.pt_total = 0;
     const int pt_total = f.pt_total;

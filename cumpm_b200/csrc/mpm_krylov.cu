@@ -386,8 +386,18 @@ __global__ void k_arn_update(double2* __restrict__ V, size_t vstride, int k, con
         if (pass == 1) *w = make_double2(0, 0);
         return;
     }
-    double2 acc = make_double2(0, 0);
-    for (int i = 0; i <= k; ++i) acc += V[size_t(i) * vstride + t] * h[size_t(i) * M + m];
+    // four independent partial sums, so that a thread has four loads of V
+    // in flight (the sum's order is fixed)
+    double2 a0 = make_double2(0, 0), a1 = a0, a2 = a0, a3 = a0;
+    int i = 0;
+    for (; i + 3 <= k; i += 4) {
+        a0 += V[size_t(i) * vstride + t] * h[size_t(i) * M + m];
+        a1 += V[size_t(i + 1) * vstride + t] * h[size_t(i + 1) * M + m];
+        a2 += V[size_t(i + 2) * vstride + t] * h[size_t(i + 2) * M + m];
+        a3 += V[size_t(i + 3) * vstride + t] * h[size_t(i + 3) * M + m];
+    }
+    for (; i <= k; ++i) a0 += V[size_t(i) * vstride + t] * h[size_t(i) * M + m];
+    const double2 acc = (a0 + a1) + (a2 + a3);
     double2 v = *w - acc;
     if (s.reorth != 1) v = v * inv_nu[m];
     *w = v;
