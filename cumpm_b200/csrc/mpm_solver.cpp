@@ -249,7 +249,7 @@ void DipoleSolver::solve_all_device(const std::vector<cdouble>& init, std::vecto
         dev_eps_ = true;
     }
     dInit_.ensure(sizeof(double2) * N_ * K * 3);
-    hX_.ensure(sizeof(cdouble) * N_ * K * 3);
+    hX_.ensure(bytes);   // the init upload now, the frame's dipoles after the solve
     std::copy(init.begin(), init.begin() + N_ * K * 3, hX_.as<cdouble>());
     MPM_CUDA(cudaMemcpyAsync(dInit_.p, hX_.p, sizeof(double2) * N_ * K * 3, cudaMemcpyHostToDevice, stream_));
     const long long n = (long long)rows * M;
@@ -272,8 +272,13 @@ void DipoleSolver::solve_all_device(const std::vector<cdouble>& init, std::vecto
     dFrame_.ensure(bytes);
     k_to_frame<<<nblk_s(n, 256), 256, 0, stream_>>>(dX_.as<double2>(), M, int(N_), int(K), dFrame_.as<double2>());
     MPM_LAUNCH();
-    MPM_CUDA(cudaMemcpyAsync(frame_dip.data(), dFrame_.p, bytes, cudaMemcpyDeviceToHost, stream_));
+    // into pinned memory at full link speed, then one copy into the frame
+    // (frame_dip arrives empty: no zero fill first)
+    // (hX_ last held the init upload, earlier on this stream)
+    MPM_CUDA(cudaMemcpyAsync(hX_.p, dFrame_.p, bytes, cudaMemcpyDeviceToHost, stream_));
     MPM_CUDA(cudaStreamSynchronize(stream_));
+    const cdouble* hf = hX_.as<cdouble>();
+    frame_dip.assign(hf, hf + rows * M);
     // particle averages per (frequency, polarisation, component)
     for (size_t f = 0; f < W; ++f) {
         const cdouble* src = frame_dip.data() + f * N_ * K * 3;
@@ -479,10 +484,13 @@ void DipoleSolver::compute(const std::vector<double>& x, const std::vector<doubl
             std::copy(pq.begin(), pq.begin() + Nq_ * K * 5, init.begin() + N_ * K * 3);
         }
     }
-    std::vector<cdouble> frame_cap(W * K * 3, 0.0), frame_dip(W * N_ * K * 3, 0.0), frame_quad(W * Nq_ * K * 5, 0.0);
+    const bool dev_batch = device_batch_ok();
+    std::vector<cdouble> frame_cap(W * K * 3, 0.0), frame_quad(W * Nq_ * K * 5, 0.0);
+    std::vector<cdouble> frame_dip;   // the device batch fills it in one copy
+    if (!dev_batch) frame_dip.assign(W * N_ * K * 3, 0.0);
     print("Wavenumber:");
     indent_++;
-    if (device_batch_ok()) {
+    if (dev_batch) {
         solve_all_device(init, frame_cap, frame_dip);
     } else if (opt_.batch_all) {
         std::vector<size_t> fr(W);
