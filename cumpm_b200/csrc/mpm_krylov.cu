@@ -72,7 +72,10 @@ __global__ void __launch_bounds__(256) k_dots1s(const double2* __restrict__ V, s
         for (size_t t = size_t(blockIdx.x) * L + j; t < n; t += size_t(gridDim.x) * L) {
             double2 wv = w[t];
             if (shift >= 0) wv -= V[size_t(shift) * vstride + t];
-            for (int k = 0; k < nv; ++k) {
+            // a fixed trip count, so that the group's loads issue together
+#pragma unroll
+            for (int k = 0; k < 8; ++k) {
+                if (k >= nv) break;
                 const double2 v = (shift >= 0 && i0 + k == nvec - 1) ? wv : V[size_t(i0 + k) * vstride + t];
                 if (conj) acc[k] += conjmul(v, wv);
                 else acc[k] += v * wv;
@@ -240,6 +243,7 @@ __device__ void gm_givens(GState& s, const double2* __restrict__ h, double wn, d
     // the previous rotations applied down the column, the running entry in
     // a register (the column's inputs and the rotations are independent loads)
     double2 carry = h[m];
+#pragma unroll 4
     for (int i = 0; i < k; ++i) {
         const double2 h2 = h[size_t(i + 1) * M + m];
         const double c = csm[i];
