@@ -1170,58 +1170,11 @@ void BatchSolver::gmres_shifted(Field& F, const double2* b, double2* x, int M, c
     for (int gi = 0; gi < G; ++gi) cyc[gi] = hbs[gi] > 0.0 && used[gi];
     const int vb = nblk((long long)ns, 256);
     const int fthr = std::min(1024, ((std::max(M, G) + 31) / 32) * 32);
-    // The seeds' operator apply (spread to contraction, and the real-space
-    // sum on the field's second stream) captured once as a CUDA graph on
-    // fixed buffers and replayed every Arnoldi step: one launch for the
-    // apply's kernels.  Every buffer the apply uses is sized by a first
-    // apply before the capture, and nothing reallocates them until this
-    // solve returns.  Not while the stage timers record (their events would
-    // land in the graph); if the capture is refused the plain apply runs.
-    cudaGraphExec_t gexec = nullptr;
-    long long glaunches = 0;
-    if (!Profiler::get().enabled()) {
-        xc_.ensure(sizeof(double2) * ns);
-        yc_.ensure(sizeof(double2) * size_t(F.rows_out()) * G);
-        MPM_CUDA(cudaMemsetAsync(xc_.p, 0, sizeof(double2) * ns, s));
-        F.apply(xc_.as<double2>(), yc_.as<double2>(), G, scs, true, r32, re32, s);
-        MPM_CUDA(cudaStreamSynchronize(s));
-        const long long before = Profiler::get().launches();
-        cudaGraph_t graph = nullptr;
-        if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
-            bool ok = true;
-            try {
-                F.apply(xc_.as<double2>(), yc_.as<double2>(), G, scs, true, r32, re32, s);
-            } catch (const std::exception&) {
-                ok = false;
-            }
-            if (cudaStreamEndCapture(s, &graph) != cudaSuccess) ok = false;
-            if (ok && graph && cudaGraphInstantiate(&gexec, graph, 0) != cudaSuccess) gexec = nullptr;
-            if (graph) cudaGraphDestroy(graph);
-        }
-        (void)cudaGetLastError();   // a refused capture's error: the plain apply runs instead
-        glaunches = Profiler::get().launches() - before;
-    }
-    struct GraphGuard {
-        cudaGraphExec_t& e;
-        ~GraphGuard() {
-            if (e) cudaGraphExecDestroy(e);
-        }
-    } gguard{gexec};
     for (int k = 0; k < restart; ++k) {
         if (std::count(cyc.begin(), cyc.end(), 1) == 0) break;
         double2* Vk = V + size_t(k) * ns;
         double2* w = V + size_t(k + 1) * ns;
-        if (gexec) {
-            // every seed goes through the graph; the ones no longer cycling
-            // are masked by the steps below
-            MPM_CUDA(cudaMemcpyAsync(xc_.p, Vk, sizeof(double2) * ns, cudaMemcpyDeviceToDevice, s));
-            MPM_CUDA(cudaGraphLaunch(gexec, s));
-            MPM_CUDA(cudaMemcpyAsync(w, yc_.p, sizeof(double2) * ns, cudaMemcpyDeviceToDevice, s));
-            for (long long q = 0; q < glaunches; ++q) note_launch();
-            st.column_matvecs += G;
-        } else {
-            st.column_matvecs += apply_cols(F, Vk, w, G, scs, true, r32, re32, cyc.data(), opt.compact, s);
-        }
+        st.column_matvecs += apply_cols(F, Vk, w, G, scs, true, r32, re32, cyc.data(), opt.compact, s);
         st.matvecs++;
         auto seed_pass = [&](int pass, const double2* hv) {
             // (every seed takes both projections: the members' Givens updates
