@@ -1086,13 +1086,18 @@ __global__ void k_cell_keys(const double* __restrict__ xyz, int n, CellArgs a, i
 // For each target: sources within rc (minimum image, d^2 <= rc^2 and then
 // d < rc as in neighbor_list.cu:186-223 + the pair kernels' cut), visiting
 // the distinct neighbouring cells.  pass 0 counts, pass 1 writes pair data.
+// Warp per target: the lanes take a cell's candidates 32 at a time, in
+// order, and a ballot places the accepted ones, so the pairs of a target
+// come out in cell-list order (the order a single thread walking the cells
+// would give).  pass 0 counts, pass 1 writes at off[j].
 __global__ void k_pairs(const double* __restrict__ src, int ns, const double* __restrict__ tgt, int nt, CellArgs a,
                         const int* __restrict__ cstart, const int* __restrict__ cend,
                         const int* __restrict__ sidx, double rc, int solver_ax, int pass,
                         int* __restrict__ cnt, const int* __restrict__ off, int* __restrict__ psrc,
                         double* __restrict__ pgeo /*[P][4]: dx,dy,dz,d*/) {
-    const int j = blockIdx.x * blockDim.x + threadIdx.x;
-    if (j >= nt) return;
+    const int j = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (j >= nt) return;   // whole warps leave together
     const double xj = tgt[j], yj = tgt[nt + j], zj = tgt[2 * nt + j];
     const int c[3] = {cell_of(xj, a.L[0], a.cs[0], a.nc[0]), cell_of(yj, a.L[1], a.cs[1], a.nc[1]),
                       cell_of(zj, a.L[2], a.cs[2], a.nc[2])};
@@ -1106,7 +1111,7 @@ __global__ void k_pairs(const double* __restrict__ src, int ns, const double* __
             if (!seen) lst[d][nl[d]++] = v;
         }
     }
-    int count = 0;
+    int count = 0;   // the same in every lane
     const int base = pass ? off[j] : 0;
     const double rc2 = rc * rc;
     for (int a2 = 0; a2 < nl[2]; ++a2)
@@ -1116,29 +1121,40 @@ __global__ void k_pairs(const double* __restrict__ src, int ns, const double* __
                 const int s0 = cstart[key];
                 if (s0 < 0) continue;
                 const int s1 = cend[key];
-                for (int k = s0; k < s1; ++k) {
-                    const int i = sidx[k];
-                    if (solver_ax && i == j) continue;
-                    double dx = src[i] - xj, dy = src[ns + i] - yj, dz = src[2 * ns + i] - zj;
-                    dx -= a.L[0] * round(dx / a.L[0]);
-                    dy -= a.L[1] * round(dy / a.L[1]);
-                    dz -= a.L[2] * round(dz / a.L[2]);
-                    const double d2 = dx * dx + dy * dy + dz * dz;
-                    if (d2 > rc2) continue;
-                    const double d = sqrt(d2);
-                    if (!(d < rc)) continue;
-                    if (pass) {
-                        const int o = base + count;
+                for (int k0 = s0; k0 < s1; k0 += 32) {
+                    const int k = k0 + lane;
+                    bool keep = false;
+                    int i = 0;
+                    double dx = 0, dy = 0, dz = 0, d = 0;
+                    if (k < s1) {
+                        i = sidx[k];
+                        if (!(solver_ax && i == j)) {
+                            dx = src[i] - xj;
+                            dy = src[ns + i] - yj;
+                            dz = src[2 * ns + i] - zj;
+                            dx -= a.L[0] * round(dx / a.L[0]);
+                            dy -= a.L[1] * round(dy / a.L[1]);
+                            dz -= a.L[2] * round(dz / a.L[2]);
+                            const double d2 = dx * dx + dy * dy + dz * dz;
+                            if (d2 <= rc2) {
+                                d = sqrt(d2);
+                                keep = d < rc;
+                            }
+                        }
+                    }
+                    const unsigned hit = __ballot_sync(0xffffffffu, keep);
+                    if (pass && keep) {
+                        const int o = base + count + __popc(hit & ((1u << lane) - 1u));
                         psrc[o] = i;
                         pgeo[4 * size_t(o) + 0] = dx;
                         pgeo[4 * size_t(o) + 1] = dy;
                         pgeo[4 * size_t(o) + 2] = dz;
                         pgeo[4 * size_t(o) + 3] = d;
                     }
-                    ++count;
+                    count += __popc(hit);
                 }
             }
-    if (!pass) cnt[j] = count;
+    if (!pass && lane == 0) cnt[j] = count;
 }
 
 __device__ double table_at(double r, const double* __restrict__ rt, const double* __restrict__ y) {
@@ -1854,7 +1870,7 @@ void Field::build_pairs(cudaStream_t s) {
     pair_cnt_.ensure(sizeof(int) * (nt + 1));
     pair_off_.ensure(sizeof(int) * (nt + 1));
     MPM_CUDA(cudaMemsetAsync(pair_cnt_.p, 0, sizeof(int) * (nt + 1), s));
-    k_pairs<<<nblk(nt, 128), 128, 0, s>>>(sources_.xyz.as<double>(), ns, tg.xyz.as<double>(), nt, a,
+    k_pairs<<<nblk((long long)nt * 32, 128), 128, 0, s>>>(sources_.xyz.as<double>(), ns, tg.xyz.as<double>(), nt, a,
                                            cell_start_.as<int>(), cell_end_.as<int>(), cell_idx_s_.as<int>(), rc,
                                            spec_.solver_ax ? 1 : 0, 0, pair_cnt_.as<int>(), nullptr, nullptr,
                                            nullptr);
@@ -1871,7 +1887,7 @@ void Field::build_pairs(cudaStream_t s) {
     pair_src_.ensure(sizeof(int) * np);
     DevBuf& geo = pair_geo_;
     geo.ensure(sizeof(double) * 4 * np);
-    k_pairs<<<nblk(nt, 128), 128, 0, s>>>(sources_.xyz.as<double>(), ns, tg.xyz.as<double>(), nt, a,
+    k_pairs<<<nblk((long long)nt * 32, 128), 128, 0, s>>>(sources_.xyz.as<double>(), ns, tg.xyz.as<double>(), nt, a,
                                            cell_start_.as<int>(), cell_end_.as<int>(), cell_idx_s_.as<int>(), rc,
                                            spec_.solver_ax ? 1 : 0, 1, nullptr, pair_off_.as<int>(),
                                            pair_src_.as<int>(), geo.as<double>());
